@@ -1,0 +1,90 @@
+"""ctypes binding of libnsgpu.so (the C ABI in include/nsgpu.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+it is missing, importing the solver raises, so a GPU run can never silently
+fall back to a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libnsgpu.so"
+
+c_int = ctypes.c_int
+c_ll = ctypes.c_longlong
+c_double = ctypes.c_double
+c_void_p = ctypes.c_void_p
+P = ctypes.POINTER
+
+NSG_OK = 0
+NSG_ERR_INVALID = 1
+NSG_ERR_CUDA = 2
+NSG_ERR_NOMEM = 8
+NSG_SINGULAR = 102
+NSG_REORDER = 103
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "nsg_last_error": (ctypes.c_char_p, []),
+    "nsg_topology_order": (c_int, [c_int, c_int, P(c_int), P(c_int), P(c_double), c_double,
+                                   P(c_void_p)]),
+    "nsg_topology_numeric": (c_int, [c_void_p, P(c_double), c_double, P(c_int)]),
+    "nsg_topology_import": (c_int, [c_int, c_int, P(c_int), P(c_int), c_int, P(c_int), P(c_int),
+                                    P(c_int), P(c_void_p)]),
+    "nsg_topology_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_ll), P(c_int),
+                                  P(c_int), P(c_int)]),
+    "nsg_topology_export": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int), P(c_int)]),
+    "nsg_topology_free": (None, [c_void_p]),
+    "nsg_batch_create": (c_int, [c_int, P(c_void_p), P(c_void_p)]),
+    "nsg_batch_free": (None, [c_void_p]),
+    "nsg_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll)]),
+    "nsg_batch_refactor": (c_int, [c_void_p, c_void_p, c_double, c_int, c_void_p, c_void_p,
+                                   c_void_p]),
+    "nsg_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "nsg_batch_solve_transposed": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "nsg_batch_lu": (c_void_p, [c_void_p]),
+    "nsg_batch_lu_to_host": (c_int, [c_void_p, P(c_double)]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libnsgpu.so once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m neospice_b200.build`")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class NsgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def check(code: int) -> int:
+    if code != NSG_OK:
+        raise NsgError(code, lib().nsg_last_error().decode())
+    return code
+
+
+def iptr(a):
+    return a.ctypes.data_as(P(c_int))
+
+
+def dptr(a):
+    return a.ctypes.data_as(P(c_double))
+
+
+def llptr(a):
+    return a.ctypes.data_as(P(c_ll))

@@ -1,0 +1,305 @@
+// C ABI of libnsgpu (declared in include/nsgpu.h): host symbolic phase, batch
+// set-up and the launches of the batched refactor and sweeps.
+#include "nsgpu.h"
+
+#include "host/plan.hpp"
+#include "host/sparse_order.hpp"
+#include "kernels/lu_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace nsg {
+cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
+                            int count, const double* A, double* LU, double diag_gmin,
+                            int check_pivots, double rel_threshold, int32_t* status,
+                            int32_t* fail_step, cudaStream_t stream);
+cudaError_t launch_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
+                         int count, const double* LU, double* X, double* W, bool transposed,
+                         cudaStream_t stream);
+}  // namespace nsg
+
+struct nsg_topology {
+    std::unique_ptr<nsg::MarkowitzOrder> engine;  // null for an imported topology
+    std::vector<int32_t> slot_elem;
+    nsg::TopologyPlan plan;
+};
+
+struct nsg_batch {
+    int count = 0;
+    std::vector<long long> a_off, x_off, lu_off;
+    int32_t* d_pool = nullptr;
+    nsg::PlanDesc* d_plans = nullptr;
+    nsg::InstDesc* d_insts = nullptr;
+    double* d_lu = nullptr;
+    double* d_work = nullptr;
+    ~nsg_batch() {
+        cudaFree(d_pool);
+        cudaFree(d_plans);
+        cudaFree(d_insts);
+        cudaFree(d_lu);
+        cudaFree(d_work);
+    }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+// Run a body, mapping C++ exceptions to status codes.
+template <class F>
+int guarded(const char* where, F&& body) {
+    try {
+        g_last_error.clear();
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(NSG_ERR_NOMEM, std::string(where) + ": out of host memory");
+    } catch (const std::exception& e) {
+        return fail(NSG_ERR_INVALID, std::string(where) + ": " + e.what());
+    }
+}
+
+int cuda_fail(const char* where, cudaError_t e) {
+    return fail(e == cudaErrorMemoryAllocation ? NSG_ERR_NOMEM : NSG_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), count * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (src) e = cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// NeoSolver::numeric's load + preorder + gmin + order_and_factor on the
+// host engine (neo_solver.cpp:219-245).
+int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin) {
+    auto& mo = *t.engine;
+    mo.clear_fillins();
+    for (size_t k = 0; k < t.slot_elem.size(); ++k) mo.value(t.slot_elem[k]) = values[k];
+    mo.mna_preorder();
+    mo.add_diag_gmin(diag_gmin);
+    const nsg::OrderStatus st = mo.order_and_factor(1e-3, 1e-13, true);
+    if (st == nsg::OrderStatus::no_memory) return NSG_ERR_NOMEM;
+    if (st == nsg::OrderStatus::singular) return NSG_SINGULAR;
+    return NSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nsg_last_error(void) { return g_last_error.c_str(); }
+
+int nsg_topology_order(int n, int nnz, const int* col_ptr, const int* row_idx,
+                       const double* values, double diag_gmin, nsg_topology** out) {
+    return guarded("nsg_topology_order", [&]() -> int {
+        if (!out || n <= 0 || nnz <= 0 || !col_ptr || !row_idx || !values)
+            return fail(NSG_ERR_INVALID, "nsg_topology_order: bad arguments");
+        *out = nullptr;
+        if (col_ptr[0] != 0 || col_ptr[n] != nnz)
+            return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr does not span nnz");
+        auto t = std::make_unique<nsg_topology>();
+        t->engine = std::make_unique<nsg::MarkowitzOrder>(n);
+        t->slot_elem.resize(nnz);
+        for (int j = 0; j < n; ++j) {
+            if (col_ptr[j + 1] < col_ptr[j])
+                return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr not monotone");
+            for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) {
+                if (row_idx[p] < 0 || row_idx[p] >= n ||
+                    (p > col_ptr[j] && row_idx[p] <= row_idx[p - 1]))
+                    return fail(NSG_ERR_INVALID, "nsg_topology_order: rows not sorted/unique");
+                t->slot_elem[p] = t->engine->get_element(row_idx[p] + 1, j + 1);
+            }
+        }
+        const int rc = numeric_on_engine(*t, values, diag_gmin);
+        if (rc == NSG_SINGULAR) return fail(NSG_SINGULAR, "nsg_topology_order: singular matrix");
+        if (rc != NSG_OK) return fail(rc, "nsg_topology_order: ordering failed");
+        t->plan = nsg::build_plan(*t->engine, t->slot_elem);
+        *out = t.release();
+        return NSG_OK;
+    });
+}
+
+int nsg_topology_numeric(nsg_topology* topo, const double* values, double diag_gmin,
+                         int* reordered) {
+    return guarded("nsg_topology_numeric", [&]() -> int {
+        if (!topo || !values) return fail(NSG_ERR_INVALID, "nsg_topology_numeric: bad arguments");
+        if (!topo->engine)
+            return fail(NSG_ERR_INVALID,
+                        "nsg_topology_numeric: imported topology has no ordering state");
+        const int before = topo->engine->fillin_count();
+        const int rc = numeric_on_engine(*topo, values, diag_gmin);
+        const int step = topo->engine->reorder_step();
+        if (reordered) *reordered = step;
+        if (rc != NSG_OK) return fail(rc, "nsg_topology_numeric: singular matrix");
+        if (step != 0 || topo->engine->fillin_count() != before)
+            topo->plan = nsg::build_plan(*topo->engine, topo->slot_elem);
+        return NSG_OK;
+    });
+}
+
+int nsg_topology_import(int n, int nnz, const int* int_to_ext_row, const int* int_to_ext_col,
+                        int n_elem, const int* elem_row, const int* elem_col,
+                        const int* slot_to_elem, nsg_topology** out) {
+    return guarded("nsg_topology_import", [&]() -> int {
+        if (!out || !int_to_ext_row || !int_to_ext_col || !elem_row || !elem_col || !slot_to_elem)
+            return fail(NSG_ERR_INVALID, "nsg_topology_import: null argument");
+        *out = nullptr;
+        auto t = std::make_unique<nsg_topology>();
+        t->plan = nsg::build_plan_from_structure(n, nnz, int_to_ext_row, int_to_ext_col, n_elem,
+                                                 elem_row, elem_col, slot_to_elem);
+        *out = t.release();
+        return NSG_OK;
+    });
+}
+
+int nsg_topology_info(const nsg_topology* topo, int* n, int* nnz, int* nnz_lu,
+                      long long* updates, int* col_levels, int* fwd_levels, int* bwd_levels) {
+    if (!topo) return fail(NSG_ERR_INVALID, "nsg_topology_info: null topology");
+    const auto& p = topo->plan;
+    if (n) *n = p.n;
+    if (nnz) *nnz = p.nnz_a;
+    if (nnz_lu) *nnz_lu = p.nnz_lu;
+    if (updates) *updates = p.updates;
+    if (col_levels) *col_levels = static_cast<int>(p.col_lev_ptr.size()) - 1;
+    if (fwd_levels) *fwd_levels = static_cast<int>(p.fwd_lev_ptr.size()) - 1;
+    if (bwd_levels) *bwd_levels = static_cast<int>(p.bwd_lev_ptr.size()) - 1;
+    return NSG_OK;
+}
+
+int nsg_topology_export(const nsg_topology* topo, int* int_to_ext_row, int* int_to_ext_col,
+                        int* elem_row, int* elem_col, int* slot_to_elem) {
+    if (!topo) return fail(NSG_ERR_INVALID, "nsg_topology_export: null topology");
+    const auto& p = topo->plan;
+    for (int i = 0; i < p.n; ++i) {
+        if (int_to_ext_row) int_to_ext_row[i] = p.perm_row[i] + 1;
+        if (int_to_ext_col) int_to_ext_col[i] = p.perm_col[i] + 1;
+    }
+    for (int j = 0; j < p.n; ++j)
+        for (int q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
+            if (elem_row) elem_row[q] = p.row_idx[q] + 1;
+            if (elem_col) elem_col[q] = j + 1;
+        }
+    if (slot_to_elem) std::memcpy(slot_to_elem, p.a_to_lu.data(), sizeof(int) * p.nnz_a);
+    return NSG_OK;
+}
+
+void nsg_topology_free(nsg_topology* topo) { delete topo; }
+
+int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
+    return guarded("nsg_batch_create", [&]() -> int {
+        if (!out || count <= 0 || !topos)
+            return fail(NSG_ERR_INVALID, "nsg_batch_create: bad arguments");
+        *out = nullptr;
+        auto b = std::make_unique<nsg_batch>();
+        b->count = count;
+        std::unordered_map<const nsg_topology*, int32_t> plan_of;
+        std::vector<nsg::PlanDesc> plans;
+        std::vector<int32_t> pool;
+        std::vector<nsg::InstDesc> insts(count);
+        b->a_off.assign(count + 1, 0);
+        b->x_off.assign(count + 1, 0);
+        b->lu_off.assign(count + 1, 0);
+        for (int i = 0; i < count; ++i) {
+            const nsg_topology* t = topos[i];
+            if (!t) return fail(NSG_ERR_INVALID, "nsg_batch_create: null topology");
+            auto it = plan_of.find(t);
+            if (it == plan_of.end()) {
+                nsg::PlanDesc d{};
+                const auto& p = t->plan;
+                d.n = p.n;
+                d.nnz_a = p.nnz_a;
+                d.nnz_lu = p.nnz_lu;
+                d.n_col_lev = static_cast<int32_t>(p.col_lev_ptr.size()) - 1;
+                d.n_fwd_lev = static_cast<int32_t>(p.fwd_lev_ptr.size()) - 1;
+                d.n_bwd_lev = static_cast<int32_t>(p.bwd_lev_ptr.size()) - 1;
+                d.n_tbw_lev = static_cast<int32_t>(p.tbw_lev_ptr.size()) - 1;
+                p.append_to(pool, d.off);
+                it = plan_of.emplace(t, static_cast<int32_t>(plans.size())).first;
+                plans.push_back(d);
+            }
+            const auto& p = t->plan;
+            insts[i].plan = it->second;
+            insts[i].a_off = b->a_off[i];
+            insts[i].lu_off = b->lu_off[i];
+            insts[i].x_off = b->x_off[i];
+            insts[i].w_off = b->x_off[i];
+            b->a_off[i + 1] = b->a_off[i] + p.nnz_a;
+            b->x_off[i + 1] = b->x_off[i] + p.n;
+            // keep each instance's LU 32-byte aligned
+            b->lu_off[i + 1] = b->lu_off[i] + ((p.nnz_lu + 3) & ~3);
+        }
+        cudaError_t e;
+        if ((e = upload(&b->d_pool, pool.data(), pool.size())) != cudaSuccess ||
+            (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
+            (e = upload(&b->d_insts, insts.data(), insts.size())) != cudaSuccess ||
+            (e = upload<double>(&b->d_lu, nullptr, b->lu_off[count])) != cudaSuccess ||
+            (e = upload<double>(&b->d_work, nullptr, b->x_off[count])) != cudaSuccess)
+            return cuda_fail("nsg_batch_create", e);
+        *out = b.release();
+        return NSG_OK;
+    });
+}
+
+void nsg_batch_free(nsg_batch* batch) { delete batch; }
+
+int nsg_batch_layout(const nsg_batch* b, long long* value_offsets, long long* vector_offsets,
+                     long long* lu_offsets) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_batch_layout: null batch");
+    const size_t bytes = sizeof(long long) * (b->count + 1);
+    if (value_offsets) std::memcpy(value_offsets, b->a_off.data(), bytes);
+    if (vector_offsets) std::memcpy(vector_offsets, b->x_off.data(), bytes);
+    if (lu_offsets) std::memcpy(lu_offsets, b->lu_off.data(), bytes);
+    return NSG_OK;
+}
+
+int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
+                       int check_pivots, int* d_status, int* d_fail_step, void* stream) {
+    if (!b || !d_values || !d_status)
+        return fail(NSG_ERR_INVALID, "nsg_batch_refactor: null argument");
+    cudaError_t e = nsg::launch_refactor(b->d_plans, b->d_pool, b->d_insts, b->count, d_values,
+                                         b->d_lu, diag_gmin, check_pivots, 1e-3, d_status,
+                                         d_fail_step, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
+}
+
+int nsg_batch_solve(nsg_batch* b, double* d_x, void* stream) {
+    if (!b || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve: null argument");
+    cudaError_t e = nsg::launch_solve(b->d_plans, b->d_pool, b->d_insts, b->count, b->d_lu, d_x,
+                                      b->d_work, false, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve", e);
+}
+
+int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
+    if (!b || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve_transposed: null argument");
+    cudaError_t e = nsg::launch_solve(b->d_plans, b->d_pool, b->d_insts, b->count, b->d_lu, d_x,
+                                      b->d_work, true, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve_transposed", e);
+}
+
+const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
+
+int nsg_batch_lu_to_host(const nsg_batch* b, double* out) {
+    if (!b || !out) return fail(NSG_ERR_INVALID, "nsg_batch_lu_to_host: null argument");
+    cudaError_t e = cudaMemcpy(out, b->d_lu, sizeof(double) * b->lu_off[b->count],
+                               cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_lu_to_host", e);
+}
+
+}  // extern "C"

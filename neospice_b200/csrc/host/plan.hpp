@@ -1,0 +1,84 @@
+// Device plan of one factored topology: the LU pattern in pivot (internal)
+// order plus everything the batched refactor and the four triangular sweeps
+// need, as flat int32 arrays ready to upload.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace nsg {
+
+class MarkowitzOrder;
+
+struct TopologyPlan {
+    int32_t n = 0;
+    int32_t nnz_a = 0;   // slots of the caller's CSC pattern
+    int32_t nnz_lu = 0;  // originals + fill-ins
+
+    // internal index i (0-based) -> external row / column (0-based).
+    std::vector<int32_t> perm_row, perm_col;
+
+    // LU in CSC, internal order, rows ascending within a column.  In column
+    // j: positions col_ptr[j]..diag_pos[j]-1 are U (rows < j), diag_pos[j] is
+    // the pivot, diag_pos[j]+1..col_ptr[j+1]-1 are L (rows > j).
+    std::vector<int32_t> col_ptr, row_idx, diag_pos;
+
+    // Load map: per LU position, the caller's CSC slot, or -1 for a fill-in.
+    std::vector<int32_t> lu_src;
+    // Inverse: per caller slot, its LU position.
+    std::vector<int32_t> a_to_lu;
+
+    // Refactor update map.  For the U entry at position q = (r, j):
+    // upd_start[q] indexes upd_dst, where the |L(:, r)| destinations in
+    // column j of L(:, r)'s rows are stored in L(:, r)'s order.
+    std::vector<int32_t> upd_start, upd_dst;
+
+    // L by rows (strictly lower, columns ascending) and U by rows (strictly
+    // upper, columns ascending): LU position and column of each entry.
+    std::vector<int32_t> lrow_ptr, lrow_pos, lrow_col;
+    std::vector<int32_t> urow_ptr, urow_pos, urow_col;
+
+    // Level schedules (ptr over levels, then members sorted by level).
+    //   col:  column j after every r with U(r, j) != 0  (refactor and the
+    //         forward sweep of the transposed solve)
+    //   fwd:  row i after every c with L(i, c) != 0      (forward solve)
+    //   bwd:  row i after every c with U(i, c) != 0      (backward solve)
+    //   tbw:  column i after every r with L(r, i) != 0   (transposed backward)
+    std::vector<int32_t> col_lev_ptr, col_lev;
+    std::vector<int32_t> fwd_lev_ptr, fwd_lev;
+    std::vector<int32_t> bwd_lev_ptr, bwd_lev;
+    std::vector<int32_t> tbw_lev_ptr, tbw_lev;
+
+    // Algorithmic work: multiply-subtract updates of one refactor (each is
+    // 2 flops), and the reciprocal pivots.
+    int64_t updates = 0;
+
+    int64_t refactor_flops() const { return 2 * updates + n; }
+    // Compulsory bytes of one refactor: read A, write LU, the index stream
+    // (update map + LU pattern), the reciprocal diagonal.
+    int64_t refactor_bytes() const {
+        return 8LL * nnz_a + 8LL * nnz_lu + 4LL * (updates + nnz_lu + n) + 8LL * n;
+    }
+    int64_t solve_bytes() const { return 12LL * nnz_lu + 16LL * n; }
+
+    // Total int32 words this plan occupies on the device.
+    int64_t device_words() const;
+    // Append all arrays to pool; offsets (in int32 words) go to off[].
+    void append_to(std::vector<int32_t>& pool, int64_t* off) const;
+};
+
+// Build from the host ordering engine after order_and_factor.  slot_elem[k]
+// is the engine element of caller CSC slot k.
+TopologyPlan build_plan(const MarkowitzOrder& mo, const std::vector<int32_t>& slot_elem);
+
+// Build from an exported structure (the reference's own NeoSolver state):
+// elements column by column in internal order (1-based rows/cols), the slot
+// map and 1-based permutations.  Throws std::invalid_argument on a malformed
+// structure.
+TopologyPlan build_plan_from_structure(int32_t n, int32_t nnz_a,
+                                       const int32_t* int_to_ext_row,
+                                       const int32_t* int_to_ext_col,
+                                       int32_t n_elem, const int32_t* elem_row,
+                                       const int32_t* elem_col,
+                                       const int32_t* slot_to_elem);
+
+}  // namespace nsg

@@ -1,0 +1,39 @@
+// Device-side descriptors shared by the host batch code and the kernels.
+#pragma once
+#include <cstdint>
+
+namespace nsg {
+
+// Index of each plan array in PlanDesc::off; order matches the host's
+// NSG_PLAN_ARRAYS list in plan.cpp.
+enum PlanArray : int {
+    PA_perm_row, PA_perm_col, PA_col_ptr, PA_row_idx, PA_diag_pos, PA_lu_src,
+    PA_upd_start, PA_upd_dst, PA_lrow_ptr, PA_lrow_pos, PA_lrow_col, PA_urow_ptr,
+    PA_urow_pos, PA_urow_col, PA_col_lev_ptr, PA_col_lev, PA_fwd_lev_ptr, PA_fwd_lev,
+    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_COUNT
+};
+
+struct PlanDesc {
+    int32_t n, nnz_a, nnz_lu;
+    int32_t n_col_lev, n_fwd_lev, n_bwd_lev, n_tbw_lev;
+    int32_t pad;
+    int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
+};
+
+struct InstDesc {
+    int32_t plan;   // index into the PlanDesc array
+    int32_t pad;
+    int64_t a_off;   // into the caller's A values (doubles)
+    int64_t lu_off;  // into the batch's LU values
+    int64_t x_off;   // into the caller's rhs / solution vectors
+    int64_t w_off;   // into the batch's sweep workspace
+};
+
+// Per-instance status codes written by the refactor.
+enum : int32_t {
+    kStatusOk = 0,
+    kStatusSingular = 102,  // exact zero pivot (SparseError::ZeroDiag)
+    kStatusReorder = 103,   // pivot failed the relative threshold
+};
+
+}  // namespace nsg

@@ -1,0 +1,168 @@
+"""The oracle: test infrastructure, never part of the product.
+
+Two checkers, loaded with ctypes:
+
+* ``port()``  — oracle/_ref/libnsoracle.so, the plain-C restatement of the
+  reference's fixed-pivot refactor and solves (ns_oracle.c).
+* ``ref()``   — oracle/_ref/libnsref.so, the reference's own C++ sources
+  compiled by oracle/Makefile plus the export shim ref_shim.cpp.  Present only
+  where the reference sources were available at build time.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use
+this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+PORT_SO = OUT / "libnsoracle.so"
+REF_SO = OUT / "libnsref.so"
+REFERENCE_SRC = pathlib.Path("/root/reference")
+
+_V = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+
+def build(reference: bool = True) -> None:
+    """Build the C port, and the reference library when its sources exist."""
+    targets = ["port"]
+    if reference and (REFERENCE_SRC / "src").is_dir():
+        targets.append("ref")
+    subprocess.run(["make", "-s", f"-j{8}", *targets], cwd=HERE, check=True)
+
+
+_port = None
+_ref = None
+
+
+def port() -> ctypes.CDLL:
+    global _port
+    if _port is None:
+        if not PORT_SO.exists():
+            build(reference=False)
+        lib = ctypes.CDLL(str(PORT_SO))
+        lib.nso_refactor.argtypes = [_I, _I, _I, _V, _V, _V, _V, _D, _I, _V, _V]
+        lib.nso_solve.argtypes = [_I, _I, _V, _V, _V, _V, _V, _V]
+        lib.nso_solve_transposed.argtypes = [_I, _I, _V, _V, _V, _V, _V, _V]
+        _port = lib
+    return _port
+
+
+def have_ref() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(str(REF_SO))
+        lib.nsref_solver_create.restype = _V
+        lib.nsref_solver_create.argtypes = [_I, _I, _V, _V]
+        lib.nsref_solver_destroy.argtypes = [_V]
+        lib.nsref_solver_numeric.argtypes = [_V, _V, _D]
+        lib.nsref_solver_refactor.argtypes = [_V, _V, _D]
+        lib.nsref_solver_solve.argtypes = [_V, _V]
+        lib.nsref_solver_solve_transposed.argtypes = [_V, _V]
+        lib.nsref_solver_element_count.argtypes = [_V]
+        lib.nsref_solver_export.argtypes = [_V] * 7
+        lib.nsref_mesh_dc.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V, _V]
+        _ref = lib
+    return _ref
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+class Structure:
+    """A factored topology in the reference's export format (1-based)."""
+
+    def __init__(self, n, int_to_ext_row, int_to_ext_col, elem_row, elem_col, slot_to_elem):
+        self.n = int(n)
+        self.int_to_ext_row = np.ascontiguousarray(int_to_ext_row, np.int32)
+        self.int_to_ext_col = np.ascontiguousarray(int_to_ext_col, np.int32)
+        self.elem_row = np.ascontiguousarray(elem_row, np.int32)
+        self.elem_col = np.ascontiguousarray(elem_col, np.int32)
+        self.slot_to_elem = np.ascontiguousarray(slot_to_elem, np.int32)
+
+    @property
+    def n_elem(self):
+        return len(self.elem_row)
+
+    def same_as(self, other) -> bool:
+        return all(np.array_equal(getattr(self, k), getattr(other, k)) for k in
+                   ("int_to_ext_row", "int_to_ext_col", "elem_row", "elem_col", "slot_to_elem"))
+
+
+# --- the C port ------------------------------------------------------------
+
+def port_refactor(st: Structure, a, gmin=0.0, check_pivots=False):
+    a = np.ascontiguousarray(a, np.float64)
+    lu = np.zeros(st.n_elem)
+    step = ctypes.c_int(-1)
+    rc = port().nso_refactor(st.n, len(st.slot_to_elem), st.n_elem, _p(st.elem_row),
+                             _p(st.elem_col), _p(st.slot_to_elem), _p(a), gmin,
+                             int(check_pivots), _p(lu), ctypes.addressof(step))
+    return rc, lu, step.value
+
+
+def port_solve(st: Structure, lu, b, transposed=False):
+    x = np.array(b, np.float64, copy=True)
+    fn = port().nso_solve_transposed if transposed else port().nso_solve
+    rc = fn(st.n, st.n_elem, _p(st.elem_row), _p(st.elem_col), _p(st.int_to_ext_row),
+            _p(st.int_to_ext_col), _p(np.ascontiguousarray(lu, np.float64)), _p(x))
+    if rc != 0:
+        raise RuntimeError(f"oracle solve failed: {rc}")
+    return x
+
+
+# --- the reference itself ----------------------------------------------------
+
+class RefSolver:
+    """The reference's NeoSolver on a CSC pattern, through the export shim."""
+
+    def __init__(self, n, col_ptr, row_idx):
+        self.n = int(n)
+        self.col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+        self.row_idx = np.ascontiguousarray(row_idx, np.int32)
+        self.h = ref().nsref_solver_create(self.n, len(self.row_idx), _p(self.col_ptr),
+                                           _p(self.row_idx))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.nsref_solver_destroy(self.h)
+            self.h = None
+
+    def numeric(self, values, gmin=0.0) -> int:
+        v = np.ascontiguousarray(values, np.float64)
+        return ref().nsref_solver_numeric(self.h, _p(v), gmin)
+
+    def refactorize(self, values, gmin=0.0) -> int:
+        v = np.ascontiguousarray(values, np.float64)
+        return ref().nsref_solver_refactor(self.h, _p(v), gmin)
+
+    def solve(self, b, transposed=False):
+        x = np.array(b, np.float64, copy=True)
+        fn = ref().nsref_solver_solve_transposed if transposed else ref().nsref_solver_solve
+        if fn(self.h, _p(x)) != 0:
+            raise RuntimeError("reference solve failed")
+        return x
+
+    def export(self):
+        ne = ref().nsref_solver_element_count(self.h)
+        n = self.n
+        r = np.zeros(n, np.int32)
+        c = np.zeros(n, np.int32)
+        er = np.zeros(ne, np.int32)
+        ec = np.zeros(ne, np.int32)
+        ev = np.zeros(ne)
+        se = np.zeros(len(self.row_idx), np.int32)
+        ref().nsref_solver_export(self.h, _p(r), _p(c), _p(er), _p(ec), _p(ev), _p(se))
+        return Structure(n, r, c, er, ec, se), ev

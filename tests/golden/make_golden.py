@@ -1,0 +1,70 @@
+"""Generate tests/golden/solver_cases.npz from the reference itself.
+
+Runs the reference's own NeoSolver (oracle/_ref/libnsref.so, built from the
+reference sources by oracle/Makefile) on seeded matrices and records, per
+case: the CSC pattern and values, the exported symbolic structure after
+NeoSolver::numeric (pivot permutations, LU pattern, slot map), the factored
+values, the values after NeoSolver::refactorize on perturbed values, and the
+solutions of solve and solve_transposed.  Run from the repository root:
+``python tests/golden/make_golden.py``.
+"""
+from __future__ import annotations
+
+import pathlib
+import sys
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import oracle  # noqa: E402
+from matrices import banded, mna_mesh, random_matrix  # noqa: E402
+
+
+def cases():
+    rng = np.random.default_rng(20261203)
+    out = []
+    for k in range(36):
+        n = int(rng.integers(2, 48))
+        out.append(random_matrix(rng, n, float(rng.uniform(0.05, 0.4)), diag_dominant=(k % 2 == 0),
+                                 zero_diag_frac=float(rng.uniform(0.0, 0.4)), integer=(k % 5 == 0)))
+    for side, nv in ((3, 1), (6, 2), (9, 3), (12, 1)):
+        out.append(mna_mesh(rng, side, nv))
+    out.append(banded(100, 7, seed=1))
+    return out
+
+
+def main():
+    oracle.build()
+    rng = np.random.default_rng(7)
+    rec = {}
+    kept = 0
+    for (n, cp, ri, vals) in cases():
+        rs = oracle.RefSolver(n, cp, ri)
+        if rs.numeric(vals) != 0:
+            continue
+        st, lu0 = rs.export()
+        vals2 = vals * np.exp(0.05 * rng.standard_normal(len(vals)))
+        rc = rs.refactorize(vals2)
+        _, lu1 = rs.export()
+        b = rng.standard_normal(n)
+        x = rs.solve(b)
+        xt = rs.solve(b, transposed=True)
+        p = f"c{kept:02d}_"
+        rec.update({p + "n": np.int32(n), p + "col_ptr": cp, p + "row_idx": ri, p + "vals": vals,
+                    p + "vals2": vals2, p + "refactor_rc": np.int32(rc),
+                    p + "int_to_ext_row": st.int_to_ext_row, p + "int_to_ext_col": st.int_to_ext_col,
+                    p + "elem_row": st.elem_row, p + "elem_col": st.elem_col,
+                    p + "slot_to_elem": st.slot_to_elem, p + "lu_numeric": lu0,
+                    p + "lu_refactor": lu1, p + "b": b, p + "x": x, p + "xt": xt})
+        kept += 1
+    rec["count"] = np.int32(kept)
+    path = pathlib.Path(__file__).with_name("solver_cases.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {kept} cases to {path}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,134 @@
+"""GPU parity: the batched refactor, solve and transposed solve must be
+bit-identical to the reference (golden fixtures) and to the oracle port."""
+import numpy as np
+import pytest
+import torch
+
+import golden_cases
+import oracle
+from matrices import banded, mna_mesh, random_matrix
+from neospice_b200 import _lib as L
+from neospice_b200.solver import Batch, Topology
+
+pytestmark = pytest.mark.gpu
+CASES = golden_cases.load()
+
+
+def _pack(batch, per_instance, offsets):
+    out = np.zeros(int(offsets[-1]))
+    for i, v in enumerate(per_instance):
+        out[offsets[i]:offsets[i] + len(v)] = v
+    return torch.from_numpy(out).cuda()
+
+
+def _unpack(arr, offsets, sizes):
+    arr = arr.cpu().numpy() if torch.is_tensor(arr) else arr
+    return [arr[offsets[i]:offsets[i] + s] for i, s in enumerate(sizes)]
+
+
+def _run(topos, vals, bs, gmin=0.0, check=False):
+    batch = Batch(topos)
+    d_a = _pack(batch, vals, batch.value_offsets)
+    st, fs = batch.refactor(d_a, gmin, check_pivots=check)
+    lu = batch.lu_values()
+    infos = [t.info() for t in topos]
+    lus = _unpack(lu, batch.lu_offsets, [i["nnz_lu"] for i in infos])
+    out = {"status": st.cpu().numpy(), "step": fs.cpu().numpy(), "lu": lus}
+    if bs is not None:
+        d_x = _pack(batch, bs, batch.vector_offsets)
+        batch.solve(d_x)
+        d_xt = _pack(batch, bs, batch.vector_offsets)
+        batch.solve_transposed(d_xt)
+        torch.cuda.synchronize()
+        ns = [i["n"] for i in infos]
+        out["x"] = _unpack(d_x, batch.vector_offsets, ns)
+        out["xt"] = _unpack(d_xt, batch.vector_offsets, ns)
+    return out
+
+
+def test_refactor_and_solves_match_golden_bitwise():
+    topos = [Topology.order(int(c["n"]), c["col_ptr"], c["row_idx"], c["vals"]) for c in CASES]
+    first = _run(topos, [c["vals"] for c in CASES], None)
+    for c, lu, s in zip(CASES, first["lu"], first["status"]):
+        assert s == 0
+        np.testing.assert_array_equal(lu, c["lu_numeric"])
+    res = _run(topos, [c["vals2"] for c in CASES], [c["b"] for c in CASES])
+    for k, c in enumerate(CASES):
+        rc = int(c["refactor_rc"])
+        assert (res["status"][k] != 0) == (rc != 0)
+        if rc:
+            continue
+        np.testing.assert_array_equal(res["lu"][k], c["lu_refactor"])
+        np.testing.assert_array_equal(res["x"][k], c["x"])
+        np.testing.assert_array_equal(res["xt"][k], c["xt"])
+
+
+def test_imported_structure_matches():
+    c = CASES[-1]
+    st = c["structure"]
+    topo = Topology.import_structure(st.n, len(st.slot_to_elem), st.int_to_ext_row,
+                                     st.int_to_ext_col, st.elem_row, st.elem_col, st.slot_to_elem)
+    res = _run([topo], [c["vals2"]], [c["b"]])
+    np.testing.assert_array_equal(res["lu"][0], c["lu_refactor"])
+    np.testing.assert_array_equal(res["x"][0], c["x"])
+
+
+def test_mixed_batch_against_port():
+    rng = np.random.default_rng(11)
+    mats = [mna_mesh(rng, s, 1 + s % 3) for s in (4, 9, 17, 30, 45)]
+    mats += [banded(1000, 7, seed=2)]
+    mats += [random_matrix(rng, int(rng.integers(5, 200)), 0.03, True, 0.0) for _ in range(20)]
+    topos, vals, bs = [], [], []
+    for (n, cp, ri, v) in mats:
+        topos.append(Topology.order(n, cp, ri, v))
+        vals.append(v * np.exp(0.05 * rng.standard_normal(len(v))))
+        bs.append(rng.standard_normal(n))
+    # repeat instances so several CTAs share one plan
+    topos, vals, bs = topos * 3, vals * 3, bs * 3
+    res = _run(topos, vals, bs, gmin=1e-12)
+    for k, t in enumerate(topos):
+        st = oracle.Structure(t.info()["n"], *t.export())
+        rc, lu, _ = oracle.port_refactor(st, vals[k], gmin=1e-12)
+        assert rc == 0 and res["status"][k] == 0
+        np.testing.assert_array_equal(res["lu"][k], lu)
+        np.testing.assert_array_equal(res["x"][k], oracle.port_solve(st, lu, bs[k]))
+        np.testing.assert_array_equal(res["xt"][k], oracle.port_solve(st, lu, bs[k], True))
+
+
+def test_zero_pivot_flagged_singular():
+    n, cp, ri, v = mna_mesh(np.random.default_rng(3), 5, 1)
+    topo = Topology.order(n, cp, ri, v)
+    st = oracle.Structure(n, *topo.export())
+    # zero the caller slot that lands on the first pivot: exact zero pivot
+    v0 = v.copy()
+    v0[np.nonzero(st.slot_to_elem == 0)[0]] = 0.0
+    rc, _, step = oracle.port_refactor(st, v0)
+    res = _run([topo, topo], [v, v0], None)
+    assert res["status"][0] == 0
+    assert res["status"][1] == L.NSG_SINGULAR == rc
+    assert res["step"][1] == step == 0
+
+
+def test_pivot_revalidation_flags_match_port():
+    rng = np.random.default_rng(8)
+    topos, vals, expect = [], [], []
+    for _ in range(40):
+        n, cp, ri, v = random_matrix(rng, 25, 0.25, diag_dominant=False, zero_diag_frac=0.1)
+        try:
+            t = Topology.order(n, cp, ri, v)
+        except L.NsgError:
+            continue
+        st = oracle.Structure(n, *t.export())
+        v2 = v * np.exp(rng.standard_normal(len(v)))
+        rc, _, step = oracle.port_refactor(st, v2, check_pivots=True)
+        topos.append(t)
+        vals.append(v2)
+        expect.append((rc, step))
+    res = _run(topos, vals, None, check=True)
+    flagged = 0
+    for k, (rc, step) in enumerate(expect):
+        assert res["status"][k] == rc
+        if rc:
+            flagged += 1
+            assert res["step"][k] == step
+    assert flagged > 0
