@@ -99,6 +99,12 @@ int nsg_batch_layout(const nsg_batch* batch, long long* value_offsets,
 int nsg_batch_refactor(nsg_batch* batch, const double* d_values, double diag_gmin,
                        int check_pivots, int* d_status, int* d_fail_step, void* stream);
 
+/* Refactor schedule: 0 (default) = dataflow (warps claim columns in pivot
+ * order and wait on per-column completion flags, column staged in shared
+ * memory; used when the batch's columns fit), 1 = level-synchronous.  Both
+ * produce bit-identical values. */
+int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
+
 /* spSolve: d_x holds b on entry and x on return, per instance
  * (SparseMatrix::solve, src/solver/solve.cpp:6-47; NeoSolver::solve). */
 int nsg_batch_solve(nsg_batch* batch, double* d_x, void* stream);
@@ -115,6 +121,82 @@ const double* nsg_batch_lu(const nsg_batch* batch);
 /* Synchronous copy of all LU values to host memory (lu_offsets[count]
  * doubles). */
 int nsg_batch_lu_to_host(const nsg_batch* batch, double* out);
+
+/* ---- Circuits (host) --------------------------------------------------------
+ * Typed construction mirroring the reference's Circuit API
+ * (src/core/circuit.hpp:179-237) for the devices of the batched DC path:
+ * nodes are 0..num_nodes-1 and -1 is ground (Circuit::node("0") == GND).
+ * nsg_circuit_finalize mirrors Circuit::finalize (src/core/circuit.cpp:201-283):
+ * ngspice load order, branch unknowns after the nodes, sparsity pattern,
+ * dead-node placeholders.  Parameters are kept in creation order: resistor
+ * {ohms}, vsource {volts}, isource {amps}, diode {IS, N}. */
+typedef struct nsg_circuit nsg_circuit;
+
+int nsg_circuit_create(int num_nodes, nsg_circuit** out);
+void nsg_circuit_free(nsg_circuit* c);
+/* Circuit::R (src/core/circuit.hpp:180). */
+int nsg_circuit_add_resistor(nsg_circuit* c, int a, int b, double ohms);
+/* Circuit::V with a DC value (src/core/circuit.hpp:187). */
+int nsg_circuit_add_vsource(nsg_circuit* c, int p, int n, double volts);
+/* Circuit::I with a DC value (src/core/circuit.hpp:189). */
+int nsg_circuit_add_isource(nsg_circuit* c, int p, int n, double amps);
+/* Circuit::D with a level-1 model card D(IS=is N=n) (src/core/circuit.hpp:206;
+ * series resistance 0, T = TNOM). */
+int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, double n_emission);
+/* Bulk forms: count devices in one call, arrays of terminals and values,
+ * created in array order (identical to count single calls). */
+int nsg_circuit_add_resistors(nsg_circuit* c, int count, const int* a, const int* b,
+                              const double* ohms);
+int nsg_circuit_add_isources(nsg_circuit* c, int count, const int* p, const int* n,
+                             const double* amps);
+int nsg_circuit_add_diodes(nsg_circuit* c, int count, const int* anode, const int* cathode,
+                           const double* is, const double* n_emission);
+int nsg_circuit_finalize(nsg_circuit* c);
+int nsg_circuit_info(const nsg_circuit* c, int* num_vars, int* num_nodes, int* nnz,
+                     int* num_params);
+/* CSC pattern (col_ptr: num_vars+1, row_idx: nnz) and parameters. */
+int nsg_circuit_pattern(const nsg_circuit* c, int* col_ptr, int* row_idx);
+int nsg_circuit_params(const nsg_circuit* c, double* params);
+/* Matrix values and rhs of the first DC Newton iteration (MODEDCOP |
+ * MODEINITJCT from a zero guess), in slot order -- what the reference's
+ * first NeoSolver::numeric orders on. */
+int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs);
+
+/* ---- Batched DC operating point (device) ------------------------------------
+ * Simulator::run_dc / solve_dc's direct Newton attempt (src/core/dc.cpp:53-118,
+ * newton.cpp:51-419) for `count` circuits in one launch, one thread block per
+ * circuit.  symbolic: NSG_SYMBOLIC_PER_INSTANCE orders every circuit on its own
+ * first-iteration matrix (bit-identical to the reference's pivots);
+ * NSG_SYMBOLIC_PER_PATTERN orders once per distinct sparsity pattern and lets
+ * the GPU re-validate the pivots of every instance at its second iteration
+ * (a failing instance reports NSG_REORDER).  threads: host threads for the
+ * symbolic phase (<= 0: all cores). */
+#define NSG_SYMBOLIC_PER_INSTANCE 0
+#define NSG_SYMBOLIC_PER_PATTERN 1
+typedef struct nsg_dc_batch nsg_dc_batch;
+
+int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, int threads,
+                        nsg_dc_batch** out);
+void nsg_dc_batch_free(nsg_dc_batch* b);
+/* Offsets (count+1 each) of every instance's parameters and solution in the
+ * packed arrays nsg_dc_batch_run reads and writes. */
+int nsg_dc_batch_layout(const nsg_dc_batch* b, long long* param_offsets,
+                        long long* solution_offsets);
+/* Totals over instances: unknowns, matrix slots, LU entries, refactor
+ * updates; number of distinct symbolic results. */
+int nsg_dc_batch_stats(const nsg_dc_batch* b, long long* n, long long* nnz, long long* nnz_lu,
+                       long long* updates, int* distinct_topologies);
+/* SimOptions reltol, vntol, abstol, gmin and itl1 (defaults 1e-3, 1e-6,
+ * 1e-12, 1e-12, 100; src/core/types.hpp:24-66). */
+int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, double abstol,
+                             double gmin, int max_iter);
+/* Run every instance to convergence.  d_params: packed parameters (device;
+ * NULL = the circuits' own values); d_solutions: packed solutions (device),
+ * the returned iterate as newton_solve returns it; d_status: 0 converged,
+ * 1 no convergence in itl1 iterations, 102 singular, 103 pivot re-validation
+ * failed, 104 a bounded wait gave up; d_iterations: Newton iterations. */
+int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
+                     int* d_iterations, void* stream);
 
 #ifdef __cplusplus
 }

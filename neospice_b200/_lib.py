@@ -24,6 +24,9 @@ NSG_ERR_CUDA = 2
 NSG_ERR_NOMEM = 8
 NSG_SINGULAR = 102
 NSG_REORDER = 103
+NSG_TIMEOUT = 104
+NSG_SYMBOLIC_PER_INSTANCE = 0
+NSG_SYMBOLIC_PER_PATTERN = 1
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -42,10 +45,32 @@ SIGNATURES = {
     "nsg_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll)]),
     "nsg_batch_refactor": (c_int, [c_void_p, c_void_p, c_double, c_int, c_void_p, c_void_p,
                                    c_void_p]),
+    "nsg_batch_set_schedule": (c_int, [c_void_p, c_int]),
     "nsg_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
     "nsg_batch_solve_transposed": (c_int, [c_void_p, c_void_p, c_void_p]),
     "nsg_batch_lu": (c_void_p, [c_void_p]),
     "nsg_batch_lu_to_host": (c_int, [c_void_p, P(c_double)]),
+    "nsg_circuit_create": (c_int, [c_int, P(c_void_p)]),
+    "nsg_circuit_free": (None, [c_void_p]),
+    "nsg_circuit_add_resistor": (c_int, [c_void_p, c_int, c_int, c_double]),
+    "nsg_circuit_add_vsource": (c_int, [c_void_p, c_int, c_int, c_double]),
+    "nsg_circuit_add_isource": (c_int, [c_void_p, c_int, c_int, c_double]),
+    "nsg_circuit_add_diode": (c_int, [c_void_p, c_int, c_int, c_double, c_double]),
+    "nsg_circuit_add_resistors": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
+    "nsg_circuit_add_isources": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
+    "nsg_circuit_add_diodes": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double),
+                                       P(c_double)]),
+    "nsg_circuit_finalize": (c_int, [c_void_p]),
+    "nsg_circuit_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int)]),
+    "nsg_circuit_pattern": (c_int, [c_void_p, P(c_int), P(c_int)]),
+    "nsg_circuit_params": (c_int, [c_void_p, P(c_double)]),
+    "nsg_circuit_initial_matrix": (c_int, [c_void_p, c_double, P(c_double), P(c_double)]),
+    "nsg_dc_batch_create": (c_int, [c_int, P(c_void_p), c_int, c_int, P(c_void_p)]),
+    "nsg_dc_batch_free": (None, [c_void_p]),
+    "nsg_dc_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll)]),
+    "nsg_dc_batch_stats": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll), P(c_ll), P(c_int)]),
+    "nsg_dc_batch_set_options": (c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int]),
+    "nsg_dc_batch_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

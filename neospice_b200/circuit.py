@@ -1,0 +1,166 @@
+"""Circuits and batched DC operating points on the GPU.
+
+``Circuit`` mirrors the reference's typed Circuit API (src/core/circuit.hpp:
+179-237) for resistors, DC voltage/current sources and level-1 diodes; nodes
+are integers and ``GND`` (-1) is ground.  ``DcBatch`` runs the direct Newton
+attempt of Simulator::run_dc (src/core/dc.cpp:53-118) for many circuits in
+one kernel launch.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+GND = -1
+
+
+class Circuit:
+    def __init__(self, num_nodes: int):
+        h = ctypes.c_void_p()
+        L.check(L.lib().nsg_circuit_create(int(num_nodes), ctypes.byref(h)))
+        self._h = h
+        self.num_nodes = int(num_nodes)
+        self._final = False
+
+    @property
+    def handle(self):
+        return self._h
+
+    def R(self, a: int, b: int, ohms: float):
+        L.check(L.lib().nsg_circuit_add_resistor(self._h, int(a), int(b), float(ohms)))
+
+    def V(self, p: int, n: int, volts: float):
+        L.check(L.lib().nsg_circuit_add_vsource(self._h, int(p), int(n), float(volts)))
+
+    def I(self, p: int, n: int, amps: float):  # noqa: E743 - the reference's name
+        L.check(L.lib().nsg_circuit_add_isource(self._h, int(p), int(n), float(amps)))
+
+    def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0):
+        L.check(L.lib().nsg_circuit_add_diode(self._h, int(anode), int(cathode), float(IS), float(N)))
+
+    def add_resistors(self, a, b, ohms):
+        a, b = np.ascontiguousarray(a, np.int32), np.ascontiguousarray(b, np.int32)
+        ohms = np.ascontiguousarray(ohms, np.float64)
+        L.check(L.lib().nsg_circuit_add_resistors(self._h, len(a), L.iptr(a), L.iptr(b),
+                                                  L.dptr(ohms)))
+
+    def add_isources(self, p, n, amps):
+        p, n = np.ascontiguousarray(p, np.int32), np.ascontiguousarray(n, np.int32)
+        amps = np.ascontiguousarray(amps, np.float64)
+        L.check(L.lib().nsg_circuit_add_isources(self._h, len(p), L.iptr(p), L.iptr(n),
+                                                 L.dptr(amps)))
+
+    def add_diodes(self, anode, cathode, IS, N):
+        a, k = np.ascontiguousarray(anode, np.int32), np.ascontiguousarray(cathode, np.int32)
+        IS = np.ascontiguousarray(np.broadcast_to(IS, a.shape), np.float64)
+        N = np.ascontiguousarray(np.broadcast_to(N, a.shape), np.float64)
+        L.check(L.lib().nsg_circuit_add_diodes(self._h, len(a), L.iptr(a), L.iptr(k), L.dptr(IS),
+                                               L.dptr(N)))
+
+    def finalize(self):
+        L.check(L.lib().nsg_circuit_finalize(self._h))
+        self._final = True
+        return self
+
+    def info(self) -> dict:
+        nv, nn, nnz, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        L.check(L.lib().nsg_circuit_info(self._h, ctypes.byref(nv), ctypes.byref(nn),
+                                         ctypes.byref(nnz), ctypes.byref(npar)))
+        return dict(num_vars=nv.value, num_nodes=nn.value, nnz=nnz.value, num_params=npar.value)
+
+    def pattern(self):
+        i = self.info()
+        cp = np.zeros(i["num_vars"] + 1, np.int32)
+        ri = np.zeros(i["nnz"], np.int32)
+        L.check(L.lib().nsg_circuit_pattern(self._h, L.iptr(cp), L.iptr(ri)))
+        return cp, ri
+
+    def params(self):
+        p = np.zeros(self.info()["num_params"])
+        L.check(L.lib().nsg_circuit_params(self._h, L.dptr(p)))
+        return p
+
+    def initial_matrix(self, gmin=1e-12):
+        i = self.info()
+        a = np.zeros(i["nnz"])
+        r = np.zeros(i["num_vars"])
+        L.check(L.lib().nsg_circuit_initial_matrix(self._h, float(gmin), L.dptr(a), L.dptr(r)))
+        return a, r
+
+    def __del__(self):
+        if getattr(self, "_h", None) and L._lib is not None:
+            L._lib.nsg_circuit_free(self._h)
+            self._h = None
+
+
+class DcBatch:
+    """Batched DC operating point of finalized circuits (one CTA each)."""
+
+    PER_INSTANCE = L.NSG_SYMBOLIC_PER_INSTANCE
+    PER_PATTERN = L.NSG_SYMBOLIC_PER_PATTERN
+
+    def __init__(self, circuits, symbolic=PER_PATTERN, threads=0):
+        self.circuits = list(circuits)
+        arr = (ctypes.c_void_p * len(self.circuits))(*[c.handle for c in self.circuits])
+        h = ctypes.c_void_p()
+        L.check(L.lib().nsg_dc_batch_create(len(self.circuits), arr, int(symbolic), int(threads),
+                                            ctypes.byref(h)))
+        self._h = h
+        cnt = len(self.circuits) + 1
+        self.param_offsets = np.zeros(cnt, np.int64)
+        self.solution_offsets = np.zeros(cnt, np.int64)
+        L.check(L.lib().nsg_dc_batch_layout(self._h, L.llptr(self.param_offsets),
+                                            L.llptr(self.solution_offsets)))
+
+    @property
+    def count(self):
+        return len(self.circuits)
+
+    def stats(self) -> dict:
+        n, nnz, nlu, upd = (ctypes.c_longlong() for _ in range(4))
+        topo = ctypes.c_int()
+        L.check(L.lib().nsg_dc_batch_stats(self._h, ctypes.byref(n), ctypes.byref(nnz),
+                                           ctypes.byref(nlu), ctypes.byref(upd),
+                                           ctypes.byref(topo)))
+        return dict(n=n.value, nnz=nnz.value, nnz_lu=nlu.value, updates=upd.value,
+                    topologies=topo.value)
+
+    def set_options(self, reltol=1e-3, vntol=1e-6, abstol=1e-12, gmin=1e-12, max_iter=100):
+        L.check(L.lib().nsg_dc_batch_set_options(self._h, reltol, vntol, abstol, gmin,
+                                                 int(max_iter)))
+
+    def params(self):
+        """Packed default parameters of all circuits (host)."""
+        return np.concatenate([c.params() for c in self.circuits])
+
+    def run(self, d_params=None, d_solutions=None, d_status=None, d_iterations=None,
+            stream=None):
+        """Launch the batched Newton solve; returns device tensors
+        (solutions, status, iterations)."""
+        import torch
+        dev = torch.device("cuda")
+        if d_solutions is None:
+            d_solutions = torch.empty(int(self.solution_offsets[-1]), dtype=torch.float64, device=dev)
+        if d_status is None:
+            d_status = torch.empty(self.count, dtype=torch.int32, device=dev)
+        if d_iterations is None:
+            d_iterations = torch.empty(self.count, dtype=torch.int32, device=dev)
+        sp = torch.cuda.current_stream().cuda_stream if stream is None else \
+            getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().nsg_dc_batch_run(self._h, None if d_params is None else d_params.data_ptr(),
+                                         d_solutions.data_ptr(), d_status.data_ptr(),
+                                         d_iterations.data_ptr(), sp))
+        return d_solutions, d_status, d_iterations
+
+    def split(self, packed):
+        arr = packed.cpu().numpy() if hasattr(packed, "cpu") else np.asarray(packed)
+        o = self.solution_offsets
+        return [arr[o[i]:o[i + 1]] for i in range(self.count)]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and L._lib is not None:
+            L._lib.nsg_dc_batch_free(self._h)
+            self._h = None

@@ -1,13 +1,8 @@
 // C ABI of libnsgpu (declared in include/nsgpu.h): host symbolic phase, batch
 // set-up and the launches of the batched refactor and sweeps.
-#include "nsgpu.h"
+#include "capi_internal.hpp"
 
-#include "host/plan.hpp"
-#include "host/sparse_order.hpp"
-#include "kernels/lu_device.cuh"
-
-#include <cuda_runtime.h>
-
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -21,36 +16,14 @@ namespace nsg {
 cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                             int count, const double* A, double* LU, double diag_gmin,
                             int check_pivots, double rel_threshold, int32_t* status,
-                            int32_t* fail_step, cudaStream_t stream);
+                            int32_t* fail_step, int max_col, int max_n, bool allow_flow,
+                            cudaStream_t stream);
 cudaError_t launch_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                          int count, const double* LU, double* X, double* W, bool transposed,
                          cudaStream_t stream);
 }  // namespace nsg
 
-struct nsg_topology {
-    std::unique_ptr<nsg::MarkowitzOrder> engine;  // null for an imported topology
-    std::vector<int32_t> slot_elem;
-    nsg::TopologyPlan plan;
-};
-
-struct nsg_batch {
-    int count = 0;
-    std::vector<long long> a_off, x_off, lu_off;
-    int32_t* d_pool = nullptr;
-    nsg::PlanDesc* d_plans = nullptr;
-    nsg::InstDesc* d_insts = nullptr;
-    double* d_lu = nullptr;
-    double* d_work = nullptr;
-    ~nsg_batch() {
-        cudaFree(d_pool);
-        cudaFree(d_plans);
-        cudaFree(d_insts);
-        cudaFree(d_lu);
-        cudaFree(d_work);
-    }
-};
-
-namespace {
+namespace nsg_internal {
 
 thread_local std::string g_last_error;
 
@@ -59,31 +32,11 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-// Run a body, mapping C++ exceptions to status codes.
-template <class F>
-int guarded(const char* where, F&& body) {
-    try {
-        g_last_error.clear();
-        return body();
-    } catch (const std::bad_alloc&) {
-        return fail(NSG_ERR_NOMEM, std::string(where) + ": out of host memory");
-    } catch (const std::exception& e) {
-        return fail(NSG_ERR_INVALID, std::string(where) + ": " + e.what());
-    }
-}
+void clear_error() { g_last_error.clear(); }
 
 int cuda_fail(const char* where, cudaError_t e) {
     return fail(e == cudaErrorMemoryAllocation ? NSG_ERR_NOMEM : NSG_ERR_CUDA,
                 std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-template <class T>
-cudaError_t upload(T** dst, const T* src, size_t count) {
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), count * sizeof(T));
-    if (e != cudaSuccess) return e;
-    if (src) e = cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
-    return e;
 }
 
 // NeoSolver::numeric's load + preorder + gmin + order_and_factor on the
@@ -100,39 +53,64 @@ int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin) {
     return NSG_OK;
 }
 
-}  // namespace
+int order_topology(int n, int nnz, const int* col_ptr, const int* row_idx, const double* values,
+                   double diag_gmin, std::unique_ptr<nsg_topology>& out) {
+    if (n <= 0 || nnz <= 0 || !col_ptr || !row_idx || !values)
+        return fail(NSG_ERR_INVALID, "nsg_topology_order: bad arguments");
+    if (col_ptr[0] != 0 || col_ptr[n] != nnz)
+        return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr does not span nnz");
+    auto t = std::make_unique<nsg_topology>();
+    t->engine = std::make_unique<nsg::MarkowitzOrder>(n);
+    t->slot_elem.resize(nnz);
+    for (int j = 0; j < n; ++j) {
+        if (col_ptr[j + 1] < col_ptr[j])
+            return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr not monotone");
+        for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) {
+            if (row_idx[p] < 0 || row_idx[p] >= n ||
+                (p > col_ptr[j] && row_idx[p] <= row_idx[p - 1]))
+                return fail(NSG_ERR_INVALID, "nsg_topology_order: rows not sorted/unique");
+            t->slot_elem[p] = t->engine->get_element(row_idx[p] + 1, j + 1);
+        }
+    }
+    const int rc = numeric_on_engine(*t, values, diag_gmin);
+    if (rc == NSG_SINGULAR) return fail(NSG_SINGULAR, "nsg_topology_order: singular matrix");
+    if (rc != NSG_OK) return fail(rc, "nsg_topology_order: ordering failed");
+    t->plan = nsg::build_plan(*t->engine, t->slot_elem);
+    out = std::move(t);
+    return NSG_OK;
+}
+
+nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& pool) {
+    nsg::PlanDesc d{};
+    d.n = p.n;
+    d.nnz_a = p.nnz_a;
+    d.nnz_lu = p.nnz_lu;
+    d.n_col_lev = static_cast<int32_t>(p.col_lev_ptr.size()) - 1;
+    d.n_fwd_lev = static_cast<int32_t>(p.fwd_lev_ptr.size()) - 1;
+    d.n_bwd_lev = static_cast<int32_t>(p.bwd_lev_ptr.size()) - 1;
+    d.n_tbw_lev = static_cast<int32_t>(p.tbw_lev_ptr.size()) - 1;
+    d.max_col = p.max_col;
+    p.append_to(pool, d.off);
+    return d;
+}
+
+}  // namespace nsg_internal
+
+using namespace nsg_internal;
 
 extern "C" {
 
-const char* nsg_last_error(void) { return g_last_error.c_str(); }
+const char* nsg_last_error(void) { return nsg_internal::g_last_error.c_str(); }
 
 int nsg_topology_order(int n, int nnz, const int* col_ptr, const int* row_idx,
                        const double* values, double diag_gmin, nsg_topology** out) {
     return guarded("nsg_topology_order", [&]() -> int {
-        if (!out || n <= 0 || nnz <= 0 || !col_ptr || !row_idx || !values)
-            return fail(NSG_ERR_INVALID, "nsg_topology_order: bad arguments");
+        if (!out) return fail(NSG_ERR_INVALID, "nsg_topology_order: null out");
         *out = nullptr;
-        if (col_ptr[0] != 0 || col_ptr[n] != nnz)
-            return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr does not span nnz");
-        auto t = std::make_unique<nsg_topology>();
-        t->engine = std::make_unique<nsg::MarkowitzOrder>(n);
-        t->slot_elem.resize(nnz);
-        for (int j = 0; j < n; ++j) {
-            if (col_ptr[j + 1] < col_ptr[j])
-                return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr not monotone");
-            for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) {
-                if (row_idx[p] < 0 || row_idx[p] >= n ||
-                    (p > col_ptr[j] && row_idx[p] <= row_idx[p - 1]))
-                    return fail(NSG_ERR_INVALID, "nsg_topology_order: rows not sorted/unique");
-                t->slot_elem[p] = t->engine->get_element(row_idx[p] + 1, j + 1);
-            }
-        }
-        const int rc = numeric_on_engine(*t, values, diag_gmin);
-        if (rc == NSG_SINGULAR) return fail(NSG_SINGULAR, "nsg_topology_order: singular matrix");
-        if (rc != NSG_OK) return fail(rc, "nsg_topology_order: ordering failed");
-        t->plan = nsg::build_plan(*t->engine, t->slot_elem);
-        *out = t.release();
-        return NSG_OK;
+        std::unique_ptr<nsg_topology> t;
+        const int rc = order_topology(n, nnz, col_ptr, row_idx, values, diag_gmin, t);
+        if (rc == NSG_OK) *out = t.release();
+        return rc;
     });
 }
 
@@ -221,20 +199,12 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             if (!t) return fail(NSG_ERR_INVALID, "nsg_batch_create: null topology");
             auto it = plan_of.find(t);
             if (it == plan_of.end()) {
-                nsg::PlanDesc d{};
-                const auto& p = t->plan;
-                d.n = p.n;
-                d.nnz_a = p.nnz_a;
-                d.nnz_lu = p.nnz_lu;
-                d.n_col_lev = static_cast<int32_t>(p.col_lev_ptr.size()) - 1;
-                d.n_fwd_lev = static_cast<int32_t>(p.fwd_lev_ptr.size()) - 1;
-                d.n_bwd_lev = static_cast<int32_t>(p.bwd_lev_ptr.size()) - 1;
-                d.n_tbw_lev = static_cast<int32_t>(p.tbw_lev_ptr.size()) - 1;
-                p.append_to(pool, d.off);
                 it = plan_of.emplace(t, static_cast<int32_t>(plans.size())).first;
-                plans.push_back(d);
+                plans.push_back(make_plan_desc(t->plan, pool));
             }
             const auto& p = t->plan;
+            b->max_col = std::max(b->max_col, p.max_col);
+            b->max_n = std::max(b->max_n, p.n);
             insts[i].plan = it->second;
             insts[i].a_off = b->a_off[i];
             insts[i].lu_off = b->lu_off[i];
@@ -275,7 +245,8 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
         return fail(NSG_ERR_INVALID, "nsg_batch_refactor: null argument");
     cudaError_t e = nsg::launch_refactor(b->d_plans, b->d_pool, b->d_insts, b->count, d_values,
                                          b->d_lu, diag_gmin, check_pivots, 1e-3, d_status,
-                                         d_fail_step, static_cast<cudaStream_t>(stream));
+                                         d_fail_step, b->max_col, b->max_n, b->allow_flow,
+                                         static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
 }
 
@@ -294,6 +265,13 @@ int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
 }
 
 const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
+
+int nsg_batch_set_schedule(nsg_batch* b, int schedule) {
+    if (!b || schedule < 0 || schedule > 1)
+        return fail(NSG_ERR_INVALID, "nsg_batch_set_schedule: bad arguments");
+    b->allow_flow = (schedule == 0);
+    return NSG_OK;
+}
 
 int nsg_batch_lu_to_host(const nsg_batch* b, double* out) {
     if (!b || !out) return fail(NSG_ERR_INVALID, "nsg_batch_lu_to_host: null argument");

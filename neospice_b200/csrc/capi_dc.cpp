@@ -1,0 +1,388 @@
+// C ABI of circuits and batched DC operating points (include/nsgpu.h).
+#include "capi_internal.hpp"
+
+#include "host/circuit.hpp"
+#include "kernels/dc_device.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <thread>
+#include <tuple>
+
+namespace nsg {
+cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
+                             int count, const int32_t* prog, const double* params, double* work,
+                             double* solutions, int32_t* status, int32_t* iterations,
+                             const NewtonOptions& opt, int max_col, int max_n,
+                             cudaStream_t stream);
+}  // namespace nsg
+
+using namespace nsg_internal;
+
+struct nsg_circuit {
+    explicit nsg_circuit(int nodes) : c(nodes) {}
+    nsg::Circuit c;
+};
+
+struct nsg_dc_batch {
+    int count = 0;
+    std::vector<std::unique_ptr<nsg_topology>> topos;  // distinct symbolic results
+    std::vector<long long> param_off, sol_off;
+    std::vector<double> host_params;
+    long long updates = 0, nnz_lu = 0, nnz = 0, n = 0;
+    int max_col = 0, max_n = 0;
+    nsg::NewtonOptions opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, 0};
+    int32_t* d_lu_pool = nullptr;
+    nsg::PlanDesc* d_plans = nullptr;
+    int32_t* d_prog = nullptr;
+    nsg::DcDesc* d_descs = nullptr;
+    double* d_work = nullptr;
+    double* d_params = nullptr;
+    ~nsg_dc_batch() {
+        cudaFree(d_lu_pool);
+        cudaFree(d_plans);
+        cudaFree(d_prog);
+        cudaFree(d_descs);
+        cudaFree(d_work);
+        cudaFree(d_params);
+    }
+};
+
+namespace {
+
+// Append an int vector to the pool at a 16-byte boundary; return its offset.
+int64_t append(std::vector<int32_t>& pool, const std::vector<int32_t>& v) {
+    while (pool.size() % 4) pool.push_back(0);
+    const int64_t off = static_cast<int64_t>(pool.size());
+    pool.insert(pool.end(), v.begin(), v.end());
+    return off;
+}
+
+int64_t align4(int64_t x) { return (x + 3) & ~int64_t{3}; }
+
+bool same_structure(const nsg::TopologyPlan& a, const nsg::TopologyPlan& b) {
+    return a.n == b.n && a.perm_row == b.perm_row && a.perm_col == b.perm_col &&
+           a.col_ptr == b.col_ptr && a.row_idx == b.row_idx && a.lu_src == b.lu_src;
+}
+
+// Run f(i) for i in [0, count) on up to `threads` host threads.
+template <class F>
+void parallel_for(int count, int threads, F&& f) {
+    threads = std::max(1, std::min(threads, count));
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    std::vector<std::exception_ptr> errs(threads);
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t] {
+            try {
+                for (int i; (i = next.fetch_add(1)) < count;) f(i);
+            } catch (...) {
+                errs[t] = std::current_exception();
+            }
+        });
+    for (auto& th : pool) th.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+int nsg_circuit_create(int num_nodes, nsg_circuit** out) {
+    return guarded("nsg_circuit_create", [&]() -> int {
+        if (!out) return fail(NSG_ERR_INVALID, "nsg_circuit_create: null out");
+        *out = new nsg_circuit(num_nodes);
+        return NSG_OK;
+    });
+}
+
+void nsg_circuit_free(nsg_circuit* c) { delete c; }
+
+int nsg_circuit_add_resistor(nsg_circuit* c, int a, int b, double ohms) {
+    return guarded("nsg_circuit_add_resistor", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_resistor(a, b, ohms);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_vsource(nsg_circuit* c, int p, int n, double volts) {
+    return guarded("nsg_circuit_add_vsource", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_vsource(p, n, volts);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_isource(nsg_circuit* c, int p, int n, double amps) {
+    return guarded("nsg_circuit_add_isource", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_isource(p, n, amps);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, double n_emission) {
+    return guarded("nsg_circuit_add_diode", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_diode(anode, cathode, is, n_emission);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_resistors(nsg_circuit* c, int count, const int* a, const int* b,
+                              const double* ohms) {
+    return guarded("nsg_circuit_add_resistors", [&]() -> int {
+        if (!c || count < 0 || (count && (!a || !b || !ohms)))
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        for (int i = 0; i < count; ++i) c->c.add_resistor(a[i], b[i], ohms[i]);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_isources(nsg_circuit* c, int count, const int* p, const int* n,
+                             const double* amps) {
+    return guarded("nsg_circuit_add_isources", [&]() -> int {
+        if (!c || count < 0 || (count && (!p || !n || !amps)))
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        for (int i = 0; i < count; ++i) c->c.add_isource(p[i], n[i], amps[i]);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_diodes(nsg_circuit* c, int count, const int* anode, const int* cathode,
+                           const double* is, const double* n_emission) {
+    return guarded("nsg_circuit_add_diodes", [&]() -> int {
+        if (!c || count < 0 || (count && (!anode || !cathode || !is || !n_emission)))
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        for (int i = 0; i < count; ++i) c->c.add_diode(anode[i], cathode[i], is[i], n_emission[i]);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_finalize(nsg_circuit* c) {
+    return guarded("nsg_circuit_finalize", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.finalize();
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_info(const nsg_circuit* c, int* num_vars, int* num_nodes, int* nnz,
+                     int* num_params) {
+    if (!c) return fail(NSG_ERR_INVALID, "nsg_circuit_info: null circuit");
+    if (!c->c.finalized()) return fail(NSG_ERR_INVALID, "nsg_circuit_info: not finalized");
+    if (num_vars) *num_vars = c->c.num_vars();
+    if (num_nodes) *num_nodes = c->c.num_nodes();
+    if (nnz) *nnz = c->c.nnz();
+    if (num_params) *num_params = static_cast<int>(c->c.params().size());
+    return NSG_OK;
+}
+
+int nsg_circuit_pattern(const nsg_circuit* c, int* col_ptr, int* row_idx) {
+    if (!c || !c->c.finalized()) return fail(NSG_ERR_INVALID, "nsg_circuit_pattern: not finalized");
+    if (col_ptr) std::memcpy(col_ptr, c->c.col_ptr().data(), sizeof(int) * c->c.col_ptr().size());
+    if (row_idx) std::memcpy(row_idx, c->c.row_idx().data(), sizeof(int) * c->c.row_idx().size());
+    return NSG_OK;
+}
+
+int nsg_circuit_params(const nsg_circuit* c, double* params) {
+    if (!c || !params) return fail(NSG_ERR_INVALID, "nsg_circuit_params: null argument");
+    std::memcpy(params, c->c.params().data(), sizeof(double) * c->c.params().size());
+    return NSG_OK;
+}
+
+int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs) {
+    return guarded("nsg_circuit_initial_matrix", [&]() -> int {
+        if (!c || !c->c.finalized()) return fail(NSG_ERR_INVALID, "not finalized");
+        std::vector<double> a, r;
+        c->c.initjct_values(a, r, gmin);
+        if (values) std::memcpy(values, a.data(), sizeof(double) * a.size());
+        if (rhs) std::memcpy(rhs, r.data(), sizeof(double) * r.size());
+        return NSG_OK;
+    });
+}
+
+int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, int threads,
+                        nsg_dc_batch** out) {
+    return guarded("nsg_dc_batch_create", [&]() -> int {
+        if (!out || count <= 0 || !circuits)
+            return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: bad arguments");
+        if (symbolic != NSG_SYMBOLIC_PER_INSTANCE && symbolic != NSG_SYMBOLIC_PER_PATTERN)
+            return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: unknown symbolic mode");
+        *out = nullptr;
+        for (int i = 0; i < count; ++i)
+            if (!circuits[i] || !circuits[i]->c.finalized())
+                return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: circuit not finalized");
+        auto b = std::make_unique<nsg_dc_batch>();
+        b->count = count;
+        if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+
+        // Symbolic phase on the first-iteration (INITJCT) matrix, as the
+        // reference's first NeoSolver::numeric in newton_solve sees it.
+        std::vector<int> rep(count);  // instance whose ordering instance i uses
+        if (symbolic == NSG_SYMBOLIC_PER_PATTERN) {
+            std::map<std::pair<std::vector<int32_t>, std::vector<int32_t>>, int> first;
+            for (int i = 0; i < count; ++i) {
+                const auto& c = circuits[i]->c;
+                auto key = std::make_pair(c.col_ptr(), c.row_idx());
+                rep[i] = first.emplace(std::move(key), i).first->second;
+            }
+        } else {
+            for (int i = 0; i < count; ++i) rep[i] = i;
+        }
+        std::vector<int> todo;
+        for (int i = 0; i < count; ++i)
+            if (rep[i] == i) todo.push_back(i);
+        std::vector<std::unique_ptr<nsg_topology>> ordered(count);
+        std::vector<int> rcs(count, NSG_OK);
+        parallel_for(static_cast<int>(todo.size()), threads, [&](int k) {
+            const int i = todo[k];
+            const auto& c = circuits[i]->c;
+            std::vector<double> a, r;
+            c.initjct_values(a, r, b->opt.gmin);
+            rcs[i] = order_topology(c.num_vars(), c.nnz(), c.col_ptr().data(), c.row_idx().data(),
+                                    a.data(), b->opt.diag_gmin, ordered[i]);
+        });
+        for (int i : todo)
+            if (rcs[i] != NSG_OK)
+                return fail(rcs[i], "nsg_dc_batch_create: symbolic phase failed for instance " +
+                                        std::to_string(i));
+        // Share identical symbolic results between instances.
+        std::vector<int> topo_of(count, -1);
+        for (int i : todo) {
+            for (size_t t = 0; t < b->topos.size(); ++t)
+                if (b->topos[t]->plan.n == ordered[i]->plan.n &&
+                    same_structure(b->topos[t]->plan, ordered[i]->plan)) {
+                    topo_of[i] = static_cast<int>(t);
+                    break;
+                }
+            if (topo_of[i] < 0) {
+                topo_of[i] = static_cast<int>(b->topos.size());
+                b->topos.push_back(std::move(ordered[i]));
+            }
+        }
+        for (int i = 0; i < count; ++i) topo_of[i] = topo_of[rep[i]];
+
+        // Device plans, programs, descriptors, workspace.
+        std::vector<int32_t> lu_pool, prog;
+        std::vector<nsg::PlanDesc> plans;
+        for (const auto& t : b->topos) {
+            plans.push_back(make_plan_desc(t->plan, lu_pool));
+            b->max_col = std::max(b->max_col, t->plan.max_col);
+            b->max_n = std::max(b->max_n, t->plan.n);
+        }
+        std::vector<nsg::DcDesc> descs(count);
+        b->param_off.assign(count + 1, 0);
+        b->sol_off.assign(count + 1, 0);
+        int64_t work = 0;
+        for (int i = 0; i < count; ++i) {
+            const auto& c = circuits[i]->c;
+            const auto& p = b->topos[topo_of[i]]->plan;
+            nsg::DcDesc& d = descs[i];
+            d.plan = topo_of[i];
+            d.n = c.num_vars();
+            d.num_nodes = c.num_nodes();
+            d.nnz = c.nnz();
+            d.n_const = c.n_const_terms();
+            d.n_diodes = static_cast<int32_t>(c.diodes().size());
+            d.prog_off[nsg::DP_slot_ptr] = append(prog, c.slot_ptr());
+            d.prog_off[nsg::DP_slot_terms] = append(prog, c.slot_terms());
+            d.prog_off[nsg::DP_rhs_ptr] = append(prog, c.rhs_ptr());
+            d.prog_off[nsg::DP_rhs_terms] = append(prog, c.rhs_terms());
+            d.prog_off[nsg::DP_ucb_ptr] = append(prog, c.ucb_ptr());
+            d.prog_off[nsg::DP_ucb_terms] = append(prog, c.ucb_terms());
+            d.prog_off[nsg::DP_term_op] = append(prog, c.term_op());
+            d.prog_off[nsg::DP_term_param] = append(prog, c.term_param());
+            std::vector<int32_t> dio;
+            for (const auto& dr : c.diodes()) {
+                dio.push_back(dr.pos);
+                dio.push_back(dr.neg);
+                dio.push_back(dr.param);
+            }
+            d.prog_off[nsg::DP_diodes] = append(prog, dio);
+            d.param_off = b->param_off[i];
+            d.sol_off = b->sol_off[i];
+            b->param_off[i + 1] = b->param_off[i] + static_cast<int64_t>(c.params().size());
+            b->sol_off[i + 1] = b->sol_off[i] + c.num_vars();
+            b->host_params.insert(b->host_params.end(), c.params().begin(), c.params().end());
+            d.x_off = work; work = align4(work + d.n);
+            d.xold_off = work; work = align4(work + d.n);
+            d.w_off = work; work = align4(work + d.n);
+            d.a_off = work; work = align4(work + d.nnz);
+            d.lu_off = work; work = align4(work + p.nnz_lu);
+            d.tv_off = work; work = align4(work + c.n_terms());
+            d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
+            d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
+            b->updates += p.updates;
+            b->nnz_lu += p.nnz_lu;
+            b->nnz += p.nnz_a;
+            b->n += p.n;
+        }
+        const size_t smem = (sizeof(double) * 16 * ((b->max_col + 31) & ~31)) +
+                            sizeof(int32_t) * b->max_n;
+        if (smem > 200 * 1024)
+            return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: instance too large for the "
+                                         "shared-memory refactor (longest LU column " +
+                                         std::to_string(b->max_col) + ")");
+        cudaError_t e;
+        if ((e = upload(&b->d_lu_pool, lu_pool.data(), lu_pool.size())) != cudaSuccess ||
+            (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
+            (e = upload(&b->d_prog, prog.data(), prog.size())) != cudaSuccess ||
+            (e = upload(&b->d_descs, descs.data(), descs.size())) != cudaSuccess ||
+            (e = upload<double>(&b->d_work, nullptr, static_cast<size_t>(work))) != cudaSuccess ||
+            (e = upload(&b->d_params, b->host_params.data(), b->host_params.size())) != cudaSuccess)
+            return cuda_fail("nsg_dc_batch_create", e);
+        *out = b.release();
+        return NSG_OK;
+    });
+}
+
+void nsg_dc_batch_free(nsg_dc_batch* b) { delete b; }
+
+int nsg_dc_batch_layout(const nsg_dc_batch* b, long long* param_offsets,
+                        long long* solution_offsets) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_layout: null batch");
+    const size_t bytes = sizeof(long long) * (b->count + 1);
+    if (param_offsets) std::memcpy(param_offsets, b->param_off.data(), bytes);
+    if (solution_offsets) std::memcpy(solution_offsets, b->sol_off.data(), bytes);
+    return NSG_OK;
+}
+
+int nsg_dc_batch_stats(const nsg_dc_batch* b, long long* n, long long* nnz, long long* nnz_lu,
+                       long long* updates, int* distinct_topologies) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_stats: null batch");
+    if (n) *n = b->n;
+    if (nnz) *nnz = b->nnz;
+    if (nnz_lu) *nnz_lu = b->nnz_lu;
+    if (updates) *updates = b->updates;
+    if (distinct_topologies) *distinct_topologies = static_cast<int>(b->topos.size());
+    return NSG_OK;
+}
+
+int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, double abstol,
+                             double gmin, int max_iter) {
+    if (!b || max_iter <= 0) return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_options: bad arguments");
+    b->opt.reltol = reltol;
+    b->opt.vntol = vntol;
+    b->opt.abstol = abstol;
+    b->opt.gmin = gmin;
+    b->opt.max_iter = max_iter;
+    return NSG_OK;
+}
+
+int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
+                     int* d_iterations, void* stream) {
+    if (!b || !d_solutions || !d_status || !d_iterations)
+        return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: null argument");
+    cudaError_t e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, b->count, b->d_prog,
+                                          d_params ? d_params : b->d_params, b->d_work, d_solutions,
+                                          d_status, d_iterations, b->opt, b->max_col, b->max_n,
+                                          static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_dc_batch_run", e);
+}
+
+}  // extern "C"

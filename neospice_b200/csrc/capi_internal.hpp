@@ -1,0 +1,82 @@
+// Internal definitions shared by the C ABI translation units.
+#pragma once
+#include "nsgpu.h"
+
+#include "host/plan.hpp"
+#include "host/sparse_order.hpp"
+#include "kernels/lu_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <exception>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+struct nsg_topology {
+    std::unique_ptr<nsg::MarkowitzOrder> engine;  // null for an imported topology
+    std::vector<int32_t> slot_elem;
+    nsg::TopologyPlan plan;
+};
+
+struct nsg_batch {
+    int count = 0;
+    std::vector<long long> a_off, x_off, lu_off;
+    int32_t* d_pool = nullptr;
+    nsg::PlanDesc* d_plans = nullptr;
+    nsg::InstDesc* d_insts = nullptr;
+    double* d_lu = nullptr;
+    double* d_work = nullptr;
+    int max_col = 0;
+    int max_n = 0;
+    bool allow_flow = true;
+    ~nsg_batch() {
+        cudaFree(d_pool);
+        cudaFree(d_plans);
+        cudaFree(d_insts);
+        cudaFree(d_lu);
+        cudaFree(d_work);
+    }
+};
+
+namespace nsg_internal {
+
+int fail(int code, const std::string& msg);
+int cuda_fail(const char* where, cudaError_t e);
+void clear_error();
+
+// Run a body, mapping C++ exceptions to status codes.
+template <class F>
+int guarded(const char* where, F&& body) {
+    try {
+        clear_error();
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(NSG_ERR_NOMEM, std::string(where) + ": out of host memory");
+    } catch (const std::exception& e) {
+        return fail(NSG_ERR_INVALID, std::string(where) + ": " + e.what());
+    }
+}
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), count * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (src) e = cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// NeoSolver::numeric on the host engine (load, preorder, gmin, ordering).
+int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin);
+
+// nsg_topology_order without the C wrapper (throws on bad input).
+int order_topology(int n, int nnz, const int* col_ptr, const int* row_idx, const double* values,
+                   double diag_gmin, std::unique_ptr<nsg_topology>& out);
+
+// PlanDesc for a plan whose arrays were appended to pool.
+nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& pool);
+
+}  // namespace nsg_internal

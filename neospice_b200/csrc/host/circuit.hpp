@@ -1,0 +1,117 @@
+// Host-side circuit topology for the batched Newton loop.
+//
+// A Circuit is built through typed calls that mirror the reference's Circuit
+// API (src/core/circuit.hpp:179-237) for the devices on the GPU path, then
+// finalized the way Circuit::finalize does it (src/core/circuit.cpp:201-283):
+// ngspice load order, branch indices, sparsity pattern, dead-node
+// placeholders.  Finalization also compiles a stamp program: for every matrix
+// slot and right-hand-side row, the list of device terms in the order the
+// reference's devices add them, so the GPU sums every entry in the same
+// sequence of IEEE additions.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace nsg {
+
+// ngspice load rank of each device family (src/core/circuit.cpp:34-59).
+enum class DevKind : int32_t { Diode = 22, ISource = 31, Resistor = 41, VSource = 50 };
+
+// How a constant term value is made from the instance's parameters.
+enum TermOp : int32_t {
+    kTermRecip = 0,     // +1/p           (resistor conductance)
+    kTermNegRecip = 1,  // -(1/p)
+    kTermValue = 2,     // +p             (source value)
+    kTermNegValue = 3,  // -p
+    kTermOne = 4,       // +1.0
+    kTermMinusOne = 5,  // -1.0
+    kTermZero = 6,      // +0.0
+    kTermMinusZero = 7, // -0.0
+    kTermGmin = 8,      // the dead-node pin conductance (SimOptions::gmin)
+};
+
+// Values each diode writes per Newton iteration, in this order, after the
+// constant terms (DIOload's right-hand side and matrix loads,
+// src/devices/dio/dio_load.cpp:392-406, for RS = 0 so gspr = 0).
+enum DiodeTerm : int32_t { kDGd = 0, kDGdPlusGspr = 1, kDNegGd = 2, kDCdeq = 3, kDNegCdeq = 4,
+                           kDiodeTerms = 5 };
+
+struct DeviceRec {
+    DevKind kind;
+    int32_t created;   // creation index over all devices
+    int32_t a, b;      // terminals (0-based node, -1 = ground)
+    int32_t param;     // first parameter index
+    int32_t branch;    // VSource branch unknown, else -1
+};
+
+class Circuit {
+public:
+    explicit Circuit(int32_t num_nodes);
+
+    // Parameters of every device are kept in creation order in params():
+    // resistor {ohms}, vsource {volts}, isource {amps}, diode {IS, N}.
+    int32_t add_resistor(int32_t a, int32_t b, double ohms);
+    int32_t add_vsource(int32_t p, int32_t n, double volts);
+    int32_t add_isource(int32_t p, int32_t n, double amps);
+    int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission);
+
+    void finalize();
+    bool finalized() const { return finalized_; }
+
+    int32_t num_nodes() const { return num_nodes_; }
+    int32_t num_vars() const { return num_vars_; }
+    int32_t nnz() const { return static_cast<int32_t>(row_idx_.size()); }
+    const std::vector<int32_t>& col_ptr() const { return col_ptr_; }
+    const std::vector<int32_t>& row_idx() const { return row_idx_; }
+    const std::vector<double>& params() const { return params_; }
+    const std::vector<int32_t>& dead_nodes() const { return dead_nodes_; }
+
+    // Diodes in load order: anode, cathode (-1 = ground), parameter index.
+    struct DiodeRec { int32_t pos, neg, param; };
+    const std::vector<DiodeRec>& diodes() const { return diodes_; }
+
+    // Stamp program (valid after finalize).
+    // Constant terms: term_op/term_param, count n_const_terms().  Dynamic
+    // terms follow: kDiodeTerms per diode in load order.
+    int32_t n_const_terms() const { return static_cast<int32_t>(term_op_.size()); }
+    int32_t n_terms() const { return n_const_terms() + kDiodeTerms * static_cast<int32_t>(diodes_.size()); }
+    const std::vector<int32_t>& term_op() const { return term_op_; }
+    const std::vector<int32_t>& term_param() const { return term_param_; }
+    // Per matrix slot / rhs row: ptr (size+1) and term indices, in add order.
+    const std::vector<int32_t>& slot_ptr() const { return slot_ptr_; }
+    const std::vector<int32_t>& slot_terms() const { return slot_terms_; }
+    const std::vector<int32_t>& rhs_ptr() const { return rhs_ptr_; }     // native devices
+    const std::vector<int32_t>& rhs_terms() const { return rhs_terms_; }
+    const std::vector<int32_t>& ucb_ptr() const { return ucb_ptr_; }     // UCB-style devices
+    const std::vector<int32_t>& ucb_terms() const { return ucb_terms_; }
+
+    // Host evaluation of the matrix and rhs at the first Newton iteration of
+    // a DC operating point (MODEDCOP | MODEINITJCT, zero initial guess), with
+    // host libm -- the values the reference's first NeoSolver::numeric sees.
+    void initjct_values(std::vector<double>& a, std::vector<double>& rhs,
+                        double gmin) const;
+
+private:
+    int32_t num_nodes_;
+    int32_t num_vars_ = 0;
+    bool finalized_ = false;
+    std::vector<DeviceRec> devices_;
+    std::vector<double> params_;
+    std::vector<int32_t> col_ptr_, row_idx_, dead_nodes_;
+    std::vector<DiodeRec> diodes_;
+    std::vector<int32_t> term_op_, term_param_;
+    std::vector<int32_t> slot_ptr_, slot_terms_, rhs_ptr_, rhs_terms_, ucb_ptr_, ucb_terms_;
+
+    void check_node(int32_t v) const;
+    int32_t offset(int32_t r, int32_t c) const;  // -1 when ground or absent
+};
+
+// Physical constants as the reference's diode shim defines them
+// (src/devices/dio/dio_shim.hpp:23, ucb_compat.hpp), and the nominal
+// temperature (src/core/types.hpp:18).
+constexpr double kKoverQ = 1.38064852e-23 / 1.6021766208e-19;
+constexpr double kRoot2 = 1.4142135623730950488;
+constexpr double kEuler = 2.7182818284590452354;
+constexpr double kTNominal = 300.15;
+
+}  // namespace nsg

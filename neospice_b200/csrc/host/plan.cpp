@@ -54,12 +54,14 @@ void finish(TopologyPlan& p) {
                 if (d < 0)
                     throw std::invalid_argument("plan: fill pattern not closed at column " +
                                                 std::to_string(j));
-                p.upd_dst.push_back(d);
+                p.upd_dst.push_back(d - p.col_ptr[j]);  // relative to column j
             }
         }
         for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) where[p.row_idx[q]] = -1;
     }
     p.updates = static_cast<int64_t>(p.upd_dst.size());
+    p.max_col = 0;
+    for (int32_t j = 0; j < n; ++j) p.max_col = std::max(p.max_col, p.col_ptr[j + 1] - p.col_ptr[j]);
     if (p.updates > INT32_MAX) throw std::invalid_argument("plan: update map too large");
 
     // Row-wise L and U.

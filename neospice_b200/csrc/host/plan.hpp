@@ -13,6 +13,7 @@ struct TopologyPlan {
     int32_t n = 0;
     int32_t nnz_a = 0;   // slots of the caller's CSC pattern
     int32_t nnz_lu = 0;  // originals + fill-ins
+    int32_t max_col = 0; // longest LU column
 
     // internal index i (0-based) -> external row / column (0-based).
     std::vector<int32_t> perm_row, perm_col;
@@ -28,8 +29,9 @@ struct TopologyPlan {
     std::vector<int32_t> a_to_lu;
 
     // Refactor update map.  For the U entry at position q = (r, j):
-    // upd_start[q] indexes upd_dst, where the |L(:, r)| destinations in
-    // column j of L(:, r)'s rows are stored in L(:, r)'s order.
+    // upd_start[q] indexes upd_dst, where the |L(:, r)| destinations of
+    // L(:, r)'s rows are stored in L(:, r)'s order, as positions relative to
+    // the start of column j.
     std::vector<int32_t> upd_start, upd_dst;
 
     // L by rows (strictly lower, columns ascending) and U by rows (strictly

@@ -1,0 +1,260 @@
+// CTA-level building blocks: one thread block refactors / solves one
+// instance.  Used by the standalone batched kernels (lu_kernels.cu) and by the
+// fused Newton kernel (newton_dc.cu).
+//
+// Rounding order.  Every value is produced by the same sequence of IEEE
+// double operations as the reference's SparseMatrix::factor / solve /
+// solve_transposed (src/solver/factor.cpp:980-1052, solve.cpp:6-47,
+// :102-141): updates into one entry are applied in ascending pivot order, one
+// at a time, with separately rounded multiply and subtract (__dmul_rn,
+// __dsub_rn: no FMA contraction).  Results are therefore bit-identical to the
+// reference under the same pivot sequence.
+#pragma once
+#include "lu_device.cuh"
+
+#include <cuda_runtime.h>
+
+namespace nsg {
+
+constexpr int kFlowWarps = 16;
+constexpr int kFlowThreads = kFlowWarps * 32;
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ double lu_mul(double x, double y) { return __dmul_rn(x, y); }
+__device__ __forceinline__ double lu_sub(double x, double y) { return __dsub_rn(x, y); }
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Shared memory of the dataflow refactor: kFlowWarps column buffers of
+// colbuf doubles, then n int32 completion flags.
+__host__ __device__ inline size_t flow_smem_bytes(int colbuf, int n) {
+    return sizeof(double) * kFlowWarps * colbuf + sizeof(int32_t) * n;
+}
+
+struct RefactorResult {
+    int32_t code;  // kStatus*
+    int32_t step;  // failing pivot step or -1
+};
+
+// Dataflow refactor of one instance by the whole CTA (blockDim.x ==
+// kFlowThreads).  Warps claim columns in pivot order from a shared counter;
+// before using column r a warp waits for done[r], so independent columns
+// overlap and the dense trailing block pipelines as a wavefront.  Column j
+// stays in a per-warp shared buffer from its load (A gathered through lu_src,
+// diag_gmin added to the pivot) to its write-back.  check_pivots applies the
+// re-validation test of SparseMatrix::order_and_factor (factor.cpp:929-947);
+// otherwise only an exact zero pivot fails, as in SparseMatrix::factor.  Every
+// wait is bounded: past kSpinLimit polls the instance reports kStatusTimeout
+// and the warp moves on, so the CTA always finishes.  Begins and ends with
+// __syncthreads().
+__device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
+                                                   const double* __restrict__ a, double* __restrict__ lu,
+                                                   double diag_gmin, int check_pivots,
+                                                   double rel_threshold, double* smem, int colbuf) {
+    const int32_t n = pd.n;
+    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
+    const int32_t* row_idx = pool + pd.off[PA_row_idx];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const int32_t* lu_src = pool + pd.off[PA_lu_src];
+    const int32_t* upd_start = pool + pd.off[PA_upd_start];
+    const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    double* buf = smem + warp * colbuf;
+    volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + kFlowWarps * colbuf);
+
+    __shared__ int32_t s_next, s_fail_step, s_fail_code;
+    __syncthreads();
+    for (int32_t j = threadIdx.x; j < n; j += blockDim.x) done[j] = 0;
+    if (threadIdx.x == 0) {
+        s_next = 0;
+        s_fail_step = INT32_MAX;
+        s_fail_code = kStatusOk;
+    }
+    __syncthreads();
+
+    for (;;) {
+        int32_t j = 0;
+        if (lane == 0) j = atomicAdd(&s_next, 1);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j >= n) break;
+        const int32_t c0 = col_ptr[j];
+        const int32_t len = col_ptr[j + 1] - c0;
+        const int32_t dj = diag_pos[j] - c0;
+        for (int32_t t = lane; t < len; t += 32) {
+            const int32_t s = lu_src[c0 + t];
+            double v = (s >= 0) ? a[s] : 0.0;
+            if (t == dj && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+            buf[t] = v;
+        }
+        __syncwarp();
+        bool timed_out = false;
+        for (int32_t q = 0; q < dj; ++q) {
+            const int32_t r = row_idx[c0 + q];
+            if (lane == 0) {
+                int spins = 0;
+                while (done[r] == 0) {
+                    if (++spins > kSpinLimit) {
+                        timed_out = true;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                __threadfence_block();
+            }
+            timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
+            __syncwarp();
+            if (timed_out) break;
+            const int32_t dr = diag_pos[r];
+            const double u = lu_mul(buf[q], lu[dr]);
+            __syncwarp();
+            if (lane == 0) buf[q] = u;
+            const int32_t l0 = dr + 1;
+            const int32_t cnt = col_ptr[r + 1] - l0;
+            const int32_t* dst = upd_dst + upd_start[c0 + q];
+            for (int32_t t = lane; t < cnt; t += 32) {
+                const int32_t d = dst[t];
+                buf[d] = lu_sub(buf[d], lu_mul(u, lu[l0 + t]));
+            }
+            __syncwarp();
+        }
+        const double piv = buf[dj];
+        bool fail;
+        if (check_pivots) {
+            double largest = 0.0;
+            for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(buf[t]));
+            largest = warp_max(largest);
+            fail = !(largest * rel_threshold < fabs(piv));
+        } else {
+            fail = (piv == 0.0);
+        }
+        for (int32_t t = lane; t < len; t += 32) lu[c0 + t] = (t == dj) ? 1.0 / piv : buf[t];
+        __syncwarp();
+        if (lane == 0) {
+            if (timed_out) {
+                s_fail_code = kStatusTimeout;
+                atomicMin(&s_fail_step, j);
+            } else if (fail) {
+                atomicMin(&s_fail_step, j);
+                if (s_fail_code != kStatusTimeout)
+                    s_fail_code = check_pivots ? kStatusReorder : kStatusSingular;
+            }
+            __threadfence_block();
+            done[j] = 1;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    RefactorResult res;
+    res.code = s_fail_code;
+    res.step = (s_fail_code == kStatusOk) ? -1 : s_fail_step;
+    __syncthreads();
+    return res;
+}
+
+// x <- A^{-1} x (SparseMatrix::solve) by the whole CTA; w is an n-vector of
+// scratch.  Level-synchronous, a thread per row.  Begins and ends with
+// __syncthreads().
+__device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__ pool,
+                                 const double* __restrict__ lu, double* __restrict__ x,
+                                 double* __restrict__ w) {
+    const int32_t n = pd.n;
+    const int32_t* perm_row = pool + pd.off[PA_perm_row];
+    const int32_t* perm_col = pool + pd.off[PA_perm_col];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
+    __syncthreads();
+    {   // forward: L with the reciprocal pivot, row-oriented gather
+        const int32_t* lp = pool + pd.off[PA_lrow_ptr];
+        const int32_t* lpos = pool + pd.off[PA_lrow_pos];
+        const int32_t* lcol = pool + pd.off[PA_lrow_col];
+        const int32_t* lev_ptr = pool + pd.off[PA_fwd_lev_ptr];
+        const int32_t* lev = pool + pd.off[PA_fwd_lev];
+        for (int32_t l = 0; l < pd.n_fwd_lev; ++l) {
+            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
+                const int32_t i = lev[k];
+                double t = w[i];
+                for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
+                    const double xc = w[lcol[e]];
+                    if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu[lpos[e]]));
+                }
+                w[i] = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
+            }
+            __syncthreads();
+        }
+    }
+    {   // backward: unit-diagonal U, row dot products
+        const int32_t* up = pool + pd.off[PA_urow_ptr];
+        const int32_t* upos = pool + pd.off[PA_urow_pos];
+        const int32_t* ucol = pool + pd.off[PA_urow_col];
+        const int32_t* lev_ptr = pool + pd.off[PA_bwd_lev_ptr];
+        const int32_t* lev = pool + pd.off[PA_bwd_lev];
+        for (int32_t l = 0; l < pd.n_bwd_lev; ++l) {
+            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
+                const int32_t i = lev[k];
+                double t = w[i];
+                for (int32_t e = up[i]; e < up[i + 1]; ++e)
+                    t = lu_sub(t, lu_mul(lu[upos[e]], w[ucol[e]]));
+                w[i] = t;
+            }
+            __syncthreads();
+        }
+    }
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_col[i]] = w[i];
+    __syncthreads();
+}
+
+// x <- A^{-T} x (SparseMatrix::solve_transposed) by the whole CTA.
+__device__ inline void cta_solve_transposed(const PlanDesc& pd, const int32_t* __restrict__ pool,
+                                            const double* __restrict__ lu, double* __restrict__ x,
+                                            double* __restrict__ w) {
+    const int32_t n = pd.n;
+    const int32_t* perm_row = pool + pd.off[PA_perm_row];
+    const int32_t* perm_col = pool + pd.off[PA_perm_col];
+    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
+    const int32_t* row_idx = pool + pd.off[PA_row_idx];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_col[i]];
+    __syncthreads();
+    {   // forward over U^T: column c gathers its U entries, rows ascending
+        const int32_t* lev_ptr = pool + pd.off[PA_col_lev_ptr];
+        const int32_t* lev = pool + pd.off[PA_col_lev];
+        for (int32_t l = 0; l < pd.n_col_lev; ++l) {
+            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
+                const int32_t c = lev[k];
+                double t = w[c];
+                for (int32_t q = col_ptr[c]; q < diag_pos[c]; ++q) {
+                    const double xr = w[row_idx[q]];
+                    if (xr != 0.0) t = lu_sub(t, lu_mul(xr, lu[q]));
+                }
+                w[c] = t;
+            }
+            __syncthreads();
+        }
+    }
+    {   // backward over L^T with the reciprocal pivot
+        const int32_t* lev_ptr = pool + pd.off[PA_tbw_lev_ptr];
+        const int32_t* lev = pool + pd.off[PA_tbw_lev];
+        for (int32_t l = 0; l < pd.n_tbw_lev; ++l) {
+            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
+                const int32_t i = lev[k];
+                double t = w[i];
+                for (int32_t q = diag_pos[i] + 1; q < col_ptr[i + 1]; ++q)
+                    t = lu_sub(t, lu_mul(lu[q], w[row_idx[q]]));
+                w[i] = lu_mul(t, lu[diag_pos[i]]);
+            }
+            __syncthreads();
+        }
+    }
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_row[i]] = w[i];
+    __syncthreads();
+}
+
+}  // namespace nsg

@@ -16,7 +16,7 @@ enum PlanArray : int {
 struct PlanDesc {
     int32_t n, nnz_a, nnz_lu;
     int32_t n_col_lev, n_fwd_lev, n_bwd_lev, n_tbw_lev;
-    int32_t pad;
+    int32_t max_col;  // longest LU column
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
 };
 
@@ -34,6 +34,7 @@ enum : int32_t {
     kStatusOk = 0,
     kStatusSingular = 102,  // exact zero pivot (SparseError::ZeroDiag)
     kStatusReorder = 103,   // pivot failed the relative threshold
+    kStatusTimeout = 104,   // a bounded dependency wait gave up (no result)
 };
 
 }  // namespace nsg

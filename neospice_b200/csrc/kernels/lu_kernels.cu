@@ -13,14 +13,13 @@
 // at a time, with separately rounded multiply and subtract (__dmul_rn,
 // __dsub_rn: no FMA contraction).  Results are therefore bit-identical to the
 // reference under the same pivot sequence.
-#include "lu_device.cuh"
+#include "lu_cta.cuh"
 
 #include <cuda_runtime.h>
 
 namespace nsg {
 
 namespace {
-
 struct PlanView {
     const int32_t* a[PA_COUNT];
     __device__ PlanView(const PlanDesc& d, const int32_t* pool) {
@@ -29,16 +28,8 @@ struct PlanView {
     }
     __device__ const int32_t* operator[](int k) const { return a[k]; }
 };
-
 __device__ __forceinline__ double mul(double x, double y) { return __dmul_rn(x, y); }
 __device__ __forceinline__ double sub(double x, double y) { return __dsub_rn(x, y); }
-
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
 }  // namespace
 
 // Load A into the LU pattern, add diag_gmin to every pivot, then eliminate
@@ -99,8 +90,9 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
                 const int32_t l0 = diag_pos[r] + 1;
                 const int32_t cnt = col_ptr[r + 1] - l0;
                 const int32_t* dst = upd_dst + upd_start[q];
+                const int32_t c0 = col_ptr[j];
                 for (int32_t t = lane; t < cnt; t += 32) {
-                    const int32_t d = dst[t];
+                    const int32_t d = c0 + dst[t];
                     lu[d] = sub(lu[d], mul(u, lu[l0 + t]));
                 }
                 __syncwarp();
@@ -134,62 +126,31 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
     }
 }
 
+// Dataflow refactor (cta_refactor_flow), one CTA per instance.
+__global__ void __launch_bounds__(kFlowThreads)
+refactor_flow_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
+                     const InstDesc* __restrict__ insts, const double* __restrict__ A,
+                     double* __restrict__ LU, double diag_gmin, int check_pivots,
+                     double rel_threshold, int32_t* __restrict__ status,
+                     int32_t* __restrict__ fail_step, int colbuf) {
+    extern __shared__ double smem[];
+    const InstDesc inst = insts[blockIdx.x];
+    const RefactorResult r =
+        cta_refactor_flow(plans[inst.plan], pool, A + inst.a_off, LU + inst.lu_off, diag_gmin,
+                          check_pivots, rel_threshold, smem, colbuf);
+    if (threadIdx.x == 0) {
+        status[blockIdx.x] = r.code;
+        if (fail_step) fail_step[blockIdx.x] = r.step;
+    }
+}
+
 // x <- A^{-1} x with the factored LU (SparseMatrix::solve).
 __global__ void __launch_bounds__(256)
 solve_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
              const InstDesc* __restrict__ insts, const double* __restrict__ LU,
              double* __restrict__ X, double* __restrict__ W) {
     const InstDesc inst = insts[blockIdx.x];
-    const PlanDesc& pd = plans[inst.plan];
-    const PlanView p(pd, pool);
-    const int32_t n = pd.n;
-    const double* lu = LU + inst.lu_off;
-    double* x = X + inst.x_off;
-    double* w = W + inst.w_off;
-    const int32_t* perm_row = p[PA_perm_row];
-    const int32_t* perm_col = p[PA_perm_col];
-    const int32_t* diag_pos = p[PA_diag_pos];
-
-    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
-    __syncthreads();
-
-    {   // forward: L with the reciprocal pivot, row-oriented gather
-        const int32_t* lp = p[PA_lrow_ptr];
-        const int32_t* lpos = p[PA_lrow_pos];
-        const int32_t* lcol = p[PA_lrow_col];
-        const int32_t* lev_ptr = p[PA_fwd_lev_ptr];
-        const int32_t* lev = p[PA_fwd_lev];
-        for (int32_t l = 0; l < pd.n_fwd_lev; ++l) {
-            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
-                const int32_t i = lev[k];
-                double t = w[i];
-                for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
-                    const double xc = w[lcol[e]];
-                    if (xc != 0.0) t = sub(t, mul(xc, lu[lpos[e]]));
-                }
-                w[i] = (t != 0.0) ? mul(t, lu[diag_pos[i]]) : t;
-            }
-            __syncthreads();
-        }
-    }
-    {   // backward: unit-diagonal U, row dot products
-        const int32_t* up = p[PA_urow_ptr];
-        const int32_t* upos = p[PA_urow_pos];
-        const int32_t* ucol = p[PA_urow_col];
-        const int32_t* lev_ptr = p[PA_bwd_lev_ptr];
-        const int32_t* lev = p[PA_bwd_lev];
-        for (int32_t l = 0; l < pd.n_bwd_lev; ++l) {
-            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
-                const int32_t i = lev[k];
-                double t = w[i];
-                for (int32_t e = up[i]; e < up[i + 1]; ++e)
-                    t = sub(t, mul(lu[upos[e]], w[ucol[e]]));
-                w[i] = t;
-            }
-            __syncthreads();
-        }
-    }
-    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_col[i]] = w[i];
+    cta_solve(plans[inst.plan], pool, LU + inst.lu_off, X + inst.x_off, W + inst.w_off);
 }
 
 // x <- A^{-T} x with the same LU (SparseMatrix::solve_transposed).
@@ -198,61 +159,34 @@ solve_transposed_kernel(const PlanDesc* __restrict__ plans, const int32_t* __res
                         const InstDesc* __restrict__ insts, const double* __restrict__ LU,
                         double* __restrict__ X, double* __restrict__ W) {
     const InstDesc inst = insts[blockIdx.x];
-    const PlanDesc& pd = plans[inst.plan];
-    const PlanView p(pd, pool);
-    const int32_t n = pd.n;
-    const double* lu = LU + inst.lu_off;
-    double* x = X + inst.x_off;
-    double* w = W + inst.w_off;
-    const int32_t* perm_row = p[PA_perm_row];
-    const int32_t* perm_col = p[PA_perm_col];
-    const int32_t* col_ptr = p[PA_col_ptr];
-    const int32_t* row_idx = p[PA_row_idx];
-    const int32_t* diag_pos = p[PA_diag_pos];
-
-    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_col[i]];
-    __syncthreads();
-
-    {   // forward over U^T: column c gathers its U entries, rows ascending
-        const int32_t* lev_ptr = p[PA_col_lev_ptr];
-        const int32_t* lev = p[PA_col_lev];
-        for (int32_t l = 0; l < pd.n_col_lev; ++l) {
-            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
-                const int32_t c = lev[k];
-                double t = w[c];
-                for (int32_t q = col_ptr[c]; q < diag_pos[c]; ++q) {
-                    const double xr = w[row_idx[q]];
-                    if (xr != 0.0) t = sub(t, mul(xr, lu[q]));
-                }
-                w[c] = t;
-            }
-            __syncthreads();
-        }
-    }
-    {   // backward over L^T with the reciprocal pivot
-        const int32_t* lev_ptr = p[PA_tbw_lev_ptr];
-        const int32_t* lev = p[PA_tbw_lev];
-        for (int32_t l = 0; l < pd.n_tbw_lev; ++l) {
-            for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
-                const int32_t i = lev[k];
-                double t = w[i];
-                for (int32_t q = diag_pos[i] + 1; q < col_ptr[i + 1]; ++q)
-                    t = sub(t, mul(lu[q], w[row_idx[q]]));
-                w[i] = mul(t, lu[diag_pos[i]]);
-            }
-            __syncthreads();
-        }
-    }
-    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_row[i]] = w[i];
+    cta_solve_transposed(plans[inst.plan], pool, LU + inst.lu_off, X + inst.x_off, W + inst.w_off);
 }
 
+// max_col / max_n: largest LU column and order over the batch's plans.
 cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                             int count, const double* A, double* LU, double diag_gmin,
                             int check_pivots, double rel_threshold, int32_t* status,
-                            int32_t* fail_step, cudaStream_t stream) {
+                            int32_t* fail_step, int max_col, int max_n, bool allow_flow,
+                            cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
-    refactor_kernel<<<count, 256, 0, stream>>>(plans, pool, insts, A, LU, diag_gmin,
-                                               check_pivots, rel_threshold, status, fail_step);
+    const int colbuf = (max_col + 31) & ~31;
+    const size_t smem = flow_smem_bytes(colbuf, max_n);
+    if (allow_flow && smem <= 200 * 1024) {
+        static bool configured = false;
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(refactor_flow_kernel,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024);
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        refactor_flow_kernel<<<count, kFlowThreads, smem, stream>>>(
+            plans, pool, insts, A, LU, diag_gmin, check_pivots, rel_threshold, status, fail_step,
+            colbuf);
+    } else {
+        refactor_kernel<<<count, 256, 0, stream>>>(plans, pool, insts, A, LU, diag_gmin,
+                                                   check_pivots, rel_threshold, status, fail_step);
+    }
     return cudaGetLastError();
 }
 

@@ -115,6 +115,10 @@ class Batch:
     def count(self):
         return len(self.topologies)
 
+    def set_schedule(self, schedule: int):
+        """0 = dataflow refactor (default), 1 = level-synchronous."""
+        L.check(L.lib().nsg_batch_set_schedule(self._h, int(schedule)))
+
     def refactor(self, d_values, diag_gmin=0.0, check_pivots=False, d_status=None,
                  d_fail_step=None, stream=None):
         """Batched spFactor; returns the device status tensor (int32)."""

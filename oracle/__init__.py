@@ -73,6 +73,8 @@ def ref() -> ctypes.CDLL:
         lib.nsref_solver_element_count.argtypes = [_V]
         lib.nsref_solver_export.argtypes = [_V] * 7
         lib.nsref_mesh_dc.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V, _V]
+        lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
+                                           _V, _V, _V]
         _ref = lib
     return _ref
 
@@ -166,3 +168,45 @@ class RefSolver:
         se = np.zeros(len(self.row_idx), np.int32)
         ref().nsref_solver_export(self.h, _p(r), _p(c), _p(er), _p(ec), _p(ev), _p(se))
         return Structure(n, r, c, er, ec, se), ev
+
+
+# --- the reference on diode meshes (neospice_b200.workloads.DiodeMesh) -------
+
+def _mesh_args(m):
+    arrs = dict(r_h=np.ascontiguousarray(m.r_h, np.float64),
+                r_v=np.ascontiguousarray(m.r_v, np.float64),
+                dn=np.ascontiguousarray(m.diode_nodes, np.int32),
+                isn=np.ascontiguousarray(m.isrc_nodes, np.int32),
+                ia=np.ascontiguousarray(m.isrc_amps, np.float64))
+    args = (m.side, _p(arrs["r_h"]), _p(arrs["r_v"]), len(arrs["dn"]), _p(arrs["dn"]),
+            float(m.diode_is), float(m.diode_n), len(arrs["isn"]), _p(arrs["isn"]),
+            _p(arrs["ia"]), float(m.v_corner))
+    return args, arrs
+
+
+def ref_mesh_dc(m):
+    """The reference's DC operating point of a diode mesh: (solution,
+    Newton iterations, seconds)."""
+    args, keep = _mesh_args(m)
+    sol = np.zeros(m.num_vars)
+    it = ctypes.c_int(0)
+    sec = ctypes.c_double(0.0)
+    nv = ref().nsref_mesh_dc(*args, _p(sol), ctypes.addressof(it), ctypes.addressof(sec))
+    if nv != m.num_vars:
+        raise RuntimeError(f"reference DC failed ({nv})")
+    return sol, it.value, sec.value
+
+
+def ref_mesh_initjct(m):
+    """The reference's first-iteration matrix: (col_ptr, row_idx, values, rhs)."""
+    args, keep = _mesh_args(m)
+    nv = ctypes.c_int(0)
+    nnz = ref().nsref_mesh_initjct(*args, ctypes.addressof(nv), None, None, None, None)
+    cp = np.zeros(nv.value + 1, np.int32)
+    ri = np.zeros(nnz, np.int32)
+    vals = np.zeros(nnz)
+    rhs = np.zeros(nv.value)
+    rc = ref().nsref_mesh_initjct(*args, ctypes.addressof(nv), _p(cp), _p(ri), _p(vals), _p(rhs))
+    if rc != nnz:
+        raise RuntimeError("reference INITJCT evaluation failed")
+    return cp, ri, vals, rhs

@@ -25,6 +25,7 @@
 #include "core/circuit.hpp"
 #include "core/dc.hpp"
 #include "core/matrix.hpp"
+#include "core/newton.hpp"
 #include "core/solver_iface.hpp"
 #include "solver/config.hpp"
 #include "solver/error.hpp"
@@ -166,59 +167,108 @@ int nsref_solver_export(void* h, int* int_to_ext_row, int* int_to_ext_col,
     return e_idx;
 }
 
-// Diode-clamped resistor mesh, DC operating point through the reference's
-// typed Circuit API and Simulator::run_dc.  Node (x, y) is "n<y*side+x>" and is
-// created in that order, so its MNA index is y*side+x; the corner source's
-// branch current follows at index side*side.  r_h holds the (side-1)*side
-// horizontal resistors (x, y)-(x+1, y) row by row, r_v the side*(side-1)
-// vertical ones (x, y)-(x, y+1).  Devices are created R (horizontal, then
-// vertical), D, I, V in that order.  Returns the number of unknowns written
-// to solution, or -1 when the reference threw.
-int nsref_mesh_dc(int side, const double* r_h, const double* r_v,
-                  int n_diodes, const int* diode_node, double is, double n_emis,
-                  int n_isrc, const int* isrc_node, const double* isrc_amps,
-                  double v_corner, double* solution, int* iterations,
-                  double* seconds) {
+namespace {
+
+// The diode-clamped mesh through the reference's typed Circuit API.  Node
+// (x, y) is "n<y*side+x>" and is created in that order, so its MNA index is
+// y*side+x; the corner source's branch current follows at index side*side.
+// r_h holds the (side-1)*side horizontal resistors (x, y)-(x+1, y) row by
+// row, r_v the side*(side-1) vertical ones (x, y)-(x, y+1).  Devices are
+// created R (horizontal, then vertical), D, I, V in that order.
+void build_mesh(Circuit& ckt, int side, const double* r_h, const double* r_v, int n_diodes,
+                const int* diode_node, double is, double n_emis, int n_isrc,
+                const int* isrc_node, const double* isrc_amps, double v_corner) {
+    const int N = side * side;
+    std::vector<NodeId> nodes(N);
+    for (int i = 0; i < N; ++i) nodes[i] = ckt.node("n" + std::to_string(i));
+    int k = 0;
+    for (int y = 0; y < side; ++y)
+        for (int x = 0; x + 1 < side; ++x, ++k)
+            ckt.R("rh" + std::to_string(k), nodes[y * side + x], nodes[y * side + x + 1], r_h[k]);
+    k = 0;
+    for (int y = 0; y + 1 < side; ++y)
+        for (int x = 0; x < side; ++x, ++k)
+            ckt.R("rv" + std::to_string(k), nodes[y * side + x], nodes[(y + 1) * side + x], r_v[k]);
+    char card[160];
+    std::snprintf(card, sizeof card, ".model dmod D(IS=%.17g N=%.17g)", is, n_emis);
+    ckt.model(card);
+    for (int d = 0; d < n_diodes; ++d)
+        ckt.D("d" + std::to_string(d), nodes[diode_node[d]], GND, "dmod");
+    for (int s = 0; s < n_isrc; ++s)
+        ckt.I("i" + std::to_string(s), GND, nodes[isrc_node[s]], isrc_amps[s]);
+    ckt.V("vc", nodes[0], GND, v_corner);
+    ckt.finalize_if_needed();
+}
+
+}  // namespace
+
+// DC operating point of the mesh through solve_dc (Simulator::run_dc's
+// engine).  Returns the number of unknowns written to solution, or -1 when
+// the reference threw.
+int nsref_mesh_dc(int side, const double* r_h, const double* r_v, int n_diodes,
+                  const int* diode_node, double is, double n_emis, int n_isrc,
+                  const int* isrc_node, const double* isrc_amps, double v_corner,
+                  double* solution, int* iterations, double* seconds) {
     try {
         auto t0 = std::chrono::steady_clock::now();
         Circuit ckt;
-        const int N = side * side;
-        std::vector<NodeId> nodes(N);
-        for (int i = 0; i < N; ++i) nodes[i] = ckt.node("n" + std::to_string(i));
-        int k = 0;
-        for (int y = 0; y < side; ++y)
-            for (int x = 0; x + 1 < side; ++x, ++k)
-                ckt.R("rh" + std::to_string(k), nodes[y * side + x],
-                      nodes[y * side + x + 1], r_h[k]);
-        k = 0;
-        for (int y = 0; y + 1 < side; ++y)
-            for (int x = 0; x < side; ++x, ++k)
-                ckt.R("rv" + std::to_string(k), nodes[y * side + x],
-                      nodes[(y + 1) * side + x], r_v[k]);
-        char card[160];
-        std::snprintf(card, sizeof card, ".model dmod D(IS=%.17g N=%.17g)", is, n_emis);
-        ckt.model(card);
-        for (int d = 0; d < n_diodes; ++d)
-            ckt.D("d" + std::to_string(d), nodes[diode_node[d]], GND, "dmod");
-        for (int s = 0; s < n_isrc; ++s)
-            ckt.I("i" + std::to_string(s), GND, nodes[isrc_node[s]], isrc_amps[s]);
-        ckt.V("vc", nodes[0], GND, v_corner);
-        ckt.finalize_if_needed();
+        build_mesh(ckt, side, r_h, r_v, n_diodes, diode_node, is, n_emis, n_isrc, isrc_node,
+                   isrc_amps, v_corner);
         DCResult res = solve_dc(ckt);
         const auto* op = ckt.operating_point();
-        int nv = ckt.num_vars();
-        if (op) {
-            for (int i = 0; i < nv; ++i) solution[i] = (*op)[i];
-        } else {
-            for (int i = 0; i < N; ++i)
-                solution[i] = res.voltage("n" + std::to_string(i));
-        }
+        const int nv = ckt.num_vars();
+        if (!op) return -1;
+        for (int i = 0; i < nv; ++i) solution[i] = (*op)[i];
         if (iterations) *iterations = res.status.iterations;
         auto t1 = std::chrono::steady_clock::now();
         if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
         return nv;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "nsref_mesh_dc: %s\n", e.what());
+        return -1;
+    }
+}
+
+// The matrix and rhs of the first DC Newton iteration (MODEDCOP |
+// MODEINITJCT, zero guess): newton_solve's device-load block
+// (src/core/newton.cpp:141-175) run once.  col_ptr (num_vars+1), row_idx
+// (nnz), values (nnz), rhs (num_vars).  Returns nnz, or -1.  Call with null
+// arrays to get sizes: *num_vars and the return value.
+int nsref_mesh_initjct(int side, const double* r_h, const double* r_v, int n_diodes,
+                       const int* diode_node, double is, double n_emis, int n_isrc,
+                       const int* isrc_node, const double* isrc_amps, double v_corner,
+                       int* num_vars, int* col_ptr, int* row_idx, double* values, double* rhs_out) {
+    try {
+        Circuit ckt;
+        build_mesh(ckt, side, r_h, r_v, n_diodes, diode_node, is, n_emis, n_isrc, isrc_node,
+                   isrc_amps, v_corner);
+        const int n = ckt.num_vars();
+        const auto& pattern = ckt.pattern();
+        if (num_vars) *num_vars = n;
+        if (!col_ptr) return pattern.nnz();
+        CSCData csc = pattern.to_csc();
+        for (int j = 0; j <= n; ++j) col_ptr[j] = csc.col_ptr[j];
+        for (int k = 0; k < pattern.nnz(); ++k) row_idx[k] = csc.row_idx[k];
+
+        ckt.integrator_ctx.options = &ckt.options;
+        ckt.integrator_ctx.mode = 0x10 | 0x200;  // MODEDCOP | MODEINITJCT
+        NumericMatrix mat(pattern);
+        std::vector<double> solution(n, 0.0), rhs(n, 0.0);
+        std::vector<double> ob_sol(n + 1, 0.0), ob_rhs(n + 1, 0.0);
+        OneBasedEvalArrays arrays{ob_sol.data(), ob_rhs.data(), n + 1};
+        tls_integrator_ctx = &ckt.integrator_ctx;
+        tls_one_based_eval_arrays = &arrays;
+        for (Device* dev : ckt.device_load_order()) dev->evaluate(solution, mat, rhs);
+        tls_one_based_eval_arrays = nullptr;
+        tls_integrator_ctx = nullptr;
+        for (int i = 0; i < n; ++i) rhs[i] += ob_rhs[i + 1];
+        const double pin = (ckt.options.gmin > 0.0) ? ckt.options.gmin : 1e-12;
+        for (int32_t idx : ckt.dead_node_indices()) mat.add(pattern.offset(idx, idx), pin);
+        for (int k = 0; k < pattern.nnz(); ++k) values[k] = mat.data()[k];
+        for (int i = 0; i < n; ++i) rhs_out[i] = rhs[i];
+        return pattern.nnz();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_mesh_initjct: %s\n", e.what());
         return -1;
     }
 }

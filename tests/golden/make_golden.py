@@ -1,12 +1,19 @@
 """Generate tests/golden/solver_cases.npz from the reference itself.
 
-Runs the reference's own NeoSolver (oracle/_ref/libnsref.so, built from the
-reference sources by oracle/Makefile) on seeded matrices and records, per
-case: the CSC pattern and values, the exported symbolic structure after
-NeoSolver::numeric (pivot permutations, LU pattern, slot map), the factored
-values, the values after NeoSolver::refactorize on perturbed values, and the
-solutions of solve and solve_transposed.  Run from the repository root:
-``python tests/golden/make_golden.py``.
+Runs the reference's own code (oracle/_ref/libnsref.so, built from the
+reference sources by oracle/Makefile).
+
+solver_cases.npz: on seeded matrices, per case the CSC pattern and values,
+the exported symbolic structure after NeoSolver::numeric (pivot permutations,
+LU pattern, slot map), the factored values, the values after
+NeoSolver::refactorize on perturbed values, and the solutions of solve and
+solve_transposed.
+
+mesh_dc.npz: seeded diode-clamped meshes (neospice_b200.workloads), per case
+the mesh, the reference's first-iteration matrix and rhs, and its DC
+operating point (solve_dc) with the Newton iteration count.
+
+Run from the repository root: ``python tests/golden/make_golden.py``.
 """
 from __future__ import annotations
 
@@ -66,5 +73,26 @@ def main():
     print(f"wrote {kept} cases to {path}")
 
 
+def mesh_main():
+    from neospice_b200 import workloads
+    rec = {}
+    sides = [4, 5, 7, 9, 12, 16, 16, 20]
+    for k, side in enumerate(sides):
+        m = workloads.diode_mesh(np.random.default_rng([77, k]), side=side)
+        cp, ri, vals, rhs = oracle.ref_mesh_initjct(m)
+        sol, iters, _ = oracle.ref_mesh_dc(m)
+        p = f"m{k:02d}_"
+        rec.update({p + "side": np.int32(side), p + "r_h": m.r_h, p + "r_v": m.r_v,
+                    p + "diode_nodes": m.diode_nodes, p + "isrc_nodes": m.isrc_nodes,
+                    p + "isrc_amps": m.isrc_amps, p + "col_ptr": cp, p + "row_idx": ri,
+                    p + "a0": vals, p + "rhs0": rhs, p + "solution": sol,
+                    p + "iterations": np.int32(iters)})
+    rec["count"] = np.int32(len(sides))
+    path = pathlib.Path(__file__).with_name("mesh_dc.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(sides)} meshes to {path}")
+
+
 if __name__ == "__main__":
     main()
+    mesh_main()

@@ -18,3 +18,19 @@ def load():
                                           d["elem_row"], d["elem_col"], d["slot_to_elem"])
         out.append(d)
     return out
+
+
+MESH_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "mesh_dc.npz"
+
+
+def load_meshes():
+    from neospice_b200.workloads import DiodeMesh
+    z = np.load(MESH_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"m{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        d["mesh"] = DiodeMesh(int(d["side"]), d["r_h"], d["r_v"], d["diode_nodes"],
+                              d["isrc_nodes"], d["isrc_amps"])
+        out.append(d)
+    return out

@@ -1,0 +1,100 @@
+"""Host circuit layer: pattern, first-iteration matrix and pivot order of
+the diode-mesh circuits must equal the reference's, bit for bit."""
+import numpy as np
+import pytest
+
+import golden_cases
+import oracle
+from neospice_b200 import _lib as L
+from neospice_b200 import workloads
+from neospice_b200.circuit import GND, Circuit
+from neospice_b200.solver import Topology
+
+MESHES = golden_cases.load_meshes()
+
+
+@pytest.mark.parametrize("k", range(len(MESHES)))
+def test_mesh_pattern_and_initial_matrix_match_golden(k):
+    g = MESHES[k]
+    c = g["mesh"].build()
+    cp, ri = c.pattern()
+    np.testing.assert_array_equal(cp, g["col_ptr"])
+    np.testing.assert_array_equal(ri, g["row_idx"])
+    a, r = c.initial_matrix()
+    np.testing.assert_array_equal(a, g["a0"])
+    np.testing.assert_array_equal(r, g["rhs0"])
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built here")
+def test_random_meshes_match_reference():
+    for k in range(6):
+        m = workloads.diode_mesh(np.random.default_rng([5, k]), side_range=(3, 24))
+        c = m.build()
+        cp, ri = c.pattern()
+        a, r = c.initial_matrix()
+        rcp, rri, rv, rr = oracle.ref_mesh_initjct(m)
+        np.testing.assert_array_equal(cp, rcp)
+        np.testing.assert_array_equal(ri, rri)
+        np.testing.assert_array_equal(a, rv)
+        np.testing.assert_array_equal(r, rr)
+        rs = oracle.RefSolver(len(rcp) - 1, rcp, rri)
+        assert rs.numeric(rv) == 0
+        st, _ = rs.export()
+        t = Topology.order(len(cp) - 1, cp, ri, a)
+        assert st.same_as(oracle.Structure(st.n, *t.export()))
+
+
+def test_pivot_order_depends_only_on_pattern_for_meshes():
+    """Same-side meshes with different values and diode/source placements
+    get the same pivot sequence: the basis of per-pattern symbolic sharing."""
+    for side in (6, 11):
+        exports = []
+        for k in range(4):
+            m = workloads.diode_mesh(np.random.default_rng([side, k]), side=side)
+            c = m.build()
+            cp, ri = c.pattern()
+            a, _ = c.initial_matrix()
+            exports.append(Topology.order(len(cp) - 1, cp, ri, a).export())
+        for e in exports[1:]:
+            assert all(np.array_equal(x, y) for x, y in zip(e, exports[0]))
+
+
+def test_load_order_and_branch_numbering():
+    # two sources: the newest is loaded first and gets the first branch index
+    c = Circuit(2)
+    c.R(0, 1, 1e3)
+    c.V(0, GND, 1.0)
+    c.V(1, GND, 2.0)
+    c.finalize()
+    assert c.info()["num_vars"] == 4
+    cp, ri = c.pattern()
+    # branch 2 belongs to the second source (node 1), branch 3 to the first
+    col2 = set(ri[cp[2]:cp[3]])
+    col3 = set(ri[cp[3]:cp[4]])
+    assert col2 == {1} and col3 == {0}
+
+
+def test_dead_node_gets_pinned_diagonal():
+    c = Circuit(3)
+    c.R(0, GND, 1e3)
+    c.V(0, GND, 1.0)
+    c.I(GND, 1, 0.0)  # node 1: only a current source -> dead
+    c.R(2, GND, 10.0)
+    c.finalize()
+    cp, ri = c.pattern()
+    assert 1 in ri[cp[1]:cp[2]]
+    a, _ = c.initial_matrix(gmin=1e-12)
+    assert a[cp[1]] == 1e-12
+
+
+def test_circuit_misuse_raises():
+    c = Circuit(2)
+    with pytest.raises(L.NsgError):
+        c.R(0, 5, 1.0)  # node out of range
+    with pytest.raises(L.NsgError):
+        c.D(0, GND, IS=-1.0)
+    c.R(0, 1, 1.0)
+    c.R(1, GND, 1.0)
+    c.finalize()
+    with pytest.raises(L.NsgError):
+        c.R(0, 1, 1.0)  # after finalize

@@ -26,8 +26,9 @@ def _unpack(arr, offsets, sizes):
     return [arr[offsets[i]:offsets[i] + s] for i, s in enumerate(sizes)]
 
 
-def _run(topos, vals, bs, gmin=0.0, check=False):
+def _run(topos, vals, bs, gmin=0.0, check=False, schedule=0):
     batch = Batch(topos)
+    batch.set_schedule(schedule)
     d_a = _pack(batch, vals, batch.value_offsets)
     st, fs = batch.refactor(d_a, gmin, check_pivots=check)
     lu = batch.lu_values()
@@ -46,13 +47,14 @@ def _run(topos, vals, bs, gmin=0.0, check=False):
     return out
 
 
-def test_refactor_and_solves_match_golden_bitwise():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_refactor_and_solves_match_golden_bitwise(schedule):
     topos = [Topology.order(int(c["n"]), c["col_ptr"], c["row_idx"], c["vals"]) for c in CASES]
-    first = _run(topos, [c["vals"] for c in CASES], None)
+    first = _run(topos, [c["vals"] for c in CASES], None, schedule=schedule)
     for c, lu, s in zip(CASES, first["lu"], first["status"]):
         assert s == 0
         np.testing.assert_array_equal(lu, c["lu_numeric"])
-    res = _run(topos, [c["vals2"] for c in CASES], [c["b"] for c in CASES])
+    res = _run(topos, [c["vals2"] for c in CASES], [c["b"] for c in CASES], schedule=schedule)
     for k, c in enumerate(CASES):
         rc = int(c["refactor_rc"])
         assert (res["status"][k] != 0) == (rc != 0)
@@ -73,7 +75,8 @@ def test_imported_structure_matches():
     np.testing.assert_array_equal(res["x"][0], c["x"])
 
 
-def test_mixed_batch_against_port():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_mixed_batch_against_port(schedule):
     rng = np.random.default_rng(11)
     mats = [mna_mesh(rng, s, 1 + s % 3) for s in (4, 9, 17, 30, 45)]
     mats += [banded(1000, 7, seed=2)]
@@ -85,7 +88,7 @@ def test_mixed_batch_against_port():
         bs.append(rng.standard_normal(n))
     # repeat instances so several CTAs share one plan
     topos, vals, bs = topos * 3, vals * 3, bs * 3
-    res = _run(topos, vals, bs, gmin=1e-12)
+    res = _run(topos, vals, bs, gmin=1e-12, schedule=schedule)
     for k, t in enumerate(topos):
         st = oracle.Structure(t.info()["n"], *t.export())
         rc, lu, _ = oracle.port_refactor(st, vals[k], gmin=1e-12)
@@ -109,7 +112,8 @@ def test_zero_pivot_flagged_singular():
     assert res["step"][1] == step == 0
 
 
-def test_pivot_revalidation_flags_match_port():
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_pivot_revalidation_flags_match_port(schedule):
     rng = np.random.default_rng(8)
     topos, vals, expect = [], [], []
     for _ in range(40):
@@ -124,7 +128,7 @@ def test_pivot_revalidation_flags_match_port():
         topos.append(t)
         vals.append(v2)
         expect.append((rc, step))
-    res = _run(topos, vals, None, check=True)
+    res = _run(topos, vals, None, check=True, schedule=schedule)
     flagged = 0
     for k, (rc, step) in enumerate(expect):
         assert res["status"][k] == rc
