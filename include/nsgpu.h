@@ -186,6 +186,10 @@ int nsg_dc_batch_layout(const nsg_dc_batch* b, long long* param_offsets,
  * updates; number of distinct symbolic results. */
 int nsg_dc_batch_stats(const nsg_dc_batch* b, long long* n, long long* nnz, long long* nnz_lu,
                        long long* updates, int* distinct_topologies);
+/* Per-instance sizes (arrays of count): unknowns, matrix slots, LU entries,
+ * refactor multiply-subtract updates. */
+int nsg_dc_batch_instance_stats(const nsg_dc_batch* b, long long* n, long long* nnz,
+                                long long* nnz_lu, long long* updates);
 /* SimOptions reltol, vntol, abstol, gmin and itl1 (defaults 1e-3, 1e-6,
  * 1e-12, 1e-12, 100; src/core/types.hpp:24-66). */
 int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, double abstol,

@@ -69,6 +69,7 @@ SIGNATURES = {
     "nsg_dc_batch_free": (None, [c_void_p]),
     "nsg_dc_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll)]),
     "nsg_dc_batch_stats": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll), P(c_ll), P(c_int)]),
+    "nsg_dc_batch_instance_stats": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll), P(c_ll)]),
     "nsg_dc_batch_set_options": (c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int]),
     "nsg_dc_batch_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
 }

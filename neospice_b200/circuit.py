@@ -128,6 +128,13 @@ class DcBatch:
         return dict(n=n.value, nnz=nnz.value, nnz_lu=nlu.value, updates=upd.value,
                     topologies=topo.value)
 
+    def instance_stats(self) -> dict:
+        arrs = {k: np.zeros(self.count, np.int64) for k in ("n", "nnz", "nnz_lu", "updates")}
+        L.check(L.lib().nsg_dc_batch_instance_stats(self._h, L.llptr(arrs["n"]),
+                                                    L.llptr(arrs["nnz"]), L.llptr(arrs["nnz_lu"]),
+                                                    L.llptr(arrs["updates"])))
+        return arrs
+
     def set_options(self, reltol=1e-3, vntol=1e-6, abstol=1e-12, gmin=1e-12, max_iter=100):
         L.check(L.lib().nsg_dc_batch_set_options(self._h, reltol, vntol, abstol, gmin,
                                                  int(max_iter)))

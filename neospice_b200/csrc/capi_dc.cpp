@@ -30,6 +30,7 @@ struct nsg_dc_batch {
     int count = 0;
     std::vector<std::unique_ptr<nsg_topology>> topos;  // distinct symbolic results
     std::vector<long long> param_off, sol_off;
+    std::vector<long long> inst_n, inst_nnz, inst_nnz_lu, inst_updates;
     std::vector<double> host_params;
     long long updates = 0, nnz_lu = 0, nnz = 0, n = 0;
     int max_col = 0, max_n = 0;
@@ -317,6 +318,10 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             d.tv_off = work; work = align4(work + c.n_terms());
             d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
             d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
+            b->inst_n.push_back(p.n);
+            b->inst_nnz.push_back(p.nnz_a);
+            b->inst_nnz_lu.push_back(p.nnz_lu);
+            b->inst_updates.push_back(p.updates);
             b->updates += p.updates;
             b->nnz_lu += p.nnz_lu;
             b->nnz += p.nnz_a;
@@ -360,6 +365,17 @@ int nsg_dc_batch_stats(const nsg_dc_batch* b, long long* n, long long* nnz, long
     if (nnz_lu) *nnz_lu = b->nnz_lu;
     if (updates) *updates = b->updates;
     if (distinct_topologies) *distinct_topologies = static_cast<int>(b->topos.size());
+    return NSG_OK;
+}
+
+int nsg_dc_batch_instance_stats(const nsg_dc_batch* b, long long* n, long long* nnz,
+                                long long* nnz_lu, long long* updates) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_instance_stats: null batch");
+    const size_t bytes = sizeof(long long) * b->count;
+    if (n) std::memcpy(n, b->inst_n.data(), bytes);
+    if (nnz) std::memcpy(nnz, b->inst_nnz.data(), bytes);
+    if (nnz_lu) std::memcpy(nnz_lu, b->inst_nnz_lu.data(), bytes);
+    if (updates) std::memcpy(updates, b->inst_updates.data(), bytes);
     return NSG_OK;
 }
 
