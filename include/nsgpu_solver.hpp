@@ -1,0 +1,177 @@
+// nsgpu::GpuSolver -- a header-only C++ class with the method set and error
+// conventions of the reference's ISolver (src/core/solver_iface.hpp:16-41) and
+// NeoSolver (src/core/neo_solver.cpp:184-297), on top of the C ABI in
+// nsgpu.h.  One instance per object: this is the plain, one-instance-per-launch
+// GPU path; batches of instances use nsg_batch_* / nsg_dc_batch_* directly.
+//
+//   symbolic(n, col_ptr, row_idx)   NeoSolver::symbolic (pattern in CSC)
+//   numeric(values, diag_gmin)      NeoSolver::numeric: first call orders on the
+//                                   host (Sparse-1.3 Markowitz, bit-identical
+//                                   pivots); later calls re-validate the pivots
+//                                   on the GPU and re-order on the host only if
+//                                   one fails.  Returns true when singular.
+//   refactorize(values, diag_gmin)  NeoSolver::refactorize (spFactor) on the GPU.
+//                                   Returns true when singular.
+//   solve(rhs)                      NeoSolver::solve (spSolve), in place.
+//   solve_transposed(rhs)           spSolveTransposed, in place.
+//
+// Misuse throws std::logic_error, a size mismatch std::invalid_argument, a
+// CUDA or allocation failure std::runtime_error -- as NeoSolver does.
+#pragma once
+#include "nsgpu.h"
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace nsgpu {
+
+class GpuSolver {
+public:
+    GpuSolver() = default;
+    GpuSolver(const GpuSolver&) = delete;
+    GpuSolver& operator=(const GpuSolver&) = delete;
+    ~GpuSolver() { release(); }
+
+    const char* name() const { return "gpu-markowitz"; }
+
+    void symbolic(int n, const std::vector<int>& col_ptr, const std::vector<int>& row_idx) {
+        if (n <= 0 || static_cast<int>(col_ptr.size()) != n + 1 ||
+            col_ptr.back() != static_cast<int>(row_idx.size()))
+            throw std::invalid_argument("GpuSolver::symbolic: malformed pattern");
+        release();
+        n_ = n;
+        col_ptr_ = col_ptr;
+        row_idx_ = row_idx;
+        symbolized_ = true;
+        numeric_called_ = false;
+        factored_ = false;
+    }
+
+    bool numeric(const std::vector<double>& values, double diag_gmin = 0.0) {
+        require_symbolic("numeric");
+        check_values(values);
+        numeric_called_ = true;
+        if (!topo_) {
+            nsg_topology* t = nullptr;
+            const int rc = nsg_topology_order(n_, nnz(), col_ptr_.data(), row_idx_.data(),
+                                              values.data(), diag_gmin, &t);
+            if (rc == NSG_SINGULAR) return true;
+            check(rc, "numeric");
+            topo_ = t;
+            rebuild_batch();
+            upload(values);
+            factored_ = (gpu_refactor(diag_gmin, 0) == NSG_OK);
+            return !factored_;
+        }
+        upload(values);
+        int st = gpu_refactor(diag_gmin, 1);
+        if (st == NSG_REORDER) {
+            int step = 0;
+            const int rc = nsg_topology_numeric(topo_, values.data(), diag_gmin, &step);
+            if (rc == NSG_SINGULAR) return true;
+            check(rc, "numeric");
+            rebuild_batch();
+            st = gpu_refactor(diag_gmin, 0);
+        }
+        factored_ = (st == NSG_OK);
+        return !factored_;
+    }
+
+    bool refactorize(const std::vector<double>& values, double diag_gmin = 0.0) {
+        require_symbolic("refactorize");
+        if (!numeric_called_)
+            throw std::logic_error("GpuSolver::refactorize: numeric() not called");
+        if (!topo_) return true;  // the first numeric() found the matrix singular
+        check_values(values);
+        upload(values);
+        const int st = gpu_refactor(diag_gmin, 0);
+        factored_ = (st == NSG_OK);
+        return !factored_;
+    }
+
+    void solve(std::vector<double>& rhs) { sweep(rhs, false); }
+    void solve_transposed(std::vector<double>& rhs) { sweep(rhs, true); }
+
+private:
+    int n_ = 0;
+    bool symbolized_ = false;
+    bool numeric_called_ = false;  // NeoSolver's factored_ flag
+    bool factored_ = false;        // the last factorization succeeded
+    std::vector<int> col_ptr_, row_idx_;
+    nsg_topology* topo_ = nullptr;
+    nsg_batch* batch_ = nullptr;
+    double* d_values_ = nullptr;
+    double* d_x_ = nullptr;
+    int* d_status_ = nullptr;
+
+    int nnz() const { return static_cast<int>(row_idx_.size()); }
+
+    static void check(int rc, const char* what) {
+        if (rc != NSG_OK)
+            throw std::runtime_error(std::string("GpuSolver::") + what + ": " + nsg_last_error());
+    }
+    static void cuda(cudaError_t e, const char* what) {
+        if (e != cudaSuccess)
+            throw std::runtime_error(std::string("GpuSolver::") + what + ": " +
+                                     cudaGetErrorString(e));
+    }
+    void require_symbolic(const char* what) const {
+        if (!symbolized_)
+            throw std::logic_error(std::string("GpuSolver::") + what + ": symbolic() not called");
+    }
+    void check_values(const std::vector<double>& v) const {
+        if (static_cast<int>(v.size()) != nnz())
+            throw std::invalid_argument("GpuSolver: values size mismatch");
+    }
+    void rebuild_batch() {
+        if (batch_) nsg_batch_free(batch_);
+        batch_ = nullptr;
+        check(nsg_batch_create(1, &topo_, &batch_), "batch");
+        if (!d_values_) {
+            cuda(cudaMalloc(reinterpret_cast<void**>(&d_values_), sizeof(double) * nnz()), "alloc");
+            cuda(cudaMalloc(reinterpret_cast<void**>(&d_x_), sizeof(double) * n_), "alloc");
+            cuda(cudaMalloc(reinterpret_cast<void**>(&d_status_), sizeof(int)), "alloc");
+        }
+    }
+    void upload(const std::vector<double>& values) {
+        cuda(cudaMemcpy(d_values_, values.data(), sizeof(double) * nnz(), cudaMemcpyHostToDevice),
+             "upload");
+    }
+    int gpu_refactor(double diag_gmin, int check_pivots) {
+        check(nsg_batch_refactor(batch_, d_values_, diag_gmin, check_pivots, d_status_, nullptr,
+                                 nullptr), "refactor");
+        int st = 0;
+        cuda(cudaMemcpy(&st, d_status_, sizeof(int), cudaMemcpyDeviceToHost), "status");
+        if (st == 104) throw std::runtime_error("GpuSolver: refactor wait timed out");
+        return st;
+    }
+    void sweep(std::vector<double>& rhs, bool transposed) {
+        require_symbolic(transposed ? "solve_transposed" : "solve");
+        if (!numeric_called_)
+            throw std::logic_error("GpuSolver::solve: numeric() not called");
+        if (!factored_)
+            throw std::runtime_error("GpuSolver::solve: no valid factorization (singular)");
+        if (static_cast<int>(rhs.size()) != n_)
+            throw std::invalid_argument("GpuSolver::solve: rhs size mismatch");
+        cuda(cudaMemcpy(d_x_, rhs.data(), sizeof(double) * n_, cudaMemcpyHostToDevice), "rhs");
+        check(transposed ? nsg_batch_solve_transposed(batch_, d_x_, nullptr)
+                         : nsg_batch_solve(batch_, d_x_, nullptr), "solve");
+        cuda(cudaMemcpy(rhs.data(), d_x_, sizeof(double) * n_, cudaMemcpyDeviceToHost), "result");
+    }
+    void release() {
+        if (batch_) nsg_batch_free(batch_);
+        if (topo_) nsg_topology_free(topo_);
+        if (d_values_) cudaFree(d_values_);
+        if (d_x_) cudaFree(d_x_);
+        if (d_status_) cudaFree(d_status_);
+        batch_ = nullptr;
+        topo_ = nullptr;
+        d_values_ = d_x_ = nullptr;
+        d_status_ = nullptr;
+    }
+};
+
+}  // namespace nsgpu
