@@ -113,6 +113,26 @@ int nsg_batch_solve(nsg_batch* batch, double* d_x, void* stream);
  * (SparseMatrix::solve_transposed, src/solver/solve.cpp:102-141). */
 int nsg_batch_solve_transposed(nsg_batch* batch, double* d_x, void* stream);
 
+/* Allocation-free solve.  No counterpart in the reference: it exists for
+ * callers that must not allocate device memory when they solve -- a simulator
+ * held to a fixed memory budget, code running inside another framework's
+ * memory pool, or a latency-critical loop that cannot afford the implicit
+ * synchronisation of cudaMalloc/cudaFree.  Same result as nsg_batch_solve
+ * (bit for bit), but the per-instance sweep workspace comes from a fixed
+ * array of NSG_STATIC_SCRATCH_DOUBLES doubles (8 MiB) compiled into the
+ * library, which every GPU that loads the library keeps until the process
+ * exits; the call itself allocates nothing.
+ *   - Batches whose unknowns total more than NSG_STATIC_SCRATCH_DOUBLES are
+ *     rejected with NSG_ERR_INVALID (see nsg_last_error).
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (different
+ *     streams, or different batches at once) race.  The array keeps the last
+ *     call's contents; nothing in it has to start at zero. */
+#define NSG_STATIC_SCRATCH_DOUBLES (1LL << 20)
+int nsg_batch_solve_static_scratch(nsg_batch* batch, double* d_x, void* stream);
+
 /* Device pointer to the factored LU values (layout per nsg_batch_layout and
  * the topology export: L unscaled, U scaled by the reciprocal pivot, pivots
  * stored as reciprocals — the reference's in-place element values). */

@@ -27,6 +27,7 @@ NSG_REORDER = 103
 NSG_TIMEOUT = 104
 NSG_SYMBOLIC_PER_INSTANCE = 0
 NSG_SYMBOLIC_PER_PATTERN = 1
+NSG_STATIC_SCRATCH_DOUBLES = 1 << 20
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -48,6 +49,7 @@ SIGNATURES = {
     "nsg_batch_set_schedule": (c_int, [c_void_p, c_int]),
     "nsg_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
     "nsg_batch_solve_transposed": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "nsg_batch_solve_static_scratch": (c_int, [c_void_p, c_void_p, c_void_p]),
     "nsg_batch_lu": (c_void_p, [c_void_p]),
     "nsg_batch_lu_to_host": (c_int, [c_void_p, P(c_double)]),
     "nsg_circuit_create": (c_int, [c_int, P(c_void_p)]),
