@@ -206,6 +206,7 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             b->max_col = std::max(b->max_col, p.max_col);
             b->max_n = std::max(b->max_n, p.n);
             insts[i].plan = it->second;
+            insts[i].index = i;
             insts[i].a_off = b->a_off[i];
             insts[i].lu_off = b->lu_off[i];
             insts[i].x_off = b->x_off[i];
@@ -215,6 +216,10 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             // keep each instance's LU 32-byte aligned
             b->lu_off[i + 1] = b->lu_off[i] + ((p.nnz_lu + 3) & ~3);
         }
+        // Largest instances first: the grid's tail is made of small ones.
+        std::stable_sort(insts.begin(), insts.end(), [&](const nsg::InstDesc& x, const nsg::InstDesc& y) {
+            return topos[x.index]->plan.updates > topos[y.index]->plan.updates;
+        });
         cudaError_t e;
         if ((e = upload(&b->d_pool, pool.data(), pool.size())) != cudaSuccess ||
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||

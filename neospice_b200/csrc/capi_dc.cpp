@@ -17,6 +17,7 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              double* solutions, int32_t* status, int32_t* iterations,
                              const NewtonOptions& opt, int max_col, int max_n,
                              cudaStream_t stream);
+size_t dc_smem_bytes(int max_col, int max_n);
 }  // namespace nsg
 
 using namespace nsg_internal;
@@ -284,6 +285,7 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             const auto& c = circuits[i]->c;
             const auto& p = b->topos[topo_of[i]]->plan;
             nsg::DcDesc& d = descs[i];
+            d.index = i;
             d.plan = topo_of[i];
             d.n = c.num_vars();
             d.num_nodes = c.num_nodes();
@@ -327,8 +329,12 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             b->nnz += p.nnz_a;
             b->n += p.n;
         }
-        const size_t smem = (sizeof(double) * 16 * ((b->max_col + 31) & ~31)) +
-                            sizeof(int32_t) * b->max_n;
+        // Launch the most expensive instances first so the grid's tail is
+        // made of small ones.
+        std::stable_sort(descs.begin(), descs.end(), [&](const nsg::DcDesc& x, const nsg::DcDesc& y) {
+            return b->inst_updates[x.index] > b->inst_updates[y.index];
+        });
+        const size_t smem = nsg::dc_smem_bytes(b->max_col, b->max_n);
         if (smem > 200 * 1024)
             return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: instance too large for the "
                                          "shared-memory refactor (longest LU column " +

@@ -13,6 +13,7 @@ enum DcProgArray : int {
 };
 
 struct DcDesc {
+    int32_t index;       // the instance's position in the caller's arrays
     int32_t plan;        // PlanDesc index (LU structure)
     int32_t n;           // unknowns
     int32_t num_nodes;   // node unknowns come first, branch currents after

@@ -93,12 +93,20 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
             buf[t] = v;
         }
         __syncwarp();
+        // One-step lookahead: while the update of U entry q runs, the pivot
+        // reciprocal, the first 32 entries of L(:, r) and their destinations
+        // for entry q+1 are already in registers (when column r is done).
         bool timed_out = false;
-        for (int32_t q = 0; q < dj; ++q) {
+        double rd_c = 0.0, lv_c = 0.0;
+        int32_t l0_c = 0, cnt_c = 0, us_c = 0, ld_c = 0;
+        bool have_c = false;
+        auto fetch = [&](int32_t q, bool wait, double& rd, double& lv, int32_t& l0, int32_t& cnt,
+                         int32_t& us, int32_t& ld) -> bool {
             const int32_t r = row_idx[c0 + q];
+            int ready = 0;
             if (lane == 0) {
                 int spins = 0;
-                while (done[r] == 0) {
+                while ((ready = done[r]) == 0 && wait) {
                     if (++spins > kSpinLimit) {
                         timed_out = true;
                         break;
@@ -107,21 +115,45 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
                 }
                 __threadfence_block();
             }
+            ready = __shfl_sync(0xffffffffu, ready, 0);
             timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
             __syncwarp();
-            if (timed_out) break;
+            if (!ready) return false;
             const int32_t dr = diag_pos[r];
-            const double u = lu_mul(buf[q], lu[dr]);
+            rd = lu[dr];
+            l0 = dr + 1;
+            cnt = col_ptr[r + 1] - l0;
+            us = upd_start[c0 + q];
+            lv = (lane < cnt) ? lu[l0 + lane] : 0.0;
+            ld = (lane < cnt) ? upd_dst[us + lane] : 0;
+            return true;
+        }
+        ;
+        for (int32_t q = 0; q < dj; ++q) {
+            if (!have_c) {
+                fetch(q, true, rd_c, lv_c, l0_c, cnt_c, us_c, ld_c);
+                if (timed_out) break;
+            }
+            double rd_n = 0.0, lv_n = 0.0;
+            int32_t l0_n = 0, cnt_n = 0, us_n = 0, ld_n = 0;
+            const bool have_n =
+                (q + 1 < dj) && fetch(q + 1, false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
+            const double u = lu_mul(buf[q], rd_c);
             __syncwarp();
             if (lane == 0) buf[q] = u;
-            const int32_t l0 = dr + 1;
-            const int32_t cnt = col_ptr[r + 1] - l0;
-            const int32_t* dst = upd_dst + upd_start[c0 + q];
-            for (int32_t t = lane; t < cnt; t += 32) {
-                const int32_t d = dst[t];
-                buf[d] = lu_sub(buf[d], lu_mul(u, lu[l0 + t]));
+            if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
+            for (int32_t t = lane + 32; t < cnt_c; t += 32) {
+                const int32_t d = upd_dst[us_c + t];
+                buf[d] = lu_sub(buf[d], lu_mul(u, lu[l0_c + t]));
             }
             __syncwarp();
+            have_c = have_n;
+            rd_c = rd_n;
+            lv_c = lv_n;
+            l0_c = l0_n;
+            cnt_c = cnt_n;
+            us_c = us_n;
+            ld_c = ld_n;
         }
         const double piv = buf[dj];
         bool fail;
@@ -208,6 +240,95 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
     }
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_col[i]] = w[i];
     __syncthreads();
+}
+
+// Shared memory of the dataflow solve: the n-vector and n completion flags.
+__host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
+    return (sizeof(double) + sizeof(int32_t)) * static_cast<size_t>(n);
+}
+
+// Wait (bounded) until flag[i] is set; returns false on timeout.
+__device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
+    if (flag[i] == 0) {
+        int spins = 0;
+        while (flag[i] == 0) {
+            if (++spins > kSpinLimit) return false;
+            __nanosleep(32);
+        }
+    }
+    __threadfence_block();
+    return true;
+}
+
+// x <- A^{-1} x (SparseMatrix::solve) by the whole CTA, dataflow schedule:
+// thread t takes rows t, t + blockDim, ... of the level-sorted order and
+// waits, entry by entry, for the rows it reads.  The vector and the flags live
+// in shared memory (flow_solve_smem_bytes).  Same arithmetic, in the same
+// order per row, as cta_solve.  Returns false if a bounded wait gave up.
+__device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
+                                      const double* __restrict__ lu, double* __restrict__ x,
+                                      double* smem) {
+    const int32_t n = pd.n;
+    const int32_t* perm_row = pool + pd.off[PA_perm_row];
+    const int32_t* perm_col = pool + pd.off[PA_perm_col];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    double* w = smem;
+    volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + n);
+    __shared__ int32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) s_ok = 1;
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        w[i] = x[perm_row[i]];
+        done[i] = 0;
+    }
+    __syncthreads();
+    bool ok = true;
+    {   // forward: L with the reciprocal pivot
+        const int32_t* lp = pool + pd.off[PA_lrow_ptr];
+        const int32_t* lpos = pool + pd.off[PA_lrow_pos];
+        const int32_t* lcol = pool + pd.off[PA_lrow_col];
+        const int32_t* order = pool + pd.off[PA_fwd_lev];
+        for (int32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            const int32_t i = order[k];
+            double t = w[i];
+            for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
+                const int32_t c = lcol[e];
+                if (ok && !wait_flag(done, c)) ok = false;
+                const double xc = w[c];
+                if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu[lpos[e]]));
+            }
+            w[i] = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
+            __threadfence_block();
+            done[i] = 1;
+        }
+    }
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) done[i] = 0;
+    __syncthreads();
+    {   // backward: unit-diagonal U
+        const int32_t* up = pool + pd.off[PA_urow_ptr];
+        const int32_t* upos = pool + pd.off[PA_urow_pos];
+        const int32_t* ucol = pool + pd.off[PA_urow_col];
+        const int32_t* order = pool + pd.off[PA_bwd_lev];
+        for (int32_t k = threadIdx.x; k < n; k += blockDim.x) {
+            const int32_t i = order[k];
+            double t = w[i];
+            for (int32_t e = up[i]; e < up[i + 1]; ++e) {
+                const int32_t c = ucol[e];
+                if (ok && !wait_flag(done, c)) ok = false;
+                t = lu_sub(t, lu_mul(lu[upos[e]], w[c]));
+            }
+            w[i] = t;
+            __threadfence_block();
+            done[i] = 1;
+        }
+    }
+    if (!ok) s_ok = 0;
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_col[i]] = w[i];
+    const bool all_ok = (s_ok != 0);
+    __syncthreads();
+    return all_ok;
 }
 
 // x <- A^{-T} x (SparseMatrix::solve_transposed) by the whole CTA.

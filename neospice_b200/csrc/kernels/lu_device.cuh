@@ -22,7 +22,7 @@ struct PlanDesc {
 
 struct InstDesc {
     int32_t plan;   // index into the PlanDesc array
-    int32_t pad;
+    int32_t index;  // the instance's position in the caller's arrays
     int64_t a_off;   // into the caller's A values (doubles)
     int64_t lu_off;  // into the batch's LU values
     int64_t x_off;   // into the caller's rhs / solution vectors

@@ -121,8 +121,8 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        status[blockIdx.x] = s_fail_code;
-        if (fail_step) fail_step[blockIdx.x] = (s_fail_code == kStatusOk) ? -1 : s_fail_step;
+        status[inst.index] = s_fail_code;
+        if (fail_step) fail_step[inst.index] = (s_fail_code == kStatusOk) ? -1 : s_fail_step;
     }
 }
 
@@ -139,8 +139,8 @@ refactor_flow_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
         cta_refactor_flow(plans[inst.plan], pool, A + inst.a_off, LU + inst.lu_off, diag_gmin,
                           check_pivots, rel_threshold, smem, colbuf);
     if (threadIdx.x == 0) {
-        status[blockIdx.x] = r.code;
-        if (fail_step) fail_step[blockIdx.x] = r.step;
+        status[inst.index] = r.code;
+        if (fail_step) fail_step[inst.index] = r.step;
     }
 }
 

@@ -57,7 +57,6 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     const double* par = params + d.param_off;
     double* x = work + d.x_off;
     double* xold = work + d.xold_off;
-    double* w = work + d.w_off;
     double* a = work + d.a_off;
     double* lu = work + d.lu_off;
     double* tv = work + d.tv_off;
@@ -162,7 +161,11 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
             continue;
         }
 
-        cta_solve(pd, lu_pool, lu, x, w);
+        if (!cta_solve_flow(pd, lu_pool, lu, x, smem)) {
+            result = kStatusTimeout;
+            iters = iter + 1;
+            break;
+        }
 
         // Convergence test (newton.cpp:267-292).
         if (threadIdx.x == 0) s_conv = 1;
@@ -198,9 +201,16 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     double* out = solutions + d.sol_off;
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = xold[i];
     if (threadIdx.x == 0) {
-        status[blockIdx.x] = result;
-        iterations[blockIdx.x] = iters;
+        status[d.index] = result;
+        iterations[d.index] = iters;
     }
+}
+
+size_t dc_smem_bytes(int max_col, int max_n) {
+    const int colbuf = (max_col + 31) & ~31;
+    const size_t a = flow_smem_bytes(colbuf, max_n);
+    const size_t b = flow_solve_smem_bytes(max_n);
+    return a > b ? a : b;
 }
 
 cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
@@ -210,7 +220,7 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
-    const size_t smem = flow_smem_bytes(colbuf, max_n);
+    const size_t smem = dc_smem_bytes(max_col, max_n);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
