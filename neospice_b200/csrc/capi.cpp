@@ -17,9 +17,10 @@ cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const In
                             int count, const double* A, double* LU, double diag_gmin,
                             int check_pivots, double rel_threshold, int32_t* status,
                             int32_t* fail_step, int max_col, int max_n, bool allow_flow,
-                            cudaStream_t stream);
+                            double* lrows, double* urows, cudaStream_t stream);
 cudaError_t launch_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                          int count, const double* LU, double* X, double* W, bool transposed,
+                         const double* lrows, const double* urows, int max_n,
                          cudaStream_t stream);
 }  // namespace nsg
 
@@ -90,6 +91,8 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.n_bwd_lev = static_cast<int32_t>(p.bwd_lev_ptr.size()) - 1;
     d.n_tbw_lev = static_cast<int32_t>(p.tbw_lev_ptr.size()) - 1;
     d.max_col = p.max_col;
+    d.nnz_l = p.lrow_ptr[p.n];
+    d.nnz_u = p.urow_ptr[p.n];
     p.append_to(pool, d.off);
     return d;
 }
@@ -194,6 +197,7 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
         b->a_off.assign(count + 1, 0);
         b->x_off.assign(count + 1, 0);
         b->lu_off.assign(count + 1, 0);
+        int64_t lrows = 0, urows = 0;
         for (int i = 0; i < count; ++i) {
             const nsg_topology* t = topos[i];
             if (!t) return fail(NSG_ERR_INVALID, "nsg_batch_create: null topology");
@@ -211,6 +215,10 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             insts[i].lu_off = b->lu_off[i];
             insts[i].x_off = b->x_off[i];
             insts[i].w_off = b->x_off[i];
+            insts[i].lrows_off = lrows;
+            insts[i].urows_off = urows;
+            lrows += (p.lrow_ptr[p.n] + 3) & ~3;
+            urows += (p.urow_ptr[p.n] + 3) & ~3;
             b->a_off[i + 1] = b->a_off[i] + p.nnz_a;
             b->x_off[i + 1] = b->x_off[i] + p.n;
             // keep each instance's LU 32-byte aligned
@@ -225,7 +233,9 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
             (e = upload(&b->d_insts, insts.data(), insts.size())) != cudaSuccess ||
             (e = upload<double>(&b->d_lu, nullptr, b->lu_off[count])) != cudaSuccess ||
-            (e = upload<double>(&b->d_work, nullptr, b->x_off[count])) != cudaSuccess)
+            (e = upload<double>(&b->d_work, nullptr, b->x_off[count])) != cudaSuccess ||
+            (e = upload<double>(&b->d_lrows, nullptr, lrows)) != cudaSuccess ||
+            (e = upload<double>(&b->d_urows, nullptr, urows)) != cudaSuccess)
             return cuda_fail("nsg_batch_create", e);
         *out = b.release();
         return NSG_OK;
@@ -251,21 +261,24 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
     cudaError_t e = nsg::launch_refactor(b->d_plans, b->d_pool, b->d_insts, b->count, d_values,
                                          b->d_lu, diag_gmin, check_pivots, 1e-3, d_status,
                                          d_fail_step, b->max_col, b->max_n, b->allow_flow,
-                                         static_cast<cudaStream_t>(stream));
+                                         b->d_lrows, b->d_urows, static_cast<cudaStream_t>(stream));
+    if (e == cudaSuccess) b->rows_valid = b->allow_flow;
     return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
 }
 
 int nsg_batch_solve(nsg_batch* b, double* d_x, void* stream) {
     if (!b || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve: null argument");
     cudaError_t e = nsg::launch_solve(b->d_plans, b->d_pool, b->d_insts, b->count, b->d_lu, d_x,
-                                      b->d_work, false, static_cast<cudaStream_t>(stream));
+                                      b->d_work, false, b->rows_valid ? b->d_lrows : nullptr,
+                                      b->d_urows, b->max_n, static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve", e);
 }
 
 int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
     if (!b || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve_transposed: null argument");
     cudaError_t e = nsg::launch_solve(b->d_plans, b->d_pool, b->d_insts, b->count, b->d_lu, d_x,
-                                      b->d_work, true, static_cast<cudaStream_t>(stream));
+                                      b->d_work, true, nullptr, nullptr, b->max_n,
+                                      static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve_transposed", e);
 }
 

@@ -317,6 +317,8 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             d.w_off = work; work = align4(work + d.n);
             d.a_off = work; work = align4(work + d.nnz);
             d.lu_off = work; work = align4(work + p.nnz_lu);
+            d.lrows_off = work; work = align4(work + p.lrow_ptr[p.n]);
+            d.urows_off = work; work = align4(work + p.urow_ptr[p.n]);
             d.tv_off = work; work = align4(work + c.n_terms());
             d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
             d.dconst_off = work; work = align4(work + 3 * d.n_diodes);

@@ -29,6 +29,9 @@ struct nsg_batch {
     nsg::InstDesc* d_insts = nullptr;
     double* d_lu = nullptr;
     double* d_work = nullptr;
+    double* d_lrows = nullptr;  // row-major L copy written by the dataflow refactor
+    double* d_urows = nullptr;  // row-major U copy
+    bool rows_valid = false;    // the copies match d_lu (last refactor was dataflow)
     int max_col = 0;
     int max_n = 0;
     bool allow_flow = true;
@@ -38,6 +41,8 @@ struct nsg_batch {
         cudaFree(d_insts);
         cudaFree(d_lu);
         cudaFree(d_work);
+        cudaFree(d_lrows);
+        cudaFree(d_urows);
     }
 };
 

@@ -95,6 +95,12 @@ void finish(TopologyPlan& p) {
             }
         }
 
+    p.rowcopy_pos.assign(p.nnz_lu, -1);
+    for (int32_t i = 0; i < n; ++i) {
+        for (int32_t k = p.lrow_ptr[i]; k < p.lrow_ptr[i + 1]; ++k) p.rowcopy_pos[p.lrow_pos[k]] = k;
+        for (int32_t k = p.urow_ptr[i]; k < p.urow_ptr[i + 1]; ++k) p.rowcopy_pos[p.urow_pos[k]] = k;
+    }
+
     // Level schedules.
     std::vector<int32_t> lev(n, 0);
     for (int32_t j = 0; j < n; ++j) {
@@ -142,7 +148,7 @@ void finish(TopologyPlan& p) {
     X(perm_row) X(perm_col) X(col_ptr) X(row_idx) X(diag_pos) X(lu_src)         \
     X(upd_start) X(upd_dst) X(lrow_ptr) X(lrow_pos) X(lrow_col) X(urow_ptr)     \
     X(urow_pos) X(urow_col) X(col_lev_ptr) X(col_lev) X(fwd_lev_ptr) X(fwd_lev) \
-    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev)
+    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos)
 
 int64_t TopologyPlan::device_words() const {
     int64_t w = 0;

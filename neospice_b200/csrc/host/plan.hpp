@@ -38,6 +38,10 @@ struct TopologyPlan {
     // upper, columns ascending): LU position and column of each entry.
     std::vector<int32_t> lrow_ptr, lrow_pos, lrow_col;
     std::vector<int32_t> urow_ptr, urow_pos, urow_col;
+    // Per LU position: its index in the row-major copy of L (rows > column)
+    // or of U (rows < column), which the refactor writes alongside the
+    // column-major values so the sweeps read contiguous rows; -1 for pivots.
+    std::vector<int32_t> rowcopy_pos;
 
     // Level schedules (ptr over levels, then members sorted by level).
     //   col:  column j after every r with U(r, j) != 0  (refactor and the

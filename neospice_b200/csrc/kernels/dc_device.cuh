@@ -26,6 +26,7 @@ struct DcDesc {
     // workspace (doubles): solution, previous iterate, sweep scratch, matrix
     // values, LU values, term values, diode state, diode constants
     int64_t x_off, xold_off, w_off, a_off, lu_off, tv_off, dstate_off, dconst_off;
+    int64_t lrows_off, urows_off;  // row-major copies of L and U for the sweeps
 };
 
 // SimOptions of the reference (src/core/types.hpp:24-66) used by the loop.

@@ -51,10 +51,14 @@ struct RefactorResult {
 // wait is bounded: past kSpinLimit polls the instance reports kStatusTimeout
 // and the warp moves on, so the CTA always finishes.  Begins and ends with
 // __syncthreads().
+// When lrows/urows are given, every L and U entry is also written to its
+// position in the row-major copies the dataflow sweeps read.
 __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
                                                    const double* __restrict__ a, double* __restrict__ lu,
                                                    double diag_gmin, int check_pivots,
-                                                   double rel_threshold, double* smem, int colbuf) {
+                                                   double rel_threshold, double* smem, int colbuf,
+                                                   double* __restrict__ lrows = nullptr,
+                                                   double* __restrict__ urows = nullptr) {
     const int32_t n = pd.n;
     const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
     const int32_t* row_idx = pool + pd.off[PA_row_idx];
@@ -166,6 +170,13 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
             fail = (piv == 0.0);
         }
         for (int32_t t = lane; t < len; t += 32) lu[c0 + t] = (t == dj) ? 1.0 / piv : buf[t];
+        if (lrows) {
+            const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
+            for (int32_t t = lane; t < len; t += 32) {
+                if (t < dj) urows[rowcopy[c0 + t]] = buf[t];
+                else if (t > dj) lrows[rowcopy[c0 + t]] = buf[t];
+            }
+        }
         __syncwarp();
         if (lane == 0) {
             if (timed_out) {
@@ -247,14 +258,16 @@ __host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
     return (sizeof(double) + sizeof(int32_t)) * static_cast<size_t>(n);
 }
 
-// Wait (bounded) until flag[i] is set; returns false on timeout.
+// Wait (bounded) until flag[i] is set; returns false on timeout.  The
+// producer stores its value, fences, then sets the flag; the consumer reads
+// the flag and then the value through volatile accesses, which keeps their
+// order, and fences after a wait that actually spun.
 __device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
-    if (flag[i] == 0) {
-        int spins = 0;
-        while (flag[i] == 0) {
-            if (++spins > kSpinLimit) return false;
-            __nanosleep(32);
-        }
+    if (flag[i] != 0) return true;
+    int spins = 0;
+    while (flag[i] == 0) {
+        if (++spins > kSpinLimit) return false;
+        __nanosleep(32);
     }
     __threadfence_block();
     return true;
@@ -263,16 +276,19 @@ __device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
 // x <- A^{-1} x (SparseMatrix::solve) by the whole CTA, dataflow schedule:
 // thread t takes rows t, t + blockDim, ... of the level-sorted order and
 // waits, entry by entry, for the rows it reads.  The vector and the flags live
-// in shared memory (flow_solve_smem_bytes).  Same arithmetic, in the same
-// order per row, as cta_solve.  Returns false if a bounded wait gave up.
+// in shared memory (flow_solve_smem_bytes); L and U are read from the
+// row-major copies the refactor wrote.  Same arithmetic, in the same order
+// per row, as cta_solve.  Returns false if a bounded wait gave up.
 __device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
-                                      const double* __restrict__ lu, double* __restrict__ x,
+                                      const double* __restrict__ lu,
+                                      const double* __restrict__ lrows,
+                                      const double* __restrict__ urows, double* __restrict__ x,
                                       double* smem) {
     const int32_t n = pd.n;
     const int32_t* perm_row = pool + pd.off[PA_perm_row];
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
-    double* w = smem;
+    volatile double* w = smem;
     volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + n);
     __shared__ int32_t s_ok;
     __syncthreads();
@@ -285,17 +301,18 @@ __device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restr
     bool ok = true;
     {   // forward: L with the reciprocal pivot
         const int32_t* lp = pool + pd.off[PA_lrow_ptr];
-        const int32_t* lpos = pool + pd.off[PA_lrow_pos];
         const int32_t* lcol = pool + pd.off[PA_lrow_col];
         const int32_t* order = pool + pd.off[PA_fwd_lev];
         for (int32_t k = threadIdx.x; k < n; k += blockDim.x) {
             const int32_t i = order[k];
             double t = w[i];
-            for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
+            const int32_t e1 = lp[i + 1];
+            for (int32_t e = lp[i]; e < e1; ++e) {
                 const int32_t c = lcol[e];
+                const double lv = lrows[e];
                 if (ok && !wait_flag(done, c)) ok = false;
                 const double xc = w[c];
-                if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu[lpos[e]]));
+                if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lv));
             }
             w[i] = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
             __threadfence_block();
@@ -307,16 +324,17 @@ __device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restr
     __syncthreads();
     {   // backward: unit-diagonal U
         const int32_t* up = pool + pd.off[PA_urow_ptr];
-        const int32_t* upos = pool + pd.off[PA_urow_pos];
         const int32_t* ucol = pool + pd.off[PA_urow_col];
         const int32_t* order = pool + pd.off[PA_bwd_lev];
         for (int32_t k = threadIdx.x; k < n; k += blockDim.x) {
             const int32_t i = order[k];
             double t = w[i];
-            for (int32_t e = up[i]; e < up[i + 1]; ++e) {
+            const int32_t e1 = up[i + 1];
+            for (int32_t e = up[i]; e < e1; ++e) {
                 const int32_t c = ucol[e];
+                const double uv = urows[e];
                 if (ok && !wait_flag(done, c)) ok = false;
-                t = lu_sub(t, lu_mul(lu[upos[e]], w[c]));
+                t = lu_sub(t, lu_mul(uv, w[c]));
             }
             w[i] = t;
             __threadfence_block();

@@ -10,13 +10,15 @@ enum PlanArray : int {
     PA_perm_row, PA_perm_col, PA_col_ptr, PA_row_idx, PA_diag_pos, PA_lu_src,
     PA_upd_start, PA_upd_dst, PA_lrow_ptr, PA_lrow_pos, PA_lrow_col, PA_urow_ptr,
     PA_urow_pos, PA_urow_col, PA_col_lev_ptr, PA_col_lev, PA_fwd_lev_ptr, PA_fwd_lev,
-    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_COUNT
+    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_rowcopy_pos, PA_COUNT
 };
 
 struct PlanDesc {
     int32_t n, nnz_a, nnz_lu;
     int32_t n_col_lev, n_fwd_lev, n_bwd_lev, n_tbw_lev;
     int32_t max_col;  // longest LU column
+    int32_t nnz_l, nnz_u;  // strictly lower / upper entries
+    int32_t pad;
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
 };
 
@@ -27,6 +29,8 @@ struct InstDesc {
     int64_t lu_off;  // into the batch's LU values
     int64_t x_off;   // into the caller's rhs / solution vectors
     int64_t w_off;   // into the batch's sweep workspace
+    int64_t lrows_off;  // into the batch's row-major L copy
+    int64_t urows_off;  // into the batch's row-major U copy
 };
 
 // Per-instance status codes written by the refactor.

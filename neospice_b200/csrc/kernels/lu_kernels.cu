@@ -132,12 +132,14 @@ refactor_flow_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
                      const InstDesc* __restrict__ insts, const double* __restrict__ A,
                      double* __restrict__ LU, double diag_gmin, int check_pivots,
                      double rel_threshold, int32_t* __restrict__ status,
-                     int32_t* __restrict__ fail_step, int colbuf) {
+                     int32_t* __restrict__ fail_step, int colbuf,
+                     double* __restrict__ lrows, double* __restrict__ urows) {
     extern __shared__ double smem[];
     const InstDesc inst = insts[blockIdx.x];
     const RefactorResult r =
         cta_refactor_flow(plans[inst.plan], pool, A + inst.a_off, LU + inst.lu_off, diag_gmin,
-                          check_pivots, rel_threshold, smem, colbuf);
+                          check_pivots, rel_threshold, smem, colbuf, lrows + inst.lrows_off,
+                          urows + inst.urows_off);
     if (threadIdx.x == 0) {
         status[inst.index] = r.code;
         if (fail_step) fail_step[inst.index] = r.step;
@@ -151,6 +153,18 @@ solve_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ poo
              double* __restrict__ X, double* __restrict__ W) {
     const InstDesc inst = insts[blockIdx.x];
     cta_solve(plans[inst.plan], pool, LU + inst.lu_off, X + inst.x_off, W + inst.w_off);
+}
+
+// x <- A^{-1} x, dataflow sweeps on the row-major copies (cta_solve_flow).
+__global__ void __launch_bounds__(kFlowThreads)
+solve_flow_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
+                  const InstDesc* __restrict__ insts, const double* __restrict__ LU,
+                  const double* __restrict__ lrows, const double* __restrict__ urows,
+                  double* __restrict__ X) {
+    extern __shared__ double smem[];
+    const InstDesc inst = insts[blockIdx.x];
+    cta_solve_flow(plans[inst.plan], pool, LU + inst.lu_off, lrows + inst.lrows_off,
+                   urows + inst.urows_off, X + inst.x_off, smem);
 }
 
 // x <- A^{-T} x with the same LU (SparseMatrix::solve_transposed).
@@ -167,7 +181,7 @@ cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const In
                             int count, const double* A, double* LU, double diag_gmin,
                             int check_pivots, double rel_threshold, int32_t* status,
                             int32_t* fail_step, int max_col, int max_n, bool allow_flow,
-                            cudaStream_t stream) {
+                            double* lrows, double* urows, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
     const size_t smem = flow_smem_bytes(colbuf, max_n);
@@ -182,7 +196,7 @@ cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const In
         }
         refactor_flow_kernel<<<count, kFlowThreads, smem, stream>>>(
             plans, pool, insts, A, LU, diag_gmin, check_pivots, rel_threshold, status, fail_step,
-            colbuf);
+            colbuf, lrows, urows);
     } else {
         refactor_kernel<<<count, 256, 0, stream>>>(plans, pool, insts, A, LU, diag_gmin,
                                                    check_pivots, rel_threshold, status, fail_step);
@@ -192,8 +206,23 @@ cudaError_t launch_refactor(const PlanDesc* plans, const int32_t* pool, const In
 
 cudaError_t launch_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                          int count, const double* LU, double* X, double* W, bool transposed,
+                         const double* lrows, const double* urows, int max_n,
                          cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
+    const size_t smem = flow_solve_smem_bytes(max_n);
+    if (!transposed && lrows && smem <= 200 * 1024) {
+        static bool configured = false;
+        if (!configured) {
+            cudaError_t e = cudaFuncSetAttribute(solve_flow_kernel,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 200 * 1024);
+            if (e != cudaSuccess) return e;
+            configured = true;
+        }
+        solve_flow_kernel<<<count, kFlowThreads, smem, stream>>>(plans, pool, insts, LU, lrows,
+                                                                  urows, X);
+        return cudaGetLastError();
+    }
     if (transposed)
         solve_transposed_kernel<<<count, 256, 0, stream>>>(plans, pool, insts, LU, X, W);
     else

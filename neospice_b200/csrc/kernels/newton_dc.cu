@@ -35,7 +35,8 @@ __device__ __forceinline__ double term_value(int32_t op, double p, double gmin) 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kFlowThreads)
+// Two CTAs per SM: registers are capped at 64 per thread.
+__global__ void __launch_bounds__(kFlowThreads, 2)
 newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ lu_pool,
                  const DcDesc* __restrict__ descs, const int32_t* __restrict__ prog,
                  const double* __restrict__ params, double* __restrict__ work,
@@ -59,6 +60,8 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     double* xold = work + d.xold_off;
     double* a = work + d.a_off;
     double* lu = work + d.lu_off;
+    double* lrows = work + d.lrows_off;
+    double* urows = work + d.urows_off;
     double* tv = work + d.tv_off;
     double* dstate = work + d.dstate_off;   // (vd, cd, gd) per diode
     double* dconst = work + d.dconst_off;   // (csat, vte, vcrit) per diode
@@ -139,7 +142,8 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         // refactor) re-validates pivots; refactorize checks zero pivots only.
         const bool numeric = force_numeric || initjct;
         const RefactorResult fr = cta_refactor_flow(pd, lu_pool, a, lu, opt.diag_gmin,
-                                                    numeric && !first_numeric, 1e-3, smem, colbuf);
+                                                    numeric && !first_numeric, 1e-3, smem, colbuf,
+                                                    lrows, urows);
         if (fr.code == kStatusTimeout) {
             result = kStatusTimeout;
             iters = iter + 1;
@@ -161,7 +165,7 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
             continue;
         }
 
-        if (!cta_solve_flow(pd, lu_pool, lu, x, smem)) {
+        if (!cta_solve_flow(pd, lu_pool, lu, lrows, urows, x, smem)) {
             result = kStatusTimeout;
             iters = iter + 1;
             break;
