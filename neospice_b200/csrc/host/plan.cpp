@@ -95,6 +95,15 @@ void finish(TopologyPlan& p) {
             }
         }
 
+    p.umeta.assign(4 * static_cast<size_t>(p.nnz_lu), 0);
+    for (int32_t j = 0; j < n; ++j)
+        for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j]; ++q) {
+            const int32_t r = p.row_idx[q];
+            p.umeta[4 * q] = r;
+            p.umeta[4 * q + 1] = p.diag_pos[r];
+            p.umeta[4 * q + 2] = p.col_ptr[r + 1] - p.diag_pos[r] - 1;
+            p.umeta[4 * q + 3] = p.upd_start[q];
+        }
     p.rowcopy_pos.assign(p.nnz_lu, -1);
     for (int32_t i = 0; i < n; ++i) {
         for (int32_t k = p.lrow_ptr[i]; k < p.lrow_ptr[i + 1]; ++k) p.rowcopy_pos[p.lrow_pos[k]] = k;
@@ -148,7 +157,7 @@ void finish(TopologyPlan& p) {
     X(perm_row) X(perm_col) X(col_ptr) X(row_idx) X(diag_pos) X(lu_src)         \
     X(upd_start) X(upd_dst) X(lrow_ptr) X(lrow_pos) X(lrow_col) X(urow_ptr)     \
     X(urow_pos) X(urow_col) X(col_lev_ptr) X(col_lev) X(fwd_lev_ptr) X(fwd_lev) \
-    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos)
+    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos) X(umeta)
 
 int64_t TopologyPlan::device_words() const {
     int64_t w = 0;

@@ -42,6 +42,10 @@ struct TopologyPlan {
     // or of U (rows < column), which the refactor writes alongside the
     // column-major values so the sweeps read contiguous rows; -1 for pivots.
     std::vector<int32_t> rowcopy_pos;
+    // Per LU position q of a U entry (r, j): {r, diag_pos[r], |L(:, r)|,
+    // upd_start[q]} packed as four int32 (zeros elsewhere), so one 16-byte
+    // load gives the refactor everything it needs to apply entry q.
+    std::vector<int32_t> umeta;
 
     // Level schedules (ptr over levels, then members sorted by level).
     //   col:  column j after every r with U(r, j) != 0  (refactor and the

@@ -97,20 +97,28 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
             buf[t] = v;
         }
         __syncwarp();
-        // One-step lookahead: while the update of U entry q runs, the pivot
-        // reciprocal, the first 32 entries of L(:, r) and their destinations
-        // for entry q+1 are already in registers (when column r is done).
+        // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
+        // entries at a time in registers (lane k holds entry base+k) and
+        // broadcast by shuffle.  One-step lookahead: while the update of
+        // entry q runs, the pivot reciprocal, the first 32 entries of L(:, r)
+        // and their destinations for entry q+1 are loaded (when column r is
+        // done), so a step waits on at most one global round trip.
+        const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]) + c0;
         bool timed_out = false;
+        int4 chunk = make_int4(0, 0, 0, 0), next_chunk = make_int4(0, 0, 0, 0);
+        if (lane < dj) chunk = umeta[lane];
+        if (32 + lane < dj) next_chunk = umeta[32 + lane];
         double rd_c = 0.0, lv_c = 0.0;
         int32_t l0_c = 0, cnt_c = 0, us_c = 0, ld_c = 0;
         bool have_c = false;
-        auto fetch = [&](int32_t q, bool wait, double& rd, double& lv, int32_t& l0, int32_t& cnt,
-                         int32_t& us, int32_t& ld) -> bool {
-            const int32_t r = row_idx[c0 + q];
+        // Load the operands of entry q (metadata m) if column m.x is done,
+        // or after waiting for it.
+        auto fetch = [&](const int4 m, bool wait, double& rd, double& lv, int32_t& l0,
+                         int32_t& cnt, int32_t& us, int32_t& ld) -> bool {
             int ready = 0;
             if (lane == 0) {
                 int spins = 0;
-                while ((ready = done[r]) == 0 && wait) {
+                while ((ready = done[m.x]) == 0 && wait) {
                     if (++spins > kSpinLimit) {
                         timed_out = true;
                         break;
@@ -123,25 +131,39 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
             timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
             __syncwarp();
             if (!ready) return false;
-            const int32_t dr = diag_pos[r];
-            rd = lu[dr];
-            l0 = dr + 1;
-            cnt = col_ptr[r + 1] - l0;
-            us = upd_start[c0 + q];
+            rd = lu[m.y];
+            l0 = m.y + 1;
+            cnt = m.z;
+            us = m.w;
             lv = (lane < cnt) ? lu[l0 + lane] : 0.0;
             ld = (lane < cnt) ? upd_dst[us + lane] : 0;
             return true;
-        }
-        ;
+        };
+        auto meta = [&](int32_t q) -> int4 {
+            const int k = q & 31;
+            const int4 src = ((q >> 5) == 0) ? chunk : next_chunk;
+            int4 m;
+            m.x = __shfl_sync(0xffffffffu, src.x, k);
+            m.y = __shfl_sync(0xffffffffu, src.y, k);
+            m.z = __shfl_sync(0xffffffffu, src.z, k);
+            m.w = __shfl_sync(0xffffffffu, src.w, k);
+            return m;
+        };
+        int32_t base = 0;  // entry index held in chunk's lane 0
         for (int32_t q = 0; q < dj; ++q) {
+            if (q - base == 32) {  // advance the register window by 32 entries
+                base += 32;
+                chunk = next_chunk;
+                next_chunk = (base + 32 + lane < dj) ? umeta[base + 32 + lane] : make_int4(0, 0, 0, 0);
+            }
             if (!have_c) {
-                fetch(q, true, rd_c, lv_c, l0_c, cnt_c, us_c, ld_c);
+                fetch(meta(q - base), true, rd_c, lv_c, l0_c, cnt_c, us_c, ld_c);
                 if (timed_out) break;
             }
             double rd_n = 0.0, lv_n = 0.0;
             int32_t l0_n = 0, cnt_n = 0, us_n = 0, ld_n = 0;
-            const bool have_n =
-                (q + 1 < dj) && fetch(q + 1, false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
+            const bool have_n = (q + 1 < dj) &&
+                                fetch(meta(q + 1 - base), false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
             const double u = lu_mul(buf[q], rd_c);
             __syncwarp();
             if (lane == 0) buf[q] = u;

@@ -10,7 +10,7 @@ enum PlanArray : int {
     PA_perm_row, PA_perm_col, PA_col_ptr, PA_row_idx, PA_diag_pos, PA_lu_src,
     PA_upd_start, PA_upd_dst, PA_lrow_ptr, PA_lrow_pos, PA_lrow_col, PA_urow_ptr,
     PA_urow_pos, PA_urow_col, PA_col_lev_ptr, PA_col_lev, PA_fwd_lev_ptr, PA_fwd_lev,
-    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_rowcopy_pos, PA_COUNT
+    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_rowcopy_pos, PA_umeta, PA_COUNT
 };
 
 struct PlanDesc {
