@@ -23,6 +23,21 @@ constexpr int kSpinLimit = 1 << 22;
 __device__ __forceinline__ double lu_mul(double x, double y) { return __dmul_rn(x, y); }
 __device__ __forceinline__ double lu_sub(double x, double y) { return __dsub_rn(x, y); }
 
+// Completion flags in shared memory: the producer publishes with a release
+// store after writing its values, the consumer reads with an acquire load
+// before reading them (PTX ld.acquire / st.release at CTA scope).
+__device__ __forceinline__ int32_t flag_acquire(const volatile int32_t* f) {
+    int32_t v;
+    const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(const_cast<int32_t*>(f)));
+    asm volatile("ld.acquire.cta.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void flag_release(volatile int32_t* f, int32_t v) {
+    const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(const_cast<int32_t*>(f)));
+    asm volatile("st.release.cta.shared.b32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -118,14 +133,13 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
             int ready = 0;
             if (lane == 0) {
                 int spins = 0;
-                while ((ready = done[m.x]) == 0 && wait) {
+                while ((ready = flag_acquire(done + m.x)) == 0 && wait) {
                     if (++spins > kSpinLimit) {
                         timed_out = true;
                         break;
                     }
                     __nanosleep(64);
                 }
-                __threadfence_block();
             }
             ready = __shfl_sync(0xffffffffu, ready, 0);
             timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
@@ -209,8 +223,7 @@ __device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int
                 if (s_fail_code != kStatusTimeout)
                     s_fail_code = check_pivots ? kStatusReorder : kStatusSingular;
             }
-            __threadfence_block();
-            done[j] = 1;
+            flag_release(done + j, 1);
         }
         __syncwarp();
     }
@@ -280,18 +293,16 @@ __host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
     return (sizeof(double) + sizeof(int32_t)) * static_cast<size_t>(n);
 }
 
-// Wait (bounded) until flag[i] is set; returns false on timeout.  The
-// producer stores its value, fences, then sets the flag; the consumer reads
-// the flag and then the value through volatile accesses, which keeps their
-// order, and fences after a wait that actually spun.
+// Wait (bounded) until flag[i] is set; returns false on timeout.  The flag is
+// read with acquire semantics, so the value read after it is the one the
+// producer wrote before its release store.
 __device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
-    if (flag[i] != 0) return true;
+    if (flag_acquire(flag + i) != 0) return true;
     int spins = 0;
-    while (flag[i] == 0) {
+    while (flag_acquire(flag + i) == 0) {
         if (++spins > kSpinLimit) return false;
         __nanosleep(32);
     }
-    __threadfence_block();
     return true;
 }
 
@@ -337,8 +348,7 @@ __device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restr
                 if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lv));
             }
             w[i] = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
-            __threadfence_block();
-            done[i] = 1;
+            flag_release(done + i, 1);
         }
     }
     __syncthreads();
@@ -359,8 +369,7 @@ __device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restr
                 t = lu_sub(t, lu_mul(uv, w[c]));
             }
             w[i] = t;
-            __threadfence_block();
-            done[i] = 1;
+            flag_release(done + i, 1);
         }
     }
     if (!ok) s_ok = 0;
