@@ -73,6 +73,13 @@ def ref() -> ctypes.CDLL:
         lib.nsref_solver_element_count.argtypes = [_V]
         lib.nsref_solver_export.argtypes = [_V] * 7
         lib.nsref_mesh_dc.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V, _V]
+        lib.nsref_sim_run.restype = _V
+        lib.nsref_sim_run.argtypes = [ctypes.c_char_p, _I, _D, _D]
+        lib.nsref_sim_info.argtypes = [_V, _V, _V, _V, _V, _V, _V]
+        lib.nsref_sim_copy.argtypes = [_V, _V, _V]
+        lib.nsref_sim_error.restype = ctypes.c_char_p
+        lib.nsref_sim_error.argtypes = [_V]
+        lib.nsref_sim_free.argtypes = [_V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
         _ref = lib
@@ -210,3 +217,27 @@ def ref_mesh_initjct(m):
     if rc != nnz:
         raise RuntimeError("reference INITJCT evaluation failed")
     return cp, ri, vals, rhs
+
+
+def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0):
+    """Run a circuit description (see nsref_sim_run in ref_shim.cpp) through
+    the reference: analysis 0 = DC operating point, 1 = transient.  Returns
+    (times, values [npoints x width], info dict)."""
+    lib = ref()
+    h = lib.nsref_sim_run(desc.encode(), int(analysis), float(tstep), float(tstop))
+    try:
+        nn, nv, npts, it, rej = (ctypes.c_int() for _ in range(5))
+        sec = ctypes.c_double()
+        rc = lib.nsref_sim_info(h, ctypes.addressof(nn), ctypes.addressof(nv), ctypes.addressof(npts),
+                                ctypes.addressof(it), ctypes.addressof(sec), ctypes.addressof(rej))
+        if rc != 0:
+            raise RuntimeError("reference failed: " + lib.nsref_sim_error(h).decode())
+        width = nv.value if analysis == 0 else nn.value
+        times = np.zeros(npts.value)
+        values = np.zeros((npts.value, width))
+        lib.nsref_sim_copy(h, _p(times), _p(values))
+        info = dict(num_nodes=nn.value, num_vars=nv.value, points=npts.value,
+                    iterations=it.value, seconds=sec.value, rejected=rej.value)
+        return times, values, info
+    finally:
+        lib.nsref_sim_free(h)

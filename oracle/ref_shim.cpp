@@ -12,10 +12,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <memory>
-#include <sstream>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -24,6 +24,10 @@
 #include "api/neospice.hpp"
 #include "core/circuit.hpp"
 #include "core/dc.hpp"
+#include "core/transient.hpp"
+#include "devices/capacitor.hpp"
+#include "devices/isource.hpp"
+#include "devices/vsource.hpp"
 #include "core/matrix.hpp"
 #include "core/newton.hpp"
 #include "core/solver_iface.hpp"
@@ -272,5 +276,164 @@ int nsref_mesh_initjct(int side, const double* r_h, const double* r_v, int n_dio
         return -1;
     }
 }
+
+// ---------------------------------------------------------------------------
+// Generic runner on a line-based circuit description, built through the
+// reference's typed Circuit API in the order given (so node numbering and
+// device load order match a circuit built the same way elsewhere):
+//   nodes N                          nodes n0..n{N-1} (MNA indices 0..N-1)
+//   R a b ohms | C a b farads [ic] | V a b dc | I a b dc
+//   VPULSE a b v1 v2 td tr tf pw per | IPULSE ... | VPWL a b t0 v0 t1 v1 ...
+//   IPWL a b t0 v0 ... | D a k IS N | MODEL name card... | M d g s b model W L
+//   OPT name value                   (reltol, abstol, vntol, gmin, itl4, method)
+// Node -1 is ground.  analysis 0 = DC operating point, 1 = transient.
+struct SimResult {
+    std::string error;
+    int num_nodes = 0, num_vars = 0, iterations = 0, rejected = 0;
+    double seconds = 0.0;
+    std::vector<double> times;
+    std::vector<double> values;  // npoints x (num_vars for DC, num_nodes for tran)
+};
+
+static NodeId node_of(const std::vector<NodeId>& nodes, int k) {
+    return k < 0 ? GND : nodes.at(k);
+}
+
+void* nsref_sim_run(const char* desc, int analysis, double tstep, double tstop) {
+    auto* res = new SimResult;
+    try {
+        auto t0 = std::chrono::steady_clock::now();
+        Circuit ckt;
+        // Tokenised by hand (strtod/strtol): iostreams are avoided because
+        // the loading process may carry a different C++ runtime.
+        std::vector<std::vector<std::string>> lines;
+        {
+            std::vector<std::string> cur;
+            std::string tok;
+            for (const char* p = desc;; ++p) {
+                const char c = *p;
+                if (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\0') {
+                    if (!tok.empty()) cur.push_back(tok), tok.clear();
+                    if ((c == '\n' || c == '\0') && !cur.empty()) lines.push_back(cur), cur.clear();
+                    if (c == '\0') break;
+                } else {
+                    tok.push_back(c);
+                }
+            }
+        }
+        std::vector<NodeId> nodes;
+        int dev = 0;
+        for (const auto& tk : lines) {
+            const std::string& kind = tk[0];
+            const std::string name = kind + std::to_string(dev++);
+            auto I_ = [&](size_t k) { return static_cast<int>(std::strtol(tk.at(k).c_str(), nullptr, 10)); };
+            auto D_ = [&](size_t k) { return std::strtod(tk.at(k).c_str(), nullptr); };
+            auto rest = [&](size_t from) {
+                std::vector<double> v;
+                for (size_t k = from; k < tk.size(); ++k) v.push_back(D_(k));
+                return v;
+            };
+            if (kind == "nodes") {
+                const int n = I_(1);
+                for (int i = 0; i < n; ++i) nodes.push_back(ckt.node("n" + std::to_string(i)));
+            } else if (kind == "R" || kind == "C" || kind == "V" || kind == "I") {
+                NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
+                auto v = rest(3);
+                if (kind == "R") ckt.R(name, a, b, v.at(0));
+                else if (kind == "C") {
+                    if (v.size() > 1) ckt.C(name, a, b, v[0], v[1]);
+                    else ckt.C(name, a, b, v.at(0));
+                } else if (kind == "V") ckt.V(name, a, b, v.at(0));
+                else ckt.I(name, a, b, v.at(0));
+            } else if (kind == "VPULSE" || kind == "IPULSE" || kind == "VPWL" || kind == "IPWL") {
+                NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
+                auto v = rest(3);
+                const bool is_v = kind[0] == 'V';
+                DevId id = is_v ? ckt.V(name, a, b, 0.0) : ckt.I(name, a, b, 0.0);
+                Device* d = ckt.devices()[static_cast<int32_t>(id)].get();
+                if (kind == "VPULSE" || kind == "IPULSE") {
+                    PulseParams pp{v.at(0), v.at(1), v.at(2), v.at(3), v.at(4), v.at(5), v.at(6)};
+                    if (is_v) static_cast<VSource*>(d)->set_pulse(pp);
+                    else static_cast<ISource*>(d)->set_pulse(pp);
+                } else {
+                    PwlParams pw;
+                    for (size_t k = 0; k + 1 < v.size(); k += 2) pw.points.emplace_back(v[k], v[k + 1]);
+                    if (is_v) static_cast<VSource*>(d)->set_pwl(pw);
+                    else static_cast<ISource*>(d)->set_pwl(pw);
+                }
+            } else if (kind == "D") {
+                char card[160];
+                std::snprintf(card, sizeof card, ".model dm%d D(IS=%.17g N=%.17g)", dev, D_(3), D_(4));
+                ckt.model(card);
+                ckt.D(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), "dm" + std::to_string(dev));
+            } else if (kind == "MODEL") {
+                std::string card;
+                for (size_t k = 1; k < tk.size(); ++k) card += (k > 1 ? " " : "") + tk[k];
+                ckt.model(card);
+            } else if (kind == "M") {
+                ckt.M(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), node_of(nodes, I_(3)),
+                      node_of(nodes, I_(4)), tk.at(5), D_(6), D_(7));
+            } else if (kind == "OPT") {
+                const std::string& key = tk.at(1);
+                const double val = D_(2);
+                if (key == "reltol") ckt.options.reltol = val;
+                else if (key == "abstol") ckt.options.abstol = val;
+                else if (key == "vntol") ckt.options.vntol = val;
+                else if (key == "gmin") ckt.options.gmin = val;
+                else if (key == "itl4") ckt.options.itl4 = static_cast<int>(val);
+                else if (key == "gear") ckt.options.method = val != 0.0 ? "gear" : "trap";
+            } else {
+                throw std::invalid_argument("unknown line kind: " + kind);
+            }
+        }
+        ckt.finalize_if_needed();
+        res->num_nodes = ckt.num_nodes();
+        res->num_vars = ckt.num_vars();
+        if (analysis == 0) {
+            DCResult r = solve_dc(ckt);
+            const auto* op = ckt.operating_point();
+            if (!op) throw std::runtime_error("no operating point");
+            res->times.push_back(0.0);
+            res->values.assign(op->begin(), op->end());
+            res->iterations = r.status.iterations;
+        } else {
+            TransientResult r = solve_transient(ckt, tstep, tstop);
+            res->times = r.time;
+            const size_t np = r.time.size();
+            res->values.resize(np * res->num_nodes);
+            for (int i = 0; i < res->num_nodes; ++i)
+                for (size_t k = 0; k < np; ++k) res->values[k * res->num_nodes + i] = r.voltages_dense[i][k];
+            res->iterations = r.status.iterations;
+            res->rejected = r.rejected_steps;
+        }
+        res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } catch (const std::exception& e) {
+        res->error = e.what();
+    }
+    return res;
+}
+
+int nsref_sim_info(void* h, int* num_nodes, int* num_vars, int* npoints, int* iterations,
+                   double* seconds, int* rejected) {
+    auto* r = static_cast<SimResult*>(h);
+    if (num_nodes) *num_nodes = r->num_nodes;
+    if (num_vars) *num_vars = r->num_vars;
+    if (npoints) *npoints = static_cast<int>(r->times.size());
+    if (iterations) *iterations = r->iterations;
+    if (seconds) *seconds = r->seconds;
+    if (rejected) *rejected = r->rejected;
+    return r->error.empty() ? 0 : -1;
+}
+
+int nsref_sim_copy(void* h, double* times, double* values) {
+    auto* r = static_cast<SimResult*>(h);
+    std::memcpy(times, r->times.data(), sizeof(double) * r->times.size());
+    std::memcpy(values, r->values.data(), sizeof(double) * r->values.size());
+    return 0;
+}
+
+const char* nsref_sim_error(void* h) { return static_cast<SimResult*>(h)->error.c_str(); }
+
+void nsref_sim_free(void* h) { delete static_cast<SimResult*>(h); }
 
 }  // extern "C"
