@@ -149,22 +149,39 @@ int nsg_batch_lu_to_host(const nsg_batch* batch, double* out);
  * nsg_circuit_finalize mirrors Circuit::finalize (src/core/circuit.cpp:201-283):
  * ngspice load order, branch unknowns after the nodes, sparsity pattern,
  * dead-node placeholders.  Parameters are kept in creation order: resistor
- * {ohms}, vsource {volts}, isource {amps}, diode {IS, N}. */
+ * {ohms}, capacitor {farads, ic}, DC source {value}, PULSE source {v1, v2,
+ * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode {IS, N}. */
 typedef struct nsg_circuit nsg_circuit;
+
+#define NSG_WAVE_DC 0
+#define NSG_WAVE_PULSE 1
+#define NSG_WAVE_PWL 2
 
 int nsg_circuit_create(int num_nodes, nsg_circuit** out);
 void nsg_circuit_free(nsg_circuit* c);
-/* Circuit::R (src/core/circuit.hpp:180). */
+/* Circuit::R (src/core/circuit.hpp:179). */
 int nsg_circuit_add_resistor(nsg_circuit* c, int a, int b, double ohms);
-/* Circuit::V with a DC value (src/core/circuit.hpp:187). */
+/* Circuit::V with a DC value (src/core/circuit.hpp:186). */
 int nsg_circuit_add_vsource(nsg_circuit* c, int p, int n, double volts);
 /* Circuit::I with a DC value (src/core/circuit.hpp:189). */
 int nsg_circuit_add_isource(nsg_circuit* c, int p, int n, double amps);
-/* Circuit::D with a level-1 model card D(IS=is N=n) (src/core/circuit.hpp:206;
+/* Circuit::D with a level-1 model card D(IS=is N=n) (src/core/circuit.hpp:210;
  * series resistance 0, T = TNOM). */
 int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, double n_emission);
+/* Circuit::C (src/core/circuit.hpp:180) with an optional IC= value
+ * (has_ic != 0). */
+int nsg_circuit_add_capacitor(nsg_circuit* c, int a, int b, double farads, int has_ic,
+                              double ic);
+/* Circuit::V / Circuit::I followed by VSource::set_pulse / set_pwl
+ * (src/devices/vsource.hpp, isource.hpp): is_voltage selects V or I, wave is
+ * NSG_WAVE_*, values as listed above (PULSE: 7 values, a value <= 0 for tr,
+ * tf, pw or per takes the transient's default; PWL: time/value pairs). */
+int nsg_circuit_add_source_wave(nsg_circuit* c, int is_voltage, int p, int n, int wave,
+                                int nvalues, const double* values);
 /* Bulk forms: count devices in one call, arrays of terminals and values,
  * created in array order (identical to count single calls). */
+int nsg_circuit_add_capacitors(nsg_circuit* c, int count, const int* a, const int* b,
+                               const double* farads);
 int nsg_circuit_add_resistors(nsg_circuit* c, int count, const int* a, const int* b,
                               const double* ohms);
 int nsg_circuit_add_isources(nsg_circuit* c, int count, const int* p, const int* n,
@@ -221,6 +238,35 @@ int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, doubl
  * failed, 104 a bounded wait gave up; d_iterations: Newton iterations. */
 int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
                      int* d_iterations, void* stream);
+
+/* ---- Batched transient analysis (device) ------------------------------------
+ * solve_transient (src/core/transient.cpp:694-1067) for `count` circuits in one
+ * launch, one thread block per circuit, each with its own adaptive timestep:
+ * DC operating point (MODETRANOP), then the accept/reject loop of
+ * TimeStepController (src/core/timestep.cpp) with trapezoidal / backward-Euler
+ * capacitor companions and the capacitor truncation-error estimate.  The DC
+ * solver and the transient solver are ordered separately on their own first
+ * matrices, as the reference creates two solvers.  Circuits may hold R, C,
+ * DC/PULSE/PWL V and I sources (no diodes).  Every accepted timepoint (and
+ * t = 0) is written for the `nprobe` unknowns in probes[], at most max_points
+ * per circuit. */
+typedef struct nsg_tran_batch nsg_tran_batch;
+
+int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep, double tstop,
+                          int max_points, int nprobe, const int* probes, int threads,
+                          nsg_tran_batch** out);
+void nsg_tran_batch_free(nsg_tran_batch* b);
+/* Launch the whole batch on a stream (asynchronous). */
+int nsg_tran_batch_run(nsg_tran_batch* b, void* stream);
+/* Wait for the device and copy results to host arrays (any may be NULL):
+ * times [count*max_points], values [count*max_points*nprobe] (point-major),
+ * npoints [count] (points stored: t = 0 and the first accepted timepoints,
+ * at most max_points), status [count] (0 ok, 2 DC operating point failed, 3
+ * Newton failed at the minimum step, 4 step limit, 104 a bounded wait gave
+ * up), stats [count*4] (accepted steps, rejected steps, Newton iterations,
+ * DC failure code). */
+int nsg_tran_batch_results(const nsg_tran_batch* b, double* times, double* values, int* npoints,
+                           int* status, int* stats);
 
 #ifdef __cplusplus
 }

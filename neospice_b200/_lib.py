@@ -27,6 +27,9 @@ NSG_REORDER = 103
 NSG_TIMEOUT = 104
 NSG_SYMBOLIC_PER_INSTANCE = 0
 NSG_SYMBOLIC_PER_PATTERN = 1
+NSG_WAVE_DC = 0
+NSG_WAVE_PULSE = 1
+NSG_WAVE_PWL = 2
 NSG_STATIC_SCRATCH_DOUBLES = 1 << 20
 
 # name -> (restype, argtypes)
@@ -74,6 +77,16 @@ SIGNATURES = {
     "nsg_dc_batch_instance_stats": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll), P(c_ll)]),
     "nsg_dc_batch_set_options": (c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int]),
     "nsg_dc_batch_run": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nsg_circuit_add_capacitor": (c_int, [c_void_p, c_int, c_int, c_double, c_int, c_double]),
+    "nsg_circuit_add_source_wave": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int,
+                                            P(c_double)]),
+    "nsg_circuit_add_capacitors": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
+    "nsg_tran_batch_create": (c_int, [c_int, P(c_void_p), c_double, c_double, c_int, c_int,
+                                      P(c_int), c_int, P(c_void_p)]),
+    "nsg_tran_batch_free": (None, [c_void_p]),
+    "nsg_tran_batch_run": (c_int, [c_void_p, c_void_p]),
+    "nsg_tran_batch_results": (c_int, [c_void_p, P(c_double), P(c_double), P(c_int), P(c_int),
+                                       P(c_int)]),
 }
 
 _lib = None

@@ -1,10 +1,12 @@
-"""Circuits and batched DC operating points on the GPU.
+"""Circuits, batched DC operating points and batched transients on the GPU.
 
 ``Circuit`` mirrors the reference's typed Circuit API (src/core/circuit.hpp:
-179-237) for resistors, DC voltage/current sources and level-1 diodes; nodes
-are integers and ``GND`` (-1) is ground.  ``DcBatch`` runs the direct Newton
-attempt of Simulator::run_dc (src/core/dc.cpp:53-118) for many circuits in
-one kernel launch.
+179-237) for resistors, capacitors, DC / PULSE / PWL voltage and current
+sources and level-1 diodes; nodes are integers and ``GND`` (-1) is ground.
+``DcBatch`` runs the direct Newton attempt of Simulator::run_dc
+(src/core/dc.cpp:53-118) for many circuits in one kernel launch;
+``TranBatch`` runs solve_transient (src/core/transient.cpp:694-1067) for many
+circuits in one launch, each with its own adaptive timestep.
 """
 from __future__ import annotations
 
@@ -40,6 +42,36 @@ class Circuit:
 
     def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0):
         L.check(L.lib().nsg_circuit_add_diode(self._h, int(anode), int(cathode), float(IS), float(N)))
+
+    def C(self, a: int, b: int, farads: float, ic: float | None = None):
+        L.check(L.lib().nsg_circuit_add_capacitor(self._h, int(a), int(b), float(farads),
+                                                  int(ic is not None),
+                                                  0.0 if ic is None else float(ic)))
+
+    def _wave(self, is_v: bool, p: int, n: int, wave: int, values):
+        v = np.ascontiguousarray(values, np.float64)
+        L.check(L.lib().nsg_circuit_add_source_wave(self._h, int(is_v), int(p), int(n), int(wave),
+                                                    len(v), L.dptr(v)))
+
+    def VPULSE(self, p: int, n: int, v1, v2, td=0.0, tr=0.0, tf=0.0, pw=0.0, per=0.0):
+        """V source with PULSE(v1 v2 td tr tf pw per) (VSource::set_pulse)."""
+        self._wave(True, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
+
+    def IPULSE(self, p: int, n: int, v1, v2, td=0.0, tr=0.0, tf=0.0, pw=0.0, per=0.0):
+        self._wave(False, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
+
+    def VPWL(self, p: int, n: int, points):
+        """V source with PWL(t0 v0 t1 v1 ...) (VSource::set_pwl)."""
+        self._wave(True, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
+
+    def IPWL(self, p: int, n: int, points):
+        self._wave(False, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
+
+    def add_capacitors(self, a, b, farads):
+        a, b = np.ascontiguousarray(a, np.int32), np.ascontiguousarray(b, np.int32)
+        f = np.ascontiguousarray(np.broadcast_to(farads, a.shape), np.float64)
+        L.check(L.lib().nsg_circuit_add_capacitors(self._h, len(a), L.iptr(a), L.iptr(b),
+                                                   L.dptr(f)))
 
     def add_resistors(self, a, b, ohms):
         a, b = np.ascontiguousarray(a, np.int32), np.ascontiguousarray(b, np.int32)
@@ -170,4 +202,59 @@ class DcBatch:
     def __del__(self):
         if getattr(self, "_h", None) and L._lib is not None:
             L._lib.nsg_dc_batch_free(self._h)
+            self._h = None
+
+
+class TranBatch:
+    """Batched transient analysis of finalized circuits (one CTA each).
+
+    ``probes`` are unknown indices (node voltages first, then branch
+    currents) recorded at t = 0 and every accepted timepoint, at most
+    ``max_points`` per circuit."""
+
+    def __init__(self, circuits, tstep, tstop, probes, max_points=4096, threads=0):
+        self.circuits = list(circuits)
+        self.probes = np.ascontiguousarray(probes, np.int32)
+        self.max_points = int(max_points)
+        arr = (ctypes.c_void_p * len(self.circuits))(*[c.handle for c in self.circuits])
+        h = ctypes.c_void_p()
+        L.check(L.lib().nsg_tran_batch_create(len(self.circuits), arr, float(tstep), float(tstop),
+                                              self.max_points, len(self.probes),
+                                              L.iptr(self.probes), int(threads), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def count(self):
+        return len(self.circuits)
+
+    def run(self, stream=None):
+        import torch
+        sp = torch.cuda.current_stream().cuda_stream if stream is None else \
+            getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().nsg_tran_batch_run(self._h, sp))
+
+    def results(self):
+        """Per circuit: dict(time, values [points x probes], status, steps,
+        rejected, newton_iters)."""
+        c, m, k = self.count, self.max_points, len(self.probes)
+        t = np.zeros(c * m)
+        v = np.zeros(c * m * k)
+        npts = np.zeros(c, np.int32)
+        st = np.zeros(c, np.int32)
+        stats = np.zeros(4 * c, np.int32)
+        L.check(L.lib().nsg_tran_batch_results(self._h, L.dptr(t), L.dptr(v), L.iptr(npts),
+                                               L.iptr(st), L.iptr(stats)))
+        out = []
+        for i in range(c):
+            p = int(npts[i])
+            out.append(dict(time=t[i * m:i * m + p].copy(),
+                            values=v[i * m * k:(i * m + p) * k].reshape(p, k).copy(),
+                            status=int(st[i]), steps=int(stats[4 * i]),
+                            rejected=int(stats[4 * i + 1]), newton_iters=int(stats[4 * i + 2]),
+                            dc_code=int(stats[4 * i + 3])))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and L._lib is not None:
+            L._lib.nsg_tran_batch_free(self._h)
             self._h = None

@@ -22,11 +22,6 @@ size_t dc_smem_bytes(int max_col, int max_n);
 
 using namespace nsg_internal;
 
-struct nsg_circuit {
-    explicit nsg_circuit(int nodes) : c(nodes) {}
-    nsg::Circuit c;
-};
-
 struct nsg_dc_batch {
     int count = 0;
     std::vector<std::unique_ptr<nsg_topology>> topos;  // distinct symbolic results
@@ -91,6 +86,52 @@ void parallel_for(int count, int threads, F&& f) {
 
 }  // namespace
 
+namespace nsg_internal {
+
+// Program arrays and workspace of one instance (everything but index, plan,
+// parameter and solution offsets).
+void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPlan& p,
+                   std::vector<int32_t>& prog, int64_t& work) {
+    d.n = c.num_vars();
+    d.num_nodes = c.num_nodes();
+    d.nnz = c.nnz();
+    d.n_const = c.n_const_terms();
+    d.n_diodes = static_cast<int32_t>(c.diodes().size());
+    d.n_caps = static_cast<int32_t>(c.caps().size());
+    d.n_srcs = static_cast<int32_t>(c.wave_sources().size());
+    d.n_states = c.num_states();
+    d.prog_off[nsg::DP_slot_ptr] = append(prog, c.slot_ptr());
+    d.prog_off[nsg::DP_slot_terms] = append(prog, c.slot_terms());
+    d.prog_off[nsg::DP_rhs_ptr] = append(prog, c.rhs_ptr());
+    d.prog_off[nsg::DP_rhs_terms] = append(prog, c.rhs_terms());
+    d.prog_off[nsg::DP_ucb_ptr] = append(prog, c.ucb_ptr());
+    d.prog_off[nsg::DP_ucb_terms] = append(prog, c.ucb_terms());
+    d.prog_off[nsg::DP_term_op] = append(prog, c.term_op());
+    d.prog_off[nsg::DP_term_param] = append(prog, c.term_param());
+    std::vector<int32_t> tab;
+    for (const auto& dr : c.diodes()) tab.insert(tab.end(), {dr.pos, dr.neg, dr.param});
+    d.prog_off[nsg::DP_diodes] = append(prog, tab);
+    tab.clear();
+    for (const auto& cr : c.caps()) tab.insert(tab.end(), {cr.pos, cr.neg, cr.param, cr.has_ic, cr.state});
+    d.prog_off[nsg::DP_caps] = append(prog, tab);
+    tab.clear();
+    for (const auto& sr : c.wave_sources()) tab.insert(tab.end(), {sr.is_voltage, sr.wave, sr.param, sr.nparam});
+    d.prog_off[nsg::DP_srcs] = append(prog, tab);
+    d.x_off = work; work = align4(work + d.n);
+    d.xold_off = work; work = align4(work + d.n);
+    d.w_off = work; work = align4(work + d.n);
+    d.a_off = work; work = align4(work + d.nnz);
+    d.lu_off = work; work = align4(work + p.nnz_lu);
+    d.lrows_off = work; work = align4(work + p.lrow_ptr[p.n]);
+    d.urows_off = work; work = align4(work + p.urow_ptr[p.n]);
+    d.tv_off = work; work = align4(work + c.n_terms());
+    d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
+    d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
+    d.state_off = work; work = align4(work + 4 * static_cast<int64_t>(d.n_states));
+}
+
+}  // namespace nsg_internal
+
 extern "C" {
 
 int nsg_circuit_create(int num_nodes, nsg_circuit** out) {
@@ -131,6 +172,38 @@ int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, dou
     return guarded("nsg_circuit_add_diode", [&]() -> int {
         if (!c) return fail(NSG_ERR_INVALID, "null circuit");
         c->c.add_diode(anode, cathode, is, n_emission);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_capacitor(nsg_circuit* c, int a, int b, double farads, int has_ic,
+                              double ic) {
+    return guarded("nsg_circuit_add_capacitor", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_capacitor(a, b, farads, has_ic != 0, ic);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_source_wave(nsg_circuit* c, int is_voltage, int p, int n, int wave,
+                                int nvalues, const double* values) {
+    return guarded("nsg_circuit_add_source_wave", [&]() -> int {
+        if (!c || nvalues < 0 || (nvalues && !values))
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        if (wave != NSG_WAVE_DC && wave != NSG_WAVE_PULSE && wave != NSG_WAVE_PWL)
+            return fail(NSG_ERR_INVALID, "nsg_circuit_add_source_wave: unknown waveform");
+        c->c.add_source_wave(is_voltage != 0, p, n, static_cast<nsg::Wave>(wave),
+                             std::vector<double>(values, values + nvalues));
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_capacitors(nsg_circuit* c, int count, const int* a, const int* b,
+                               const double* farads) {
+    return guarded("nsg_circuit_add_capacitors", [&]() -> int {
+        if (!c || count < 0 || (count && (!a || !b || !farads)))
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        for (int i = 0; i < count; ++i) c->c.add_capacitor(a[i], b[i], farads[i], false, 0.0);
         return NSG_OK;
     });
 }
@@ -285,43 +358,14 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             const auto& c = circuits[i]->c;
             const auto& p = b->topos[topo_of[i]]->plan;
             nsg::DcDesc& d = descs[i];
+            fill_instance(d, c, p, prog, work);
             d.index = i;
             d.plan = topo_of[i];
-            d.n = c.num_vars();
-            d.num_nodes = c.num_nodes();
-            d.nnz = c.nnz();
-            d.n_const = c.n_const_terms();
-            d.n_diodes = static_cast<int32_t>(c.diodes().size());
-            d.prog_off[nsg::DP_slot_ptr] = append(prog, c.slot_ptr());
-            d.prog_off[nsg::DP_slot_terms] = append(prog, c.slot_terms());
-            d.prog_off[nsg::DP_rhs_ptr] = append(prog, c.rhs_ptr());
-            d.prog_off[nsg::DP_rhs_terms] = append(prog, c.rhs_terms());
-            d.prog_off[nsg::DP_ucb_ptr] = append(prog, c.ucb_ptr());
-            d.prog_off[nsg::DP_ucb_terms] = append(prog, c.ucb_terms());
-            d.prog_off[nsg::DP_term_op] = append(prog, c.term_op());
-            d.prog_off[nsg::DP_term_param] = append(prog, c.term_param());
-            std::vector<int32_t> dio;
-            for (const auto& dr : c.diodes()) {
-                dio.push_back(dr.pos);
-                dio.push_back(dr.neg);
-                dio.push_back(dr.param);
-            }
-            d.prog_off[nsg::DP_diodes] = append(prog, dio);
             d.param_off = b->param_off[i];
             d.sol_off = b->sol_off[i];
             b->param_off[i + 1] = b->param_off[i] + static_cast<int64_t>(c.params().size());
             b->sol_off[i + 1] = b->sol_off[i] + c.num_vars();
             b->host_params.insert(b->host_params.end(), c.params().begin(), c.params().end());
-            d.x_off = work; work = align4(work + d.n);
-            d.xold_off = work; work = align4(work + d.n);
-            d.w_off = work; work = align4(work + d.n);
-            d.a_off = work; work = align4(work + d.nnz);
-            d.lu_off = work; work = align4(work + p.nnz_lu);
-            d.lrows_off = work; work = align4(work + p.lrow_ptr[p.n]);
-            d.urows_off = work; work = align4(work + p.urow_ptr[p.n]);
-            d.tv_off = work; work = align4(work + c.n_terms());
-            d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
-            d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
             b->inst_n.push_back(p.n);
             b->inst_nnz.push_back(p.nnz_a);
             b->inst_nnz_lu.push_back(p.nnz_lu);

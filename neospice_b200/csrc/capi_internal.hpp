@@ -2,6 +2,7 @@
 #pragma once
 #include "nsgpu.h"
 
+#include "host/circuit.hpp"
 #include "host/plan.hpp"
 #include "host/sparse_order.hpp"
 #include "kernels/lu_device.cuh"
@@ -19,6 +20,11 @@ struct nsg_topology {
     std::unique_ptr<nsg::MarkowitzOrder> engine;  // null for an imported topology
     std::vector<int32_t> slot_elem;
     nsg::TopologyPlan plan;
+};
+
+struct nsg_circuit {
+    explicit nsg_circuit(int nodes) : c(nodes) {}
+    nsg::Circuit c;
 };
 
 struct nsg_batch {
@@ -84,4 +90,10 @@ int order_topology(int n, int nnz, const int* col_ptr, const int* row_idx, const
 // PlanDesc for a plan whose arrays were appended to pool.
 nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& pool);
 
+}  // namespace nsg_internal
+
+namespace nsg { struct DcDesc; }
+namespace nsg_internal {
+void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPlan& p,
+                   std::vector<int32_t>& prog, int64_t& work);
 }  // namespace nsg_internal

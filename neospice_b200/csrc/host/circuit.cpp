@@ -1,8 +1,10 @@
 #include "circuit.hpp"
 
 #include "kernels/diode_model.cuh"
+#include "kernels/source_wave.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -19,49 +21,61 @@ void Circuit::check_node(int32_t v) const {
         throw std::out_of_range("Circuit: node " + std::to_string(v) + " out of range");
 }
 
-int32_t Circuit::add_resistor(int32_t a, int32_t b, double ohms) {
+int32_t Circuit::add_device(DevKind kind, int32_t a, int32_t b, const std::vector<double>& p,
+                            Wave wave, bool has_ic) {
     check_node(a);
     check_node(b);
+    DeviceRec d;
+    d.kind = kind;
+    d.created = static_cast<int32_t>(devices_.size());
+    d.a = a;
+    d.b = b;
+    d.param = static_cast<int32_t>(params_.size());
+    d.nparam = static_cast<int32_t>(p.size());
+    d.branch = -1;
+    d.wave = wave;
+    d.has_ic = has_ic;
+    devices_.push_back(d);
+    params_.insert(params_.end(), p.begin(), p.end());
+    return d.created;
+}
+
+int32_t Circuit::add_resistor(int32_t a, int32_t b, double ohms) {
     if (!(ohms != 0.0)) throw std::invalid_argument("Circuit: zero resistance");
-    devices_.push_back({DevKind::Resistor, static_cast<int32_t>(devices_.size()), a, b,
-                        static_cast<int32_t>(params_.size()), -1});
-    params_.push_back(ohms);
-    return devices_.back().created;
+    return add_device(DevKind::Resistor, a, b, {ohms});
+}
+
+int32_t Circuit::add_capacitor(int32_t a, int32_t b, double farads, bool has_ic, double ic) {
+    return add_device(DevKind::Capacitor, a, b, {farads, has_ic ? ic : 0.0}, Wave::DC, has_ic);
 }
 
 int32_t Circuit::add_vsource(int32_t p, int32_t n, double volts) {
-    check_node(p);
-    check_node(n);
-    devices_.push_back({DevKind::VSource, static_cast<int32_t>(devices_.size()), p, n,
-                        static_cast<int32_t>(params_.size()), -1});
-    params_.push_back(volts);
-    return devices_.back().created;
+    return add_device(DevKind::VSource, p, n, {volts});
 }
 
 int32_t Circuit::add_isource(int32_t p, int32_t n, double amps) {
-    check_node(p);
-    check_node(n);
-    devices_.push_back({DevKind::ISource, static_cast<int32_t>(devices_.size()), p, n,
-                        static_cast<int32_t>(params_.size()), -1});
-    params_.push_back(amps);
-    return devices_.back().created;
+    return add_device(DevKind::ISource, p, n, {amps});
+}
+
+int32_t Circuit::add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wave,
+                                 const std::vector<double>& values) {
+    if (wave == Wave::Pulse && values.size() != 7)
+        throw std::invalid_argument("Circuit: PULSE takes v1 v2 td tr tf pw per");
+    if (wave == Wave::Pwl && (values.size() < 2 || values.size() % 2))
+        throw std::invalid_argument("Circuit: PWL takes (time, value) pairs");
+    if (wave == Wave::DC && values.size() != 1)
+        throw std::invalid_argument("Circuit: DC source takes one value");
+    return add_device(is_voltage ? DevKind::VSource : DevKind::ISource, p, n, values, wave);
 }
 
 int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_emission) {
-    check_node(anode);
-    check_node(cathode);
     if (!(is > 0.0) || !(n_emission > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
-    devices_.push_back({DevKind::Diode, static_cast<int32_t>(devices_.size()), anode, cathode,
-                        static_cast<int32_t>(params_.size()), -1});
-    params_.push_back(is);
-    params_.push_back(n_emission);
-    return devices_.back().created;
+    return add_device(DevKind::Diode, anode, cathode, {is, n_emission});
 }
 
 int32_t Circuit::offset(int32_t r, int32_t c) const {
     if (r < 0 || c < 0) return -1;
-    // binary search in column c
     const auto b = row_idx_.begin() + col_ptr_[c];
     const auto e = row_idx_.begin() + col_ptr_[c + 1];
     const auto it = std::lower_bound(b, e, r);
@@ -96,14 +110,14 @@ void Circuit::finalize() {
     for (const auto& d : order) {
         switch (d.kind) {
             case DevKind::Resistor:
+            case DevKind::Capacitor:
                 stamp(d.a, d.a); stamp(d.a, d.b); stamp(d.b, d.a); stamp(d.b, d.b);
                 break;
             case DevKind::VSource:
                 stamp(d.a, d.branch); stamp(d.b, d.branch); stamp(d.branch, d.a); stamp(d.branch, d.b);
                 break;
             case DevKind::Diode:  // pos == posPrime (RS = 0)
-                stamp(d.a, d.a); stamp(d.b, d.a); stamp(d.a, d.a); stamp(d.a, d.b);
-                stamp(d.a, d.a); stamp(d.b, d.b); stamp(d.a, d.a);
+                stamp(d.a, d.a); stamp(d.b, d.a); stamp(d.a, d.b); stamp(d.b, d.b);
                 break;
             case DevKind::ISource:
                 break;
@@ -131,7 +145,32 @@ void Circuit::finalize() {
             throw std::invalid_argument("Circuit: unknown " + std::to_string(j) +
                                         " has an empty column (floating branch?)");
 
-    // Stamp program: replay each device's evaluate() in load order.
+    // Device tables in load order (state slots assigned in load order, as
+    // Circuit::rebind_device_states does).
+    diodes_.clear();
+    caps_.clear();
+    wsrc_.clear();
+    std::vector<int32_t> index_in_table(order.size(), -1);
+    int32_t state = 0;
+    for (size_t k = 0; k < order.size(); ++k) {
+        const auto& d = order[k];
+        if (d.kind == DevKind::Diode) {
+            index_in_table[k] = static_cast<int32_t>(diodes_.size());
+            diodes_.push_back({d.a, d.b, d.param});
+        } else if (d.kind == DevKind::Capacitor) {
+            index_in_table[k] = static_cast<int32_t>(caps_.size());
+            caps_.push_back({d.a, d.b, d.param, d.has_ic ? 1 : 0, state});
+            state += 2;
+        } else if ((d.kind == DevKind::VSource || d.kind == DevKind::ISource) && d.wave != Wave::DC) {
+            index_in_table[k] = static_cast<int32_t>(wsrc_.size());
+            wsrc_.push_back({d.kind == DevKind::VSource ? 1 : 0, static_cast<int32_t>(d.wave),
+                             d.param, d.nparam});
+        }
+    }
+
+    // Stamp program: replay each device's evaluate() in load order.  Dynamic
+    // terms are recorded as -1 - (block offset) and renumbered once the
+    // constant count is known.
     const int32_t nnz = static_cast<int32_t>(row_idx_.size());
     std::vector<std::vector<int32_t>> slot(nnz), rhs(num_vars_), ucb(num_vars_);
     term_op_.clear();
@@ -141,40 +180,52 @@ void Circuit::finalize() {
         term_param_.push_back(param);
         return static_cast<int32_t>(term_op_.size()) - 1;
     };
-    // Dynamic (per-iteration) terms are recorded as -1 - (diode * kDiodeTerms
-    // + which) and renumbered after the constants once their count is known.
-    auto dyn_term = [](int32_t diode, int32_t which) { return -1 - (diode * kDiodeTerms + which); };
+    const int32_t nd = static_cast<int32_t>(diodes_.size());
+    const int32_t nc = static_cast<int32_t>(caps_.size());
+    auto diode_term = [&](int32_t id, int32_t w) { return -1 - (id * kDiodeTerms + w); };
+    auto cap_term = [&](int32_t id, int32_t w) { return -1 - (nd * kDiodeTerms + id * kCapTerms + w); };
+    auto src_term = [&](int32_t id, int32_t w) {
+        return -1 - (nd * kDiodeTerms + nc * kCapTerms + id * kSrcTerms + w);
+    };
     auto add_slot = [&](int32_t r, int32_t c, int32_t term) {
         const int32_t off = offset(r, c);
         if (off >= 0) slot[off].push_back(term);
     };
-    diodes_.clear();
-    for (const auto& d : order) {
+    for (size_t k = 0; k < order.size(); ++k) {
+        const auto& d = order[k];
+        const int32_t id = index_in_table[k];
         switch (d.kind) {
+            case DevKind::Capacitor:
+                add_slot(d.a, d.a, cap_term(id, kCGeq));
+                add_slot(d.a, d.b, cap_term(id, kCNegGeq));
+                add_slot(d.b, d.a, cap_term(id, kCNegGeq));
+                add_slot(d.b, d.b, cap_term(id, kCGeq));
+                if (d.a >= 0) rhs[d.a].push_back(cap_term(id, kCNegCeq));
+                if (d.b >= 0) rhs[d.b].push_back(cap_term(id, kCCeq));
+                break;
             case DevKind::Diode: {
-                const int32_t id = static_cast<int32_t>(diodes_.size());
-                diodes_.push_back({d.a, d.b, d.param});
                 // rhs (UCB array): neg += cdeq, posPrime -= cdeq
-                if (d.b >= 0) ucb[d.b].push_back(dyn_term(id, kDCdeq));
-                if (d.a >= 0) ucb[d.a].push_back(dyn_term(id, kDNegCdeq));
+                if (d.b >= 0) ucb[d.b].push_back(diode_term(id, kDCdeq));
+                if (d.a >= 0) ucb[d.a].push_back(diode_term(id, kDNegCdeq));
                 // matrix, in DIOload's order
                 const int32_t zero = konst(kTermZero, -1), mzero = konst(kTermMinusZero, -1);
-                auto dslot = [&](int32_t r, int32_t c, int32_t which) {
-                    const int32_t off = offset(r, c);
-                    if (off >= 0) slot[off].push_back(dyn_term(id, which));
-                };
-                add_slot(d.a, d.a, zero);                 // PosPos += gspr
-                dslot(d.b, d.b, kDGd);                    // NegNeg += gd
-                dslot(d.a, d.a, kDGdPlusGspr);            // PosPrimePosPrime += gd + gspr
-                add_slot(d.a, d.a, mzero);                // PosPosPrime -= gspr
-                dslot(d.b, d.a, kDNegGd);                 // NegPosPrime -= gd
-                add_slot(d.a, d.a, mzero);                // PosPrimePos -= gspr
-                dslot(d.a, d.b, kDNegGd);                 // PosPrimeNeg -= gd
+                add_slot(d.a, d.a, zero);                          // PosPos += gspr
+                add_slot(d.b, d.b, diode_term(id, kDGd));          // NegNeg += gd
+                add_slot(d.a, d.a, diode_term(id, kDGdPlusGspr));  // PosPrimePosPrime += gd + gspr
+                add_slot(d.a, d.a, mzero);                         // PosPosPrime -= gspr
+                add_slot(d.b, d.a, diode_term(id, kDNegGd));       // NegPosPrime -= gd
+                add_slot(d.a, d.a, mzero);                         // PosPrimePos -= gspr
+                add_slot(d.a, d.b, diode_term(id, kDNegGd));       // PosPrimeNeg -= gd
                 break;
             }
             case DevKind::ISource:
-                if (d.a >= 0) rhs[d.a].push_back(konst(kTermNegValue, d.param));
-                if (d.b >= 0) rhs[d.b].push_back(konst(kTermValue, d.param));
+                if (d.wave == Wave::DC) {
+                    if (d.a >= 0) rhs[d.a].push_back(konst(kTermNegValue, d.param));
+                    if (d.b >= 0) rhs[d.b].push_back(konst(kTermValue, d.param));
+                } else {
+                    if (d.a >= 0) rhs[d.a].push_back(src_term(id, kSNegVal));
+                    if (d.b >= 0) rhs[d.b].push_back(src_term(id, kSVal));
+                }
                 break;
             case DevKind::Resistor: {
                 const int32_t g = konst(kTermRecip, d.param), mg = konst(kTermNegRecip, d.param);
@@ -190,7 +241,8 @@ void Circuit::finalize() {
                 add_slot(d.b, d.branch, mone);
                 add_slot(d.branch, d.a, one);
                 add_slot(d.branch, d.b, mone);
-                rhs[d.branch].push_back(konst(kTermValue, d.param));
+                rhs[d.branch].push_back(d.wave == Wave::DC ? konst(kTermValue, d.param)
+                                                           : src_term(id, kSVal));
                 break;
             }
         }
@@ -214,9 +266,48 @@ void Circuit::finalize() {
     finalized_ = true;
 }
 
-void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, double gmin) const {
-    if (!finalized_) throw std::logic_error("Circuit: not finalized");
-    std::vector<double> tv(n_terms(), 0.0);
+std::vector<double> Circuit::resolved_params(double tstep, double tstop) const {
+    std::vector<double> out = params_;
+    for (const auto& d : devices_) {
+        if ((d.kind != DevKind::VSource && d.kind != DevKind::ISource) || d.wave != Wave::Pulse)
+            continue;
+        double* p = &out[d.param];  // v1 v2 td tr tf pw per
+        if (p[3] <= 0) p[3] = tstep;
+        if (p[4] <= 0) p[4] = tstep;
+        if (p[5] <= 0) p[5] = tstop;
+        if (p[6] <= 0) p[6] = tstop;
+    }
+    return out;
+}
+
+std::vector<double> Circuit::source_breakpoints(const std::vector<double>& params,
+                                                double tstop) const {
+    const double tstart = 0.0;
+    std::vector<double> bps;
+    for (const auto& d : devices_) {  // the reference walks devices in creation order
+        if (d.kind != DevKind::VSource && d.kind != DevKind::ISource) continue;
+        const double* p = &params[d.param];
+        if (d.wave == Wave::Pwl) {
+            for (int32_t k = 0; k + 1 < d.nparam; k += 2)
+                if (p[k] > tstart && p[k] <= tstop) bps.push_back(p[k]);
+        } else if (d.wave == Wave::Pulse) {
+            const double td = p[2], tr = p[3], tf = p[4], pw = p[5], per = p[6];
+            if (per <= 0.0) continue;
+            const int max_periods = static_cast<int>((tstop - td) / per) + 2;
+            for (int k = 0; k < max_periods; ++k) {
+                const double t0 = td + k * per;
+                if (t0 > tstop) break;
+                const double edges[] = {t0, t0 + tr, t0 + tr + pw, t0 + tr + pw + tf};
+                for (double e : edges)
+                    if (e > tstart && e <= tstop) bps.push_back(e);
+            }
+        }
+    }
+    return bps;
+}
+
+void Circuit::const_term_values(std::vector<double>& tv, double gmin) const {
+    tv.assign(n_terms(), 0.0);
     for (int32_t k = 0; k < n_const_terms(); ++k) {
         const double p = term_param_[k] >= 0 ? params_[term_param_[k]] : 0.0;
         switch (term_op_[k]) {
@@ -231,12 +322,39 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
             case kTermGmin: tv[k] = gmin; break;
         }
     }
+}
+
+void Circuit::sum_program(const std::vector<double>& tv, std::vector<double>* a,
+                          std::vector<double>* rhs) const {
+    if (a) {
+        a->assign(nnz(), 0.0);
+        for (int32_t s = 0; s < nnz(); ++s) {
+            double v = 0.0;
+            for (int32_t k = slot_ptr_[s]; k < slot_ptr_[s + 1]; ++k) v += tv[slot_terms_[k]];
+            (*a)[s] = v;
+        }
+    }
+    if (rhs) {
+        rhs->assign(num_vars_, 0.0);
+        for (int32_t i = 0; i < num_vars_; ++i) {
+            double v = 0.0, u = 0.0;
+            for (int32_t k = rhs_ptr_[i]; k < rhs_ptr_[i + 1]; ++k) v += tv[rhs_terms_[k]];
+            for (int32_t k = ucb_ptr_[i]; k < ucb_ptr_[i + 1]; ++k) u += tv[ucb_terms_[k]];
+            (*rhs)[i] = v + u;
+        }
+    }
+}
+
+void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, double gmin) const {
+    if (!finalized_) throw std::logic_error("Circuit: not finalized");
+    std::vector<double> tv;
+    const_term_values(tv, gmin);
     const double vt = kKoverQ * kTNominal;
     for (size_t d = 0; d < diodes_.size(); ++d) {
         const double csat = params_[diodes_[d].param];
         const double vte = params_[diodes_[d].param + 1] * vt;
         const DiodeDC r = diode_dc_load(true, 0.0, 0.0, 0.0, csat, vte, diode_vcrit(vte, csat), gmin);
-        double* t = &tv[n_const_terms() + kDiodeTerms * d];
+        double* t = &tv[diode_term_base() + kDiodeTerms * d];
         const double cdeq = r.cd - r.gd * r.vd;
         t[kDGd] = r.gd;
         t[kDGdPlusGspr] = r.gd + 0.0;
@@ -244,19 +362,28 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
         t[kDCdeq] = cdeq;
         t[kDNegCdeq] = -cdeq;
     }
-    a.assign(nnz(), 0.0);
-    for (int32_t s = 0; s < nnz(); ++s) {
-        double v = 0.0;
-        for (int32_t k = slot_ptr_[s]; k < slot_ptr_[s + 1]; ++k) v += tv[slot_terms_[k]];
-        a[s] = v;
+    // Waveform sources at t = 0.
+    for (size_t s = 0; s < wsrc_.size(); ++s) {
+        const double v = wave_value(wsrc_[s].wave, &params_[wsrc_[s].param], wsrc_[s].nparam, 0.0);
+        tv[src_term_base() + kSrcTerms * s + kSVal] = v;
+        tv[src_term_base() + kSrcTerms * s + kSNegVal] = -v;
     }
-    rhs.assign(num_vars_, 0.0);
-    for (int32_t i = 0; i < num_vars_; ++i) {
-        double v = 0.0, u = 0.0;
-        for (int32_t k = rhs_ptr_[i]; k < rhs_ptr_[i + 1]; ++k) v += tv[rhs_terms_[k]];
-        for (int32_t k = ucb_ptr_[i]; k < ucb_ptr_[i + 1]; ++k) u += tv[ucb_terms_[k]];
-        rhs[i] = v + u;
+    sum_program(tv, &a, &rhs);
+}
+
+void Circuit::first_transient_matrix(std::vector<double>& a, double dt0, double gmin) const {
+    if (!finalized_) throw std::logic_error("Circuit: not finalized");
+    if (!diodes_.empty())
+        throw std::logic_error("Circuit: first_transient_matrix needs a linear circuit");
+    std::vector<double> tv;
+    const_term_values(tv, gmin);
+    const double ag0 = 1.0 / dt0;  // fill_integrator_context, order 1
+    for (size_t c = 0; c < caps_.size(); ++c) {
+        const double geq = ag0 * params_[caps_[c].param];
+        tv[cap_term_base() + kCapTerms * c + kCGeq] = geq;
+        tv[cap_term_base() + kCapTerms * c + kCNegGeq] = -geq;
     }
+    sum_program(tv, &a, nullptr);
 }
 
 }  // namespace nsg

@@ -15,13 +15,16 @@
 namespace nsg {
 
 // ngspice load rank of each device family (src/core/circuit.cpp:34-59).
-enum class DevKind : int32_t { Diode = 22, ISource = 31, Resistor = 41, VSource = 50 };
+enum class DevKind : int32_t { Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50 };
+
+// Independent-source waveforms (src/devices/vsource.cpp:80-131).
+enum class Wave : int32_t { DC = 0, Pulse = 1, Pwl = 2 };
 
 // How a constant term value is made from the instance's parameters.
 enum TermOp : int32_t {
     kTermRecip = 0,     // +1/p           (resistor conductance)
     kTermNegRecip = 1,  // -(1/p)
-    kTermValue = 2,     // +p             (source value)
+    kTermValue = 2,     // +p             (DC source value)
     kTermNegValue = 3,  // -p
     kTermOne = 4,       // +1.0
     kTermMinusOne = 5,  // -1.0
@@ -30,18 +33,25 @@ enum TermOp : int32_t {
     kTermGmin = 8,      // the dead-node pin conductance (SimOptions::gmin)
 };
 
-// Values each diode writes per Newton iteration, in this order, after the
-// constant terms (DIOload's right-hand side and matrix loads,
-// src/devices/dio/dio_load.cpp:392-406, for RS = 0 so gspr = 0).
+// Dynamic terms, recomputed every Newton iteration, follow the constants in
+// this order: diodes, capacitors, waveform sources.
+// Per diode (DIOload's loads, src/devices/dio/dio_load.cpp:392-406, RS = 0):
 enum DiodeTerm : int32_t { kDGd = 0, kDGdPlusGspr = 1, kDNegGd = 2, kDCdeq = 3, kDNegCdeq = 4,
                            kDiodeTerms = 5 };
+// Per capacitor (Capacitor::evaluate, src/devices/capacitor.cpp:28-100):
+enum CapTerm : int32_t { kCGeq = 0, kCNegGeq = 1, kCNegCeq = 2, kCCeq = 3, kCapTerms = 4 };
+// Per waveform source: the value and its negation at the current time.
+enum SrcTerm : int32_t { kSVal = 0, kSNegVal = 1, kSrcTerms = 2 };
 
 struct DeviceRec {
     DevKind kind;
     int32_t created;   // creation index over all devices
     int32_t a, b;      // terminals (0-based node, -1 = ground)
     int32_t param;     // first parameter index
+    int32_t nparam;    // parameter count
     int32_t branch;    // VSource branch unknown, else -1
+    Wave wave;         // sources
+    bool has_ic;       // capacitors
 };
 
 class Circuit {
@@ -49,10 +59,16 @@ public:
     explicit Circuit(int32_t num_nodes);
 
     // Parameters of every device are kept in creation order in params():
-    // resistor {ohms}, vsource {volts}, isource {amps}, diode {IS, N}.
+    // resistor {ohms}; capacitor {farads, ic}; DC source {value}; PULSE
+    // source {v1, v2, td, tr, tf, pw, per}; PWL source {t0, v0, t1, v1, ...};
+    // diode {IS, N}.
     int32_t add_resistor(int32_t a, int32_t b, double ohms);
+    int32_t add_capacitor(int32_t a, int32_t b, double farads, bool has_ic, double ic);
     int32_t add_vsource(int32_t p, int32_t n, double volts);
     int32_t add_isource(int32_t p, int32_t n, double amps);
+    // Waveform sources: is_voltage selects V or I; values per Wave above.
+    int32_t add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wave,
+                            const std::vector<double>& values);
     int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission);
 
     void finalize();
@@ -64,17 +80,28 @@ public:
     const std::vector<int32_t>& col_ptr() const { return col_ptr_; }
     const std::vector<int32_t>& row_idx() const { return row_idx_; }
     const std::vector<double>& params() const { return params_; }
+    std::vector<double>& params_mut() { return params_; }
     const std::vector<int32_t>& dead_nodes() const { return dead_nodes_; }
 
-    // Diodes in load order: anode, cathode (-1 = ground), parameter index.
+    // Devices with per-iteration evaluation, in load order.
     struct DiodeRec { int32_t pos, neg, param; };
+    struct CapRec { int32_t pos, neg, param, has_ic, state; };  // state: base of {q, i}
+    struct SrcRec { int32_t is_voltage, wave, param, nparam; };
     const std::vector<DiodeRec>& diodes() const { return diodes_; }
+    const std::vector<CapRec>& caps() const { return caps_; }
+    const std::vector<SrcRec>& wave_sources() const { return wsrc_; }
+    int32_t num_states() const { return 2 * static_cast<int32_t>(caps_.size()); }
 
     // Stamp program (valid after finalize).
-    // Constant terms: term_op/term_param, count n_const_terms().  Dynamic
-    // terms follow: kDiodeTerms per diode in load order.
     int32_t n_const_terms() const { return static_cast<int32_t>(term_op_.size()); }
-    int32_t n_terms() const { return n_const_terms() + kDiodeTerms * static_cast<int32_t>(diodes_.size()); }
+    int32_t diode_term_base() const { return n_const_terms(); }
+    int32_t cap_term_base() const {
+        return diode_term_base() + kDiodeTerms * static_cast<int32_t>(diodes_.size());
+    }
+    int32_t src_term_base() const {
+        return cap_term_base() + kCapTerms * static_cast<int32_t>(caps_.size());
+    }
+    int32_t n_terms() const { return src_term_base() + kSrcTerms * static_cast<int32_t>(wsrc_.size()); }
     const std::vector<int32_t>& term_op() const { return term_op_; }
     const std::vector<int32_t>& term_param() const { return term_param_; }
     // Per matrix slot / rhs row: ptr (size+1) and term indices, in add order.
@@ -85,11 +112,21 @@ public:
     const std::vector<int32_t>& ucb_ptr() const { return ucb_ptr_; }     // UCB-style devices
     const std::vector<int32_t>& ucb_terms() const { return ucb_terms_; }
 
+    // Source breakpoints in (0, tstop] after resolving PULSE defaults with
+    // (tstep, tstop) (VSource::resolve_defaults / get_breakpoints,
+    // src/devices/vsource.cpp:51-78, 233-264), in device order.
+    std::vector<double> resolved_params(double tstep, double tstop) const;
+    std::vector<double> source_breakpoints(const std::vector<double>& params, double tstop) const;
+
     // Host evaluation of the matrix and rhs at the first Newton iteration of
     // a DC operating point (MODEDCOP | MODEINITJCT, zero initial guess), with
     // host libm -- the values the reference's first NeoSolver::numeric sees.
     void initjct_values(std::vector<double>& a, std::vector<double>& rhs,
                         double gmin) const;
+    // Matrix of the first transient iteration of a circuit without nonlinear
+    // devices: constants plus each capacitor's ag0*C (backward Euler, step
+    // dt0), the matrix the transient solver first orders on.
+    void first_transient_matrix(std::vector<double>& a, double dt0, double gmin) const;
 
 private:
     int32_t num_nodes_;
@@ -99,11 +136,18 @@ private:
     std::vector<double> params_;
     std::vector<int32_t> col_ptr_, row_idx_, dead_nodes_;
     std::vector<DiodeRec> diodes_;
+    std::vector<CapRec> caps_;
+    std::vector<SrcRec> wsrc_;
     std::vector<int32_t> term_op_, term_param_;
     std::vector<int32_t> slot_ptr_, slot_terms_, rhs_ptr_, rhs_terms_, ucb_ptr_, ucb_terms_;
 
     void check_node(int32_t v) const;
+    int32_t add_device(DevKind kind, int32_t a, int32_t b, const std::vector<double>& p,
+                       Wave wave = Wave::DC, bool has_ic = false);
     int32_t offset(int32_t r, int32_t c) const;  // -1 when ground or absent
+    void const_term_values(std::vector<double>& tv, double gmin) const;
+    void sum_program(const std::vector<double>& tv, std::vector<double>* a,
+                     std::vector<double>* rhs) const;
 };
 
 // Physical constants as the reference's diode shim defines them

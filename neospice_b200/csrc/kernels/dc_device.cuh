@@ -9,7 +9,7 @@ namespace nsg {
 // Stamp-program arrays of one circuit in the program pool.
 enum DcProgArray : int {
     DP_slot_ptr, DP_slot_terms, DP_rhs_ptr, DP_rhs_terms, DP_ucb_ptr, DP_ucb_terms,
-    DP_term_op, DP_term_param, DP_diodes, DP_COUNT
+    DP_term_op, DP_term_param, DP_diodes, DP_caps, DP_srcs, DP_COUNT
 };
 
 struct DcDesc {
@@ -20,6 +20,9 @@ struct DcDesc {
     int32_t nnz;         // matrix slots
     int32_t n_const;     // constant terms
     int32_t n_diodes;
+    int32_t n_caps;
+    int32_t n_srcs;      // waveform sources
+    int32_t n_states;    // per state vector (2 per capacitor)
     int64_t prog_off[DP_COUNT];  // int32-word offsets into the program pool
     int64_t param_off;           // into the caller's parameter array
     int64_t sol_off;             // into the caller's solution array
@@ -27,6 +30,7 @@ struct DcDesc {
     // values, LU values, term values, diode state, diode constants
     int64_t x_off, xold_off, w_off, a_off, lu_off, tv_off, dstate_off, dconst_off;
     int64_t lrows_off, urows_off;  // row-major copies of L and U for the sweeps
+    int64_t state_off;             // four state vectors of n_states doubles
 };
 
 // SimOptions of the reference (src/core/types.hpp:24-66) used by the loop.
@@ -41,6 +45,8 @@ struct NewtonOptions {
 };
 
 constexpr int kDiodeTermCount = 5;
+constexpr int kCapTermCount = 4;
+constexpr int kSrcTermCount = 2;
 // CONSTKoverQ * 300.15 evaluated as the reference's diode temperature code does.
 constexpr double kKoverQTimesTnom = (1.38064852e-23 / 1.6021766208e-19) * 300.15;
 

@@ -1,0 +1,349 @@
+// Per-instance Newton machinery shared by the DC and transient kernels: one
+// CTA (kFlowThreads threads) owns one circuit instance.
+#pragma once
+#include "dc_device.cuh"
+#include "diode_model.cuh"
+#include "lu_cta.cuh"
+#include "source_wave.cuh"
+
+namespace nsg {
+
+// CKTmode bits (ngspice cktdefs.h, as used in src/core/newton.cpp:109-115,
+// src/devices/capacitor.cpp:37-44).
+constexpr int kModeTran = 0x1;
+constexpr int kModeAc = 0x2;
+constexpr int kModeDcOp = 0x10;
+constexpr int kModeTranOp = 0x20;
+constexpr int kModeDcMask = 0x70;
+constexpr int kModeInitFloat = 0x100;
+constexpr int kModeInitJct = 0x200;
+constexpr int kModeInitFix = 0x400;
+constexpr int kModeInitTran = 0x1000;
+constexpr int kModeInitPred = 0x2000;
+constexpr int kModeUic = 0x10000;
+constexpr int kModeInitMask = 0x3F00;
+
+// Integrator context of one instance (IntegratorCtx, src/core/types.hpp:73-94),
+// written by thread 0, read by every thread after a barrier.
+struct IntegCtx {
+    double ag[3];
+    double xmu_ratio;
+    double delta;
+    double delta_old[3];
+    double time;      // source time (update_source_time)
+    int mode;
+    int order;
+    int method;       // 0 trapezoidal, 1 Gear
+    int pad;
+};
+
+// Views of one instance's program and workspace.
+struct Inst {
+    const int32_t* slot_ptr;
+    const int32_t* slot_terms;
+    const int32_t* rhs_ptr;
+    const int32_t* rhs_terms;
+    const int32_t* ucb_ptr;
+    const int32_t* ucb_terms;
+    const int32_t* term_op;
+    const int32_t* term_param;
+    const int32_t* diodes;  // (pos, neg, param)
+    const int32_t* caps;    // (pos, neg, param, has_ic, state)
+    const int32_t* srcs;    // (is_voltage, wave, param, nparam)
+    const double* par;
+    double* x;
+    double* xold;
+    double* a;
+    double* lu;
+    double* lrows;
+    double* urows;
+    double* tv;
+    double* dstate;
+    double* dconst;
+    double* st[4];          // capacitor state ring state0..state3
+    int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs;
+};
+
+__device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const double* params,
+                                 double* work) {
+    Inst v;
+    v.slot_ptr = prog + d.prog_off[DP_slot_ptr];
+    v.slot_terms = prog + d.prog_off[DP_slot_terms];
+    v.rhs_ptr = prog + d.prog_off[DP_rhs_ptr];
+    v.rhs_terms = prog + d.prog_off[DP_rhs_terms];
+    v.ucb_ptr = prog + d.prog_off[DP_ucb_ptr];
+    v.ucb_terms = prog + d.prog_off[DP_ucb_terms];
+    v.term_op = prog + d.prog_off[DP_term_op];
+    v.term_param = prog + d.prog_off[DP_term_param];
+    v.diodes = prog + d.prog_off[DP_diodes];
+    v.caps = prog + d.prog_off[DP_caps];
+    v.srcs = prog + d.prog_off[DP_srcs];
+    v.par = params + d.param_off;
+    v.x = work + d.x_off;
+    v.xold = work + d.xold_off;
+    v.a = work + d.a_off;
+    v.lu = work + d.lu_off;
+    v.lrows = work + d.lrows_off;
+    v.urows = work + d.urows_off;
+    v.tv = work + d.tv_off;
+    v.dstate = work + d.dstate_off;
+    v.dconst = work + d.dconst_off;
+    for (int k = 0; k < 4; ++k) v.st[k] = work + d.state_off + k * static_cast<int64_t>(d.n_states);
+    v.n = d.n;
+    v.num_nodes = d.num_nodes;
+    v.nnz = d.nnz;
+    v.n_const = d.n_const;
+    v.n_diodes = d.n_diodes;
+    v.n_caps = d.n_caps;
+    v.n_srcs = d.n_srcs;
+    return v;
+}
+
+__device__ __forceinline__ double term_value(int32_t op, double p, double gmin) {
+    switch (op) {
+        case 0: return 1.0 / p;
+        case 1: return -(1.0 / p);
+        case 2: return p;
+        case 3: return -p;
+        case 4: return 1.0;
+        case 5: return -1.0;
+        case 6: return 0.0;
+        case 7: return -0.0;
+        default: return gmin;
+    }
+}
+
+// Constant term values, diode constants (csat, vte, Vcrit at T = TNOM).
+__device__ inline void load_constants(const Inst& v, double gmin) {
+    for (int32_t k = threadIdx.x; k < v.n_const; k += blockDim.x) {
+        const int32_t pi = v.term_param[k];
+        v.tv[k] = term_value(v.term_op[k], pi >= 0 ? v.par[pi] : 0.0, gmin);
+    }
+    for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+        const int32_t pi = v.diodes[3 * k + 2];
+        const double csat = v.par[pi];
+        const double vte = v.par[pi + 1] * kKoverQTimesTnom;
+        v.dconst[3 * k] = csat;
+        v.dconst[3 * k + 1] = vte;
+        v.dconst[3 * k + 2] = diode_vcrit(vte, csat);
+    }
+}
+
+// Device loads of one Newton iteration at the guess xold: diodes (DIOload,
+// DC), capacitors (Capacitor::evaluate, state-vector path), waveform
+// sources (value_at).  Writes the dynamic terms; returns through s_dev_conv
+// whether every device reports convergence (diodes' CKTnoncon and conv_test).
+__device__ inline void eval_devices(const Inst& v, const IntegCtx& c, const NewtonOptions& opt,
+                                    int32_t* s_dev_conv) {
+    const int mode = c.mode;
+    double* tv_d = v.tv + v.n_const;
+    double* tv_c = tv_d + kDiodeTermCount * v.n_diodes;
+    double* tv_s = tv_c + kCapTermCount * v.n_caps;
+    const bool initjct = (mode & kModeInitJct) != 0;
+    for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+        const int32_t pos = v.diodes[3 * k], neg = v.diodes[3 * k + 1];
+        const double vp = pos >= 0 ? v.xold[pos] : 0.0;
+        const double vn = neg >= 0 ? v.xold[neg] : 0.0;
+        const DiodeDC r = diode_dc_load(initjct, vp, vn, v.dstate[3 * k], v.dconst[3 * k],
+                                        v.dconst[3 * k + 1], v.dconst[3 * k + 2], opt.gmin);
+        v.dstate[3 * k] = r.vd;
+        v.dstate[3 * k + 1] = r.cd;
+        v.dstate[3 * k + 2] = r.gd;
+        const double cdeq = r.cd - r.gd * r.vd;
+        double* t = tv_d + kDiodeTermCount * k;
+        t[0] = r.gd;
+        t[1] = r.gd + 0.0;
+        t[2] = -r.gd;
+        t[3] = cdeq;
+        t[4] = -cdeq;
+        // DIODevice::conv_test (dio_device.cpp:296-307) on the stored state
+        const double delvd = (vp - vn) - r.vd;
+        const double cdhat = r.cd + r.gd * delvd;
+        const double tol = opt.reltol * fmax(fabs(cdhat), fabs(r.cd)) + opt.abstol;
+        if (!((r.check == 0) && (fabs(cdhat - r.cd) <= tol))) *s_dev_conv = 0;
+    }
+    for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
+        const int32_t* cr = v.caps + 5 * k;
+        const double cap = v.par[cr[2]];
+        double* t = tv_c + kCapTermCount * k;
+        const int32_t s = cr[4];  // {q, i} at s, s+1
+        if (!(mode & (kModeTran | kModeAc | kModeTranOp))) {
+            t[0] = t[1] = t[2] = t[3] = 0.0;
+            continue;
+        }
+        const bool cond1 = ((mode & kModeDcMask) && (mode & kModeInitJct)) ||
+                           ((mode & kModeUic) && (mode & kModeInitTran));
+        double vcap;
+        if (cond1) {
+            vcap = cr[3] ? v.par[cr[2] + 1] : 0.0;
+        } else {
+            const double vp = cr[0] >= 0 ? v.xold[cr[0]] : 0.0;
+            const double vn = cr[1] >= 0 ? v.xold[cr[1]] : 0.0;
+            vcap = vp - vn;
+        }
+        if (mode & (kModeTran | kModeAc)) {
+            double* s0 = v.st[0];
+            double* s1 = v.st[1];
+            if (mode & kModeInitPred) {
+                s0[s] = s1[s];
+            } else {
+                s0[s] = cap * vcap;
+                if (mode & kModeInitTran) s1[s] = s0[s];
+            }
+            int order = c.order < 1 ? 1 : (c.order > 2 ? 2 : c.order);
+            double deriv;
+            if (order == 1) {
+                deriv = c.ag[0] * s0[s] + c.ag[1] * s1[s];
+            } else if (c.method == 0) {
+                deriv = -s1[s + 1] * c.xmu_ratio + c.ag[0] * s0[s] + c.ag[1] * s1[s];
+            } else {
+                deriv = c.ag[0] * s0[s] + c.ag[1] * s1[s] + c.ag[2] * v.st[2][s];
+            }
+            s0[s + 1] = deriv;
+            const double geq = c.ag[0] * cap;
+            const double ceq = s0[s + 1] - c.ag[0] * s0[s];
+            if (mode & kModeInitTran) s1[s + 1] = s0[s + 1];
+            t[0] = 1.0 * geq;
+            t[1] = -1.0 * geq;
+            t[2] = -1.0 * ceq;
+            t[3] = 1.0 * ceq;
+        } else {
+            v.st[0][s] = cap * vcap;
+            t[0] = t[1] = t[2] = t[3] = 0.0;
+        }
+    }
+    for (int32_t k = threadIdx.x; k < v.n_srcs; k += blockDim.x) {
+        const int32_t* sr = v.srcs + 4 * k;
+        const double val = wave_value(sr[1], v.par + sr[2], sr[3], c.time);
+        tv_s[kSrcTermCount * k] = val;
+        tv_s[kSrcTermCount * k + 1] = -val;
+    }
+}
+
+// Matrix values and rhs (into x) from the stamp program, in load order.
+__device__ inline void assemble(const Inst& v) {
+    for (int32_t s = threadIdx.x; s < v.nnz; s += blockDim.x) {
+        double acc = 0.0;
+        for (int32_t k = v.slot_ptr[s]; k < v.slot_ptr[s + 1]; ++k)
+            acc = __dadd_rn(acc, v.tv[v.slot_terms[k]]);
+        v.a[s] = acc;
+    }
+    for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) {
+        double nat = 0.0, ucb = 0.0;
+        for (int32_t k = v.rhs_ptr[i]; k < v.rhs_ptr[i + 1]; ++k) nat = __dadd_rn(nat, v.tv[v.rhs_terms[k]]);
+        for (int32_t k = v.ucb_ptr[i]; k < v.ucb_ptr[i + 1]; ++k) ucb = __dadd_rn(ucb, v.tv[v.ucb_terms[k]]);
+        v.x[i] = __dadd_rn(nat, ucb);
+    }
+}
+
+// Solver state of one instance across newton() calls (NeoSolver's flags).
+struct SolverState {
+    bool factored;  // a numeric() has succeeded on this plan
+};
+
+struct NewtonOutcome {
+    int32_t code;   // kDcConverged, kDcNoConvergence, kStatus*
+    int32_t iters;
+};
+
+// newton_solve (src/core/newton.cpp:51-419) for the whole CTA: x holds the
+// initial guess and receives the solution (the previous iterate on
+// convergence).  *ctx is the instance's integrator context in shared memory
+// (mode updated in place, restored on exit).
+__device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const int32_t* lu_pool,
+                                       IntegCtx* ctx, const NewtonOptions& opt, int max_iter,
+                                       SolverState* solver, double* smem, int colbuf) {
+    __shared__ int32_t s_conv, s_dev_conv;
+    const int saved_mode = ctx->mode;
+    bool force_numeric = false;
+    NewtonOutcome out{kDcNoConvergence, max_iter};
+    __syncthreads();
+    for (int iter = 0; iter < max_iter; ++iter) {
+        for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.xold[i] = v.x[i];
+        if (threadIdx.x == 0) s_dev_conv = 1;
+        __syncthreads();
+        eval_devices(v, *ctx, opt, &s_dev_conv);
+        __syncthreads();
+        assemble(v);
+        __syncthreads();
+
+        const int mode = ctx->mode;
+        const bool numeric = force_numeric || (mode & kModeInitJct) || !solver->factored;
+        const RefactorResult fr =
+            cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, numeric && solver->factored,
+                              1e-3, smem, colbuf, v.lrows, v.urows);
+        if (fr.code == kStatusTimeout) {
+            out = {kStatusTimeout, iter + 1};
+            break;
+        }
+        if (numeric) {
+            if (fr.code != kStatusOk) {
+                // NeoSolver::numeric would re-order (103) or report singular.
+                out = {fr.code, iter + 1};
+                break;
+            }
+            solver->factored = true;
+            force_numeric = false;
+        } else if (fr.code != kStatusOk) {
+            force_numeric = true;  // newton.cpp:229-234: retry with numeric
+            for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
+            __syncthreads();
+            continue;
+        }
+        if (!cta_solve_flow(pd, lu_pool, v.lu, v.lrows, v.urows, v.x, smem)) {
+            out = {kStatusTimeout, iter + 1};
+            break;
+        }
+
+        // Convergence test (newton.cpp:267-292).
+        if (threadIdx.x == 0) s_conv = 1;
+        __syncthreads();
+        for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) {
+            const double vn = v.x[i], vo = v.xold[i];
+            bool ok = !(isnan(vn) || isinf(vn));
+            if (ok) {
+                const double tol = opt.reltol * fmax(fabs(vn), fabs(vo)) +
+                                   (i < v.num_nodes ? opt.vntol : opt.abstol);
+                ok = fabs(vn - vo) <= tol;
+            }
+            if (!ok) s_conv = 0;
+        }
+        __syncthreads();
+        const bool conv = (s_conv != 0) && iter > 0 && (s_dev_conv != 0);
+
+        bool done = false;
+        if (mode & kModeInitFloat) {
+            if (conv) {
+                for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
+                out = {kDcConverged, iter + 1};
+                done = true;
+            }
+        } else if (mode & kModeInitJct) {
+            if (threadIdx.x == 0) ctx->mode = (mode & ~kModeInitMask) | kModeInitFix;
+            force_numeric = true;
+        } else if (mode & kModeInitFix) {
+            if (conv && threadIdx.x == 0) ctx->mode = (mode & ~kModeInitMask) | kModeInitFloat;
+        } else if (mode & kModeInitTran) {
+            if (threadIdx.x == 0) ctx->mode = (mode & ~kModeInitMask) | kModeInitFloat;
+            force_numeric = true;  // NISHOULDREORDER after MODEINITTRAN (newton.cpp:396-399)
+        } else if (mode & kModeInitPred) {
+            if (threadIdx.x == 0) ctx->mode = (mode & ~kModeInitMask) | kModeInitFloat;
+        } else if (conv) {
+            for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
+            out = {kDcConverged, iter + 1};
+            done = true;
+        }
+        __syncthreads();
+        if (done) break;
+    }
+    __syncthreads();
+    if (out.code != kDcConverged && out.code != kDcNoConvergence) {
+        // failure inside the loop: the caller's guess is the last iterate
+        for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
+    }
+    if (threadIdx.x == 0) ctx->mode = saved_mode;
+    __syncthreads();
+    return out;
+}
+
+}  // namespace nsg

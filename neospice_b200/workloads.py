@@ -75,3 +75,70 @@ def diode_mesh_batch(count: int, seed: int = 0, side_range=(16, 96)):
     """`count` independent meshes; instance i uses the seed sequence (seed, i)."""
     return [diode_mesh(np.random.default_rng([seed, i]), side_range=side_range)
             for i in range(count)]
+
+
+@dataclasses.dataclass
+class Netlist:
+    """A circuit as an ordered device list, built through the typed API in
+    list order (so node numbering and device load order are fixed).  Devices:
+    ("R", a, b, ohms), ("C", a, b, farads), ("V", p, n, volts),
+    ("I", p, n, amps), ("VPULSE"|"IPULSE", p, n, v1, v2, td, tr, tf, pw, per),
+    ("VPWL"|"IPWL", p, n, t0, v0, t1, v1, ...), ("D", anode, cathode, IS, N).
+    Node -1 is ground."""
+    num_nodes: int
+    devices: list
+
+    def build(self) -> Circuit:
+        c = Circuit(self.num_nodes)
+        for d in self.devices:
+            kind, a, b, vals = d[0], d[1], d[2], d[3:]
+            if kind == "R":
+                c.R(a, b, vals[0])
+            elif kind == "C":
+                c.C(a, b, vals[0], vals[1] if len(vals) > 1 else None)
+            elif kind == "V":
+                c.V(a, b, vals[0])
+            elif kind == "I":
+                c.I(a, b, vals[0])
+            elif kind in ("VPULSE", "IPULSE"):
+                (c.VPULSE if kind[0] == "V" else c.IPULSE)(a, b, *vals)
+            elif kind in ("VPWL", "IPWL"):
+                pts = np.asarray(vals, np.float64).reshape(-1, 2)
+                (c.VPWL if kind[0] == "V" else c.IPWL)(a, b, pts)
+            elif kind == "D":
+                c.D(a, b, vals[0], vals[1])
+            else:
+                raise ValueError(f"unknown device kind {kind!r}")
+        return c.finalize()
+
+
+def rc_ladder(rng: np.random.Generator, stages: int, r_ohm=1e3, c_farad=1e-12, sigma=0.2,
+              period=2e-9) -> Netlist:
+    """A PULSE(0 1 0 100p 100p period/2-100p period) source at node 0 driving
+    an RC ladder of `stages` sections: R (lognormal around r_ohm) from node
+    i to node i+1, C (lognormal around c_farad) from node i+1 to ground."""
+    dev = [("VPULSE", 0, GND, 0.0, 1.0, 0.0, 1e-10, 1e-10, period / 2 - 1e-10, period)]
+    r = r_ohm * np.exp(sigma * rng.standard_normal(stages))
+    cc = c_farad * np.exp(sigma * rng.standard_normal(stages))
+    for i in range(stages):
+        dev.append(("R", i, i + 1, float(r[i])))
+        dev.append(("C", i + 1, GND, float(cc[i])))
+    return Netlist(stages + 1, dev)
+
+
+def rc_tree(rng: np.random.Generator, nodes: int, r_ohm=50.0, c_farad=2e-15, sigma=0.2,
+            r_drive=1e3) -> Netlist:
+    """A random RC interconnect tree: node 0 is the driver node (a 0 -> 1 V
+    PULSE through r_drive), each node k >= 1 hangs from a uniformly drawn
+    earlier node by a resistor (lognormal around r_ohm) and has a capacitor
+    to ground (lognormal around c_farad).  The last node is the far end."""
+    dev = [("VPULSE", nodes, GND, 0.0, 1.0, 1e-11, 5e-11, 5e-11, 1e-9, 2e-9),
+           ("R", nodes, 0, r_drive)]
+    r = r_ohm * np.exp(sigma * rng.standard_normal(nodes))
+    cc = c_farad * np.exp(sigma * rng.standard_normal(nodes))
+    parent = [0] + [int(rng.integers(0, k)) for k in range(1, nodes)]
+    for k in range(1, nodes):
+        dev.append(("R", parent[k], k, float(r[k])))
+    for k in range(nodes):
+        dev.append(("C", k, GND, float(cc[k])))
+    return Netlist(nodes + 1, dev)

@@ -9,6 +9,11 @@ LU pattern, slot map), the factored values, the values after
 NeoSolver::refactorize on perturbed values, and the solutions of solve and
 solve_transposed.
 
+tran_rc.npz: seeded linear RC netlists (neospice_b200.workloads) with PULSE
+and PWL sources, per case the device list (JSON), tstep/tstop, and the
+reference's solve_transient output: every timepoint, all node voltages,
+total Newton iterations and rejected steps.
+
 mesh_dc.npz: seeded diode-clamped meshes (neospice_b200.workloads), per case
 the mesh, the reference's first-iteration matrix and rhs, and its DC
 operating point (solve_dc) with the Newton iteration count.
@@ -93,6 +98,56 @@ def mesh_main():
     print(f"wrote {len(sides)} meshes to {path}")
 
 
+def tran_netlists():
+    """(netlist, tstep, tstop) cases of tran_rc.npz."""
+    from neospice_b200 import workloads as W
+    cases = []
+    for k, stages in enumerate((1, 2, 3, 5, 8, 13, 20)):
+        nl = W.rc_ladder(np.random.default_rng([31, k]), stages)
+        cases.append((nl, 1e-11, 4e-9))
+    for k, nodes in enumerate((6, 25, 60)):
+        cases.append((W.rc_tree(np.random.default_rng([32, k]), nodes), 1e-12, 3e-10))
+    # Steps limited by the truncation-error estimate (one with rejections).
+    for k, (stages, tstep, tstop) in enumerate(((3, 1e-10, 4e-9), (8, 2e-10, 1e-8),
+                                                 (5, 1e-9, 2e-8))):
+        cases.append((W.rc_ladder(np.random.default_rng([33, k]), stages), tstep, tstop))
+    for k, (nodes, tstep, tstop) in enumerate(((25, 1e-11, 3e-10), (60, 2e-11, 1e-9))):
+        cases.append((W.rc_tree(np.random.default_rng([34, k]), nodes), tstep, tstop))
+    # PWL current load into an RC node, a DC source through R, one capacitor
+    # with an initial condition, a PULSE with default rise/fall/width/period.
+    cases.append((W.Netlist(4, [
+        ("V", 0, -1, 1.0), ("R", 0, 1, 100.0), ("C", 1, -1, 1e-12, 0.3),
+        ("R", 1, 2, 250.0), ("C", 2, -1, 2e-12),
+        ("IPWL", 2, -1, 0.0, 0.0, 1e-10, 1e-3, 3e-10, 1e-3, 3.5e-10, 0.0),
+        ("VPULSE", 3, -1, 0.0, 0.5, 2e-10, 0.0, 0.0, 0.0, 0.0), ("R", 3, 2, 500.0),
+        ("C", 3, 1, 5e-13)]), 1e-11, 1e-9))
+    return cases
+
+
+def tran_main():
+    import json
+    import netlists
+    rec = {}
+    cases = tran_netlists()
+    for k, (nl, tstep, tstop) in enumerate(cases):
+        t, v, info = oracle.ref_sim(netlists.ref_desc(nl), 1, tstep, tstop)
+        p = f"t{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices])),
+                    p + "tstep": np.float64(tstep), p + "tstop": np.float64(tstop),
+                    p + "times": t, p + "values": v,
+                    p + "iterations": np.int32(info["iterations"]),
+                    p + "rejected": np.int32(info["rejected"])})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("tran_rc.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} transients to {path}")
+
+
 if __name__ == "__main__":
-    main()
-    mesh_main()
+    which = sys.argv[1:] or ["solver", "mesh", "tran"]
+    if "solver" in which:
+        main()
+    if "mesh" in which:
+        mesh_main()
+    if "tran" in which:
+        tran_main()

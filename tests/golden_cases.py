@@ -34,3 +34,20 @@ def load_meshes():
                               d["isrc_nodes"], d["isrc_amps"])
         out.append(d)
     return out
+
+
+TRAN_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "tran_rc.npz"
+
+
+def load_transients():
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(TRAN_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"t{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev])
+        out.append(d)
+    return out

@@ -98,3 +98,37 @@ def test_circuit_misuse_raises():
     c.finalize()
     with pytest.raises(L.NsgError):
         c.R(0, 1, 1.0)  # after finalize
+
+
+def test_capacitor_and_wave_sources_params_order():
+    from neospice_b200.circuit import Circuit
+    c = Circuit(3)
+    c.R(0, 1, 10.0)
+    c.C(1, -1, 1e-12, ic=0.25)
+    c.VPULSE(0, -1, 0.0, 1.0, 1e-9, 0.0, 0.0, 0.0, 0.0)
+    c.IPWL(2, -1, [(0.0, 0.0), (1e-9, 1e-3)])
+    c.C(2, 1, 2e-12)
+    c.finalize()
+    p = c.params()
+    np.testing.assert_array_equal(p, [10.0, 1e-12, 0.25, 0.0, 1.0, 1e-9, 0, 0, 0, 0,
+                                      0.0, 0.0, 1e-9, 1e-3, 2e-12, 0.0])
+    assert c.info()["num_vars"] == 4  # 3 nodes + the V branch
+
+
+def test_tran_batch_rejects_diodes_and_bad_probes():
+    from neospice_b200 import _lib as L
+    from neospice_b200.circuit import Circuit, TranBatch
+    c = Circuit(2)
+    c.R(0, 1, 10.0)
+    c.D(1, -1, 1e-14, 1.0)
+    c.V(0, -1, 1.0)
+    c.finalize()
+    with pytest.raises(L.NsgError, match="diodes"):
+        TranBatch([c], 1e-12, 1e-10, [0])
+    d = Circuit(2)
+    d.R(0, 1, 10.0)
+    d.C(1, -1, 1e-12)
+    d.V(0, -1, 1.0)
+    d.finalize()
+    with pytest.raises(L.NsgError, match="probe"):
+        TranBatch([d], 1e-12, 1e-10, [7])
