@@ -178,6 +178,20 @@ int nsg_circuit_add_capacitor(nsg_circuit* c, int a, int b, double farads, int h
  * tf, pw or per takes the transient's default; PWL: time/value pairs). */
 int nsg_circuit_add_source_wave(nsg_circuit* c, int is_voltage, int p, int n, int wave,
                                 int nvalues, const double* values);
+/* A level-1 MOSFET model card (Circuit::model with ".model NAME NMOS|PMOS
+ * (LEVEL=1 ...)", src/core/circuit.hpp:259): type +1 NMOS / -1 PMOS and
+ * nparams (key, value) pairs with the MOS1 parameter names of
+ * src/devices/mos1/mos1_devsup.cpp:123-159 (vto kp gamma phi lambda cbd cbs is
+ * pb cgso cgdo cgbo cj mj cjsw mjsw js tox ld u0 fc nsub tpg nss tnom; kf, af
+ * and level are accepted and ignored).  Nonzero rd, rs or rsh (internal
+ * nodes) are rejected.  *model_out receives the model index. */
+int nsg_circuit_add_mos1_model(nsg_circuit* c, int type, int nparams, const char* const* keys,
+                               const double* values, int* model_out);
+/* Circuit::M with W and L (src/core/circuit.hpp:218-219).  Its parameter
+ * block has 43 values: W, L, VTO, then the card at the circuit temperature
+ * (the MOS1setup / MOS1temp results the device load reads). */
+int nsg_circuit_add_mosfet(nsg_circuit* c, int d, int g, int s, int b, int model, double w,
+                           double l);
 /* Bulk forms: count devices in one call, arrays of terminals and values,
  * created in array order (identical to count single calls). */
 int nsg_circuit_add_capacitors(nsg_circuit* c, int count, const int* a, const int* b,
@@ -200,9 +214,10 @@ int nsg_circuit_params(const nsg_circuit* c, double* params);
 int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs);
 
 /* ---- Batched DC operating point (device) ------------------------------------
- * Simulator::run_dc / solve_dc's direct Newton attempt (src/core/dc.cpp:53-118,
- * newton.cpp:51-419) for `count` circuits in one launch, one thread block per
- * circuit.  symbolic: NSG_SYMBOLIC_PER_INSTANCE orders every circuit on its own
+ * Simulator::run_dc / solve_dc (src/core/dc.cpp:53-175, newton.cpp:51-419):
+ * the direct Newton attempt, then true gmin stepping and gmin stepping
+ * (src/core/convergence.cpp:216-469) for instances it fails on, for `count`
+ * circuits in one launch, one thread block per circuit.  symbolic: NSG_SYMBOLIC_PER_INSTANCE orders every circuit on its own
  * first-iteration matrix (bit-identical to the reference's pivots);
  * NSG_SYMBOLIC_PER_PATTERN orders once per distinct sparsity pattern and lets
  * the GPU re-validate the pivots of every instance at its second iteration
@@ -234,10 +249,23 @@ int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, doubl
 /* Run every instance to convergence.  d_params: packed parameters (device;
  * NULL = the circuits' own values); d_solutions: packed solutions (device),
  * the returned iterate as newton_solve returns it; d_status: 0 converged,
- * 1 no convergence in itl1 iterations, 102 singular, 103 pivot re-validation
+ * 1 no convergence (direct attempt and gmin stepping failed), 102 singular, 103 pivot re-validation
  * failed, 104 a bounded wait gave up; d_iterations: Newton iterations. */
 int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
                      int* d_iterations, void* stream);
+/* Host re-ordering (default on): when an instance's pivots fail the
+ * re-validation of a later NeoSolver::numeric, nsg_dc_batch_run waits for the
+ * stream, re-orders that instance on the host exactly as the reference's
+ * order_and_factor does from the failing step, and resumes it on the device
+ * at the same Newton iteration (d_status 103 then no longer appears).  Off:
+ * nsg_dc_batch_run stays asynchronous and such instances report 103.
+ * nsg_dc_batch_reorders: instances re-ordered so far. */
+int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable);
+int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);
+/* After a run (synchronises the device): per instance the method that gave
+ * the result, as the reference's ConvergenceMethod (0 direct Newton, 1 gmin
+ * stepping), and the number of Newton solves it took (either may be NULL). */
+int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves);
 
 /* ---- Batched transient analysis (device) ------------------------------------
  * solve_transient (src/core/transient.cpp:694-1067) for `count` circuits in one

@@ -81,6 +81,13 @@ SIGNATURES = {
     "nsg_circuit_add_source_wave": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int,
                                             P(c_double)]),
     "nsg_circuit_add_capacitors": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
+    "nsg_circuit_add_mos1_model": (c_int, [c_void_p, c_int, c_int, P(ctypes.c_char_p), P(c_double),
+                                           P(c_int)]),
+    "nsg_circuit_add_mosfet": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,
+                                       c_double]),
+    "nsg_dc_batch_set_reorder": (c_int, [c_void_p, c_int]),
+    "nsg_dc_batch_reorders": (c_int, [c_void_p, P(c_ll)]),
+    "nsg_dc_batch_methods": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "nsg_tran_batch_create": (c_int, [c_int, P(c_void_p), c_double, c_double, c_int, c_int,
                                       P(c_int), c_int, P(c_void_p)]),
     "nsg_tran_batch_free": (None, [c_void_p]),

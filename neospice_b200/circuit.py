@@ -2,7 +2,7 @@
 
 ``Circuit`` mirrors the reference's typed Circuit API (src/core/circuit.hpp:
 179-237) for resistors, capacitors, DC / PULSE / PWL voltage and current
-sources and level-1 diodes; nodes are integers and ``GND`` (-1) is ground.
+sources, level-1 diodes and level-1 MOSFETs; nodes are integers and ``GND`` (-1) is ground.
 ``DcBatch`` runs the direct Newton attempt of Simulator::run_dc
 (src/core/dc.cpp:53-118) for many circuits in one kernel launch;
 ``TranBatch`` runs solve_transient (src/core/transient.cpp:694-1067) for many
@@ -66,6 +66,22 @@ class Circuit:
 
     def IPWL(self, p: int, n: int, points):
         self._wave(False, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
+
+    def model_mos1(self, mtype: str, **params) -> int:
+        """A level-1 MOSFET model card, e.g. model_mos1("nmos", VTO=0.7,
+        KP=110e-6); returns the model index for M()."""
+        t = {"nmos": 1, "pmos": -1}[mtype.lower()]
+        keys = (ctypes.c_char_p * max(1, len(params)))(*[k.encode() for k in params])
+        vals = np.ascontiguousarray([float(v) for v in params.values()] or [0.0], np.float64)
+        out = ctypes.c_int()
+        L.check(L.lib().nsg_circuit_add_mos1_model(self._h, t, len(params), keys, L.dptr(vals),
+                                                   ctypes.byref(out)))
+        return out.value
+
+    def M(self, d: int, g: int, s: int, b: int, model: int, W: float = 1e-6, L_: float = 1e-7):
+        """Circuit::M(name, d, g, s, b, model, w, l)."""
+        L.check(L.lib().nsg_circuit_add_mosfet(self._h, int(d), int(g), int(s), int(b), int(model),
+                                               float(W), float(L_)))
 
     def add_capacitors(self, a, b, farads):
         a, b = np.ascontiguousarray(a, np.int32), np.ascontiguousarray(b, np.int32)
@@ -170,6 +186,22 @@ class DcBatch:
     def set_options(self, reltol=1e-3, vntol=1e-6, abstol=1e-12, gmin=1e-12, max_iter=100):
         L.check(L.lib().nsg_dc_batch_set_options(self._h, reltol, vntol, abstol, gmin,
                                                  int(max_iter)))
+
+    def set_reorder(self, enable: bool):
+        L.check(L.lib().nsg_dc_batch_set_reorder(self._h, int(bool(enable))))
+
+    def reorders(self) -> int:
+        n = ctypes.c_longlong()
+        L.check(L.lib().nsg_dc_batch_reorders(self._h, ctypes.byref(n)))
+        return n.value
+
+    def methods(self):
+        """(method, solves) per instance after a run: 0 direct Newton, 1 gmin
+        stepping; Newton solves taken."""
+        m = np.zeros(self.count, np.int32)
+        n = np.zeros(self.count, np.int32)
+        L.check(L.lib().nsg_dc_batch_methods(self._h, L.iptr(m), L.iptr(n)))
+        return m, n
 
     def params(self):
         """Packed default parameters of all circuits (host)."""

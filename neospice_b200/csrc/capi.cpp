@@ -1,6 +1,7 @@
 // C ABI of libnsgpu (declared in include/nsgpu.h): host symbolic phase, batch
 // set-up and the launches of the batched refactor and sweeps.
 #include "capi_internal.hpp"
+#include "kernels/dc_device.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -95,6 +96,92 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.nnz_u = p.urow_ptr[p.n];
     p.append_to(pool, d.off);
     return d;
+}
+
+
+std::unique_ptr<nsg_topology> clone_topology(const nsg_topology& t) {
+    if (!t.engine) throw std::logic_error("clone_topology: topology has no ordering engine");
+    auto c = std::make_unique<nsg_topology>();
+    c->engine = std::make_unique<nsg::MarkowitzOrder>(*t.engine);
+    c->slot_elem = t.slot_elem;
+    c->plan = t.plan;
+    return c;
+}
+
+bool same_plan(const nsg::TopologyPlan& a, const nsg::TopologyPlan& b) {
+    return a.n == b.n && a.perm_row == b.perm_row && a.perm_col == b.perm_col &&
+           a.col_ptr == b.col_ptr && a.row_idx == b.row_idx && a.lu_src == b.lu_src;
+}
+
+int intern_topology(std::vector<std::unique_ptr<nsg_topology>>& topos,
+                    std::unique_ptr<nsg_topology> t) {
+    for (size_t k = 0; k < topos.size(); ++k)
+        if (same_plan(topos[k]->plan, t->plan)) return static_cast<int>(k);
+    topos.push_back(std::move(t));
+    return static_cast<int>(topos.size()) - 1;
+}
+
+int reorder_instance(std::vector<std::unique_ptr<nsg_topology>>& topos, int topo,
+                     const double* values, double diag_gmin, int* new_topo) {
+    auto c = clone_topology(*topos[topo]);
+    const int rc = numeric_on_engine(*c, values, diag_gmin);
+    if (rc != NSG_OK) return rc;
+    c->plan = nsg::build_plan(*c->engine, c->slot_elem);
+    *new_topo = intern_topology(topos, std::move(c));
+    return NSG_OK;
+}
+
+void place_lu_workspace(nsg::DcDesc& d, const nsg::TopologyPlan& p, int64_t& work_size) {
+    auto take = [&](int64_t n) {
+        const int64_t off = work_size;
+        work_size += (n + 3) & ~int64_t{3};
+        return off;
+    };
+    d.lu_off = take(p.nnz_lu);
+    d.lrows_off = take(p.lrow_ptr[p.n]);
+    d.urows_off = take(p.urow_ptr[p.n]);
+}
+
+cudaError_t grow_workspace(double** d_work, int64_t* capacity, int64_t needed) {
+    if (needed <= *capacity) return cudaSuccess;
+    const int64_t cap = needed + needed / 4;
+    double* w = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&w), sizeof(double) * cap);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(w, *d_work, sizeof(double) * (*capacity), cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(w);
+        return e;
+    }
+    cudaFree(*d_work);
+    *d_work = w;
+    *capacity = cap;
+    return cudaSuccess;
+}
+
+int refresh_plans(const std::vector<std::unique_ptr<nsg_topology>>& topos, int32_t** d_lu_pool,
+                  nsg::PlanDesc** d_plans, int* max_col, int* max_n) {
+    std::vector<int32_t> pool;
+    std::vector<nsg::PlanDesc> plans;
+    for (const auto& t : topos) {
+        plans.push_back(make_plan_desc(t->plan, pool));
+        *max_col = std::max(*max_col, t->plan.max_col);
+        *max_n = std::max(*max_n, t->plan.n);
+    }
+    int32_t* p = nullptr;
+    nsg::PlanDesc* q = nullptr;
+    cudaError_t e;
+    if ((e = upload(&p, pool.data(), pool.size())) != cudaSuccess ||
+        (e = upload(&q, plans.data(), plans.size())) != cudaSuccess) {
+        cudaFree(p);
+        cudaFree(q);
+        return cuda_fail("refresh_plans", e);
+    }
+    cudaFree(*d_lu_pool);
+    cudaFree(*d_plans);
+    *d_lu_pool = p;
+    *d_plans = q;
+    return NSG_OK;
 }
 
 }  // namespace nsg_internal

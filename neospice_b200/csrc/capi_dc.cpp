@@ -13,8 +13,9 @@
 
 namespace nsg {
 cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
-                             int count, const int32_t* prog, const double* params, double* work,
-                             double* solutions, int32_t* status, int32_t* iterations,
+                             const int32_t* subset, int count, const int32_t* prog,
+                             const double* params, double* work, double* solutions,
+                             int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
                              cudaStream_t stream);
 size_t dc_smem_bytes(int max_col, int max_n);
@@ -37,6 +38,15 @@ struct nsg_dc_batch {
     nsg::DcDesc* d_descs = nullptr;
     double* d_work = nullptr;
     double* d_params = nullptr;
+    // Host re-ordering of instances whose pivots fail re-validation.
+    bool reorder = true;
+    long long reorders = 0;
+    std::vector<nsg::DcDesc> descs;   // host copy, launch order
+    std::vector<int> desc_pos;        // instance index -> position in descs
+    std::vector<int> topo_of;         // instance index -> topology
+    int64_t work_size = 0, work_cap = 0;
+    nsg::DcCtl* d_ctl = nullptr;
+    int32_t* d_subset = nullptr;
     ~nsg_dc_batch() {
         cudaFree(d_lu_pool);
         cudaFree(d_plans);
@@ -44,6 +54,8 @@ struct nsg_dc_batch {
         cudaFree(d_descs);
         cudaFree(d_work);
         cudaFree(d_params);
+        cudaFree(d_ctl);
+        cudaFree(d_subset);
     }
 };
 
@@ -99,6 +111,7 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     d.n_diodes = static_cast<int32_t>(c.diodes().size());
     d.n_caps = static_cast<int32_t>(c.caps().size());
     d.n_srcs = static_cast<int32_t>(c.wave_sources().size());
+    d.n_mos = static_cast<int32_t>(c.mosfets().size());
     d.n_states = c.num_states();
     d.prog_off[nsg::DP_slot_ptr] = append(prog, c.slot_ptr());
     d.prog_off[nsg::DP_slot_terms] = append(prog, c.slot_terms());
@@ -117,6 +130,9 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     tab.clear();
     for (const auto& sr : c.wave_sources()) tab.insert(tab.end(), {sr.is_voltage, sr.wave, sr.param, sr.nparam});
     d.prog_off[nsg::DP_srcs] = append(prog, tab);
+    tab.clear();
+    for (const auto& m : c.mosfets()) tab.insert(tab.end(), {m.d, m.g, m.s, m.b, m.param, m.state});
+    d.prog_off[nsg::DP_mos] = append(prog, tab);
     d.x_off = work; work = align4(work + d.n);
     d.xold_off = work; work = align4(work + d.n);
     d.w_off = work; work = align4(work + d.n);
@@ -128,6 +144,9 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
     d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
     d.state_off = work; work = align4(work + 4 * static_cast<int64_t>(d.n_states));
+    d.mrec_off = work; work = align4(work + nsg::kMosRecCount * static_cast<int64_t>(d.n_mos));
+    d.dcsave_off = work;
+    work = align4(work + d.n + 3 * static_cast<int64_t>(d.n_states) + 3 * d.n_diodes);
 }
 
 }  // namespace nsg_internal
@@ -194,6 +213,31 @@ int nsg_circuit_add_source_wave(nsg_circuit* c, int is_voltage, int p, int n, in
             return fail(NSG_ERR_INVALID, "nsg_circuit_add_source_wave: unknown waveform");
         c->c.add_source_wave(is_voltage != 0, p, n, static_cast<nsg::Wave>(wave),
                              std::vector<double>(values, values + nvalues));
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_mos1_model(nsg_circuit* c, int type, int nparams, const char* const* keys,
+                               const double* values, int* model_out) {
+    return guarded("nsg_circuit_add_mos1_model", [&]() -> int {
+        if (!c || nparams < 0 || (nparams && (!keys || !values)) || !model_out)
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        nsg::Mos1Card card;
+        card.type = type;
+        for (int i = 0; i < nparams; ++i) {
+            if (!keys[i]) return fail(NSG_ERR_INVALID, "nsg_circuit_add_mos1_model: null key");
+            card.params.emplace_back(keys[i], values[i]);
+        }
+        *model_out = c->c.add_mos1_model(card);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_mosfet(nsg_circuit* c, int d, int g, int s, int b, int model, double w,
+                           double l) {
+    return guarded("nsg_circuit_add_mosfet", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_mosfet(d, g, s, b, model, w, l);
         return NSG_OK;
     });
 }
@@ -385,14 +429,21 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             return fail(NSG_ERR_INVALID, "nsg_dc_batch_create: instance too large for the "
                                          "shared-memory refactor (longest LU column " +
                                          std::to_string(b->max_col) + ")");
+        b->desc_pos.assign(count, 0);
+        for (int k = 0; k < count; ++k) b->desc_pos[descs[k].index] = k;
+        b->topo_of = topo_of;
+        b->work_size = b->work_cap = work;
         cudaError_t e;
         if ((e = upload(&b->d_lu_pool, lu_pool.data(), lu_pool.size())) != cudaSuccess ||
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
             (e = upload(&b->d_prog, prog.data(), prog.size())) != cudaSuccess ||
             (e = upload(&b->d_descs, descs.data(), descs.size())) != cudaSuccess ||
             (e = upload<double>(&b->d_work, nullptr, static_cast<size_t>(work))) != cudaSuccess ||
-            (e = upload(&b->d_params, b->host_params.data(), b->host_params.size())) != cudaSuccess)
+            (e = upload(&b->d_params, b->host_params.data(), b->host_params.size())) != cudaSuccess ||
+            (e = upload<nsg::DcCtl>(&b->d_ctl, nullptr, count)) != cudaSuccess ||
+            (e = upload<int32_t>(&b->d_subset, nullptr, count)) != cudaSuccess)
             return cuda_fail("nsg_dc_batch_create", e);
+        b->descs = std::move(descs);
         *out = b.release();
         return NSG_OK;
     });
@@ -442,15 +493,96 @@ int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, doubl
     return NSG_OK;
 }
 
+int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_reorder: null batch");
+    b->reorder = enable != 0;
+    return NSG_OK;
+}
+
+int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count) {
+    if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_dc_batch_reorders: null argument");
+    *count = b->reorders;
+    return NSG_OK;
+}
+
+int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_methods: null batch");
+    std::vector<nsg::DcCtl> ctl(b->count);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ctl.data(), b->d_ctl, sizeof(nsg::DcCtl) * b->count, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_methods", e);
+    for (int i = 0; i < b->count; ++i) {
+        if (method) method[i] = ctl[i].method;
+        if (solves) solves[i] = ctl[i].solves;
+    }
+    return NSG_OK;
+}
+
 int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
                      int* d_iterations, void* stream) {
-    if (!b || !d_solutions || !d_status || !d_iterations)
-        return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: null argument");
-    cudaError_t e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, b->count, b->d_prog,
-                                          d_params ? d_params : b->d_params, b->d_work, d_solutions,
-                                          d_status, d_iterations, b->opt, b->max_col, b->max_n,
-                                          static_cast<cudaStream_t>(stream));
-    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_dc_batch_run", e);
+    return guarded("nsg_dc_batch_run", [&]() -> int {
+        if (!b || !d_solutions || !d_status || !d_iterations)
+            return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: null argument");
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const double* params = d_params ? d_params : b->d_params;
+        cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::DcCtl) * b->count, st);
+        if (e == cudaSuccess)
+            e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, nullptr, b->count,
+                                      b->d_prog, params, b->d_work, d_solutions, d_status,
+                                      d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n, st);
+        if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_run", e);
+        if (!b->reorder) return NSG_OK;
+        // Instances whose pivots failed re-validation: re-order on the host
+        // (NeoSolver::numeric's order_and_factor from the failing step) and
+        // resume them on the device.
+        std::vector<int> status(b->count);
+        for (int round = 0; round < 64; ++round) {
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess ||
+                (e = cudaMemcpy(status.data(), d_status, sizeof(int) * b->count,
+                                cudaMemcpyDeviceToHost)) != cudaSuccess)
+                return cuda_fail("nsg_dc_batch_run", e);
+            std::vector<int32_t> subset;
+            for (int i = 0; i < b->count; ++i) {
+                if (status[i] != NSG_REORDER) continue;
+                nsg::DcDesc& d = b->descs[b->desc_pos[i]];
+                std::vector<double> a(d.nnz);
+                nsg::DcCtl ctl;
+                if ((e = cudaMemcpy(a.data(), b->d_work + d.a_off, sizeof(double) * d.nnz,
+                                    cudaMemcpyDeviceToHost)) != cudaSuccess ||
+                    (e = cudaMemcpy(&ctl, b->d_ctl + i, sizeof ctl, cudaMemcpyDeviceToHost)) !=
+                        cudaSuccess)
+                    return cuda_fail("nsg_dc_batch_run", e);
+                int topo = 0;
+                const int rc = reorder_instance(b->topos, b->topo_of[i], a.data(),
+                                                ctl.numeric_diag_gmin, &topo);
+                if (rc != NSG_OK) continue;  // stays NSG_REORDER: the host could not re-order
+                b->topo_of[i] = topo;
+                d.plan = topo;
+                place_lu_workspace(d, b->topos[topo]->plan, b->work_size);
+                subset.push_back(b->desc_pos[i]);
+                ++b->reorders;
+            }
+            if (subset.empty()) break;
+            int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col, &b->max_n);
+            if (rc != NSG_OK) return rc;
+            if (nsg::dc_smem_bytes(b->max_col, b->max_n) > 200 * 1024)
+                return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: re-ordered instance too large "
+                                             "for the shared-memory refactor");
+            if ((e = grow_workspace(&b->d_work, &b->work_cap, b->work_size)) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_descs, b->descs.data(), sizeof(nsg::DcDesc) * b->count,
+                                cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_subset, subset.data(), sizeof(int32_t) * subset.size(),
+                                cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, b->d_subset,
+                                           static_cast<int>(subset.size()), b->d_prog, params,
+                                           b->d_work, d_solutions, d_status, d_iterations,
+                                           b->d_ctl, b->opt, b->max_col, b->max_n, st)) !=
+                    cudaSuccess)
+                return cuda_fail("nsg_dc_batch_run", e);
+        }
+        return NSG_OK;
+    });
 }
 
 }  // extern "C"

@@ -96,4 +96,24 @@ namespace nsg { struct DcDesc; }
 namespace nsg_internal {
 void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPlan& p,
                    std::vector<int32_t>& prog, int64_t& work);
+
+// Host (re-)ordering of one instance that stopped on the device.
+// reorder_instance: a copy of topos[topo]'s engine runs NeoSolver::numeric on
+// the instance's matrix values (re-validate, re-order from the failing
+// step); the result is shared with an existing topology of identical
+// structure (intern_topology) or appended.  *new_topo receives its index.
+std::unique_ptr<nsg_topology> clone_topology(const nsg_topology& t);
+bool same_plan(const nsg::TopologyPlan& a, const nsg::TopologyPlan& b);
+int intern_topology(std::vector<std::unique_ptr<nsg_topology>>& topos,
+                    std::unique_ptr<nsg_topology> t);
+int reorder_instance(std::vector<std::unique_ptr<nsg_topology>>& topos, int topo,
+                     const double* values, double diag_gmin, int* new_topo);
+// Fresh LU / row-copy regions for a re-ordered instance at the end of the
+// workspace (work_size grows).
+void place_lu_workspace(nsg::DcDesc& d, const nsg::TopologyPlan& p, int64_t& work_size);
+// Reallocate the device workspace to hold `needed` doubles, keeping contents.
+cudaError_t grow_workspace(double** d_work, int64_t* capacity, int64_t needed);
+// Rebuild and re-upload the plan pool and descriptors of all topologies.
+int refresh_plans(const std::vector<std::unique_ptr<nsg_topology>>& topos, int32_t** d_lu_pool,
+                  nsg::PlanDesc** d_plans, int* max_col, int* max_n);
 }  // namespace nsg_internal

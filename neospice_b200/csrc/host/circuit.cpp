@@ -1,6 +1,7 @@
 #include "circuit.hpp"
 
 #include "kernels/diode_model.cuh"
+#include "kernels/mos1_model.cuh"
 #include "kernels/source_wave.cuh"
 
 #include <algorithm>
@@ -32,6 +33,7 @@ int32_t Circuit::add_device(DevKind kind, int32_t a, int32_t b, const std::vecto
     d.b = b;
     d.param = static_cast<int32_t>(params_.size());
     d.nparam = static_cast<int32_t>(p.size());
+    d.c = d.e = -1;
     d.branch = -1;
     d.wave = wave;
     d.has_ic = has_ic;
@@ -72,6 +74,26 @@ int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_e
     if (!(is > 0.0) || !(n_emission > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
     return add_device(DevKind::Diode, anode, cathode, {is, n_emission});
+}
+
+int32_t Circuit::add_mos1_model(const Mos1Card& card) {
+    if (finalized_) throw std::logic_error("Circuit: already finalized");
+    (void)mos1_param_block(card, 1e-6, 1e-6);  // validate the card now
+    mos_models_.push_back(card);
+    return static_cast<int32_t>(mos_models_.size()) - 1;
+}
+
+int32_t Circuit::add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
+                            double L) {
+    check_node(s);
+    check_node(b);
+    if (model < 0 || model >= static_cast<int32_t>(mos_models_.size()))
+        throw std::out_of_range("Circuit: unknown MOSFET model " + std::to_string(model));
+    if (!(W > 0.0) || !(L > 0.0)) throw std::invalid_argument("Circuit: MOSFET needs W > 0, L > 0");
+    const int32_t id = add_device(DevKind::Mosfet, d, g, mos1_param_block(mos_models_[model], W, L));
+    devices_.back().c = s;
+    devices_.back().e = b;
+    return id;
 }
 
 int32_t Circuit::offset(int32_t r, int32_t c) const {
@@ -121,6 +143,14 @@ void Circuit::finalize() {
                 break;
             case DevKind::ISource:
                 break;
+            case DevKind::Mosfet: {  // MOS1setup's TSTALLOC list with dNodePrime = d, sNodePrime = s
+                const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
+                stamp(D, D); stamp(G, G); stamp(S, S); stamp(B, B); stamp(D, D); stamp(S, S);
+                stamp(D, D); stamp(G, B); stamp(G, D); stamp(G, S); stamp(S, S); stamp(B, D);
+                stamp(B, S); stamp(D, S); stamp(D, D); stamp(B, G); stamp(D, G); stamp(S, G);
+                stamp(S, S); stamp(D, B); stamp(S, B); stamp(S, D);
+                break;
+            }
         }
     }
     std::vector<char> touched(num_vars_, 0);
@@ -150,11 +180,16 @@ void Circuit::finalize() {
     diodes_.clear();
     caps_.clear();
     wsrc_.clear();
+    mos_.clear();
     std::vector<int32_t> index_in_table(order.size(), -1);
     int32_t state = 0;
     for (size_t k = 0; k < order.size(); ++k) {
         const auto& d = order[k];
-        if (d.kind == DevKind::Diode) {
+        if (d.kind == DevKind::Mosfet) {
+            index_in_table[k] = static_cast<int32_t>(mos_.size());
+            mos_.push_back({d.a, d.b, d.c, d.e, d.param, state});
+            state += kMosStates;
+        } else if (d.kind == DevKind::Diode) {
             index_in_table[k] = static_cast<int32_t>(diodes_.size());
             diodes_.push_back({d.a, d.b, d.param});
         } else if (d.kind == DevKind::Capacitor) {
@@ -167,6 +202,7 @@ void Circuit::finalize() {
                              d.param, d.nparam});
         }
     }
+    num_states_ = state;
 
     // Stamp program: replay each device's evaluate() in load order.  Dynamic
     // terms are recorded as -1 - (block offset) and renumbered once the
@@ -184,8 +220,12 @@ void Circuit::finalize() {
     const int32_t nc = static_cast<int32_t>(caps_.size());
     auto diode_term = [&](int32_t id, int32_t w) { return -1 - (id * kDiodeTerms + w); };
     auto cap_term = [&](int32_t id, int32_t w) { return -1 - (nd * kDiodeTerms + id * kCapTerms + w); };
+    const int32_t nw = static_cast<int32_t>(wsrc_.size());
     auto src_term = [&](int32_t id, int32_t w) {
         return -1 - (nd * kDiodeTerms + nc * kCapTerms + id * kSrcTerms + w);
+    };
+    auto mos_term = [&](int32_t id, int32_t w) {
+        return -1 - (nd * kDiodeTerms + nc * kCapTerms + nw * kSrcTerms + id * kMosTerms + w);
     };
     auto add_slot = [&](int32_t r, int32_t c, int32_t term) {
         const int32_t off = offset(r, c);
@@ -195,6 +235,21 @@ void Circuit::finalize() {
         const auto& d = order[k];
         const int32_t id = index_in_table[k];
         switch (d.kind) {
+            case DevKind::Mosfet: {
+                // MOS1load: the four rhs updates (UCB array: gate, bulk,
+                // drain', source'), then the 22 matrix adds in order.
+                const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
+                if (G >= 0) ucb[G].push_back(mos_term(id, kTRhsG));
+                if (B >= 0) ucb[B].push_back(mos_term(id, kTRhsB));
+                if (D >= 0) ucb[D].push_back(mos_term(id, kTRhsDP));
+                if (S >= 0) ucb[S].push_back(mos_term(id, kTRhsSP));
+                const int32_t rc[22][2] = {{D, D}, {G, G}, {S, S}, {B, B}, {D, D}, {S, S},
+                                           {D, D}, {G, B}, {G, D}, {G, S}, {S, S}, {B, G},
+                                           {B, D}, {B, S}, {D, D}, {D, G}, {D, B}, {D, S},
+                                           {S, G}, {S, S}, {S, B}, {S, D}};
+                for (int32_t w = 0; w < 22; ++w) add_slot(rc[w][0], rc[w][1], mos_term(id, w));
+                break;
+            }
             case DevKind::Capacitor:
                 add_slot(d.a, d.a, cap_term(id, kCGeq));
                 add_slot(d.a, d.b, cap_term(id, kCNegGeq));
@@ -361,6 +416,18 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
         t[kDNegGd] = -r.gd;
         t[kDCdeq] = cdeq;
         t[kDNegCdeq] = -cdeq;
+    }
+    // MOSFETs at MODEDCOP | MODEINITJCT from zero state.
+    {
+        std::vector<double> rec(kMosRec, 0.0), st(kMosStates, 0.0);
+        const Mos1Integ ic{0, 0, 0, 0, 0, 0, 1, 0};
+        const double v0[4] = {0, 0, 0, 0};
+        for (size_t m = 0; m < mos_.size(); ++m) {
+            std::fill(rec.begin(), rec.end(), 0.0);
+            std::fill(st.begin(), st.end(), 0.0);
+            mos1_load(&params_[mos_[m].param], rec.data(), st.data(), st.data(), st.data(),
+                      kM1DcOp | kM1InitJct, ic, gmin, v0, &tv[mos_term_base() + kMosTerms * m]);
+        }
     }
     // Waveform sources at t = 0.
     for (size_t s = 0; s < wsrc_.size(); ++s) {

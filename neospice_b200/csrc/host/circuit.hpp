@@ -10,12 +10,16 @@
 // sequence of IEEE additions.
 #pragma once
 #include <cstdint>
+#include <string>
+#include <utility>
 #include <vector>
 
 namespace nsg {
 
 // ngspice load rank of each device family (src/core/circuit.cpp:34-59).
-enum class DevKind : int32_t { Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50 };
+enum class DevKind : int32_t {
+    Mosfet = 3, Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50
+};
 
 // Independent-source waveforms (src/devices/vsource.cpp:80-131).
 enum class Wave : int32_t { DC = 0, Pulse = 1, Pwl = 2 };
@@ -42,17 +46,38 @@ enum DiodeTerm : int32_t { kDGd = 0, kDGdPlusGspr = 1, kDNegGd = 2, kDCdeq = 3, 
 enum CapTerm : int32_t { kCGeq = 0, kCNegGeq = 1, kCNegCeq = 2, kCCeq = 3, kCapTerms = 4 };
 // Per waveform source: the value and its negation at the current time.
 enum SrcTerm : int32_t { kSVal = 0, kSNegVal = 1, kSrcTerms = 2 };
+// Per MOSFET: the Mos1Term values of kernels/mos1_model.cuh (22 matrix
+// terms in MOS1load's order, then the gate, bulk, drain and source rhs).
+constexpr int32_t kMosTerms = 26;
+constexpr int32_t kMosStates = 17;  // MOS1numStates
+constexpr int32_t kMosRec = 12;     // persistent per-load values
 
 struct DeviceRec {
     DevKind kind;
     int32_t created;   // creation index over all devices
-    int32_t a, b;      // terminals (0-based node, -1 = ground)
+    int32_t a, b;      // terminals (0-based node, -1 = ground); MOSFET: drain, gate
+    int32_t c, e;      // MOSFET: source, bulk
     int32_t param;     // first parameter index
     int32_t nparam;    // parameter count
     int32_t branch;    // VSource branch unknown, else -1
     Wave wave;         // sources
     bool has_ic;       // capacitors
 };
+
+// A level-1 MOSFET model card: the type (+1 NMOS, -1 PMOS) and the given
+// parameters (ngspice names, MOS1mPTable of
+// src/devices/mos1/mos1_devsup.cpp:123-159).
+struct Mos1Card {
+    int32_t type = 1;
+    std::vector<std::pair<std::string, double>> params;
+};
+
+// The MOS1 parameter block (kernels/mos1_model.cuh, Mos1Param) of one
+// instance of `card` with width W and length L at the nominal temperature:
+// MOS1setup's defaults and MOS1temp (src/devices/mos1/mos1_setup.cpp,
+// mos1_temp.cpp).  Throws std::invalid_argument on an unknown or
+// unsupported parameter (nonzero RD, RS or RSH).
+std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L);
 
 class Circuit {
 public:
@@ -70,6 +95,12 @@ public:
     int32_t add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wave,
                             const std::vector<double>& values);
     int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission);
+    // Level-1 MOSFET models and instances (Circuit::model,
+    // src/core/circuit.hpp:259, and Circuit::M with W and L, :218-219).
+    // Returns the model / device index.
+    int32_t add_mos1_model(const Mos1Card& card);
+    int32_t add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
+                       double L);
 
     void finalize();
     bool finalized() const { return finalized_; }
@@ -87,10 +118,12 @@ public:
     struct DiodeRec { int32_t pos, neg, param; };
     struct CapRec { int32_t pos, neg, param, has_ic, state; };  // state: base of {q, i}
     struct SrcRec { int32_t is_voltage, wave, param, nparam; };
+    struct MosRec { int32_t d, g, s, b, param, state; };
     const std::vector<DiodeRec>& diodes() const { return diodes_; }
     const std::vector<CapRec>& caps() const { return caps_; }
     const std::vector<SrcRec>& wave_sources() const { return wsrc_; }
-    int32_t num_states() const { return 2 * static_cast<int32_t>(caps_.size()); }
+    const std::vector<MosRec>& mosfets() const { return mos_; }
+    int32_t num_states() const { return num_states_; }
 
     // Stamp program (valid after finalize).
     int32_t n_const_terms() const { return static_cast<int32_t>(term_op_.size()); }
@@ -101,7 +134,10 @@ public:
     int32_t src_term_base() const {
         return cap_term_base() + kCapTerms * static_cast<int32_t>(caps_.size());
     }
-    int32_t n_terms() const { return src_term_base() + kSrcTerms * static_cast<int32_t>(wsrc_.size()); }
+    int32_t mos_term_base() const {
+        return src_term_base() + kSrcTerms * static_cast<int32_t>(wsrc_.size());
+    }
+    int32_t n_terms() const { return mos_term_base() + kMosTerms * static_cast<int32_t>(mos_.size()); }
     const std::vector<int32_t>& term_op() const { return term_op_; }
     const std::vector<int32_t>& term_param() const { return term_param_; }
     // Per matrix slot / rhs row: ptr (size+1) and term indices, in add order.
@@ -121,6 +157,7 @@ public:
     // Host evaluation of the matrix and rhs at the first Newton iteration of
     // a DC operating point (MODEDCOP | MODEINITJCT, zero initial guess), with
     // host libm -- the values the reference's first NeoSolver::numeric sees.
+    // (MODETRANOP | MODEINITJCT gives the same values for these devices.)
     void initjct_values(std::vector<double>& a, std::vector<double>& rhs,
                         double gmin) const;
     // Matrix of the first transient iteration of a circuit without nonlinear
@@ -138,6 +175,9 @@ private:
     std::vector<DiodeRec> diodes_;
     std::vector<CapRec> caps_;
     std::vector<SrcRec> wsrc_;
+    std::vector<MosRec> mos_;
+    std::vector<Mos1Card> mos_models_;
+    int32_t num_states_ = 0;
     std::vector<int32_t> term_op_, term_param_;
     std::vector<int32_t> slot_ptr_, slot_terms_, rhs_ptr_, rhs_terms_, ucb_ptr_, ucb_terms_;
 

@@ -9,7 +9,7 @@ namespace nsg {
 // Stamp-program arrays of one circuit in the program pool.
 enum DcProgArray : int {
     DP_slot_ptr, DP_slot_terms, DP_rhs_ptr, DP_rhs_terms, DP_ucb_ptr, DP_ucb_terms,
-    DP_term_op, DP_term_param, DP_diodes, DP_caps, DP_srcs, DP_COUNT
+    DP_term_op, DP_term_param, DP_diodes, DP_caps, DP_srcs, DP_mos, DP_COUNT
 };
 
 struct DcDesc {
@@ -22,7 +22,8 @@ struct DcDesc {
     int32_t n_diodes;
     int32_t n_caps;
     int32_t n_srcs;      // waveform sources
-    int32_t n_states;    // per state vector (2 per capacitor)
+    int32_t n_mos;       // MOSFETs (level 1)
+    int32_t n_states;    // per state vector (2 per capacitor, 17 per MOSFET)
     int64_t prog_off[DP_COUNT];  // int32-word offsets into the program pool
     int64_t param_off;           // into the caller's parameter array
     int64_t sol_off;             // into the caller's solution array
@@ -31,6 +32,8 @@ struct DcDesc {
     int64_t x_off, xold_off, w_off, a_off, lu_off, tv_off, dstate_off, dconst_off;
     int64_t lrows_off, urows_off;  // row-major copies of L and U for the sweeps
     int64_t state_off;             // four state vectors of n_states doubles
+    int64_t mrec_off;              // per-MOSFET persistent load values
+    int64_t dcsave_off;            // gmin-stepping save area (x, state0..2, diode state)
 };
 
 // SimOptions of the reference (src/core/types.hpp:24-66) used by the loop.
@@ -47,8 +50,51 @@ struct NewtonOptions {
 constexpr int kDiodeTermCount = 5;
 constexpr int kCapTermCount = 4;
 constexpr int kSrcTermCount = 2;
+constexpr int kMosTermCount = 26;
+constexpr int kMosRecCount = 12;
 // CONSTKoverQ * 300.15 evaluated as the reference's diode temperature code does.
 constexpr double kKoverQTimesTnom = (1.38064852e-23 / 1.6021766208e-19) * 300.15;
+
+// Integrator context of one instance (IntegratorCtx, src/core/types.hpp:73-94),
+// written by thread 0, read by every thread after a barrier.
+struct IntegCtx {
+    double ag[3];
+    double xmu_ratio;
+    double delta;
+    double delta_old[3];
+    double time;      // source time (update_source_time)
+    int32_t mode;
+    int32_t order;
+    int32_t method;   // 0 trapezoidal, 1 Gear
+    int32_t pad;
+};
+
+// Solver state of one instance across newton() calls (NeoSolver's flag).
+struct SolverState {
+    int32_t factored;  // a numeric() has succeeded on this plan
+};
+
+// Operating-point phases (kernels/dc_op.cuh): the direct attempt, true gmin
+// stepping and its final solve, diagonal gmin stepping and its final solve.
+enum DcOpPhase : int32_t {
+    kOpDirect = 0,
+    kOpTrueGmin = 1,
+    kOpTrueGminFinal = 2,
+    kOpDiagGmin = 3,
+    kOpDiagGminFinal = 4,
+    kOpDone = 5,
+};
+
+// Operating-point controller of one instance, kept in global memory across
+// launches (zeroed by the host before a fresh run).
+struct DcCtl {
+    int32_t phase, total, code, ctx_mode;  // ctx_mode: mode of the next Newton call
+    int32_t active, r_iter, r_mode, r_devconv;  // Newton resume record
+    int32_t action, solves, method, pad;  // method: ConvergenceMethod of the result
+    double cur, factor, old, numeric_diag_gmin;  // stepping gmin, factor, OldGmin; diag_gmin of a stopped numeric()
+};
+
+enum : int32_t { kActNone = 0, kActZeroSave = 1, kActSave = 2, kActRestore = 3 };
 
 // Per-instance DC status.
 enum : int32_t {

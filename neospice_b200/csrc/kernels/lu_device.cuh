@@ -39,6 +39,7 @@ enum : int32_t {
     kStatusSingular = 102,  // exact zero pivot (SparseError::ZeroDiag)
     kStatusReorder = 103,   // pivot failed the relative threshold
     kStatusTimeout = 104,   // a bounded dependency wait gave up (no result)
+    kStatusNeedOrder = 105, // a solver's first numeric(): the host orders on this matrix
 };
 
 }  // namespace nsg

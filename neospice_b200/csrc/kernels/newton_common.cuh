@@ -4,6 +4,7 @@
 #include "dc_device.cuh"
 #include "diode_model.cuh"
 #include "lu_cta.cuh"
+#include "mos1_model.cuh"
 #include "source_wave.cuh"
 
 namespace nsg {
@@ -23,20 +24,6 @@ constexpr int kModeInitPred = 0x2000;
 constexpr int kModeUic = 0x10000;
 constexpr int kModeInitMask = 0x3F00;
 
-// Integrator context of one instance (IntegratorCtx, src/core/types.hpp:73-94),
-// written by thread 0, read by every thread after a barrier.
-struct IntegCtx {
-    double ag[3];
-    double xmu_ratio;
-    double delta;
-    double delta_old[3];
-    double time;      // source time (update_source_time)
-    int mode;
-    int order;
-    int method;       // 0 trapezoidal, 1 Gear
-    int pad;
-};
-
 // Views of one instance's program and workspace.
 struct Inst {
     const int32_t* slot_ptr;
@@ -50,6 +37,7 @@ struct Inst {
     const int32_t* diodes;  // (pos, neg, param)
     const int32_t* caps;    // (pos, neg, param, has_ic, state)
     const int32_t* srcs;    // (is_voltage, wave, param, nparam)
+    const int32_t* mos;     // (d, g, s, b, param, state)
     const double* par;
     double* x;
     double* xold;
@@ -61,7 +49,8 @@ struct Inst {
     double* dstate;
     double* dconst;
     double* st[4];          // capacitor state ring state0..state3
-    int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs;
+    double* mrec;           // per-MOSFET load values (kMosRecCount each)
+    int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs, n_mos;
 };
 
 __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const double* params,
@@ -78,6 +67,7 @@ __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const dou
     v.diodes = prog + d.prog_off[DP_diodes];
     v.caps = prog + d.prog_off[DP_caps];
     v.srcs = prog + d.prog_off[DP_srcs];
+    v.mos = prog + d.prog_off[DP_mos];
     v.par = params + d.param_off;
     v.x = work + d.x_off;
     v.xold = work + d.xold_off;
@@ -96,6 +86,8 @@ __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const dou
     v.n_diodes = d.n_diodes;
     v.n_caps = d.n_caps;
     v.n_srcs = d.n_srcs;
+    v.n_mos = d.n_mos;
+    v.mrec = work + d.mrec_off;
     return v;
 }
 
@@ -133,7 +125,7 @@ __device__ inline void load_constants(const Inst& v, double gmin) {
 // DC), capacitors (Capacitor::evaluate, state-vector path), waveform
 // sources (value_at).  Writes the dynamic terms; returns through s_dev_conv
 // whether every device reports convergence (diodes' CKTnoncon and conv_test).
-__device__ inline void eval_devices(const Inst& v, const IntegCtx& c, const NewtonOptions& opt,
+static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& c, const NewtonOptions& opt,
                                     int32_t* s_dev_conv) {
     const int mode = c.mode;
     double* tv_d = v.tv + v.n_const;
@@ -212,6 +204,19 @@ __device__ inline void eval_devices(const Inst& v, const IntegCtx& c, const Newt
             t[0] = t[1] = t[2] = t[3] = 0.0;
         }
     }
+    double* tv_m = tv_s + kSrcTermCount * v.n_srcs;
+    if (v.n_mos > 0) {
+        const Mos1Integ ic{c.ag[0], c.ag[1], c.ag[2], c.xmu_ratio, c.delta, c.delta_old[1],
+                           c.order, c.method};
+        for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
+            const int32_t* mr = v.mos + 6 * k;
+            double vn[4];
+            for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? v.xold[mr[q]] : 0.0;
+            const int32_t s = mr[5];
+            mos1_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
+                      v.st[2] + s, mode, ic, opt.gmin, vn, tv_m + kMosTermCount * k);
+        }
+    }
     for (int32_t k = threadIdx.x; k < v.n_srcs; k += blockDim.x) {
         const int32_t* sr = v.srcs + 4 * k;
         const double val = wave_value(sr[1], v.par + sr[2], sr[3], c.time);
@@ -236,53 +241,74 @@ __device__ inline void assemble(const Inst& v) {
     }
 }
 
-// Solver state of one instance across newton() calls (NeoSolver's flags).
-struct SolverState {
-    bool factored;  // a numeric() has succeeded on this plan
-};
-
 struct NewtonOutcome {
-    int32_t code;   // kDcConverged, kDcNoConvergence, kStatus*
+    int32_t code;       // kDcConverged, kDcNoConvergence, kStatus*
     int32_t iters;
+    int32_t fail_iter;  // kStatusReorder / kStatusNeedOrder: the 0-based iteration that stopped,
+    int32_t fail_mode;  // the mode it ran in
+    int32_t fail_dev_conv;  // and its device-load convergence verdict
 };
 
 // newton_solve (src/core/newton.cpp:51-419) for the whole CTA: x holds the
 // initial guess and receives the solution (the previous iterate on
-// convergence).  *ctx is the instance's integrator context in shared memory
-// (mode updated in place, restored on exit).
+// convergence).  *ctx is the instance's integrator context (mode updated in
+// place, restored to saved_mode on exit).
+//
+// A numeric() whose pivot re-validation fails (NeoSolver would re-order on
+// the host) ends the call with kStatusReorder, fail_iter, fail_mode and
+// fail_dev_conv, the term values of that iteration left in v.tv.  After the
+// host has re-ordered on that matrix, calling again with resume_iter =
+// fail_iter, resume_dev_conv = fail_dev_conv, ctx->mode = fail_mode and
+// saved_mode = the original call's mode continues the same Newton solve: the
+// matrix is re-assembled from v.tv (no device re-evaluation) and refactored
+// with the new pivots.  With host_orders_first the solver's first numeric()
+// stops the same way with kStatusNeedOrder, for the host to order a fresh
+// topology on that matrix.
 __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const int32_t* lu_pool,
                                        IntegCtx* ctx, const NewtonOptions& opt, int max_iter,
-                                       SolverState* solver, double* smem, int colbuf) {
+                                       SolverState* solver, double* smem, int colbuf,
+                                       int resume_iter = -1, int saved_mode = -1,
+                                       int resume_dev_conv = 1, bool host_orders_first = false) {
     __shared__ int32_t s_conv, s_dev_conv;
-    const int saved_mode = ctx->mode;
+    if (saved_mode < 0) saved_mode = ctx->mode;
     bool force_numeric = false;
-    NewtonOutcome out{kDcNoConvergence, max_iter};
+    NewtonOutcome out{kDcNoConvergence, max_iter, -1, 0, 1};
     __syncthreads();
-    for (int iter = 0; iter < max_iter; ++iter) {
-        for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.xold[i] = v.x[i];
-        if (threadIdx.x == 0) s_dev_conv = 1;
-        __syncthreads();
-        eval_devices(v, *ctx, opt, &s_dev_conv);
+    for (int iter = resume_iter < 0 ? 0 : resume_iter; iter < max_iter; ++iter) {
+        const bool resumed = (iter == resume_iter);
+        if (!resumed) {
+            for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.xold[i] = v.x[i];
+            if (threadIdx.x == 0) s_dev_conv = 1;
+            __syncthreads();
+            eval_devices(v, *ctx, opt, &s_dev_conv);
+        } else if (threadIdx.x == 0) {
+            s_dev_conv = resume_dev_conv;  // this iteration's loads ran before the host round trip
+        }
         __syncthreads();
         assemble(v);
         __syncthreads();
 
         const int mode = ctx->mode;
-        const bool numeric = force_numeric || (mode & kModeInitJct) || !solver->factored;
+        const bool numeric = resumed || force_numeric || (mode & kModeInitJct) || !solver->factored;
+        if (host_orders_first && numeric && !solver->factored && !resumed) {
+            out = {kStatusNeedOrder, iter + 1, iter, mode, s_dev_conv};
+            break;
+        }
         const RefactorResult fr =
-            cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, numeric && solver->factored,
-                              1e-3, smem, colbuf, v.lrows, v.urows);
+            cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin,
+                              numeric && solver->factored && !resumed, 1e-3, smem, colbuf,
+                              v.lrows, v.urows);
         if (fr.code == kStatusTimeout) {
-            out = {kStatusTimeout, iter + 1};
+            out = {kStatusTimeout, iter + 1, -1, 0, 1};
             break;
         }
         if (numeric) {
             if (fr.code != kStatusOk) {
                 // NeoSolver::numeric would re-order (103) or report singular.
-                out = {fr.code, iter + 1};
+                out = {fr.code, iter + 1, iter, mode, s_dev_conv};
                 break;
             }
-            solver->factored = true;
+            if (threadIdx.x == 0) solver->factored = 1;
             force_numeric = false;
         } else if (fr.code != kStatusOk) {
             force_numeric = true;  // newton.cpp:229-234: retry with numeric
@@ -291,7 +317,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             continue;
         }
         if (!cta_solve_flow(pd, lu_pool, v.lu, v.lrows, v.urows, v.x, smem)) {
-            out = {kStatusTimeout, iter + 1};
+            out = {kStatusTimeout, iter + 1, -1, 0, 1};
             break;
         }
 
@@ -309,13 +335,25 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             if (!ok) s_conv = 0;
         }
         __syncthreads();
+        if (v.n_mos > 0 && s_conv != 0 && iter > 0) {
+            // MOS1Device::device_converged(solution) on the new solution
+            for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
+                const int32_t* mr = v.mos + 6 * k;
+                double vn[4];
+                for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? v.x[mr[q]] : 0.0;
+                if (!mos1_converged(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + mr[5], vn,
+                                    opt.reltol, opt.abstol))
+                    s_dev_conv = 0;
+            }
+            __syncthreads();
+        }
         const bool conv = (s_conv != 0) && iter > 0 && (s_dev_conv != 0);
 
         bool done = false;
         if (mode & kModeInitFloat) {
             if (conv) {
                 for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
-                out = {kDcConverged, iter + 1};
+                out = {kDcConverged, iter + 1, -1, 0, 1};
                 done = true;
             }
         } else if (mode & kModeInitJct) {
@@ -330,7 +368,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             if (threadIdx.x == 0) ctx->mode = (mode & ~kModeInitMask) | kModeInitFloat;
         } else if (conv) {
             for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
-            out = {kDcConverged, iter + 1};
+            out = {kDcConverged, iter + 1, -1, 0, 1};
             done = true;
         }
         __syncthreads();
@@ -338,7 +376,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
     }
     __syncthreads();
     if (out.code != kDcConverged && out.code != kDcNoConvergence) {
-        // failure inside the loop: the caller's guess is the last iterate
+        // stopped inside the loop: the caller's guess is the last iterate
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];
     }
     if (threadIdx.x == 0) ctx->mode = saved_mode;

@@ -1,49 +1,64 @@
-// Batched DC operating point: the direct Newton attempt of solve_dc
-// (src/core/dc.cpp:53-118; newton_solve, src/core/newton.cpp:51-419) for one
-// circuit instance per CTA, all instances in a single launch.  Each
-// iteration: device loads, matrix and right-hand-side assembly from the stamp
-// program, fixed-pivot refactor (dataflow), forward/backward solve, the NIiter
-// convergence test and the INITJCT -> INITFIX -> INITFLOAT mode cascade.
+// Batched DC operating point: solve_dc (src/core/dc.cpp:53-175; newton_solve,
+// src/core/newton.cpp:51-419) with its direct attempt and the gmin-stepping
+// aids, for one circuit instance per CTA, all instances in a single launch.
+// Each iteration: device loads, matrix and right-hand-side assembly from the
+// stamp program, fixed-pivot refactor (dataflow), forward/backward solve, the
+// NIiter convergence test and the INITJCT -> INITFIX -> INITFLOAT cascade.
 // Instances converge and stop independently (per-instance convergence mask =
 // its CTA leaving the loop).
-#include "newton_common.cuh"
+#include "dc_op.cuh"
 
 #include <cuda_runtime.h>
 
 namespace nsg {
 
-// Two CTAs per SM: registers are capped at 64 per thread.
+// Two CTAs per SM: registers are capped at 64 per thread.  subset (optional)
+// lists the descriptor positions to run, one per block.  ctls[index] is the
+// instance's operating-point controller: zeroed by the host for a fresh run,
+// kept across launches when an instance stopped with kStatusReorder.
 __global__ void __launch_bounds__(kFlowThreads, 2)
 newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ lu_pool,
-                 const DcDesc* __restrict__ descs, const int32_t* __restrict__ prog,
-                 const double* __restrict__ params, double* __restrict__ work,
-                 double* __restrict__ solutions, int32_t* __restrict__ status,
-                 int32_t* __restrict__ iterations, NewtonOptions opt, int colbuf) {
+                 const DcDesc* __restrict__ descs, const int32_t* __restrict__ subset,
+                 const int32_t* __restrict__ prog, const double* __restrict__ params,
+                 double* __restrict__ work, double* __restrict__ solutions,
+                 int32_t* __restrict__ status, int32_t* __restrict__ iterations,
+                 DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf) {
     extern __shared__ double smem[];
-    const DcDesc d = descs[blockIdx.x];
+    const DcDesc d = descs[subset ? subset[blockIdx.x] : blockIdx.x];
     const PlanDesc& pd = plans[d.plan];
     const Inst v = make_inst(d, prog, params, work);
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
+    __shared__ int32_t s_fresh;
+    DcCtl* ctl = ctls + d.index;
+    constexpr int kFirst = kModeDcOp | kModeInitJct, kCont = kModeDcOp | kModeInitFloat;
 
-    load_constants(v, opt.gmin);
-    for (int32_t k = threadIdx.x; k < 3 * v.n_diodes; k += blockDim.x) v.dstate[k] = 0.0;
-    for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;
+    if (threadIdx.x == 0) s_fresh = (ctl->active == 0);
+    __syncthreads();
+    const bool fresh = s_fresh != 0;
+    if (fresh) {
+        for (int32_t k = threadIdx.x; k < 3 * v.n_diodes; k += blockDim.x) v.dstate[k] = 0.0;
+        for (int32_t k = threadIdx.x; k < kMosRecCount * v.n_mos; k += blockDim.x) v.mrec[k] = 0.0;
+        for (int32_t k = threadIdx.x; k < 4 * d.n_states; k += blockDim.x) v.st[0][k] = 0.0;
+        for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;
+    }
     if (threadIdx.x == 0) {
+        if (fresh) dc_op_start(ctl, kFirst);
         ctx = IntegCtx{};
-        ctx.mode = kModeDcOp | kModeInitJct;  // solve_dc (dc.cpp:104)
         ctx.order = 1;
         ctx.time = 0.0;
-        solver.factored = false;
+        solver.factored = fresh ? 0 : 1;
     }
     __syncthreads();
-    const NewtonOutcome r = newton(v, pd, lu_pool, &ctx, opt, opt.max_iter, &solver, smem, colbuf);
+    // solve_dc (dc.cpp:53-175): direct attempt, true gmin stepping, gmin stepping
+    const int32_t code = dc_operating_point(v, d.n_states, pd, lu_pool, &ctx, &solver, ctl, opt,
+                                            kFirst, kCont, true, work + d.dcsave_off, smem, colbuf);
 
     double* out = solutions + d.sol_off;
     for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) out[i] = v.x[i];
     if (threadIdx.x == 0) {
-        status[d.index] = r.code;
-        iterations[d.index] = r.iters;
+        status[d.index] = code;
+        iterations[d.index] = ctl->total;
     }
 }
 
@@ -55,8 +70,9 @@ size_t dc_smem_bytes(int max_col, int max_n) {
 }
 
 cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
-                             int count, const int32_t* prog, const double* params, double* work,
-                             double* solutions, int32_t* status, int32_t* iterations,
+                             const int32_t* subset, int count, const int32_t* prog,
+                             const double* params, double* work, double* solutions,
+                             int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
                              cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
@@ -71,9 +87,9 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    newton_dc_kernel<<<count, kFlowThreads, smem, stream>>>(plans, lu_pool, descs, prog, params,
-                                                             work, solutions, status, iterations,
-                                                             opt, colbuf);
+    newton_dc_kernel<<<count, kFlowThreads, smem, stream>>>(plans, lu_pool, descs, subset, prog,
+                                                             params, work, solutions, status,
+                                                             iterations, ctls, opt, colbuf);
     return cudaGetLastError();
 }
 

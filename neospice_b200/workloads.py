@@ -84,15 +84,20 @@ class Netlist:
     ("R", a, b, ohms), ("C", a, b, farads), ("V", p, n, volts),
     ("I", p, n, amps), ("VPULSE"|"IPULSE", p, n, v1, v2, td, tr, tf, pw, per),
     ("VPWL"|"IPWL", p, n, t0, v0, t1, v1, ...), ("D", anode, cathode, IS, N).
-    Node -1 is ground."""
+    ("M", d, g, s, b, model_name, W, L) with models[model_name] =
+    ("nmos"|"pmos", {param: value}) (level-1 cards).  Node -1 is ground."""
     num_nodes: int
     devices: list
+    models: dict = dataclasses.field(default_factory=dict)
 
     def build(self) -> Circuit:
         c = Circuit(self.num_nodes)
+        mid = {name: c.model_mos1(t, **p) for name, (t, p) in self.models.items()}
         for d in self.devices:
             kind, a, b, vals = d[0], d[1], d[2], d[3:]
-            if kind == "R":
+            if kind == "M":
+                c.M(a, b, vals[0], vals[1], mid[vals[2]], vals[3], vals[4])
+            elif kind == "R":
                 c.R(a, b, vals[0])
             elif kind == "C":
                 c.C(a, b, vals[0], vals[1] if len(vals) > 1 else None)
@@ -142,3 +147,47 @@ def rc_tree(rng: np.random.Generator, nodes: int, r_ohm=50.0, c_farad=2e-15, sig
     for k in range(nodes):
         dev.append(("C", k, GND, float(cc[k])))
     return Netlist(nodes + 1, dev)
+
+
+def inverter_chain(stages: int, vin=0.0, vdd=1.8, c_load=10e-15, pulse=None) -> Netlist:
+    """A chain of `stages` CMOS inverters (level-1: NMOS VTO=0.7 KP=110u
+    W/L=2u/1u, PMOS VTO=-0.7 KP=50u W/L=4u/1u), a load capacitor per stage
+    output, VDD on node 0, the input on node 1 (a DC value, or
+    pulse=(v1, v2, td, tr, tf, pw, per)), stage k's output on node k+2."""
+    models = {"nch": ("nmos", {"VTO": 0.7, "KP": 110e-6}),
+              "pch": ("pmos", {"VTO": -0.7, "KP": 50e-6})}
+    dev = [("V", 0, GND, vdd)]
+    dev.append(("VPULSE", 1, GND, *pulse) if pulse is not None else ("V", 1, GND, vin))
+    for k in range(stages):
+        i, o = k + 1, k + 2
+        dev.append(("M", o, i, GND, GND, "nch", 2e-6, 1e-6))
+        dev.append(("M", o, i, 0, 0, "pch", 4e-6, 1e-6))
+        dev.append(("C", o, GND, c_load))
+    return Netlist(stages + 2, dev, models)
+
+
+def mos_network(rng: np.random.Generator, nodes: int, vdd=1.8, pulse=None) -> Netlist:
+    """A seeded MOS network: VDD on node 0, an input on node 1 (a random DC
+    level, or a PULSE), and for every further node an NMOS pull-down and a
+    PMOS pull-up whose gates hang from random earlier nodes, a resistor to a
+    random earlier node and a capacitor to ground.  The cards exercise body
+    effect, channel-length modulation, lateral diffusion and oxide-derived
+    parameters."""
+    models = {
+        "n1": ("nmos", {"VTO": 0.6, "KP": 120e-6, "GAMMA": 0.4, "PHI": 0.7, "LAMBDA": 0.05,
+                        "LD": 5e-8}),
+        "p1": ("pmos", {"VTO": -0.65, "KP": 45e-6, "GAMMA": 0.5, "LAMBDA": 0.08}),
+        "n2": ("nmos", {"TOX": 2e-8, "NSUB": 1e16, "U0": 500, "LAMBDA": 0.02}),
+    }
+    vin = float(rng.uniform(0, vdd))
+    dev = [("V", 0, GND, vdd),
+           ("VPULSE", 1, GND, *pulse) if pulse is not None else ("V", 1, GND, vin)]
+    for k in range(2, nodes):
+        g1, g2 = int(rng.integers(1, k)), int(rng.integers(1, k))
+        nm = "n1" if rng.random() < 0.6 else "n2"
+        dev.append(("M", k, g1, GND, GND, nm, float(rng.uniform(1e-6, 4e-6)), 1e-6))
+        dev.append(("M", k, g2, 0, 0, "p1", float(rng.uniform(2e-6, 8e-6)), 1e-6))
+        dev.append(("R", k, int(rng.integers(1, k)),
+                    float(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))))
+        dev.append(("C", k, GND, 1e-14))
+    return Netlist(nodes, dev, models)

@@ -80,6 +80,8 @@ def ref() -> ctypes.CDLL:
         lib.nsref_sim_error.restype = ctypes.c_char_p
         lib.nsref_sim_error.argtypes = [_V]
         lib.nsref_sim_free.argtypes = [_V]
+        lib.nsref_sim_initjct.argtypes = [ctypes.c_char_p, _V, _V, _V, _V, _V]
+        lib.nsref_sim_method.argtypes = [_V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
         _ref = lib
@@ -219,6 +221,24 @@ def ref_mesh_initjct(m):
     return cp, ri, vals, rhs
 
 
+def ref_sim_initjct(desc: str):
+    """The reference's first DC Newton matrix of a described circuit:
+    (col_ptr, row_idx, values, rhs)."""
+    lib = ref()
+    nv = ctypes.c_int(0)
+    d = desc.encode()
+    nnz = lib.nsref_sim_initjct(d, ctypes.addressof(nv), None, None, None, None)
+    if nnz < 0:
+        raise RuntimeError("reference INITJCT evaluation failed")
+    cp = np.zeros(nv.value + 1, np.int32)
+    ri = np.zeros(nnz, np.int32)
+    vals = np.zeros(nnz)
+    rhs = np.zeros(nv.value)
+    if lib.nsref_sim_initjct(d, ctypes.addressof(nv), _p(cp), _p(ri), _p(vals), _p(rhs)) != nnz:
+        raise RuntimeError("reference INITJCT evaluation failed")
+    return cp, ri, vals, rhs
+
+
 def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0):
     """Run a circuit description (see nsref_sim_run in ref_shim.cpp) through
     the reference: analysis 0 = DC operating point, 1 = transient.  Returns
@@ -237,7 +257,8 @@ def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0
         values = np.zeros((npts.value, width))
         lib.nsref_sim_copy(h, _p(times), _p(values))
         info = dict(num_nodes=nn.value, num_vars=nv.value, points=npts.value,
-                    iterations=it.value, seconds=sec.value, rejected=rej.value)
+                    iterations=it.value, seconds=sec.value, rejected=rej.value,
+                    method=lib.nsref_sim_method(h))
         return times, values, info
     finally:
         lib.nsref_sim_free(h)

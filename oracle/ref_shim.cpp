@@ -289,7 +289,7 @@ int nsref_mesh_initjct(int side, const double* r_h, const double* r_v, int n_dio
 // Node -1 is ground.  analysis 0 = DC operating point, 1 = transient.
 struct SimResult {
     std::string error;
-    int num_nodes = 0, num_vars = 0, iterations = 0, rejected = 0;
+    int num_nodes = 0, num_vars = 0, iterations = 0, rejected = 0, method = 0;
     double seconds = 0.0;
     std::vector<double> times;
     std::vector<double> values;  // npoints x (num_vars for DC, num_nodes for tran)
@@ -299,94 +299,100 @@ static NodeId node_of(const std::vector<NodeId>& nodes, int k) {
     return k < 0 ? GND : nodes.at(k);
 }
 
+// Build a circuit from a description (format above) through the typed API.
+static void build_from_desc(Circuit& ckt, const char* desc) {
+    // Tokenised by hand (strtod/strtol): iostreams are avoided because
+    // the loading process may carry a different C++ runtime.
+    std::vector<std::vector<std::string>> lines;
+    {
+        std::vector<std::string> cur;
+        std::string tok;
+        for (const char* p = desc;; ++p) {
+            const char c = *p;
+            if (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\0') {
+                if (!tok.empty()) cur.push_back(tok), tok.clear();
+                if ((c == '\n' || c == '\0') && !cur.empty()) lines.push_back(cur), cur.clear();
+                if (c == '\0') break;
+            } else {
+                tok.push_back(c);
+            }
+        }
+    }
+    std::vector<NodeId> nodes;
+    int dev = 0;
+    for (const auto& tk : lines) {
+        const std::string& kind = tk[0];
+        const std::string name = kind + std::to_string(dev++);
+        auto I_ = [&](size_t k) { return static_cast<int>(std::strtol(tk.at(k).c_str(), nullptr, 10)); };
+        auto D_ = [&](size_t k) { return std::strtod(tk.at(k).c_str(), nullptr); };
+        auto rest = [&](size_t from) {
+            std::vector<double> v;
+            for (size_t k = from; k < tk.size(); ++k) v.push_back(D_(k));
+            return v;
+        };
+        if (kind == "nodes") {
+            const int n = I_(1);
+            for (int i = 0; i < n; ++i) nodes.push_back(ckt.node("n" + std::to_string(i)));
+        } else if (kind == "R" || kind == "C" || kind == "V" || kind == "I") {
+            NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
+            auto v = rest(3);
+            if (kind == "R") ckt.R(name, a, b, v.at(0));
+            else if (kind == "C") {
+                if (v.size() > 1) ckt.C(name, a, b, v[0], v[1]);
+                else ckt.C(name, a, b, v.at(0));
+            } else if (kind == "V") ckt.V(name, a, b, v.at(0));
+            else ckt.I(name, a, b, v.at(0));
+        } else if (kind == "VPULSE" || kind == "IPULSE" || kind == "VPWL" || kind == "IPWL") {
+            NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
+            auto v = rest(3);
+            const bool is_v = kind[0] == 'V';
+            DevId id = is_v ? ckt.V(name, a, b, 0.0) : ckt.I(name, a, b, 0.0);
+            Device* d = ckt.devices()[static_cast<int32_t>(id)].get();
+            if (kind == "VPULSE" || kind == "IPULSE") {
+                PulseParams pp{v.at(0), v.at(1), v.at(2), v.at(3), v.at(4), v.at(5), v.at(6)};
+                if (is_v) static_cast<VSource*>(d)->set_pulse(pp);
+                else static_cast<ISource*>(d)->set_pulse(pp);
+            } else {
+                PwlParams pw;
+                for (size_t k = 0; k + 1 < v.size(); k += 2) pw.points.emplace_back(v[k], v[k + 1]);
+                if (is_v) static_cast<VSource*>(d)->set_pwl(pw);
+                else static_cast<ISource*>(d)->set_pwl(pw);
+            }
+        } else if (kind == "D") {
+            char card[160];
+            std::snprintf(card, sizeof card, ".model dm%d D(IS=%.17g N=%.17g)", dev, D_(3), D_(4));
+            ckt.model(card);
+            ckt.D(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), "dm" + std::to_string(dev));
+        } else if (kind == "MODEL") {
+            std::string card;
+            for (size_t k = 1; k < tk.size(); ++k) card += (k > 1 ? " " : "") + tk[k];
+            ckt.model(card);
+        } else if (kind == "M") {
+            ckt.M(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), node_of(nodes, I_(3)),
+                  node_of(nodes, I_(4)), tk.at(5), D_(6), D_(7));
+        } else if (kind == "OPT") {
+            const std::string& key = tk.at(1);
+            const double val = D_(2);
+            if (key == "reltol") ckt.options.reltol = val;
+            else if (key == "abstol") ckt.options.abstol = val;
+            else if (key == "vntol") ckt.options.vntol = val;
+            else if (key == "gmin") ckt.options.gmin = val;
+            else if (key == "itl4") ckt.options.itl4 = static_cast<int>(val);
+            else if (key == "gear") ckt.options.method = val != 0.0 ? "gear" : "trap";
+            else if (key == "verbose") ckt.options.verbose = val != 0.0;
+        } else {
+            throw std::invalid_argument("unknown line kind: " + kind);
+        }
+    }
+    ckt.finalize_if_needed();
+}
+
 void* nsref_sim_run(const char* desc, int analysis, double tstep, double tstop) {
     auto* res = new SimResult;
     try {
         auto t0 = std::chrono::steady_clock::now();
         Circuit ckt;
-        // Tokenised by hand (strtod/strtol): iostreams are avoided because
-        // the loading process may carry a different C++ runtime.
-        std::vector<std::vector<std::string>> lines;
-        {
-            std::vector<std::string> cur;
-            std::string tok;
-            for (const char* p = desc;; ++p) {
-                const char c = *p;
-                if (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\0') {
-                    if (!tok.empty()) cur.push_back(tok), tok.clear();
-                    if ((c == '\n' || c == '\0') && !cur.empty()) lines.push_back(cur), cur.clear();
-                    if (c == '\0') break;
-                } else {
-                    tok.push_back(c);
-                }
-            }
-        }
-        std::vector<NodeId> nodes;
-        int dev = 0;
-        for (const auto& tk : lines) {
-            const std::string& kind = tk[0];
-            const std::string name = kind + std::to_string(dev++);
-            auto I_ = [&](size_t k) { return static_cast<int>(std::strtol(tk.at(k).c_str(), nullptr, 10)); };
-            auto D_ = [&](size_t k) { return std::strtod(tk.at(k).c_str(), nullptr); };
-            auto rest = [&](size_t from) {
-                std::vector<double> v;
-                for (size_t k = from; k < tk.size(); ++k) v.push_back(D_(k));
-                return v;
-            };
-            if (kind == "nodes") {
-                const int n = I_(1);
-                for (int i = 0; i < n; ++i) nodes.push_back(ckt.node("n" + std::to_string(i)));
-            } else if (kind == "R" || kind == "C" || kind == "V" || kind == "I") {
-                NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
-                auto v = rest(3);
-                if (kind == "R") ckt.R(name, a, b, v.at(0));
-                else if (kind == "C") {
-                    if (v.size() > 1) ckt.C(name, a, b, v[0], v[1]);
-                    else ckt.C(name, a, b, v.at(0));
-                } else if (kind == "V") ckt.V(name, a, b, v.at(0));
-                else ckt.I(name, a, b, v.at(0));
-            } else if (kind == "VPULSE" || kind == "IPULSE" || kind == "VPWL" || kind == "IPWL") {
-                NodeId a = node_of(nodes, I_(1)), b = node_of(nodes, I_(2));
-                auto v = rest(3);
-                const bool is_v = kind[0] == 'V';
-                DevId id = is_v ? ckt.V(name, a, b, 0.0) : ckt.I(name, a, b, 0.0);
-                Device* d = ckt.devices()[static_cast<int32_t>(id)].get();
-                if (kind == "VPULSE" || kind == "IPULSE") {
-                    PulseParams pp{v.at(0), v.at(1), v.at(2), v.at(3), v.at(4), v.at(5), v.at(6)};
-                    if (is_v) static_cast<VSource*>(d)->set_pulse(pp);
-                    else static_cast<ISource*>(d)->set_pulse(pp);
-                } else {
-                    PwlParams pw;
-                    for (size_t k = 0; k + 1 < v.size(); k += 2) pw.points.emplace_back(v[k], v[k + 1]);
-                    if (is_v) static_cast<VSource*>(d)->set_pwl(pw);
-                    else static_cast<ISource*>(d)->set_pwl(pw);
-                }
-            } else if (kind == "D") {
-                char card[160];
-                std::snprintf(card, sizeof card, ".model dm%d D(IS=%.17g N=%.17g)", dev, D_(3), D_(4));
-                ckt.model(card);
-                ckt.D(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), "dm" + std::to_string(dev));
-            } else if (kind == "MODEL") {
-                std::string card;
-                for (size_t k = 1; k < tk.size(); ++k) card += (k > 1 ? " " : "") + tk[k];
-                ckt.model(card);
-            } else if (kind == "M") {
-                ckt.M(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), node_of(nodes, I_(3)),
-                      node_of(nodes, I_(4)), tk.at(5), D_(6), D_(7));
-            } else if (kind == "OPT") {
-                const std::string& key = tk.at(1);
-                const double val = D_(2);
-                if (key == "reltol") ckt.options.reltol = val;
-                else if (key == "abstol") ckt.options.abstol = val;
-                else if (key == "vntol") ckt.options.vntol = val;
-                else if (key == "gmin") ckt.options.gmin = val;
-                else if (key == "itl4") ckt.options.itl4 = static_cast<int>(val);
-                else if (key == "gear") ckt.options.method = val != 0.0 ? "gear" : "trap";
-            } else {
-                throw std::invalid_argument("unknown line kind: " + kind);
-            }
-        }
-        ckt.finalize_if_needed();
+        build_from_desc(ckt, desc);
         res->num_nodes = ckt.num_nodes();
         res->num_vars = ckt.num_vars();
         if (analysis == 0) {
@@ -396,6 +402,7 @@ void* nsref_sim_run(const char* desc, int analysis, double tstep, double tstop) 
             res->times.push_back(0.0);
             res->values.assign(op->begin(), op->end());
             res->iterations = r.status.iterations;
+            res->method = static_cast<int>(r.status.convergence_method);
         } else {
             TransientResult r = solve_transient(ckt, tstep, tstop);
             res->times = r.time;
@@ -437,3 +444,44 @@ const char* nsref_sim_error(void* h) { return static_cast<SimResult*>(h)->error.
 void nsref_sim_free(void* h) { delete static_cast<SimResult*>(h); }
 
 }  // extern "C"
+
+// The matrix and rhs of the first DC Newton iteration of a described circuit
+// (as nsref_mesh_initjct).  Returns nnz, or -1.
+extern "C" int nsref_sim_initjct(const char* desc, int* num_vars, int* col_ptr, int* row_idx,
+                                 double* values, double* rhs_out) {
+    try {
+        Circuit ckt;
+        build_from_desc(ckt, desc);
+        const int n = ckt.num_vars();
+        const auto& pattern = ckt.pattern();
+        if (num_vars) *num_vars = n;
+        if (!col_ptr) return pattern.nnz();
+        CSCData csc = pattern.to_csc();
+        for (int j = 0; j <= n; ++j) col_ptr[j] = csc.col_ptr[j];
+        for (int k = 0; k < pattern.nnz(); ++k) row_idx[k] = csc.row_idx[k];
+        ckt.integrator_ctx.options = &ckt.options;
+        ckt.integrator_ctx.mode = 0x10 | 0x200;  // MODEDCOP | MODEINITJCT
+        NumericMatrix mat(pattern);
+        std::vector<double> solution(n, 0.0), rhs(n, 0.0);
+        std::vector<double> ob_sol(n + 1, 0.0), ob_rhs(n + 1, 0.0);
+        OneBasedEvalArrays arrays{ob_sol.data(), ob_rhs.data(), n + 1};
+        tls_integrator_ctx = &ckt.integrator_ctx;
+        tls_one_based_eval_arrays = &arrays;
+        for (Device* dev : ckt.device_load_order()) dev->evaluate(solution, mat, rhs);
+        tls_one_based_eval_arrays = nullptr;
+        tls_integrator_ctx = nullptr;
+        for (int i = 0; i < n; ++i) rhs[i] += ob_rhs[i + 1];
+        const double pin = (ckt.options.gmin > 0.0) ? ckt.options.gmin : 1e-12;
+        for (int32_t idx : ckt.dead_node_indices()) mat.add(pattern.offset(idx, idx), pin);
+        for (int k = 0; k < pattern.nnz(); ++k) values[k] = mat.data()[k];
+        for (int i = 0; i < n; ++i) rhs_out[i] = rhs[i];
+        return pattern.nnz();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_sim_initjct: %s\n", e.what());
+        return -1;
+    }
+}
+
+// The DC convergence method of a finished run (ConvergenceMethod as an int:
+// 0 = the direct Newton attempt, 1 = gmin stepping).
+extern "C" int nsref_sim_method(void* h) { return static_cast<SimResult*>(h)->method; }

@@ -9,10 +9,15 @@ LU pattern, slot map), the factored values, the values after
 NeoSolver::refactorize on perturbed values, and the solutions of solve and
 solve_transposed.
 
-tran_rc.npz: seeded linear RC netlists (neospice_b200.workloads) with PULSE
-and PWL sources, per case the device list (JSON), tstep/tstop, and the
+tran_rc.npz: seeded RC netlists, CMOS inverter chains and MOS networks
+(neospice_b200.workloads) with PULSE and PWL sources, per case the device
+list and model cards (JSON), tstep/tstop, and the
 reference's solve_transient output: every timepoint, all node voltages,
 total Newton iterations and rejected steps.
+
+mos_dc.npz: CMOS inverter chains and seeded MOS networks, per case the
+netlist (JSON) and the reference's solve_dc operating point, Newton
+iteration count and convergence method (0 direct, 1 gmin stepping).
 
 mesh_dc.npz: seeded diode-clamped meshes (neospice_b200.workloads), per case
 the mesh, the reference's first-iteration matrix and rhs, and its DC
@@ -113,6 +118,14 @@ def tran_netlists():
         cases.append((W.rc_ladder(np.random.default_rng([33, k]), stages), tstep, tstop))
     for k, (nodes, tstep, tstop) in enumerate(((25, 1e-11, 3e-10), (60, 2e-11, 1e-9))):
         cases.append((W.rc_tree(np.random.default_rng([34, k]), nodes), tstep, tstop))
+    # CMOS inverter chains and MOS networks driven by a pulse (the 10-stage
+    # chain's operating point needs gmin stepping).
+    pulse = (0.0, 1.8, 0.0, 1e-10, 1e-10, 1e-9, 2e-9)
+    cases.append((W.inverter_chain(3, pulse=pulse), 2e-12, 2e-9))
+    cases.append((W.inverter_chain(5, pulse=pulse), 5e-12, 4e-9))
+    cases.append((W.inverter_chain(10, pulse=pulse), 1e-11, 2e-9))
+    cases.append((W.mos_network(np.random.default_rng([51, 0]), 6, pulse=pulse), 5e-12, 2e-9))
+    cases.append((W.mos_network(np.random.default_rng([51, 1]), 9, pulse=pulse), 1e-11, 3e-9))
     # PWL current load into an RC node, a DC source through R, one capacitor
     # with an initial condition, a PULSE with default rise/fall/width/period.
     cases.append((W.Netlist(4, [
@@ -124,6 +137,36 @@ def tran_netlists():
     return cases
 
 
+def mos_netlists():
+    """DC cases of mos_dc.npz: CMOS inverter chains at several input levels
+    (the longer ones need gmin stepping) and seeded MOS networks with body
+    effect, channel-length modulation and oxide-derived parameters."""
+    from neospice_b200 import workloads as W
+    cases = []
+    for stages, vin in ((1, 0.0), (2, 0.5), (3, 0.9), (4, 0.75), (5, 1.3), (8, 1.8), (12, 0.0)):
+        cases.append(W.inverter_chain(stages, vin))
+    for k in range(6):
+        cases.append(W.mos_network(np.random.default_rng([41, k]), int(4 + 3 * k)))
+    return cases
+
+
+def mos_main():
+    import json
+    import netlists
+    rec = {}
+    cases = mos_netlists()
+    for k, nl in enumerate(cases):
+        _, v, info = oracle.ref_sim(netlists.ref_desc(nl), 0)
+        p = f"d{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "solution": v[0], p + "iterations": np.int32(info["iterations"]),
+                    p + "method": np.int32(info["method"])})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("mos_dc.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} MOS operating points to {path}")
+
+
 def tran_main():
     import json
     import netlists
@@ -132,7 +175,7 @@ def tran_main():
     for k, (nl, tstep, tstop) in enumerate(cases):
         t, v, info = oracle.ref_sim(netlists.ref_desc(nl), 1, tstep, tstop)
         p = f"t{k:02d}_"
-        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices])),
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
                     p + "tstep": np.float64(tstep), p + "tstop": np.float64(tstop),
                     p + "times": t, p + "values": v,
                     p + "iterations": np.int32(info["iterations"]),
@@ -144,10 +187,12 @@ def tran_main():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos"]
     if "solver" in which:
         main()
     if "mesh" in which:
         mesh_main()
     if "tran" in which:
         tran_main()
+    if "mos" in which:
+        mos_main()

@@ -47,7 +47,26 @@ def load_transients():
     for k in range(int(z["count"])):
         p = f"t{k:02d}_"
         d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
-        nn, dev = json.loads(str(d["netlist"]))
-        d["netlist"] = Netlist(nn, [tuple(x) for x in dev])
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        out.append(d)
+    return out
+
+
+MOS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "mos_dc.npz"
+
+
+def load_mos_dc():
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(MOS_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"d{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
         out.append(d)
     return out

@@ -132,3 +132,31 @@ def test_tran_batch_rejects_diodes_and_bad_probes():
     d.finalize()
     with pytest.raises(L.NsgError, match="probe"):
         TranBatch([d], 1e-12, 1e-10, [7])
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built here")
+def test_mos_first_matrix_matches_reference():
+    """MOS1load at MODEDCOP | MODEINITJCT on the host: pattern, matrix and
+    rhs bit-identical to the reference's first Newton iteration."""
+    import netlists
+    for g in golden_cases.load_mos_dc():
+        nl = g["netlist"]
+        cp, ri, a, r = oracle.ref_sim_initjct(netlists.ref_desc(nl))
+        c = nl.build()
+        cp2, ri2 = c.pattern()
+        a2, r2 = c.initial_matrix()
+        np.testing.assert_array_equal(cp2, cp)
+        np.testing.assert_array_equal(ri2, ri)
+        np.testing.assert_array_equal(a2, a)
+        np.testing.assert_array_equal(r2, r)
+
+
+def test_mos_model_card_validation():
+    c = Circuit(3)
+    with pytest.raises(L.NsgError, match="unknown parameter"):
+        c.model_mos1("nmos", VTO=0.7, BOGUS=1.0)
+    with pytest.raises(L.NsgError, match="not supported"):
+        c.model_mos1("nmos", VTO=0.7, RD=10.0)
+    m = c.model_mos1("nmos", VTO=0.7, KP=1e-4, RD=0.0)
+    with pytest.raises(L.NsgError, match="W > 0"):
+        c.M(0, 1, 2, -1, m, 0.0, 1e-6)
