@@ -270,12 +270,13 @@ int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves);
 /* ---- Batched transient analysis (device) ------------------------------------
  * solve_transient (src/core/transient.cpp:694-1067) for `count` circuits in one
  * launch, one thread block per circuit, each with its own adaptive timestep:
- * DC operating point (MODETRANOP), then the accept/reject loop of
- * TimeStepController (src/core/timestep.cpp) with trapezoidal / backward-Euler
- * capacitor companions and the capacitor truncation-error estimate.  The DC
- * solver and the transient solver are ordered separately on their own first
- * matrices, as the reference creates two solvers.  Circuits may hold R, C,
- * DC/PULSE/PWL V and I sources (no diodes).  Every accepted timepoint (and
+ * DC operating point (MODETRANOP, with gmin stepping when the direct attempt
+ * fails), then the accept/reject loop of TimeStepController
+ * (src/core/timestep.cpp) with trapezoidal / Gear / backward-Euler charge
+ * integration and the truncation-error estimate of every charge state.  The
+ * DC solver and the transient solver are ordered separately on their own
+ * first matrices, as the reference creates two solvers.  Circuits may hold
+ * R, C, DC/PULSE/PWL V and I sources and level-1 MOSFETs (no diodes).  Every accepted timepoint (and
  * t = 0) is written for the `nprobe` unknowns in probes[], at most max_points
  * per circuit. */
 typedef struct nsg_tran_batch nsg_tran_batch;
@@ -284,7 +285,12 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                           int max_points, int nprobe, const int* probes, int threads,
                           nsg_tran_batch** out);
 void nsg_tran_batch_free(nsg_tran_batch* b);
-/* Launch the whole batch on a stream (asynchronous). */
+/* Run the whole batch on a stream.  Instances stop for the host when a
+ * solver needs ordering -- the transient solver on the first transient
+ * iteration's matrix as the device computes it, either solver after a failed
+ * pivot re-validation -- so the call waits for the stream, orders those
+ * instances as NeoSolver::numeric does and resumes them; it returns when
+ * every instance has finished. */
 int nsg_tran_batch_run(nsg_tran_batch* b, void* stream);
 /* Wait for the device and copy results to host arrays (any may be NULL):
  * times [count*max_points], values [count*max_points*nprobe] (point-major),
@@ -295,6 +301,9 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream);
  * DC failure code). */
 int nsg_tran_batch_results(const nsg_tran_batch* b, double* times, double* values, int* npoints,
                            int* status, int* stats);
+/* Host orderings done so far: the transient solver's first ordering per
+ * instance plus every re-ordering after a failed pivot re-validation. */
+int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count);
 
 #ifdef __cplusplus
 }

@@ -91,6 +91,7 @@ SIGNATURES = {
     "nsg_tran_batch_create": (c_int, [c_int, P(c_void_p), c_double, c_double, c_int, c_int,
                                       P(c_int), c_int, P(c_void_p)]),
     "nsg_tran_batch_free": (None, [c_void_p]),
+    "nsg_tran_batch_orderings": (c_int, [c_void_p, P(c_ll)]),
     "nsg_tran_batch_run": (c_int, [c_void_p, c_void_p]),
     "nsg_tran_batch_results": (c_int, [c_void_p, P(c_double), P(c_double), P(c_int), P(c_int),
                                        P(c_int)]),

@@ -265,6 +265,11 @@ class TranBatch:
             getattr(stream, "cuda_stream", stream)
         L.check(L.lib().nsg_tran_batch_run(self._h, sp))
 
+    def orderings(self) -> int:
+        n = ctypes.c_longlong()
+        L.check(L.lib().nsg_tran_batch_orderings(self._h, ctypes.byref(n)))
+        return n.value
+
     def results(self):
         """Per circuit: dict(time, values [points x probes], status, steps,
         rejected, newton_iters)."""

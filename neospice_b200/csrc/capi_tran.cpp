@@ -13,10 +13,11 @@
 
 namespace nsg {
 cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
-                             const TranDesc* tdescs, int count, const int32_t* prog,
-                             const double* params_dc, const double* params_tran, double* work,
-                             const double* bps, const int32_t* probes, double* times,
-                             double* values, int32_t* npoints, int32_t* status, int32_t* stats,
+                             const TranDesc* tdescs, const int32_t* subset, int count,
+                             const int32_t* prog, const double* params_dc,
+                             const double* params_tran, double* work, const double* bps,
+                             const int32_t* probes, double* times, double* values,
+                             int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
                              const TranOptions& o, int max_col, int max_n, cudaStream_t stream);
 size_t tran_smem_bytes(int max_col, int max_n);
 }  // namespace nsg
@@ -27,9 +28,12 @@ struct nsg_tran_batch {
     int count = 0;
     nsg::TranOptions opt{};
     std::vector<std::unique_ptr<nsg_topology>> topos;
-    std::vector<long long> param_off;
-    std::vector<double> host_params;
+    std::vector<nsg::DcDesc> descs;      // launch order = instance order
+    std::vector<nsg::TranDesc> tdescs;
+    std::vector<std::vector<int32_t>> col_ptr, row_idx;  // per-instance pattern
     int max_col = 0, max_n = 0;
+    int64_t work_size = 0, work_cap = 0;
+    long long orderings = 0;
     int32_t* d_lu_pool = nullptr;
     nsg::PlanDesc* d_plans = nullptr;
     int32_t* d_prog = nullptr;
@@ -45,6 +49,8 @@ struct nsg_tran_batch {
     int32_t* d_npoints = nullptr;
     int32_t* d_status = nullptr;
     int32_t* d_stats = nullptr;
+    nsg::TranCtl* d_ctl = nullptr;
+    int32_t* d_subset = nullptr;
     ~nsg_tran_batch() {
         for (void* p : {static_cast<void*>(d_lu_pool), static_cast<void*>(d_plans),
                         static_cast<void*>(d_prog), static_cast<void*>(d_descs),
@@ -53,7 +59,8 @@ struct nsg_tran_batch {
                         static_cast<void*>(d_bps), static_cast<void*>(d_probes),
                         static_cast<void*>(d_times), static_cast<void*>(d_values),
                         static_cast<void*>(d_npoints), static_cast<void*>(d_status),
-                        static_cast<void*>(d_stats)})
+                        static_cast<void*>(d_stats), static_cast<void*>(d_ctl),
+                        static_cast<void*>(d_subset)})
             cudaFree(p);
     }
 };
@@ -95,7 +102,7 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: circuit not finalized");
             if (!circuits[i]->c.diodes().empty())
                 return fail(NSG_ERR_INVALID,
-                            "nsg_tran_batch_create: diodes are not supported in transient yet");
+                            "nsg_tran_batch_create: diodes are not supported in the transient");
             for (int j = 0; j < nprobe; ++j)
                 if (probes[j] < 0 || probes[j] >= circuits[i]->c.num_vars())
                     return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: probe out of range");
@@ -121,11 +128,12 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         o.nprobe = nprobe;
 
         // Per instance: parameters with PULSE defaults resolved, breakpoints,
-        // initial dt and the first step's dt, and the two symbolic results
-        // (the DC solver and the transient solver each order on their own
-        // first matrix, as the reference creates two solvers).
+        // the initial dt, and the DC solver's ordering on the first DC Newton
+        // matrix.  The transient solver is ordered later, on the first
+        // transient iteration's matrix as the device computes it (the
+        // reference creates two solvers, each ordered on its first matrix).
         std::vector<std::vector<double>> ptran(count), bps(count);
-        std::vector<double> dt0(count), dt1(count);
+        std::vector<double> dt0(count);
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
             ptran[i] = c.resolved_params(tstep, tstop);
@@ -138,17 +146,9 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                 dt = std::max(dt, o.dt_min * 2.0);
             }
             dt0[i] = dt;
-            // the first loop iteration's clamps (transient.cpp:896-905)
-            double d1 = std::max(std::min(dt, o.dt_max), o.dt_min);
-            if (!bps[i].empty()) {
-                const double bpt = bps[i][0];
-                if (d1 > bpt - 1e-18 || d1 > bpt - 0.1 * d1) d1 = bpt;
-            }
-            if (d1 > tstop) d1 = tstop;
-            dt1[i] = d1;
         }
-        std::vector<std::unique_ptr<nsg_topology>> ord_dc(count), ord_tr(count);
-        std::vector<int> rc_dc(count, NSG_OK), rc_tr(count, NSG_OK);
+        std::vector<std::unique_ptr<nsg_topology>> ord_dc(count);
+        std::vector<int> rc_dc(count, NSG_OK);
         std::atomic<int> next{0};
         std::vector<std::thread> pool;
         for (int t = 0; t < std::min(threads, count); ++t)
@@ -159,32 +159,15 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                     c.initjct_values(a, r, o.nopt.gmin);
                     rc_dc[i] = order_topology(c.num_vars(), c.nnz(), c.col_ptr().data(),
                                               c.row_idx().data(), a.data(), 0.0, ord_dc[i]);
-                    c.first_transient_matrix(a, dt1[i], o.nopt.gmin);
-                    rc_tr[i] = order_topology(c.num_vars(), c.nnz(), c.col_ptr().data(),
-                                              c.row_idx().data(), a.data(), 0.0, ord_tr[i]);
                 }
             });
         for (auto& th : pool) th.join();
         for (int i = 0; i < count; ++i)
-            if (rc_dc[i] != NSG_OK || rc_tr[i] != NSG_OK)
+            if (rc_dc[i] != NSG_OK)
                 return fail(NSG_SINGULAR, "nsg_tran_batch_create: symbolic phase failed for "
                                           "instance " + std::to_string(i));
-        auto intern = [&](std::unique_ptr<nsg_topology>& t) -> int {
-            for (size_t k = 0; k < b->topos.size(); ++k) {
-                const auto& p = b->topos[k]->plan;
-                const auto& q = t->plan;
-                if (p.n == q.n && p.perm_row == q.perm_row && p.perm_col == q.perm_col &&
-                    p.col_ptr == q.col_ptr && p.row_idx == q.row_idx && p.lu_src == q.lu_src)
-                    return static_cast<int>(k);
-            }
-            b->topos.push_back(std::move(t));
-            return static_cast<int>(b->topos.size()) - 1;
-        };
-        std::vector<int> plan_dc(count), plan_tr(count);
-        for (int i = 0; i < count; ++i) {
-            plan_dc[i] = intern(ord_dc[i]);
-            plan_tr[i] = intern(ord_tr[i]);
-        }
+        std::vector<int> plan_dc(count);
+        for (int i = 0; i < count; ++i) plan_dc[i] = intern_topology(b->topos, std::move(ord_dc[i]));
 
         std::vector<int32_t> lu_pool, prog;
         std::vector<nsg::PlanDesc> plans;
@@ -193,36 +176,23 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             b->max_col = std::max(b->max_col, t->plan.max_col);
             b->max_n = std::max(b->max_n, t->plan.n);
         }
-        std::vector<nsg::DcDesc> descs(count);
-        std::vector<nsg::TranDesc> tdescs(count);
-        std::vector<double> params_tran, all_bps;
-        b->param_off.assign(count + 1, 0);
-        int64_t work = 0;
+        b->descs.resize(count);
+        b->tdescs.resize(count);
+        std::vector<double> params_dc, params_tran, all_bps;
+        int64_t work = 0, param_off = 0;
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
-            // workspace sized for the larger of the two LU patterns
-            const auto& pd = b->topos[plan_dc[i]]->plan;
-            const auto& pt = b->topos[plan_tr[i]]->plan;
-            const auto& big = (pd.nnz_lu >= pt.nnz_lu) ? pd : pt;
-            nsg::DcDesc& d = descs[i];
-            fill_instance(d, c, big, prog, work);
-            if (pd.lrow_ptr[pd.n] > big.lrow_ptr[big.n] || pd.urow_ptr[pd.n] > big.urow_ptr[big.n] ||
-                pt.lrow_ptr[pt.n] > big.lrow_ptr[big.n] || pt.urow_ptr[pt.n] > big.urow_ptr[big.n]) {
-                // row copies sized per plan: give each the larger of the two
-                d.lrows_off = work;
-                work += (std::max(pd.lrow_ptr[pd.n], pt.lrow_ptr[pt.n]) + 3) & ~3;
-                d.urows_off = work;
-                work += (std::max(pd.urow_ptr[pd.n], pt.urow_ptr[pt.n]) + 3) & ~3;
-            }
+            nsg::DcDesc& d = b->descs[i];
+            fill_instance(d, c, b->topos[plan_dc[i]]->plan, prog, work);
             d.index = i;
             d.plan = plan_dc[i];
-            d.param_off = b->param_off[i];
+            d.param_off = param_off;
             d.sol_off = 0;
-            b->param_off[i + 1] = b->param_off[i] + static_cast<int64_t>(c.params().size());
-            b->host_params.insert(b->host_params.end(), c.params().begin(), c.params().end());
+            param_off += static_cast<int64_t>(c.params().size());
+            params_dc.insert(params_dc.end(), c.params().begin(), c.params().end());
             params_tran.insert(params_tran.end(), ptran[i].begin(), ptran[i].end());
-            nsg::TranDesc& t = tdescs[i];
-            t.tran_plan = plan_tr[i];
+            nsg::TranDesc& t = b->tdescs[i];
+            t.tran_plan = -1;
             t.n_bps = static_cast<int32_t>(bps[i].size());
             t.bp_off = static_cast<int64_t>(all_bps.size());
             all_bps.insert(all_bps.end(), bps[i].begin(), bps[i].end());
@@ -230,7 +200,10 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             t.hist_off = work;
             work += (3 * static_cast<int64_t>(c.num_vars()) + 3) & ~int64_t{3};
             t.dt0 = dt0[i];
+            b->col_ptr.push_back(c.col_ptr());
+            b->row_idx.push_back(c.row_idx());
         }
+        b->work_size = b->work_cap = work;
         const size_t smem = nsg::tran_smem_bytes(b->max_col, b->max_n);
         if (smem > 200 * 1024)
             return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: instance too large for the "
@@ -241,10 +214,10 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         if ((e = upload(&b->d_lu_pool, lu_pool.data(), lu_pool.size())) != cudaSuccess ||
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
             (e = upload(&b->d_prog, prog.data(), prog.size())) != cudaSuccess ||
-            (e = upload(&b->d_descs, descs.data(), descs.size())) != cudaSuccess ||
-            (e = upload(&b->d_tdescs, tdescs.data(), tdescs.size())) != cudaSuccess ||
+            (e = upload(&b->d_descs, b->descs.data(), b->descs.size())) != cudaSuccess ||
+            (e = upload(&b->d_tdescs, b->tdescs.data(), b->tdescs.size())) != cudaSuccess ||
             (e = upload<double>(&b->d_work, nullptr, static_cast<size_t>(work))) != cudaSuccess ||
-            (e = upload(&b->d_params_dc, b->host_params.data(), b->host_params.size())) != cudaSuccess ||
+            (e = upload(&b->d_params_dc, params_dc.data(), params_dc.size())) != cudaSuccess ||
             (e = upload(&b->d_params_tran, params_tran.data(), params_tran.size())) != cudaSuccess ||
             (e = upload(&b->d_bps, all_bps.data(), all_bps.size())) != cudaSuccess ||
             (e = upload(&b->d_probes, pr.data(), pr.size())) != cudaSuccess ||
@@ -252,7 +225,9 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             (e = upload<double>(&b->d_values, nullptr, nout * nprobe)) != cudaSuccess ||
             (e = upload<int32_t>(&b->d_npoints, nullptr, count)) != cudaSuccess ||
             (e = upload<int32_t>(&b->d_status, nullptr, count)) != cudaSuccess ||
-            (e = upload<int32_t>(&b->d_stats, nullptr, 4 * static_cast<size_t>(count))) != cudaSuccess)
+            (e = upload<int32_t>(&b->d_stats, nullptr, 4 * static_cast<size_t>(count))) != cudaSuccess ||
+            (e = upload<nsg::TranCtl>(&b->d_ctl, nullptr, count)) != cudaSuccess ||
+            (e = upload<int32_t>(&b->d_subset, nullptr, count)) != cudaSuccess)
             return cuda_fail("nsg_tran_batch_create", e);
         *out = b.release();
         return NSG_OK;
@@ -262,12 +237,82 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
 void nsg_tran_batch_free(nsg_tran_batch* b) { delete b; }
 
 int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
-    if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_run: null batch");
-    cudaError_t e = nsg::launch_transient(
-        b->d_plans, b->d_lu_pool, b->d_descs, b->d_tdescs, b->count, b->d_prog, b->d_params_dc,
-        b->d_params_tran, b->d_work, b->d_bps, b->d_probes, b->d_times, b->d_values, b->d_npoints,
-        b->d_status, b->d_stats, b->opt, b->max_col, b->max_n, static_cast<cudaStream_t>(stream));
-    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_tran_batch_run", e);
+    return guarded("nsg_tran_batch_run", [&]() -> int {
+        if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_run: null batch");
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        auto launch = [&](const int32_t* subset, int n) {
+            return nsg::launch_transient(b->d_plans, b->d_lu_pool, b->d_descs, b->d_tdescs, subset,
+                                         n, b->d_prog, b->d_params_dc, b->d_params_tran, b->d_work,
+                                         b->d_bps, b->d_probes, b->d_times, b->d_values,
+                                         b->d_npoints, b->d_status, b->d_stats, b->d_ctl, b->opt,
+                                         b->max_col, b->max_n, st);
+        };
+        cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::TranCtl) * b->count, st);
+        if (e == cudaSuccess) e = launch(nullptr, b->count);
+        if (e != cudaSuccess) return cuda_fail("nsg_tran_batch_run", e);
+        // Instances stop for the host when a solver needs its first ordering
+        // (the transient solver, on the first transient matrix) or a
+        // re-ordering after a failed pivot re-validation; each is ordered
+        // here exactly as NeoSolver::numeric would and resumed on the device.
+        std::vector<int> status(b->count);
+        for (int round = 0; round < 1000000; ++round) {
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess ||
+                (e = cudaMemcpy(status.data(), b->d_status, sizeof(int) * b->count,
+                                cudaMemcpyDeviceToHost)) != cudaSuccess)
+                return cuda_fail("nsg_tran_batch_run", e);
+            std::vector<int32_t> subset;
+            for (int i = 0; i < b->count; ++i) {
+                if (status[i] != NSG_REORDER && status[i] != 105) continue;
+                nsg::DcDesc& d = b->descs[i];
+                nsg::TranDesc& t = b->tdescs[i];
+                nsg::TranCtl ctl;
+                std::vector<double> a(d.nnz);
+                if ((e = cudaMemcpy(&ctl, b->d_ctl + i, sizeof ctl, cudaMemcpyDeviceToHost)) !=
+                        cudaSuccess ||
+                    (e = cudaMemcpy(a.data(), b->d_work + d.a_off, sizeof(double) * d.nnz,
+                                    cudaMemcpyDeviceToHost)) != cudaSuccess)
+                    return cuda_fail("nsg_tran_batch_run", e);
+                int topo = -1, rc;
+                if (ctl.need == 105) {
+                    std::unique_ptr<nsg_topology> fresh;
+                    rc = order_topology(d.n, d.nnz, b->col_ptr[i].data(), b->row_idx[i].data(),
+                                        a.data(), ctl.need_diag_gmin, fresh);
+                    if (rc == NSG_OK) topo = intern_topology(b->topos, std::move(fresh));
+                } else {
+                    const int cur = ctl.need_plan == 0 ? d.plan : t.tran_plan;
+                    rc = reorder_instance(b->topos, cur, a.data(), ctl.need_diag_gmin, &topo);
+                }
+                if (rc != NSG_OK) continue;  // keeps its status: the host could not order it
+                if (ctl.need_plan == 0) d.plan = topo;
+                else t.tran_plan = topo;
+                place_lu_workspace(d, b->topos[topo]->plan, b->work_size);
+                subset.push_back(i);
+                ++b->orderings;
+            }
+            if (subset.empty()) break;
+            int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col, &b->max_n);
+            if (rc != NSG_OK) return rc;
+            if (nsg::tran_smem_bytes(b->max_col, b->max_n) > 200 * 1024)
+                return fail(NSG_ERR_INVALID, "nsg_tran_batch_run: an ordered instance is too "
+                                             "large for the shared-memory refactor");
+            if ((e = grow_workspace(&b->d_work, &b->work_cap, b->work_size)) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_descs, b->descs.data(), sizeof(nsg::DcDesc) * b->count,
+                                cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_tdescs, b->tdescs.data(), sizeof(nsg::TranDesc) * b->count,
+                                cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = cudaMemcpy(b->d_subset, subset.data(), sizeof(int32_t) * subset.size(),
+                                cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = launch(b->d_subset, static_cast<int>(subset.size()))) != cudaSuccess)
+                return cuda_fail("nsg_tran_batch_run", e);
+        }
+        return NSG_OK;
+    });
+}
+
+int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count) {
+    if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_tran_batch_orderings: null argument");
+    *count = b->orderings;
+    return NSG_OK;
 }
 
 int nsg_tran_batch_results(const nsg_tran_batch* b, double* times, double* values, int* npoints,

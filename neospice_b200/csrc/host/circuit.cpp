@@ -438,19 +438,4 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
     sum_program(tv, &a, &rhs);
 }
 
-void Circuit::first_transient_matrix(std::vector<double>& a, double dt0, double gmin) const {
-    if (!finalized_) throw std::logic_error("Circuit: not finalized");
-    if (!diodes_.empty())
-        throw std::logic_error("Circuit: first_transient_matrix needs a linear circuit");
-    std::vector<double> tv;
-    const_term_values(tv, gmin);
-    const double ag0 = 1.0 / dt0;  // fill_integrator_context, order 1
-    for (size_t c = 0; c < caps_.size(); ++c) {
-        const double geq = ag0 * params_[caps_[c].param];
-        tv[cap_term_base() + kCapTerms * c + kCGeq] = geq;
-        tv[cap_term_base() + kCapTerms * c + kCNegGeq] = -geq;
-    }
-    sum_program(tv, &a, nullptr);
-}
-
 }  // namespace nsg

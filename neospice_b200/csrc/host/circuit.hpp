@@ -160,10 +160,6 @@ public:
     // (MODETRANOP | MODEINITJCT gives the same values for these devices.)
     void initjct_values(std::vector<double>& a, std::vector<double>& rhs,
                         double gmin) const;
-    // Matrix of the first transient iteration of a circuit without nonlinear
-    // devices: constants plus each capacitor's ag0*C (backward Euler, step
-    // dt0), the matrix the transient solver first orders on.
-    void first_transient_matrix(std::vector<double>& a, double dt0, double gmin) const;
 
 private:
     int32_t num_nodes_;

@@ -7,7 +7,8 @@
 namespace nsg {
 
 struct TranDesc {
-    int32_t tran_plan;  // PlanDesc of the transient solver (ordered on the first step's matrix)
+    int32_t tran_plan;  // PlanDesc of the transient solver (ordered by the host on the
+                        // first transient iteration's matrix; -1 until then)
     int32_t n_bps;      // source breakpoints of this instance
     int64_t bp_off;     // into the breakpoint array
     int64_t out_off;    // first output point slot of this instance
@@ -27,13 +28,35 @@ struct TranOptions {
     int32_t nprobe;       // unknowns stored per output point
 };
 
+enum TranPhase : int32_t { kTrInit = 0, kTrDc = 1, kTrPrepare = 2, kTrStep = 3, kTrDone = 4 };
+
+// Everything one instance's transient carries between launches (global
+// memory, zeroed by the host before a fresh run; a launch works on a copy in
+// shared memory and writes it back when it stops).
+struct TranCtl {
+    DcCtl dc;               // the operating point's controller
+    IntegCtx ctx;           // integrator context
+    double time, dt, prev_dt, prev_prev_dt, saved_delta, proposed_dt, device_dt;
+    double need_diag_gmin;  // diag_gmin of the numeric() the host must redo
+    int32_t phase, status, step_mode, need;
+    int32_t order, step_count, steps_after_bp, order_cooldown;
+    int32_t ringing_cooldown, rejected, total_iterations, newton_iters;
+    int32_t bp_head, points, tried_delmin, crossed_src_bp;
+    SolverState dc_solver, tr_solver;  // the DC and the transient solver
+    int32_t ringing, need_plan;        // need_plan: 0 DC, 1 transient
+    int32_t nr_active, nr_iter, nr_mode, nr_devconv;  // transient Newton resume record
+    int32_t hist[3], pad0;
+    int32_t stperm[4];      // buffer of state0..state3 in the ring
+};
+
 // Per-instance transient status.
 enum : int32_t {
     kTranOk = 0,
     kTranDcFailed = 2,      // the initial operating point did not converge
     kTranNewtonFailed = 3,  // Newton failed at the minimum timestep
     kTranTooManySteps = 4,  // kMaxTransientIterations reached
-    // kStatusReorder (103), kStatusTimeout (104)
+    // kStatusReorder (103), kStatusTimeout (104), kStatusNeedOrder (105):
+    // 103 / 105 stop the instance for the host, which (re-)orders and resumes it
 };
 
 }  // namespace nsg
