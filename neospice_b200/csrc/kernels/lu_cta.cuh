@@ -68,7 +68,7 @@ struct RefactorResult {
 // __syncthreads().
 // When lrows/urows are given, every L and U entry is also written to its
 // position in the row-major copies the dataflow sweeps read.
-__device__ inline RefactorResult cta_refactor_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
+static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
                                                    const double* __restrict__ a, double* __restrict__ lu,
                                                    double diag_gmin, int check_pivots,
                                                    double rel_threshold, double* smem, int colbuf,
@@ -312,7 +312,7 @@ __device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
 // in shared memory (flow_solve_smem_bytes); L and U are read from the
 // row-major copies the refactor wrote.  Same arithmetic, in the same order
 // per row, as cta_solve.  Returns false if a bounded wait gave up.
-__device__ inline bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
+static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int32_t* __restrict__ pool,
                                       const double* __restrict__ lu,
                                       const double* __restrict__ lrows,
                                       const double* __restrict__ urows, double* __restrict__ x,
