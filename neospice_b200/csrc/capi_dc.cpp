@@ -17,7 +17,7 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params, double* work, double* solutions,
                              int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
-                             cudaStream_t stream);
+                             long long max_stage, cudaStream_t stream);
 size_t dc_smem_bytes(int max_col, int max_n);
 }  // namespace nsg
 
@@ -145,6 +145,10 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
     d.state_off = work; work = align4(work + 4 * static_cast<int64_t>(d.n_states));
     d.mrec_off = work; work = align4(work + nsg::kMosRecCount * static_cast<int64_t>(d.n_mos));
+    d.stage_len = work - d.x_off;
+}
+
+void place_dcsave(nsg::DcDesc& d, int64_t& work) {
     d.dcsave_off = work;
     work = align4(work + d.n + 3 * static_cast<int64_t>(d.n_states) + 3 * d.n_diodes);
 }
@@ -403,6 +407,7 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             const auto& p = b->topos[topo_of[i]]->plan;
             nsg::DcDesc& d = descs[i];
             fill_instance(d, c, p, prog, work);
+            place_dcsave(d, work);
             d.index = i;
             d.plan = topo_of[i];
             d.param_off = b->param_off[i];
@@ -530,7 +535,8 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
         if (e == cudaSuccess)
             e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, nullptr, b->count,
                                       b->d_prog, params, b->d_work, d_solutions, d_status,
-                                      d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n, st);
+                                      d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n,
+                                      max_stage_len(b->descs), st);
         if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_run", e);
         if (!b->reorder) return NSG_OK;
         // Instances whose pivots failed re-validation: re-order on the host
@@ -577,7 +583,8 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
                 (e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, b->d_subset,
                                            static_cast<int>(subset.size()), b->d_prog, params,
                                            b->d_work, d_solutions, d_status, d_iterations,
-                                           b->d_ctl, b->opt, b->max_col, b->max_n, st)) !=
+                                           b->d_ctl, b->opt, b->max_col, b->max_n,
+                                           max_stage_len(b->descs), st)) !=
                     cudaSuccess)
                 return cuda_fail("nsg_dc_batch_run", e);
         }

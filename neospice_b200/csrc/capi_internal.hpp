@@ -5,6 +5,7 @@
 #include "host/circuit.hpp"
 #include "host/plan.hpp"
 #include "host/sparse_order.hpp"
+#include "kernels/dc_device.cuh"
 #include "kernels/lu_device.cuh"
 
 #include <cuda_runtime.h>
@@ -96,6 +97,14 @@ namespace nsg { struct DcDesc; }
 namespace nsg_internal {
 void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPlan& p,
                    std::vector<int32_t>& prog, int64_t& work);
+// The gmin-stepping save area, placed after the staged regions.
+void place_dcsave(nsg::DcDesc& d, int64_t& work);
+// Largest stage_len over instances (doubles).
+inline int64_t max_stage_len(const std::vector<nsg::DcDesc>& ds) {
+    int64_t m = 0;
+    for (const auto& d : ds) m = d.stage_len > m ? d.stage_len : m;
+    return m;
+}
 
 // Host (re-)ordering of one instance that stopped on the device.
 // reorder_instance: a copy of topos[topo]'s engine runs NeoSolver::numeric on

@@ -18,7 +18,8 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params_tran, double* work, const double* bps,
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
-                             const TranOptions& o, int max_col, int max_n, cudaStream_t stream);
+                             const TranOptions& o, int max_col, int max_n, long long max_stage,
+                             cudaStream_t stream);
 size_t tran_smem_bytes(int max_col, int max_n);
 }  // namespace nsg
 
@@ -199,6 +200,8 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             t.out_off = static_cast<int64_t>(i) * max_points;
             t.hist_off = work;
             work += (3 * static_cast<int64_t>(c.num_vars()) + 3) & ~int64_t{3};
+            d.stage_len = work - d.x_off;
+            place_dcsave(d, work);
             t.dt0 = dt0[i];
             b->col_ptr.push_back(c.col_ptr());
             b->row_idx.push_back(c.row_idx());
@@ -245,7 +248,7 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                                          n, b->d_prog, b->d_params_dc, b->d_params_tran, b->d_work,
                                          b->d_bps, b->d_probes, b->d_times, b->d_values,
                                          b->d_npoints, b->d_status, b->d_stats, b->d_ctl, b->opt,
-                                         b->max_col, b->max_n, st);
+                                         b->max_col, b->max_n, max_stage_len(b->descs), st);
         };
         cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::TranCtl) * b->count, st);
         if (e == cudaSuccess) e = launch(nullptr, b->count);

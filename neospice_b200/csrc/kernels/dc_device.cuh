@@ -34,6 +34,9 @@ struct DcDesc {
     int64_t state_off;             // four state vectors of n_states doubles
     int64_t mrec_off;              // per-MOSFET persistent load values
     int64_t dcsave_off;            // gmin-stepping save area (x, state0..2, diode state)
+    // Doubles from x_off on that a launch may stage in shared memory (every
+    // per-iteration region: vectors, matrix, LU, terms, states, history).
+    int64_t stage_len;
 };
 
 // SimOptions of the reference (src/core/types.hpp:24-66) used by the loop.

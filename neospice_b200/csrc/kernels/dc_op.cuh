@@ -67,7 +67,7 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
                                              SolverState* solver, DcCtl* ctl,
                                              const NewtonOptions& opt, int firstmode,
                                              int contmode, bool true_gmin_first, double* save,
-                                             double* smem, int colbuf) {
+                                             double* smem, int colbuf, int smem_doubles) {
     const double gtarget = opt.gmin;  // max(gmin, gshunt = 0)
     const int itl2 = 50;
     // Bound on Newton solves per operating point: a stepping that creeps by
@@ -105,7 +105,7 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
         const bool resume = s_active != 0;
         const NewtonOutcome r = newton(v, pd, lu_pool, ctx, o, max_iter, solver, smem, colbuf,
                                        resume ? s_r_iter : -1, s_entry_mode,
-                                       resume ? s_r_devconv : 1);
+                                       resume ? s_r_devconv : 1, false, smem_doubles);
         if (r.code == kStatusReorder) {
             if (threadIdx.x == 0) {
                 ctl->active = 1;

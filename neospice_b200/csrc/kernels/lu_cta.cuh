@@ -288,6 +288,150 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
     __syncthreads();
 }
 
+// Small instances: the whole LU lives in shared memory and warp 0 alone
+// refactors and sweeps it, column after column / level after level with
+// __syncwarp only -- no completion flags and no global-memory round trips on
+// the dependency chain, which dominate for circuits of a few dozen unknowns.
+// Same operations in the same order as cta_refactor_flow / cta_solve_flow,
+// so the values are bit-identical.  lu_s: pd.nnz_lu doubles; w_s: pd.n.
+// Dynamic shared memory of a Newton kernel launch: the LU scratch (flow or
+// small path) followed by an optional stage for instance workspaces, capped
+// so that two CTAs still fit on an SM.
+constexpr size_t kStageCapBytes = 100 * 1024;
+__host__ __device__ inline size_t stage_bytes_for(size_t scratch_bytes, long long max_stage) {
+    if (scratch_bytes >= kStageCapBytes || max_stage <= 0) return 0;
+    const size_t want = static_cast<size_t>(max_stage) * sizeof(double);
+    const size_t room = kStageCapBytes - scratch_bytes;
+    return want < room ? want : room;
+}
+
+__host__ __device__ inline bool small_fits(int n, int nnz_lu, int smem_doubles) {
+    return n <= 128 && nnz_lu + n <= smem_doubles;
+}
+
+// Refactor into lu_s (and lu, written back at the end).  Begins and ends with
+// __syncthreads().
+static __device__ __noinline__ RefactorResult cta_refactor_small(
+    const PlanDesc& pd, const int32_t* __restrict__ pool, const double* __restrict__ a,
+    double* __restrict__ lu, double diag_gmin, int check_pivots, double rel_threshold,
+    double* lu_s) {
+    const int32_t n = pd.n;
+    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const int32_t* lu_src = pool + pd.off[PA_lu_src];
+    const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]);
+    const int lane = threadIdx.x & 31;
+    __shared__ int32_t s_fail_step;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int32_t fail_step = INT32_MAX;
+        for (int32_t j = 0; j < n; ++j) {
+            const int32_t c0 = col_ptr[j];
+            const int32_t len = col_ptr[j + 1] - c0;
+            const int32_t dj = diag_pos[j] - c0;
+            for (int32_t t = lane; t < len; t += 32) {
+                const int32_t src = lu_src[c0 + t];
+                double v = (src >= 0) ? a[src] : 0.0;
+                if (t == dj && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+                lu_s[c0 + t] = v;
+            }
+            __syncwarp();
+            for (int32_t q = 0; q < dj; ++q) {
+                const int4 m = umeta[c0 + q];  // r, diag_pos[r], |L(:, r)|, upd_start
+                const double u = lu_mul(lu_s[c0 + q], lu_s[m.y]);
+                for (int32_t t = lane; t < m.z; t += 32) {
+                    const int32_t d = upd_dst[m.w + t];
+                    lu_s[c0 + d] = lu_sub(lu_s[c0 + d], lu_mul(u, lu_s[m.y + 1 + t]));
+                }
+                __syncwarp();
+                if (lane == 0) lu_s[c0 + q] = u;
+                __syncwarp();
+            }
+            const double piv = lu_s[c0 + dj];
+            bool fail;
+            if (check_pivots) {
+                double largest = 0.0;
+                for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(lu_s[c0 + t]));
+                largest = warp_max(largest);
+                fail = !(largest * rel_threshold < fabs(piv));
+            } else {
+                fail = (piv == 0.0);
+            }
+            if (fail && j < fail_step) fail_step = j;
+            __syncwarp();
+            if (lane == 0) lu_s[c0 + dj] = 1.0 / piv;
+            __syncwarp();
+        }
+        if (lane == 0) s_fail_step = fail_step;
+    }
+    __syncthreads();
+    for (int32_t k = threadIdx.x; k < pd.nnz_lu; k += blockDim.x) lu[k] = lu_s[k];
+    RefactorResult res;
+    res.step = s_fail_step == INT32_MAX ? -1 : s_fail_step;
+    res.code = s_fail_step == INT32_MAX ? kStatusOk
+                                        : (check_pivots ? kStatusReorder : kStatusSingular);
+    __syncthreads();
+    return res;
+}
+
+// x <- A^{-1} x from the LU in lu_s (warp 0, level by level).  Begins and ends
+// with __syncthreads().
+static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
+                                                    const int32_t* __restrict__ pool,
+                                                    const double* lu_s, double* __restrict__ x,
+                                                    double* w) {
+    const int32_t n = pd.n;
+    const int32_t* perm_row = pool + pd.off[PA_perm_row];
+    const int32_t* perm_col = pool + pd.off[PA_perm_col];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const int lane = threadIdx.x & 31;
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        {   // forward: L with the reciprocal pivot
+            const int32_t* lp = pool + pd.off[PA_lrow_ptr];
+            const int32_t* lpos = pool + pd.off[PA_lrow_pos];
+            const int32_t* lcol = pool + pd.off[PA_lrow_col];
+            const int32_t* lev_ptr = pool + pd.off[PA_fwd_lev_ptr];
+            const int32_t* lev = pool + pd.off[PA_fwd_lev];
+            for (int32_t l = 0; l < pd.n_fwd_lev; ++l) {
+                for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
+                    const int32_t i = lev[k];
+                    double t = w[i];
+                    for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
+                        const double xc = w[lcol[e]];
+                        if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu_s[lpos[e]]));
+                    }
+                    w[i] = (t != 0.0) ? lu_mul(t, lu_s[diag_pos[i]]) : t;
+                }
+                __syncwarp();
+            }
+        }
+        {   // backward: unit-diagonal U, row dot products
+            const int32_t* up = pool + pd.off[PA_urow_ptr];
+            const int32_t* upos = pool + pd.off[PA_urow_pos];
+            const int32_t* ucol = pool + pd.off[PA_urow_col];
+            const int32_t* lev_ptr = pool + pd.off[PA_bwd_lev_ptr];
+            const int32_t* lev = pool + pd.off[PA_bwd_lev];
+            for (int32_t l = 0; l < pd.n_bwd_lev; ++l) {
+                for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
+                    const int32_t i = lev[k];
+                    double t = w[i];
+                    for (int32_t e = up[i]; e < up[i + 1]; ++e)
+                        t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
+                    w[i] = t;
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) x[perm_col[i]] = w[i];
+    __syncthreads();
+}
+
 // Shared memory of the dataflow solve: the n-vector and n completion flags.
 __host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
     return (sizeof(double) + sizeof(int32_t)) * static_cast<size_t>(n);

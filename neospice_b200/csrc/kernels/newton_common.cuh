@@ -53,8 +53,28 @@ struct Inst {
     int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs, n_mos;
 };
 
+// Address of workspace offset `off`: in the shared-memory stage when the
+// instance is staged and the offset lies in its staged span, else global.
+__device__ __forceinline__ double* ws_at(const DcDesc& d, double* work, double* stage,
+                                         int64_t off) {
+    return (stage && off >= d.x_off && off < d.x_off + d.stage_len) ? stage + (off - d.x_off)
+                                                                     : work + off;
+}
+
+// Copy the staged span between global memory and the stage (whole CTA).
+__device__ inline void stage_copy(const DcDesc& d, double* work, double* stage, bool in) {
+    if (!stage) return;
+    __syncthreads();
+    double* g = work + d.x_off;
+    for (int64_t i = threadIdx.x; i < d.stage_len; i += blockDim.x) {
+        if (in) stage[i] = g[i];
+        else g[i] = stage[i];
+    }
+    __syncthreads();
+}
+
 __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const double* params,
-                                 double* work) {
+                                 double* work, double* stage = nullptr) {
     Inst v;
     v.slot_ptr = prog + d.prog_off[DP_slot_ptr];
     v.slot_terms = prog + d.prog_off[DP_slot_terms];
@@ -69,16 +89,17 @@ __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const dou
     v.srcs = prog + d.prog_off[DP_srcs];
     v.mos = prog + d.prog_off[DP_mos];
     v.par = params + d.param_off;
-    v.x = work + d.x_off;
-    v.xold = work + d.xold_off;
-    v.a = work + d.a_off;
-    v.lu = work + d.lu_off;
-    v.lrows = work + d.lrows_off;
-    v.urows = work + d.urows_off;
-    v.tv = work + d.tv_off;
-    v.dstate = work + d.dstate_off;
-    v.dconst = work + d.dconst_off;
-    for (int k = 0; k < 4; ++k) v.st[k] = work + d.state_off + k * static_cast<int64_t>(d.n_states);
+    v.x = ws_at(d, work, stage, d.x_off);
+    v.xold = ws_at(d, work, stage, d.xold_off);
+    v.a = ws_at(d, work, stage, d.a_off);
+    v.lu = ws_at(d, work, stage, d.lu_off);
+    v.lrows = ws_at(d, work, stage, d.lrows_off);
+    v.urows = ws_at(d, work, stage, d.urows_off);
+    v.tv = ws_at(d, work, stage, d.tv_off);
+    v.dstate = ws_at(d, work, stage, d.dstate_off);
+    v.dconst = ws_at(d, work, stage, d.dconst_off);
+    for (int k = 0; k < 4; ++k)
+        v.st[k] = ws_at(d, work, stage, d.state_off) + k * static_cast<int64_t>(d.n_states);
     v.n = d.n;
     v.num_nodes = d.num_nodes;
     v.nnz = d.nnz;
@@ -87,7 +108,7 @@ __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const dou
     v.n_caps = d.n_caps;
     v.n_srcs = d.n_srcs;
     v.n_mos = d.n_mos;
-    v.mrec = work + d.mrec_off;
+    v.mrec = ws_at(d, work, stage, d.mrec_off);
     return v;
 }
 
@@ -268,11 +289,17 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
                                        IntegCtx* ctx, const NewtonOptions& opt, int max_iter,
                                        SolverState* solver, double* smem, int colbuf,
                                        int resume_iter = -1, int saved_mode = -1,
-                                       int resume_dev_conv = 1, bool host_orders_first = false) {
+                                       int resume_dev_conv = 1, bool host_orders_first = false,
+                                       int smem_doubles = 0) {
     __shared__ int32_t s_conv, s_dev_conv;
     if (saved_mode < 0) saved_mode = ctx->mode;
     bool force_numeric = false;
     NewtonOutcome out{kDcNoConvergence, max_iter, -1, 0, 1};
+    // Small instances keep the LU in shared memory (warp-level refactor and
+    // sweeps); larger ones use the dataflow schedule over global memory.
+    const bool small = small_fits(pd.n, pd.nnz_lu, smem_doubles);
+    double* lu_s = smem;
+    double* w_s = smem + pd.nnz_lu;
     __syncthreads();
     for (int iter = resume_iter < 0 ? 0 : resume_iter; iter < max_iter; ++iter) {
         const bool resumed = (iter == resume_iter);
@@ -294,10 +321,11 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             out = {kStatusNeedOrder, iter + 1, iter, mode, s_dev_conv};
             break;
         }
+        const int check = numeric && solver->factored && !resumed;
         const RefactorResult fr =
-            cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin,
-                              numeric && solver->factored && !resumed, 1e-3, smem, colbuf,
-                              v.lrows, v.urows);
+            small ? cta_refactor_small(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, lu_s)
+                  : cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, smem,
+                                      colbuf, v.lrows, v.urows);
         if (fr.code == kStatusTimeout) {
             out = {kStatusTimeout, iter + 1, -1, 0, 1};
             break;
@@ -316,7 +344,9 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             __syncthreads();
             continue;
         }
-        if (!cta_solve_flow(pd, lu_pool, v.lu, v.lrows, v.urows, v.x, smem)) {
+        if (small) {
+            cta_solve_small(pd, lu_pool, lu_s, v.x, w_s);
+        } else if (!cta_solve_flow(pd, lu_pool, v.lu, v.lrows, v.urows, v.x, smem)) {
             out = {kStatusTimeout, iter + 1, -1, 0, 1};
             break;
         }

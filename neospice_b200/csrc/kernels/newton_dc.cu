@@ -22,11 +22,14 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  const int32_t* __restrict__ prog, const double* __restrict__ params,
                  double* __restrict__ work, double* __restrict__ solutions,
                  int32_t* __restrict__ status, int32_t* __restrict__ iterations,
-                 DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf) {
+                 DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf, int scratch_doubles,
+                 int stage_doubles) {
     extern __shared__ double smem[];
     const DcDesc d = descs[subset ? subset[blockIdx.x] : blockIdx.x];
     const PlanDesc& pd = plans[d.plan];
-    const Inst v = make_inst(d, prog, params, work);
+    double* stage = (d.stage_len <= stage_doubles) ? smem + scratch_doubles : nullptr;
+    stage_copy(d, work, stage, true);
+    const Inst v = make_inst(d, prog, params, work, stage);
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
     __shared__ int32_t s_fresh;
@@ -52,8 +55,10 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     __syncthreads();
     // solve_dc (dc.cpp:53-175): direct attempt, true gmin stepping, gmin stepping
     const int32_t code = dc_operating_point(v, d.n_states, pd, lu_pool, &ctx, &solver, ctl, opt,
-                                            kFirst, kCont, true, work + d.dcsave_off, smem, colbuf);
+                                            kFirst, kCont, true, work + d.dcsave_off, smem, colbuf,
+                                            scratch_doubles);
 
+    stage_copy(d, work, stage, false);
     double* out = solutions + d.sol_off;
     for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) out[i] = v.x[i];
     if (threadIdx.x == 0) {
@@ -74,10 +79,12 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params, double* work, double* solutions,
                              int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
-                             cudaStream_t stream) {
+                             long long max_stage, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
-    const size_t smem = dc_smem_bytes(max_col, max_n);
+    const size_t scratch = (dc_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
+    const size_t stage = stage_bytes_for(scratch, max_stage);
+    const size_t smem = scratch + stage;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
@@ -89,7 +96,9 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
     }
     newton_dc_kernel<<<count, kFlowThreads, smem, stream>>>(plans, lu_pool, descs, subset, prog,
                                                              params, work, solutions, status,
-                                                             iterations, ctls, opt, colbuf);
+                                                             iterations, ctls, opt, colbuf,
+                                                             static_cast<int>(scratch / sizeof(double)),
+                                                             static_cast<int>(stage / sizeof(double)));
     return cudaGetLastError();
 }
 

@@ -154,11 +154,12 @@ __device__ inline bool prepare_step(TranCtl& k, const TranDesc& td, const double
     return true;
 }
 
-// Thread 0: write the controller back and report the instance.
-__device__ inline void finish(const DcDesc& d, TranCtl* g, const TranCtl& k,
-                              const TranOptions& o, int32_t* npoints, int32_t* status,
-                              int32_t* stats, int32_t code) {
-    __syncthreads();
+// Copy the stage back, then (thread 0) write the controller back and report
+// the instance.
+__device__ inline void finish(const DcDesc& d, double* work, double* stage, TranCtl* g,
+                              const TranCtl& k, const TranOptions& o, int32_t* npoints,
+                              int32_t* status, int32_t* stats, int32_t code) {
+    stage_copy(d, work, stage, false);
     if (threadIdx.x != 0) return;
     *g = k;
     status[d.index] = code;
@@ -181,7 +182,8 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  const int32_t* __restrict__ probes, double* __restrict__ times,
                  double* __restrict__ values, int32_t* __restrict__ npoints,
                  int32_t* __restrict__ status, int32_t* __restrict__ stats,
-                 TranCtl* __restrict__ ctls, TranOptions o, int colbuf) {
+                 TranCtl* __restrict__ ctls, TranOptions o, int colbuf, int scratch_doubles,
+                 int stage_doubles) {
     extern __shared__ double smem[];
     const int pos = subset ? subset[blockIdx.x] : blockIdx.x;
     const DcDesc d = descs[pos];
@@ -190,8 +192,10 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     __shared__ TranCtl k;
     __shared__ double s_red[kFlowWarps];
     __shared__ int32_t s_flag;
-    Inst v = make_inst(d, prog, params_dc, work);
-    double* hist = work + td.hist_off;  // three history vectors (ring)
+    double* stage = (d.stage_len <= stage_doubles) ? smem + scratch_doubles : nullptr;
+    stage_copy(d, work, stage, true);
+    Inst v = make_inst(d, prog, params_dc, work, stage);
+    double* hist = ws_at(d, work, stage, td.hist_off);  // three history vectors (ring)
     const double* bp = bps + td.bp_off;
     constexpr int kFirst = kModeTranOp | kModeInitJct, kCont = kModeTranOp | kModeInitFloat;
 
@@ -216,7 +220,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         __syncthreads();
     }
     {
-        double* base = work + d.state_off;
+        double* base = ws_at(d, work, stage, d.state_off);
         for (int q = 0; q < 4; ++q) v.st[q] = base + static_cast<int64_t>(k.stperm[q]) * d.n_states;
     }
 
@@ -224,19 +228,19 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     if (k.phase == kTrDc) {
         const int32_t code = dc_operating_point(v, d.n_states, plans[d.plan], lu_pool, &k.ctx,
                                                 &k.dc_solver, &k.dc, o.nopt, kFirst, kCont, false,
-                                                work + d.dcsave_off, smem, colbuf);
+                                                work + d.dcsave_off, smem, colbuf, scratch_doubles);
         if (code == kStatusReorder) {
             if (threadIdx.x == 0) {
                 k.need = kStatusReorder;
                 k.need_plan = 0;
                 k.need_diag_gmin = k.dc.numeric_diag_gmin;
             }
-            finish(d, g, k, o, npoints, status, stats, kStatusReorder);
+            finish(d, work, stage, g, k, o, npoints, status, stats, kStatusReorder);
             return;
         }
         if (code != kDcConverged) {
             if (threadIdx.x == 0) k.phase = kTrDone;
-            finish(d, g, k, o, npoints, status, stats,
+            finish(d, work, stage, g, k, o, npoints, status, stats,
                    code == kStatusTimeout ? code : kTranDcFailed);
             return;
         }
@@ -285,7 +289,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         __syncthreads();
         const NewtonOutcome r = newton(v, tpd, lu_pool, &k.ctx, o.nopt, o.itl4, &k.tr_solver, smem,
                                        colbuf, resume ? nr_iter : -1, step_mode,
-                                       resume ? nr_devconv : 1, host_first);
+                                       resume ? nr_devconv : 1, host_first, scratch_doubles);
         if (r.code == kStatusReorder || r.code == kStatusNeedOrder) {
             if (threadIdx.x == 0) {
                 k.nr_active = 1;
@@ -296,7 +300,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                 k.need_plan = 1;
                 k.need_diag_gmin = o.nopt.diag_gmin;
             }
-            finish(d, g, k, o, npoints, status, stats, r.code);
+            finish(d, work, stage, g, k, o, npoints, status, stats, r.code);
             return;
         }
         if (threadIdx.x == 0) k.nr_active = 0;
@@ -452,7 +456,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     }
     __syncthreads();
     if (threadIdx.x == 0) k.phase = kTrDone;
-    finish(d, g, k, o, npoints, status, stats, k.status);
+    finish(d, work, stage, g, k, o, npoints, status, stats, k.status);
 }
 
 size_t tran_smem_bytes(int max_col, int max_n) {
@@ -468,10 +472,13 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params_tran, double* work, const double* bps,
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
-                             const TranOptions& o, int max_col, int max_n, cudaStream_t stream) {
+                             const TranOptions& o, int max_col, int max_n, long long max_stage,
+                             cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
-    const size_t smem = tran_smem_bytes(max_col, max_n);
+    const size_t scratch = (tran_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
+    const size_t stage = stage_bytes_for(scratch, max_stage);
+    const size_t smem = scratch + stage;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
@@ -483,7 +490,8 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
     }
     transient_kernel<<<count, kFlowThreads, smem, stream>>>(
         plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes,
-        times, values, npoints, status, stats, ctls, o, colbuf);
+        times, values, npoints, status, stats, ctls, o, colbuf,
+        static_cast<int>(scratch / sizeof(double)), static_cast<int>(stage / sizeof(double)));
     return cudaGetLastError();
 }
 

@@ -191,3 +191,16 @@ def mos_network(rng: np.random.Generator, nodes: int, vdd=1.8, pulse=None) -> Ne
                     float(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))))
         dev.append(("C", k, GND, 1e-14))
     return Netlist(nodes, dev, models)
+
+
+def inverter_chain_mc(rng: np.random.Generator, stages: int = 32, sigma_vto=0.03,
+                      sigma_kp=0.05, pulse=(0.0, 1.8, 0.0, 1e-10, 1e-10, 1e-9, 2e-9)) -> Netlist:
+    """A Monte Carlo variant of inverter_chain: the NMOS and PMOS threshold
+    voltages drawn with a Gaussian sigma_vto (V) and the transconductances
+    with a relative Gaussian sigma_kp, per instance, from rng."""
+    nl = inverter_chain(stages, pulse=pulse)
+    dv = sigma_vto * rng.standard_normal(2)
+    dk = 1.0 + sigma_kp * rng.standard_normal(2)
+    nl.models = {"nch": ("nmos", {"VTO": 0.7 + dv[0], "KP": 110e-6 * dk[0]}),
+                 "pch": ("pmos", {"VTO": -0.7 + dv[1], "KP": 50e-6 * dk[1]})}
+    return nl
