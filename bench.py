@@ -1,7 +1,7 @@
 """Benchmark: batched DC operating point of diode-clamped resistor meshes.
 
-Workload (one step): the DC operating point -- the direct Newton attempt of
-Simulator::run_dc -- of 4096 seeded meshes per GPU, grid side drawn uniformly
+Workload (one step): the DC operating point (Simulator::run_dc: direct
+Newton attempt, gmin stepping where it fails) of 4096 seeded meshes per GPU, grid side drawn uniformly
 from 16..96 (257..9217 unknowns), resistors lognormal around 1 kOhm (sigma
 0.1), level-1 diodes (IS=1e-14, N=1) at 5% of the nodes, 0-1 mA current
 sources at 2%, a 1 V corner source; Newton from a zero guess, all instances in
@@ -13,6 +13,11 @@ Under torchrun (N > 1) every rank solves its own 4096 instances (weak
 scaling, no collective on the data path); the time is the max over ranks.
 --impl reference times the reference's own CPU code (oracle/_ref, built from
 the reference sources) on this host's cores on a bounded sample per step.
+
+At N = 1 the line also carries "plain_vs_batched": the transient of a
+32-stage CMOS inverter chain through the plain path (one instance per
+launch) and the batched path (Monte Carlo variants in one launch), with the
+nominal instance's parity against the reference.
 """
 from __future__ import annotations
 
@@ -43,6 +48,10 @@ def _args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=64,
                     help="instances in the CPU-baseline sample (0 = skip)")
+    ap.add_argument("--no-inverter", action="store_true",
+                    help="skip the plain-vs-batched transient measurement")
+    ap.add_argument("--inverter-batch", type=int, default=296,
+                    help="instances of the batched inverter-chain transient")
     return ap.parse_args()
 
 
@@ -294,11 +303,84 @@ def run_ours(a, rank, world, local_rank):
             line["parity"] = {"checked": len(idx), "max_rel_err_vs_reference": worst,
                               "iterations_equal": bool(all(int(iters[i]) == ref_iters[k]
                                                            for k, i in enumerate(idx)))}
+        if not a.no_inverter and world == 1:
+            try:
+                line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch)
+            except Exception as exc:
+                line["plain_vs_batched"] = {"error": str(exc)}
         print(json.dumps(line), flush=True)
 
     del batch
     if world > 1:
         dist.destroy_process_group()
+
+
+# --- plain vs batched transient (32-stage CMOS inverter chain) ---------------------
+
+INV_PULSE = (0.0, 1.8, 0.0, 1e-10, 1e-10, 1e-9, 2e-9)
+
+
+def inverter_plain_vs_batched(batch_count):
+    """Transient of a 32-stage level-1 CMOS inverter chain (10 fF per stage,
+    VDD 1.8 V, PULSE 0->1.8 V 100p/100p 1n/2n, .tran 1p 20n): the plain path
+    (one instance per launch) and the batched path (batch_count Monte Carlo
+    variants in one launch), each timed end to end through TranBatch.run
+    (device clock), plus parity of the nominal instance with the reference's
+    solve_transient."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.circuit import TranBatch
+
+    nominal = W.inverter_chain(32, pulse=INV_PULSE)
+    probes = np.arange(nominal.num_nodes, dtype=np.int32)
+
+    def timed(nls, reps):
+        b = TranBatch([n.build() for n in nls], 1e-12, 20e-9, probes, max_points=21000)
+        b.run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            b.run()
+        e1.record()
+        torch.cuda.synchronize()
+        return b, e0.elapsed_time(e1) / 1000.0 / reps
+
+    bp, t_plain = timed([nominal], 2)
+    rp = bp.results()[0]
+    mc = [W.inverter_chain_mc(np.random.default_rng([7, i])) for i in range(batch_count)]
+    bb, t_batch = timed(mc, 1)
+    ok = sum(r["status"] == 0 for r in bb.results())
+    out = {
+        "workload": "transient, 32-stage CMOS inverter chain (MOS1), PULSE input, .tran 1p 20n; "
+                    f"batched = {batch_count} Monte Carlo variants (VTO sigma 30 mV, KP 5%)",
+        "plain": {"value": round(1.0 / t_plain, 4), "unit": "circuit-solves/s",
+                  "seconds_per_solve": round(t_plain, 4), "points": len(rp["time"]),
+                  "newton_iterations": rp["newton_iters"]},
+        "batched": {"value": round(batch_count / t_batch, 3), "unit": "circuit-solves/s",
+                    "instances": batch_count, "seconds": round(t_batch, 4), "ok": ok},
+        "ratio": round((batch_count / t_batch) * t_plain, 2),
+    }
+    try:
+        import oracle
+        sys.path.insert(0, str(ROOT / "tests"))
+        import netlists
+        if oracle.have_ref():
+            t0 = time.perf_counter()
+            tr, vr, info = oracle.ref_sim(netlists.ref_desc(nominal), 1, 1e-12, 20e-9)
+            t_ref = time.perf_counter() - t0
+            same_pts = len(tr) == len(rp["time"])
+            err = float(np.max(np.abs(rp["values"] - vr) / np.maximum(np.abs(vr), 1e-3))) \
+                if same_pts else None
+            out["parity"] = {"timepoints_equal": bool(same_pts and np.allclose(tr, rp["time"],
+                                                                                rtol=1e-12, atol=0)),
+                             "max_rel_err_vs_reference": err,
+                             "iterations_equal": info["iterations"] == rp["newton_iters"]}
+            out["cpu_reference_1core"] = {"value": round(1.0 / t_ref, 4), "unit": "circuit-solves/s"}
+    except Exception as exc:  # the parity check is informative only
+        out["parity"] = {"error": str(exc)}
+    return out
 
 
 # --- reference arm -----------------------------------------------------------------

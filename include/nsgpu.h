@@ -267,6 +267,19 @@ int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);
  * stepping), and the number of Newton solves it took (either may be NULL). */
 int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves);
 
+/* DC adjoint: for every instance, the gradient of a scalar loss L with
+ * respect to the circuit parameters through the operating point, given
+ * d_solutions (the run's solutions) and d_cotangent = dL/dx (packed like the
+ * solutions).  The Jacobian is re-evaluated at the solution, factored with
+ * the instance's pivots and solved transposed (SparseMatrix::solve_transposed,
+ * src/solver/solve.cpp:102-141); then dL/dp = -lambda^T dF/dp for resistances,
+ * DC source values and MOSFET W, L and VTO, written to d_grads (packed like
+ * the parameters; every other parameter gets 0).  The analytic counterpart of
+ * the reference's finite-difference .sens (src/core/sens.cpp:57-140).
+ * d_status: 0, or 102 when the Jacobian at the solution is singular. */
+int nsg_dc_batch_adjoint(nsg_dc_batch* b, const double* d_params, const double* d_solutions,
+                         const double* d_cotangent, double* d_grads, int* d_status, void* stream);
+
 /* ---- Batched transient analysis (device) ------------------------------------
  * solve_transient (src/core/transient.cpp:694-1067) for `count` circuits in one
  * launch, one thread block per circuit, each with its own adaptive timestep:

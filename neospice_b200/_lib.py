@@ -88,6 +88,8 @@ SIGNATURES = {
     "nsg_dc_batch_set_reorder": (c_int, [c_void_p, c_int]),
     "nsg_dc_batch_reorders": (c_int, [c_void_p, P(c_ll)]),
     "nsg_dc_batch_methods": (c_int, [c_void_p, P(c_int), P(c_int)]),
+    "nsg_dc_batch_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p]),
     "nsg_tran_batch_create": (c_int, [c_int, P(c_void_p), c_double, c_double, c_int, c_int,
                                       P(c_int), c_int, P(c_void_p)]),
     "nsg_tran_batch_free": (None, [c_void_p]),

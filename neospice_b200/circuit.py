@@ -226,6 +226,19 @@ class DcBatch:
                                          d_iterations.data_ptr(), sp))
         return d_solutions, d_status, d_iterations
 
+    def adjoint(self, d_solutions, d_cotangent, d_params=None, stream=None):
+        """dL/dparams (device tensor, packed like params()) for cotangents
+        dL/dx at the run's solutions; status per instance (0, or 102)."""
+        import torch
+        grads = torch.empty(int(self.param_offsets[-1]), dtype=torch.float64, device="cuda")
+        status = torch.empty(self.count, dtype=torch.int32, device="cuda")
+        sp = torch.cuda.current_stream().cuda_stream if stream is None else \
+            getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().nsg_dc_batch_adjoint(
+            self._h, None if d_params is None else d_params.data_ptr(), d_solutions.data_ptr(),
+            d_cotangent.contiguous().data_ptr(), grads.data_ptr(), status.data_ptr(), sp))
+        return grads, status
+
     def split(self, packed):
         arr = packed.cpu().numpy() if hasattr(packed, "cpu") else np.asarray(packed)
         o = self.solution_offsets

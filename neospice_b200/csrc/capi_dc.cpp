@@ -19,6 +19,11 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const NewtonOptions& opt, int max_col, int max_n,
                              long long max_stage, cudaStream_t stream);
 size_t dc_smem_bytes(int max_col, int max_n);
+cudaError_t launch_dc_adjoint(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
+                              int count, const int32_t* prog, const double* params, double* work,
+                              const double* solutions, const double* cotangent, double* grads,
+                              int32_t* status, const NewtonOptions& opt, int max_col, int max_n,
+                              cudaStream_t stream);
 }  // namespace nsg
 
 using namespace nsg_internal;
@@ -133,6 +138,8 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     tab.clear();
     for (const auto& m : c.mosfets()) tab.insert(tab.end(), {m.d, m.g, m.s, m.b, m.param, m.state});
     d.prog_off[nsg::DP_mos] = append(prog, tab);
+    d.prog_off[nsg::DP_grad] = append(prog, c.grad_program());
+    d.n_grad = static_cast<int32_t>(c.grad_program().size() / 5);
     d.x_off = work; work = align4(work + d.n);
     d.xold_off = work; work = align4(work + d.n);
     d.w_off = work; work = align4(work + d.n);
@@ -522,6 +529,20 @@ int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves) {
         if (solves) solves[i] = ctl[i].solves;
     }
     return NSG_OK;
+}
+
+int nsg_dc_batch_adjoint(nsg_dc_batch* b, const double* d_params, const double* d_solutions,
+                         const double* d_cotangent, double* d_grads, int* d_status, void* stream) {
+    if (!b || !d_solutions || !d_cotangent || !d_grads || !d_status)
+        return fail(NSG_ERR_INVALID, "nsg_dc_batch_adjoint: null argument");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(d_grads, 0, sizeof(double) * b->param_off[b->count], st);
+    if (e == cudaSuccess)
+        e = nsg::launch_dc_adjoint(b->d_plans, b->d_lu_pool, b->d_descs, b->count, b->d_prog,
+                                   d_params ? d_params : b->d_params, b->d_work, d_solutions,
+                                   d_cotangent, d_grads, d_status, b->opt, b->max_col, b->max_n,
+                                   st);
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_dc_batch_adjoint", e);
 }
 
 int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,

@@ -302,6 +302,23 @@ void Circuit::finalize() {
             }
         }
     }
+    // Gradient program (creation order): resistors, DC sources, MOSFETs.
+    grad_.clear();
+    for (const auto& d : devices_) {
+        if (d.kind == DevKind::Resistor) {
+            grad_.insert(grad_.end(), {kGradResistor, d.param, d.a, d.b, 0});
+        } else if (d.kind == DevKind::VSource && d.wave == Wave::DC) {
+            int32_t br = -1;
+            for (const auto& o : order)
+                if (o.created == d.created) br = o.branch;
+            grad_.insert(grad_.end(), {kGradVSource, d.param, br, -1, 0});
+        } else if (d.kind == DevKind::ISource && d.wave == Wave::DC) {
+            grad_.insert(grad_.end(), {kGradISource, d.param, d.a, d.b, 0});
+        }
+    }
+    for (size_t m = 0; m < mos_.size(); ++m)
+        grad_.insert(grad_.end(), {kGradMosfet, mos_[m].param, mos_[m].d, mos_[m].s,
+                                   static_cast<int32_t>(m)});
     const int32_t pin = konst(kTermGmin, -1);
     for (int32_t i : dead_nodes_) slot[offset(i, i)].push_back(pin);
 

@@ -148,6 +148,13 @@ public:
     const std::vector<int32_t>& ucb_ptr() const { return ucb_ptr_; }     // UCB-style devices
     const std::vector<int32_t>& ucb_terms() const { return ucb_terms_; }
 
+    // Gradient program of the DC adjoint: one record {kind, param, a, b, aux}
+    // per differentiable parameter group (kGrad*), a/b the nodes or branch
+    // the residual derivative lands on.
+    enum GradKind : int32_t { kGradResistor = 1, kGradVSource = 2, kGradISource = 3,
+                              kGradMosfet = 4 };
+    const std::vector<int32_t>& grad_program() const { return grad_; }
+
     // Source breakpoints in (0, tstop] after resolving PULSE defaults with
     // (tstep, tstop) (VSource::resolve_defaults / get_breakpoints,
     // src/devices/vsource.cpp:51-78, 233-264), in device order.
@@ -174,7 +181,7 @@ private:
     std::vector<MosRec> mos_;
     std::vector<Mos1Card> mos_models_;
     int32_t num_states_ = 0;
-    std::vector<int32_t> term_op_, term_param_;
+    std::vector<int32_t> term_op_, term_param_, grad_;
     std::vector<int32_t> slot_ptr_, slot_terms_, rhs_ptr_, rhs_terms_, ucb_ptr_, ucb_terms_;
 
     void check_node(int32_t v) const;

@@ -9,7 +9,7 @@ namespace nsg {
 // Stamp-program arrays of one circuit in the program pool.
 enum DcProgArray : int {
     DP_slot_ptr, DP_slot_terms, DP_rhs_ptr, DP_rhs_terms, DP_ucb_ptr, DP_ucb_terms,
-    DP_term_op, DP_term_param, DP_diodes, DP_caps, DP_srcs, DP_mos, DP_COUNT
+    DP_term_op, DP_term_param, DP_diodes, DP_caps, DP_srcs, DP_mos, DP_grad, DP_COUNT
 };
 
 struct DcDesc {
@@ -23,6 +23,7 @@ struct DcDesc {
     int32_t n_caps;
     int32_t n_srcs;      // waveform sources
     int32_t n_mos;       // MOSFETs (level 1)
+    int32_t n_grad;      // gradient-program records (DC adjoint)
     int32_t n_states;    // per state vector (2 per capacitor, 17 per MOSFET)
     int64_t prog_off[DP_COUNT];  // int32-word offsets into the program pool
     int64_t param_off;           // into the caller's parameter array

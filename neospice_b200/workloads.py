@@ -204,3 +204,16 @@ def inverter_chain_mc(rng: np.random.Generator, stages: int = 32, sigma_vto=0.03
     nl.models = {"nch": ("nmos", {"VTO": 0.7 + dv[0], "KP": 110e-6 * dk[0]}),
                  "pch": ("pmos", {"VTO": -0.7 + dv[1], "KP": 50e-6 * dk[1]})}
     return nl
+
+
+def resistor_network(rng: np.random.Generator, nodes: int) -> Netlist:
+    """A seeded linear resistor network: a 1 V source on node 0, every further
+    node tied to a random earlier node and to ground by resistors (lognormal
+    around 1 kOhm), current sources of U(0, 1 mA) into a third of the nodes."""
+    dev = [("V", 0, GND, 1.0)]
+    for k in range(1, nodes):
+        dev.append(("R", int(rng.integers(0, k)), k, float(1e3 * np.exp(0.3 * rng.standard_normal()))))
+        dev.append(("R", k, GND, float(1e3 * np.exp(0.3 * rng.standard_normal()))))
+        if rng.random() < 1 / 3:
+            dev.append(("I", GND, k, float(rng.uniform(0, 1e-3))))
+    return Netlist(nodes, dev)

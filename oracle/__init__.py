@@ -82,6 +82,7 @@ def ref() -> ctypes.CDLL:
         lib.nsref_sim_free.argtypes = [_V]
         lib.nsref_sim_initjct.argtypes = [ctypes.c_char_p, _V, _V, _V, _V, _V]
         lib.nsref_sim_method.argtypes = [_V]
+        lib.nsref_sim_sens.argtypes = [ctypes.c_char_p, _I, _V, _V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
         _ref = lib
@@ -237,6 +238,21 @@ def ref_sim_initjct(desc: str):
     if lib.nsref_sim_initjct(d, ctypes.addressof(nv), _p(cp), _p(ri), _p(vals), _p(rhs)) != nnz:
         raise RuntimeError("reference INITJCT evaluation failed")
     return cp, ri, vals, rhs
+
+
+def ref_sim_sens(desc: str, output_node: int):
+    """The reference's solve_sens of v(output node): (sensitivities in the
+    reference's order -- resistors, voltage sources, current sources, each in
+    creation order --, output value)."""
+    lib = ref()
+    d = desc.encode()
+    k = lib.nsref_sim_sens(d, int(output_node), None, None)
+    if k < 0:
+        raise RuntimeError("reference sensitivity analysis failed")
+    out = np.zeros(max(k, 1))
+    val = ctypes.c_double()
+    lib.nsref_sim_sens(d, int(output_node), _p(out), ctypes.addressof(val))
+    return out[:k], val.value
 
 
 def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0):

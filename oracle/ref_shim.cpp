@@ -25,6 +25,7 @@
 #include "core/circuit.hpp"
 #include "core/dc.hpp"
 #include "core/transient.hpp"
+#include "core/sens.hpp"
 #include "devices/capacitor.hpp"
 #include "devices/isource.hpp"
 #include "devices/vsource.hpp"
@@ -485,3 +486,22 @@ extern "C" int nsref_sim_initjct(const char* desc, int* num_vars, int* col_ptr, 
 // The DC convergence method of a finished run (ConvergenceMethod as an int:
 // 0 = the direct Newton attempt, 1 = gmin stepping).
 extern "C" int nsref_sim_method(void* h) { return static_cast<SimResult*>(h)->method; }
+
+// The reference's DC sensitivity analysis (solve_sens, src/core/sens.cpp:57-140)
+// of v(n<output_node>) for a described circuit: entries in the reference's
+// order (resistors, then voltage sources, then current sources, each in
+// creation order).  Returns the entry count (sens may be NULL to ask), or -1.
+extern "C" int nsref_sim_sens(const char* desc, int output_node, double* sens, double* out_value) {
+    try {
+        Circuit ckt;
+        build_from_desc(ckt, desc);
+        SensResult r = solve_sens(ckt, "v(n" + std::to_string(output_node) + ")");
+        if (out_value) *out_value = r.output_value;
+        if (sens)
+            for (size_t k = 0; k < r.entries.size(); ++k) sens[k] = r.entries[k].sensitivity;
+        return static_cast<int>(r.entries.size());
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_sim_sens: %s\n", e.what());
+        return -1;
+    }
+}

@@ -19,6 +19,10 @@ mos_dc.npz: CMOS inverter chains and seeded MOS networks, per case the
 netlist (JSON) and the reference's solve_dc operating point, Newton
 iteration count and convergence method (0 direct, 1 gmin stepping).
 
+sens_dc.npz: seeded resistor and MOS networks, per case the netlist, the
+output node and the reference's solve_sens of v(output) (finite-difference
+sensitivities to every resistance, voltage source and current source).
+
 mesh_dc.npz: seeded diode-clamped meshes (neospice_b200.workloads), per case
 the mesh, the reference's first-iteration matrix and rhs, and its DC
 operating point (solve_dc) with the Newton iteration count.
@@ -167,6 +171,35 @@ def mos_main():
     print(f"wrote {len(cases)} MOS operating points to {path}")
 
 
+def sens_netlists():
+    """(netlist, output node) cases of sens_dc.npz: linear resistor networks
+    with voltage and current sources, and seeded MOS networks."""
+    from neospice_b200 import workloads as W
+    cases = []
+    for k, nodes in enumerate((6, 12, 25)):
+        cases.append((W.resistor_network(np.random.default_rng([61, k]), nodes), nodes - 1))
+    for k in range(3):
+        nl = W.mos_network(np.random.default_rng([62, k]), 6 + 3 * k)
+        cases.append((nl, nl.num_nodes - 1))
+    return cases
+
+
+def sens_main():
+    import json
+    import netlists
+    rec = {}
+    cases = sens_netlists()
+    for k, (nl, out) in enumerate(cases):
+        sens, val = oracle.ref_sim_sens(netlists.ref_desc(nl), out)
+        p = f"s{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "output": np.int32(out), p + "sens": sens, p + "value": np.float64(val)})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("sens_dc.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} sensitivity cases to {path}")
+
+
 def tran_main():
     import json
     import netlists
@@ -187,7 +220,7 @@ def tran_main():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos", "sens"]
     if "solver" in which:
         main()
     if "mesh" in which:
@@ -196,3 +229,5 @@ if __name__ == "__main__":
         tran_main()
     if "mos" in which:
         mos_main()
+    if "sens" in which:
+        sens_main()

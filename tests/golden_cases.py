@@ -70,3 +70,33 @@ def load_mos_dc():
                                {k2: (t, p2) for k2, (t, p2) in models.items()})
         out.append(d)
     return out
+
+
+SENS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "sens_dc.npz"
+
+
+def load_sens():
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(SENS_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"s{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        out.append(d)
+    return out
+
+
+def param_starts(netlist):
+    """(kind, first parameter index) of every device of a Netlist, in
+    creation order (the layout of Circuit.params())."""
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 2, "M": 43}
+    out, at = [], 0
+    for d in netlist.devices:
+        k = d[0]
+        out.append((k, at))
+        at += sizes[k] if k in sizes else len(d) - 3
+    return out
