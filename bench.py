@@ -58,8 +58,8 @@ def _args():
 # --- workload ------------------------------------------------------------------
 
 def make_meshes(count, seed, rank):
-    from neospice_b200 import workloads
-    return workloads.diode_mesh_batch(count, seed=seed + 1000003 * rank)
+    from neospice_b200 import sharding, workloads
+    return workloads.diode_mesh_batch(count, seed=sharding.rank_seed(seed, rank))
 
 
 def sample_indices(count, k, offset=0):
@@ -240,10 +240,8 @@ def run_ours(a, rank, world, local_rank):
     barrier()
     sec_e2e = f0.elapsed_time(f1) / 1000.0
 
-    if world > 1:
-        t = torch.tensor([sec, sec_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec, sec_e2e = float(t[0]), float(t[1])
+    from neospice_b200 import sharding
+    sec, sec_e2e = sharding.max_over_ranks([sec, sec_e2e])
 
     if rank == 0:
         solves = world * a.count * a.steps
