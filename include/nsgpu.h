@@ -47,6 +47,42 @@ const char* nsg_last_error(void);
 int nsg_topology_order(int n, int nnz, const int* col_ptr, const int* row_idx,
                        const double* values, double diag_gmin, nsg_topology** out);
 
+/* Factorization engines (make_solver, src/core/make_solver.cpp:156-178).
+ *   NSG_SOLVER_MARKOWITZ  NeoSolver: Sparse-1.3 Markowitz ordering.
+ *   NSG_SOLVER_AMDLU      AmdLuSolver (src/core/amd_lu_solver.cpp:11-358):
+ *                         AMD column order, left-looking LU with threshold
+ *                         partial pivoting, fixed-pivot replay refactor.
+ *   NSG_SOLVER_AUTO_AMDLU AutoFallbackSolver (make_solver.cpp:71-145): AMD-LU,
+ *                         switching to Markowitz for good when the first
+ *                         factorization is singular. */
+#define NSG_SOLVER_MARKOWITZ 0
+#define NSG_SOLVER_AMDLU 1
+#define NSG_SOLVER_AUTO_AMDLU 2
+
+/* make_solver(num_vars, is_linear)'s choice: NEOSPICE_SOLVER=amdlu|klu or
+ * markowitz|sparse, else NEOSPICE_FORCE_AMDLU (non-empty, not "0"), else
+ * NSG_SOLVER_AUTO_AMDLU for linear circuits of at least 256 unknowns and
+ * NSG_SOLVER_MARKOWITZ otherwise (make_solver.cpp:41-55, 166-174). */
+int nsg_solver_select(int num_vars, int is_linear);
+
+/* nsg_topology_order with an explicit engine: for the AMD-LU engines,
+ * AmdLuSolver::symbolic then numeric (amd_lu_solver.cpp:11-38, 74-197,
+ * 273-278); the pivot sequence, fill and replay order are the reference's.
+ * Device values of an AMD-LU topology follow AmdLuSolver's layout: U
+ * unscaled, L divided by the pivot, pivots stored as is. */
+int nsg_topology_order_solver(int n, int nnz, const int* col_ptr, const int* row_idx,
+                              const double* values, double diag_gmin, int solver,
+                              nsg_topology** out);
+
+/* Engine of a topology's current plan (NSG_SOLVER_MARKOWITZ or
+ * NSG_SOLVER_AMDLU; an auto topology reports the engine it settled on), or
+ * NSG_ERR_INVALID. */
+int nsg_topology_solver(const nsg_topology* topo);
+
+/* amd_ordering (src/core/amd.cpp:14-143) of a CSC pattern: perm[k] = the
+ * original column eliminated at step k (n ints). */
+int nsg_amd_order(int n, const int* col_ptr, const int* row_idx, int* perm);
+
 /* nsg_topology_numeric: a later NeoSolver::numeric on the same topology
  * (neo_solver.cpp:219-245): re-validate every pivot on the new values and
  * re-order from the first failing step, as SparseMatrix::order_and_factor
@@ -94,6 +130,13 @@ int nsg_batch_layout(const nsg_batch* batch, long long* value_offsets,
  * add_diag_gmin (neo_solver.cpp:247-265, factor.cpp:980-1052), with the
  * fixed pivots.  check_pivots != 0 instead applies the re-validation test of
  * a later NeoSolver::numeric (factor.cpp:929-947) and reports NSG_REORDER.
+ * AMD-LU topologies: AmdLuSolver::refactorize's replay
+ * (amd_lu_solver.cpp:214-271).  Where its pivot-growth test fails the
+ * reference re-factors the same values with factor_; the kernel checks
+ * whether factor_'s threshold pivoting would choose the plan's pivots (then
+ * the replayed values are factor_'s, bit for bit) and reports NSG_REORDER
+ * otherwise (run nsg_topology_numeric).  With check_pivots != 0, a numeric():
+ * NSG_REORDER unless factor_ would choose the same pivots on these values.
  * d_status[i] / d_fail_step[i] (device int arrays, fail_step optional)
  * receive the per-instance code and the failing 0-based pivot step. */
 int nsg_batch_refactor(nsg_batch* batch, const double* d_values, double diag_gmin,
@@ -267,6 +310,12 @@ int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);
  * stepping), and the number of Newton solves it took (either may be NULL). */
 int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves);
 
+/* Engine (NSG_SOLVER_MARKOWITZ or NSG_SOLVER_AMDLU) of each instance's
+ * current plan: make_solver's choice for the circuit (make_solver.cpp:
+ * 156-178; NEOSPICE_SOLVER / NEOSPICE_FORCE_AMDLU are read when the batch is
+ * created), after any AutoFallbackSolver switch. */
+int nsg_dc_batch_engines(const nsg_dc_batch* b, int* engine);
+
 /* DC adjoint: for every instance, the gradient of a scalar loss L with
  * respect to the circuit parameters through the operating point, given
  * d_solutions (the run's solutions) and d_cotangent = dL/dx (packed like the
@@ -317,6 +366,10 @@ int nsg_tran_batch_results(const nsg_tran_batch* b, double* times, double* value
 /* Host orderings done so far: the transient solver's first ordering per
  * instance plus every re-ordering after a failed pivot re-validation. */
 int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count);
+
+/* Engines of each instance's DC and transient solvers (the reference creates
+ * one of each, transient.cpp:713, :726), or -1 for a solver not yet ordered. */
+int nsg_tran_batch_engines(const nsg_tran_batch* b, int* dc_engine, int* tran_engine);
 
 #ifdef __cplusplus
 }

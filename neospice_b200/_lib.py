@@ -38,6 +38,13 @@ SIGNATURES = {
     "nsg_topology_order": (c_int, [c_int, c_int, P(c_int), P(c_int), P(c_double), c_double,
                                    P(c_void_p)]),
     "nsg_topology_numeric": (c_int, [c_void_p, P(c_double), c_double, P(c_int)]),
+    "nsg_topology_order_solver": (c_int, [c_int, c_int, P(c_int), P(c_int), P(c_double),
+                                          c_double, c_int, P(c_void_p)]),
+    "nsg_solver_select": (c_int, [c_int, c_int]),
+    "nsg_topology_solver": (c_int, [c_void_p]),
+    "nsg_amd_order": (c_int, [c_int, P(c_int), P(c_int), P(c_int)]),
+    "nsg_dc_batch_engines": (c_int, [c_void_p, P(c_int)]),
+    "nsg_tran_batch_engines": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "nsg_topology_import": (c_int, [c_int, c_int, P(c_int), P(c_int), c_int, P(c_int), P(c_int),
                                     P(c_int), P(c_void_p)]),
     "nsg_topology_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_ll), P(c_int),

@@ -16,6 +16,9 @@ import numpy as np
 
 from . import _lib as L
 
+# NSG_SOLVER_* engine codes of a plan.
+ENGINE_NAMES = {0: "markowitz", 1: "amdlu"}
+
 GND = -1
 
 
@@ -195,6 +198,13 @@ class DcBatch:
         L.check(L.lib().nsg_dc_batch_reorders(self._h, ctypes.byref(n)))
         return n.value
 
+    def engines(self) -> list:
+        """Factorization engine of each instance: "markowitz" or "amdlu"
+        (make_solver's choice for the circuit)."""
+        out = np.zeros(self.count, np.int32)
+        L.check(L.lib().nsg_dc_batch_engines(self._h, L.iptr(out)))
+        return [ENGINE_NAMES.get(int(k)) for k in out]
+
     def methods(self):
         """(method, solves) per instance after a run: 0 direct Newton, 1 gmin
         stepping; Newton solves taken."""
@@ -282,6 +292,14 @@ class TranBatch:
         n = ctypes.c_longlong()
         L.check(L.lib().nsg_tran_batch_orderings(self._h, ctypes.byref(n)))
         return n.value
+
+    def engines(self):
+        """(DC engines, transient engines) per circuit: "markowitz",
+        "amdlu", or None for a solver not ordered yet."""
+        dc = np.zeros(self.count, np.int32)
+        tr = np.zeros(self.count, np.int32)
+        L.check(L.lib().nsg_tran_batch_engines(self._h, L.iptr(dc), L.iptr(tr)))
+        return ([ENGINE_NAMES.get(int(k)) for k in dc], [ENGINE_NAMES.get(int(k)) for k in tr])
 
     def results(self):
         """Per circuit: dict(time, values [points x probes], status, steps,

@@ -4,6 +4,7 @@
 #include "kernels/dc_device.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -41,9 +42,66 @@ int cuda_fail(const char* where, cudaError_t e) {
                 std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-// NeoSolver::numeric's load + preorder + gmin + order_and_factor on the
-// host engine (neo_solver.cpp:219-245).
+namespace {
+// A 0-based CSC pattern with monotone column pointers and sorted, unique,
+// in-range rows.
+bool valid_csc(int n, const int* col_ptr, const int* row_idx) {
+    for (int j = 0; j < n; ++j) {
+        if (col_ptr[j + 1] < col_ptr[j]) return false;
+        for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p)
+            if (row_idx[p] < 0 || row_idx[p] >= n || (p > col_ptr[j] && row_idx[p] <= row_idx[p - 1]))
+                return false;
+    }
+    return true;
+}
+
+// NeoSolver::symbolic on a valid CSC pattern: one engine element per slot.
+void make_markowitz(nsg_topology& t, int n, const int* col_ptr, const int* row_idx) {
+    t.engine = std::make_unique<nsg::MarkowitzOrder>(n);
+    t.slot_elem.assign(col_ptr[n], 0);
+    for (int j = 0; j < n; ++j)
+        for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p)
+            t.slot_elem[p] = t.engine->get_element(row_idx[p] + 1, j + 1);
+}
+}  // namespace
+
+int select_solver(int num_vars, bool is_linear) {
+    // read_choice (make_solver.cpp:41-55): NEOSPICE_SOLVER first, then the
+    // legacy NEOSPICE_FORCE_AMDLU alias.
+    if (const char* s = std::getenv("NEOSPICE_SOLVER")) {
+        if (std::strcmp(s, "amdlu") == 0 || std::strcmp(s, "klu") == 0) return NSG_SOLVER_AMDLU;
+        if (std::strcmp(s, "markowitz") == 0 || std::strcmp(s, "sparse") == 0)
+            return NSG_SOLVER_MARKOWITZ;
+    }
+    if (const char* f = std::getenv("NEOSPICE_FORCE_AMDLU"))
+        if (f[0] != '\0' && std::strcmp(f, "0") != 0) return NSG_SOLVER_AMDLU;
+    // Auto: AMD-LU (with the Markowitz fallback) for linear circuits of at
+    // least 256 unknowns (kAmdLuAutoThreshold).
+    return (num_vars >= 256 && is_linear) ? NSG_SOLVER_AUTO_AMDLU : NSG_SOLVER_MARKOWITZ;
+}
+
+void rebuild_plan(nsg_topology& t) {
+    t.plan = t.amd ? nsg::build_plan_amd(*t.amd) : nsg::build_plan(*t.engine, t.slot_elem);
+}
+
+// numeric() on the host engine.  Markowitz: NeoSolver::numeric's load +
+// preorder + gmin + order_and_factor (neo_solver.cpp:219-245).  AMD-LU:
+// AmdLuSolver::numeric = factor_ (amd_lu_solver.cpp:273-278), wrapped by
+// AutoFallbackSolver::numeric (make_solver.cpp:85-101) when auto-selected.
 int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin) {
+    if (t.amd) {
+        const bool ok = t.amd->factor(values, diag_gmin);
+        if (!ok && t.auto_fallback && !t.committed) {
+            const auto& f = *t.amd;
+            make_markowitz(t, f.size(), f.col_ptr().data(), f.row_idx().data());
+            t.amd.reset();
+            t.committed = true;
+            return numeric_on_engine(t, values, diag_gmin);
+        }
+        t.committed = true;
+        return ok ? NSG_OK : NSG_SINGULAR;
+    }
+    t.committed = true;
     auto& mo = *t.engine;
     mo.clear_fillins();
     for (size_t k = 0; k < t.slot_elem.size(); ++k) mo.value(t.slot_elem[k]) = values[k];
@@ -56,28 +114,31 @@ int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin) {
 }
 
 int order_topology(int n, int nnz, const int* col_ptr, const int* row_idx, const double* values,
-                   double diag_gmin, std::unique_ptr<nsg_topology>& out) {
+                   double diag_gmin, std::unique_ptr<nsg_topology>& out, int solver) {
     if (n <= 0 || nnz <= 0 || !col_ptr || !row_idx || !values)
         return fail(NSG_ERR_INVALID, "nsg_topology_order: bad arguments");
     if (col_ptr[0] != 0 || col_ptr[n] != nnz)
         return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr does not span nnz");
+    if (solver != NSG_SOLVER_MARKOWITZ && solver != NSG_SOLVER_AMDLU &&
+        solver != NSG_SOLVER_AUTO_AMDLU)
+        return fail(NSG_ERR_INVALID, "nsg_topology_order: unknown solver");
+    if (!valid_csc(n, col_ptr, row_idx))
+        return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr not monotone or rows not "
+                                     "sorted/unique");
     auto t = std::make_unique<nsg_topology>();
-    t->engine = std::make_unique<nsg::MarkowitzOrder>(n);
-    t->slot_elem.resize(nnz);
-    for (int j = 0; j < n; ++j) {
-        if (col_ptr[j + 1] < col_ptr[j])
-            return fail(NSG_ERR_INVALID, "nsg_topology_order: col_ptr not monotone");
-        for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) {
-            if (row_idx[p] < 0 || row_idx[p] >= n ||
-                (p > col_ptr[j] && row_idx[p] <= row_idx[p - 1]))
-                return fail(NSG_ERR_INVALID, "nsg_topology_order: rows not sorted/unique");
-            t->slot_elem[p] = t->engine->get_element(row_idx[p] + 1, j + 1);
-        }
+    if (solver == NSG_SOLVER_MARKOWITZ) {
+        make_markowitz(*t, n, col_ptr, row_idx);
+    } else {
+        // AmdLuSolver::symbolic: the AMD order of the pattern.
+        t->amd = std::make_unique<nsg::AmdLuFactor>(
+            n, std::vector<int32_t>(col_ptr, col_ptr + n + 1),
+            std::vector<int32_t>(row_idx, row_idx + nnz));
+        t->auto_fallback = (solver == NSG_SOLVER_AUTO_AMDLU);
     }
     const int rc = numeric_on_engine(*t, values, diag_gmin);
     if (rc == NSG_SINGULAR) return fail(NSG_SINGULAR, "nsg_topology_order: singular matrix");
     if (rc != NSG_OK) return fail(rc, "nsg_topology_order: ordering failed");
-    t->plan = nsg::build_plan(*t->engine, t->slot_elem);
+    rebuild_plan(*t);
     out = std::move(t);
     return NSG_OK;
 }
@@ -94,23 +155,28 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.max_col = p.max_col;
     d.nnz_l = p.lrow_ptr[p.n];
     d.nnz_u = p.urow_ptr[p.n];
+    d.kind = p.kind;
     p.append_to(pool, d.off);
     return d;
 }
 
 
 std::unique_ptr<nsg_topology> clone_topology(const nsg_topology& t) {
-    if (!t.engine) throw std::logic_error("clone_topology: topology has no ordering engine");
+    if (!t.engine && !t.amd) throw std::logic_error("clone_topology: topology has no ordering engine");
     auto c = std::make_unique<nsg_topology>();
-    c->engine = std::make_unique<nsg::MarkowitzOrder>(*t.engine);
+    if (t.engine) c->engine = std::make_unique<nsg::MarkowitzOrder>(*t.engine);
+    if (t.amd) c->amd = std::make_unique<nsg::AmdLuFactor>(*t.amd);
     c->slot_elem = t.slot_elem;
+    c->auto_fallback = t.auto_fallback;
+    c->committed = t.committed;
     c->plan = t.plan;
     return c;
 }
 
 bool same_plan(const nsg::TopologyPlan& a, const nsg::TopologyPlan& b) {
-    return a.n == b.n && a.perm_row == b.perm_row && a.perm_col == b.perm_col &&
-           a.col_ptr == b.col_ptr && a.row_idx == b.row_idx && a.lu_src == b.lu_src;
+    return a.kind == b.kind && a.n == b.n && a.perm_row == b.perm_row &&
+           a.perm_col == b.perm_col && a.col_ptr == b.col_ptr && a.row_idx == b.row_idx &&
+           a.lu_src == b.lu_src && a.piv_rank == b.piv_rank && a.gmin_pos == b.gmin_pos;
 }
 
 int intern_topology(std::vector<std::unique_ptr<nsg_topology>>& topos,
@@ -126,7 +192,7 @@ int reorder_instance(std::vector<std::unique_ptr<nsg_topology>>& topos, int topo
     auto c = clone_topology(*topos[topo]);
     const int rc = numeric_on_engine(*c, values, diag_gmin);
     if (rc != NSG_OK) return rc;
-    c->plan = nsg::build_plan(*c->engine, c->slot_elem);
+    rebuild_plan(*c);
     *new_topo = intern_topology(topos, std::move(c));
     return NSG_OK;
 }
@@ -204,20 +270,66 @@ int nsg_topology_order(int n, int nnz, const int* col_ptr, const int* row_idx,
     });
 }
 
+int nsg_topology_order_solver(int n, int nnz, const int* col_ptr, const int* row_idx,
+                              const double* values, double diag_gmin, int solver,
+                              nsg_topology** out) {
+    return guarded("nsg_topology_order_solver", [&]() -> int {
+        if (!out) return fail(NSG_ERR_INVALID, "nsg_topology_order_solver: null out");
+        *out = nullptr;
+        std::unique_ptr<nsg_topology> t;
+        const int rc = order_topology(n, nnz, col_ptr, row_idx, values, diag_gmin, t, solver);
+        if (rc == NSG_OK) *out = t.release();
+        return rc;
+    });
+}
+
+int nsg_solver_select(int num_vars, int is_linear) {
+    return select_solver(num_vars, is_linear != 0);
+}
+
+int nsg_topology_solver(const nsg_topology* topo) {
+    if (!topo) return fail(NSG_ERR_INVALID, "nsg_topology_solver: null topology");
+    return topo->plan.kind == nsg::kPlanKindAmdLu ? NSG_SOLVER_AMDLU : NSG_SOLVER_MARKOWITZ;
+}
+
+int nsg_amd_order(int n, const int* col_ptr, const int* row_idx, int* perm) {
+    return guarded("nsg_amd_order", [&]() -> int {
+        if (n <= 0 || !col_ptr || !row_idx || !perm)
+            return fail(NSG_ERR_INVALID, "nsg_amd_order: bad arguments");
+        if (col_ptr[0] != 0 || !valid_csc(n, col_ptr, row_idx))
+            return fail(NSG_ERR_INVALID, "nsg_amd_order: malformed pattern");
+        const std::vector<int32_t> q = nsg::amd_order(n, col_ptr, row_idx);
+        std::memcpy(perm, q.data(), sizeof(int) * q.size());
+        return NSG_OK;
+    });
+}
+
 int nsg_topology_numeric(nsg_topology* topo, const double* values, double diag_gmin,
                          int* reordered) {
     return guarded("nsg_topology_numeric", [&]() -> int {
         if (!topo || !values) return fail(NSG_ERR_INVALID, "nsg_topology_numeric: bad arguments");
-        if (!topo->engine)
+        if (!topo->engine && !topo->amd)
             return fail(NSG_ERR_INVALID,
                         "nsg_topology_numeric: imported topology has no ordering state");
+        if (topo->amd) {
+            // AmdLuSolver::numeric: a full factor_ with fresh pivots.
+            const int rc = numeric_on_engine(*topo, values, diag_gmin);
+            if (rc != NSG_OK) {
+                if (reordered) *reordered = 0;
+                return fail(rc, "nsg_topology_numeric: singular matrix");
+            }
+            nsg_topology probe;
+            probe.plan = topo->plan;
+            rebuild_plan(*topo);
+            if (reordered) *reordered = same_plan(probe.plan, topo->plan) ? 0 : 1;
+            return NSG_OK;
+        }
         const int before = topo->engine->fillin_count();
         const int rc = numeric_on_engine(*topo, values, diag_gmin);
         const int step = topo->engine->reorder_step();
         if (reordered) *reordered = step;
         if (rc != NSG_OK) return fail(rc, "nsg_topology_numeric: singular matrix");
-        if (step != 0 || topo->engine->fillin_count() != before)
-            topo->plan = nsg::build_plan(*topo->engine, topo->slot_elem);
+        if (step != 0 || topo->engine->fillin_count() != before) rebuild_plan(*topo);
         return NSG_OK;
     });
 }
@@ -345,8 +457,11 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
                        int check_pivots, int* d_status, int* d_fail_step, void* stream) {
     if (!b || !d_values || !d_status)
         return fail(NSG_ERR_INVALID, "nsg_batch_refactor: null argument");
+    // check_pivots: a numeric() (re-validate / re-choose the pivots), else a
+    // refactorize() (AMD-LU topologies run the replay's growth test).
+    const int mode = check_pivots ? nsg::kCheckNumeric : nsg::kCheckRefactor;
     cudaError_t e = nsg::launch_refactor(b->d_plans, b->d_pool, b->d_insts, b->count, d_values,
-                                         b->d_lu, diag_gmin, check_pivots, 1e-3, d_status,
+                                         b->d_lu, diag_gmin, mode, 1e-3, d_status,
                                          d_fail_step, b->max_col, b->max_n, b->allow_flow,
                                          b->d_lrows, b->d_urows, static_cast<cudaStream_t>(stream));
     if (e == cudaSuccess) b->rows_valid = b->allow_flow;

@@ -76,11 +76,6 @@ int64_t append(std::vector<int32_t>& pool, const std::vector<int32_t>& v) {
 
 int64_t align4(int64_t x) { return (x + 3) & ~int64_t{3}; }
 
-bool same_structure(const nsg::TopologyPlan& a, const nsg::TopologyPlan& b) {
-    return a.n == b.n && a.perm_row == b.perm_row && a.perm_col == b.perm_col &&
-           a.col_ptr == b.col_ptr && a.row_idx == b.row_idx && a.lu_src == b.lu_src;
-}
-
 // Run f(i) for i in [0, count) on up to `threads` host threads.
 template <class F>
 void parallel_for(int count, int threads, F&& f) {
@@ -375,7 +370,8 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
             std::vector<double> a, r;
             c.initjct_values(a, r, b->opt.gmin);
             rcs[i] = order_topology(c.num_vars(), c.nnz(), c.col_ptr().data(), c.row_idx().data(),
-                                    a.data(), b->opt.diag_gmin, ordered[i]);
+                                    a.data(), b->opt.diag_gmin, ordered[i],
+                                    select_solver(c.num_vars(), c.is_linear()));
         });
         for (int i : todo)
             if (rcs[i] != NSG_OK)
@@ -386,7 +382,7 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
         for (int i : todo) {
             for (size_t t = 0; t < b->topos.size(); ++t)
                 if (b->topos[t]->plan.n == ordered[i]->plan.n &&
-                    same_structure(b->topos[t]->plan, ordered[i]->plan)) {
+                    same_plan(b->topos[t]->plan, ordered[i]->plan)) {
                     topo_of[i] = static_cast<int>(t);
                     break;
                 }
@@ -514,6 +510,15 @@ int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable) {
 int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count) {
     if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_dc_batch_reorders: null argument");
     *count = b->reorders;
+    return NSG_OK;
+}
+
+int nsg_dc_batch_engines(const nsg_dc_batch* b, int* engine) {
+    if (!b || !engine) return fail(NSG_ERR_INVALID, "nsg_dc_batch_engines: null argument");
+    for (int i = 0; i < b->count; ++i)
+        engine[i] = b->topos[b->topo_of[i]]->plan.kind == nsg::kPlanKindAmdLu
+                        ? NSG_SOLVER_AMDLU
+                        : NSG_SOLVER_MARKOWITZ;
     return NSG_OK;
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 #include "nsgpu.h"
 
+#include "host/amd_lu.hpp"
 #include "host/circuit.hpp"
 #include "host/plan.hpp"
 #include "host/sparse_order.hpp"
@@ -17,9 +18,18 @@
 #include <string>
 #include <vector>
 
+// One symbolic result.  Exactly one engine is set for a topology that can
+// re-order: the Markowitz engine (NeoSolver) or the AMD-LU engine
+// (AmdLuSolver); an imported topology has neither.
 struct nsg_topology {
-    std::unique_ptr<nsg::MarkowitzOrder> engine;  // null for an imported topology
-    std::vector<int32_t> slot_elem;
+    std::unique_ptr<nsg::MarkowitzOrder> engine;
+    std::vector<int32_t> slot_elem;  // Markowitz: engine element of each caller slot
+    std::unique_ptr<nsg::AmdLuFactor> amd;
+    // make_solver's AutoFallbackSolver (make_solver.cpp:71-145): an AMD-LU
+    // engine that switches to Markowitz for good when its first
+    // factorization is singular.
+    bool auto_fallback = false;
+    bool committed = false;  // a first factorization has been attempted
     nsg::TopologyPlan plan;
 };
 
@@ -81,12 +91,21 @@ cudaError_t upload(T** dst, const T* src, size_t count) {
     return e;
 }
 
-// NeoSolver::numeric on the host engine (load, preorder, gmin, ordering).
+// numeric() of the topology's engine on the host: NeoSolver's load,
+// preorder, gmin and ordering, or AmdLuSolver's full factor_ (with the
+// AutoFallbackSolver switch on a singular first factorization).
 int numeric_on_engine(nsg_topology& t, const double* values, double diag_gmin);
+// Rebuild t.plan from its engine after a successful numeric_on_engine.
+void rebuild_plan(nsg_topology& t);
 
-// nsg_topology_order without the C wrapper (throws on bad input).
+// make_solver's choice (make_solver.cpp:156-178) for a circuit: NSG_SOLVER_*.
+int select_solver(int num_vars, bool is_linear);
+
+// nsg_topology_order without the C wrapper (throws on bad input); solver is
+// an NSG_SOLVER_* engine.
 int order_topology(int n, int nnz, const int* col_ptr, const int* row_idx, const double* values,
-                   double diag_gmin, std::unique_ptr<nsg_topology>& out);
+                   double diag_gmin, std::unique_ptr<nsg_topology>& out,
+                   int solver = NSG_SOLVER_MARKOWITZ);
 
 // PlanDesc for a plan whose arrays were appended to pool.
 nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& pool);

@@ -32,6 +32,7 @@ struct nsg_tran_batch {
     std::vector<nsg::DcDesc> descs;      // launch order = instance order
     std::vector<nsg::TranDesc> tdescs;
     std::vector<std::vector<int32_t>> col_ptr, row_idx;  // per-instance pattern
+    std::vector<int> solver;  // per-instance engine (NSG_SOLVER_*), as make_solver picks it
     int max_col = 0, max_n = 0;
     int64_t work_size = 0, work_cap = 0;
     long long orderings = 0;
@@ -135,8 +136,10 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         // reference creates two solvers, each ordered on its first matrix).
         std::vector<std::vector<double>> ptran(count), bps(count);
         std::vector<double> dt0(count);
+        b->solver.resize(count);
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
+            b->solver[i] = select_solver(c.num_vars(), c.is_linear());
             ptran[i] = c.resolved_params(tstep, tstop);
             bps[i] = controller_breakpoints(c.source_breakpoints(ptran[i], tstop), tstop, max_step);
             double dt = std::min(tstop / 100.0, tstep) / 10.0;  // transient.cpp:851
@@ -159,7 +162,8 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                     std::vector<double> a, r;
                     c.initjct_values(a, r, o.nopt.gmin);
                     rc_dc[i] = order_topology(c.num_vars(), c.nnz(), c.col_ptr().data(),
-                                              c.row_idx().data(), a.data(), 0.0, ord_dc[i]);
+                                              c.row_idx().data(), a.data(), 0.0, ord_dc[i],
+                                              b->solver[i]);
                 }
             });
         for (auto& th : pool) th.join();
@@ -279,7 +283,7 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                 if (ctl.need == 105) {
                     std::unique_ptr<nsg_topology> fresh;
                     rc = order_topology(d.n, d.nnz, b->col_ptr[i].data(), b->row_idx[i].data(),
-                                        a.data(), ctl.need_diag_gmin, fresh);
+                                        a.data(), ctl.need_diag_gmin, fresh, b->solver[i]);
                     if (rc == NSG_OK) topo = intern_topology(b->topos, std::move(fresh));
                 } else {
                     const int cur = ctl.need_plan == 0 ? d.plan : t.tran_plan;
@@ -310,6 +314,20 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
         }
         return NSG_OK;
     });
+}
+
+int nsg_tran_batch_engines(const nsg_tran_batch* b, int* dc_engine, int* tran_engine) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_engines: null batch");
+    auto kind = [&](int topo) {
+        if (topo < 0) return -1;  // not ordered yet
+        return b->topos[topo]->plan.kind == nsg::kPlanKindAmdLu ? NSG_SOLVER_AMDLU
+                                                                 : NSG_SOLVER_MARKOWITZ;
+    };
+    for (int i = 0; i < b->count; ++i) {
+        if (dc_engine) dc_engine[i] = kind(b->descs[i].plan);
+        if (tran_engine) tran_engine[i] = kind(b->tdescs[i].tran_plan);
+    }
+    return NSG_OK;
 }
 
 int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count) {

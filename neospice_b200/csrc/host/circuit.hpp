@@ -104,6 +104,9 @@ public:
 
     void finalize();
     bool finalized() const { return finalized_; }
+    // Circuit::is_linear (src/core/circuit.hpp:171-175): no nonlinear device
+    // (diodes and MOSFETs here).
+    bool is_linear() const { return diodes_.empty() && mos_.empty(); }
 
     int32_t num_nodes() const { return num_nodes_; }
     int32_t num_vars() const { return num_vars_; }

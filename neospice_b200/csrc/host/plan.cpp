@@ -1,5 +1,6 @@
 #include "plan.hpp"
 
+#include "amd_lu.hpp"
 #include "sparse_order.hpp"
 
 #include <algorithm>
@@ -31,13 +32,20 @@ void finish(TopologyPlan& p) {
     p.diag_pos.assign(n, -1);
     for (int32_t j = 0; j < n; ++j) {
         for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
-            if (q > p.col_ptr[j] && p.row_idx[q] <= p.row_idx[q - 1])
+            if (p.kind == kPlanKindMarkowitz && q > p.col_ptr[j] &&
+                p.row_idx[q] <= p.row_idx[q - 1])
                 throw std::invalid_argument("plan: rows not ascending in column " +
                                             std::to_string(j));
             if (p.row_idx[q] == j) p.diag_pos[j] = q;
         }
         if (p.diag_pos[j] < 0)
             throw std::invalid_argument("plan: no pivot in column " + std::to_string(j));
+        for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
+            const int32_t r = p.row_idx[q];
+            if (r < 0 || r >= n || (q < p.diag_pos[j] && r >= j) || (q > p.diag_pos[j] && r <= j))
+                throw std::invalid_argument("plan: U/L rows out of place in column " +
+                                            std::to_string(j));
+        }
     }
 
     // Update map for the left-looking refactor.
@@ -45,7 +53,11 @@ void finish(TopologyPlan& p) {
     p.upd_start.assign(p.nnz_lu, 0);
     p.upd_dst.clear();
     for (int32_t j = 0; j < n; ++j) {
-        for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) where[p.row_idx[q]] = q;
+        for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
+            if (where[p.row_idx[q]] >= 0)
+                throw std::invalid_argument("plan: duplicate row in column " + std::to_string(j));
+            where[p.row_idx[q]] = q;
+        }
         for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j]; ++q) {
             const int32_t r = p.row_idx[q];
             p.upd_start[q] = static_cast<int32_t>(p.upd_dst.size());
@@ -157,7 +169,8 @@ void finish(TopologyPlan& p) {
     X(perm_row) X(perm_col) X(col_ptr) X(row_idx) X(diag_pos) X(lu_src)         \
     X(upd_start) X(upd_dst) X(lrow_ptr) X(lrow_pos) X(lrow_col) X(urow_ptr)     \
     X(urow_pos) X(urow_col) X(col_lev_ptr) X(col_lev) X(fwd_lev_ptr) X(fwd_lev) \
-    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos) X(umeta)
+    X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos) X(umeta) \
+    X(piv_rank) X(gmin_pos)
 
 int64_t TopologyPlan::device_words() const {
     int64_t w = 0;
@@ -196,6 +209,47 @@ TopologyPlan build_plan(const MarkowitzOrder& mo, const std::vector<int32_t>& sl
             p.lu_src.push_back(slot_of[e]);
         }
         p.col_ptr[j] = static_cast<int32_t>(p.row_idx.size());
+    }
+    finish(p);
+    return p;
+}
+
+TopologyPlan build_plan_amd(const AmdLuFactor& f) {
+    if (!f.factored()) throw std::logic_error("build_plan_amd: engine not factored");
+    TopologyPlan p;
+    p.kind = kPlanKindAmdLu;
+    p.n = f.size();
+    p.nnz_a = f.nnz();
+    const int32_t n = p.n;
+    const auto& q = f.q();
+    const auto& pinv = f.pinv();
+    const auto& acp = f.col_ptr();
+    const auto& ari = f.row_idx();
+    p.perm_row.assign(n, -1);
+    for (int32_t r = 0; r < n; ++r) p.perm_row[pinv[r]] = r;
+    p.perm_col = q;
+    p.piv_rank = f.piv_rank();
+    p.gmin_pos.assign(n, -1);
+    p.col_ptr.assign(n + 1, 0);
+    p.row_idx.reserve(f.Li().size() + f.Ui().size());
+    p.lu_src.reserve(f.Li().size() + f.Ui().size());
+    std::vector<int32_t> slot_at(n, -1);  // pivot-step row -> A slot of this column
+    for (int32_t k = 0; k < n; ++k) {
+        const int32_t col = q[k];
+        for (int32_t a = acp[col]; a < acp[col + 1]; ++a) slot_at[pinv[ari[a]]] = a;
+        const int32_t c0 = static_cast<int32_t>(p.row_idx.size());
+        auto push = [&](int32_t s) {
+            if (s == pinv[col]) p.gmin_pos[k] = static_cast<int32_t>(p.row_idx.size()) - c0;
+            p.row_idx.push_back(s);
+            p.lu_src.push_back(slot_at[s]);
+        };
+        // U(:, k) above the pivot in replay order, the pivot (stored last in
+        // U(:, k) by the reference), then L(:, k) after its unit diagonal.
+        for (int32_t u = f.Up()[k]; u < f.Up()[k + 1] - 1; ++u) push(f.Ui()[u]);
+        push(k);
+        for (int32_t l = f.Lp()[k] + 1; l < f.Lp()[k + 1]; ++l) push(f.Li()[l]);
+        for (int32_t a = acp[col]; a < acp[col + 1]; ++a) slot_at[pinv[ari[a]]] = -1;
+        p.col_ptr[k + 1] = static_cast<int32_t>(p.row_idx.size());
     }
     finish(p);
     return p;

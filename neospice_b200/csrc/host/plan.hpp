@@ -8,8 +8,16 @@
 namespace nsg {
 
 class MarkowitzOrder;
+class AmdLuFactor;
+
+// Engines whose pivot sequence a plan replays.
+enum PlanKindHost : int32_t {
+    kPlanKindMarkowitz = 0,  // SparseMatrix (Sparse 1.3): U scaled by 1/pivot
+    kPlanKindAmdLu = 1,      // AmdLuSolver: L scaled by 1/pivot
+};
 
 struct TopologyPlan {
+    int32_t kind = kPlanKindMarkowitz;
     int32_t n = 0;
     int32_t nnz_a = 0;   // slots of the caller's CSC pattern
     int32_t nnz_lu = 0;  // originals + fill-ins
@@ -18,9 +26,12 @@ struct TopologyPlan {
     // internal index i (0-based) -> external row / column (0-based).
     std::vector<int32_t> perm_row, perm_col;
 
-    // LU in CSC, internal order, rows ascending within a column.  In column
-    // j: positions col_ptr[j]..diag_pos[j]-1 are U (rows < j), diag_pos[j] is
-    // the pivot, diag_pos[j]+1..col_ptr[j+1]-1 are L (rows > j).
+    // LU in CSC, internal order.  In column j: positions
+    // col_ptr[j]..diag_pos[j]-1 are U (rows < j), diag_pos[j] is the pivot,
+    // diag_pos[j]+1..col_ptr[j+1]-1 are L (rows > j).  Markowitz plans keep
+    // rows ascending; AMD-LU plans keep the U rows in the order the
+    // refactor must apply them (the reach's topological order) and the L
+    // rows in the reference's stored order.
     std::vector<int32_t> col_ptr, row_idx, diag_pos;
 
     // Load map: per LU position, the caller's CSC slot, or -1 for a fill-in.
@@ -58,6 +69,13 @@ struct TopologyPlan {
     std::vector<int32_t> bwd_lev_ptr, bwd_lev;
     std::vector<int32_t> tbw_lev_ptr, tbw_lev;
 
+    // AMD-LU plans only (empty otherwise), per column k: the pivot's rank
+    // among the candidate rows (pivot + L rows, in reach order; -1 when the
+    // pivot was outside the reach), and the position, relative to the
+    // column start, of the entry that receives diag_gmin (the row of the
+    // column's own diagonal element of A), or -1 when the column has none.
+    std::vector<int32_t> piv_rank, gmin_pos;
+
     // Algorithmic work: multiply-subtract updates of one refactor (each is
     // 2 flops), and the reciprocal pivots.
     int64_t updates = 0;
@@ -79,6 +97,10 @@ struct TopologyPlan {
 // Build from the host ordering engine after order_and_factor.  slot_elem[k]
 // is the engine element of caller CSC slot k.
 TopologyPlan build_plan(const MarkowitzOrder& mo, const std::vector<int32_t>& slot_elem);
+
+// Build from the AMD-LU engine after a successful factor(): the pivot
+// sequence, L/U structure and replay order of AmdLuSolver::factor_.
+TopologyPlan build_plan_amd(const AmdLuFactor& f);
 
 // Build from an exported structure (the reference's own NeoSolver state):
 // elements column by column in internal order (1-based rows/cols), the slot

@@ -44,6 +44,102 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
+// Verdict on column k of an AMD-LU replay, computed by one warp from the
+// column's values after all its U updates (col: relative to the column
+// start; dj: the pivot's position; colmax: the largest |U(r, k)| applied).
+//   growth_fail (kCheckRefactor only): refactor_replay_'s growth test
+//     (amd_lu_solver.cpp:250-259), u_kk == 0 or |u_kk| < 1e-3 *
+//     max(colmax, |u_kk|).  On any such column the reference abandons the
+//     replay and runs a full factor_ on the same values.
+//   code (kCheckNumeric and kCheckRefactor): whether factor_ on these
+//     values (amd_lu_solver.cpp:134-157) would pick the plan's pivot row --
+//     the first candidate of largest |x| in reach order, unless the row of
+//     the column's own diagonal is a candidate within 1e-3 of that maximum;
+//     no candidate above zero -> kStatusSingular, another row ->
+//     kStatusReorder.  When every column agrees, factor_ reproduces the
+//     replay's values bit for bit, so a failed growth test costs nothing.
+//   kCheckNone: code is kStatusSingular for u_kk == 0.
+// Ends with __syncwarp(): the caller may overwrite the column afterwards.
+struct AmdColumn {
+    int32_t code;
+    bool growth_fail;
+};
+
+__device__ inline AmdColumn amd_column_status(const double* col, int32_t dj, int32_t len,
+                                              double colmax, int check, int32_t piv_rank,
+                                              int32_t gpos, int lane) {
+    const double piv = col[dj];
+    AmdColumn r{(piv == 0.0) ? kStatusSingular : kStatusOk, false};
+    if (check == kCheckRefactor) {
+        const double a = fabs(piv);
+        const double cm = a > colmax ? a : colmax;
+        r.growth_fail = (piv == 0.0 || (cm > 0.0 && a < 1e-3 * cm));
+    }
+    if (check == kCheckNumeric || check == kCheckRefactor) {
+        double best = -1.0;
+        int32_t best_rank = INT32_MAX, best_pos = -1;
+        for (int32_t t = dj + lane; t < len; t += 32) {
+            int32_t rank;
+            if (t == dj) {
+                if (piv_rank < 0) continue;  // the pivot was not in the reach
+                rank = piv_rank;
+            } else {
+                const int32_t m = t - dj - 1;
+                rank = (piv_rank >= 0 && m >= piv_rank) ? m + 1 : m;
+            }
+            const double v = fabs(col[t]);
+            if (v > best || (v == best && rank < best_rank)) {
+                best = v;
+                best_rank = rank;
+                best_pos = t;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int32_t orank = __shfl_xor_sync(0xffffffffu, best_rank, o);
+            const int32_t opos = __shfl_xor_sync(0xffffffffu, best_pos, o);
+            if (ob > best || (ob == best && orank < best_rank)) {
+                best = ob;
+                best_rank = orank;
+                best_pos = opos;
+            }
+        }
+        if (best_pos < 0 || best <= 0.0) {
+            r.code = kStatusSingular;
+        } else {
+            int32_t chosen = best_pos;
+            if (gpos >= dj && fabs(col[gpos]) >= best * 1e-3) chosen = gpos;
+            r.code = (chosen != dj) ? kStatusReorder : (piv == 0.0 ? kStatusSingular : kStatusOk);
+        }
+    }
+    __syncwarp();
+    return r;
+}
+
+// Outcome of an AMD-LU refactor from the first column verdict that failed
+// (packed by fail_key, ~0 if none) and whether any growth test failed.  A
+// refactorize() whose growth tests all pass keeps the replay; otherwise, as
+// for a numeric(), the first failing verdict decides.
+__device__ __forceinline__ bool amd_verdict_counts(int check, bool any_growth_fail) {
+    return check != kCheckRefactor || any_growth_fail;
+}
+
+// Value stored at relative position t of a finished column (pivot at dj):
+// Markowitz keeps L as eliminated and stores 1 / pivot; AMD-LU divides L by
+// the pivot and keeps the pivot.
+__device__ __forceinline__ double lu_store_value(bool amd, double v, int32_t t, int32_t dj,
+                                                 double piv) {
+    if (amd) return t > dj ? __ddiv_rn(v, piv) : v;
+    return t == dj ? 1.0 / piv : v;
+}
+
+// First failing column and its status, packed for one atomicMin.
+__device__ __forceinline__ unsigned long long fail_key(int32_t step, int32_t code) {
+    return (static_cast<unsigned long long>(static_cast<uint32_t>(step)) << 32) |
+           static_cast<uint32_t>(code);
+}
+
 // Shared memory of the dataflow refactor: kFlowWarps column buffers of
 // colbuf doubles, then n int32 completion flags.
 __host__ __device__ inline size_t flow_smem_bytes(int colbuf, int n) {
@@ -60,9 +156,11 @@ struct RefactorResult {
 // before using column r a warp waits for done[r], so independent columns
 // overlap and the dense trailing block pipelines as a wavefront.  Column j
 // stays in a per-warp shared buffer from its load (A gathered through lu_src,
-// diag_gmin added to the pivot) to its write-back.  check_pivots applies the
-// re-validation test of SparseMatrix::order_and_factor (factor.cpp:929-947);
-// otherwise only an exact zero pivot fails, as in SparseMatrix::factor.  Every
+// diag_gmin added) to its write-back.  check_pivots is a kCheck* mode: for
+// Markowitz plans kCheckNumeric applies the re-validation test of
+// SparseMatrix::order_and_factor (factor.cpp:929-947), otherwise only an
+// exact zero pivot fails, as in SparseMatrix::factor; AMD-LU plans follow
+// amd_column_status.  Every
 // wait is bounded: past kSpinLimit polls the instance reports kStatusTimeout
 // and the warp moves on, so the CTA always finishes.  Begins and ends with
 // __syncthreads().
@@ -82,18 +180,23 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
     const int32_t* upd_start = pool + pd.off[PA_upd_start];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
 
+    const bool amd = pd.kind == kPlanAmdLu;
+    const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
+    const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     double* buf = smem + warp * colbuf;
     volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + kFlowWarps * colbuf);
 
-    __shared__ int32_t s_next, s_fail_step, s_fail_code;
+    __shared__ int32_t s_next, s_timeout, s_growth;
+    __shared__ unsigned long long s_fail;
     __syncthreads();
     for (int32_t j = threadIdx.x; j < n; j += blockDim.x) done[j] = 0;
     if (threadIdx.x == 0) {
         s_next = 0;
-        s_fail_step = INT32_MAX;
-        s_fail_code = kStatusOk;
+        s_timeout = 0;
+        s_growth = 0;
+        s_fail = ~0ull;
     }
     __syncthreads();
 
@@ -105,13 +208,15 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
         const int32_t c0 = col_ptr[j];
         const int32_t len = col_ptr[j + 1] - c0;
         const int32_t dj = diag_pos[j] - c0;
+        const int32_t gp = amd ? gmin_pos[j] : dj;
         for (int32_t t = lane; t < len; t += 32) {
             const int32_t s = lu_src[c0 + t];
             double v = (s >= 0) ? a[s] : 0.0;
-            if (t == dj && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+            if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
             buf[t] = v;
         }
         __syncwarp();
+        double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
         // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
         // entries at a time in registers (lane k holds entry base+k) and
         // broadcast by shuffle.  One-step lookahead: while the update of
@@ -178,7 +283,8 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
             int32_t l0_n = 0, cnt_n = 0, us_n = 0, ld_n = 0;
             const bool have_n = (q + 1 < dj) &&
                                 fetch(meta(q + 1 - base), false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
-            const double u = lu_mul(buf[q], rd_c);
+            const double u = amd ? buf[q] : lu_mul(buf[q], rd_c);
+            colmax = fmax(colmax, fabs(u));
             __syncwarp();
             if (lane == 0) buf[q] = u;
             if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
@@ -196,52 +302,67 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
             ld_c = ld_n;
         }
         const double piv = buf[dj];
-        bool fail;
-        if (check_pivots) {
+        int32_t code;
+        bool growth_fail = false;
+        if (amd) {
+            const AmdColumn v = amd_column_status(buf, dj, len, colmax, check_pivots, piv_rank[j],
+                                                  gmin_pos[j], lane);
+            code = v.code;
+            growth_fail = v.growth_fail;
+        } else if (check_pivots == kCheckNumeric) {
             double largest = 0.0;
             for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(buf[t]));
             largest = warp_max(largest);
-            fail = !(largest * rel_threshold < fabs(piv));
+            code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
         } else {
-            fail = (piv == 0.0);
+            code = (piv == 0.0) ? kStatusSingular : kStatusOk;
         }
-        for (int32_t t = lane; t < len; t += 32) lu[c0 + t] = (t == dj) ? 1.0 / piv : buf[t];
-        if (lrows) {
-            const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
-            for (int32_t t = lane; t < len; t += 32) {
-                if (t < dj) urows[rowcopy[c0 + t]] = buf[t];
-                else if (t > dj) lrows[rowcopy[c0 + t]] = buf[t];
+        const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
+        for (int32_t t = lane; t < len; t += 32) {
+            const double v = lu_store_value(amd, buf[t], t, dj, piv);
+            lu[c0 + t] = v;
+            if (lrows) {
+                if (t < dj) urows[rowcopy[c0 + t]] = v;
+                else if (t > dj) lrows[rowcopy[c0 + t]] = v;
             }
         }
         __syncwarp();
         if (lane == 0) {
-            if (timed_out) {
-                s_fail_code = kStatusTimeout;
-                atomicMin(&s_fail_step, j);
-            } else if (fail) {
-                atomicMin(&s_fail_step, j);
-                if (s_fail_code != kStatusTimeout)
-                    s_fail_code = check_pivots ? kStatusReorder : kStatusSingular;
-            }
+            if (timed_out) s_timeout = 1;
+            else if (code != kStatusOk) atomicMin(&s_fail, fail_key(j, code));
+            if (growth_fail) s_growth = 1;
             flag_release(done + j, 1);
         }
         __syncwarp();
     }
     __syncthreads();
     RefactorResult res;
-    res.code = s_fail_code;
-    res.step = (s_fail_code == kStatusOk) ? -1 : s_fail_step;
+    if (s_timeout) {
+        res.code = kStatusTimeout;
+        res.step = -1;
+    } else if (s_fail == ~0ull || (amd && !amd_verdict_counts(check_pivots, s_growth != 0))) {
+        res.code = kStatusOk;
+        res.step = -1;
+    } else {
+        res.code = static_cast<int32_t>(s_fail & 0xffffffffu);
+        res.step = static_cast<int32_t>(s_fail >> 32);
+    }
     __syncthreads();
     return res;
 }
 
-// x <- A^{-1} x (SparseMatrix::solve) by the whole CTA; w is an n-vector of
-// scratch.  Level-synchronous, a thread per row.  Begins and ends with
-// __syncthreads().
+// x <- A^{-1} x (SparseMatrix::solve, or AmdLuSolver::solve,
+// amd_lu_solver.cpp:303-344, for AMD-LU plans) by the whole CTA; w is an
+// n-vector of scratch.  Level-synchronous, a thread per row.  Each row
+// applies its updates in the order the reference's column-oriented sweeps
+// reach it: forward columns ascending; backward ascending for Markowitz
+// (row dot product, solve.cpp:30-44), descending for AMD-LU.  Begins and ends
+// with __syncthreads().
 __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__ pool,
                                  const double* __restrict__ lu, double* __restrict__ x,
                                  double* __restrict__ w) {
     const int32_t n = pd.n;
+    const bool amd = pd.kind == kPlanAmdLu;
     const int32_t* perm_row = pool + pd.off[PA_perm_row];
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
@@ -258,6 +379,12 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
             for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
                 const int32_t i = lev[k];
                 double t = w[i];
+                if (amd) {
+                    for (int32_t e = lp[i]; e < lp[i + 1]; ++e)
+                        t = lu_sub(t, lu_mul(lu[lpos[e]], w[lcol[e]]));
+                    w[i] = t;
+                    continue;
+                }
                 for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
                     const double xc = w[lcol[e]];
                     if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu[lpos[e]]));
@@ -267,7 +394,8 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
             __syncthreads();
         }
     }
-    {   // backward: unit-diagonal U, row dot products
+    {   // backward: Markowitz unit-diagonal U, row dot products in ascending
+        // column order; AMD-LU columns descending, then the pivot division
         const int32_t* up = pool + pd.off[PA_urow_ptr];
         const int32_t* upos = pool + pd.off[PA_urow_pos];
         const int32_t* ucol = pool + pd.off[PA_urow_col];
@@ -277,6 +405,12 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
             for (int32_t k = lev_ptr[l] + threadIdx.x; k < lev_ptr[l + 1]; k += blockDim.x) {
                 const int32_t i = lev[k];
                 double t = w[i];
+                if (amd) {
+                    for (int32_t e = up[i + 1] - 1; e >= up[i]; --e)
+                        t = lu_sub(t, lu_mul(lu[upos[e]], w[ucol[e]]));
+                    w[i] = __ddiv_rn(t, lu[diag_pos[i]]);
+                    continue;
+                }
                 for (int32_t e = up[i]; e < up[i + 1]; ++e)
                     t = lu_sub(t, lu_mul(lu[upos[e]], w[ucol[e]]));
                 w[i] = t;
@@ -321,25 +455,32 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
     const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]);
+    const bool amd = pd.kind == kPlanAmdLu;
+    const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
+    const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
     const int lane = threadIdx.x & 31;
-    __shared__ int32_t s_fail_step;
+    __shared__ int32_t s_fail_step, s_fail_code;
     __syncthreads();
     if (threadIdx.x < 32) {
-        int32_t fail_step = INT32_MAX;
+        int32_t fail_step = INT32_MAX, fail_code = kStatusOk;
+        bool any_growth = false;
         for (int32_t j = 0; j < n; ++j) {
             const int32_t c0 = col_ptr[j];
             const int32_t len = col_ptr[j + 1] - c0;
             const int32_t dj = diag_pos[j] - c0;
+            const int32_t gp = amd ? gmin_pos[j] : dj;
             for (int32_t t = lane; t < len; t += 32) {
                 const int32_t src = lu_src[c0 + t];
                 double v = (src >= 0) ? a[src] : 0.0;
-                if (t == dj && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+                if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
                 lu_s[c0 + t] = v;
             }
             __syncwarp();
+            double colmax = 0.0;
             for (int32_t q = 0; q < dj; ++q) {
                 const int4 m = umeta[c0 + q];  // r, diag_pos[r], |L(:, r)|, upd_start
-                const double u = lu_mul(lu_s[c0 + q], lu_s[m.y]);
+                const double u = amd ? lu_s[c0 + q] : lu_mul(lu_s[c0 + q], lu_s[m.y]);
+                colmax = fmax(colmax, fabs(u));
                 for (int32_t t = lane; t < m.z; t += 32) {
                     const int32_t d = upd_dst[m.w + t];
                     lu_s[c0 + d] = lu_sub(lu_s[c0 + d], lu_mul(u, lu_s[m.y + 1 + t]));
@@ -349,28 +490,44 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
                 __syncwarp();
             }
             const double piv = lu_s[c0 + dj];
-            bool fail;
-            if (check_pivots) {
+            int32_t code;
+            if (amd) {
+                const AmdColumn v = amd_column_status(lu_s + c0, dj, len, colmax, check_pivots,
+                                                      piv_rank[j], gmin_pos[j], lane);
+                code = v.code;
+                any_growth = any_growth || v.growth_fail;
+            } else if (check_pivots == kCheckNumeric) {
                 double largest = 0.0;
                 for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(lu_s[c0 + t]));
                 largest = warp_max(largest);
-                fail = !(largest * rel_threshold < fabs(piv));
+                code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
             } else {
-                fail = (piv == 0.0);
+                code = (piv == 0.0) ? kStatusSingular : kStatusOk;
             }
-            if (fail && j < fail_step) fail_step = j;
+            if (code != kStatusOk && j < fail_step) {
+                fail_step = j;
+                fail_code = code;
+            }
             __syncwarp();
-            if (lane == 0) lu_s[c0 + dj] = 1.0 / piv;
+            if (amd) {
+                for (int32_t t = dj + 1 + lane; t < len; t += 32)
+                    lu_s[c0 + t] = __ddiv_rn(lu_s[c0 + t], piv);
+            } else if (lane == 0) {
+                lu_s[c0 + dj] = 1.0 / piv;
+            }
             __syncwarp();
         }
-        if (lane == 0) s_fail_step = fail_step;
+        if (amd && !amd_verdict_counts(check_pivots, any_growth)) fail_step = INT32_MAX;
+        if (lane == 0) {
+            s_fail_step = fail_step;
+            s_fail_code = fail_code;
+        }
     }
     __syncthreads();
     for (int32_t k = threadIdx.x; k < pd.nnz_lu; k += blockDim.x) lu[k] = lu_s[k];
     RefactorResult res;
     res.step = s_fail_step == INT32_MAX ? -1 : s_fail_step;
-    res.code = s_fail_step == INT32_MAX ? kStatusOk
-                                        : (check_pivots ? kStatusReorder : kStatusSingular);
+    res.code = s_fail_step == INT32_MAX ? kStatusOk : s_fail_code;
     __syncthreads();
     return res;
 }
@@ -385,12 +542,13 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
     const int32_t* perm_row = pool + pd.off[PA_perm_row];
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const bool amd = pd.kind == kPlanAmdLu;
     const int lane = threadIdx.x & 31;
     __syncthreads();
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
     __syncthreads();
     if (threadIdx.x < 32) {
-        {   // forward: L with the reciprocal pivot
+        {   // forward: L (Markowitz: then the reciprocal pivot)
             const int32_t* lp = pool + pd.off[PA_lrow_ptr];
             const int32_t* lpos = pool + pd.off[PA_lrow_pos];
             const int32_t* lcol = pool + pd.off[PA_lrow_col];
@@ -400,6 +558,12 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
                 for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
                     const int32_t i = lev[k];
                     double t = w[i];
+                    if (amd) {
+                        for (int32_t e = lp[i]; e < lp[i + 1]; ++e)
+                            t = lu_sub(t, lu_mul(lu_s[lpos[e]], w[lcol[e]]));
+                        w[i] = t;
+                        continue;
+                    }
                     for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
                         const double xc = w[lcol[e]];
                         if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu_s[lpos[e]]));
@@ -409,7 +573,8 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
                 __syncwarp();
             }
         }
-        {   // backward: unit-diagonal U, row dot products
+        {   // backward: U row dot products (AMD-LU: columns descending, then
+            // the pivot division)
             const int32_t* up = pool + pd.off[PA_urow_ptr];
             const int32_t* upos = pool + pd.off[PA_urow_pos];
             const int32_t* ucol = pool + pd.off[PA_urow_col];
@@ -419,6 +584,12 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
                 for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
                     const int32_t i = lev[k];
                     double t = w[i];
+                    if (amd) {
+                        for (int32_t e = up[i + 1] - 1; e >= up[i]; --e)
+                            t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
+                        w[i] = __ddiv_rn(t, lu_s[diag_pos[i]]);
+                        continue;
+                    }
                     for (int32_t e = up[i]; e < up[i + 1]; ++e)
                         t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
                     w[i] = t;
@@ -465,6 +636,7 @@ static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int
     const int32_t* perm_row = pool + pd.off[PA_perm_row];
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const bool amd = pd.kind == kPlanAmdLu;
     volatile double* w = smem;
     volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + n);
     __shared__ int32_t s_ok;
@@ -489,30 +661,34 @@ static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int
                 const double lv = lrows[e];
                 if (ok && !wait_flag(done, c)) ok = false;
                 const double xc = w[c];
-                if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lv));
+                if (amd) t = lu_sub(t, lu_mul(lv, xc));
+                else if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lv));
             }
-            w[i] = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
+            if (!amd) t = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
+            w[i] = t;
             flag_release(done + i, 1);
         }
     }
     __syncthreads();
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) done[i] = 0;
     __syncthreads();
-    {   // backward: unit-diagonal U
+    {   // backward: Markowitz unit-diagonal U, columns ascending; AMD-LU
+        // columns descending, then the pivot division
         const int32_t* up = pool + pd.off[PA_urow_ptr];
         const int32_t* ucol = pool + pd.off[PA_urow_col];
         const int32_t* order = pool + pd.off[PA_bwd_lev];
         for (int32_t k = threadIdx.x; k < n; k += blockDim.x) {
             const int32_t i = order[k];
             double t = w[i];
-            const int32_t e1 = up[i + 1];
-            for (int32_t e = up[i]; e < e1; ++e) {
+            const int32_t e0 = up[i], e1 = up[i + 1];
+            for (int32_t m = 0; m < e1 - e0; ++m) {
+                const int32_t e = amd ? e1 - 1 - m : e0 + m;
                 const int32_t c = ucol[e];
                 const double uv = urows[e];
                 if (ok && !wait_flag(done, c)) ok = false;
                 t = lu_sub(t, lu_mul(uv, w[c]));
             }
-            w[i] = t;
+            w[i] = amd ? __ddiv_rn(t, lu[diag_pos[i]]) : t;
             flag_release(done + i, 1);
         }
     }
@@ -524,7 +700,9 @@ static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int
     return all_ok;
 }
 
-// x <- A^{-T} x (SparseMatrix::solve_transposed) by the whole CTA.
+// x <- A^{-T} x (SparseMatrix::solve_transposed) by the whole CTA.  AMD-LU
+// plans (the reference's AmdLuSolver has no transposed solve) use
+// A^T = Q U^T L^T P: U^T forward with the pivot division, then unit L^T.
 __device__ inline void cta_solve_transposed(const PlanDesc& pd, const int32_t* __restrict__ pool,
                                             const double* __restrict__ lu, double* __restrict__ x,
                                             double* __restrict__ w) {
@@ -534,10 +712,12 @@ __device__ inline void cta_solve_transposed(const PlanDesc& pd, const int32_t* _
     const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
     const int32_t* row_idx = pool + pd.off[PA_row_idx];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const bool amd = pd.kind == kPlanAmdLu;
     __syncthreads();
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_col[i]];
     __syncthreads();
-    {   // forward over U^T: column c gathers its U entries, rows ascending
+    {   // forward over U^T: column c gathers its U entries in stored order
+        // (AMD-LU: then divides by the pivot)
         const int32_t* lev_ptr = pool + pd.off[PA_col_lev_ptr];
         const int32_t* lev = pool + pd.off[PA_col_lev];
         for (int32_t l = 0; l < pd.n_col_lev; ++l) {
@@ -548,12 +728,12 @@ __device__ inline void cta_solve_transposed(const PlanDesc& pd, const int32_t* _
                     const double xr = w[row_idx[q]];
                     if (xr != 0.0) t = lu_sub(t, lu_mul(xr, lu[q]));
                 }
-                w[c] = t;
+                w[c] = amd ? __ddiv_rn(t, lu[diag_pos[c]]) : t;
             }
             __syncthreads();
         }
     }
-    {   // backward over L^T with the reciprocal pivot
+    {   // backward over L^T (Markowitz: then the reciprocal pivot)
         const int32_t* lev_ptr = pool + pd.off[PA_tbw_lev_ptr];
         const int32_t* lev = pool + pd.off[PA_tbw_lev];
         for (int32_t l = 0; l < pd.n_tbw_lev; ++l) {
@@ -562,7 +742,7 @@ __device__ inline void cta_solve_transposed(const PlanDesc& pd, const int32_t* _
                 double t = w[i];
                 for (int32_t q = diag_pos[i] + 1; q < col_ptr[i + 1]; ++q)
                     t = lu_sub(t, lu_mul(lu[q], w[row_idx[q]]));
-                w[i] = lu_mul(t, lu[diag_pos[i]]);
+                w[i] = amd ? t : lu_mul(t, lu[diag_pos[i]]);
             }
             __syncthreads();
         }

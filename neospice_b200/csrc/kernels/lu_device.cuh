@@ -10,7 +10,8 @@ enum PlanArray : int {
     PA_perm_row, PA_perm_col, PA_col_ptr, PA_row_idx, PA_diag_pos, PA_lu_src,
     PA_upd_start, PA_upd_dst, PA_lrow_ptr, PA_lrow_pos, PA_lrow_col, PA_urow_ptr,
     PA_urow_pos, PA_urow_col, PA_col_lev_ptr, PA_col_lev, PA_fwd_lev_ptr, PA_fwd_lev,
-    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_rowcopy_pos, PA_umeta, PA_COUNT
+    PA_bwd_lev_ptr, PA_bwd_lev, PA_tbw_lev_ptr, PA_tbw_lev, PA_rowcopy_pos, PA_umeta,
+    PA_piv_rank, PA_gmin_pos, PA_COUNT
 };
 
 struct PlanDesc {
@@ -18,7 +19,7 @@ struct PlanDesc {
     int32_t n_col_lev, n_fwd_lev, n_bwd_lev, n_tbw_lev;
     int32_t max_col;  // longest LU column
     int32_t nnz_l, nnz_u;  // strictly lower / upper entries
-    int32_t pad;
+    int32_t kind;          // kPlanMarkowitz or kPlanAmdLu
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
 };
 
@@ -32,6 +33,26 @@ struct InstDesc {
     int64_t lrows_off;  // into the batch's row-major L copy
     int64_t urows_off;  // into the batch's row-major U copy
 };
+
+// Engine whose factorization a plan replays.
+//   kPlanMarkowitz: SparseMatrix::factor (src/solver/factor.cpp:980-1052).
+//     U(r, j) = a(r, j) * (1 / p_r), L unscaled, the pivot stored as its
+//     reciprocal; U entries applied in ascending row order.
+//   kPlanAmdLu: AmdLuSolver::refactor_replay_ (src/core/amd_lu_solver.cpp:
+//     214-271).  U unscaled, L(i, k) = x_i / u_kk, the pivot stored as is; U
+//     entries applied in the stored (reach) order.
+enum : int32_t { kPlanMarkowitz = 0, kPlanAmdLu = 1 };
+
+// What a refactor checks beyond an exact zero pivot.
+//   kCheckNone:     nothing (spFactor; a replay whose pivots the host chose).
+//   kCheckNumeric:  a numeric() on an already factored solver.  Markowitz:
+//     the pivot re-validation of order_and_factor (factor.cpp:929-947).
+//     AMD-LU: factor_'s threshold pivot choice (amd_lu_solver.cpp:134-157)
+//     must pick the plan's pivot row.  Failure -> kStatusReorder.
+//   kCheckRefactor: a refactorize().  Markowitz: as kCheckNone.  AMD-LU: the
+//     replay's pivot-growth test (amd_lu_solver.cpp:256-259); failure ->
+//     kStatusReorder (the reference falls back to a full factor_).
+enum : int { kCheckNone = 0, kCheckNumeric = 1, kCheckRefactor = 2 };
 
 // Per-instance status codes written by the refactor.
 enum : int32_t {

@@ -32,12 +32,14 @@ __device__ __forceinline__ double mul(double x, double y) { return __dmul_rn(x, 
 __device__ __forceinline__ double sub(double x, double y) { return __dsub_rn(x, y); }
 }  // namespace
 
-// Load A into the LU pattern, add diag_gmin to every pivot, then eliminate
-// column by column.  check_pivots != 0 applies the re-validation test of
-// SparseMatrix::order_and_factor (factor.cpp:929-947): the pivot must exceed
-// rel_threshold times the largest entry below it, else the instance is
-// flagged kStatusReorder at that step.  Otherwise only an exact zero pivot is
-// flagged (kStatusSingular), as in SparseMatrix::factor.
+// Load A into the LU pattern, add diag_gmin to every pivot (AMD-LU: to the
+// column's own diagonal entry of A), then eliminate column by column.
+// check_pivots is a kCheck* mode.  Markowitz plans: kCheckNumeric applies the
+// re-validation test of SparseMatrix::order_and_factor (factor.cpp:929-947):
+// the pivot must exceed rel_threshold times the largest entry below it, else
+// the instance is flagged kStatusReorder at that step; otherwise only an
+// exact zero pivot is flagged (kStatusSingular), as in SparseMatrix::factor.
+// AMD-LU plans follow amd_column_status.
 __global__ void __launch_bounds__(256)
 refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
                 const InstDesc* __restrict__ insts, const double* __restrict__ A,
@@ -58,11 +60,14 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
     const double* a = A + inst.a_off;
     double* lu = LU + inst.lu_off;
 
-    __shared__ int32_t s_fail_step;
-    __shared__ int32_t s_fail_code;
+    const bool amd = pd.kind == kPlanAmdLu;
+    const int32_t* piv_rank = p[PA_piv_rank];
+    const int32_t* gmin_pos = p[PA_gmin_pos];
+    __shared__ unsigned long long s_fail;
+    __shared__ int32_t s_growth;
     if (threadIdx.x == 0) {
-        s_fail_step = INT32_MAX;
-        s_fail_code = kStatusOk;
+        s_fail = ~0ull;
+        s_growth = 0;
     }
 
     for (int32_t q = threadIdx.x; q < pd.nnz_lu; q += blockDim.x) {
@@ -71,8 +76,10 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
     }
     __syncthreads();
     if (diag_gmin != 0.0)
-        for (int32_t j = threadIdx.x; j < pd.n; j += blockDim.x)
-            lu[diag_pos[j]] = __dadd_rn(lu[diag_pos[j]], diag_gmin);
+        for (int32_t j = threadIdx.x; j < pd.n; j += blockDim.x) {
+            const int32_t g = amd ? (gmin_pos[j] < 0 ? -1 : col_ptr[j] + gmin_pos[j]) : diag_pos[j];
+            if (g >= 0) lu[g] = __dadd_rn(lu[g], diag_gmin);
+        }
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
@@ -82,9 +89,11 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
         for (int32_t k = lev_ptr[l] + warp; k < lev_ptr[l + 1]; k += nwarps) {
             const int32_t j = lev[k];
             const int32_t dj = diag_pos[j];
+            double colmax = 0.0;
             for (int32_t q = col_ptr[j]; q < dj; ++q) {
                 const int32_t r = row_idx[q];
-                const double u = mul(lu[q], lu[diag_pos[r]]);
+                const double u = amd ? lu[q] : mul(lu[q], lu[diag_pos[r]]);
+                colmax = fmax(colmax, fabs(u));
                 __syncwarp();
                 if (lane == 0) lu[q] = u;
                 const int32_t l0 = diag_pos[r] + 1;
@@ -98,31 +107,39 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
                 __syncwarp();
             }
             const double piv = lu[dj];
-            bool fail;
-            if (check_pivots) {
+            const int32_t c0 = col_ptr[j];
+            const int32_t len = col_ptr[j + 1] - c0;
+            int32_t code;
+            if (amd) {
+                const AmdColumn v = amd_column_status(lu + c0, dj - c0, len, colmax, check_pivots,
+                                                      piv_rank[j], gmin_pos[j], lane);
+                code = v.code;
+                if (lane == 0 && v.growth_fail) s_growth = 1;
+            } else if (check_pivots == kCheckNumeric) {
                 double largest = 0.0;
                 for (int32_t q = dj + 1 + lane; q < col_ptr[j + 1]; q += 32)
                     largest = fmax(largest, fabs(lu[q]));
                 largest = warp_max(largest);
-                fail = !(largest * rel_threshold < fabs(piv));
+                code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
             } else {
-                fail = (piv == 0.0);
+                code = (piv == 0.0) ? kStatusSingular : kStatusOk;
             }
             __syncwarp();
-            if (lane == 0) {
-                if (fail) {
-                    atomicMin(&s_fail_step, j);
-                    s_fail_code = check_pivots ? kStatusReorder : kStatusSingular;
-                }
+            if (amd) {
+                for (int32_t q = dj + 1 + lane; q < col_ptr[j + 1]; q += 32)
+                    lu[q] = __ddiv_rn(lu[q], piv);
+            } else if (lane == 0) {
                 lu[dj] = 1.0 / piv;
             }
+            if (lane == 0 && code != kStatusOk) atomicMin(&s_fail, fail_key(j, code));
             __syncwarp();
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        status[inst.index] = s_fail_code;
-        if (fail_step) fail_step[inst.index] = (s_fail_code == kStatusOk) ? -1 : s_fail_step;
+        const bool ok = s_fail == ~0ull || (amd && !amd_verdict_counts(check_pivots, s_growth != 0));
+        status[inst.index] = ok ? kStatusOk : static_cast<int32_t>(s_fail & 0xffffffffu);
+        if (fail_step) fail_step[inst.index] = ok ? -1 : static_cast<int32_t>(s_fail >> 32);
     }
 }
 

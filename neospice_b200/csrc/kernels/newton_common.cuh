@@ -321,7 +321,12 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             out = {kStatusNeedOrder, iter + 1, iter, mode, s_dev_conv};
             break;
         }
-        const int check = numeric && solver->factored && !resumed;
+        // numeric() on a factored solver re-validates (Markowitz) or
+        // re-chooses (AMD-LU) the pivots; refactorize() replays them (AMD-LU
+        // with the growth test).  A resumed iteration replays the pivots the
+        // host just chose.
+        const int check = numeric ? ((solver->factored && !resumed) ? kCheckNumeric : kCheckNone)
+                                  : kCheckRefactor;
         const RefactorResult fr =
             small ? cta_refactor_small(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, lu_s)
                   : cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, smem,
@@ -338,6 +343,12 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
             }
             if (threadIdx.x == 0) solver->factored = 1;
             force_numeric = false;
+        } else if (fr.code == kStatusReorder) {
+            // AMD-LU replay failed its growth test: the reference's
+            // refactorize() falls back to a full factor_ on this matrix,
+            // which the host performs before this iteration resumes.
+            out = {fr.code, iter + 1, iter, mode, s_dev_conv};
+            break;
         } else if (fr.code != kStatusOk) {
             force_numeric = true;  // newton.cpp:229-234: retry with numeric
             for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = v.xold[i];

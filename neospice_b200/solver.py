@@ -13,6 +13,27 @@ import numpy as np
 from . import _lib as L
 
 
+# Engine codes of nsg_topology_order_solver (NSG_SOLVER_*).
+SOLVERS = {"markowitz": 0, "amdlu": 1, "auto-amdlu": 2}
+
+
+def select_solver(num_vars: int, is_linear: bool) -> str:
+    """make_solver's engine choice (src/core/make_solver.cpp:156-178), with
+    the NEOSPICE_SOLVER / NEOSPICE_FORCE_AMDLU overrides."""
+    k = L.lib().nsg_solver_select(int(num_vars), int(bool(is_linear)))
+    return {v: n for n, v in SOLVERS.items()}[k]
+
+
+def amd_order(n, col_ptr, row_idx) -> np.ndarray:
+    """amd_ordering (src/core/amd.cpp:14-143): perm[k] = column eliminated at
+    step k."""
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_idx, np.int32)
+    perm = np.zeros(int(n), np.int32)
+    L.check(L.lib().nsg_amd_order(int(n), L.iptr(cp), L.iptr(ri), L.iptr(perm)))
+    return perm
+
+
 class Topology:
     """One factored sparsity structure: pivot sequence + fill pattern.
 
@@ -30,14 +51,25 @@ class Topology:
         return self._h
 
     @classmethod
-    def order(cls, n, col_ptr, row_idx, values, diag_gmin=0.0) -> "Topology":
+    def order(cls, n, col_ptr, row_idx, values, diag_gmin=0.0, solver="markowitz") -> "Topology":
+        """Symbolic phase + first numeric().  ``solver``: "markowitz"
+        (NeoSolver), "amdlu" (AmdLuSolver) or "auto-amdlu" (make_solver's
+        AutoFallbackSolver: AMD-LU, Markowitz if the first factor is
+        singular)."""
         cp = np.ascontiguousarray(col_ptr, np.int32)
         ri = np.ascontiguousarray(row_idx, np.int32)
         v = np.ascontiguousarray(values, np.float64)
         h = ctypes.c_void_p()
-        L.check(L.lib().nsg_topology_order(int(n), len(ri), L.iptr(cp), L.iptr(ri), L.dptr(v),
-                                           float(diag_gmin), ctypes.byref(h)))
+        L.check(L.lib().nsg_topology_order_solver(int(n), len(ri), L.iptr(cp), L.iptr(ri),
+                                                  L.dptr(v), float(diag_gmin), SOLVERS[solver],
+                                                  ctypes.byref(h)))
         return cls(h)
+
+    @property
+    def solver(self) -> str:
+        """Engine of the current plan: "markowitz" or "amdlu"."""
+        k = L.lib().nsg_topology_solver(self._h)
+        return "amdlu" if k == SOLVERS["amdlu"] else "markowitz"
 
     @classmethod
     def import_structure(cls, n, nnz, int_to_ext_row, int_to_ext_col, elem_row, elem_col,

@@ -217,3 +217,39 @@ def resistor_network(rng: np.random.Generator, nodes: int) -> Netlist:
         if rng.random() < 1 / 3:
             dev.append(("I", GND, k, float(rng.uniform(0, 1e-3))))
     return Netlist(nodes, dev)
+
+
+def power_grid(rng: np.random.Generator, side: int, pad_pitch: int, n_loads: int,
+               r_ohm=0.1, r_sigma=0.05, c_farad=1e-12, i_max=5e-3, t_edge=1e-9,
+               t_rise=5e-11, vdd=1.0) -> Netlist:
+    """An on-chip power grid: a side x side mesh of resistors (lognormal
+    around r_ohm) with a decoupling capacitor c_farad from every node to
+    ground, vdd pads (DC voltage sources to ground) on a lattice of pitch
+    pad_pitch starting at (pitch/2, pitch/2), and n_loads PWL current loads
+    to ground at random nodes, each stepping from 0 to U(0, i_max) over
+    t_rise at a random time in [0, t_edge].  Node (x, y) is y*side + x."""
+    dev = []
+    n = side * side
+    r = r_ohm * np.exp(r_sigma * rng.standard_normal(2 * side * (side - 1)))
+    k = 0
+    for y in range(side):
+        for x in range(side - 1):
+            dev.append(("R", y * side + x, y * side + x + 1, float(r[k])))
+            k += 1
+    for y in range(side - 1):
+        for x in range(side):
+            dev.append(("R", y * side + x, (y + 1) * side + x, float(r[k])))
+            k += 1
+    for i in range(n):
+        dev.append(("C", i, GND, float(c_farad)))
+    h = pad_pitch // 2
+    for y in range(h, side, pad_pitch):
+        for x in range(h, side, pad_pitch):
+            dev.append(("V", y * side + x, GND, float(vdd)))
+    nodes = rng.choice(n, size=n_loads, replace=n_loads > n)
+    amps = rng.uniform(0.0, i_max, n_loads)
+    edges = rng.uniform(0.0, t_edge, n_loads)
+    for node, a, t0 in zip(nodes, amps, edges):
+        dev.append(("IPWL", int(node), GND, 0.0, 0.0, float(t0), 0.0, float(t0 + t_rise),
+                    float(a)))
+    return Netlist(n, dev)

@@ -51,6 +51,8 @@ def port() -> ctypes.CDLL:
         lib.nso_refactor.argtypes = [_I, _I, _I, _V, _V, _V, _V, _D, _I, _V, _V]
         lib.nso_solve.argtypes = [_I, _I, _V, _V, _V, _V, _V, _V]
         lib.nso_solve_transposed.argtypes = [_I, _I, _V, _V, _V, _V, _V, _V]
+        lib.nso_amd_replay.argtypes = [_I, _V, _V, _V, _V, _V, _V, _V, _V, _V, _D, _V, _V, _V]
+        lib.nso_amd_solve.argtypes = [_I] + [_V] * 9
         _port = lib
     return _port
 
@@ -85,6 +87,17 @@ def ref() -> ctypes.CDLL:
         lib.nsref_sim_sens.argtypes = [ctypes.c_char_p, _I, _V, _V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
+        lib.nsref_amd_order.argtypes = [_I, _V, _V, _V]
+        lib.nsref_amdlu_create.restype = _V
+        lib.nsref_amdlu_create.argtypes = [_I, _I, _V, _V]
+        lib.nsref_amdlu_destroy.argtypes = [_V]
+        lib.nsref_amdlu_numeric.argtypes = [_V, _V, _D]
+        lib.nsref_amdlu_refactor.argtypes = [_V, _V, _D]
+        lib.nsref_amdlu_counts.argtypes = [_V, _V, _V]
+        lib.nsref_amdlu_solve.argtypes = [_V, _V]
+        lib.nsref_amdlu_sizes.argtypes = [_V, _V, _V]
+        lib.nsref_amdlu_export.argtypes = [_V] * 9
+        lib.nsref_make_solver_name.argtypes = [_I, _I, ctypes.c_char_p, _I]
         _ref = lib
     return _ref
 
@@ -135,6 +148,33 @@ def port_solve(st: Structure, lu, b, transposed=False):
     return x
 
 
+def port_amd_replay(f: dict, col_ptr, row_idx, a, gmin=0.0):
+    """The C port of AmdLuSolver::refactor_replay_ on the factor structure f
+    (RefAmdLu.export format): (rc, Lx, Ux, fail_step)."""
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_idx, np.int32)
+    a = np.ascontiguousarray(a, np.float64)
+    lx = np.array(f["Lx"], np.float64, copy=True)
+    ux = np.array(f["Ux"], np.float64, copy=True)
+    step = ctypes.c_int(-1)
+    n = len(f["q"])
+    rc = port().nso_amd_replay(n, _p(cp), _p(ri), *(_p(np.ascontiguousarray(f[k], np.int32))
+                                                    for k in ("q", "pinv", "Lp", "Li", "Up", "Ui")),
+                               _p(a), float(gmin), _p(lx), _p(ux), ctypes.addressof(step))
+    return rc, lx, ux, step.value
+
+
+def port_amd_solve(f: dict, lx, ux, b):
+    """The C port of AmdLuSolver::solve."""
+    x = np.array(b, np.float64, copy=True)
+    ints = {k: np.ascontiguousarray(f[k], np.int32) for k in ("q", "pinv", "Lp", "Li", "Up", "Ui")}
+    lx = np.ascontiguousarray(lx, np.float64)
+    ux = np.ascontiguousarray(ux, np.float64)
+    port().nso_amd_solve(len(ints["q"]), _p(ints["q"]), _p(ints["pinv"]), _p(ints["Lp"]),
+                         _p(ints["Li"]), _p(lx), _p(ints["Up"]), _p(ints["Ui"]), _p(ux), _p(x))
+    return x
+
+
 # --- the reference itself ----------------------------------------------------
 
 class RefSolver:
@@ -178,6 +218,69 @@ class RefSolver:
         se = np.zeros(len(self.row_idx), np.int32)
         ref().nsref_solver_export(self.h, _p(r), _p(c), _p(er), _p(ec), _p(ev), _p(se))
         return Structure(n, r, c, er, ec, se), ev
+
+
+def ref_amd_order(n, col_ptr, row_idx):
+    """The reference's amd_ordering (src/core/amd.cpp:14-143)."""
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_idx, np.int32)
+    perm = np.zeros(int(n), np.int32)
+    ref().nsref_amd_order(int(n), _p(cp), _p(ri), _p(perm))
+    return perm
+
+
+def ref_make_solver_name(num_vars, is_linear) -> str:
+    """make_solver(num_vars, is_linear)->name() under the current environment."""
+    buf = ctypes.create_string_buffer(64)
+    ref().nsref_make_solver_name(int(num_vars), int(bool(is_linear)), buf, 64)
+    return buf.value.decode()
+
+
+class RefAmdLu:
+    """The reference's AmdLuSolver on a CSC pattern, through the export shim."""
+
+    def __init__(self, n, col_ptr, row_idx):
+        self.n = int(n)
+        self.col_ptr = np.ascontiguousarray(col_ptr, np.int32)
+        self.row_idx = np.ascontiguousarray(row_idx, np.int32)
+        self.h = ref().nsref_amdlu_create(self.n, len(self.row_idx), _p(self.col_ptr),
+                                          _p(self.row_idx))
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.nsref_amdlu_destroy(self.h)
+            self.h = None
+
+    def numeric(self, values, gmin=0.0) -> int:
+        v = np.ascontiguousarray(values, np.float64)
+        return ref().nsref_amdlu_numeric(self.h, _p(v), gmin)
+
+    def refactorize(self, values, gmin=0.0) -> int:
+        v = np.ascontiguousarray(values, np.float64)
+        return ref().nsref_amdlu_refactor(self.h, _p(v), gmin)
+
+    def counts(self):
+        fast, fb = ctypes.c_int(0), ctypes.c_int(0)
+        ref().nsref_amdlu_counts(self.h, ctypes.addressof(fast), ctypes.addressof(fb))
+        return fast.value, fb.value
+
+    def solve(self, b):
+        x = np.array(b, np.float64, copy=True)
+        if ref().nsref_amdlu_solve(self.h, _p(x)) != 0:
+            raise RuntimeError("reference solve failed")
+        return x
+
+    def export(self) -> dict:
+        nl, nu = ctypes.c_int(0), ctypes.c_int(0)
+        ref().nsref_amdlu_sizes(self.h, ctypes.addressof(nl), ctypes.addressof(nu))
+        n = self.n
+        f = dict(q=np.zeros(n, np.int32), pinv=np.zeros(n, np.int32),
+                 Lp=np.zeros(n + 1, np.int32), Li=np.zeros(nl.value, np.int32),
+                 Lx=np.zeros(nl.value), Up=np.zeros(n + 1, np.int32),
+                 Ui=np.zeros(nu.value, np.int32), Ux=np.zeros(nu.value))
+        ref().nsref_amdlu_export(self.h, *(_p(f[k]) for k in
+                                           ("q", "pinv", "Lp", "Li", "Lx", "Up", "Ui", "Ux")))
+        return f
 
 
 # --- the reference on diode meshes (neospice_b200.workloads.DiodeMesh) -------

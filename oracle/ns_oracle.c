@@ -177,3 +177,65 @@ out:
     free(urow_elem);
     return rc;
 }
+
+/* ---- AMD-LU ------------------------------------------------------------- */
+
+int nso_amd_replay(int n, const int* a_colptr, const int* a_rowidx, const int* q,
+                   const int* pinv, const int* Lp, const int* Li, const int* Up, const int* Ui,
+                   const double* a, double diag_gmin, double* Lx, double* Ux, int* fail_step) {
+    /* Dense accumulator over pivot steps, cleared entry by entry as the
+     * reference's replay does. */
+    double* x = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+    int rc = 0;
+    if (!x) return 8;
+    if (fail_step) *fail_step = -1;
+    for (int k = 0; k < n && rc == 0; ++k) {
+        const int col = q[k];
+        for (int p = a_colptr[col]; p < a_colptr[col + 1]; ++p) x[pinv[a_rowidx[p]]] = a[p];
+        if (diag_gmin != 0.0) x[pinv[col]] += diag_gmin;
+        double colmax = 0.0;
+        for (int up = Up[k]; up < Up[k + 1] - 1; ++up) {
+            const int j = Ui[up];
+            const double u = x[j];
+            x[j] = 0.0;
+            Ux[up] = u;
+            if (fabs(u) > colmax) colmax = fabs(u);
+            for (int p = Lp[j] + 1; p < Lp[j + 1]; ++p) x[Li[p]] -= Lx[p] * u;
+        }
+        const double ukk = x[k];
+        x[k] = 0.0;
+        const double aukk = fabs(ukk);
+        if (aukk > colmax) colmax = aukk;
+        if (ukk == 0.0 || (colmax > 0.0 && aukk < 1e-3 * colmax)) {
+            rc = 103;
+            if (fail_step) *fail_step = k;
+            break;
+        }
+        Ux[Up[k + 1] - 1] = ukk;
+        for (int p = Lp[k] + 1; p < Lp[k + 1]; ++p) {
+            Lx[p] = x[Li[p]] / ukk;
+            x[Li[p]] = 0.0;
+        }
+    }
+    free(x);
+    return rc;
+}
+
+int nso_amd_solve(int n, const int* q, const int* pinv, const int* Lp, const int* Li,
+                  const double* Lx, const int* Up, const int* Ui, const double* Ux, double* x) {
+    double* y = (double*)malloc((size_t)(n > 0 ? n : 1) * sizeof(double));
+    if (!y) return 8;
+    for (int i = 0; i < n; ++i) y[pinv[i]] = x[i];
+    for (int j = 0; j < n; ++j) {
+        const double yj = y[j];
+        for (int p = Lp[j] + 1; p < Lp[j + 1]; ++p) y[Li[p]] -= Lx[p] * yj;
+    }
+    for (int j = n - 1; j >= 0; --j) {
+        y[j] /= Ux[Up[j + 1] - 1];
+        const double yj = y[j];
+        for (int p = Up[j]; p < Up[j + 1] - 1; ++p) y[Ui[p]] -= Ux[p] * yj;
+    }
+    for (int k = 0; k < n; ++k) x[q[k]] = y[k];
+    free(y);
+    return 0;
+}

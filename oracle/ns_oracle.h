@@ -39,6 +39,23 @@ int nso_solve_transposed(int n, int n_elem, const int* elem_row, const int* elem
                          const int* int_to_ext_row, const int* int_to_ext_col,
                          const double* lu, double* x);
 
+/* ---- AMD-LU (src/core/amd_lu_solver.cpp) ------------------------------------
+ * Factor arguments use AmdLuSolver's own storage (oracle/ref_shim.cpp,
+ * nsref_amdlu_export): q[k] the column of step k, pinv[r] the step of row r,
+ * L in CSC over steps with the unit diagonal first (Lp, Li), U in CSC over
+ * steps with the pivot last (Up, Ui); a_colptr/a_rowidx the caller's CSC. */
+
+/* AmdLuSolver::refactor_replay_ (amd_lu_solver.cpp:214-271) on values a:
+ * writes Lx and Ux.  Returns 0 on success, 103 when the pivot-growth test
+ * fails at a step (*fail_step receives it; the reference would re-factor). */
+int nso_amd_replay(int n, const int* a_colptr, const int* a_rowidx, const int* q,
+                   const int* pinv, const int* Lp, const int* Li, const int* Up, const int* Ui,
+                   const double* a, double diag_gmin, double* Lx, double* Ux, int* fail_step);
+
+/* AmdLuSolver::solve (amd_lu_solver.cpp:303-344): x holds b on entry. */
+int nso_amd_solve(int n, const int* q, const int* pinv, const int* Lp, const int* Li,
+                  const double* Lx, const int* Up, const int* Ui, const double* Ux, double* x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,8 +36,11 @@
 #include "solver/error.hpp"
 #include "solver/element.hpp"
 
+#include "core/amd.hpp"
+
 #define private public
 #include "core/neo_solver.hpp"
+#include "core/amd_lu_solver.hpp"
 #include "solver/matrix.hpp"
 #undef private
 
@@ -170,6 +173,111 @@ int nsref_solver_export(void* h, int* int_to_ext_row, int* int_to_ext_col,
         slot_to_elem[k] = (it == where.end()) ? -1 : it->second;
     }
     return e_idx;
+}
+
+// ---- AMD-LU (src/core/amd.cpp, src/core/amd_lu_solver.cpp) ----------------
+
+// amd_ordering on a CSC pattern; perm receives n entries.
+int nsref_amd_order(int n, const int* col_ptr, const int* row_idx, int* perm) {
+    auto q = amd_ordering(n, col_ptr, row_idx);
+    for (size_t k = 0; k < q.size(); ++k) perm[k] = q[k];
+    return static_cast<int>(q.size());
+}
+
+namespace {
+struct RefAmd {
+    int n = 0;
+    int nnz = 0;
+    SparsityPattern pattern;
+    NumericMatrix mat;
+    AmdLuSolver solver;
+    RefAmd(int n_, std::vector<std::pair<int32_t, int32_t>> entries)
+        : n(n_), nnz(static_cast<int>(entries.size())),
+          pattern(n_, std::move(entries)), mat(pattern) {}
+};
+}  // namespace
+
+// AmdLuSolver::symbolic on a CSC pattern (0-based, rows sorted per column).
+void* nsref_amdlu_create(int n, int nnz, const int* col_ptr, const int* row_idx) {
+    std::vector<std::pair<int32_t, int32_t>> entries;
+    entries.reserve(nnz);
+    for (int j = 0; j < n; ++j)
+        for (int p = col_ptr[j]; p < col_ptr[j + 1]; ++p) entries.emplace_back(row_idx[p], j);
+    auto* ra = new RefAmd(n, std::move(entries));
+    ra->solver.symbolic(ra->pattern);
+    return ra;
+}
+
+void nsref_amdlu_destroy(void* h) { delete static_cast<RefAmd*>(h); }
+
+// AmdLuSolver::numeric: 1 when singular, -1 when the reference threw.
+int nsref_amdlu_numeric(void* h, const double* values, double diag_gmin) {
+    auto* ra = static_cast<RefAmd*>(h);
+    std::memcpy(ra->mat.data(), values, sizeof(double) * ra->nnz);
+    try {
+        return ra->solver.numeric(ra->pattern, ra->mat, diag_gmin) ? 1 : 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// AmdLuSolver::refactorize (replay, full factor_ on a failed growth test).
+int nsref_amdlu_refactor(void* h, const double* values, double diag_gmin) {
+    auto* ra = static_cast<RefAmd*>(h);
+    std::memcpy(ra->mat.data(), values, sizeof(double) * ra->nnz);
+    try {
+        return ra->solver.refactorize(ra->mat, diag_gmin) ? 1 : 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// Replay / fallback counters of refactorize().
+void nsref_amdlu_counts(void* h, int* fast, int* fallback) {
+    auto* ra = static_cast<RefAmd*>(h);
+    *fast = ra->solver.refactor_fast_count();
+    *fallback = ra->solver.refactor_fallback_count();
+}
+
+int nsref_amdlu_solve(void* h, double* rhs) {
+    auto* ra = static_cast<RefAmd*>(h);
+    std::vector<double> v(rhs, rhs + ra->n);
+    try {
+        ra->solver.solve(v);
+    } catch (const std::exception&) {
+        return -1;
+    }
+    std::memcpy(rhs, v.data(), sizeof(double) * ra->n);
+    return 0;
+}
+
+// Sizes of L and U (entries incl. the diagonals).
+void nsref_amdlu_sizes(void* h, int* nnz_l, int* nnz_u) {
+    auto* ra = static_cast<RefAmd*>(h);
+    *nnz_l = static_cast<int>(ra->solver.Li_.size());
+    *nnz_u = static_cast<int>(ra->solver.Ui_.size());
+}
+
+// The factor as AmdLuSolver stores it: q (n), pinv (n), Lp/Up (n+1),
+// Li/Lx (nnz_l), Ui/Ux (nnz_u); L rows in pivot-step space.
+void nsref_amdlu_export(void* h, int* q, int* pinv, int* Lp, int* Li, double* Lx, int* Up,
+                        int* Ui, double* Ux) {
+    auto& s = static_cast<RefAmd*>(h)->solver;
+    std::copy(s.q_.begin(), s.q_.end(), q);
+    std::copy(s.pinv_.begin(), s.pinv_.end(), pinv);
+    std::copy(s.Lp_.begin(), s.Lp_.end(), Lp);
+    std::copy(s.Li_.begin(), s.Li_.end(), Li);
+    std::copy(s.Lx_.begin(), s.Lx_.end(), Lx);
+    std::copy(s.Up_.begin(), s.Up_.end(), Up);
+    std::copy(s.Ui_.begin(), s.Ui_.end(), Ui);
+    std::copy(s.Ux_.begin(), s.Ux_.end(), Ux);
+}
+
+// make_solver(num_vars, is_linear)->name() under the current environment.
+int nsref_make_solver_name(int num_vars, int is_linear, char* out, int cap) {
+    auto s = make_solver(num_vars, is_linear != 0);
+    std::snprintf(out, cap, "%s", s->name());
+    return 0;
 }
 
 namespace {

@@ -27,6 +27,19 @@ mesh_dc.npz: seeded diode-clamped meshes (neospice_b200.workloads), per case
 the mesh, the reference's first-iteration matrix and rhs, and its DC
 operating point (solve_dc) with the Newton iteration count.
 
+linear_large.npz: linear resistor networks, RC ladders and trees and RC
+power grids of 256 or more unknowns (the reference's AMD-LU range), per case
+the netlist and the reference's DC operating point or transient output with
+its Newton iteration and rejection counts.
+
+amd_cases.npz: the reference's AmdLuSolver (amd_lu_solver.cpp) on the
+known-answer matrices of its unit tests (restated from their formulas),
+seeded random matrices and resistor meshes with voltage-source branches; per
+case the CSC pattern, values and diag_gmin, the factor after numeric() (AMD
+order q, row pivots pinv, L and U exactly as the solver stores them), the
+factor after refactorize() on second values (with the replay / fallback
+counters), a right-hand side and the reference's solution.
+
 Run from the repository root: ``python tests/golden/make_golden.py``.
 """
 from __future__ import annotations
@@ -219,8 +232,177 @@ def tran_main():
     print(f"wrote {len(cases)} transients to {path}")
 
 
+def linear_netlists():
+    """Linear circuits of 256 or more unknowns, which the reference solves
+    with its AMD-LU engine: (kind, netlist, tstep, tstop); kind 0 = DC
+    operating point, 1 = transient."""
+    from neospice_b200 import workloads as W
+    cases = [
+        (0, W.resistor_network(np.random.default_rng([61, 0]), 300), 0.0, 0.0),
+        (0, W.resistor_network(np.random.default_rng([61, 1]), 700), 0.0, 0.0),
+        (0, W.power_grid(np.random.default_rng([62, 0]), 20, 10, 30), 0.0, 0.0),
+        (1, W.rc_ladder(np.random.default_rng([63, 0]), 300), 1e-11, 2e-9),
+        (1, W.rc_tree(np.random.default_rng([64, 0]), 400), 1e-12, 3e-10),
+        (1, W.power_grid(np.random.default_rng([65, 0]), 16, 8, 12, t_edge=2e-10), 1e-11, 4e-10),
+    ]
+    return cases
+
+
+def linear_main():
+    import json
+    import netlists
+    rec = {}
+    cases = linear_netlists()
+    for k, (kind, nl, tstep, tstop) in enumerate(cases):
+        t, v, info = oracle.ref_sim(netlists.ref_desc(nl), kind, tstep, tstop)
+        p = f"l{k:02d}_"
+        rec.update({p + "kind": np.int32(kind),
+                    p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "tstep": np.float64(tstep), p + "tstop": np.float64(tstop),
+                    p + "times": t, p + "values": v,
+                    p + "num_vars": np.int32(info["num_vars"]),
+                    p + "iterations": np.int32(info["iterations"]),
+                    p + "rejected": np.int32(info["rejected"])})
+        print(k, kind, info["num_vars"], info["points"], info["iterations"], f"{info['seconds']:.2f}s")
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("linear_large.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} linear circuits to {path}")
+
+
+def _csc(n, entries):
+    """CSC of {(row, col): value}, rows ascending per column."""
+    keys = sorted(entries, key=lambda rc: (rc[1], rc[0]))
+    cp = np.zeros(n + 1, np.int32)
+    for (_, c) in keys:
+        cp[c + 1] += 1
+    cp = np.cumsum(cp).astype(np.int32)
+    ri = np.array([r for (r, _) in keys], np.int32)
+    v = np.array([entries[k] for k in keys], np.float64)
+    return n, cp, ri, v
+
+
+def amd_known_answer_cases():
+    """The matrices of the reference's AmdLuSolver unit tests
+    (tests/unit/test_amd_lu.cpp), rebuilt from their formulas: (name, n,
+    entries, second entries or None, gmin, x_true or None, tol)."""
+    out = []
+    out.append(("dense1x1", 1, {(0, 0): 3.0}, None, 0.0, [7.0], 1e-12))
+    out.append(("dense2x2", 2, {(0, 0): 2.0, (1, 0): 1.0, (0, 1): 1.0, (1, 1): 3.0}, None, 0.0,
+                [1.6, 1.8], 1e-10))
+    out.append(("dense8_diag_dominant", 8,
+                {(i, j): (20.0 if i == j else 1.0) for i in range(8) for j in range(8)}, None,
+                0.0, [i + 1.0 for i in range(8)], 1e-9))
+
+    def tri(n, d, o):
+        e = {}
+        for i in range(n):
+            e[(i, i)] = d
+            if i > 0:
+                e[(i, i - 1)] = o
+            if i < n - 1:
+                e[(i, i + 1)] = o
+        return e
+    out.append(("tridiagonal60", 60, tri(60, 4.0, -1.0), None, 0.0,
+                [(i % 5) + 1.0 for i in range(60)], 1e-9))
+    arrow = {(i, i): (100.0 if i == 0 else 5.0) for i in range(16)}
+    for i in range(1, 16):
+        arrow[(0, i)] = 1.0
+        arrow[(i, 0)] = 1.0
+    out.append(("arrowhead16", 16, arrow, None, 0.0, [(i % 3) + 0.5 for i in range(16)], 1e-9))
+    out.append(("indefinite2x2", 2, {(0, 1): 1.0, (1, 0): 1.0, (1, 1): 1.0}, None, 0.0,
+                [1.0, 1.0], 1e-12))
+    z = {(0, 2): 1.0, (1, 2): 1.0, (1, 3): 1.0, (2, 0): 1.0, (2, 1): 1.0, (2, 2): 5.0,
+         (3, 1): 1.0, (3, 3): 3.0}
+    out.append(("zero_diag_block4", 4, z, None, 0.0, [2.0, -1.0, 0.5, 1.5], 1e-9))
+    out.append(("diag_gmin2x2", 2, {(0, 0): 0.0, (1, 1): 0.0}, None, 1e-3, None, 1e-9))
+    out.append(("refactorize40", 40, tri(40, 4.0, -1.0), tri(40, 8.0, -2.0), 0.0,
+                [1.0] * 40, 1e-10))
+
+    def fast(s):
+        e = {}
+        for i in range(50):
+            e[(i, i)] = 10.0 * s + 0.1 * i
+            if i > 0:
+                e[(i, i - 1)] = -1.0 * s
+            if i < 49:
+                e[(i, i + 1)] = -1.5 * s
+            if i + 2 < 50:
+                e[(i, i + 2)] = -0.3 * s
+        return e
+    out.append(("replay50", 50, fast(1.0), fast(1.7), 0.0,
+                [np.sin(0.2 * i) + 1.3 for i in range(50)], 1e-9))
+    a0 = [[10, 1, 2], [1, 12, 3], [2, 1, 15]]
+    a1 = [[1e-12, 1, 2], [1, 12, 3], [2, 1, 15]]
+    out.append(("growth_fallback3", 3, {(i, j): float(a0[i][j]) for i in range(3) for j in range(3)},
+                {(i, j): float(a1[i][j]) for i in range(3) for j in range(3)}, 0.0,
+                [2.0, -1.0, 0.5], 1e-7))
+    out.append(("replay_gmin30", 30, tri(30, 3.0, -1.0), tri(30, 4.2, -1.4), 1e-2, None, 1e-12))
+    out.append(("structurally_singular2", 2, {(0, 0): 1.0, (1, 0): 1.0}, None, 0.0, None, 0.0))
+    return out
+
+
+def amd_main():
+    oracle.build()
+    rng = np.random.default_rng(20261204)
+    cases = []
+    for (name, n, e, e2, gmin, xt, tol) in amd_known_answer_cases():
+        n, cp, ri, v = _csc(n, e)
+        v2 = _csc(n, e2)[3] if e2 is not None else v * np.exp(0.05 * rng.standard_normal(len(v)))
+        cases.append((name, n, cp, ri, v, v2, gmin, xt, tol))
+    for k in range(24):
+        n = int(rng.integers(3, 90))
+        n, cp, ri, v = random_matrix(rng, n, float(rng.uniform(0.03, 0.3)),
+                                     diag_dominant=(k % 2 == 0),
+                                     zero_diag_frac=float(rng.uniform(0.0, 0.3)),
+                                     integer=(k % 6 == 0))
+        v2 = v * np.exp((0.5 if k % 4 == 3 else 0.05) * rng.standard_normal(len(v)))
+        cases.append((f"random{k:02d}", n, cp, ri, v, v2, 0.0, None, 0.0))
+    for side, nv in ((8, 1), (16, 2), (20, 3), (24, 1)):
+        n, cp, ri, v = mna_mesh(rng, side, nv)
+        v2 = v * np.exp(0.02 * rng.standard_normal(len(v)))
+        cases.append((f"mesh{side}", n, cp, ri, v, v2, 0.0, None, 0.0))
+    rec = {}
+    for k, (name, n, cp, ri, v, v2, gmin, xt, tol) in enumerate(cases):
+        r = oracle.RefAmdLu(n, cp, ri)
+        rc = r.numeric(v, gmin)
+        p = f"a{k:02d}_"
+        rec.update({p + "name": np.array(name), p + "n": np.int32(n), p + "col_ptr": cp,
+                    p + "row_idx": ri, p + "vals": v, p + "vals2": v2,
+                    p + "gmin": np.float64(gmin), p + "numeric_rc": np.int32(rc),
+                    p + "tol": np.float64(tol)})
+        if xt is not None:
+            rec[p + "x_true"] = np.asarray(xt, np.float64)
+        if rc != 0:
+            continue
+        f1 = r.export()
+        rec.update({p + "f1_" + key: val for key, val in f1.items()})
+        rc2 = r.refactorize(v2, gmin)
+        fast, fallback = r.counts()
+        rec.update({p + "refactor_rc": np.int32(rc2), p + "fast": np.int32(fast),
+                    p + "fallback": np.int32(fallback)})
+        if rc2 != 0:
+            continue
+        rec.update({p + "f2_" + key: val for key, val in r.export().items()})
+        b = rng.standard_normal(n)
+        if xt is not None:  # the reference's check_parity: b = A(vals2) * x_true
+            a = np.zeros((n, n))
+            for j in range(n):
+                a[ri[cp[j]:cp[j + 1]], j] = v2[cp[j]:cp[j + 1]]
+            b = a @ np.asarray(xt)
+        rec.update({p + "b": b, p + "x": r.solve(b)})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("amd_cases.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} AMD-LU cases to {path}")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos", "sens"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos", "sens", "amd", "linear"]
+    if "amd" in which:
+        amd_main()
+    if "linear" in which:
+        linear_main()
     if "solver" in which:
         main()
     if "mesh" in which:

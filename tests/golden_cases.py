@@ -100,3 +100,43 @@ def param_starts(netlist):
         out.append((k, at))
         at += sizes[k] if k in sizes else len(d) - 3
     return out
+
+
+AMD_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "amd_cases.npz"
+_FACTOR_KEYS = ("q", "pinv", "Lp", "Li", "Lx", "Up", "Ui", "Ux")
+
+
+def load_amd():
+    """AMD-LU cases (made by the reference's AmdLuSolver): per case the
+    pattern, values, and the factors f1 (after numeric) / f2 (after
+    refactorize) as dicts in the reference's storage."""
+    z = np.load(AMD_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"a{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        d["name"] = str(d["name"])
+        for f in ("f1", "f2"):
+            if f + "_q" in d:
+                d[f] = {key: d.pop(f + "_" + key) for key in _FACTOR_KEYS}
+        out.append(d)
+    return out
+
+
+LINEAR_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "linear_large.npz"
+
+
+def load_linear():
+    """Linear circuits of 256+ unknowns (the reference's AMD-LU range)."""
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(LINEAR_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"l{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        out.append(d)
+    return out
