@@ -44,7 +44,8 @@ def run(topos, vals, gmins, bs=None, check=False, schedule=0):
     st, _ = batch.refactor(d_a, gmins[0], check_pivots=check)
     status[:] = st.cpu().numpy()
     lu = batch.lu_values()
-    lus = [lu[batch.lu_offsets[i]:batch.lu_offsets[i + 1]] for i in range(len(topos))]
+    sizes = [t.info()["nnz_lu"] for t in topos]
+    lus = [lu[batch.lu_offsets[i]:batch.lu_offsets[i] + sizes[i]] for i in range(len(topos))]
     xs = xts = None
     if bs is not None:
         x = np.zeros(int(batch.vector_offsets[-1]))
@@ -55,8 +56,10 @@ def run(topos, vals, gmins, bs=None, check=False, schedule=0):
         batch.solve(d_x)
         batch.solve_transposed(d_xt)
         hx, hxt = d_x.cpu().numpy(), d_xt.cpu().numpy()
-        xs = [hx[batch.vector_offsets[i]:batch.vector_offsets[i + 1]] for i in range(len(topos))]
-        xts = [hxt[batch.vector_offsets[i]:batch.vector_offsets[i + 1]] for i in range(len(topos))]
+        ns = [t.info()["n"] for t in topos]
+        xs = [hx[batch.vector_offsets[i]:batch.vector_offsets[i] + ns[i]] for i in range(len(topos))]
+        xts = [hxt[batch.vector_offsets[i]:batch.vector_offsets[i] + ns[i]]
+               for i in range(len(topos))]
     return status, lus, xs, xts
 
 
