@@ -50,6 +50,10 @@ def _args():
                     help="instances in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--no-inverter", action="store_true",
                     help="skip the plain-vs-batched transient measurement")
+    ap.add_argument("--no-power-grid", action="store_true",
+                    help="skip the single large power-grid refactor/solve section")
+    ap.add_argument("--grid-side", type=int, default=300,
+                    help="side of the power-grid mesh of that section")
     ap.add_argument("--inverter-batch", type=int, default=296,
                     help="instances of the batched inverter-chain transient")
     return ap.parse_args()
@@ -306,6 +310,11 @@ def run_ours(a, rank, world, local_rank):
                 line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch)
             except Exception as exc:
                 line["plain_vs_batched"] = {"error": str(exc)}
+        if not a.no_power_grid and world == 1:
+            try:
+                line["power_grid"] = power_grid_refactor(a.grid_side, a.steps, a.warmup)
+            except Exception as exc:
+                line["power_grid"] = {"error": str(exc)}
         print(json.dumps(line), flush=True)
 
     del batch
@@ -377,6 +386,96 @@ def inverter_plain_vs_batched(batch_count):
                              "iterations_equal": info["iterations"] == rp["newton_iters"]}
             out["cpu_reference_1core"] = {"value": round(1.0 / t_ref, 4), "unit": "circuit-solves/s"}
     except Exception as exc:  # the parity check is informative only
+        out["parity"] = {"error": str(exc)}
+    return out
+
+
+# --- one large topology: power-grid refactor and solve ------------------------------
+
+def power_grid_refactor(side, reps, warmup):
+    """The large-single-topology case at a reduced size: a side x side RC
+    power grid (0.1 Ohm lognormal sigma 0.05 mesh, 1 pF per node, VDD pads
+    on a pitch-50 lattice, side^2/100 PWL loads), linear, so the AMD-LU
+    engine (as the reference's make_solver picks it).  Times the grid-wide
+    fixed-pivot replay refactor and the forward/backward sweeps of the
+    transient matrix (conductances + C/h with h = 10 ps) with CUDA events,
+    against the reference's AmdLuSolver refactorize + solve on one core."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.solver import Batch, Topology
+
+    nl = W.power_grid(np.random.default_rng(2026), side, 50, max(1, side * side // 100))
+    c = nl.build()
+    cp, ri = c.pattern()
+    g, _ = c.initial_matrix(0.0)
+    n = len(cp) - 1
+    # transient companion matrix: each 1 pF cap adds C/h to its node's diagonal
+    tran = g.copy()
+    caps = {d[1] for d in nl.devices if d[0] == "C"}
+    for j in caps:
+        for p in range(cp[j], cp[j + 1]):
+            if ri[p] == j:
+                tran[p] += 1e-12 / 1e-11
+    t0 = time.perf_counter()
+    topo = Topology.order(n, cp, ri, tran, solver="amdlu")
+    t_symbolic = time.perf_counter() - t0
+    info = topo.info()
+    batch = Batch([topo])
+    batch.set_schedule(2)
+    d_a = torch.from_numpy(tran).cuda()
+    rhs = np.random.default_rng(5).standard_normal(n)
+    d_b = torch.from_numpy(rhs).cuda()
+    d_x = torch.empty_like(d_b)
+    for _ in range(max(warmup, 1)):
+        st, _ = batch.refactor(d_a)
+        d_x.copy_(d_b)
+        batch.solve(d_x)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    for _ in range(reps):
+        batch.refactor(d_a, d_status=st)
+    ev[1].record()
+    for _ in range(reps):
+        d_x.copy_(d_b)
+        batch.solve(d_x)
+    ev[2].record()
+    torch.cuda.synchronize()
+    t_ref = ev[0].elapsed_time(ev[1]) / 1e3 / reps
+    t_sol = ev[1].elapsed_time(ev[2]) / 1e3 / reps
+    x = d_x.cpu().numpy()
+    nnz, nlu, upd = len(ri), info["nnz_lu"], info["updates"]
+    b_ref = 8 * nnz + 8 * nlu + 4 * (upd + nlu + n) + 8 * n
+    b_sol = 12 * nlu + 16 * n
+    peak, peak_kind = measured_peaks()
+    out = {
+        "workload": f"power grid {side}x{side} (n={n}), {len([d for d in nl.devices if d[0] == 'V'])} "
+                    f"pads, AMD-LU replay refactor + solve of the transient matrix, grid-wide schedule",
+        "status": int(st.cpu()[0]), "nnz": nnz, "nnz_lu": nlu, "updates": upd,
+        "host_symbolic_s": round(t_symbolic, 3),
+        "refactor_ms": round(1e3 * t_ref, 4), "solve_ms": round(1e3 * t_sol, 4),
+        "refactor_gbs": round(b_ref / t_ref / 1e9, 2), "solve_gbs": round(b_sol / t_sol / 1e9, 2),
+        "refactor_gflops": round((2 * upd + n) / t_ref / 1e9, 2),
+        "refactor_frac_hbm": round(b_ref / t_ref / 1e9 / peak, 5),
+        "solves_per_s": round(1.0 / (t_ref + t_sol), 2), "peak_gbs": peak,
+        "peak_source": peak_kind,
+    }
+    try:
+        import oracle
+        if oracle.have_ref():
+            ref = oracle.RefAmdLu(n, cp, ri)
+            ref.numeric(tran)
+            t0 = time.perf_counter()
+            ref.refactorize(tran)
+            xr = ref.solve(rhs)
+            t_cpu = time.perf_counter() - t0
+            out["cpu_reference_1core"] = {"refactor_plus_solve_ms": round(1e3 * t_cpu, 3),
+                                          "solves_per_s": round(1.0 / t_cpu, 3)}
+            out["parity"] = {"bitwise_equal": bool(np.array_equal(x, xr)),
+                             "max_rel_err": float(np.max(np.abs(x - xr) /
+                                                         np.maximum(np.abs(xr), 1e-30)))}
+    except Exception as exc:
         out["parity"] = {"error": str(exc)}
     return out
 

@@ -144,7 +144,9 @@ int nsg_batch_refactor(nsg_batch* batch, const double* d_values, double diag_gmi
 
 /* Refactor schedule: 0 (default) = dataflow (warps claim columns in pivot
  * order and wait on per-column completion flags, column staged in shared
- * memory; used when the batch's columns fit), 1 = level-synchronous.  Both
+ * memory; used when the batch's columns fit), 1 = level-synchronous, both
+ * one CTA per instance; 2 = grid-wide (instances one after another, each
+ * refactored and swept by every SM, for a few large topologies).  All
  * produce bit-identical values. */
 int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
 

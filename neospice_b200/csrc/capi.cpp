@@ -24,6 +24,17 @@ cudaError_t launch_solve(const PlanDesc* plans, const int32_t* pool, const InstD
                          int count, const double* LU, double* X, double* W, bool transposed,
                          const double* lrows, const double* urows, int max_n,
                          cudaStream_t stream);
+size_t grid_scratch_bytes(int max_n);
+cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
+                                 const InstDesc* insts, int count, const int32_t* n_of,
+                                 const double* A, double* LU, double diag_gmin, int check_pivots,
+                                 double rel_threshold, int32_t* status, int32_t* fail_step,
+                                 double* lrows, double* urows, void* scratch,
+                                 cudaStream_t stream);
+cudaError_t launch_grid_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
+                              int count, const int32_t* n_of, const double* LU,
+                              const double* lrows, const double* urows, double* X, double* W,
+                              void* scratch, cudaStream_t stream);
 }  // namespace nsg
 
 namespace nsg_internal {
@@ -427,6 +438,8 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
         std::stable_sort(insts.begin(), insts.end(), [&](const nsg::InstDesc& x, const nsg::InstDesc& y) {
             return topos[x.index]->plan.updates > topos[y.index]->plan.updates;
         });
+        // Unknowns per launch slot (the grid-wide schedule walks insts[]).
+        for (const auto& d : insts) b->n_of.push_back(topos[d.index]->plan.n);
         cudaError_t e;
         if ((e = upload(&b->d_pool, pool.data(), pool.size())) != cudaSuccess ||
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
@@ -460,6 +473,18 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
     // check_pivots: a numeric() (re-validate / re-choose the pivots), else a
     // refactorize() (AMD-LU topologies run the replay's growth test).
     const int mode = check_pivots ? nsg::kCheckNumeric : nsg::kCheckRefactor;
+    if (b->schedule == 2) {
+        if (!b->d_grid) {
+            cudaError_t e = cudaMalloc(&b->d_grid, nsg::grid_scratch_bytes(b->max_n));
+            if (e != cudaSuccess) return cuda_fail("nsg_batch_refactor", e);
+        }
+        cudaError_t e = nsg::launch_grid_refactor(
+            b->d_plans, b->d_pool, b->d_insts, b->count, b->n_of.data(), d_values, b->d_lu,
+            diag_gmin, mode, 1e-3, d_status, d_fail_step, b->d_lrows, b->d_urows, b->d_grid,
+            static_cast<cudaStream_t>(stream));
+        if (e == cudaSuccess) b->rows_valid = true;
+        return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
+    }
     cudaError_t e = nsg::launch_refactor(b->d_plans, b->d_pool, b->d_insts, b->count, d_values,
                                          b->d_lu, diag_gmin, mode, 1e-3, d_status,
                                          d_fail_step, b->max_col, b->max_n, b->allow_flow,
@@ -470,6 +495,13 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
 
 int nsg_batch_solve(nsg_batch* b, double* d_x, void* stream) {
     if (!b || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve: null argument");
+    if (b->schedule == 2 && b->rows_valid && b->d_grid) {
+        cudaError_t e = nsg::launch_grid_solve(b->d_plans, b->d_pool, b->d_insts, b->count,
+                                               b->n_of.data(), b->d_lu, b->d_lrows, b->d_urows,
+                                               d_x, b->d_work, b->d_grid,
+                                               static_cast<cudaStream_t>(stream));
+        return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve", e);
+    }
     cudaError_t e = nsg::launch_solve(b->d_plans, b->d_pool, b->d_insts, b->count, b->d_lu, d_x,
                                       b->d_work, false, b->rows_valid ? b->d_lrows : nullptr,
                                       b->d_urows, b->max_n, static_cast<cudaStream_t>(stream));
@@ -487,9 +519,11 @@ int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
 const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
 
 int nsg_batch_set_schedule(nsg_batch* b, int schedule) {
-    if (!b || schedule < 0 || schedule > 1)
+    if (!b || schedule < 0 || schedule > 2)
         return fail(NSG_ERR_INVALID, "nsg_batch_set_schedule: bad arguments");
     b->allow_flow = (schedule == 0);
+    b->schedule = schedule;
+    b->rows_valid = false;
     return NSG_OK;
 }
 

@@ -52,7 +52,11 @@ struct nsg_batch {
     int max_col = 0;
     int max_n = 0;
     bool allow_flow = true;
+    int schedule = 0;             // nsg_batch_set_schedule
+    std::vector<int32_t> n_of;    // unknowns of the instance in each slot of d_insts
+    void* d_grid = nullptr;       // flags and state of the grid-wide schedule
     ~nsg_batch() {
+        cudaFree(d_grid);
         cudaFree(d_pool);
         cudaFree(d_plans);
         cudaFree(d_insts);

@@ -151,6 +151,167 @@ struct RefactorResult {
     int32_t step;  // failing pivot step or -1
 };
 
+// Outcome of one column of the dataflow refactor.
+struct ColumnResult {
+    int32_t code;      // kStatusOk / kStatusSingular / kStatusReorder verdict
+    bool growth_fail;  // AMD-LU kCheckRefactor: the replay's growth test failed
+    bool timed_out;    // a bounded dependency wait gave up
+};
+
+// Loads of another column's factor values: through L1 when one SM owns the
+// whole instance, L2-only (ld.global.cg) when columns are finished by other
+// SMs and an L1 line could hold values from before their completion.
+template <bool kCrossSm>
+__device__ __forceinline__ double lu_peer(const double* p) {
+    if constexpr (kCrossSm) return __ldcg(p);
+    return *p;
+}
+
+// Column j of the left-looking dataflow refactor, by one warp.  buf holds the
+// column while it is eliminated (shared memory, or the column's own place in
+// lu); probe(r) reads column r's completion flag (acquire).  Loads A
+// (through lu_src, diag_gmin added), applies every U entry in stored order
+// after column r is done, judges the pivot (check_pivots, kCheck*), and
+// writes the column (and its row-major copies) to lu.  Ends with
+// __syncwarp(); the caller publishes completion.
+template <bool kCrossSm, class Probe>
+__device__ __forceinline__ ColumnResult refactor_column(
+    const PlanDesc& pd, const int32_t* __restrict__ pool, const double* __restrict__ a,
+    double* lu, double diag_gmin, int check_pivots, double rel_threshold, int32_t j, double* buf,
+    double* __restrict__ lrows, double* __restrict__ urows, Probe probe) {
+    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const int32_t* lu_src = pool + pd.off[PA_lu_src];
+    const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const bool amd = pd.kind == kPlanAmdLu;
+    const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
+    const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
+    const int lane = threadIdx.x & 31;
+
+    const int32_t c0 = col_ptr[j];
+    const int32_t len = col_ptr[j + 1] - c0;
+    const int32_t dj = diag_pos[j] - c0;
+    const int32_t gp = amd ? gmin_pos[j] : dj;
+    for (int32_t t = lane; t < len; t += 32) {
+        const int32_t s = lu_src[c0 + t];
+        double v = (s >= 0) ? a[s] : 0.0;
+        if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+        buf[t] = v;
+    }
+    __syncwarp();
+    double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
+    // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
+    // entries at a time in registers (lane k holds entry base+k) and
+    // broadcast by shuffle.  One-step lookahead: while the update of entry q
+    // runs, the pivot reciprocal, the first 32 entries of L(:, r) and their
+    // destinations for entry q+1 are loaded (when column r is done), so a
+    // step waits on at most one global round trip.
+    const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]) + c0;
+    bool timed_out = false;
+    int4 chunk = make_int4(0, 0, 0, 0), next_chunk = make_int4(0, 0, 0, 0);
+    if (lane < dj) chunk = umeta[lane];
+    if (32 + lane < dj) next_chunk = umeta[32 + lane];
+    double rd_c = 0.0, lv_c = 0.0;
+    int32_t l0_c = 0, cnt_c = 0, us_c = 0, ld_c = 0;
+    bool have_c = false;
+    // Load the operands of entry q (metadata m) if column m.x is done, or
+    // after waiting for it.
+    auto fetch = [&](const int4 m, bool wait, double& rd, double& lv, int32_t& l0, int32_t& cnt,
+                     int32_t& us, int32_t& ld) -> bool {
+        int ready = 0;
+        if (lane == 0) {
+            int spins = 0;
+            while ((ready = probe(m.x)) == 0 && wait) {
+                if (++spins > kSpinLimit) {
+                    timed_out = true;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        ready = __shfl_sync(0xffffffffu, ready, 0);
+        timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
+        __syncwarp();
+        if (!ready) return false;
+        rd = lu_peer<kCrossSm>(lu + m.y);
+        l0 = m.y + 1;
+        cnt = m.z;
+        us = m.w;
+        lv = (lane < cnt) ? lu_peer<kCrossSm>(lu + l0 + lane) : 0.0;
+        ld = (lane < cnt) ? upd_dst[us + lane] : 0;
+        return true;
+    };
+    auto meta = [&](int32_t q) -> int4 {
+        const int k = q & 31;
+        const int4 src = ((q >> 5) == 0) ? chunk : next_chunk;
+        int4 m;
+        m.x = __shfl_sync(0xffffffffu, src.x, k);
+        m.y = __shfl_sync(0xffffffffu, src.y, k);
+        m.z = __shfl_sync(0xffffffffu, src.z, k);
+        m.w = __shfl_sync(0xffffffffu, src.w, k);
+        return m;
+    };
+    int32_t base = 0;  // entry index held in chunk's lane 0
+    for (int32_t q = 0; q < dj; ++q) {
+        if (q - base == 32) {  // advance the register window by 32 entries
+            base += 32;
+            chunk = next_chunk;
+            next_chunk = (base + 32 + lane < dj) ? umeta[base + 32 + lane] : make_int4(0, 0, 0, 0);
+        }
+        if (!have_c) {
+            fetch(meta(q - base), true, rd_c, lv_c, l0_c, cnt_c, us_c, ld_c);
+            if (timed_out) break;
+        }
+        double rd_n = 0.0, lv_n = 0.0;
+        int32_t l0_n = 0, cnt_n = 0, us_n = 0, ld_n = 0;
+        const bool have_n = (q + 1 < dj) &&
+                            fetch(meta(q + 1 - base), false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
+        const double u = amd ? buf[q] : lu_mul(buf[q], rd_c);
+        colmax = fmax(colmax, fabs(u));
+        __syncwarp();
+        if (lane == 0) buf[q] = u;
+        if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
+        for (int32_t t = lane + 32; t < cnt_c; t += 32) {
+            const int32_t d = upd_dst[us_c + t];
+            buf[d] = lu_sub(buf[d], lu_mul(u, lu_peer<kCrossSm>(lu + l0_c + t)));
+        }
+        __syncwarp();
+        have_c = have_n;
+        rd_c = rd_n;
+        lv_c = lv_n;
+        l0_c = l0_n;
+        cnt_c = cnt_n;
+        us_c = us_n;
+        ld_c = ld_n;
+    }
+    const double piv = buf[dj];
+    ColumnResult res{kStatusOk, false, timed_out};
+    if (amd) {
+        const AmdColumn v = amd_column_status(buf, dj, len, colmax, check_pivots, piv_rank[j],
+                                              gmin_pos[j], lane);
+        res.code = v.code;
+        res.growth_fail = v.growth_fail;
+    } else if (check_pivots == kCheckNumeric) {
+        double largest = 0.0;
+        for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(buf[t]));
+        largest = warp_max(largest);
+        res.code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
+    } else {
+        res.code = (piv == 0.0) ? kStatusSingular : kStatusOk;
+    }
+    const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
+    for (int32_t t = lane; t < len; t += 32) {
+        const double v = lu_store_value(amd, buf[t], t, dj, piv);
+        lu[c0 + t] = v;
+        if (lrows) {
+            if (t < dj) urows[rowcopy[c0 + t]] = v;
+            else if (t > dj) lrows[rowcopy[c0 + t]] = v;
+        }
+    }
+    __syncwarp();
+    return res;
+}
+
 // Dataflow refactor of one instance by the whole CTA (blockDim.x ==
 // kFlowThreads).  Warps claim columns in pivot order from a shared counter;
 // before using column r a warp waits for done[r], so independent columns
@@ -173,16 +334,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
                                                    double* __restrict__ lrows = nullptr,
                                                    double* __restrict__ urows = nullptr) {
     const int32_t n = pd.n;
-    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
-    const int32_t* row_idx = pool + pd.off[PA_row_idx];
-    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
-    const int32_t* lu_src = pool + pd.off[PA_lu_src];
-    const int32_t* upd_start = pool + pd.off[PA_upd_start];
-    const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
-
     const bool amd = pd.kind == kPlanAmdLu;
-    const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
-    const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     double* buf = smem + warp * colbuf;
@@ -205,132 +357,13 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
         if (lane == 0) j = atomicAdd(&s_next, 1);
         j = __shfl_sync(0xffffffffu, j, 0);
         if (j >= n) break;
-        const int32_t c0 = col_ptr[j];
-        const int32_t len = col_ptr[j + 1] - c0;
-        const int32_t dj = diag_pos[j] - c0;
-        const int32_t gp = amd ? gmin_pos[j] : dj;
-        for (int32_t t = lane; t < len; t += 32) {
-            const int32_t s = lu_src[c0 + t];
-            double v = (s >= 0) ? a[s] : 0.0;
-            if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
-            buf[t] = v;
-        }
-        __syncwarp();
-        double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
-        // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
-        // entries at a time in registers (lane k holds entry base+k) and
-        // broadcast by shuffle.  One-step lookahead: while the update of
-        // entry q runs, the pivot reciprocal, the first 32 entries of L(:, r)
-        // and their destinations for entry q+1 are loaded (when column r is
-        // done), so a step waits on at most one global round trip.
-        const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]) + c0;
-        bool timed_out = false;
-        int4 chunk = make_int4(0, 0, 0, 0), next_chunk = make_int4(0, 0, 0, 0);
-        if (lane < dj) chunk = umeta[lane];
-        if (32 + lane < dj) next_chunk = umeta[32 + lane];
-        double rd_c = 0.0, lv_c = 0.0;
-        int32_t l0_c = 0, cnt_c = 0, us_c = 0, ld_c = 0;
-        bool have_c = false;
-        // Load the operands of entry q (metadata m) if column m.x is done,
-        // or after waiting for it.
-        auto fetch = [&](const int4 m, bool wait, double& rd, double& lv, int32_t& l0,
-                         int32_t& cnt, int32_t& us, int32_t& ld) -> bool {
-            int ready = 0;
-            if (lane == 0) {
-                int spins = 0;
-                while ((ready = flag_acquire(done + m.x)) == 0 && wait) {
-                    if (++spins > kSpinLimit) {
-                        timed_out = true;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            ready = __shfl_sync(0xffffffffu, ready, 0);
-            timed_out = __shfl_sync(0xffffffffu, timed_out, 0);
-            __syncwarp();
-            if (!ready) return false;
-            rd = lu[m.y];
-            l0 = m.y + 1;
-            cnt = m.z;
-            us = m.w;
-            lv = (lane < cnt) ? lu[l0 + lane] : 0.0;
-            ld = (lane < cnt) ? upd_dst[us + lane] : 0;
-            return true;
-        };
-        auto meta = [&](int32_t q) -> int4 {
-            const int k = q & 31;
-            const int4 src = ((q >> 5) == 0) ? chunk : next_chunk;
-            int4 m;
-            m.x = __shfl_sync(0xffffffffu, src.x, k);
-            m.y = __shfl_sync(0xffffffffu, src.y, k);
-            m.z = __shfl_sync(0xffffffffu, src.z, k);
-            m.w = __shfl_sync(0xffffffffu, src.w, k);
-            return m;
-        };
-        int32_t base = 0;  // entry index held in chunk's lane 0
-        for (int32_t q = 0; q < dj; ++q) {
-            if (q - base == 32) {  // advance the register window by 32 entries
-                base += 32;
-                chunk = next_chunk;
-                next_chunk = (base + 32 + lane < dj) ? umeta[base + 32 + lane] : make_int4(0, 0, 0, 0);
-            }
-            if (!have_c) {
-                fetch(meta(q - base), true, rd_c, lv_c, l0_c, cnt_c, us_c, ld_c);
-                if (timed_out) break;
-            }
-            double rd_n = 0.0, lv_n = 0.0;
-            int32_t l0_n = 0, cnt_n = 0, us_n = 0, ld_n = 0;
-            const bool have_n = (q + 1 < dj) &&
-                                fetch(meta(q + 1 - base), false, rd_n, lv_n, l0_n, cnt_n, us_n, ld_n);
-            const double u = amd ? buf[q] : lu_mul(buf[q], rd_c);
-            colmax = fmax(colmax, fabs(u));
-            __syncwarp();
-            if (lane == 0) buf[q] = u;
-            if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
-            for (int32_t t = lane + 32; t < cnt_c; t += 32) {
-                const int32_t d = upd_dst[us_c + t];
-                buf[d] = lu_sub(buf[d], lu_mul(u, lu[l0_c + t]));
-            }
-            __syncwarp();
-            have_c = have_n;
-            rd_c = rd_n;
-            lv_c = lv_n;
-            l0_c = l0_n;
-            cnt_c = cnt_n;
-            us_c = us_n;
-            ld_c = ld_n;
-        }
-        const double piv = buf[dj];
-        int32_t code;
-        bool growth_fail = false;
-        if (amd) {
-            const AmdColumn v = amd_column_status(buf, dj, len, colmax, check_pivots, piv_rank[j],
-                                                  gmin_pos[j], lane);
-            code = v.code;
-            growth_fail = v.growth_fail;
-        } else if (check_pivots == kCheckNumeric) {
-            double largest = 0.0;
-            for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(buf[t]));
-            largest = warp_max(largest);
-            code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
-        } else {
-            code = (piv == 0.0) ? kStatusSingular : kStatusOk;
-        }
-        const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
-        for (int32_t t = lane; t < len; t += 32) {
-            const double v = lu_store_value(amd, buf[t], t, dj, piv);
-            lu[c0 + t] = v;
-            if (lrows) {
-                if (t < dj) urows[rowcopy[c0 + t]] = v;
-                else if (t > dj) lrows[rowcopy[c0 + t]] = v;
-            }
-        }
-        __syncwarp();
+        const ColumnResult c = refactor_column<false>(
+            pd, pool, a, lu, diag_gmin, check_pivots, rel_threshold, j, buf, lrows, urows,
+            [&](int32_t r) { return flag_acquire(done + r); });
         if (lane == 0) {
-            if (timed_out) s_timeout = 1;
-            else if (code != kStatusOk) atomicMin(&s_fail, fail_key(j, code));
-            if (growth_fail) s_growth = 1;
+            if (c.timed_out) s_timeout = 1;
+            else if (c.code != kStatusOk) atomicMin(&s_fail, fail_key(j, c.code));
+            if (c.growth_fail) s_growth = 1;
             flag_release(done + j, 1);
         }
         __syncwarp();

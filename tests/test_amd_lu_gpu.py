@@ -70,7 +70,7 @@ def by_gmin(cases):
     return groups.items()
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 def test_numeric_values_match_reference(schedule):
     """numeric() on the ordering values: the pivot check passes and the
     factor equals AmdLuSolver::factor_'s, bit for bit."""
@@ -84,7 +84,7 @@ def test_numeric_values_match_reference(schedule):
             np.testing.assert_array_equal(lu, packed_factor(c["f1"]), err_msg=c["name"])
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 def test_refactorize_and_solve_match_reference(schedule):
     """refactorize() on second values: the replay (or, where its growth test
     fails, the factor_ the reference falls back to) and the solve."""

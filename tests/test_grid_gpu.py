@@ -1,0 +1,68 @@
+"""The grid-wide schedule (one large instance refactored and swept by every
+SM): bit-identical to the one-CTA-per-instance schedules, and to the
+reference's AmdLuSolver on a power grid of 10^4 unknowns."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from neospice_b200 import workloads as W
+from neospice_b200.solver import Batch, Topology
+
+pytestmark = pytest.mark.gpu
+
+
+def grid_matrix(side, pitch, loads, seed):
+    c = W.power_grid(np.random.default_rng(seed), side, pitch, loads).build()
+    cp, ri = c.pattern()
+    vals, _ = c.initial_matrix(0.0)
+    return len(cp) - 1, cp, ri, vals
+
+
+def factor_and_solve(topo, vals, b, schedule, check=False):
+    batch = Batch([topo])
+    batch.set_schedule(schedule)
+    d_a = torch.from_numpy(np.asarray(vals, np.float64)).cuda()
+    st, fs = batch.refactor(d_a, 0.0, check_pivots=check)
+    d_x = torch.from_numpy(np.asarray(b, np.float64).copy()).cuda()
+    batch.solve(d_x)
+    torch.cuda.synchronize()
+    info = topo.info()
+    return int(st.cpu()[0]), batch.lu_values()[:info["nnz_lu"]], d_x.cpu().numpy()
+
+
+@pytest.mark.parametrize("engine", ["amdlu", "markowitz"])
+def test_grid_schedule_matches_cta_schedule(engine):
+    rng = np.random.default_rng(3)
+    n, cp, ri, vals = grid_matrix(40, 8, 20, 1)
+    topo = Topology.order(n, cp, ri, vals, solver=engine)
+    vals2 = vals * np.exp(0.01 * rng.standard_normal(len(vals)))
+    b = rng.standard_normal(n)
+    s0, lu0, x0 = factor_and_solve(topo, vals2, b, 0)
+    s2, lu2, x2 = factor_and_solve(topo, vals2, b, 2)
+    assert s0 == s2 == 0
+    np.testing.assert_array_equal(lu2, lu0)
+    np.testing.assert_array_equal(x2, x0)
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built")
+def test_grid_schedule_power_grid_matches_reference():
+    """A 100 x 100 power grid with pads: the reference's AmdLuSolver numeric
+    + refactorize + solve, and this library's grid-wide replay, bit for bit."""
+    rng = np.random.default_rng(4)
+    n, cp, ri, vals = grid_matrix(100, 20, 100, 2)
+    ref = oracle.RefAmdLu(n, cp, ri)
+    assert ref.numeric(vals) == 0
+    topo = Topology.order(n, cp, ri, vals, solver="amdlu")
+    vals2 = vals * np.exp(0.02 * rng.standard_normal(len(vals)))
+    assert ref.refactorize(vals2) == 0
+    b = rng.standard_normal(n)
+    x_ref = ref.solve(b)
+    s, lu, x = factor_and_solve(topo, vals2, b, 2)
+    assert s == 0
+    f = ref.export()
+    packed = np.concatenate([np.concatenate([f["Ux"][f["Up"][k]:f["Up"][k + 1]],
+                                             f["Lx"][f["Lp"][k] + 1:f["Lp"][k + 1]]])
+                             for k in range(n)])
+    np.testing.assert_array_equal(lu, packed)
+    np.testing.assert_array_equal(x, x_ref)

@@ -47,7 +47,7 @@ def _run(topos, vals, bs, gmin=0.0, check=False, schedule=0):
     return out
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 def test_refactor_and_solves_match_golden_bitwise(schedule):
     topos = [Topology.order(int(c["n"]), c["col_ptr"], c["row_idx"], c["vals"]) for c in CASES]
     first = _run(topos, [c["vals"] for c in CASES], None, schedule=schedule)
@@ -75,7 +75,7 @@ def test_imported_structure_matches():
     np.testing.assert_array_equal(res["x"][0], c["x"])
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 def test_mixed_batch_against_port(schedule):
     rng = np.random.default_rng(11)
     mats = [mna_mesh(rng, s, 1 + s % 3) for s in (4, 9, 17, 30, 45)]
@@ -112,7 +112,7 @@ def test_zero_pivot_flagged_singular():
     assert res["step"][1] == step == 0
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 2])
 def test_pivot_revalidation_flags_match_port(schedule):
     rng = np.random.default_rng(8)
     topos, vals, expect = [], [], []
