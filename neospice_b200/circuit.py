@@ -293,6 +293,52 @@ class TranBatch:
         L.check(L.lib().nsg_tran_batch_orderings(self._h, ctypes.byref(n)))
         return n.value
 
+    # --- adjoint -------------------------------------------------------------
+    def record(self, enable: bool = True):
+        """Record each accepted step's integration formula and the operating
+        point during the next run(), for adjoint()."""
+        L.check(L.lib().nsg_tran_batch_record(self._h, int(bool(enable))))
+
+    def set_adjoint_options(self, reltol=1e-3, vntol=1e-6, abstol=1e-12, max_iter=100):
+        """Newton tolerances of the adjoint's re-solves of the recorded steps."""
+        L.check(L.lib().nsg_tran_batch_set_adjoint_options(self._h, float(reltol), float(vntol),
+                                                           float(abstol), int(max_iter)))
+
+    def params(self):
+        """(offsets [count+1], DC parameter vector, transient parameter
+        vector): the packed circuit parameters (PULSE defaults resolved in
+        the transient one)."""
+        off = np.zeros(self.count + 1, np.int64)
+        L.check(L.lib().nsg_tran_batch_params(self._h, L.llptr(off), None, None))
+        dc = np.zeros(int(off[-1]))
+        tr = np.zeros(int(off[-1]))
+        L.check(L.lib().nsg_tran_batch_params(self._h, L.llptr(off), L.dptr(dc), L.dptr(tr)))
+        return off, dc, tr
+
+    def adjoint(self, probes, d_targets, weight=1.0, every=32, d_params_dc=None,
+                d_params_tran=None, stream=None):
+        """Loss w * sum_n (x_n[probe] - target_n)^2 over the recorded run's
+        timepoints (targets packed like the output points: max_points per
+        circuit) and its gradient with respect to the parameters (R, C,
+        MOSFET W / L / VTO; others zero), by the discrete adjoint with a
+        checkpoint every `every` steps.  Returns device tensors (grads packed
+        like params(), loss per circuit, status per circuit)."""
+        import torch
+        off = np.zeros(self.count + 1, np.int64)
+        L.check(L.lib().nsg_tran_batch_params(self._h, L.llptr(off), None, None))
+        grads = torch.empty(int(off[-1]), dtype=torch.float64, device="cuda")
+        loss = torch.empty(self.count, dtype=torch.float64, device="cuda")
+        status = torch.empty(self.count, dtype=torch.int32, device="cuda")
+        pr = np.ascontiguousarray(probes, np.int32)
+        sp = torch.cuda.current_stream().cuda_stream if stream is None else \
+            getattr(stream, "cuda_stream", stream)
+        L.check(L.lib().nsg_tran_batch_adjoint(
+            self._h, L.iptr(pr), d_targets.contiguous().data_ptr(), float(weight), int(every),
+            None if d_params_dc is None else d_params_dc.data_ptr(),
+            None if d_params_tran is None else d_params_tran.data_ptr(),
+            grads.data_ptr(), loss.data_ptr(), status.data_ptr(), sp))
+        return grads, loss, status
+
     def engines(self):
         """(DC engines, transient engines) per circuit: "markowitz",
         "amdlu", or None for a solver not ordered yet."""

@@ -2,6 +2,7 @@
 #include "capi_internal.hpp"
 
 #include "host/circuit.hpp"
+#include "kernels/mos1_model.cuh"
 #include "kernels/tran_device.cuh"
 
 #include <algorithm>
@@ -19,8 +20,20 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
                              const TranOptions& o, int max_col, int max_n, long long max_stage,
-                             cudaStream_t stream);
+                             StepRecord* rec_steps, double* rec_x0, cudaStream_t stream);
 size_t tran_smem_bytes(int max_col, int max_n);
+struct AdjDesc {
+    int32_t n_steps, every, probe, n_ckpt;
+    int64_t rec_off, x0_off, ws_off, ckpt_len;
+};
+cudaError_t launch_tran_adjoint(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
+                                const TranDesc* tdescs, const AdjDesc* adescs, int count,
+                                const int32_t* prog, const double* params_dc,
+                                const double* params_tran, double* work, double* adj_ws,
+                                const StepRecord* recs, const double* times, const double* rec_x0,
+                                const double* targets, double weight, double* grads, double* loss,
+                                int32_t* status, const NewtonOptions& opt, int max_iter,
+                                int max_col, int max_n, cudaStream_t stream);
 }  // namespace nsg
 
 using namespace nsg_internal;
@@ -53,7 +66,24 @@ struct nsg_tran_batch {
     int32_t* d_stats = nullptr;
     nsg::TranCtl* d_ctl = nullptr;
     int32_t* d_subset = nullptr;
+    // Adjoint: recording of the forward run's steps and operating points,
+    // the replay's Newton options, whether each circuit's devices are ones
+    // the adjoint covers (no MOSFET charge), and its workspace.
+    bool record = false, recorded = false;
+    nsg::StepRecord* d_rec = nullptr;
+    double* d_x0 = nullptr;
+    std::vector<char> adjoint_ok;
+    std::vector<int64_t> param_count;
+    nsg::NewtonOptions adj_opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, 0};
+    int adj_max_iter = 100;
+    double* d_adj_ws = nullptr;
+    int64_t adj_ws_cap = 0;
+    nsg::AdjDesc* d_adescs = nullptr;
     ~nsg_tran_batch() {
+        cudaFree(d_rec);
+        cudaFree(d_x0);
+        cudaFree(d_adj_ws);
+        cudaFree(d_adescs);
         for (void* p : {static_cast<void*>(d_lu_pool), static_cast<void*>(d_plans),
                         static_cast<void*>(d_prog), static_cast<void*>(d_descs),
                         static_cast<void*>(d_tdescs), static_cast<void*>(d_work),
@@ -184,9 +214,20 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         b->descs.resize(count);
         b->tdescs.resize(count);
         std::vector<double> params_dc, params_tran, all_bps;
-        int64_t work = 0, param_off = 0;
+        int64_t work = 0, param_off = 0, x0_off = 0;
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
+            // The adjoint covers MOSFETs without charge: no oxide, overlap or
+            // junction capacitance in the parameter block.
+            bool ok = true;
+            for (const auto& m : c.mosfets()) {
+                const double* P = c.params().data() + m.param;
+                for (int q : {nsg::kMOxCapFactor, nsg::kMCgso, nsg::kMCgdo, nsg::kMCgbo,
+                              nsg::kMCbd, nsg::kMCbdsw, nsg::kMCbs, nsg::kMCbssw})
+                    if (P[q] != 0.0) ok = false;
+            }
+            b->adjoint_ok.push_back(ok ? 1 : 0);
+            b->param_count.push_back(static_cast<int64_t>(c.params().size()));
             nsg::DcDesc& d = b->descs[i];
             fill_instance(d, c, b->topos[plan_dc[i]]->plan, prog, work);
             d.index = i;
@@ -207,6 +248,8 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             d.stage_len = work - d.x_off;
             place_dcsave(d, work);
             t.dt0 = dt0[i];
+            t.x0_off = x0_off;
+            x0_off += c.num_vars();
             b->col_ptr.push_back(c.col_ptr());
             b->row_idx.push_back(c.row_idx());
         }
@@ -252,8 +295,11 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                                          n, b->d_prog, b->d_params_dc, b->d_params_tran, b->d_work,
                                          b->d_bps, b->d_probes, b->d_times, b->d_values,
                                          b->d_npoints, b->d_status, b->d_stats, b->d_ctl, b->opt,
-                                         b->max_col, b->max_n, max_stage_len(b->descs), st);
+                                         b->max_col, b->max_n, max_stage_len(b->descs),
+                                         b->record ? b->d_rec : nullptr,
+                                         b->record ? b->d_x0 : nullptr, st);
         };
+        b->recorded = false;
         cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::TranCtl) * b->count, st);
         if (e == cudaSuccess) e = launch(nullptr, b->count);
         if (e != cudaSuccess) return cuda_fail("nsg_tran_batch_run", e);
@@ -296,7 +342,10 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                 subset.push_back(i);
                 ++b->orderings;
             }
-            if (subset.empty()) break;
+            if (subset.empty()) {
+                b->recorded = b->record;
+                break;
+            }
             int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col, &b->max_n);
             if (rc != NSG_OK) return rc;
             if (nsg::tran_smem_bytes(b->max_col, b->max_n) > 200 * 1024)
@@ -328,6 +377,146 @@ int nsg_tran_batch_engines(const nsg_tran_batch* b, int* dc_engine, int* tran_en
         if (tran_engine) tran_engine[i] = kind(b->tdescs[i].tran_plan);
     }
     return NSG_OK;
+}
+
+int nsg_tran_batch_record(nsg_tran_batch* b, int enable) {
+    return guarded("nsg_tran_batch_record", [&]() -> int {
+        if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_record: null batch");
+        b->record = enable != 0;
+        if (b->record && !b->d_rec) {
+            int64_t nx = 0;
+            for (const auto& d : b->descs) nx += d.n;
+            cudaError_t e;
+            if ((e = upload<nsg::StepRecord>(&b->d_rec, nullptr,
+                                             static_cast<size_t>(b->count) * b->opt.max_points)) !=
+                    cudaSuccess ||
+                (e = upload<double>(&b->d_x0, nullptr, static_cast<size_t>(nx))) != cudaSuccess)
+                return cuda_fail("nsg_tran_batch_record", e);
+        }
+        return NSG_OK;
+    });
+}
+
+int nsg_tran_batch_set_adjoint_options(nsg_tran_batch* b, double reltol, double vntol,
+                                       double abstol, int max_iter) {
+    if (!b || !(reltol > 0.0) || !(vntol >= 0.0) || !(abstol >= 0.0) || max_iter < 1)
+        return fail(NSG_ERR_INVALID, "nsg_tran_batch_set_adjoint_options: bad arguments");
+    b->adj_opt.reltol = reltol;
+    b->adj_opt.vntol = vntol;
+    b->adj_opt.abstol = abstol;
+    b->adj_max_iter = max_iter;
+    return NSG_OK;
+}
+
+int nsg_tran_batch_params(const nsg_tran_batch* b, long long* offsets, double* params_dc,
+                          double* params_tran) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_params: null batch");
+    int64_t total = 0;
+    for (int i = 0; i < b->count; ++i) {
+        if (offsets) offsets[i] = total;
+        total += b->param_count[i];
+    }
+    if (offsets) offsets[b->count] = total;
+    cudaError_t e = cudaSuccess;
+    if (params_dc)
+        e = cudaMemcpy(params_dc, b->d_params_dc, sizeof(double) * total, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && params_tran)
+        e = cudaMemcpy(params_tran, b->d_params_tran, sizeof(double) * total,
+                       cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_tran_batch_params", e);
+}
+
+int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_targets,
+                           double weight, int every, const double* d_params_dc,
+                           const double* d_params_tran, double* d_grads, double* d_loss,
+                           int* d_status, void* stream) {
+    return guarded("nsg_tran_batch_adjoint", [&]() -> int {
+        if (!b || !probe || !d_targets || !d_grads || !d_loss || !d_status || every < 1)
+            return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: bad arguments");
+        if (!b->recorded)
+            return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: no recorded run (enable "
+                                         "nsg_tran_batch_record before nsg_tran_batch_run)");
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        std::vector<int> npts(b->count), status(b->count);
+        cudaError_t e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess ||
+            (e = cudaMemcpy(npts.data(), b->d_npoints, sizeof(int) * b->count,
+                            cudaMemcpyDeviceToHost)) != cudaSuccess ||
+            (e = cudaMemcpy(status.data(), b->d_status, sizeof(int) * b->count,
+                            cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return cuda_fail("nsg_tran_batch_adjoint", e);
+        std::vector<nsg::AdjDesc> ad(b->count);
+        int64_t ws = 0;
+        for (int i = 0; i < b->count; ++i) {
+            const auto& d = b->descs[i];
+            const auto& t = b->tdescs[i];
+            if (status[i] != 0 || t.tran_plan < 0)
+                return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
+                                                 std::to_string(i) + " has no completed run");
+            if (npts[i] >= b->opt.max_points)
+                return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
+                                                 std::to_string(i) +
+                                                 " filled max_points; the schedule is incomplete");
+            if (!b->adjoint_ok[i])
+                return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
+                                                 std::to_string(i) +
+                                                 " has MOSFETs with charge (not covered)");
+            if (probe[i] < 0 || probe[i] >= d.n)
+                return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: probe out of range");
+            nsg::AdjDesc& a = ad[i];
+            a.n_steps = npts[i] - 1;
+            a.every = every;
+            a.probe = probe[i];
+            a.n_ckpt = a.n_steps / every + 1;
+            a.rec_off = t.out_off;
+            a.x0_off = t.x0_off;
+            const int64_t nmos = d.n_mos, ndio = d.n_diodes;
+            a.ckpt_len = (2 * d.n + 2 * d.n_states + 3 * ndio + 12 * nmos + 3) & ~int64_t{3};
+            a.ws_off = ws;
+            ws += a.n_ckpt * a.ckpt_len + (every + 2) * (int64_t{d.n} + d.n_states) +
+                  3 * int64_t{d.n_caps} + d.n;
+            ws = (ws + 3) & ~int64_t{3};
+            // The LU region must hold both the DC and the transient plan.
+            const auto& pd = b->topos[d.plan]->plan;
+            const auto& pt = b->topos[t.tran_plan]->plan;
+            if (pd.nnz_lu > pt.nnz_lu || pd.lrow_ptr[pd.n] > pt.lrow_ptr[pt.n] ||
+                pd.urow_ptr[pd.n] > pt.urow_ptr[pt.n]) {
+                nsg::TopologyPlan big = pd.nnz_lu >= pt.nnz_lu ? pd : pt;
+                big.lrow_ptr[big.n] = std::max(pd.lrow_ptr[pd.n], pt.lrow_ptr[pt.n]);
+                big.urow_ptr[big.n] = std::max(pd.urow_ptr[pd.n], pt.urow_ptr[pt.n]);
+                place_lu_workspace(b->descs[i], big, b->work_size);
+            }
+        }
+        if ((e = grow_workspace(&b->d_work, &b->work_cap, b->work_size)) != cudaSuccess ||
+            (e = cudaMemcpy(b->d_descs, b->descs.data(), sizeof(nsg::DcDesc) * b->count,
+                            cudaMemcpyHostToDevice)) != cudaSuccess)
+            return cuda_fail("nsg_tran_batch_adjoint", e);
+        if (ws > b->adj_ws_cap) {
+            cudaFree(b->d_adj_ws);
+            b->d_adj_ws = nullptr;
+            b->adj_ws_cap = 0;
+            if ((e = cudaMalloc(reinterpret_cast<void**>(&b->d_adj_ws), sizeof(double) * ws)) !=
+                cudaSuccess)
+                return cuda_fail("nsg_tran_batch_adjoint", e);
+            b->adj_ws_cap = ws;
+        }
+        if (!b->d_adescs &&
+            (e = upload<nsg::AdjDesc>(&b->d_adescs, nullptr, b->count)) != cudaSuccess)
+            return cuda_fail("nsg_tran_batch_adjoint", e);
+        int64_t nparam = 0;
+        for (auto c : b->param_count) nparam += c;
+        if ((e = cudaMemcpy(b->d_adescs, ad.data(), sizeof(nsg::AdjDesc) * b->count,
+                            cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemsetAsync(d_grads, 0, sizeof(double) * nparam, st)) != cudaSuccess ||
+            (e = nsg::launch_tran_adjoint(
+                 b->d_plans, b->d_lu_pool, b->d_descs, b->d_tdescs, b->d_adescs, b->count,
+                 b->d_prog, d_params_dc ? d_params_dc : b->d_params_dc,
+                 d_params_tran ? d_params_tran : b->d_params_tran, b->d_work, b->d_adj_ws,
+                 b->d_rec, b->d_times, b->d_x0, d_targets, weight, d_grads, d_loss, d_status,
+                 b->adj_opt, b->adj_max_iter, b->max_col, b->max_n, st)) != cudaSuccess)
+            return cuda_fail("nsg_tran_batch_adjoint", e);
+        return NSG_OK;
+    });
 }
 
 int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count) {

@@ -284,13 +284,16 @@ struct NewtonOutcome {
 // matrix is re-assembled from v.tv (no device re-evaluation) and refactored
 // with the new pivots.  With host_orders_first the solver's first numeric()
 // stops the same way with kStatusNeedOrder, for the host to order a fresh
-// topology on that matrix.
+// topology on that matrix.  With fixed_pivots every factorization replays the
+// plan's pivots unchecked (only a zero pivot fails): for callers that need a
+// solution of the equations, not the reference's pivoting (the adjoint's
+// re-solves).
 __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const int32_t* lu_pool,
                                        IntegCtx* ctx, const NewtonOptions& opt, int max_iter,
                                        SolverState* solver, double* smem, int colbuf,
                                        int resume_iter = -1, int saved_mode = -1,
                                        int resume_dev_conv = 1, bool host_orders_first = false,
-                                       int smem_doubles = 0) {
+                                       int smem_doubles = 0, bool fixed_pivots = false) {
     __shared__ int32_t s_conv, s_dev_conv;
     if (saved_mode < 0) saved_mode = ctx->mode;
     bool force_numeric = false;
@@ -325,8 +328,9 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
         // re-chooses (AMD-LU) the pivots; refactorize() replays them (AMD-LU
         // with the growth test).  A resumed iteration replays the pivots the
         // host just chose.
-        const int check = numeric ? ((solver->factored && !resumed) ? kCheckNumeric : kCheckNone)
-                                  : kCheckRefactor;
+        const int check = fixed_pivots ? kCheckNone
+                          : numeric ? ((solver->factored && !resumed) ? kCheckNumeric : kCheckNone)
+                                    : kCheckRefactor;
         const RefactorResult fr =
             small ? cta_refactor_small(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, lu_s)
                   : cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, smem,

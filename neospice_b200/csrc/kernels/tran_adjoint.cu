@@ -1,0 +1,390 @@
+// Batched transient adjoint: gradients of
+//   L = w * sum_n (x_n[probe] - target_n)^2      (n = 0: the operating point)
+// through the discrete transient of one instance per CTA, with respect to
+// resistances, capacitances and the W, L and VTO of level-1 MOSFETs.
+//
+// The forward run (transient_kernel with recording on) fixes the timepoints
+// and, per accepted step, the integration formula (NIintegrate coefficients,
+// order, method).  This kernel replays that schedule -- Newton on each step
+// with the plan's pivots -- keeping a checkpoint every K steps, then walks the
+// steps backwards, re-solving each K-step segment from its checkpoint.  With
+// the capacitor currents i_n = ag0 q_n + ag1 q_{n-1} + ag2 q_{n-2}
+// - r i_{n-1} (q = C v; r = xmu/(1-xmu) for the trapezoidal rule, else 0)
+// and the step residual R_n = f(x_n) + B i_n - s(t_n), the discrete adjoint
+// is, per step from last to first (eta, mu per capacitor):
+//   mu_n    = -r_{n+1} eta_{n+1}
+//   J_n^T lambda_n = dl_n/dx_n + B (ag0_n C mu_n + ag1_{n+1} C eta_{n+1}
+//                                   + ag2_{n+2} C eta_{n+2})
+//   eta_n   = mu_n - B^T lambda_n
+//   dL/dC  += eta_n (ag0_n v_n + ag1_n v_{n-1} + ag2_n v_{n-2})
+//   dL/dp  -= lambda_n^T dR_n/dp      (R, MOSFET W / L / VTO)
+// with J_n the Newton matrix at x_n (the forward's own assembly and
+// fixed-pivot refactor) and lambda from the transposed solve; the operating
+// point closes the recursion with the DC Jacobian.  Circuits whose MOSFETs
+// carry charge (oxide, overlap or junction capacitance) are rejected by the
+// host: their charge history is not part of this recursion.
+#include "newton_common.cuh"
+#include "tran_device.cuh"
+
+#include <cuda_runtime.h>
+
+namespace nsg {
+
+// Per instance: the replayed schedule and the adjoint workspace.
+struct AdjDesc {
+    int32_t n_steps;     // accepted steps after t = 0
+    int32_t every;       // checkpoint interval K
+    int32_t probe;       // unknown in the loss
+    int32_t n_ckpt;      // checkpoints (steps 0, K, 2K, ...)
+    int64_t rec_off;     // first StepRecord / time / target (t = 0) of the instance
+    int64_t x0_off;      // the recorded operating point
+    int64_t ws_off;      // adjoint workspace
+    int64_t ckpt_len;    // doubles per checkpoint
+};
+
+namespace {
+
+// lambda^T dR/dp contributions of resistors and MOSFET channels at x (the
+// dc_adjoint_kernel contraction), accumulated into g; sources are skipped.
+__device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32_t* prog,
+                                     const double* lam, const double* x, double* g) {
+    const int32_t* gp = prog + d.prog_off[DP_grad];
+    auto at = [&](const double* vec, int32_t i) { return i >= 0 ? vec[i] : 0.0; };
+    for (int32_t r = threadIdx.x; r < d.n_grad; r += blockDim.x) {
+        const int32_t* e = gp + 5 * r;
+        const int32_t kind = e[0], p = e[1], a = e[2], b = e[3];
+        if (kind == 1) {
+            const double R = v.par[p];
+            g[p] += (at(lam, a) - at(lam, b)) * (at(x, a) - at(x, b)) / (R * R);
+        } else if (kind == 4) {
+            const double* P = v.par + p;
+            const double* rec = v.mrec + kMosRecCount * e[4];
+            const double dm = rec[kRMode];
+            const double type = P[kMType];
+            const double cdrain = dm * (rec[kRCd] + rec[kRCbd]);
+            const double leff = P[kML] - 2 * P[kMLatDiff];
+            const double dl = at(lam, a) - at(lam, b);
+            g[p + kMW] += -dl * type * dm * cdrain / P[kMW];
+            g[p + kML] += dl * type * dm * cdrain / leff;
+            g[p + kMVto] += dl * dm * rec[kRGm];
+        }
+    }
+}
+
+// Integrator context of accepted step n (1-based) from its record.
+__device__ inline IntegCtx step_ctx(const StepRecord& r, double t, int mode) {
+    IntegCtx c{};
+    for (int q = 0; q < 3; ++q) c.ag[q] = r.ag[q];
+    c.xmu_ratio = r.xmu_ratio;
+    c.delta = (r.ag[0] != 0.0) ? 1.0 / r.ag[0] : 0.0;
+    c.delta_old[0] = c.delta;
+    c.delta_old[1] = c.delta;
+    c.delta_old[2] = c.delta;
+    c.time = t;
+    c.mode = mode;
+    c.order = r.order;
+    c.method = r.method;
+    return c;
+}
+
+__device__ inline void vcopy(double* dst, const double* src, int64_t n) {
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kFlowThreads, 2)
+tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ lu_pool,
+                    const DcDesc* __restrict__ descs, const TranDesc* __restrict__ tdescs,
+                    const AdjDesc* __restrict__ adescs, const int32_t* __restrict__ prog,
+                    const double* __restrict__ params_dc, const double* __restrict__ params_tran,
+                    double* __restrict__ work, double* __restrict__ adj_ws,
+                    const StepRecord* __restrict__ recs, const double* __restrict__ times,
+                    const double* __restrict__ rec_x0, const double* __restrict__ targets,
+                    double weight, double* __restrict__ grads, double* __restrict__ loss,
+                    int32_t* __restrict__ status, NewtonOptions opt, int max_iter, int colbuf,
+                    int scratch_doubles) {
+    extern __shared__ double smem[];
+    const DcDesc d = descs[blockIdx.x];
+    const TranDesc td = tdescs[blockIdx.x];
+    const AdjDesc ad = adescs[blockIdx.x];
+    const PlanDesc& dpd = plans[d.plan];
+    const PlanDesc& tpd = plans[td.tran_plan];
+    Inst v = make_inst(d, prog, params_tran, work);
+    const int32_t n = v.n, ns = d.n_states;
+    const int64_t K = ad.every;
+    const StepRecord* rec = recs + ad.rec_off;  // rec[s] for step s >= 1
+    const double* tm = times + ad.rec_off;
+    const double* tg = targets + ad.rec_off;
+    double* g = grads + d.param_off;
+    double* ws = adj_ws + ad.ws_off;
+    // workspace: checkpoints | segment x (K+2) | segment states (K+2) | eta1 | eta2 | mu | lam
+    double* ckpt = ws;
+    double* seg_x = ckpt + ad.n_ckpt * ad.ckpt_len;
+    double* seg_s = seg_x + (K + 2) * n;
+    double* eta1 = seg_s + (K + 2) * ns;
+    double* eta2 = eta1 + v.n_caps;
+    double* mu = eta2 + v.n_caps;
+    double* lam = mu + v.n_caps;
+    double* w = work + d.w_off;
+    __shared__ IntegCtx ctx;
+    __shared__ SolverState solver;
+    __shared__ int32_t s_fail, s_dev_conv;
+    __shared__ double s_loss;
+
+    auto save_ckpt = [&](int64_t c, const double* xc, const double* xprev) {
+        double* r = ckpt + c * ad.ckpt_len;
+        vcopy(r, xc, n);
+        vcopy(r + n, xprev, n);
+        vcopy(r + 2 * n, v.st[1], ns);
+        vcopy(r + 2 * n + ns, v.st[2], ns);
+        vcopy(r + 2 * n + 2 * ns, v.dstate, 3 * v.n_diodes);
+        vcopy(r + 2 * n + 2 * ns + 3 * v.n_diodes, v.mrec, kMosRecCount * v.n_mos);
+    };
+    // Accepted step s from the current state: Newton, then rotate the ring
+    // (state3 <- state2 <- state1 <- state0).  False if Newton failed.
+    auto step = [&](int64_t s) -> bool {
+        if (threadIdx.x == 0) {
+            ctx = step_ctx(rec[s], tm[s], kModeTran | (s == 1 ? kModeInitTran : kModeInitPred));
+            solver.factored = 1;
+        }
+        __syncthreads();
+        const NewtonOutcome r = newton(v, tpd, lu_pool, &ctx, opt, max_iter, &solver, smem, colbuf,
+                                       -1, -1, 1, false, scratch_doubles, true);
+        if (r.code != kDcConverged) return false;
+        vcopy(v.st[3], v.st[2], ns);
+        __syncthreads();
+        vcopy(v.st[2], v.st[1], ns);
+        __syncthreads();
+        vcopy(v.st[1], v.st[0], ns);
+        __syncthreads();
+        return true;
+    };
+    auto fail_with = [&](int32_t code) {
+        if (threadIdx.x == 0) status[d.index] = code;
+    };
+    auto dl = [&](const double* x, int64_t s) {
+        return 2.0 * weight * (x[ad.probe] - tg[s]);
+    };
+
+    // ---- 1. operating point: the recorded x_0; states seeded from it
+    v.par = params_dc + d.param_off;
+    load_constants(v, opt.gmin);
+    vcopy(v.x, rec_x0 + td.x0_off, n);
+    vcopy(v.xold, rec_x0 + td.x0_off, n);
+    for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) v.dstate[i] = 0.0;
+    for (int32_t i = threadIdx.x; i < kMosRecCount * v.n_mos; i += blockDim.x) v.mrec[i] = 0.0;
+    for (int32_t i = threadIdx.x; i < 4 * ns; i += blockDim.x) v.st[0][i] = 0.0;
+    if (threadIdx.x == 0) {
+        ctx = IntegCtx{};
+        ctx.mode = kModeTranOp | kModeInitFloat;
+        ctx.order = 1;
+        s_dev_conv = 1;
+        s_fail = 0;
+        s_loss = 0.0;
+    }
+    __syncthreads();
+    // states at x_0 (q = C v_0; MOSFET voltages, twice so that the second
+    // load's limiting starts from x_0's own voltages)
+    for (int pass = 0; pass < 2; ++pass) {
+        eval_devices(v, ctx, opt, &s_dev_conv);
+        __syncthreads();
+    }
+    for (int32_t i = threadIdx.x; i < ns; i += blockDim.x)
+        v.st[1][i] = v.st[2][i] = v.st[3][i] = v.st[0][i];
+    for (int32_t i = threadIdx.x; i < d.n_grad; i += blockDim.x) {
+        const int32_t* e = prog + d.prog_off[DP_grad] + 5 * i;
+        g[e[1]] = 0.0;
+        if (e[0] == 4) g[e[1] + kMW] = g[e[1] + kML] = g[e[1] + kMVto] = 0.0;
+    }
+    for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) g[v.caps[5 * k + 2]] = 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double e0 = v.x[ad.probe] - tg[0];
+        s_loss = weight * e0 * e0;
+    }
+    save_ckpt(0, v.x, v.x);
+    __syncthreads();
+
+    // ---- 2. forward replay with checkpoints every K steps
+    v.par = params_tran + d.param_off;
+    load_constants(v, opt.gmin);
+    double* xprev = seg_x;  // x_{s-1} while replaying
+    vcopy(xprev, v.x, n);
+    __syncthreads();
+    for (int64_t s = 1; s <= ad.n_steps; ++s) {
+        if (!step(s)) {
+            fail_with(kTranNewtonFailed);
+            return;
+        }
+        if (threadIdx.x == 0) {
+            const double e = v.x[ad.probe] - tg[s];
+            s_loss += weight * e * e;
+        }
+        if (s % K == 0) save_ckpt(s / K, v.x, xprev);
+        __syncthreads();
+        vcopy(xprev, v.x, n);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) loss[d.index] = s_loss;
+
+    // ---- 3. backward, segment by segment
+    for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) eta1[k] = eta2[k] = 0.0;
+    __syncthreads();
+    for (int64_t c0 = ((ad.n_steps - 1) / K) * K; c0 >= 0; c0 -= K) {
+        const int64_t c1 = (c0 + K < ad.n_steps) ? c0 + K : ad.n_steps;
+        // restore checkpoint c0 and re-solve steps c0+1..c1 (slot j holds step c0-1+j)
+        const double* r = ckpt + (c0 / K) * ad.ckpt_len;
+        vcopy(v.x, r, n);
+        vcopy(seg_x + n, r, n);
+        vcopy(seg_x, r + n, n);
+        vcopy(v.st[0], r + 2 * n, ns);
+        vcopy(v.st[1], r + 2 * n, ns);
+        vcopy(seg_s + ns, r + 2 * n, ns);
+        vcopy(v.st[2], r + 2 * n + ns, ns);
+        vcopy(seg_s, r + 2 * n + ns, ns);
+        vcopy(v.dstate, r + 2 * n + 2 * ns, 3 * v.n_diodes);
+        vcopy(v.mrec, r + 2 * n + 2 * ns + 3 * v.n_diodes, kMosRecCount * v.n_mos);
+        __syncthreads();
+        for (int64_t s = c0 + 1; s <= c1; ++s) {
+            if (!step(s)) {
+                fail_with(kTranNewtonFailed);
+                return;
+            }
+            vcopy(seg_x + (s - c0 + 1) * n, v.x, n);
+            vcopy(seg_s + (s - c0 + 1) * ns, v.st[1], ns);
+            __syncthreads();
+        }
+        for (int64_t s = c1; s > c0; --s) {
+            const double* xs = seg_x + (s - c0 + 1) * n;
+            const double* x1 = seg_x + (s - c0) * n;
+            const double* x2 = seg_x + (s - c0 - 1) * n;
+            // the Newton matrix at x_s
+            vcopy(v.xold, xs, n);
+            vcopy(v.st[0], seg_s + (s - c0 + 1) * ns, ns);
+            vcopy(v.st[1], seg_s + (s - c0) * ns, ns);
+            vcopy(v.st[2], seg_s + (s - c0 - 1) * ns, ns);
+            if (threadIdx.x == 0) {
+                ctx = step_ctx(rec[s], tm[s], kModeTran | kModeInitFloat);
+                s_dev_conv = 1;
+            }
+            __syncthreads();
+            eval_devices(v, ctx, opt, &s_dev_conv);
+            __syncthreads();
+            assemble(v);
+            const RefactorResult fr = cta_refactor_flow(tpd, lu_pool, v.a, v.lu, opt.diag_gmin,
+                                                        kCheckNone, 1e-3, smem, colbuf,
+                                                        v.lrows, v.urows);
+            if (fr.code != kStatusOk) {
+                fail_with(fr.code);
+                return;
+            }
+            // right-hand side
+            for (int32_t i = threadIdx.x; i < n; i += blockDim.x) lam[i] = 0.0;
+            __syncthreads();
+            if (threadIdx.x == 0) lam[ad.probe] = dl(xs, s);
+            __syncthreads();
+            const bool has1 = s + 1 <= ad.n_steps, has2 = s + 2 <= ad.n_steps;
+            for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
+                const int32_t* cr = v.caps + 5 * k;
+                const double C = v.par[cr[2]];
+                const double m = has1 ? -rec[s + 1].xmu_ratio * eta1[k] : 0.0;
+                mu[k] = m;
+                double cc = rec[s].ag[0] * C * m;
+                if (has1) cc += rec[s + 1].ag[1] * C * eta1[k];
+                if (has2) cc += rec[s + 2].ag[2] * C * eta2[k];
+                if (cr[0] >= 0) atomicAdd(lam + cr[0], cc);
+                if (cr[1] >= 0) atomicAdd(lam + cr[1], -cc);
+            }
+            __syncthreads();
+            cta_solve_transposed(tpd, lu_pool, v.lu, lam, w);
+            // capacitor adjoints and dL/dC
+            for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
+                const int32_t* cr = v.caps + 5 * k;
+                auto at = [&](const double* vec, int32_t i) { return i >= 0 ? vec[i] : 0.0; };
+                const double e = mu[k] - (at(lam, cr[0]) - at(lam, cr[1]));
+                const double dv0 = at(xs, cr[0]) - at(xs, cr[1]);
+                const double dv1 = at(x1, cr[0]) - at(x1, cr[1]);
+                const double dv2 = at(x2, cr[0]) - at(x2, cr[1]);
+                g[cr[2]] += e * (rec[s].ag[0] * dv0 + rec[s].ag[1] * dv1 + rec[s].ag[2] * dv2);
+                eta2[k] = eta1[k];
+                eta1[k] = e;
+            }
+            grad_contract(v, d, prog, lam, xs, g);
+            __syncthreads();
+        }
+    }
+
+    // ---- 4. the operating point: DC Jacobian, cotangent from steps 1 and 2
+    const double* x0 = rec_x0 + td.x0_off;
+    v.par = params_dc + d.param_off;
+    load_constants(v, opt.gmin);
+    vcopy(v.xold, x0, n);
+    const double* r0 = ckpt;
+    vcopy(v.mrec, r0 + 2 * n + 2 * ns + 3 * v.n_diodes, kMosRecCount * v.n_mos);
+    vcopy(v.st[0], r0 + 2 * n, ns);
+    if (threadIdx.x == 0) {
+        ctx = IntegCtx{};
+        ctx.mode = kModeTranOp | kModeInitFloat;
+        ctx.order = 1;
+        s_dev_conv = 1;
+    }
+    __syncthreads();
+    eval_devices(v, ctx, opt, &s_dev_conv);
+    __syncthreads();
+    assemble(v);
+    const RefactorResult fr = cta_refactor_flow(dpd, lu_pool, v.a, v.lu, opt.diag_gmin, kCheckNone,
+                                                1e-3, smem, colbuf, v.lrows, v.urows);
+    if (fr.code != kStatusOk) {
+        fail_with(fr.code);
+        return;
+    }
+    for (int32_t i = threadIdx.x; i < n; i += blockDim.x) lam[i] = 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0) lam[ad.probe] = dl(x0, 0);
+    __syncthreads();
+    for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
+        const int32_t* cr = v.caps + 5 * k;
+        const double C = v.par[cr[2]];
+        double cc = 0.0;
+        if (ad.n_steps >= 1) cc += rec[1].ag[1] * C * eta1[k];
+        if (ad.n_steps >= 2) cc += rec[2].ag[2] * C * eta2[k];
+        if (cr[0] >= 0) atomicAdd(lam + cr[0], cc);
+        if (cr[1] >= 0) atomicAdd(lam + cr[1], -cc);
+    }
+    __syncthreads();
+    cta_solve_transposed(dpd, lu_pool, v.lu, lam, w);
+    grad_contract(v, d, prog, lam, x0, g);
+    __syncthreads();
+    if (threadIdx.x == 0) status[d.index] = kStatusOk;
+}
+
+cudaError_t launch_tran_adjoint(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
+                                const TranDesc* tdescs, const AdjDesc* adescs, int count,
+                                const int32_t* prog, const double* params_dc,
+                                const double* params_tran, double* work, double* adj_ws,
+                                const StepRecord* recs, const double* times, const double* rec_x0,
+                                const double* targets, double weight, double* grads, double* loss,
+                                int32_t* status, const NewtonOptions& opt, int max_iter,
+                                int max_col, int max_n, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    const int colbuf = (max_col + 31) & ~31;
+    const size_t a = flow_smem_bytes(colbuf, max_n), b = flow_solve_smem_bytes(max_n);
+    const size_t smem = ((a > b ? a : b) + 15) & ~size_t{15};
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(tran_adjoint_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             200 * 1024);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    tran_adjoint_kernel<<<count, kFlowThreads, smem, stream>>>(
+        plans, lu_pool, descs, tdescs, adescs, prog, params_dc, params_tran, work, adj_ws, recs,
+        times, rec_x0, targets, weight, grads, loss, status, opt, max_iter, colbuf,
+        static_cast<int>(smem / sizeof(double)));
+    return cudaGetLastError();
+}
+
+}  // namespace nsg

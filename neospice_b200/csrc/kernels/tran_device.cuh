@@ -14,6 +14,15 @@ struct TranDesc {
     int64_t out_off;    // first output point slot of this instance
     int64_t hist_off;   // workspace: three history vectors of n doubles
     double dt0;         // initial timestep (transient.cpp:851-865)
+    int64_t x0_off;     // recording: the operating point (n doubles) in the x0 record
+};
+
+// Integration record of one accepted timepoint (recording on): what the
+// adjoint needs to replay the step with the same formula.
+struct StepRecord {
+    double ag[3];       // NIintegrate coefficients
+    double xmu_ratio;   // trapezoidal: weight of the previous current
+    int32_t order, method, pad[2];
 };
 
 // SimOptions / .tran parameters of the transient driver.

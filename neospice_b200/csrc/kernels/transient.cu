@@ -183,7 +183,8 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  double* __restrict__ values, int32_t* __restrict__ npoints,
                  int32_t* __restrict__ status, int32_t* __restrict__ stats,
                  TranCtl* __restrict__ ctls, TranOptions o, int colbuf, int scratch_doubles,
-                 int stage_doubles) {
+                 int stage_doubles, StepRecord* __restrict__ rec_steps,
+                 double* __restrict__ rec_x0) {
     extern __shared__ double smem[];
     const int pos = subset ? subset[blockIdx.x] : blockIdx.x;
     const DcDesc d = descs[pos];
@@ -250,6 +251,8 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x)
             hist[i] = hist[v.n + i] = hist[2 * v.n + i] = v.x[i];
         store_point(td, o, probes, times, values, 0, 0.0, v.x);
+        if (rec_x0)
+            for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) rec_x0[td.x0_off + i] = v.x[i];
         if (threadIdx.x == 0) {
             k.points = 1;
             k.hist[0] = 0;
@@ -363,6 +366,13 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
 
         // Accept (transient.cpp:966-1051).
         if (threadIdx.x == 0) {
+            if (rec_steps && k.points < o.max_points) {
+                StepRecord& r = rec_steps[td.out_off + k.points];
+                for (int q = 0; q < 3; ++q) r.ag[q] = k.ctx.ag[q];
+                r.xmu_ratio = k.ctx.xmu_ratio;
+                r.order = k.ctx.order;
+                r.method = k.ctx.method;
+            }
             const double dt = k.dt;
             k.prev_prev_dt = k.prev_dt;
             k.prev_dt = dt;
@@ -473,7 +483,7 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
                              const TranOptions& o, int max_col, int max_n, long long max_stage,
-                             cudaStream_t stream) {
+                             StepRecord* rec_steps, double* rec_x0, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
     const size_t scratch = (tran_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
@@ -491,7 +501,8 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
     transient_kernel<<<count, kFlowThreads, smem, stream>>>(
         plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes,
         times, values, npoints, status, stats, ctls, o, colbuf,
-        static_cast<int>(scratch / sizeof(double)), static_cast<int>(stage / sizeof(double)));
+        static_cast<int>(scratch / sizeof(double)), static_cast<int>(stage / sizeof(double)),
+        rec_steps, rec_x0);
     return cudaGetLastError();
 }
 

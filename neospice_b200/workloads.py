@@ -253,3 +253,27 @@ def power_grid(rng: np.random.Generator, side: int, pad_pitch: int, n_loads: int
         dev.append(("IPWL", int(node), GND, 0.0, 0.0, float(t0), 0.0, float(t0 + t_rise),
                     float(a)))
     return Netlist(n, dev)
+
+
+def rc_tree_driven(rng: np.random.Generator, nodes: int, r_ohm=50.0, c_farad=2e-15, sigma=0.2,
+                   vdd=1.8, w_n=20e-6, w_p=40e-6, l=1e-6,
+                   pulse=(0.0, 1.8, 1e-11, 5e-11, 5e-11, 1e-9, 2e-9)) -> Netlist:
+    """A random RC interconnect tree (as rc_tree: node k >= 1 hangs from a
+    uniformly drawn earlier node by a lognormal resistor, a lognormal
+    capacitor from every node to ground) driven at node 0 by a level-1 CMOS
+    inverter (NMOS VTO=0.7 KP=110u W=w_n, PMOS VTO=-0.7 KP=50u W=w_p, L=l)
+    whose gate (node nodes) carries a PULSE; VDD on node nodes+1.  The last
+    tree node is the far end."""
+    models = {"nch": ("nmos", {"VTO": 0.7, "KP": 110e-6}),
+              "pch": ("pmos", {"VTO": -0.7, "KP": 50e-6})}
+    gate, vddn = nodes, nodes + 1
+    dev = [("V", vddn, GND, vdd), ("VPULSE", gate, GND, *pulse),
+           ("M", 0, gate, GND, GND, "nch", w_n, l), ("M", 0, gate, vddn, vddn, "pch", w_p, l)]
+    r = r_ohm * np.exp(sigma * rng.standard_normal(nodes))
+    cc = c_farad * np.exp(sigma * rng.standard_normal(nodes))
+    parent = [0] + [int(rng.integers(0, k)) for k in range(1, nodes)]
+    for k in range(1, nodes):
+        dev.append(("R", parent[k], k, float(r[k])))
+    for k in range(nodes):
+        dev.append(("C", k, GND, float(cc[k])))
+    return Netlist(nodes + 2, dev, models)

@@ -1,0 +1,110 @@
+"""GPU transient adjoint: gradients of a squared-error loss on the far-end
+voltage of an RC tree driven by a level-1 CMOS inverter, with respect to
+every R and C and the drivers' W, L and VTO, against central finite
+differences (h = 1e-6 relative) of the same discrete transient (the recorded
+timepoints and integration formulas, Newton to reltol 1e-9) to 1e-6
+relative, wherever the difference quotient resolves the gradient: the loss
+itself carries a rounding floor of about 5e-12 L (LU rounding of the
+perturbed solves), so the quotient's error floor 5e-12 L / (2 h) is allowed
+on top; checkpoint spacing does not change the result."""
+import numpy as np
+import pytest
+import torch
+
+from neospice_b200 import _lib as L
+from neospice_b200 import workloads as W
+from neospice_b200.circuit import TranBatch
+
+pytestmark = pytest.mark.gpu
+TIGHT = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15, max_iter=200)
+
+
+def setup(nodes, seed, tstep=1e-12, tstop=3e-10, count=1):
+    nls = [W.rc_tree_driven(np.random.default_rng([seed, k]), nodes) for k in range(count)]
+    far = nodes - 1
+    b = TranBatch([nl.build() for nl in nls], tstep, tstop, np.array([far], np.int32),
+                  max_points=20000)
+    b.record(True)
+    b.run()
+    res = b.results()
+    assert all(r["status"] == 0 for r in res)
+    # a synthetic target: the recorded far-end waveform, scaled and shifted
+    tg = np.zeros(count * b.max_points)
+    for i, r in enumerate(res):
+        v = r["values"][:, 0]
+        tg[i * b.max_points:i * b.max_points + len(v)] = 0.97 * v + 0.01
+    b.set_adjoint_options(**TIGHT)
+    return nls, b, torch.from_numpy(tg).cuda(), [far] * count
+
+
+def loss_at(b, probes, targets, p_dc, p_tr):
+    _, loss, st = b.adjoint(probes, targets, 1.0, 16, p_dc, p_tr)
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0
+    return loss.cpu().numpy()
+
+
+def test_tran_adjoint_matches_central_differences():
+    nls, b, tg, probes = setup(24, 81)
+    off, pdc, ptr = b.params()
+    g, loss, st = b.adjoint(probes, tg, 1.0, 16)
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0 and float(loss[0]) > 0
+    g = g.cpu().numpy()
+    nl = nls[0]
+    starts, at = [], 0
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 2, "M": 43}
+    for d in nl.devices:
+        starts.append((d[0], at))
+        at += sizes[d[0]]
+    idx = [s for k, s in starts if k == "R"][:8] + [s for k, s in starts if k == "C"][:8]
+    for k, s in starts:
+        if k == "M":
+            idx += [s + 0, s + 1, s + 2]  # W, L, VTO
+    worst = 0.0
+    for i in idx:
+        h = abs(pdc[i]) * 1e-6
+        lo_dc, hi_dc, lo_tr, hi_tr = pdc.copy(), pdc.copy(), ptr.copy(), ptr.copy()
+        hi_dc[i] += h
+        hi_tr[i] += h
+        lo_dc[i] -= h
+        lo_tr[i] -= h
+        dev = lambda a: torch.from_numpy(a).cuda()
+        lp = loss_at(b, probes, tg, dev(hi_dc), dev(hi_tr))[0]
+        lm = loss_at(b, probes, tg, dev(lo_dc), dev(lo_tr))[0]
+        fd = (lp - lm) / (2 * h)
+        floor = 5e-12 * float(loss[0]) / (2 * h)
+        assert abs(g[i] - fd) <= 1e-6 * abs(fd) + floor, (i, g[i], fd, floor)
+        if floor < 1e-8 * abs(fd):  # well resolved: the adjoint to 1e-6
+            worst = max(worst, abs(g[i] - fd) / abs(fd))
+    assert worst < 1e-6
+
+
+def test_tran_adjoint_checkpoint_spacing_and_batching():
+    """The same gradients with checkpoints every 1, 7 and 64 steps, and for a
+    circuit alone or inside a batch."""
+    nls, b, tg, probes = setup(16, 82, count=3)
+    outs = []
+    for every in (1, 7, 64):
+        g, loss, st = b.adjoint(probes, tg, 1.0, every)
+        torch.cuda.synchronize()
+        assert int(st.abs().sum()) == 0
+        outs.append((g.cpu().numpy(), loss.cpu().numpy()))
+    for g, l in outs[1:]:
+        np.testing.assert_allclose(g, outs[0][0], rtol=1e-12, atol=1e-30)
+        np.testing.assert_array_equal(l, outs[0][1])
+
+
+def test_tran_adjoint_requires_recording_and_rejects_mos_charge():
+    nl = W.rc_tree_driven(np.random.default_rng(3), 6)
+    b = TranBatch([nl.build()], 1e-12, 1e-10, np.array([5], np.int32), max_points=5000)
+    b.run()
+    tg = torch.zeros(5000, dtype=torch.float64, device="cuda")
+    with pytest.raises(L.NsgError):
+        b.adjoint([5], tg)
+    nl.models["nch"][1]["TOX"] = 2e-8  # Meyer gate capacitance: not covered
+    b2 = TranBatch([nl.build()], 1e-12, 1e-10, np.array([5], np.int32), max_points=5000)
+    b2.record(True)
+    b2.run()
+    with pytest.raises(L.NsgError):
+        b2.adjoint([5], tg)
