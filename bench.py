@@ -50,6 +50,10 @@ def _args():
                     help="instances in the CPU-baseline sample (0 = skip)")
     ap.add_argument("--no-inverter", action="store_true",
                     help="skip the plain-vs-batched transient measurement")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the batched transient-adjoint section")
+    ap.add_argument("--adjoint-batch", type=int, default=256,
+                    help="instances of the transient-adjoint section")
     ap.add_argument("--no-power-grid", action="store_true",
                     help="skip the single large power-grid refactor/solve section")
     ap.add_argument("--grid-side", type=int, default=300,
@@ -310,6 +314,11 @@ def run_ours(a, rank, world, local_rank):
                 line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch)
             except Exception as exc:
                 line["plain_vs_batched"] = {"error": str(exc)}
+        if not a.no_adjoint and world == 1:
+            try:
+                line["adjoint"] = adjoint_rc_tree(a.adjoint_batch)
+            except Exception as exc:
+                line["adjoint"] = {"error": str(exc)}
         if not a.no_power_grid and world == 1:
             try:
                 line["power_grid"] = power_grid_refactor(a.grid_side, a.steps, a.warmup)
@@ -388,6 +397,61 @@ def inverter_plain_vs_batched(batch_count):
     except Exception as exc:  # the parity check is informative only
         out["parity"] = {"error": str(exc)}
     return out
+
+
+# --- batched transient adjoint (RC trees driven by CMOS inverters) -------------------
+
+def adjoint_rc_tree(count, nodes=500, every=32):
+    """Gradients of sum_n (v_far(t_n) - target(t_n))^2 over .tran 1p 2n of
+    `count` seeded 500-node RC trees (R lognormal around 50 Ohm, C around
+    2 fF, sigma 0.2) each driven by a level-1 CMOS inverter, with respect to
+    every R and C and the drivers' W, L and VTO: the recorded forward run,
+    then the discrete adjoint with a checkpoint every `every` steps.  Both
+    timed with CUDA events; grads/s counts full gradient vectors."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.circuit import TranBatch
+
+    nls = [W.rc_tree_driven(np.random.default_rng([90, i]), nodes) for i in range(count)]
+    far = nodes - 1
+    max_points = 4096
+    b = TranBatch([nl.build() for nl in nls], 1e-12, 2e-9, np.full(1, far, np.int32),
+                  max_points=max_points)
+    b.record(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    b.run()
+    ev[1].record()
+    torch.cuda.synchronize()
+    res = b.results()
+    # seeded synthetic targets: an exponential fall with a per-instance time constant
+    rng = np.random.default_rng(91)
+    tg = np.zeros(count * max_points)
+    for i, r in enumerate(res):
+        tau = 2e-10 * np.exp(0.2 * rng.standard_normal())
+        tg[i * max_points:i * max_points + len(r["time"])] = 1.8 * np.exp(-r["time"] / tau)
+    d_tg = torch.from_numpy(tg).cuda()
+    ev[1].record()
+    g, loss, st = b.adjoint(np.full(count, far), d_tg, 1.0, every)
+    ev[2].record()
+    torch.cuda.synchronize()
+    t_fwd = ev[0].elapsed_time(ev[1]) / 1e3
+    t_adj = ev[1].elapsed_time(ev[2]) / 1e3
+    ok = int((st.cpu().numpy() == 0).sum())
+    n_params = sum(1 for d in nls[0].devices if d[0] in ("R", "C")) + 6
+    steps = [len(r["time"]) - 1 for r in res]
+    return {
+        "workload": f"transient adjoint, {count} x {nodes}-node RC tree driven by a MOS1 inverter, "
+                    f".tran 1p 2n, loss = sum (v_far - target)^2, grads w.r.t. every R, C and the "
+                    f"drivers' W/L/VTO ({n_params} per instance), checkpoint every {every} steps",
+        "grads_per_s": round(count / (t_fwd + t_adj), 3), "unit": "gradients/s",
+        "forward_s": round(t_fwd, 4), "adjoint_s": round(t_adj, 4), "ok": ok,
+        "steps_mean": float(np.mean(steps)),
+        "newton_iters_mean": float(np.mean([r["newton_iters"] for r in res])),
+        "loss_mean": float(loss.mean()),
+    }
 
 
 # --- one large topology: power-grid refactor and solve ------------------------------
