@@ -3,6 +3,10 @@
 // NeoSolver (src/core/neo_solver.cpp:184-297), on top of the C ABI in
 // nsgpu.h.  One instance per object: this is the plain, one-instance-per-launch
 // GPU path; batches of instances use nsg_batch_* / nsg_dc_batch_* directly.
+// The engine is NeoSolver's Markowitz ordering by default; NSG_SOLVER_AMDLU
+// or NSG_SOLVER_AUTO_AMDLU give AmdLuSolver / make_solver's AutoFallbackSolver
+// (src/core/amd_lu_solver.cpp, make_solver.cpp:71-145) -- pick it with
+// nsg_solver_select(num_vars, is_linear) as make_solver does.
 //
 //   symbolic(n, col_ptr, row_idx)   NeoSolver::symbolic (pattern in CSC)
 //   numeric(values, diag_gmin)      NeoSolver::numeric: first call orders on the
@@ -30,12 +34,17 @@ namespace nsgpu {
 
 class GpuSolver {
 public:
-    GpuSolver() = default;
+    explicit GpuSolver(int engine = NSG_SOLVER_MARKOWITZ) : engine_(engine) {}
     GpuSolver(const GpuSolver&) = delete;
     GpuSolver& operator=(const GpuSolver&) = delete;
     ~GpuSolver() { release(); }
 
-    const char* name() const { return "gpu-markowitz"; }
+    // ISolver::name: the engine the factorization runs (an auto engine
+    // reports the one it settled on after its first numeric()).
+    const char* name() const {
+        const int k = topo_ ? nsg_topology_solver(topo_) : engine_;
+        return k == NSG_SOLVER_MARKOWITZ ? "gpu-markowitz" : "gpu-amdlu";
+    }
 
     void symbolic(int n, const std::vector<int>& col_ptr, const std::vector<int>& row_idx) {
         if (n <= 0 || static_cast<int>(col_ptr.size()) != n + 1 ||
@@ -56,8 +65,8 @@ public:
         numeric_called_ = true;
         if (!topo_) {
             nsg_topology* t = nullptr;
-            const int rc = nsg_topology_order(n_, nnz(), col_ptr_.data(), row_idx_.data(),
-                                              values.data(), diag_gmin, &t);
+            const int rc = nsg_topology_order_solver(n_, nnz(), col_ptr_.data(), row_idx_.data(),
+                                                     values.data(), diag_gmin, engine_, &t);
             if (rc == NSG_SINGULAR) return true;
             check(rc, "numeric");
             topo_ = t;
@@ -87,7 +96,21 @@ public:
         if (!topo_) return true;  // the first numeric() found the matrix singular
         check_values(values);
         upload(values);
-        const int st = gpu_refactor(diag_gmin, 0);
+        int st = gpu_refactor(diag_gmin, 0);
+        if (st == NSG_REORDER) {
+            // AMD-LU: the replay's growth test failed and factor_ would pick
+            // other pivots -- AmdLuSolver::refactorize falls back to a full
+            // factor_ (amd_lu_solver.cpp:280-301), done here on the host.
+            int step = 0;
+            const int rc = nsg_topology_numeric(topo_, values.data(), diag_gmin, &step);
+            if (rc == NSG_SINGULAR) {
+                factored_ = false;
+                return true;
+            }
+            check(rc, "refactorize");
+            rebuild_batch();
+            st = gpu_refactor(diag_gmin, 0);
+        }
         factored_ = (st == NSG_OK);
         return !factored_;
     }
@@ -96,6 +119,7 @@ public:
     void solve_transposed(std::vector<double>& rhs) { sweep(rhs, true); }
 
 private:
+    int engine_ = NSG_SOLVER_MARKOWITZ;
     int n_ = 0;
     bool symbolized_ = false;
     bool numeric_called_ = false;  // NeoSolver's factored_ flag

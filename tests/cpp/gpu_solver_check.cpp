@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 static int failures = 0;
@@ -82,6 +83,51 @@ int main() {
         try { s.solve(b); } catch (const std::invalid_argument&) { threw = true; }
         expect(threw, "rhs size mismatch throws invalid_argument");
         expect(s.refactorize({0.0, 0.0, 0.0, 1.0}), "zero pivot refactorize reports singular");
+    }
+    {   // AMD-LU engine: the reference's AmdLuSolver unit cases
+        // (tests/unit/test_amd_lu.cpp): a row pivot on a zero diagonal, and a
+        // refactorize whose reused pivot fails the growth test.
+        cp = {0, 1, 3};
+        ri = {1, 0, 1};  // [0 1; 1 1]
+        nsgpu::GpuSolver s(NSG_SOLVER_AMDLU);
+        s.symbolic(2, cp, ri);
+        expect(!s.numeric({1.0, 1.0, 1.0}), "amdlu 2x2 zero-diagonal numeric");
+        std::vector<double> b = {1.0, 2.0};
+        s.solve(b);
+        expect(std::fabs(b[0] - 1.0) < 1e-12 && std::fabs(b[1] - 1.0) < 1e-12, "amdlu 2x2 solve");
+        expect(std::string(s.name()) == "gpu-amdlu", "amdlu name");
+        dense_pattern(3, cp, ri);
+        const double a0[3][3] = {{10, 1, 2}, {1, 12, 3}, {2, 1, 15}};
+        const double a1[3][3] = {{1e-12, 1, 2}, {1, 12, 3}, {2, 1, 15}};
+        std::vector<double> v0, v1;
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                v0.push_back(a0[i][j]);
+                v1.push_back(a1[i][j]);
+            }
+        nsgpu::GpuSolver t(NSG_SOLVER_AMDLU);
+        t.symbolic(3, cp, ri);
+        expect(!t.numeric(v0), "amdlu 3x3 numeric");
+        expect(!t.refactorize(v1), "amdlu 3x3 refactorize with growth fallback");
+        const double xt[3] = {2.0, -1.0, 0.5};
+        b.assign(3, 0.0);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) b[i] += a1[i][j] * xt[j];
+        t.solve(b);
+        double err = 0;
+        for (int i = 0; i < 3; ++i) err = std::fmax(err, std::fabs(b[i] - xt[i]));
+        expect(err < 1e-7, "amdlu 3x3 solve after fallback");
+        // structurally singular: the auto engine falls back to Markowitz,
+        // which reports singular as well
+        cp = {0, 2, 2};
+        ri = {0, 1};
+        nsgpu::GpuSolver u(NSG_SOLVER_AUTO_AMDLU);
+        u.symbolic(2, cp, ri);
+        expect(u.numeric({1.0, 1.0}), "auto engine structurally singular numeric");
+        expect(nsg_solver_select(300, 1) == NSG_SOLVER_AUTO_AMDLU &&
+                   nsg_solver_select(300, 0) == NSG_SOLVER_MARKOWITZ &&
+                   nsg_solver_select(255, 1) == NSG_SOLVER_MARKOWITZ,
+               "make_solver policy");
     }
     std::printf("%d failure(s)\n", failures);
     return failures == 0 ? 0 : 1;
