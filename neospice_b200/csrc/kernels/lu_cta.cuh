@@ -636,6 +636,9 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
     __syncthreads();
 }
 
+// Entries of a row the dataflow sweeps fetch ahead of their waits.
+constexpr int kSweepChunk = 8;
+
 // Shared memory of the dataflow solve: the n-vector and n completion flags.
 __host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
     return (sizeof(double) + sizeof(int32_t)) * static_cast<size_t>(n);
@@ -689,13 +692,26 @@ static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int
             const int32_t i = order[k];
             double t = w[i];
             const int32_t e1 = lp[i + 1];
-            for (int32_t e = lp[i]; e < e1; ++e) {
-                const int32_t c = lcol[e];
-                const double lv = lrows[e];
-                if (ok && !wait_flag(done, c)) ok = false;
-                const double xc = w[c];
-                if (amd) t = lu_sub(t, lu_mul(lv, xc));
-                else if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lv));
+            // The row's entries are fetched kSweepChunk at a time ahead of
+            // the waits, so a row pays one memory round trip per chunk, not
+            // one per entry; they are still applied one by one in order.
+            for (int32_t e0 = lp[i]; e0 < e1; e0 += kSweepChunk) {
+                int32_t cs[kSweepChunk];
+                double vs[kSweepChunk];
+#pragma unroll
+                for (int u = 0; u < kSweepChunk; ++u) {
+                    cs[u] = (e0 + u < e1) ? lcol[e0 + u] : 0;
+                    vs[u] = (e0 + u < e1) ? lrows[e0 + u] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kSweepChunk; ++u) {
+                    if (e0 + u >= e1) break;
+                    const int32_t c = cs[u];
+                    if (ok && !wait_flag(done, c)) ok = false;
+                    const double xc = w[c];
+                    if (amd) t = lu_sub(t, lu_mul(vs[u], xc));
+                    else if (xc != 0.0) t = lu_sub(t, lu_mul(xc, vs[u]));
+                }
             }
             if (!amd) t = (t != 0.0) ? lu_mul(t, lu[diag_pos[i]]) : t;
             w[i] = t;
@@ -714,12 +730,23 @@ static __device__ __noinline__ bool cta_solve_flow(const PlanDesc& pd, const int
             const int32_t i = order[k];
             double t = w[i];
             const int32_t e0 = up[i], e1 = up[i + 1];
-            for (int32_t m = 0; m < e1 - e0; ++m) {
-                const int32_t e = amd ? e1 - 1 - m : e0 + m;
-                const int32_t c = ucol[e];
-                const double uv = urows[e];
-                if (ok && !wait_flag(done, c)) ok = false;
-                t = lu_sub(t, lu_mul(uv, w[c]));
+            const int32_t len = e1 - e0;
+            for (int32_t m0 = 0; m0 < len; m0 += kSweepChunk) {
+                int32_t cs[kSweepChunk];
+                double vs[kSweepChunk];
+#pragma unroll
+                for (int u = 0; u < kSweepChunk; ++u) {
+                    const int32_t e = amd ? e1 - 1 - (m0 + u) : e0 + m0 + u;
+                    cs[u] = (m0 + u < len) ? ucol[e] : 0;
+                    vs[u] = (m0 + u < len) ? urows[e] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kSweepChunk; ++u) {
+                    if (m0 + u >= len) break;
+                    const int32_t c = cs[u];
+                    if (ok && !wait_flag(done, c)) ok = false;
+                    t = lu_sub(t, lu_mul(vs[u], w[c]));
+                }
             }
             w[i] = amd ? __ddiv_rn(t, lu[diag_pos[i]]) : t;
             flag_release(done + i, 1);
