@@ -19,6 +19,8 @@ namespace nsg {
 constexpr int kFlowWarps = 16;
 constexpr int kFlowThreads = kFlowWarps * 32;
 constexpr int kSpinLimit = 1 << 22;
+// Rounds of 32 L(:, r) rows the dataflow refactor loads before applying them.
+constexpr int kColChunk = 4;
 
 __device__ __forceinline__ double lu_mul(double x, double y) { return __dmul_rn(x, y); }
 __device__ __forceinline__ double lu_sub(double x, double y) { return __dsub_rn(x, y); }
@@ -271,9 +273,22 @@ __device__ __forceinline__ ColumnResult refactor_column(
         __syncwarp();
         if (lane == 0) buf[q] = u;
         if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
-        for (int32_t t = lane + 32; t < cnt_c; t += 32) {
-            const int32_t d = upd_dst[us_c + t];
-            buf[d] = lu_sub(buf[d], lu_mul(u, lu_peer<kCrossSm>(lu + l0_c + t)));
+        // L(:, r) beyond its first 32 rows: destinations and values are
+        // loaded kColChunk rounds at a time before they are applied (the
+        // destinations of one entry are distinct, so the order among them
+        // does not matter).
+        for (int32_t t0 = 32; t0 < cnt_c; t0 += 32 * kColChunk) {
+            int32_t dd[kColChunk];
+            double ll[kColChunk];
+#pragma unroll
+            for (int k = 0; k < kColChunk; ++k) {
+                const int32_t t = t0 + 32 * k + lane;
+                dd[k] = (t < cnt_c) ? upd_dst[us_c + t] : 0;
+                ll[k] = (t < cnt_c) ? lu_peer<kCrossSm>(lu + l0_c + t) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < kColChunk; ++k)
+                if (t0 + 32 * k + lane < cnt_c) buf[dd[k]] = lu_sub(buf[dd[k]], lu_mul(u, ll[k]));
         }
         __syncwarp();
         have_c = have_n;
