@@ -150,6 +150,16 @@ int nsg_batch_refactor(nsg_batch* batch, const double* d_values, double diag_gmi
  * produce bit-identical values. */
 int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
 
+/* Schedule autotuner: refactor d_values (as a refactorize()) and solve d_x
+ * under each schedule (0 dataflow, 1 level-synchronous, 2 grid-wide), reps
+ * times each, time them with CUDA events and keep the fastest.  times_ms[3]
+ * (optional) receives the mean refactor+solve time per schedule (-1 if it
+ * did not run), *chosen the schedule kept.  d_x is left as given; the
+ * factors are those of the last schedule timed (all schedules give
+ * bit-identical values).  Allocates temporary device memory. */
+int nsg_batch_autotune(nsg_batch* batch, const double* d_values, double* d_x, int reps,
+                       float* times_ms, int* chosen, void* stream);
+
 /* spSolve: d_x holds b on entry and x on return, per instance
  * (SparseMatrix::solve, src/solver/solve.cpp:6-47; NeoSolver::solve). */
 int nsg_batch_solve(nsg_batch* batch, double* d_x, void* stream);
@@ -306,6 +316,17 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
  * nsg_dc_batch_run stays asynchronous and such instances report 103.
  * nsg_dc_batch_reorders: instances re-ordered so far. */
 int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable);
+
+/* Replay each run's launch (controller reset + Newton kernel) from a
+ * captured CUDA graph: the first run after enabling launches normally, the
+ * next captures the launch on an internal stream and later runs with the
+ * same d_params / d_solutions / d_status / d_iterations replay it on the
+ * caller's stream.  A host re-order (new plans, a grown workspace) drops
+ * the graph; it is captured again on a later run.  Results are those of a
+ * plain launch, bit for bit. */
+int nsg_dc_batch_set_graph(nsg_dc_batch* b, int enable);
+/* Runs that replayed a graph so far. */
+int nsg_dc_batch_graph_launches(const nsg_dc_batch* b, long long* count);
 int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);
 /* After a run (synchronises the device): per instance the method that gave
  * the result, as the reference's ConvergenceMethod (0 direct Newton, 1 gmin

@@ -44,6 +44,10 @@ SIGNATURES = {
     "nsg_topology_solver": (c_int, [c_void_p]),
     "nsg_amd_order": (c_int, [c_int, P(c_int), P(c_int), P(c_int)]),
     "nsg_dc_batch_engines": (c_int, [c_void_p, P(c_int)]),
+    "nsg_dc_batch_set_graph": (c_int, [c_void_p, c_int]),
+    "nsg_dc_batch_graph_launches": (c_int, [c_void_p, P(c_ll)]),
+    "nsg_batch_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_int, P(ctypes.c_float),
+                                   P(c_int), c_void_p]),
     "nsg_tran_batch_engines": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "nsg_topology_import": (c_int, [c_int, c_int, P(c_int), P(c_int), c_int, P(c_int), P(c_int),
                                     P(c_int), P(c_void_p)]),

@@ -198,6 +198,16 @@ class DcBatch:
         L.check(L.lib().nsg_dc_batch_reorders(self._h, ctypes.byref(n)))
         return n.value
 
+    def set_graph(self, enable: bool = True):
+        """Replay run()'s launch from a captured CUDA graph (see
+        nsg_dc_batch_set_graph)."""
+        L.check(L.lib().nsg_dc_batch_set_graph(self._h, int(bool(enable))))
+
+    def graph_launches(self) -> int:
+        n = ctypes.c_longlong()
+        L.check(L.lib().nsg_dc_batch_graph_launches(self._h, ctypes.byref(n)))
+        return n.value
+
     def engines(self) -> list:
         """Factorization engine of each instance: "markowitz" or "amdlu"
         (make_solver's choice for the circuit)."""

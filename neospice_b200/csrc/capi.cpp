@@ -527,6 +527,72 @@ int nsg_batch_set_schedule(nsg_batch* b, int schedule) {
     return NSG_OK;
 }
 
+int nsg_batch_autotune(nsg_batch* b, const double* d_values, double* d_x, int reps,
+                       float* times_ms, int* chosen, void* stream) {
+    return guarded("nsg_batch_autotune", [&]() -> int {
+        if (!b || !d_values || !d_x || reps < 1)
+            return fail(NSG_ERR_INVALID, "nsg_batch_autotune: bad arguments");
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        const size_t nx = static_cast<size_t>(b->x_off[b->count]);
+        double* d_b = nullptr;
+        int32_t* d_st = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d_b), sizeof(double) * nx);
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d_st), sizeof(int32_t) * b->count);
+        if (e == cudaSuccess) e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_b, d_x, sizeof(double) * nx, cudaMemcpyDeviceToDevice, st);
+        const int saved = b->schedule;
+        int best = -1;
+        float best_ms = 0.0f;
+        // Refactor (a refactorize(), as the Newton loop's steady state) and
+        // solve of the given system under each schedule, reps times.
+        for (int sched = 0; sched < 3 && e == cudaSuccess; ++sched) {
+            float ms = -1.0f;
+            int rc = nsg_batch_set_schedule(b, sched);
+            auto once = [&]() -> int {
+                int r = nsg_batch_refactor(b, d_values, 0.0, 0, d_st, nullptr, stream);
+                if (r == NSG_OK &&
+                    (e = cudaMemcpyAsync(d_x, d_b, sizeof(double) * nx, cudaMemcpyDeviceToDevice,
+                                         st)) != cudaSuccess)
+                    return NSG_ERR_CUDA;
+                if (r == NSG_OK) r = nsg_batch_solve(b, d_x, stream);
+                return r;
+            };
+            if (rc == NSG_OK) rc = once();  // warm-up (allocates scratch)
+            if (rc == NSG_OK && (e = cudaEventRecord(e0, st)) == cudaSuccess) {
+                for (int k = 0; k < reps && rc == NSG_OK; ++k) rc = once();
+                if (rc == NSG_OK && (e = cudaEventRecord(e1, st)) == cudaSuccess &&
+                    (e = cudaEventSynchronize(e1)) == cudaSuccess &&
+                    (e = cudaEventElapsedTime(&ms, e0, e1)) == cudaSuccess)
+                    ms /= static_cast<float>(reps);
+            }
+            if (rc != NSG_OK || e != cudaSuccess) ms = -1.0f;
+            if (times_ms) times_ms[sched] = ms;
+            if (ms >= 0.0f && (best < 0 || ms < best_ms)) {
+                best = sched;
+                best_ms = ms;
+            }
+        }
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_x, d_b, sizeof(double) * nx, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(d_b);
+        cudaFree(d_st);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (e != cudaSuccess) return cuda_fail("nsg_batch_autotune", e);
+        if (best < 0) {
+            nsg_batch_set_schedule(b, saved);
+            return fail(NSG_ERR_INVALID, "nsg_batch_autotune: no schedule ran");
+        }
+        nsg_batch_set_schedule(b, best);
+        if (chosen) *chosen = best;
+        return NSG_OK;
+    });
+}
+
 int nsg_batch_lu_to_host(const nsg_batch* b, double* out) {
     if (!b || !out) return fail(NSG_ERR_INVALID, "nsg_batch_lu_to_host: null argument");
     cudaError_t e = cudaMemcpy(out, b->d_lu, sizeof(double) * b->lu_off[b->count],

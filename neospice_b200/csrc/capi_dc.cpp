@@ -52,7 +52,20 @@ struct nsg_dc_batch {
     int64_t work_size = 0, work_cap = 0;
     nsg::DcCtl* d_ctl = nullptr;
     int32_t* d_subset = nullptr;
+    // Graph replay of the launch (controller reset + Newton kernel), keyed
+    // by the caller's buffers; dropped whenever plans or workspace move.
+    bool use_graph = false;
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long graph_launches = 0, plain_launches = 0;
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
     ~nsg_dc_batch() {
+        drop_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
         cudaFree(d_lu_pool);
         cudaFree(d_plans);
         cudaFree(d_prog);
@@ -507,6 +520,25 @@ int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable) {
     return NSG_OK;
 }
 
+int nsg_dc_batch_set_graph(nsg_dc_batch* b, int enable) {
+    return guarded("nsg_dc_batch_set_graph", [&]() -> int {
+        if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_graph: null batch");
+        b->use_graph = enable != 0;
+        b->drop_graph();
+        if (b->use_graph && !b->cap_stream) {
+            const cudaError_t e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_set_graph", e);
+        }
+        return NSG_OK;
+    });
+}
+
+int nsg_dc_batch_graph_launches(const nsg_dc_batch* b, long long* count) {
+    if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_dc_batch_graph_launches: null argument");
+    *count = b->graph_launches;
+    return NSG_OK;
+}
+
 int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count) {
     if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_dc_batch_reorders: null argument");
     *count = b->reorders;
@@ -557,12 +589,47 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
             return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: null argument");
         const cudaStream_t st = static_cast<cudaStream_t>(stream);
         const double* params = d_params ? d_params : b->d_params;
-        cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::DcCtl) * b->count, st);
-        if (e == cudaSuccess)
-            e = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, nullptr, b->count,
-                                      b->d_prog, params, b->d_work, d_solutions, d_status,
-                                      d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n,
-                                      max_stage_len(b->descs), st);
+        auto first_launch = [&](cudaStream_t s) -> cudaError_t {
+            cudaError_t r = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::DcCtl) * b->count, s);
+            if (r == cudaSuccess)
+                r = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, nullptr, b->count,
+                                          b->d_prog, params, b->d_work, d_solutions, d_status,
+                                          d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n,
+                                          max_stage_len(b->descs), s);
+            return r;
+        };
+        cudaError_t e = cudaSuccess;
+        const void* key[4] = {params, d_solutions, d_status, d_iterations};
+        if (b->use_graph && b->graph && std::equal(key, key + 4, b->graph_key)) {
+            e = cudaGraphLaunch(b->graph, st);
+            ++b->graph_launches;
+        } else if (b->use_graph && b->plain_launches > 0 && b->cap_stream) {
+            // Capture the launch on the batch's own stream (the caller's may
+            // be the legacy default stream, which cannot be captured), then
+            // replay it on the caller's stream.
+            b->drop_graph();
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                const cudaError_t le = first_launch(b->cap_stream);
+                e = cudaStreamEndCapture(b->cap_stream, &g);
+                if (e == cudaSuccess) e = le;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e == cudaSuccess) {
+                std::copy(key, key + 4, b->graph_key);
+                e = cudaGraphLaunch(b->graph, st);
+                ++b->graph_launches;
+            } else {
+                b->drop_graph();
+            }
+        } else {
+            // plain launch (also the first of a graph-enabled batch, which
+            // configures the kernel before any capture)
+            e = first_launch(st);
+            ++b->plain_launches;
+        }
         if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_run", e);
         if (!b->reorder) return NSG_OK;
         // Instances whose pivots failed re-validation: re-order on the host
@@ -596,6 +663,7 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
                 ++b->reorders;
             }
             if (subset.empty()) break;
+            b->drop_graph();  // plans and workspace move
             int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col, &b->max_n);
             if (rc != NSG_OK) return rc;
             if (nsg::dc_smem_bytes(b->max_col, b->max_n) > 200 * 1024)

@@ -164,6 +164,15 @@ class Batch:
                                            d_fail_step.data_ptr(), _stream_ptr(stream)))
         return d_status, d_fail_step
 
+    def autotune(self, d_values, d_x, reps=3, stream=None):
+        """Time the schedules on this system and keep the fastest:
+        (chosen schedule, [ms per refactor+solve for schedules 0, 1, 2])."""
+        t = (ctypes.c_float * 3)()
+        c = ctypes.c_int(-1)
+        L.check(L.lib().nsg_batch_autotune(self._h, d_values.data_ptr(), d_x.data_ptr(), int(reps),
+                                           t, ctypes.byref(c), _stream_ptr(stream)))
+        return c.value, [float(v) for v in t]
+
     def solve(self, d_x, stream=None):
         L.check(L.lib().nsg_batch_solve(self._h, d_x.data_ptr(), _stream_ptr(stream)))
         return d_x

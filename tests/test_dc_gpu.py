@@ -69,3 +69,22 @@ def test_dc_mixed_sizes_against_reference():
         assert int(status[k]) == 0
         assert int(iters[k]) == ref_it
         _check(s, ref)
+
+
+def test_dc_graph_replay_matches_plain_launch():
+    """Runs replayed from a captured CUDA graph give the plain launch's
+    results bit for bit (same buffers every run)."""
+    plain = DcBatch([g["mesh"].build() for g in MESHES])
+    s0, st0, it0 = plain.run()
+    torch.cuda.synchronize()
+    batch = DcBatch([g["mesh"].build() for g in MESHES])
+    batch.set_graph(True)
+    sol = torch.empty_like(s0)
+    st = torch.empty_like(st0)
+    it = torch.empty_like(it0)
+    for _ in range(3):
+        sol.zero_()
+        batch.run(d_solutions=sol, d_status=st, d_iterations=it)
+        torch.cuda.synchronize()
+        assert torch.equal(sol, s0) and torch.equal(st, st0) and torch.equal(it, it0)
+    assert batch.graph_launches() == 2

@@ -136,3 +136,26 @@ def test_pivot_revalidation_flags_match_port(schedule):
             flagged += 1
             assert res["step"][k] == step
     assert flagged > 0
+
+
+def test_autotune_picks_a_schedule_and_keeps_results():
+    rng = np.random.default_rng(21)
+    mats = [mna_mesh(rng, s, 1 + s % 2) for s in (6, 11, 20)] * 2
+    topos = [Topology.order(n, cp, ri, v) for (n, cp, ri, v) in mats]
+    vals = [v for (_, _, _, v) in mats]
+    bs = [rng.standard_normal(n) for (n, _, _, _) in mats]
+    ref = _run(topos, vals, bs, schedule=0)
+    batch = Batch(topos)
+    d_a = _pack(batch, vals, batch.value_offsets)
+    d_x = _pack(batch, bs, batch.vector_offsets)
+    chosen, times = batch.autotune(d_a, d_x, reps=2)
+    assert chosen in (0, 1, 2) and times[chosen] >= 0 and times[chosen] == min(t for t in times if t >= 0)
+    # d_x left as given; the chosen schedule reproduces the values
+    np.testing.assert_array_equal(d_x.cpu().numpy(), _pack(batch, bs, batch.vector_offsets).cpu().numpy())
+    st, _ = batch.refactor(d_a)
+    batch.solve(d_x)
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0
+    xs = _unpack(d_x, batch.vector_offsets, [t.info()["n"] for t in topos])
+    for x, x0 in zip(xs, ref["x"]):
+        np.testing.assert_array_equal(x, x0)
