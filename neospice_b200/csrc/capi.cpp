@@ -168,6 +168,10 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.nnz_u = p.urow_ptr[p.n];
     d.kind = p.kind;
     p.append_to(pool, d.off);
+    d.words = p.device_words();
+    // the span [off[0], off[0] + words) may run past the last array by the
+    // alignment slack: keep it inside the pool
+    pool.insert(pool.end(), 4 * nsg::PA_COUNT, 0);
     return d;
 }
 

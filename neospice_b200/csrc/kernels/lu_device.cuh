@@ -21,6 +21,7 @@ struct PlanDesc {
     int32_t nnz_l, nnz_u;  // strictly lower / upper entries
     int32_t kind;          // kPlanMarkowitz or kPlanAmdLu
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
+    int64_t words;          // words from off[0] that hold all of the plan's arrays
 };
 
 struct InstDesc {

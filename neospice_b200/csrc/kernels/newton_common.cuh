@@ -262,6 +262,31 @@ __device__ inline void assemble(const Inst& v) {
     }
 }
 
+// Shared memory reserved for a staged plan (stage_plan) by the kernels that
+// run many Newton iterations per launch on small instances.
+constexpr size_t kPlanStageBytes = 16 * 1024;
+
+// Copy a plan's index arrays into shared memory (whole CTA) when the
+// instance takes the shared-memory LU path (n <= 128) and the arrays fit
+// cap_words: the refactor and the sweeps read them every Newton iteration,
+// thousands of times per launch in a transient.  Returns the pool to read
+// the plan from; *out (shared) receives the plan descriptor rebased on it.
+// Begins and ends with __syncthreads().
+__device__ inline const int32_t* stage_plan(const PlanDesc& pd, const int32_t* pool, int32_t* sm,
+                                            int64_t cap_words, PlanDesc* out) {
+    const bool fit = sm && pd.n <= 128 && pd.words > 0 && pd.words <= cap_words;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *out = pd;
+        if (fit)
+            for (int k = 0; k < PA_COUNT; ++k) out->off[k] -= pd.off[0];
+    }
+    if (fit)
+        for (int64_t i = threadIdx.x; i < pd.words; i += blockDim.x) sm[i] = pool[pd.off[0] + i];
+    __syncthreads();
+    return fit ? sm : pool;
+}
+
 struct NewtonOutcome {
     int32_t code;       // kDcConverged, kDcNoConvergence, kStatus*
     int32_t iters;

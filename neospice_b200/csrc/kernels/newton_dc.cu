@@ -23,10 +23,15 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  double* __restrict__ work, double* __restrict__ solutions,
                  int32_t* __restrict__ status, int32_t* __restrict__ iterations,
                  DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf, int scratch_doubles,
-                 int stage_doubles) {
+                 int stage_doubles, int plan_words) {
     extern __shared__ double smem[];
     const DcDesc d = descs[subset ? subset[blockIdx.x] : blockIdx.x];
-    const PlanDesc& pd = plans[d.plan];
+    __shared__ PlanDesc s_pd;
+    const int32_t* pool = stage_plan(
+        plans[d.plan], lu_pool,
+        plan_words > 0 ? reinterpret_cast<int32_t*>(smem + scratch_doubles + stage_doubles) : nullptr,
+        plan_words, &s_pd);
+    const PlanDesc& pd = s_pd;
     double* stage = (d.stage_len <= stage_doubles) ? smem + scratch_doubles : nullptr;
     stage_copy(d, work, stage, true);
     const Inst v = make_inst(d, prog, params, work, stage);
@@ -54,7 +59,7 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     }
     __syncthreads();
     // solve_dc (dc.cpp:53-175): direct attempt, true gmin stepping, gmin stepping
-    const int32_t code = dc_operating_point(v, d.n_states, pd, lu_pool, &ctx, &solver, ctl, opt,
+    const int32_t code = dc_operating_point(v, d.n_states, pd, pool, &ctx, &solver, ctl, opt,
                                             kFirst, kCont, true, work + d.dcsave_off, smem, colbuf,
                                             scratch_doubles);
 
@@ -83,8 +88,9 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
     const size_t scratch = (dc_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
-    const size_t stage = stage_bytes_for(scratch, max_stage);
-    const size_t smem = scratch + stage;
+    const size_t plan = (max_n <= 128) ? kPlanStageBytes : 0;
+    const size_t stage = stage_bytes_for(scratch + plan, max_stage);
+    const size_t smem = scratch + stage + plan;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
@@ -98,7 +104,8 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                                                              params, work, solutions, status,
                                                              iterations, ctls, opt, colbuf,
                                                              static_cast<int>(scratch / sizeof(double)),
-                                                             static_cast<int>(stage / sizeof(double)));
+                                                             static_cast<int>(stage / sizeof(double)),
+                                                             static_cast<int>(plan / sizeof(int32_t)));
     return cudaGetLastError();
 }
 

@@ -184,7 +184,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  int32_t* __restrict__ status, int32_t* __restrict__ stats,
                  TranCtl* __restrict__ ctls, TranOptions o, int colbuf, int scratch_doubles,
                  int stage_doubles, StepRecord* __restrict__ rec_steps,
-                 double* __restrict__ rec_x0) {
+                 double* __restrict__ rec_x0, int plan_words) {
     extern __shared__ double smem[];
     const int pos = subset ? subset[blockIdx.x] : blockIdx.x;
     const DcDesc d = descs[pos];
@@ -225,9 +225,16 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         for (int q = 0; q < 4; ++q) v.st[q] = base + static_cast<int64_t>(k.stperm[q]) * d.n_states;
     }
 
+    // Small instances read their plan from shared memory (the DC plan now,
+    // the transient plan for the timestep loop).
+    int32_t* plan_sm =
+        plan_words > 0 ? reinterpret_cast<int32_t*>(smem + scratch_doubles + stage_doubles) : nullptr;
+    __shared__ PlanDesc s_pd;
+
     // ---- 1. DC operating point (compute_dc_operating_point, transient.cpp:145-205)
     if (k.phase == kTrDc) {
-        const int32_t code = dc_operating_point(v, d.n_states, plans[d.plan], lu_pool, &k.ctx,
+        const int32_t* dpool = stage_plan(plans[d.plan], lu_pool, plan_sm, plan_words, &s_pd);
+        const int32_t code = dc_operating_point(v, d.n_states, s_pd, dpool, &k.ctx,
                                                 &k.dc_solver, &k.dc, o.nopt, kFirst, kCont, false,
                                                 work + d.dcsave_off, smem, colbuf, scratch_doubles);
         if (code == kStatusReorder) {
@@ -275,7 +282,9 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
 
     // ---- 3. the adaptive timestep loop (transient.cpp:873-1052)
     const bool host_first = td.tran_plan < 0;
-    const PlanDesc& tpd = plans[host_first ? d.plan : td.tran_plan];
+    const int32_t* tpool =
+        stage_plan(plans[host_first ? d.plan : td.tran_plan], lu_pool, plan_sm, plan_words, &s_pd);
+    const PlanDesc& tpd = s_pd;
     for (;;) {
         __syncthreads();
         if (k.phase == kTrPrepare) {
@@ -290,7 +299,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         __syncthreads();
         if (threadIdx.x == 0 && resume) k.ctx.mode = k.nr_mode;
         __syncthreads();
-        const NewtonOutcome r = newton(v, tpd, lu_pool, &k.ctx, o.nopt, o.itl4, &k.tr_solver, smem,
+        const NewtonOutcome r = newton(v, tpd, tpool, &k.ctx, o.nopt, o.itl4, &k.tr_solver, smem,
                                        colbuf, resume ? nr_iter : -1, step_mode,
                                        resume ? nr_devconv : 1, host_first, scratch_doubles);
         if (r.code == kStatusReorder || r.code == kStatusNeedOrder) {
@@ -487,8 +496,9 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
     const size_t scratch = (tran_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
-    const size_t stage = stage_bytes_for(scratch, max_stage);
-    const size_t smem = scratch + stage;
+    const size_t plan = (max_n <= 128) ? kPlanStageBytes : 0;
+    const size_t stage = stage_bytes_for(scratch + plan, max_stage);
+    const size_t smem = scratch + stage + plan;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
     static bool configured = false;
     if (!configured) {
@@ -502,7 +512,7 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
         plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes,
         times, values, npoints, status, stats, ctls, o, colbuf,
         static_cast<int>(scratch / sizeof(double)), static_cast<int>(stage / sizeof(double)),
-        rec_steps, rec_x0);
+        rec_steps, rec_x0, static_cast<int>(plan / sizeof(int32_t)));
     return cudaGetLastError();
 }
 
