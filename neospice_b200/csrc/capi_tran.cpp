@@ -313,31 +313,66 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                 (e = cudaMemcpy(status.data(), b->d_status, sizeof(int) * b->count,
                                 cudaMemcpyDeviceToHost)) != cudaSuccess)
                 return cuda_fail("nsg_tran_batch_run", e);
-            std::vector<int32_t> subset;
-            for (int i = 0; i < b->count; ++i) {
-                if (status[i] != NSG_REORDER && status[i] != 105) continue;
-                nsg::DcDesc& d = b->descs[i];
-                nsg::TranDesc& t = b->tdescs[i];
-                nsg::TranCtl ctl;
-                std::vector<double> a(d.nnz);
-                if ((e = cudaMemcpy(&ctl, b->d_ctl + i, sizeof ctl, cudaMemcpyDeviceToHost)) !=
-                        cudaSuccess ||
-                    (e = cudaMemcpy(a.data(), b->d_work + d.a_off, sizeof(double) * d.nnz,
+            std::vector<int32_t> subset, todo;
+            for (int i = 0; i < b->count; ++i)
+                if (status[i] == NSG_REORDER || status[i] == 105) todo.push_back(i);
+            // The matrices the stopped instances assembled, and their requests.
+            const int nt = static_cast<int>(todo.size());
+            std::vector<nsg::TranCtl> ctls(nt);
+            std::vector<std::vector<double>> mats(nt);
+            for (int k = 0; k < nt; ++k) {
+                const int i = todo[k];
+                const nsg::DcDesc& d = b->descs[i];
+                mats[k].resize(d.nnz);
+                if ((e = cudaMemcpy(&ctls[k], b->d_ctl + i, sizeof(nsg::TranCtl),
+                                    cudaMemcpyDeviceToHost)) != cudaSuccess ||
+                    (e = cudaMemcpy(mats[k].data(), b->d_work + d.a_off, sizeof(double) * d.nnz,
                                     cudaMemcpyDeviceToHost)) != cudaSuccess)
                     return cuda_fail("nsg_tran_batch_run", e);
-                int topo = -1, rc;
-                if (ctl.need == 105) {
-                    std::unique_ptr<nsg_topology> fresh;
-                    rc = order_topology(d.n, d.nnz, b->col_ptr[i].data(), b->row_idx[i].data(),
-                                        a.data(), ctl.need_diag_gmin, fresh, b->solver[i]);
-                    if (rc == NSG_OK) topo = intern_topology(b->topos, std::move(fresh));
-                } else {
-                    const int cur = ctl.need_plan == 0 ? d.plan : t.tran_plan;
-                    rc = reorder_instance(b->topos, cur, a.data(), ctl.need_diag_gmin, &topo);
+            }
+            // Order them on the host threads (instances are independent: a
+            // first ordering of a fresh topology, or NeoSolver::numeric on a
+            // copy of the current one), then share and place the results.
+            std::vector<std::unique_ptr<nsg_topology>> made(nt);
+            std::vector<int> rcs(nt, NSG_OK);
+            std::atomic<int> next_item{0};
+            auto worker = [&]() {
+                for (int k; (k = next_item.fetch_add(1)) < nt;) {
+                    const int i = todo[k];
+                    const nsg::DcDesc& d = b->descs[i];
+                    const nsg::TranCtl& ctl = ctls[k];
+                    try {
+                        if (ctl.need == 105) {
+                            rcs[k] = order_topology(d.n, d.nnz, b->col_ptr[i].data(),
+                                                    b->row_idx[i].data(), mats[k].data(),
+                                                    ctl.need_diag_gmin, made[k], b->solver[i]);
+                        } else {
+                            const int cur = ctl.need_plan == 0 ? d.plan : b->tdescs[i].tran_plan;
+                            made[k] = clone_topology(*b->topos[cur]);
+                            rcs[k] = numeric_on_engine(*made[k], mats[k].data(), ctl.need_diag_gmin);
+                            if (rcs[k] == NSG_OK) rebuild_plan(*made[k]);
+                        }
+                    } catch (const std::exception&) {
+                        rcs[k] = NSG_ERR_INVALID;
+                    }
                 }
-                if (rc != NSG_OK) continue;  // keeps its status: the host could not order it
-                if (ctl.need_plan == 0) d.plan = topo;
-                else t.tran_plan = topo;
+            };
+            const int nthreads = std::max(1, std::min<int>(nt, static_cast<int>(std::max(
+                                                                 1u, std::thread::hardware_concurrency()))));
+            if (nthreads <= 1) {
+                worker();
+            } else {
+                std::vector<std::thread> pool;
+                for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker);
+                for (auto& th : pool) th.join();
+            }
+            for (int k = 0; k < nt; ++k) {
+                if (rcs[k] != NSG_OK || !made[k]) continue;  // keeps its status: not ordered
+                const int i = todo[k];
+                nsg::DcDesc& d = b->descs[i];
+                const int topo = intern_topology(b->topos, std::move(made[k]));
+                if (ctls[k].need_plan == 0) d.plan = topo;
+                else b->tdescs[i].tran_plan = topo;
                 place_lu_workspace(d, b->topos[topo]->plan, b->work_size);
                 subset.push_back(i);
                 ++b->orderings;
