@@ -205,7 +205,8 @@ int nsg_batch_lu_to_host(const nsg_batch* batch, double* out);
  * ngspice load order, branch unknowns after the nodes, sparsity pattern,
  * dead-node placeholders.  Parameters are kept in creation order: resistor
  * {ohms}, capacitor {farads, ic}, DC source {value}, PULSE source {v1, v2,
- * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode {IS, N}. */
+ * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode: the 10
+ * values of nsg_diode_param_block. */
 typedef struct nsg_circuit nsg_circuit;
 
 #define NSG_WAVE_DC 0
@@ -223,6 +224,20 @@ int nsg_circuit_add_isource(nsg_circuit* c, int p, int n, double amps);
 /* Circuit::D with a level-1 model card D(IS=is N=n) (src/core/circuit.hpp:210;
  * series resistance 0, T = TNOM). */
 int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, double n_emission);
+/* Circuit::D with the card D(IS N CJO VJ M FC TT) (junction capacitance and
+ * transit time; series resistance 0, no sidewall, T = TNOM).  Requires
+ * IS > 0, N > 0, CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0.  The
+ * reference's defaults (src/devices/dio/dio_setup.cpp:55-82) are CJO 0,
+ * VJ 1, M 0.5, FC 0.5, TT 0. */
+int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is,
+                               double n_emission, double cjo, double vj, double m, double fc,
+                               double tt);
+/* The diode parameter block of that card (10 doubles into out): IS, N, then
+ * DIOtemp's junction capacitance, junction potential, depletion knee FC*VJ,
+ * F1, F2, F3, grading coefficient and transit time at T = TNOM
+ * (src/devices/dio/dio_temp.cpp:91-292). */
+int nsg_diode_param_block(double is, double n_emission, double cjo, double vj, double m,
+                          double fc, double tt, double* out);
 /* Circuit::C (src/core/circuit.hpp:180) with an optional IC= value
  * (has_ic != 0). */
 int nsg_circuit_add_capacitor(nsg_circuit* c, int a, int b, double farads, int has_ic,
@@ -361,7 +376,8 @@ int nsg_dc_batch_adjoint(nsg_dc_batch* b, const double* d_params, const double* 
  * integration and the truncation-error estimate of every charge state.  The
  * DC solver and the transient solver are ordered separately on their own
  * first matrices, as the reference creates two solvers.  Circuits may hold
- * R, C, DC/PULSE/PWL V and I sources and level-1 MOSFETs (no diodes).  Every accepted timepoint (and
+ * R, C, DC/PULSE/PWL V and I sources, level-1 diodes (with junction
+ * capacitance and transit time) and level-1 MOSFETs.  Every accepted timepoint (and
  * t = 0) is written for the `nprobe` unknowns in probes[], at most max_points
  * per circuit. */
 typedef struct nsg_tran_batch nsg_tran_batch;

@@ -22,6 +22,17 @@ ENGINE_NAMES = {0: "markowitz", 1: "amdlu"}
 GND = -1
 
 
+
+def diode_params(IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0, VJ: float = 1.0,
+                 M: float = 0.5, FC: float = 0.5, TT: float = 0.0) -> np.ndarray:
+    """The 10-value parameter block a diode with this card holds in
+    Circuit.params(): IS, N, then the junction values at the nominal
+    temperature (nsg_diode_param_block)."""
+    out = np.zeros(10, np.float64)
+    L.check(L.lib().nsg_diode_param_block(float(IS), float(N), float(CJO), float(VJ), float(M),
+                                          float(FC), float(TT), L.dptr(out)))
+    return out
+
 class Circuit:
     def __init__(self, num_nodes: int):
         h = ctypes.c_void_p()
@@ -43,8 +54,13 @@ class Circuit:
     def I(self, p: int, n: int, amps: float):  # noqa: E743 - the reference's name
         L.check(L.lib().nsg_circuit_add_isource(self._h, int(p), int(n), float(amps)))
 
-    def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0):
-        L.check(L.lib().nsg_circuit_add_diode(self._h, int(anode), int(cathode), float(IS), float(N)))
+    def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0,
+          VJ: float = 1.0, M: float = 0.5, FC: float = 0.5, TT: float = 0.0):
+        """Level-1 diode with the card D(IS N CJO VJ M FC TT); the junction
+        capacitance and transit time act in the transient."""
+        L.check(L.lib().nsg_circuit_add_diode_card(self._h, int(anode), int(cathode), float(IS),
+                                                   float(N), float(CJO), float(VJ), float(M),
+                                                   float(FC), float(TT)))
 
     def C(self, a: int, b: int, farads: float, ic: float | None = None):
         L.check(L.lib().nsg_circuit_add_capacitor(self._h, int(a), int(b), float(farads),

@@ -135,7 +135,7 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     d.prog_off[nsg::DP_term_op] = append(prog, c.term_op());
     d.prog_off[nsg::DP_term_param] = append(prog, c.term_param());
     std::vector<int32_t> tab;
-    for (const auto& dr : c.diodes()) tab.insert(tab.end(), {dr.pos, dr.neg, dr.param});
+    for (const auto& dr : c.diodes()) tab.insert(tab.end(), {dr.pos, dr.neg, dr.param, dr.state});
     d.prog_off[nsg::DP_diodes] = append(prog, tab);
     tab.clear();
     for (const auto& cr : c.caps()) tab.insert(tab.end(), {cr.pos, cr.neg, cr.param, cr.has_ic, cr.state});
@@ -156,7 +156,6 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     d.lrows_off = work; work = align4(work + p.lrow_ptr[p.n]);
     d.urows_off = work; work = align4(work + p.urow_ptr[p.n]);
     d.tv_off = work; work = align4(work + c.n_terms());
-    d.dstate_off = work; work = align4(work + 3 * d.n_diodes);
     d.dconst_off = work; work = align4(work + 3 * d.n_diodes);
     d.state_off = work; work = align4(work + 4 * static_cast<int64_t>(d.n_states));
     d.mrec_off = work; work = align4(work + nsg::kMosRecCount * static_cast<int64_t>(d.n_mos));
@@ -165,7 +164,7 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
 
 void place_dcsave(nsg::DcDesc& d, int64_t& work) {
     d.dcsave_off = work;
-    work = align4(work + d.n + 3 * static_cast<int64_t>(d.n_states) + 3 * d.n_diodes);
+    work = align4(work + d.n + 3 * static_cast<int64_t>(d.n_states));
 }
 
 }  // namespace nsg_internal
@@ -210,6 +209,26 @@ int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, dou
     return guarded("nsg_circuit_add_diode", [&]() -> int {
         if (!c) return fail(NSG_ERR_INVALID, "null circuit");
         c->c.add_diode(anode, cathode, is, n_emission);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is,
+                               double n_emission, double cjo, double vj, double m, double fc,
+                               double tt) {
+    return guarded("nsg_circuit_add_diode_card", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_diode(anode, cathode, is, n_emission, cjo, vj, m, fc, tt);
+        return NSG_OK;
+    });
+}
+
+int nsg_diode_param_block(double is, double n_emission, double cjo, double vj, double m,
+                          double fc, double tt, double* out) {
+    return guarded("nsg_diode_param_block", [&]() -> int {
+        if (!out) return fail(NSG_ERR_INVALID, "nsg_diode_param_block: null out");
+        const std::vector<double> p = nsg::diode_param_block(is, n_emission, cjo, vj, m, fc, tt);
+        std::copy(p.begin(), p.end(), out);
         return NSG_OK;
     });
 }

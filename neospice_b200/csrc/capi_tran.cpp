@@ -132,9 +132,6 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         for (int i = 0; i < count; ++i) {
             if (!circuits[i] || !circuits[i]->c.finalized())
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: circuit not finalized");
-            if (!circuits[i]->c.diodes().empty())
-                return fail(NSG_ERR_INVALID,
-                            "nsg_tran_batch_create: diodes are not supported in the transient");
             for (int j = 0; j < nprobe; ++j)
                 if (probes[j] < 0 || probes[j] >= circuits[i]->c.num_vars())
                     return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: probe out of range");
@@ -217,9 +214,9 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         int64_t work = 0, param_off = 0, x0_off = 0;
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
-            // The adjoint covers MOSFETs without charge: no oxide, overlap or
-            // junction capacitance in the parameter block.
-            bool ok = true;
+            // The adjoint covers MOSFETs without charge (no oxide, overlap or
+            // junction capacitance in the parameter block) and no diodes.
+            bool ok = c.diodes().empty();
             for (const auto& m : c.mosfets()) {
                 const double* P = c.params().data() + m.param;
                 for (int q : {nsg::kMOxCapFactor, nsg::kMCgso, nsg::kMCgdo, nsg::kMCgbo,
@@ -495,7 +492,7 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             if (!b->adjoint_ok[i])
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
                                                  std::to_string(i) +
-                                                 " has MOSFETs with charge (not covered)");
+                                                 " has diodes or MOSFETs with charge (not covered)");
             if (probe[i] < 0 || probe[i] >= d.n)
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: probe out of range");
             nsg::AdjDesc& a = ad[i];
@@ -505,8 +502,8 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             a.n_ckpt = a.n_steps / every + 1;
             a.rec_off = t.out_off;
             a.x0_off = t.x0_off;
-            const int64_t nmos = d.n_mos, ndio = d.n_diodes;
-            a.ckpt_len = (2 * d.n + 2 * d.n_states + 3 * ndio + 12 * nmos + 3) & ~int64_t{3};
+            const int64_t nmos = d.n_mos;
+            a.ckpt_len = (2 * d.n + 2 * d.n_states + nsg::kMosRecCount * nmos + 3) & ~int64_t{3};
             a.ws_off = ws;
             ws += a.n_ckpt * a.ckpt_len + (every + 2) * (int64_t{d.n} + d.n_states) +
                   3 * int64_t{d.n_caps} + d.n;

@@ -70,10 +70,66 @@ int32_t Circuit::add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wav
     return add_device(is_voltage ? DevKind::VSource : DevKind::ISource, p, n, values, wave);
 }
 
-int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_emission) {
-    if (!(is > 0.0) || !(n_emission > 0.0))
+// DIOtemp for one instance of area 1 at T = TNOM = CKTtemp: the grading
+// coefficient, the junction potential and capacitance after the (here
+// neutral) temperature adjustment, F1..F3 and the depletion-capacitance
+// knee, each by the reference's expression.
+std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
+                                      double fc, double tt) {
+    if (!(is > 0.0) || !(n > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
-    return add_device(DevKind::Diode, anode, cathode, {is, n_emission});
+    if (!(cjo >= 0.0) || !(vj > 0.0) || !(m >= 0.0 && m < 1.0) || !(fc >= 0.0 && fc < 1.0) ||
+        !(tt >= 0.0) || !std::isfinite(cjo) || !std::isfinite(vj) || !std::isfinite(tt))
+        throw std::invalid_argument(
+            "Circuit: diode needs CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0");
+    constexpr double kBoltz = 1.38064852e-23, kCharge = 1.6021766208e-19, kRefTemp = 300.15;
+    const double temp = kTNominal, tnom = kTNominal, dt = temp - tnom;
+    const double vtnom = kKoverQ * tnom;
+    const double xfc = std::log(1 - fc);
+    double grad = m * (1.0 + (0.0 * dt) + (0.0 * dt * dt));
+    if (grad > .9) grad = .9;
+    const double vt = kKoverQ * temp;
+    const double fact2 = temp / kRefTemp;
+    const double egfet = 1.16 - (7.02e-4 * temp * temp) / (temp + 1108);
+    const double arg = -egfet / (2 * kBoltz * temp) + 1.1150877 / (kBoltz * (kRefTemp + kRefTemp));
+    const double pbfact = -2 * vt * (1.5 * std::log(fact2) + kCharge * arg);
+    const double egfet1 = 1.16 - (7.02e-4 * tnom * tnom) / (tnom + 1108);
+    const double arg1 = -egfet1 / (kBoltz * 2 * tnom) + 1.1150877 / (2 * kBoltz * kRefTemp);
+    const double fact1 = tnom / kRefTemp;
+    const double pbfact1 = -2 * vtnom * (1.5 * std::log(fact1) + kCharge * arg1);
+    const double pbo = (vj - pbfact1) / fact1;
+    const double gmaold = (vj - pbo) / pbo;
+    double cj = cjo / (1 + grad * (400e-6 * (tnom - kRefTemp) - gmaold));
+    double pot = pbfact + fact2 * pbo;
+    const double gmanew = (pot - pbo) / pbo;
+    cj *= 1 + grad * (400e-6 * (temp - kRefTemp) - gmanew);
+    const double f1 = pot * (1 - std::exp((1 - grad) * xfc)) / (1 - grad);
+    double depcap = fc * pot;
+    if (depcap > 1.0) {
+        pot = 1.0 / fc;
+        depcap = fc * pot;
+    }
+    const double ttt = tt * (1.0 + (0.0 * dt) + (0.0 * dt * dt));
+    const double f2 = std::exp((1 + grad) * xfc);
+    const double f3 = 1 - fc * (1 + grad);
+    std::vector<double> p(kDiodeParams);
+    p[kDpCsat] = is;
+    p[kDpN] = n;
+    p[kDpCj] = cj;
+    p[kDpPot] = pot;
+    p[kDpDepCap] = depcap;
+    p[kDpF1] = f1;
+    p[kDpF2] = f2;
+    p[kDpF3] = f3;
+    p[kDpGrad] = grad;
+    p[kDpTt] = ttt;
+    return p;
+}
+
+int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
+                           double cjo, double vj, double m, double fc, double tt) {
+    return add_device(DevKind::Diode, anode, cathode,
+                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt));
 }
 
 int32_t Circuit::add_mos1_model(const Mos1Card& card) {
@@ -191,7 +247,8 @@ void Circuit::finalize() {
             state += kMosStates;
         } else if (d.kind == DevKind::Diode) {
             index_in_table[k] = static_cast<int32_t>(diodes_.size());
-            diodes_.push_back({d.a, d.b, d.param});
+            diodes_.push_back({d.a, d.b, d.param, state});
+            state += kDiodeStates;
         } else if (d.kind == DevKind::Capacitor) {
             index_in_table[k] = static_cast<int32_t>(caps_.size());
             caps_.push_back({d.a, d.b, d.param, d.has_ic ? 1 : 0, state});

@@ -79,6 +79,13 @@ struct Mos1Card {
 // unsupported parameter (nonzero RD, RS or RSH).
 std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L);
 
+// The diode parameter block (DiodeParam of kernels/diode_model.cuh) of the
+// card D(IS N CJO VJ M FC TT) at the nominal temperature: DIOtemp
+// (src/devices/dio/dio_temp.cpp:91-292).  Throws std::invalid_argument
+// outside IS > 0, N > 0, CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0.
+std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
+                                      double fc, double tt);
+
 class Circuit {
 public:
     explicit Circuit(int32_t num_nodes);
@@ -86,7 +93,7 @@ public:
     // Parameters of every device are kept in creation order in params():
     // resistor {ohms}; capacitor {farads, ic}; DC source {value}; PULSE
     // source {v1, v2, td, tr, tf, pw, per}; PWL source {t0, v0, t1, v1, ...};
-    // diode {IS, N}.
+    // diode: the DiodeParam block of kernels/diode_model.cuh.
     int32_t add_resistor(int32_t a, int32_t b, double ohms);
     int32_t add_capacitor(int32_t a, int32_t b, double farads, bool has_ic, double ic);
     int32_t add_vsource(int32_t p, int32_t n, double volts);
@@ -94,7 +101,13 @@ public:
     // Waveform sources: is_voltage selects V or I; values per Wave above.
     int32_t add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wave,
                             const std::vector<double>& values);
-    int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission);
+    // Level-1 diode (Circuit::D with a `.model D(IS N CJO VJ M FC TT)` card,
+    // src/core/circuit.hpp:210-211): IS > 0, N > 0, CJO >= 0, VJ > 0,
+    // 0 <= M < 1, 0 <= FC < 1, TT >= 0; DIOsetup's defaults
+    // (src/devices/dio/dio_setup.cpp:55-82) for the junction values.
+    int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
+                      double cjo = 0.0, double vj = 1.0, double m = 0.5, double fc = 0.5,
+                      double tt = 0.0);
     // Level-1 MOSFET models and instances (Circuit::model,
     // src/core/circuit.hpp:259, and Circuit::M with W and L, :218-219).
     // Returns the model / device index.
@@ -118,7 +131,7 @@ public:
     const std::vector<int32_t>& dead_nodes() const { return dead_nodes_; }
 
     // Devices with per-iteration evaluation, in load order.
-    struct DiodeRec { int32_t pos, neg, param; };
+    struct DiodeRec { int32_t pos, neg, param, state; };  // state: base of kDiodeStates
     struct CapRec { int32_t pos, neg, param, has_ic, state; };  // state: base of {q, i}
     struct SrcRec { int32_t is_voltage, wave, param, nparam; };
     struct MosRec { int32_t d, g, s, b, param, state; };

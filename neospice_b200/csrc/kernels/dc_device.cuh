@@ -29,12 +29,12 @@ struct DcDesc {
     int64_t param_off;           // into the caller's parameter array
     int64_t sol_off;             // into the caller's solution array
     // workspace (doubles): solution, previous iterate, sweep scratch, matrix
-    // values, LU values, term values, diode state, diode constants
-    int64_t x_off, xold_off, w_off, a_off, lu_off, tv_off, dstate_off, dconst_off;
+    // values, LU values, term values, diode constants
+    int64_t x_off, xold_off, w_off, a_off, lu_off, tv_off, dconst_off;
     int64_t lrows_off, urows_off;  // row-major copies of L and U for the sweeps
     int64_t state_off;             // four state vectors of n_states doubles
     int64_t mrec_off;              // per-MOSFET persistent load values
-    int64_t dcsave_off;            // gmin-stepping save area (x, state0..2, diode state)
+    int64_t dcsave_off;            // gmin-stepping save area (x, state0..2)
     // Doubles from x_off on that a launch may stage in shared memory (every
     // per-iteration region: vectors, matrix, LU, terms, states, history).
     int64_t stage_len;

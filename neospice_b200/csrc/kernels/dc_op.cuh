@@ -13,26 +13,22 @@
 
 namespace nsg {
 
-// Save area: x (n), state0..2 (3 n_states), diode state (3 n_diodes).
+// Save area: x (n), state0..2 (3 n_states).
 __device__ inline void dc_op_copy(const Inst& v, int32_t n_states, double* save, int action) {
     if (action == kActNone) return;
     double* sx = save;
     double* ss = save + v.n;
-    double* sd = ss + 3 * static_cast<int64_t>(n_states);
     const int64_t ns3 = 3 * static_cast<int64_t>(n_states);
     if (action == kActZeroSave) {
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = sx[i] = 0.0;
         for (int64_t i = threadIdx.x; i < ns3; i += blockDim.x)
             v.st[i / n_states][i % n_states] = ss[i] = 0.0;
-        for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) v.dstate[i] = sd[i] = 0.0;
     } else if (action == kActSave) {
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) sx[i] = v.x[i];
         for (int64_t i = threadIdx.x; i < ns3; i += blockDim.x) ss[i] = v.st[i / n_states][i % n_states];
-        for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) sd[i] = v.dstate[i];
     } else {
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = sx[i];
         for (int64_t i = threadIdx.x; i < ns3; i += blockDim.x) v.st[i / n_states][i % n_states] = ss[i];
-        for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) v.dstate[i] = sd[i];
     }
 }
 

@@ -1,7 +1,8 @@
-// DC load of the level-1 junction diode (RS = 0, no breakdown, no knee
-// currents, T = TNOM), shared by the host (first-iteration values for the
-// symbolic phase) and the GPU Newton kernel.  Follows DIOload
-// (src/devices/dio/dio_load.cpp:98-383) and DEVpnjlim
+// Load of the level-1 junction diode (RS = 0, no breakdown, no knee
+// currents, no sidewall, T = TNOM), shared by the host (first-iteration
+// values for the symbolic phase) and the GPU Newton kernels: the DC current
+// and conductance, and the depletion and diffusion charge of the transient.
+// Follows DIOload (src/devices/dio/dio_load.cpp:98-383) and DEVpnjlim
 // (src/devices/dio/dio_shim.cpp:101-121) operation for operation, with the
 // platform's exp/log.
 #pragma once
@@ -14,6 +15,33 @@
 #endif
 
 namespace nsg {
+
+// Per-instance diode parameter block: the saturation current, the emission
+// coefficient, then DIOtemp's temperature-adjusted capacitance values
+// (src/devices/dio/dio_temp.cpp:108-292) at T = TNOM.
+enum DiodeParam : int {
+    kDpCsat = 0,    // DIOtSatCur (IS * area)
+    kDpN = 1,       // N
+    kDpCj = 2,      // DIOtJctCap
+    kDpPot = 3,     // DIOtJctPot
+    kDpDepCap = 4,  // DIOtDepCap (FC * DIOtJctPot)
+    kDpF1 = 5,      // DIOtF1
+    kDpF2 = 6,      // DIOtF2
+    kDpF3 = 7,      // DIOtF3
+    kDpGrad = 8,    // DIOtGradingCoeff
+    kDpTt = 9,      // DIOtTransitTime
+    kDiodeParams = 10
+};
+
+// Diode state slots (src/devices/dio/dio_def.hpp:160-164).
+enum DiodeState : int {
+    kDsV = 0,   // DIOvoltage
+    kDsI = 1,   // DIOcurrent
+    kDsG = 2,   // DIOconduct
+    kDsQ = 3,   // DIOcapCharge
+    kDsCq = 4,  // DIOcapCurrent
+    kDiodeStates = 5
+};
 
 NSG_HD inline double pnjlim(double vnew, double vold, double vt, double vcrit, int* icheck) {
     if ((vnew > vcrit) && (fabs(vnew - vold) > (vt + vt))) {
@@ -43,21 +71,19 @@ NSG_HD inline double pnjlim(double vnew, double vold, double vt, double vcrit, i
 
 struct DiodeDC {
     double vd, cd, gd;
+    double cdb, gdb;  // bottom-junction current and conductance before gmin
     int check;  // 1: limited / junction-init iteration (counts as non-converged)
 };
 
-// csat = area-scaled saturation current at T, vte = N*vt, tvcrit = Vcrit.
-NSG_HD inline DiodeDC diode_dc_load(bool initjct, double v_pos, double v_neg, double vd_old,
-                                    double csat, double vte, double tvcrit, double gmin) {
+// Current and conductance at the junction voltage vd, limited against
+// vd_old by DEVpnjlim when `limit` (every mode but the junction
+// initialisation and MODEINITTRAN).  csat = area-scaled saturation current
+// at T, vte = N*vt, tvcrit = Vcrit.
+NSG_HD inline DiodeDC diode_eval(double vd, bool limit, double vd_old, double csat, double vte,
+                                 double tvcrit, double gmin) {
     DiodeDC r;
     r.check = 1;
-    double vd;
-    if (initjct) {
-        vd = tvcrit;
-    } else {
-        vd = v_pos - v_neg;
-        vd = pnjlim(vd, vd_old, vte, tvcrit, &r.check);
-    }
+    if (limit) vd = pnjlim(vd, vd_old, vte, tvcrit, &r.check);
     double cd, gd;
     if (vd >= -3 * vte) {
         const double evd = exp(vd / vte);
@@ -69,6 +95,8 @@ NSG_HD inline DiodeDC diode_dc_load(bool initjct, double v_pos, double v_neg, do
         cd = -csat * (1 + arg);
         gd = csat * 3 * arg / vd;
     }
+    r.cdb = cd;
+    r.gdb = gd;
     cd = cd + 0.0;  // + sidewall current (absent)
     gd = gd + 0.0;
     gd = gd + gmin;
@@ -77,6 +105,38 @@ NSG_HD inline DiodeDC diode_dc_load(bool initjct, double v_pos, double v_neg, do
     r.cd = cd;
     r.gd = gd;
     return r;
+}
+
+// The DC operating-point load: Vcrit at MODEINITJCT, else the node voltages
+// limited against the previous junction voltage.
+NSG_HD inline DiodeDC diode_dc_load(bool initjct, double v_pos, double v_neg, double vd_old,
+                                    double csat, double vte, double tvcrit, double gmin) {
+    return diode_eval(initjct ? tvcrit : v_pos - v_neg, !initjct, vd_old, csat, vte, tvcrit, gmin);
+}
+
+// Junction charge and capacitance of the charge-storage block of DIOload
+// (dio_load.cpp:309-346): depletion charge below / above FC * VJ, plus the
+// diffusion charge TT * cdb.  The sidewall terms are zero (no CJSW, no
+// sidewall current): their diffusion parts enter as the reference's +0.0
+// additions, and adding the zero depletion parts changes no sum.
+NSG_HD inline void diode_charge(const double* p, double vd, double cdb, double gdb, double* charge,
+                                double* capd) {
+    const double czero = p[kDpCj], pot = p[kDpPot], grad = p[kDpGrad], depcap = p[kDpDepCap];
+    double qdep, cdep;
+    if (vd < depcap) {
+        const double arg = 1 - vd / pot;
+        const double sarg = exp(-grad * log(arg));
+        qdep = pot * czero * (1 - arg * sarg) / (1 - grad);
+        cdep = czero * sarg;
+    } else {
+        const double czof2 = czero / p[kDpF2];
+        qdep = czero * p[kDpF1] +
+               czof2 * (p[kDpF3] * (vd - depcap) + (grad / (pot + pot)) * (vd * vd - depcap * depcap));
+        cdep = czof2 * (p[kDpF3] + grad * vd / pot);
+    }
+    const double tt = p[kDpTt];
+    *charge = tt * cdb + tt * 0.0 + qdep;
+    *capd = tt * gdb + tt * 0.0 + cdep;
 }
 
 // Vcrit of DIOtemp (src/devices/dio/dio_temp.cpp:209-212).

@@ -34,7 +34,7 @@ struct Inst {
     const int32_t* ucb_terms;
     const int32_t* term_op;
     const int32_t* term_param;
-    const int32_t* diodes;  // (pos, neg, param)
+    const int32_t* diodes;  // (pos, neg, param, state)
     const int32_t* caps;    // (pos, neg, param, has_ic, state)
     const int32_t* srcs;    // (is_voltage, wave, param, nparam)
     const int32_t* mos;     // (d, g, s, b, param, state)
@@ -46,9 +46,8 @@ struct Inst {
     double* lrows;
     double* urows;
     double* tv;
-    double* dstate;
     double* dconst;
-    double* st[4];          // capacitor state ring state0..state3
+    double* st[4];          // device state ring state0..state3
     double* mrec;           // per-MOSFET load values (kMosRecCount each)
     int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs, n_mos;
 };
@@ -96,7 +95,6 @@ __device__ inline Inst make_inst(const DcDesc& d, const int32_t* prog, const dou
     v.lrows = ws_at(d, work, stage, d.lrows_off);
     v.urows = ws_at(d, work, stage, d.urows_off);
     v.tv = ws_at(d, work, stage, d.tv_off);
-    v.dstate = ws_at(d, work, stage, d.dstate_off);
     v.dconst = ws_at(d, work, stage, d.dconst_off);
     for (int k = 0; k < 4; ++k)
         v.st[k] = ws_at(d, work, stage, d.state_off) + k * static_cast<int64_t>(d.n_states);
@@ -133,7 +131,7 @@ __device__ inline void load_constants(const Inst& v, double gmin) {
         v.tv[k] = term_value(v.term_op[k], pi >= 0 ? v.par[pi] : 0.0, gmin);
     }
     for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
-        const int32_t pi = v.diodes[3 * k + 2];
+        const int32_t pi = v.diodes[4 * k + 2];
         const double csat = v.par[pi];
         const double vte = v.par[pi + 1] * kKoverQTimesTnom;
         v.dconst[3 * k] = csat;
@@ -142,9 +140,24 @@ __device__ inline void load_constants(const Inst& v, double gmin) {
     }
 }
 
-// Device loads of one Newton iteration at the guess xold: diodes (DIOload,
-// DC), capacitors (Capacitor::evaluate, state-vector path), waveform
-// sources (value_at).  Writes the dynamic terms; returns through s_dev_conv
+// NIintegrate of the charge in state slot q (its current in q + 1):
+// backward Euler at order 1, else trapezoidal (xmu_ratio) or Gear-2
+// (src/devices/dio/dio_shim.cpp:44-73).  Returns the current.
+__device__ inline double ni_integrate(const Inst& v, const IntegCtx& c, int32_t q) {
+    const int order = c.order < 1 ? 1 : (c.order > 2 ? 2 : c.order);
+    const double* s0 = v.st[0];
+    const double* s1 = v.st[1];
+    double deriv;
+    if (order == 1) deriv = c.ag[0] * s0[q] + c.ag[1] * s1[q];
+    else if (c.method == 0) deriv = -s1[q + 1] * c.xmu_ratio + c.ag[0] * s0[q] + c.ag[1] * s1[q];
+    else deriv = c.ag[0] * s0[q] + c.ag[1] * s1[q] + c.ag[2] * v.st[2][q];
+    v.st[0][q + 1] = deriv;
+    return deriv;
+}
+
+// Device loads of one Newton iteration at the guess xold: diodes (DIOload
+// with its charge storage), capacitors (Capacitor::evaluate, state-vector
+// path), MOSFETs, waveform sources (value_at).  Writes the dynamic terms; returns through s_dev_conv
 // whether every device reports convergence (diodes' CKTnoncon and conv_test).
 static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& c, const NewtonOptions& opt,
                                     int32_t* s_dev_conv) {
@@ -152,28 +165,65 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
     double* tv_d = v.tv + v.n_const;
     double* tv_c = tv_d + kDiodeTermCount * v.n_diodes;
     double* tv_s = tv_c + kCapTermCount * v.n_caps;
-    const bool initjct = (mode & kModeInitJct) != 0;
+    const bool uic_op = (mode & kModeTranOp) && (mode & kModeUic);
+    const bool charges = (mode & (kModeTran | kModeAc)) || uic_op;
     for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
-        const int32_t pos = v.diodes[3 * k], neg = v.diodes[3 * k + 1];
+        const int32_t* dr = v.diodes + 4 * k;
+        const int32_t pos = dr[0], neg = dr[1], s = dr[3];
         const double vp = pos >= 0 ? v.xold[pos] : 0.0;
         const double vn = neg >= 0 ? v.xold[neg] : 0.0;
-        const DiodeDC r = diode_dc_load(initjct, vp, vn, v.dstate[3 * k], v.dconst[3 * k],
-                                        v.dconst[3 * k + 1], v.dconst[3 * k + 2], opt.gmin);
-        v.dstate[3 * k] = r.vd;
-        v.dstate[3 * k + 1] = r.cd;
-        v.dstate[3 * k + 2] = r.gd;
-        const double cdeq = r.cd - r.gd * r.vd;
+        double* s0 = v.st[0] + s;
+        double* s1 = v.st[1] + s;
+        // The junction voltage of this load (dio_load.cpp:100-166; no OFF,
+        // IC = 0).
+        double vd = vp - vn;
+        bool limit = false;
+        if (mode & kModeInitTran) {
+            vd = s1[kDsV];
+        } else if ((mode & kModeInitJct) && uic_op) {
+            vd = 0.0;
+        } else if (mode & kModeInitJct) {
+            vd = v.dconst[3 * k + 2];
+        } else {
+            if (mode & kModeInitPred) {  // DEVpred
+                s0[kDsV] = s1[kDsV];
+                const double xfact = c.delta / c.delta_old[1];
+                vd = ((1.0 + xfact) * s1[kDsV]) - (xfact * v.st[2][s + kDsV]);
+                s0[kDsI] = s1[kDsI];
+                s0[kDsG] = s1[kDsG];
+            }
+            limit = true;
+        }
+        const DiodeDC r = diode_eval(vd, limit, s0[kDsV], v.dconst[3 * k], v.dconst[3 * k + 1],
+                                     v.dconst[3 * k + 2], opt.gmin);
+        double cd = r.cd, gd = r.gd;
+        if (charges) {  // charge storage (dio_load.cpp:309-373)
+            double charge, capd;
+            diode_charge(v.par + dr[2], r.vd, r.cdb, r.gdb, &charge, &capd);
+            s0[kDsQ] = charge;
+            if (!uic_op) {
+                if (mode & kModeInitTran) s1[kDsQ] = s0[kDsQ];
+                const double ccap = ni_integrate(v, c, s + kDsQ);
+                gd = gd + c.ag[0] * capd;
+                cd = cd + ccap;
+                if (mode & kModeInitTran) s1[kDsCq] = s0[kDsCq];
+            }
+        }
+        s0[kDsV] = r.vd;
+        s0[kDsI] = cd;
+        s0[kDsG] = gd;
+        const double cdeq = cd - gd * r.vd;
         double* t = tv_d + kDiodeTermCount * k;
-        t[0] = r.gd;
-        t[1] = r.gd + 0.0;
-        t[2] = -r.gd;
+        t[0] = gd;
+        t[1] = gd + 0.0;
+        t[2] = -gd;
         t[3] = cdeq;
         t[4] = -cdeq;
         // DIODevice::conv_test (dio_device.cpp:296-307) on the stored state
         const double delvd = (vp - vn) - r.vd;
-        const double cdhat = r.cd + r.gd * delvd;
-        const double tol = opt.reltol * fmax(fabs(cdhat), fabs(r.cd)) + opt.abstol;
-        if (!((r.check == 0) && (fabs(cdhat - r.cd) <= tol))) *s_dev_conv = 0;
+        const double cdhat = cd + gd * delvd;
+        const double tol = opt.reltol * fmax(fabs(cdhat), fabs(cd)) + opt.abstol;
+        if (!((r.check == 0) && (fabs(cdhat - cd) <= tol))) *s_dev_conv = 0;
     }
     for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
         const int32_t* cr = v.caps + 5 * k;

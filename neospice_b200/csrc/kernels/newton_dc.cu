@@ -45,7 +45,6 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     __syncthreads();
     const bool fresh = s_fresh != 0;
     if (fresh) {
-        for (int32_t k = threadIdx.x; k < 3 * v.n_diodes; k += blockDim.x) v.dstate[k] = 0.0;
         for (int32_t k = threadIdx.x; k < kMosRecCount * v.n_mos; k += blockDim.x) v.mrec[k] = 0.0;
         for (int32_t k = threadIdx.x; k < 4 * d.n_states; k += blockDim.x) v.st[0][k] = 0.0;
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;

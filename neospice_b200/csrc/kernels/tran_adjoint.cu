@@ -138,8 +138,7 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         vcopy(r + n, xprev, n);
         vcopy(r + 2 * n, v.st[1], ns);
         vcopy(r + 2 * n + ns, v.st[2], ns);
-        vcopy(r + 2 * n + 2 * ns, v.dstate, 3 * v.n_diodes);
-        vcopy(r + 2 * n + 2 * ns + 3 * v.n_diodes, v.mrec, kMosRecCount * v.n_mos);
+        vcopy(r + 2 * n + 2 * ns, v.mrec, kMosRecCount * v.n_mos);
     };
     // Accepted step s from the current state: Newton, then rotate the ring
     // (state3 <- state2 <- state1 <- state0).  False if Newton failed.
@@ -172,7 +171,6 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     load_constants(v, opt.gmin);
     vcopy(v.x, rec_x0 + td.x0_off, n);
     vcopy(v.xold, rec_x0 + td.x0_off, n);
-    for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) v.dstate[i] = 0.0;
     for (int32_t i = threadIdx.x; i < kMosRecCount * v.n_mos; i += blockDim.x) v.mrec[i] = 0.0;
     for (int32_t i = threadIdx.x; i < 4 * ns; i += blockDim.x) v.st[0][i] = 0.0;
     if (threadIdx.x == 0) {
@@ -243,8 +241,7 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         vcopy(seg_s + ns, r + 2 * n, ns);
         vcopy(v.st[2], r + 2 * n + ns, ns);
         vcopy(seg_s, r + 2 * n + ns, ns);
-        vcopy(v.dstate, r + 2 * n + 2 * ns, 3 * v.n_diodes);
-        vcopy(v.mrec, r + 2 * n + 2 * ns + 3 * v.n_diodes, kMosRecCount * v.n_mos);
+        vcopy(v.mrec, r + 2 * n + 2 * ns, kMosRecCount * v.n_mos);
         __syncthreads();
         for (int64_t s = c0 + 1; s <= c1; ++s) {
             if (!step(s)) {
@@ -321,7 +318,7 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     load_constants(v, opt.gmin);
     vcopy(v.xold, x0, n);
     const double* r0 = ckpt;
-    vcopy(v.mrec, r0 + 2 * n + 2 * ns + 3 * v.n_diodes, kMosRecCount * v.n_mos);
+    vcopy(v.mrec, r0 + 2 * n + 2 * ns, kMosRecCount * v.n_mos);
     vcopy(v.st[0], r0 + 2 * n, ns);
     if (threadIdx.x == 0) {
         ctx = IntegCtx{};

@@ -55,14 +55,19 @@ __device__ inline double cap_trunc(const Inst& v, int32_t q, const IntegCtx& c,
     return del;
 }
 
-// Minimum over the charge states of capacitors and MOSFETs of their proposed
-// timestep (Device::compute_trunc: capacitor.cpp, mos1_device.cpp:352-366),
-// reduced across the CTA.  std::min semantics: a NaN proposal is ignored.
+// Minimum over the charge states of capacitors, diodes and MOSFETs of their
+// proposed timestep (Device::compute_trunc: capacitor.cpp,
+// dio_device.cpp:280-290, mos1_device.cpp:352-366), reduced across the CTA.
+// std::min semantics: a NaN proposal is ignored.
 __device__ inline double min_trunc(const Inst& v, const IntegCtx& c, const TranOptions& o,
                                    double* s_red) {
     double m = 1e30;
     for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) {
         const double t = cap_trunc(v, v.caps[5 * k + 4], c, o);
+        if (t < m) m = t;
+    }
+    for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+        const double t = cap_trunc(v, v.diodes[4 * k + 3] + kDsQ, c, o);
         if (t < m) m = t;
     }
     for (int32_t k = threadIdx.x; k < 5 * v.n_mos; k += blockDim.x) {
@@ -203,7 +208,6 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     if (threadIdx.x == 0) k = *g;
     __syncthreads();
     if (k.phase == kTrInit) {
-        for (int32_t i = threadIdx.x; i < 3 * v.n_diodes; i += blockDim.x) v.dstate[i] = 0.0;
         for (int32_t i = threadIdx.x; i < kMosRecCount * v.n_mos; i += blockDim.x) v.mrec[i] = 0.0;
         for (int32_t i = threadIdx.x; i < 4 * d.n_states; i += blockDim.x) v.st[0][i] = 0.0;
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;

@@ -15,7 +15,7 @@ import dataclasses
 
 import numpy as np
 
-from .circuit import GND, Circuit
+from .circuit import GND, Circuit, diode_params
 
 
 @dataclasses.dataclass
@@ -53,7 +53,8 @@ class DiodeMesh:
 
     def params(self) -> np.ndarray:
         """Parameters in the circuit's creation order."""
-        dio = np.repeat([[self.diode_is, self.diode_n]], len(self.diode_nodes), axis=0).ravel()
+        block = diode_params(self.diode_is, self.diode_n)
+        dio = np.repeat(block[None, :], len(self.diode_nodes), axis=0).ravel()
         return np.concatenate([self.r_h, self.r_v, dio, self.isrc_amps, [self.v_corner]])
 
 
@@ -83,7 +84,8 @@ class Netlist:
     list order (so node numbering and device load order are fixed).  Devices:
     ("R", a, b, ohms), ("C", a, b, farads), ("V", p, n, volts),
     ("I", p, n, amps), ("VPULSE"|"IPULSE", p, n, v1, v2, td, tr, tf, pw, per),
-    ("VPWL"|"IPWL", p, n, t0, v0, t1, v1, ...), ("D", anode, cathode, IS, N).
+    ("VPWL"|"IPWL", p, n, t0, v0, t1, v1, ...), ("D", anode, cathode, IS, N) or
+    ("D", anode, cathode, IS, N, CJO, VJ, M, FC, TT).
     ("M", d, g, s, b, model_name, W, L) with models[model_name] =
     ("nmos"|"pmos", {param: value}) (level-1 cards).  Node -1 is ground."""
     num_nodes: int
@@ -111,7 +113,7 @@ class Netlist:
                 pts = np.asarray(vals, np.float64).reshape(-1, 2)
                 (c.VPWL if kind[0] == "V" else c.IPWL)(a, b, pts)
             elif kind == "D":
-                c.D(a, b, vals[0], vals[1])
+                c.D(a, b, *vals)
             else:
                 raise ValueError(f"unknown device kind {kind!r}")
         return c.finalize()

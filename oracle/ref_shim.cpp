@@ -468,8 +468,15 @@ static void build_from_desc(Circuit& ckt, const char* desc) {
                 else static_cast<ISource*>(d)->set_pwl(pw);
             }
         } else if (kind == "D") {
-            char card[160];
-            std::snprintf(card, sizeof card, ".model dm%d D(IS=%.17g N=%.17g)", dev, D_(3), D_(4));
+            // D a k IS N [CJO VJ M FC TT]
+            char card[400];
+            if (tk.size() > 5)
+                std::snprintf(card, sizeof card,
+                              ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g FC=%.17g "
+                              "TT=%.17g)",
+                              dev, D_(3), D_(4), D_(5), D_(6), D_(7), D_(8), D_(9));
+            else
+                std::snprintf(card, sizeof card, ".model dm%d D(IS=%.17g N=%.17g)", dev, D_(3), D_(4));
             ckt.model(card);
             ckt.D(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), "dm" + std::to_string(dev));
         } else if (kind == "MODEL") {

@@ -15,6 +15,10 @@ list and model cards (JSON), tstep/tstop, and the
 reference's solve_transient output: every timepoint, all node voltages,
 total Newton iterations and rejected steps.
 
+tran_diode.npz: the same record for diode circuits with junction capacitance
+and transit time (rectifier, reverse recovery, seeded diode-RC networks,
+DIOtemp's grading and junction-potential limits).
+
 mos_dc.npz: CMOS inverter chains and seeded MOS networks, per case the
 netlist (JSON) and the reference's solve_dc operating point, Newton
 iteration count and convergence method (0 direct, 1 gmin stepping).
@@ -155,7 +159,11 @@ def tran_netlists():
 
 
 def mos_netlists():
-    """DC cases of mos_dc.npz: CMOS inverter chains at several input levels
+    """DC cases of tran_diode.npz: the same record for diode circuits with junction capacitance
+and transit time (rectifier, reverse recovery, seeded diode-RC networks,
+DIOtemp's grading and junction-potential limits).
+
+mos_dc.npz: CMOS inverter chains at several input levels
     (the longer ones need gmin stepping) and seeded MOS networks with body
     effect, channel-length modulation and oxide-derived parameters."""
     from neospice_b200 import workloads as W
@@ -213,11 +221,50 @@ def sens_main():
     print(f"wrote {len(cases)} sensitivity cases to {path}")
 
 
-def tran_main():
+def tran_diode_netlists():
+    """(netlist, tstep, tstop) cases of tran_diode.npz: diodes with junction
+    capacitance and transit time in the transient — a half-wave rectifier,
+    reverse recovery of a clamp, seeded diode-RC networks (forward bias past
+    the FC*VJ knee, reverse bias), a charge-free diode, and the grading (M >
+    0.9) and junction-potential (FC*VJ > 1) limits of DIOtemp."""
+    from neospice_b200 import workloads as W
+    cases = []
+    cases.append((W.Netlist(3, [
+        ("VPULSE", 0, -1, 0.0, 2.0, 1e-9, 1e-9, 1e-9, 5e-9, 12e-9), ("R", 0, 1, 100.0),
+        ("D", 1, 2, 1e-14, 1.0, 2e-12, 0.8, 0.4, 0.5, 5e-9),
+        ("R", 2, -1, 1000.0), ("C", 2, -1, 1e-11)]), 1e-10, 4e-8))
+    cases.append((W.Netlist(2, [
+        ("VPULSE", 0, -1, 1.0, -1.0, 5e-9, 1e-10, 1e-10, 20e-9, 40e-9), ("R", 0, 1, 50.0),
+        ("D", 1, -1, 1e-14, 1.0, 1e-12, 0.7, 0.5, 0.5, 1e-8)]), 1e-10, 3e-8))
+    for k, nodes in enumerate((5, 9)):
+        rng = np.random.default_rng([61, k])
+        dev = [("VPULSE", 0, -1, -1.0, 1.5, 1e-10, 2e-10, 2e-10, 1e-9, 3e-9)]
+        for i in range(1, nodes):
+            dev.append(("R", int(rng.integers(0, i)), i, float(rng.lognormal(np.log(200.0), 0.3))))
+            dev.append(("C", i, -1, float(rng.lognormal(np.log(1e-13), 0.3))))
+            if rng.random() < 0.6:
+                a, b = (i, -1) if rng.random() < 0.5 else (-1, i)
+                dev.append(("D", a, b, float(10 ** rng.uniform(-15, -13)), float(rng.uniform(1.0, 1.8)),
+                            float(rng.lognormal(np.log(5e-13), 0.5)), float(rng.uniform(0.5, 1.0)),
+                            float(rng.uniform(0.3, 0.6)), float(rng.uniform(0.3, 0.6)),
+                            float(rng.choice([0.0, 1e-10, 1e-9]))))
+        cases.append((W.Netlist(nodes, dev), 2e-11, 6e-9))
+    cases.append((W.Netlist(3, [
+        ("VPULSE", 0, -1, 0.0, 1.2, 0.0, 5e-10, 5e-10, 2e-9, 5e-9), ("R", 0, 1, 300.0),
+        ("D", 1, -1, 1e-14, 1.0), ("R", 1, 2, 100.0), ("C", 2, -1, 2e-12)]), 2e-11, 1e-8))
+    cases.append((W.Netlist(3, [
+        ("VPULSE", 0, -1, -2.0, 1.0, 2e-10, 2e-10, 2e-10, 2e-9, 4e-9), ("R", 0, 1, 200.0),
+        ("D", 1, -1, 1e-14, 1.0, 3e-12, 0.9, 0.95, 0.5, 2e-10),
+        ("R", 1, 2, 200.0), ("D", 2, -1, 2e-14, 1.2, 1e-12, 2.5, 0.5, 0.5, 0.0),
+        ("C", 2, -1, 1e-13)]), 2e-11, 8e-9))
+    return cases
+
+
+def tran_main(which="tran"):
     import json
     import netlists
     rec = {}
-    cases = tran_netlists()
+    cases = tran_netlists() if which == "tran" else tran_diode_netlists()
     for k, (nl, tstep, tstop) in enumerate(cases):
         t, v, info = oracle.ref_sim(netlists.ref_desc(nl), 1, tstep, tstop)
         p = f"t{k:02d}_"
@@ -227,7 +274,7 @@ def tran_main():
                     p + "iterations": np.int32(info["iterations"]),
                     p + "rejected": np.int32(info["rejected"])})
     rec["count"] = np.int32(len(cases))
-    path = pathlib.Path(__file__).with_name("tran_rc.npz")
+    path = pathlib.Path(__file__).with_name("tran_rc.npz" if which == "tran" else "tran_diode.npz")
     np.savez_compressed(path, **rec)
     print(f"wrote {len(cases)} transients to {path}")
 
@@ -398,7 +445,7 @@ def amd_main():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran", "mos", "sens", "amd", "linear"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "sens", "amd", "linear"]
     if "amd" in which:
         amd_main()
     if "linear" in which:
@@ -409,6 +456,8 @@ if __name__ == "__main__":
         mesh_main()
     if "tran" in which:
         tran_main()
+    if "trandiode" in which:
+        tran_main("trandiode")
     if "mos" in which:
         mos_main()
     if "sens" in which:

@@ -39,10 +39,10 @@ def load_meshes():
 TRAN_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "tran_rc.npz"
 
 
-def load_transients():
+def load_transients(path=None):
     import json
     from neospice_b200.workloads import Netlist
-    z = np.load(TRAN_PATH)
+    z = np.load(path or TRAN_PATH)
     out = []
     for k in range(int(z["count"])):
         p = f"t{k:02d}_"
@@ -93,7 +93,7 @@ def load_sens():
 def param_starts(netlist):
     """(kind, first parameter index) of every device of a Netlist, in
     creation order (the layout of Circuit.params())."""
-    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 2, "M": 43}
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 10, "M": 43}
     out, at = [], 0
     for d in netlist.devices:
         k = d[0]

@@ -115,16 +115,44 @@ def test_capacitor_and_wave_sources_params_order():
     assert c.info()["num_vars"] == 4  # 3 nodes + the V branch
 
 
-def test_tran_batch_rejects_diodes_and_bad_probes():
+def test_diode_param_block():
+    """DIOtemp at the nominal temperature: the junction potential and
+    capacitance come back (to rounding) as given, F1..F3 follow their
+    definitions, and the grading (M > 0.9) and junction-potential
+    (FC*VJ > 1) limits apply."""
+    from neospice_b200 import _lib as L
+    from neospice_b200.circuit import diode_params
+    p = diode_params(1e-14, 1.5, 2e-12, 0.8, 0.4, 0.5, 5e-9)
+    assert p[0] == 1e-14 and p[1] == 1.5 and p[9] == 5e-9 and p[8] == 0.4
+    np.testing.assert_allclose(p[2], 2e-12, rtol=1e-12)
+    np.testing.assert_allclose(p[3], 0.8, rtol=1e-12)
+    np.testing.assert_allclose(p[4], 0.4, rtol=1e-12)
+    xfc = np.log(1 - 0.5)
+    np.testing.assert_allclose(p[5], p[3] * (1 - np.exp((1 - 0.4) * xfc)) / (1 - 0.4), rtol=1e-14)
+    np.testing.assert_allclose(p[6], np.exp(1.4 * xfc), rtol=1e-14)
+    np.testing.assert_allclose(p[7], 1 - 0.5 * 1.4, rtol=1e-14)
+    assert diode_params(M=0.95)[8] == 0.9
+    q = diode_params(VJ=2.5, FC=0.5)
+    assert q[3] == 2.0 and q[4] == 1.0
+    d = diode_params()
+    assert d[2] == 0.0 and d[9] == 0.0
+    for bad in (dict(CJO=-1e-12), dict(VJ=0.0), dict(M=1.0), dict(FC=1.0), dict(TT=-1e-9),
+                dict(IS=0.0)):
+        with pytest.raises(L.NsgError):
+            diode_params(**bad)
+
+
+def test_tran_batch_rejects_bad_probes():
+    """Probe validation (diodes, with or without charge, are accepted)."""
     from neospice_b200 import _lib as L
     from neospice_b200.circuit import Circuit, TranBatch
     c = Circuit(2)
     c.R(0, 1, 10.0)
-    c.D(1, -1, 1e-14, 1.0)
+    c.D(1, -1, 1e-14, 1.0, CJO=1e-12, TT=1e-9)
     c.V(0, -1, 1.0)
     c.finalize()
-    with pytest.raises(L.NsgError, match="diodes"):
-        TranBatch([c], 1e-12, 1e-10, [0])
+    with pytest.raises(L.NsgError, match="probe"):
+        TranBatch([c], 1e-12, 1e-10, [5])
     d = Circuit(2)
     d.R(0, 1, 10.0)
     d.C(1, -1, 1e-12)

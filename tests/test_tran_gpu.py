@@ -1,7 +1,11 @@
 """GPU parity of the batched transient against the reference's
 solve_transient (tests/golden/tran_rc.npz, made by the reference itself):
 the same timepoints, node voltages within 1e-9 relative / 1e-12 absolute,
-the same Newton iteration and rejected-step counts."""
+the same Newton iteration and rejected-step counts.  tests/golden/tran_diode.npz
+holds the same record for diodes with junction capacitance and transit
+time."""
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -35,9 +39,9 @@ def _run(cases):
     return res
 
 
-def test_transient_matches_reference():
-    res = _run(CASES)
-    for k, (g, (r, nprobe)) in enumerate(zip(CASES, res)):
+def _check(cases):
+    res = _run(cases)
+    for k, (g, (r, nprobe)) in enumerate(zip(cases, res)):
         assert r["status"] == 0, (k, r)
         assert len(r["time"]) == len(g["times"]), (k, len(r["time"]), len(g["times"]))
         np.testing.assert_allclose(r["time"], g["times"], rtol=1e-12, atol=0, err_msg=f"case {k}")
@@ -45,6 +49,18 @@ def test_transient_matches_reference():
                                    err_msg=f"case {k}")
         assert r["newton_iters"] == int(g["iterations"]), (k, r["newton_iters"], int(g["iterations"]))
         assert r["rejected"] == int(g["rejected"]), (k, r["rejected"], int(g["rejected"]))
+
+
+def test_transient_matches_reference():
+    _check(CASES)
+
+
+def test_transient_diodes_match_reference():
+    """DIOload's charge storage (depletion below and above the FC*VJ knee,
+    diffusion charge TT*Id), its predictor and the truncation error of the
+    junction charge: timepoints, waveforms and counts as the reference's."""
+    _check(golden_cases.load_transients(
+        pathlib.Path(__file__).resolve().parent / "golden" / "tran_diode.npz"))
 
 
 def test_transient_single_instances_match_batch():
