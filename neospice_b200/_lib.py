@@ -101,6 +101,7 @@ SIGNATURES = {
     "nsg_circuit_add_mosfet": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,
                                        c_double]),
     "nsg_dc_batch_set_reorder": (c_int, [c_void_p, c_int]),
+    "nsg_dc_batch_set_first_aid": (c_int, [c_void_p, c_int]),
     "nsg_dc_batch_reorders": (c_int, [c_void_p, P(c_ll)]),
     "nsg_dc_batch_methods": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "nsg_dc_batch_adjoint": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -36,7 +36,7 @@ struct nsg_dc_batch {
     std::vector<double> host_params;
     long long updates = 0, nnz_lu = 0, nnz = 0, n = 0;
     int max_col = 0, max_n = 0;
-    nsg::NewtonOptions opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, 0};
+    nsg::NewtonOptions opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, nsg::kAidDirect};
     int32_t* d_lu_pool = nullptr;
     nsg::PlanDesc* d_plans = nullptr;
     int32_t* d_prog = nullptr;
@@ -530,6 +530,15 @@ int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, doubl
     b->opt.abstol = abstol;
     b->opt.gmin = gmin;
     b->opt.max_iter = max_iter;
+    b->drop_graph();  // the captured launch holds the options by value
+    return NSG_OK;
+}
+
+int nsg_dc_batch_set_first_aid(nsg_dc_batch* b, int aid) {
+    if (!b || (aid != nsg::kAidDirect && aid != nsg::kAidSource && aid != nsg::kAidGain))
+        return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_first_aid: bad arguments");
+    b->opt.first_aid = aid;
+    b->drop_graph();
     return NSG_OK;
 }
 

@@ -74,7 +74,7 @@ struct nsg_tran_batch {
     double* d_x0 = nullptr;
     std::vector<char> adjoint_ok;
     std::vector<int64_t> param_count;
-    nsg::NewtonOptions adj_opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, 0};
+    nsg::NewtonOptions adj_opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, nsg::kAidDirect};
     int adj_max_iter = 100;
     double* d_adj_ws = nullptr;
     int64_t adj_ws_cap = 0;
@@ -140,7 +140,7 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         b->count = count;
         if (threads <= 0) threads = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
         auto& o = b->opt;
-        o.nopt = nsg::NewtonOptions{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, 0};
+        o.nopt = nsg::NewtonOptions{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, nsg::kAidDirect};
         o.tstep = tstep;
         o.tstop = tstop;
         // transient.cpp:818-821: maxStep = min(tstep, tstop/50), dt_min = maxStep*1e-11

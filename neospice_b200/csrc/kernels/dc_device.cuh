@@ -48,8 +48,12 @@ struct NewtonOptions {
     double gmin;       // device gmin and dead-node pin
     double diag_gmin;  // solver diagonal regularisation
     int32_t max_iter;  // itl1
-    int32_t pad;
+    int32_t first_aid; // where the operating-point cascade starts: kAidDirect (0),
+                       // kAidSource (source stepping), kAidGain (gain stepping)
+    double src_fact = 1.0;  // independent-source scale (SimOptions::src_fact)
 };
+
+enum : int32_t { kAidDirect = 0, kAidSource = 1, kAidGain = 2 };
 
 constexpr int kDiodeTermCount = 5;
 constexpr int kCapTermCount = 4;
@@ -79,7 +83,9 @@ struct SolverState {
 };
 
 // Operating-point phases (kernels/dc_op.cuh): the direct attempt, true gmin
-// stepping and its final solve, diagonal gmin stepping and its final solve.
+// stepping and its final solve, diagonal gmin stepping and its final solve,
+// then source (or gain) stepping: the solve at zero sources, its diagonal
+// gmin ramp, the ramp of the source fraction.
 enum DcOpPhase : int32_t {
     kOpDirect = 0,
     kOpTrueGmin = 1,
@@ -87,6 +93,9 @@ enum DcOpPhase : int32_t {
     kOpDiagGmin = 3,
     kOpDiagGminFinal = 4,
     kOpDone = 5,
+    kOpSrcFirst = 6,
+    kOpSrcZeroGmin = 7,
+    kOpSrcStep = 8,
 };
 
 // Operating-point controller of one instance, kept in global memory across
@@ -96,6 +105,11 @@ struct DcCtl {
     int32_t active, r_iter, r_mode, r_devconv;  // Newton resume record
     int32_t action, solves, method, pad;  // method: ConvergenceMethod of the result
     double cur, factor, old, numeric_diag_gmin;  // stepping gmin, factor, OldGmin; diag_gmin of a stopped numeric()
+    // source / gain stepping: accepted fraction, step, fraction under
+    // solve, diag_gmin of the zero-source ramp; ramp index, the failed first
+    // solve's iterations, 1 for gain stepping (sources unscaled)
+    double frac, step, next, zdiag;
+    int32_t zi, r0_iters, gain, pad2;
 };
 
 enum : int32_t { kActNone = 0, kActZeroSave = 1, kActSave = 2, kActRestore = 3 };

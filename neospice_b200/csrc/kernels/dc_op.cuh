@@ -1,9 +1,13 @@
 // DC operating point of one instance with the reference's continuation
 // aids, as a resumable state machine: the direct Newton attempt, then true
 // gmin stepping (device gmin, solve_dc only) and diagonal gmin stepping
-// (true_gmin_stepping / gmin_stepping, src/core/convergence.cpp:216-469,
-// called from solve_dc, src/core/dc.cpp:53-175, and from the transient's
-// compute_dc_operating_point, src/core/transient.cpp:145-205).
+// (true_gmin_stepping / gmin_stepping, src/core/convergence.cpp:216-469),
+// source stepping (source_stepping, convergence.cpp:471-581) and, for
+// solve_dc, gain stepping (gain_stepping, convergence.cpp:583-703: the same
+// ramp over the dependent-source gains, of which this device set has none,
+// so the sources stay unscaled) — called from solve_dc, src/core/dc.cpp:53-217,
+// and from the transient's compute_dc_operating_point,
+// src/core/transient.cpp:145-205.
 //
 // The controller lives in global memory (DcCtl) so that an instance whose
 // pivots fail re-validation can stop (kStatusReorder), be re-ordered on the
@@ -32,7 +36,22 @@ __device__ inline void dc_op_copy(const Inst& v, int32_t n_states, double* save,
     }
 }
 
-__host__ __device__ inline void dc_op_start(DcCtl* c, int firstmode) {
+// Thread 0: source (gain = 0) or gain (gain = 1) stepping from a zero guess
+// and cleared states, starting with the solve at fraction 0.
+__host__ __device__ inline void dc_op_begin_source(DcCtl* c, int gain, int firstmode) {
+    c->phase = kOpSrcFirst;
+    c->gain = gain;
+    c->frac = 0.0;
+    c->step = 0.001;
+    c->next = 0.0;
+    c->total = 0;
+    c->ctx_mode = firstmode;
+    c->action = kActZeroSave;
+}
+
+// first_aid: kAidDirect runs the whole cascade; kAidSource / kAidGain run
+// source / gain stepping alone (the instance's x and states are zero then).
+__host__ __device__ inline void dc_op_start(DcCtl* c, int firstmode, int first_aid = kAidDirect) {
     c->phase = kOpDirect;
     c->total = 0;
     c->code = kDcNoConvergence;
@@ -41,6 +60,17 @@ __host__ __device__ inline void dc_op_start(DcCtl* c, int firstmode) {
     c->action = kActNone;
     c->solves = 0;
     c->method = 0;
+    if (first_aid == kAidSource || first_aid == kAidGain) {
+        dc_op_begin_source(c, first_aid == kAidGain ? 1 : 0, firstmode);
+        c->action = kActNone;
+    }
+}
+
+// Thread 0: the next fraction of source stepping (fraction + step, at most 1).
+__host__ __device__ inline void dc_op_next_fraction(DcCtl* c) {
+    double next = c->frac + c->step;
+    if (next > 1.0) next = 1.0;
+    c->next = next;
 }
 
 // Thread 0: start a stepping method from a zero guess and cleared states.
@@ -70,7 +100,8 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
     // the minimum factor would otherwise run for hours.
     constexpr int kMaxSolves = 20000;
     __shared__ int32_t s_phase, s_active, s_r_iter, s_r_devconv, s_entry_mode, s_action, s_code;
-    __shared__ double s_cur;
+    __shared__ int32_t s_gain;
+    __shared__ double s_cur, s_next, s_zdiag;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -81,6 +112,9 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
             s_r_devconv = ctl->r_devconv;
             s_entry_mode = ctl->ctx_mode;
             s_cur = ctl->cur;
+            s_gain = ctl->gain;
+            s_next = ctl->next;
+            s_zdiag = ctl->zdiag;
             ctx->mode = ctl->active ? ctl->r_mode : ctl->ctx_mode;
         }
         __syncthreads();
@@ -96,8 +130,14 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
             max_iter = itl2 > 100 ? itl2 : 100;
         } else if (phase == kOpDiagGminFinal) {
             o.diag_gmin = 0.0;
+        } else if (phase >= kOpSrcFirst) {
+            // SimOptions::src_fact at 0, then the fraction under solve; the
+            // zero-source ramp adds its diag_gmin.  Gain stepping leaves the
+            // sources at full value.
+            if (!s_gain) o.src_fact = (phase == kOpSrcStep) ? s_next : 0.0;
+            if (phase == kOpSrcZeroGmin) o.diag_gmin = s_zdiag;
         }
-        load_constants(v, o.gmin);  // the dead-node pin follows SimOptions::gmin
+        load_constants(v, o.gmin, o.src_fact);  // the dead-node pin follows SimOptions::gmin
         const bool resume = s_active != 0;
         const NewtonOutcome r = newton(v, pd, lu_pool, ctx, o, max_iter, solver, smem, colbuf,
                                        resume ? s_r_iter : -1, s_entry_mode,
@@ -119,12 +159,91 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
             DcCtl& c = *ctl;
             c.active = 0;
             c.action = kActNone;
-            c.method = (phase == kOpDirect) ? 0 : 1;  // DIRECT / GMIN_STEPPING
+            // DIRECT / GMIN_STEPPING / SOURCE_STEPPING (ConvergenceMethod,
+            // src/core/sim_status.hpp:10-17; gain stepping reports SOURCE_STEPPING)
+            c.method = (phase == kOpDirect) ? 0 : (phase >= kOpSrcFirst ? 2 : 1);
             const bool final_ok = conv && (phase == kOpDirect || phase == kOpTrueGminFinal ||
-                                           phase == kOpDiagGminFinal);
+                                           phase == kOpDiagGminFinal ||
+                                           (phase == kOpSrcStep && c.next >= 1.0));
+            // After source stepping fails: gain stepping in solve_dc, the
+            // end of the cascade in the transient's operating point (the
+            // later aids are not built).  A run started at an aid ends with it.
+            auto source_failed = [&]() {
+                if (true_gmin_first && !c.gain && opt.first_aid == kAidDirect) {
+                    dc_op_begin_source(&c, 1, firstmode);
+                } else {
+                    c.code = kDcNoConvergence;
+                    c.phase = kOpDone;
+                }
+            };
             if (++c.solves >= kMaxSolves && !final_ok) {
                 c.code = kDcNoConvergence;
                 c.phase = kOpDone;
+            } else if (phase == kOpSrcFirst) {
+                c.r0_iters = r.iters;
+                if (conv) {
+                    c.total += r.iters;
+                    c.action = kActSave;
+                    c.ctx_mode = contmode;
+                    c.phase = kOpSrcStep;
+                    dc_op_next_fraction(&c);
+                } else {
+                    // gmin ramp at zero sources: diag_gmin from gmin * 10^10
+                    double diag = opt.gmin;
+                    for (int i = 0; i < 10; ++i) diag *= 10.0;
+                    c.zdiag = diag;
+                    c.zi = 0;
+                    c.action = kActZeroSave;
+                    c.ctx_mode = firstmode;
+                    c.phase = kOpSrcZeroGmin;
+                }
+            } else if (phase == kOpSrcZeroGmin) {
+                if (!conv) {
+                    source_failed();
+                } else {
+                    c.total += r.iters;
+                    c.zdiag /= 10.0;
+                    c.ctx_mode = contmode;
+                    if (c.zi == 10) {
+                        c.total += c.r0_iters;  // the failed solve at zero sources
+                        c.action = kActSave;
+                        c.phase = kOpSrcStep;
+                        dc_op_next_fraction(&c);
+                    } else {
+                        ++c.zi;
+                    }
+                }
+            } else if (phase == kOpSrcStep) {
+                const int quarter = opt.max_iter / 4, half = opt.max_iter / 2;
+                if (conv) {
+                    c.total += r.iters;
+                    c.frac = c.next;
+                    c.action = kActSave;
+                    if (r.iters < quarter) {
+                        const double s = c.step * 1.5;
+                        c.step = (s < 0.1) ? s : 0.1;
+                    } else if (r.iters > half) {
+                        const double s = c.step * 0.5;
+                        c.step = (1e-7 < s) ? s : 1e-7;
+                    }
+                    if (c.frac < 1.0) {
+                        dc_op_next_fraction(&c);
+                    } else {
+                        c.code = kDcConverged;
+                        c.phase = kOpDone;
+                    }
+                } else if (c.step * (1.0 - c.frac) < 1e-8) {
+                    source_failed();
+                } else {
+                    c.action = kActRestore;
+                    c.step *= 0.1;
+                    if (c.step > 0.01) c.step = 0.01;
+                    if (c.step < 1e-7) {
+                        source_failed();
+                    } else {
+                        dc_op_next_fraction(&c);
+                    }
+                }
             } else if (phase == kOpDirect) {
                 if (conv) {
                     c.total = r.iters;
@@ -161,8 +280,7 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
                     if (phase == kOpTrueGmin) {
                         dc_op_begin_stepping(&c, kOpDiagGmin, firstmode);
                     } else {
-                        c.code = kDcNoConvergence;
-                        c.phase = kOpDone;
+                        dc_op_begin_source(&c, 0, firstmode);
                     }
                 } else {
                     c.factor = sqrt(sqrt(c.factor));
@@ -177,8 +295,7 @@ __device__ inline int32_t dc_operating_point(const Inst& v, int32_t n_states, co
                 } else if (phase == kOpTrueGminFinal) {
                     dc_op_begin_stepping(&c, kOpDiagGmin, firstmode);
                 } else {
-                    c.code = kDcNoConvergence;
-                    c.phase = kOpDone;
+                    dc_op_begin_source(&c, 0, firstmode);
                 }
             }
             s_action = c.action;

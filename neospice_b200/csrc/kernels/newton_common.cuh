@@ -125,10 +125,15 @@ __device__ __forceinline__ double term_value(int32_t op, double p, double gmin) 
 }
 
 // Constant term values, diode constants (csat, vte, Vcrit at T = TNOM).
-__device__ inline void load_constants(const Inst& v, double gmin) {
+// DC source values are scaled by src_fact as VSource / ISource::evaluate do
+// (vsource.cpp:208-209, isource.cpp:173-176): the value times the factor,
+// then its negation where the stamp subtracts it.
+__device__ inline void load_constants(const Inst& v, double gmin, double src_fact = 1.0) {
     for (int32_t k = threadIdx.x; k < v.n_const; k += blockDim.x) {
         const int32_t pi = v.term_param[k];
-        v.tv[k] = term_value(v.term_op[k], pi >= 0 ? v.par[pi] : 0.0, gmin);
+        const int32_t op = v.term_op[k];
+        const double p = pi >= 0 ? v.par[pi] : 0.0;
+        v.tv[k] = (op == 2) ? p * src_fact : (op == 3) ? -(p * src_fact) : term_value(op, p, gmin);
     }
     for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
         const int32_t pi = v.diodes[4 * k + 2];
@@ -290,7 +295,7 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
     }
     for (int32_t k = threadIdx.x; k < v.n_srcs; k += blockDim.x) {
         const int32_t* sr = v.srcs + 4 * k;
-        const double val = wave_value(sr[1], v.par + sr[2], sr[3], c.time);
+        const double val = wave_value(sr[1], v.par + sr[2], sr[3], c.time) * opt.src_fact;
         tv_s[kSrcTermCount * k] = val;
         tv_s[kSrcTermCount * k + 1] = -val;
     }

@@ -50,7 +50,7 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;
     }
     if (threadIdx.x == 0) {
-        if (fresh) dc_op_start(ctl, kFirst);
+        if (fresh) dc_op_start(ctl, kFirst, opt.first_aid);
         ctx = IntegCtx{};
         ctx.order = 1;
         ctx.time = 0.0;

@@ -212,7 +212,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         for (int32_t i = threadIdx.x; i < 4 * d.n_states; i += blockDim.x) v.st[0][i] = 0.0;
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) v.x[i] = 0.0;
         if (threadIdx.x == 0) {
-            dc_op_start(&k.dc, kFirst);
+            dc_op_start(&k.dc, kFirst, o.nopt.first_aid);
             k.ctx = IntegCtx{};
             k.ctx.order = 1;
             k.ctx.method = o.use_gear;

@@ -168,6 +168,43 @@ def inverter_chain(stages: int, vin=0.0, vdd=1.8, c_load=10e-15, pulse=None) -> 
     return Netlist(stages + 2, dev, models)
 
 
+def inverter_ring(stages: int, vdd=1.8, lam=0.0, c_load=10e-15) -> Netlist:
+    """A ring of `stages` CMOS inverters (level-1 cards of inverter_chain,
+    optional channel-length modulation), each output loaded by c_load; node
+    0 is VDD, node i the output of stage i (driven by stage i-1)."""
+    dev = [("V", 0, GND, vdd)]
+    for i in range(stages):
+        inp, out = 1 + (i - 1) % stages, 1 + i
+        dev += [("M", out, inp, GND, GND, "nch", 2e-6, 1e-6), ("M", out, inp, 0, 0, "pch", 4e-6, 1e-6),
+                ("C", out, GND, c_load)]
+    pn, pp = {"VTO": 0.7, "KP": 1.1e-4}, {"VTO": -0.7, "KP": 5e-5}
+    if lam:
+        pn["LAMBDA"] = pp["LAMBDA"] = lam
+    return Netlist(stages + 1, dev, {"nch": ("nmos", pn), "pch": ("pmos", pp)})
+
+
+def diode_grid(rng: np.random.Generator, side: int, vdd=1.0) -> Netlist:
+    """A side x side resistor grid as a Netlist: R ~ lognormal(ln 1k, 0.1),
+    diodes (IS 1e-14, N 1) from a seeded 10% of the nodes to ground, 0-1 mA
+    current sources into 5%, a source of vdd at node 0."""
+    n = side * side
+    dev = [("V", 0, GND, vdd)]
+    for y in range(side):
+        for x in range(side):
+            k = y * side + x
+            if x + 1 < side:
+                dev.append(("R", k, k + 1, float(rng.lognormal(np.log(1e3), 0.1))))
+            if y + 1 < side:
+                dev.append(("R", k, k + side, float(rng.lognormal(np.log(1e3), 0.1))))
+    for k in range(1, n):
+        u = rng.random()
+        if u < 0.10:
+            dev.append(("D", k, GND, 1e-14, 1.0))
+        elif u < 0.15:
+            dev.append(("I", GND, k, float(rng.uniform(0.0, 1e-3))))
+    return Netlist(n, dev)
+
+
 def mos_network(rng: np.random.Generator, nodes: int, vdd=1.8, pulse=None) -> Netlist:
     """A seeded MOS network: VDD on node 0, an input on node 1 (a random DC
     level, or a PULSE), and for every further node an NMOS pull-down and a

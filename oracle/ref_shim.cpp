@@ -37,6 +37,7 @@
 #include "solver/element.hpp"
 
 #include "core/amd.hpp"
+#include "core/convergence.hpp"
 
 #define private public
 #include "core/neo_solver.hpp"
@@ -511,7 +512,24 @@ void* nsref_sim_run(const char* desc, int analysis, double tstep, double tstop) 
         build_from_desc(ckt, desc);
         res->num_nodes = ckt.num_nodes();
         res->num_vars = ckt.num_vars();
-        if (analysis == 0) {
+        if (analysis == 2 || analysis == 3) {
+            // The reference's source_stepping (2) or gain_stepping (3) run
+            // directly, set up as solve_dc sets up its cascade (dc.cpp:80-96,
+            // 176-196): solver, symbolic, options published, MODEDCOP |
+            // MODEINITJCT, zero guess.
+            const int32_t n = ckt.num_vars();
+            std::vector<double> solution(n, 0.0);
+            auto solver = make_solver(n, ckt.is_linear());
+            solver->symbolic(ckt.pattern());
+            ckt.integrator_ctx.options = &ckt.options;
+            ckt.integrator_ctx.mode = 0x10 | 0x200;
+            NewtonResult r = analysis == 2 ? source_stepping(ckt, *solver, solution, ckt.options)
+                                           : gain_stepping(ckt, *solver, solution, ckt.options);
+            res->times.push_back(0.0);
+            res->values = solution;
+            res->iterations = r.iterations;
+            res->method = r.converged ? 2 : -1;
+        } else if (analysis == 0) {
             DCResult r = solve_dc(ckt);
             const auto* op = ckt.operating_point();
             if (!op) throw std::runtime_error("no operating point");

@@ -19,6 +19,12 @@ tran_diode.npz: the same record for diode circuits with junction capacitance
 and transit time (rectifier, reverse recovery, seeded diode-RC networks,
 DIOtemp's grading and junction-potential limits).
 
+dc_aids.npz: the reference's source_stepping and gain_stepping run alone
+(as solve_dc runs them after the gmin steppings fail) on inverter chains,
+MOS networks, diode-loaded resistor grids and inverter rings; per case the
+netlist, the aid, the solution, the Newton iterations and whether it
+converged.
+
 mos_dc.npz: CMOS inverter chains and seeded MOS networks, per case the
 netlist (JSON) and the reference's solve_dc operating point, Newton
 iteration count and convergence method (0 direct, 1 gmin stepping).
@@ -159,11 +165,7 @@ def tran_netlists():
 
 
 def mos_netlists():
-    """DC cases of tran_diode.npz: the same record for diode circuits with junction capacitance
-and transit time (rectifier, reverse recovery, seeded diode-RC networks,
-DIOtemp's grading and junction-potential limits).
-
-mos_dc.npz: CMOS inverter chains at several input levels
+    """DC cases of mos_dc.npz: CMOS inverter chains at several input levels
     (the longer ones need gmin stepping) and seeded MOS networks with body
     effect, channel-length modulation and oxide-derived parameters."""
     from neospice_b200 import workloads as W
@@ -190,6 +192,37 @@ def mos_main():
     path = pathlib.Path(__file__).with_name("mos_dc.npz")
     np.savez_compressed(path, **rec)
     print(f"wrote {len(cases)} MOS operating points to {path}")
+
+
+def aid_netlists():
+    """(netlist, analysis) cases of dc_aids.npz: the reference's
+    source_stepping (2) and gain_stepping (3) run alone on inverter chains,
+    seeded MOS networks, diode-loaded resistor grids, and inverter rings with
+    channel-length modulation on which both aids fail."""
+    from neospice_b200 import workloads as W
+    nets = [W.inverter_chain(s, v) for s, v in ((1, 0.0), (3, 0.9), (5, 1.3), (9, 0.0), (25, 1.8))]
+    nets += [W.mos_network(np.random.default_rng([43, k]), int(5 + 3 * k)) for k in range(4)]
+    nets += [W.diode_grid(np.random.default_rng([44, k]), s) for k, s in enumerate((4, 7, 10))]
+    nets += [W.inverter_ring(9, 1.8, 0.05), W.inverter_ring(13, 3.3, 0.05)]
+    return [(nl, an) for an in (2, 3) for nl in nets]
+
+
+def aid_main():
+    import json
+    import netlists
+    rec = {}
+    cases = aid_netlists()
+    for k, (nl, an) in enumerate(cases):
+        _, v, info = oracle.ref_sim(netlists.ref_desc(nl), an)
+        p = f"a{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "aid": np.int32(an), p + "solution": v[0],
+                    p + "iterations": np.int32(info["iterations"]),
+                    p + "converged": np.int32(info["method"] == 2)})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("dc_aids.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} source / gain stepping runs to {path}")
 
 
 def sens_netlists():
@@ -445,7 +478,8 @@ def amd_main():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "sens", "amd", "linear"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "aids", "sens", "amd",
+                             "linear"]
     if "amd" in which:
         amd_main()
     if "linear" in which:
@@ -460,5 +494,7 @@ if __name__ == "__main__":
         tran_main("trandiode")
     if "mos" in which:
         mos_main()
+    if "aids" in which:
+        aid_main()
     if "sens" in which:
         sens_main()

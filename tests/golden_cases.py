@@ -54,6 +54,26 @@ def load_transients(path=None):
     return out
 
 
+AIDS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "dc_aids.npz"
+
+
+def load_aids():
+    """Source / gain stepping runs of the reference (dc_aids.npz): netlist,
+    aid (2 source, 3 gain), solution, iterations, converged."""
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(AIDS_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"a{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        out.append(d)
+    return out
+
+
 MOS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "mos_dc.npz"
 
 
