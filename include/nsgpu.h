@@ -316,23 +316,25 @@ int nsg_dc_batch_instance_stats(const nsg_dc_batch* b, long long* n, long long* 
  * 1e-12, 1e-12, 100; src/core/types.hpp:24-66). */
 int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, double abstol,
                              double gmin, int max_iter);
-/* Which of solve_dc's aids (src/core/dc.cpp:53-217) each instance's
+/* Which of solve_dc's aids (src/core/dc.cpp:53-242) each instance's
  * operating point runs.  NSG_AID_DIRECT (default): the cascade — the direct
  * attempt, true gmin stepping, gmin stepping, source stepping, gain
- * stepping.  NSG_AID_SOURCE / NSG_AID_GAIN: source_stepping /
- * gain_stepping (src/core/convergence.cpp:471-703) alone from the zero
- * guess, as solve_dc runs them after the direct attempt and both gmin
- * steppings fail (gain stepping scales dependent-source gains, which these
- * circuits do not have, so it ramps a fraction with the sources at full
- * value).  d_iterations then counts that aid's Newton iterations. */
+ * stepping, pseudo-transient continuation.  NSG_AID_SOURCE / NSG_AID_GAIN /
+ * NSG_AID_PSEUDO_TRANSIENT: source_stepping / gain_stepping /
+ * pseudo_transient (src/core/convergence.cpp:471-703, 986-1097) alone from
+ * the zero guess, as solve_dc runs them after the earlier aids fail (gain
+ * stepping scales dependent-source gains, which these circuits do not have,
+ * so it ramps a fraction with the sources at full value).  d_iterations
+ * then counts that aid's Newton iterations. */
 #define NSG_AID_DIRECT 0
 #define NSG_AID_SOURCE 1
 #define NSG_AID_GAIN 2
+#define NSG_AID_PSEUDO_TRANSIENT 3
 int nsg_dc_batch_set_first_aid(nsg_dc_batch* b, int aid);
 /* Run every instance to convergence.  d_params: packed parameters (device;
  * NULL = the circuits' own values); d_solutions: packed solutions (device),
  * the returned iterate as newton_solve returns it; d_status: 0 converged,
- * 1 no convergence (the direct attempt, gmin, source and gain stepping failed), 102 singular, 103 pivot re-validation
+ * 1 no convergence (every aid failed), 102 singular, 103 pivot re-validation
  * failed, 104 a bounded wait gave up; d_iterations: Newton iterations. */
 int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solutions, int* d_status,
                      int* d_iterations, void* stream);

@@ -24,7 +24,7 @@ GND = -1
 
 
 # Operating-point aids a DC batch may start at (nsg_dc_batch_set_first_aid).
-AIDS = {"direct": 0, "source": 1, "gain": 2}
+AIDS = {"direct": 0, "source": 1, "gain": 2, "ptc": 3}
 
 def diode_params(IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0, VJ: float = 1.0,
                  M: float = 0.5, FC: float = 0.5, TT: float = 0.0) -> np.ndarray:
@@ -214,7 +214,8 @@ class DcBatch:
 
     def set_first_aid(self, aid: str):
         """Run every operating point through "direct" (the whole cascade of
-        aids), or "source" / "gain" (source or gain stepping alone)."""
+        aids), or "source" / "gain" / "ptc" (source stepping, gain stepping or
+        pseudo-transient continuation alone)."""
         L.check(L.lib().nsg_dc_batch_set_first_aid(self._h, AIDS[aid]))
 
     def reorders(self) -> int:

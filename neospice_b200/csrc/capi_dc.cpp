@@ -535,7 +535,7 @@ int nsg_dc_batch_set_options(nsg_dc_batch* b, double reltol, double vntol, doubl
 }
 
 int nsg_dc_batch_set_first_aid(nsg_dc_batch* b, int aid) {
-    if (!b || (aid != nsg::kAidDirect && aid != nsg::kAidSource && aid != nsg::kAidGain))
+    if (!b || aid < nsg::kAidDirect || aid > nsg::kAidPseudoTransient)
         return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_first_aid: bad arguments");
     b->opt.first_aid = aid;
     b->drop_graph();

@@ -49,11 +49,14 @@ struct NewtonOptions {
     double diag_gmin;  // solver diagonal regularisation
     int32_t max_iter;  // itl1
     int32_t first_aid; // where the operating-point cascade starts: kAidDirect (0),
-                       // kAidSource (source stepping), kAidGain (gain stepping)
+                       // kAidSource (source stepping), kAidGain (gain stepping),
+                       // kAidPseudoTransient
     double src_fact = 1.0;  // independent-source scale (SimOptions::src_fact)
+    int32_t want_residual = 0;  // report NewtonResult::residual (pseudo-transient)
+    int32_t pad = 0;
 };
 
-enum : int32_t { kAidDirect = 0, kAidSource = 1, kAidGain = 2 };
+enum : int32_t { kAidDirect = 0, kAidSource = 1, kAidGain = 2, kAidPseudoTransient = 3 };
 
 constexpr int kDiodeTermCount = 5;
 constexpr int kCapTermCount = 4;
@@ -96,6 +99,9 @@ enum DcOpPhase : int32_t {
     kOpSrcFirst = 6,
     kOpSrcZeroGmin = 7,
     kOpSrcStep = 8,
+    kOpPtc = 9,        // pseudo-transient: a step at diag_gmin = C/dt
+    kOpPtcProbe = 10,  // the probe solve at the target diag_gmin
+    kOpPtcFinal = 11,  // the final attempt after the step loop
 };
 
 // Operating-point controller of one instance, kept in global memory across
@@ -110,6 +116,10 @@ struct DcCtl {
     // solve's iterations, 1 for gain stepping (sources unscaled)
     double frac, step, next, zdiag;
     int32_t zi, r0_iters, gain, pad2;
+    // pseudo-transient: pseudo timestep, previous residual (-1: none), the
+    // probe threshold on C/dt; step index
+    double ptc_dt, ptc_prev, ptc_probe;
+    int32_t ptc_k, pad3;
 };
 
 enum : int32_t { kActNone = 0, kActZeroSave = 1, kActSave = 2, kActRestore = 3 };

@@ -348,7 +348,31 @@ struct NewtonOutcome {
     int32_t fail_iter;  // kStatusReorder / kStatusNeedOrder: the 0-based iteration that stopped,
     int32_t fail_mode;  // the mode it ran in
     int32_t fail_dev_conv;  // and its device-load convergence verdict
+    double residual;        // opt.want_residual: max |rhs| over the node rows of the last load
 };
+
+// newton.cpp:199-208: the largest |rhs[i]| over the node rows of the
+// assembled right-hand side (in x, before the solve overwrites it); a NaN
+// row never wins.  Whole CTA; every thread gets the value.
+static __device__ __noinline__ double rhs_residual(const Inst& v) {
+    __shared__ double s_resid[32];
+    double m = 0.0;
+    for (int32_t i = threadIdx.x; i < v.num_nodes; i += blockDim.x) {
+        const double r = fabs(v.x[i]);
+        if (r > m) m = r;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_xor_sync(0xffffffffu, m, off);
+        if (o > m) m = o;
+    }
+    if ((threadIdx.x & 31) == 0) s_resid[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w)
+        if (s_resid[w] > m) m = s_resid[w];
+    __syncthreads();
+    return m;
+}
 
 // newton_solve (src/core/newton.cpp:51-419) for the whole CTA: x holds the
 // initial guess and receives the solution (the previous iterate on
@@ -377,7 +401,8 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
     __shared__ int32_t s_conv, s_dev_conv;
     if (saved_mode < 0) saved_mode = ctx->mode;
     bool force_numeric = false;
-    NewtonOutcome out{kDcNoConvergence, max_iter, -1, 0, 1};
+    NewtonOutcome out{kDcNoConvergence, max_iter, -1, 0, 1, 0.0};
+    double residual = 0.0;
     // Small instances keep the LU in shared memory (warp-level refactor and
     // sweeps); larger ones use the dataflow schedule over global memory.
     const bool small = small_fits(pd.n, pd.nnz_lu, smem_doubles);
@@ -397,6 +422,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
         __syncthreads();
         assemble(v);
         __syncthreads();
+        if (opt.want_residual) residual = rhs_residual(v);
 
         const int mode = ctx->mode;
         const bool numeric = resumed || force_numeric || (mode & kModeInitJct) || !solver->factored;
@@ -506,6 +532,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
     }
     if (threadIdx.x == 0) ctx->mode = saved_mode;
     __syncthreads();
+    out.residual = residual;
     return out;
 }
 

@@ -360,9 +360,9 @@ def ref_sim_sens(desc: str, output_node: int):
 
 def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0):
     """Run a circuit description (see nsref_sim_run in ref_shim.cpp) through
-    the reference: analysis 0 = DC operating point, 1 = transient, 2 / 3 =
-    the reference's source_stepping / gain_stepping alone (info["method"] 2
-    when it converged, -1 when not).  Returns (times, values [npoints x
+    the reference: analysis 0 = DC operating point, 1 = transient, 2 / 3 / 4
+    = the reference's source_stepping / gain_stepping / pseudo_transient
+    alone (info["method"] 2, 2, 3 when it converged, -1 when not).  Returns (times, values [npoints x
     width], info dict)."""
     lib = ref()
     h = lib.nsref_sim_run(desc.encode(), int(analysis), float(tstep), float(tstop))
@@ -373,7 +373,7 @@ def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0
                                 ctypes.addressof(it), ctypes.addressof(sec), ctypes.addressof(rej))
         if rc != 0:
             raise RuntimeError("reference failed: " + lib.nsref_sim_error(h).decode())
-        width = nv.value if analysis in (0, 2, 3) else nn.value
+        width = nv.value if analysis in (0, 2, 3, 4) else nn.value
         times = np.zeros(npts.value)
         values = np.zeros((npts.value, width))
         lib.nsref_sim_copy(h, _p(times), _p(values))

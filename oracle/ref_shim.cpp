@@ -512,23 +512,25 @@ void* nsref_sim_run(const char* desc, int analysis, double tstep, double tstop) 
         build_from_desc(ckt, desc);
         res->num_nodes = ckt.num_nodes();
         res->num_vars = ckt.num_vars();
-        if (analysis == 2 || analysis == 3) {
-            // The reference's source_stepping (2) or gain_stepping (3) run
-            // directly, set up as solve_dc sets up its cascade (dc.cpp:80-96,
-            // 176-196): solver, symbolic, options published, MODEDCOP |
-            // MODEINITJCT, zero guess.
+        if (analysis == 2 || analysis == 3 || analysis == 4) {
+            // The reference's source_stepping (2), gain_stepping (3) or
+            // pseudo_transient (4) run directly, set up as solve_dc sets up
+            // its cascade (dc.cpp:80-96, 176-224): solver, symbolic, options
+            // published, MODEDCOP | MODEINITJCT, zero guess.
             const int32_t n = ckt.num_vars();
             std::vector<double> solution(n, 0.0);
             auto solver = make_solver(n, ckt.is_linear());
             solver->symbolic(ckt.pattern());
             ckt.integrator_ctx.options = &ckt.options;
             ckt.integrator_ctx.mode = 0x10 | 0x200;
-            NewtonResult r = analysis == 2 ? source_stepping(ckt, *solver, solution, ckt.options)
-                                           : gain_stepping(ckt, *solver, solution, ckt.options);
+            NewtonResult r =
+                analysis == 2 ? source_stepping(ckt, *solver, solution, ckt.options)
+                : analysis == 3 ? gain_stepping(ckt, *solver, solution, ckt.options)
+                                : pseudo_transient(ckt, *solver, solution, ckt.options);
             res->times.push_back(0.0);
             res->values = solution;
             res->iterations = r.iterations;
-            res->method = r.converged ? 2 : -1;
+            res->method = r.converged ? (analysis == 4 ? 3 : 2) : -1;
         } else if (analysis == 0) {
             DCResult r = solve_dc(ckt);
             const auto* op = ckt.operating_point();

@@ -19,8 +19,8 @@ tran_diode.npz: the same record for diode circuits with junction capacitance
 and transit time (rectifier, reverse recovery, seeded diode-RC networks,
 DIOtemp's grading and junction-potential limits).
 
-dc_aids.npz: the reference's source_stepping and gain_stepping run alone
-(as solve_dc runs them after the gmin steppings fail) on inverter chains,
+dc_aids.npz: the reference's source_stepping, gain_stepping and
+pseudo_transient run alone (as solve_dc runs them after the earlier aids fail) on inverter chains,
 MOS networks, diode-loaded resistor grids and inverter rings; per case the
 netlist, the aid, the solution, the Newton iterations and whether it
 converged.
@@ -196,15 +196,16 @@ def mos_main():
 
 def aid_netlists():
     """(netlist, analysis) cases of dc_aids.npz: the reference's
-    source_stepping (2) and gain_stepping (3) run alone on inverter chains,
-    seeded MOS networks, diode-loaded resistor grids, and inverter rings with
-    channel-length modulation on which both aids fail."""
+    source_stepping (2), gain_stepping (3) and pseudo_transient (4) run
+    alone on inverter chains, seeded MOS networks, diode-loaded resistor
+    grids, and inverter rings with channel-length modulation on which the
+    aids fail."""
     from neospice_b200 import workloads as W
     nets = [W.inverter_chain(s, v) for s, v in ((1, 0.0), (3, 0.9), (5, 1.3), (9, 0.0), (25, 1.8))]
     nets += [W.mos_network(np.random.default_rng([43, k]), int(5 + 3 * k)) for k in range(4)]
     nets += [W.diode_grid(np.random.default_rng([44, k]), s) for k, s in enumerate((4, 7, 10))]
     nets += [W.inverter_ring(9, 1.8, 0.05), W.inverter_ring(13, 3.3, 0.05)]
-    return [(nl, an) for an in (2, 3) for nl in nets]
+    return [(nl, an) for an in (2, 3, 4) for nl in nets]
 
 
 def aid_main():
@@ -218,11 +219,11 @@ def aid_main():
         rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
                     p + "aid": np.int32(an), p + "solution": v[0],
                     p + "iterations": np.int32(info["iterations"]),
-                    p + "converged": np.int32(info["method"] == 2)})
+                    p + "converged": np.int32(info["method"] >= 0)})
     rec["count"] = np.int32(len(cases))
     path = pathlib.Path(__file__).with_name("dc_aids.npz")
     np.savez_compressed(path, **rec)
-    print(f"wrote {len(cases)} source / gain stepping runs to {path}")
+    print(f"wrote {len(cases)} source / gain stepping and pseudo-transient runs to {path}")
 
 
 def sens_netlists():

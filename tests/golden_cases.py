@@ -58,8 +58,9 @@ AIDS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "dc_aids.npz"
 
 
 def load_aids():
-    """Source / gain stepping runs of the reference (dc_aids.npz): netlist,
-    aid (2 source, 3 gain), solution, iterations, converged."""
+    """Source / gain stepping and pseudo-transient runs of the reference
+    (dc_aids.npz): netlist, aid (2 source, 3 gain, 4 pseudo-transient),
+    solution, iterations, converged."""
     import json
     from neospice_b200.workloads import Netlist
     z = np.load(AIDS_PATH)

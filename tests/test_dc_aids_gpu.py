@@ -1,9 +1,11 @@
-"""GPU parity of the operating point's source and gain stepping against the
-reference's own source_stepping / gain_stepping run alone
-(tests/golden/dc_aids.npz): converged or not as the reference, solutions
-within 1e-9 relative / 1e-12 absolute, the same Newton iteration count
-(the aid's total, including the failed solve at zero sources and the
-diagonal-gmin ramp that rescues it)."""
+"""GPU parity of the operating point's source stepping, gain stepping and
+pseudo-transient continuation against the reference's own source_stepping
+/ gain_stepping / pseudo_transient run alone (tests/golden/dc_aids.npz):
+converged or not as the reference, solutions within 1e-9 relative / 1e-12
+absolute, the same Newton iteration count (the aid's total: for source
+stepping including the failed solve at zero sources and the diagonal-gmin
+ramp that rescues it; for pseudo-transient every step whose pseudo
+timestep follows the ratio of Newton residuals, and the probes)."""
 import numpy as np
 import pytest
 import torch
@@ -15,9 +17,10 @@ pytestmark = pytest.mark.gpu
 CASES = golden_cases.load_aids()
 
 
-@pytest.mark.parametrize("aid", ["source", "gain"])
+@pytest.mark.parametrize("aid", ["source", "gain", "ptc"])
 def test_aid_matches_reference(aid):
-    cases = [g for g in CASES if int(g["aid"]) == (2 if aid == "source" else 3)]
+    analysis = {"source": 2, "gain": 3, "ptc": 4}[aid]
+    cases = [g for g in CASES if int(g["aid"]) == analysis]
     batch = DcBatch([g["netlist"].build() for g in cases], symbolic=DcBatch.PER_INSTANCE)
     batch.set_first_aid(aid)
     sols, status, iters = batch.run()
@@ -28,7 +31,8 @@ def test_aid_matches_reference(aid):
     for k, (g, s) in enumerate(zip(cases, batch.split(sols))):
         if int(g["converged"]):
             assert status[k] == 0, (aid, k, status[k])
-            assert method[k] == 2, (aid, k, method[k])  # SOURCE_STEPPING
+            # SOURCE_STEPPING (gain stepping reports it too), PSEUDO_TRANSIENT
+            assert method[k] == (3 if aid == "ptc" else 2), (aid, k, method[k])
             np.testing.assert_allclose(s, g["solution"], rtol=1e-9, atol=1e-12,
                                        err_msg=f"{aid} case {k}")
         else:
