@@ -4,8 +4,11 @@
 #include "sparse_order.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace nsg {
 
@@ -48,33 +51,83 @@ void finish(TopologyPlan& p) {
         }
     }
 
-    // Update map for the left-looking refactor.
-    std::vector<int32_t> where(n, -1);
+    // Update map for the left-looking refactor: for U(r, j), the positions
+    // in column j of the rows of L(:, r).  Counted first (upd_start), then
+    // filled column by column — on several host threads for large plans.
     p.upd_start.assign(p.nnz_lu, 0);
-    p.upd_dst.clear();
-    for (int32_t j = 0; j < n; ++j) {
-        for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
-            if (where[p.row_idx[q]] >= 0)
-                throw std::invalid_argument("plan: duplicate row in column " + std::to_string(j));
-            where[p.row_idx[q]] = q;
-        }
+    int64_t total = 0;
+    for (int32_t j = 0; j < n; ++j)
         for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j]; ++q) {
             const int32_t r = p.row_idx[q];
-            p.upd_start[q] = static_cast<int32_t>(p.upd_dst.size());
-            for (int32_t k = p.diag_pos[r] + 1; k < p.col_ptr[r + 1]; ++k) {
-                const int32_t d = where[p.row_idx[k]];
-                if (d < 0)
-                    throw std::invalid_argument("plan: fill pattern not closed at column " +
-                                                std::to_string(j));
-                p.upd_dst.push_back(d - p.col_ptr[j]);  // relative to column j
+            if (total > INT32_MAX) break;
+            p.upd_start[q] = static_cast<int32_t>(total);
+            total += p.col_ptr[r + 1] - p.diag_pos[r] - 1;
+        }
+    if (total > INT32_MAX) throw std::invalid_argument("plan: update map too large");
+    p.upd_dst.assign(static_cast<size_t>(total), 0);
+    // First failing column of each kind (duplicate row / fill not closed),
+    // so that the error does not depend on the thread schedule.
+    std::atomic<int32_t> bad_dup{INT32_MAX}, bad_fill{INT32_MAX};
+    auto fill_columns = [&](std::atomic<int32_t>& next_col, int32_t chunk) {
+        std::vector<int32_t> where(n, -1);
+        for (;;) {
+            const int32_t j0 = next_col.fetch_add(chunk);
+            if (j0 >= n) break;
+            const int32_t j1 = std::min(n, j0 + chunk);
+            for (int32_t j = j0; j < j1; ++j) {
+                bool dup = false;
+                for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) {
+                    if (where[p.row_idx[q]] >= 0) dup = true;
+                    where[p.row_idx[q]] = q;
+                }
+                bool open = false;
+                if (!dup) {
+                    for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j] && !open; ++q) {
+                        const int32_t r = p.row_idx[q];
+                        int32_t* out = p.upd_dst.data() + p.upd_start[q];
+                        for (int32_t k = p.diag_pos[r] + 1; k < p.col_ptr[r + 1]; ++k) {
+                            const int32_t d = where[p.row_idx[k]];
+                            if (d < 0) {
+                                open = true;
+                                break;
+                            }
+                            *out++ = d - p.col_ptr[j];  // relative to column j
+                        }
+                    }
+                }
+                for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) where[p.row_idx[q]] = -1;
+                auto lower = [](std::atomic<int32_t>& a, int32_t v) {
+                    int32_t cur = a.load();
+                    while (v < cur && !a.compare_exchange_weak(cur, v)) {
+                    }
+                };
+                if (dup) lower(bad_dup, j);
+                if (open) lower(bad_fill, j);
             }
         }
-        for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) where[p.row_idx[q]] = -1;
+    };
+    {
+        std::atomic<int32_t> next_col{0};
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nthreads = total >= (int64_t{1} << 25) ? static_cast<int>(std::min(hw, 16u)) : 1;
+        if (nthreads == 1) {
+            fill_columns(next_col, n);
+        } else {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nthreads; ++t) pool.emplace_back(fill_columns, std::ref(next_col), 64);
+            for (auto& th : pool) th.join();
+        }
     }
-    p.updates = static_cast<int64_t>(p.upd_dst.size());
+    const int32_t first_bad = std::min(bad_dup.load(), bad_fill.load());
+    if (first_bad != INT32_MAX) {
+        if (bad_dup.load() == first_bad)
+            throw std::invalid_argument("plan: duplicate row in column " + std::to_string(first_bad));
+        throw std::invalid_argument("plan: fill pattern not closed at column " +
+                                    std::to_string(first_bad));
+    }
+    p.updates = total;
     p.max_col = 0;
     for (int32_t j = 0; j < n; ++j) p.max_col = std::max(p.max_col, p.col_ptr[j + 1] - p.col_ptr[j]);
-    if (p.updates > INT32_MAX) throw std::invalid_argument("plan: update map too large");
 
     // Row-wise L and U.
     std::vector<int32_t> lcount(n + 1, 0), ucount(n + 1, 0);

@@ -4,6 +4,7 @@ AmdLuSolver (golden fixtures from tests/golden/make_golden.py, and the
 reference library itself where it was built), plus the oracle's C port of
 the replay refactor and solve pinned against the same fixtures."""
 import os
+import pathlib
 
 import numpy as np
 import pytest
@@ -209,3 +210,24 @@ def test_auto_engine_falls_back_to_markowitz_on_singular_first_factor():
     c = next(c for c in CASES if c["name"] == "mesh16")
     t = Topology.order(int(c["n"]), c["col_ptr"], c["row_idx"], c["vals"], solver="auto-amdlu")
     assert t.solver == "amdlu"
+
+
+def test_update_map_matches_sequential_build(tmp_path):
+    """The refactor's update map of a large AMD-LU plan, filled on several
+    host threads, equals the one-column-at-a-time map (tests/cpp/
+    plan_map_check.cpp, compiled here from the host sources)."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if not cxx:
+        pytest.skip("no host C++ compiler")
+    root = pathlib.Path(__file__).resolve().parents[1]
+    src = root / "neospice_b200" / "csrc"
+    exe = tmp_path / "plan_map_check"
+    subprocess.run([cxx, "-std=c++17", "-O2", "-pthread", f"-I{src}",
+                    str(root / "tests" / "cpp" / "plan_map_check.cpp"),
+                    str(src / "host" / "amd_lu.cpp"), str(src / "host" / "plan.cpp"),
+                    str(src / "host" / "sparse_order.cpp"), "-o", str(exe)], check=True)
+    res = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "0 failure(s)" in res.stdout
