@@ -278,6 +278,16 @@ int nsg_circuit_info(const nsg_circuit* c, int* num_vars, int* num_nodes, int* n
 /* CSC pattern (col_ptr: num_vars+1, row_idx: nnz) and parameters. */
 int nsg_circuit_pattern(const nsg_circuit* c, int* col_ptr, int* row_idx);
 int nsg_circuit_params(const nsg_circuit* c, double* params);
+/* Overwrite one parameter (index into the layout above): a resistance,
+ * capacitance, DC source value, a MOSFET's W, L or VTO (block offsets 0-2).
+ * Derived entries of a diode or MOSFET block are not recomputed. */
+int nsg_circuit_set_param(nsg_circuit* c, int index, double value);
+/* The values of a `.step` sweep, as Simulator::run_step_sweep
+ * (src/api/neospice.cpp:228-331) produces them: start, start + step, ...
+ * (accumulated), while within stop plus a thousandth of |step|.  *count gets
+ * the number of values; at most cap are written (cap 0: only the count;
+ * NSG_ERR_INVALID when cap is too small or step is 0). */
+int nsg_step_values(double start, double stop, double step, int cap, double* values, int* count);
 /* Matrix values and rhs of the first DC Newton iteration (MODEDCOP |
  * MODEINITJCT from a zero guess), in slot order -- what the reference's
  * first NeoSolver::numeric orders on. */

@@ -5,6 +5,7 @@
 #include "kernels/dc_device.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstring>
 #include <map>
@@ -350,6 +351,32 @@ int nsg_circuit_params(const nsg_circuit* c, double* params) {
     if (!c || !params) return fail(NSG_ERR_INVALID, "nsg_circuit_params: null argument");
     std::memcpy(params, c->c.params().data(), sizeof(double) * c->c.params().size());
     return NSG_OK;
+}
+
+int nsg_circuit_set_param(nsg_circuit* c, int index, double value) {
+    if (!c || index < 0 || index >= static_cast<int>(c->c.params().size()))
+        return fail(NSG_ERR_INVALID, "nsg_circuit_set_param: bad arguments");
+    c->c.params_mut()[index] = value;
+    return NSG_OK;
+}
+
+int nsg_step_values(double start, double stop, double step, int cap, double* values, int* count) {
+    if (!count || !(step != 0.0) || !std::isfinite(start) || !std::isfinite(stop) ||
+        !std::isfinite(step) || cap < 0 || (cap > 0 && !values))
+        return fail(NSG_ERR_INVALID, "nsg_step_values: bad arguments");
+    // Simulator::run_step_sweep's loop: accumulate the step, stop a
+    // thousandth of a step past `stop`.
+    const int direction = (step > 0) ? 1 : -1;
+    const double slack = std::abs(step) * 0.001;
+    int k = 0;
+    for (double v = start; direction > 0 ? v <= stop + slack : v >= stop - slack; v += step) {
+        if (k >= (1 << 24)) return fail(NSG_ERR_INVALID, "nsg_step_values: too many steps");
+        if (k < cap) values[k] = v;
+        ++k;
+    }
+    *count = k;
+    if (cap == 0) return NSG_OK;  // a size query
+    return k <= cap ? NSG_OK : fail(NSG_ERR_INVALID, "nsg_step_values: capacity too small");
 }
 
 int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs) {

@@ -1,0 +1,54 @@
+"""Batched `.step` sweeps: every value of a stepped parameter solved as one
+instance of a single GPU batch, instead of the reference's serial loop of
+full re-runs (Simulator::run_step_sweep, src/api/neospice.cpp:228-331).
+
+`.step` of a source (StepCommand::SOURCE) or of any device value: the
+parameter is named by its index in Circuit.params() (creation order; see
+Circuit.params).  Each step is an independent operating point, as the
+reference's loop makes it by clearing the state vectors between steps
+(Circuit::reset_state, src/core/circuit.cpp:305-314)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .circuit import Circuit, DcBatch
+
+
+def step_values(start: float, stop: float, step: float) -> np.ndarray:
+    """The values the reference's `.step start stop step` loop visits:
+    start, start + step, ... (accumulated) while within stop plus a
+    thousandth of |step|."""
+    count = ctypes.c_int()
+    L.check(L.lib().nsg_step_values(float(start), float(stop), float(step), 0, None,
+                                    ctypes.byref(count)))  # the count only
+    out = np.zeros(max(count.value, 1), np.float64)
+    L.check(L.lib().nsg_step_values(float(start), float(stop), float(step), len(out),
+                                    L.dptr(out), ctypes.byref(count)))
+    return out[:count.value]
+
+
+def sweep_dc(circuit: Circuit, param: int, values, symbolic=DcBatch.PER_PATTERN, batch=None):
+    """Operating points of `circuit` with parameter `param` set to each of
+    `values`, all in one batched launch.  Returns (solutions [len(values), n]
+    as a numpy array, status, iterations) per step; `batch` may be a DcBatch
+    of len(values) copies of this circuit made by an earlier call, to reuse
+    its symbolic phase."""
+    import torch
+
+    values = np.asarray(values, np.float64).ravel()
+    base = circuit.params()
+    if not 0 <= param < len(base):
+        raise IndexError(f"parameter {param} out of range (circuit has {len(base)})")
+    if batch is None:
+        batch = DcBatch([circuit] * len(values), symbolic=symbolic)
+    if batch.count != len(values):
+        raise ValueError("batch size does not match the number of step values")
+    params = np.tile(base, len(values))
+    params[param + len(base) * np.arange(len(values))] = values
+    d_params = torch.from_numpy(params).cuda()
+    sols, status, iters = batch.run(d_params)
+    torch.cuda.synchronize()
+    return (np.stack(batch.split(sols)), status.cpu().numpy(), iters.cpu().numpy())

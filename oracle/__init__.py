@@ -85,6 +85,7 @@ def ref() -> ctypes.CDLL:
         lib.nsref_sim_initjct.argtypes = [ctypes.c_char_p, _V, _V, _V, _V, _V]
         lib.nsref_sim_method.argtypes = [_V]
         lib.nsref_sim_sens.argtypes = [ctypes.c_char_p, _I, _V, _V]
+        lib.nsref_step_dc.argtypes = [ctypes.c_char_p, _I, _D, _D, _D, _I, _V, _V, _V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
         lib.nsref_amd_order.argtypes = [_I, _V, _V, _V]
@@ -341,6 +342,25 @@ def ref_sim_initjct(desc: str):
     if lib.nsref_sim_initjct(d, ctypes.addressof(nv), _p(cp), _p(ri), _p(vals), _p(rhs)) != nnz:
         raise RuntimeError("reference INITJCT evaluation failed")
     return cp, ri, vals, rhs
+
+
+def ref_step_dc(desc: str, device_line: int, start: float, stop: float, step: float,
+                num_nodes: int):
+    """The reference's `.op` under `.step <source> start stop step`
+    (Simulator::run_step_sweep): the source is line `device_line` of the
+    description.  Returns (step values, node voltages [steps x num_nodes],
+    Newton iterations per step)."""
+    lib = ref()
+    d = desc.encode()
+    cap = 1 << 12
+    vals = np.zeros(cap)
+    volts = np.zeros(cap * num_nodes)
+    iters = np.zeros(cap, np.int32)
+    k = lib.nsref_step_dc(d, int(device_line), float(start), float(stop), float(step), cap,
+                          _p(vals), _p(volts), _p(iters))
+    if k < 0 or k > cap:
+        raise RuntimeError("reference .step run failed")
+    return vals[:k].copy(), volts[:k * num_nodes].reshape(k, num_nodes).copy(), iters[:k].copy()
 
 
 def ref_sim_sens(desc: str, output_node: int):

@@ -581,6 +581,55 @@ void nsref_sim_free(void* h) { delete static_cast<SimResult*>(h); }
 
 }  // extern "C"
 
+// Simulator::run_step_sweep (src/api/neospice.cpp:228-331) on a described
+// circuit with `.op` and `.step <source> start stop step`: the source is the
+// description's device line `device` (named as build_from_desc names it).
+// Writes up to cap step values, each step's node voltages (num_nodes each)
+// and Newton iterations; returns the step count, or -1.
+extern "C" int nsref_step_dc(const char* desc, int device, double start, double stop, double step,
+                             int cap, double* values, double* volts, int* iterations) {
+    try {
+        Circuit ckt;
+        build_from_desc(ckt, desc);
+        std::string name;
+        {
+            // the device line's kind token, as build_from_desc names devices
+            int line = 0;
+            const char* p = desc;
+            while (*p && line < device) {
+                if (*p == '\n') ++line;
+                ++p;
+            }
+            std::string kind;
+            while (*p && *p != ' ' && *p != '\n') kind.push_back(*p++);
+            name = kind + std::to_string(device);
+        }
+        StepCommand sc;
+        sc.kind = StepCommand::SOURCE;
+        sc.name = name;
+        sc.start = start;
+        sc.stop = stop;
+        sc.step = step;
+        ckt.step_commands.push_back(sc);
+        ckt.analyses.push_back(AnalysisCommand{OpCmd{}});
+        Simulator sim;
+        SimulationResult r = sim.run(ckt);
+        if (!r.step) return -1;
+        const int nsteps = static_cast<int>(r.step->step_values.size());
+        const int nn = ckt.num_nodes();
+        for (int k = 0; k < nsteps && k < cap; ++k) {
+            values[k] = r.step->step_values[k];
+            const auto& dc = std::get<DCResult>(r.step->results[k].analysis);
+            for (int i = 0; i < nn; ++i) volts[static_cast<size_t>(k) * nn + i] = dc.node_voltages_dense.at(i);
+            iterations[k] = dc.status.iterations;
+        }
+        return nsteps;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_step_dc: %s\n", e.what());
+        return -1;
+    }
+}
+
 // The matrix and rhs of the first DC Newton iteration of a described circuit
 // (as nsref_mesh_initjct).  Returns nnz, or -1.
 extern "C" int nsref_sim_initjct(const char* desc, int* num_vars, int* col_ptr, int* row_idx,

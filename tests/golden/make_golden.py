@@ -25,6 +25,11 @@ MOS networks, diode-loaded resistor grids and inverter rings; per case the
 netlist, the aid, the solution, the Newton iterations and whether it
 converged.
 
+step_dc.npz: the reference's `.op` under `.step` of a source
+(Simulator::run_step_sweep) on seeded diode-loaded resistor grids; per case
+the netlist, the stepped parameter's index, start/stop/step, the step
+values, every step's node voltages and Newton iterations.
+
 mos_dc.npz: CMOS inverter chains and seeded MOS networks, per case the
 netlist (JSON) and the reference's solve_dc operating point, Newton
 iteration count and convergence method (0 direct, 1 gmin stepping).
@@ -224,6 +229,45 @@ def aid_main():
     path = pathlib.Path(__file__).with_name("dc_aids.npz")
     np.savez_compressed(path, **rec)
     print(f"wrote {len(cases)} source / gain stepping and pseudo-transient runs to {path}")
+
+
+def step_cases():
+    """(netlist, device index, start, stop, step) cases of step_dc.npz:
+    `.op` under `.step` of the supply or of a current source of seeded
+    diode-loaded resistor grids, ascending, descending and with steps that
+    accumulate rounding."""
+    from neospice_b200 import workloads as W
+    out = []
+    for k, (side, sweeps) in enumerate(((5, [(0.0, 2.0, 0.25), (1.0, -1.0, -0.3)]),
+                                        (8, [(0.0, 1.0, 0.1), (-0.5, 0.5, 0.0999)]),
+                                        (12, [(0.2, 3.0, 0.35)]))):
+        nl = W.diode_grid(np.random.default_rng([70, k]), side)
+        for sw in sweeps:
+            out.append((nl, 0) + sw)  # the supply is device 0
+        isrc = [i for i, d in enumerate(nl.devices) if d[0] == "I"]
+        if isrc:
+            out.append((nl, isrc[0], 0.0, 2e-3, 5e-4))
+    return out
+
+
+def step_main():
+    import json
+    import netlists
+    import golden_cases
+    rec = {}
+    cases = step_cases()
+    for k, (nl, dev, start, stop, step) in enumerate(cases):
+        vals, volts, iters = oracle.ref_step_dc(netlists.ref_desc(nl), dev + 1, start, stop, step,
+                                                nl.num_nodes)
+        p = f"s{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "param": np.int32(golden_cases.param_starts(nl)[dev][1]),
+                    p + "sweep": np.array([start, stop, step]), p + "values": vals,
+                    p + "volts": volts, p + "iterations": iters})
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("step_dc.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} .step sweeps to {path}")
 
 
 def sens_netlists():
@@ -479,8 +523,8 @@ def amd_main():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "aids", "sens", "amd",
-                             "linear"]
+    which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "aids", "step", "sens",
+                             "amd", "linear"]
     if "amd" in which:
         amd_main()
     if "linear" in which:
@@ -497,5 +541,7 @@ if __name__ == "__main__":
         mos_main()
     if "aids" in which:
         aid_main()
+    if "step" in which:
+        step_main()
     if "sens" in which:
         sens_main()

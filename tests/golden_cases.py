@@ -75,6 +75,27 @@ def load_aids():
     return out
 
 
+STEP_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "step_dc.npz"
+
+
+def load_steps():
+    """`.step` sweeps of the reference (step_dc.npz): netlist, param (index
+    in Circuit.params()), sweep (start, stop, step), values, volts
+    [steps x nodes], iterations."""
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(STEP_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"s{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        out.append(d)
+    return out
+
+
 MOS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "mos_dc.npz"
 
 
