@@ -46,8 +46,11 @@ def sweep_dc(circuit: Circuit, param: int, values, symbolic=DcBatch.PER_PATTERN,
         batch = DcBatch([circuit] * len(values), symbolic=symbolic)
     if batch.count != len(values):
         raise ValueError("batch size does not match the number of step values")
-    params = np.tile(base, len(values))
-    params[param + len(base) * np.arange(len(values))] = values
+    off = batch.param_offsets
+    params = np.zeros(int(off[-1]), np.float64)
+    for i, v in enumerate(values):
+        params[off[i]:off[i + 1]] = base
+        params[off[i] + param] = v
     d_params = torch.from_numpy(params).cuda()
     sols, status, iters = batch.run(d_params)
     torch.cuda.synchronize()
