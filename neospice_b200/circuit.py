@@ -135,6 +135,11 @@ class Circuit:
         self._final = True
         return self
 
+    def set_param(self, index: int, value: float):
+        """Overwrite parameter `index` of params() (a resistance,
+        capacitance, DC source value, MOSFET W / L / VTO)."""
+        L.check(L.lib().nsg_circuit_set_param(self._h, int(index), float(value)))
+
     def info(self) -> dict:
         nv, nn, nnz, npar = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         L.check(L.lib().nsg_circuit_info(self._h, ctypes.byref(nv), ctypes.byref(nn),

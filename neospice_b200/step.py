@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
-from .circuit import Circuit, DcBatch
+from .circuit import Circuit, DcBatch, TranBatch
 
 
 def step_values(start: float, stop: float, step: float) -> np.ndarray:
@@ -55,3 +55,20 @@ def sweep_dc(circuit: Circuit, param: int, values, symbolic=DcBatch.PER_PATTERN,
     sols, status, iters = batch.run(d_params)
     torch.cuda.synchronize()
     return (np.stack(batch.split(sols)), status.cpu().numpy(), iters.cpu().numpy())
+
+
+def sweep_transient(build, param: int, values, tstep: float, tstop: float, probes,
+                    max_points: int = 100000):
+    """Transients of one circuit with parameter `param` set to each of
+    `values`, all instances of one TranBatch: `build()` returns a fresh
+    finalized Circuit (one per step).  Returns the batch's results() list
+    (per step: time, values at the probes, status, counts)."""
+    values = np.asarray(values, np.float64).ravel()
+    circuits = []
+    for v in values:
+        c = build()
+        c.set_param(param, v)
+        circuits.append(c)
+    b = TranBatch(circuits, tstep, tstop, np.asarray(probes, np.int32), max_points=max_points)
+    b.run()
+    return b.results()

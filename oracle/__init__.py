@@ -86,6 +86,8 @@ def ref() -> ctypes.CDLL:
         lib.nsref_sim_method.argtypes = [_V]
         lib.nsref_sim_sens.argtypes = [ctypes.c_char_p, _I, _V, _V]
         lib.nsref_step_dc.argtypes = [ctypes.c_char_p, _I, _D, _D, _D, _I, _V, _V, _V]
+        lib.nsref_step_tran.argtypes = [ctypes.c_char_p, _I, _D, _D, _D, _D, _D, _I, _I, _V, _V,
+                                        _V, _V]
         lib.nsref_mesh_initjct.argtypes = [_I, _V, _V, _I, _V, _D, _D, _I, _V, _V, _D, _V, _V,
                                            _V, _V, _V]
         lib.nsref_amd_order.argtypes = [_I, _V, _V, _V]
@@ -361,6 +363,31 @@ def ref_step_dc(desc: str, device_line: int, start: float, stop: float, step: fl
     if k < 0 or k > cap:
         raise RuntimeError("reference .step run failed")
     return vals[:k].copy(), volts[:k * num_nodes].reshape(k, num_nodes).copy(), iters[:k].copy()
+
+
+def ref_step_tran(desc: str, device_line: int, start: float, stop: float, step: float,
+                  tstep: float, tstop: float, num_nodes: int, cap_points: int = 1 << 18):
+    """The reference's `.tran tstep tstop` under `.step <source> start stop
+    step`.  Returns a list over steps of (times, node voltages [points x
+    num_nodes]) and the Newton iterations per step."""
+    lib = ref()
+    d = desc.encode()
+    cap_steps = 1 << 10
+    counts = np.zeros(cap_steps, np.int32)
+    iters = np.zeros(cap_steps, np.int32)
+    times = np.zeros(cap_points)
+    volts = np.zeros(cap_points * num_nodes)
+    k = lib.nsref_step_tran(d, int(device_line), float(start), float(stop), float(step),
+                            float(tstep), float(tstop), cap_steps, cap_points, _p(counts),
+                            _p(times), _p(volts), _p(iters))
+    if k < 0 or k > cap_steps or int(counts[:k].sum()) > cap_points:
+        raise RuntimeError("reference .step transient failed")
+    out, at = [], 0
+    for c in counts[:k]:
+        out.append((times[at:at + c].copy(), volts[at * num_nodes:(at + c) * num_nodes]
+                    .reshape(c, num_nodes).copy()))
+        at += c
+    return out, iters[:k].copy()
 
 
 def ref_sim_sens(desc: str, output_node: int):

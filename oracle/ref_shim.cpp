@@ -630,6 +630,63 @@ extern "C" int nsref_step_dc(const char* desc, int device, double start, double 
     }
 }
 
+// As nsref_step_dc with `.tran tstep tstop` instead of `.op`: per step the
+// number of timepoints (counts), then all steps' times and node voltages
+// (points x num_nodes) concatenated, at most cap_points points in all.
+extern "C" int nsref_step_tran(const char* desc, int device, double start, double stop,
+                               double step, double tstep, double tstop, int cap_steps,
+                               int cap_points, int* counts, double* times, double* volts,
+                               int* iterations) {
+    try {
+        Circuit ckt;
+        build_from_desc(ckt, desc);
+        std::string name;
+        {
+            int line = 0;
+            const char* p = desc;
+            while (*p && line < device) {
+                if (*p == '\n') ++line;
+                ++p;
+            }
+            std::string kind;
+            while (*p && *p != ' ' && *p != '\n') kind.push_back(*p++);
+            name = kind + std::to_string(device);
+        }
+        StepCommand sc;
+        sc.kind = StepCommand::SOURCE;
+        sc.name = name;
+        sc.start = start;
+        sc.stop = stop;
+        sc.step = step;
+        ckt.step_commands.push_back(sc);
+        TranCmd tc;
+        tc.tstep = tstep;
+        tc.tstop = tstop;
+        ckt.analyses.push_back(AnalysisCommand{tc});
+        Simulator sim;
+        SimulationResult r = sim.run(ckt);
+        if (!r.step) return -1;
+        const int nsteps = static_cast<int>(r.step->step_values.size());
+        const int nn = ckt.num_nodes();
+        int at = 0;
+        for (int k = 0; k < nsteps && k < cap_steps; ++k) {
+            const auto& tr = std::get<TransientResult>(r.step->results[k].analysis);
+            const int np = static_cast<int>(tr.time.size());
+            counts[k] = np;
+            iterations[k] = tr.status.iterations;
+            for (int t = 0; t < np && at < cap_points; ++t, ++at) {
+                times[at] = tr.time[t];
+                for (int i = 0; i < nn; ++i)
+                    volts[static_cast<size_t>(at) * nn + i] = tr.voltages_dense[i][t];
+            }
+        }
+        return nsteps;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_step_tran: %s\n", e.what());
+        return -1;
+    }
+}
+
 // The matrix and rhs of the first DC Newton iteration of a described circuit
 // (as nsref_mesh_initjct).  Returns nnz, or -1.
 extern "C" int nsref_sim_initjct(const char* desc, int* num_vars, int* col_ptr, int* row_idx,

@@ -25,6 +25,9 @@ MOS networks, diode-loaded resistor grids and inverter rings; per case the
 netlist, the aid, the solution, the Newton iterations and whether it
 converged.
 
+step_tran.npz: the same for `.tran` (every step's timepoints and node
+voltages) on an RC ladder and a diode with junction charge.
+
 step_dc.npz: the reference's `.op` under `.step` of a source
 (Simulator::run_step_sweep) on seeded diode-loaded resistor grids; per case
 the netlist, the stepped parameter's index, start/stop/step, the step
@@ -250,6 +253,23 @@ def step_cases():
     return out
 
 
+def step_tran_cases():
+    """(netlist, device index, start, stop, step, tstep, tstop) cases of
+    step_tran.npz: `.tran` under `.step` of a DC supply — an RC ladder with
+    a pulse elsewhere, and a diode with junction charge fed through R from
+    the stepped supply and kicked by a current pulse."""
+    from neospice_b200 import workloads as W
+    ladder = W.Netlist(4, [
+        ("V", 0, -1, 1.0), ("R", 0, 1, 500.0), ("C", 1, -1, 1e-12), ("R", 1, 2, 800.0),
+        ("C", 2, -1, 2e-12), ("VPULSE", 3, -1, 0.0, 1.0, 2e-10, 1e-10, 1e-10, 5e-10, 2e-9),
+        ("R", 3, 2, 1000.0)])
+    diode = W.Netlist(2, [
+        ("V", 0, -1, 0.5), ("R", 0, 1, 1000.0), ("C", 1, -1, 1e-12),
+        ("D", 1, -1, 1e-14, 1.0, 5e-13, 0.8, 0.4, 0.5, 1e-10),
+        ("IPULSE", -1, 1, 0.0, 1e-3, 2e-10, 1e-10, 1e-10, 5e-10, 2e-9)])
+    return [(ladder, 0, 0.0, 2.0, 0.5, 1e-11, 2e-9), (diode, 0, 0.2, 1.0, 0.2, 1e-11, 2e-9)]
+
+
 def step_main():
     import json
     import netlists
@@ -268,6 +288,24 @@ def step_main():
     path = pathlib.Path(__file__).with_name("step_dc.npz")
     np.savez_compressed(path, **rec)
     print(f"wrote {len(cases)} .step sweeps to {path}")
+    rec = {}
+    cases = step_tran_cases()
+    for k, (nl, dev, start, stop, step, tstep, tstop) in enumerate(cases):
+        runs, iters = oracle.ref_step_tran(netlists.ref_desc(nl), dev + 1, start, stop, step,
+                                           tstep, tstop, nl.num_nodes)
+        p = f"s{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "param": np.int32(golden_cases.param_starts(nl)[dev][1]),
+                    p + "sweep": np.array([start, stop, step]),
+                    p + "tran": np.array([tstep, tstop]), p + "iterations": iters,
+                    p + "nsteps": np.int32(len(runs))})
+        for q, (t, v) in enumerate(runs):
+            rec[p + f"t{q:02d}"] = t
+            rec[p + f"v{q:02d}"] = v
+    rec["count"] = np.int32(len(cases))
+    path = pathlib.Path(__file__).with_name("step_tran.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(cases)} .step transients to {path}")
 
 
 def sens_netlists():

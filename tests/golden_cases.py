@@ -96,6 +96,28 @@ def load_steps():
     return out
 
 
+STEP_TRAN_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "step_tran.npz"
+
+
+def load_step_transients():
+    """`.step` transients of the reference (step_tran.npz): netlist, param,
+    sweep, tran (tstep, tstop), iterations per step, runs = [(times, node
+    voltages)] per step."""
+    import json
+    from neospice_b200.workloads import Netlist
+    z = np.load(STEP_TRAN_PATH)
+    out = []
+    for k in range(int(z["count"])):
+        p = f"s{k:02d}_"
+        d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+        nn, dev, models = json.loads(str(d["netlist"]))
+        d["netlist"] = Netlist(nn, [tuple(x) for x in dev],
+                               {k2: (t, p2) for k2, (t, p2) in models.items()})
+        d["runs"] = [(d[f"t{q:02d}"], d[f"v{q:02d}"]) for q in range(int(d["nsteps"]))]
+        out.append(d)
+    return out
+
+
 MOS_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "mos_dc.npz"
 
 

@@ -33,3 +33,9 @@ def test_stepped_parameter_index():
         dev = [i for i, _ in enumerate(nl.devices)
                if golden_cases.param_starts(nl)[i][1] == int(g["param"])][0]
         assert c.params()[int(g["param"])] == nl.devices[dev][3]
+
+
+def test_transient_step_values_match_reference():
+    for g in golden_cases.load_step_transients():
+        start, stop, step = (float(x) for x in g["sweep"])
+        assert len(step_values(start, stop, step)) == len(g["runs"])
