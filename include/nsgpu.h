@@ -395,8 +395,9 @@ int nsg_dc_batch_adjoint(nsg_dc_batch* b, const double* d_params, const double* 
 /* ---- Batched transient analysis (device) ------------------------------------
  * solve_transient (src/core/transient.cpp:694-1067) for `count` circuits in one
  * launch, one thread block per circuit, each with its own adaptive timestep:
- * DC operating point (MODETRANOP, with gmin stepping when the direct attempt
- * fails), then the accept/reject loop of TimeStepController
+ * DC operating point (MODETRANOP, with gmin stepping, source stepping and
+ * pseudo-transient continuation when the direct attempt fails), then the
+ * accept/reject loop of TimeStepController
  * (src/core/timestep.cpp) with trapezoidal / Gear / backward-Euler charge
  * integration and the truncation-error estimate of every charge state.  The
  * DC solver and the transient solver are ordered separately on their own
@@ -434,6 +435,38 @@ int nsg_tran_batch_orderings(const nsg_tran_batch* b, long long* count);
 /* Engines of each instance's DC and transient solvers (the reference creates
  * one of each, transient.cpp:713, :726), or -1 for a solver not yet ordered. */
 int nsg_tran_batch_engines(const nsg_tran_batch* b, int* dc_engine, int* tran_engine);
+
+/* Transient adjoint (no counterpart in the reference, whose sensitivities
+ * are DC finite differences, src/core/sens.cpp:57-140, and whose
+ * SparseMatrix::solve_transposed, src/solver/solve.cpp:102-141, has no
+ * caller).  Recording: with enable != 0 the next nsg_tran_batch_run keeps,
+ * per accepted timepoint, the integration formula it used, and the
+ * operating point. */
+int nsg_tran_batch_record(nsg_tran_batch* b, int enable);
+/* Newton tolerances of the adjoint's replay of the recorded steps (the
+ * forward run's SimOptions by default; tighter values make the gradient
+ * agree with finite differences of the same discrete transient). */
+int nsg_tran_batch_set_adjoint_options(nsg_tran_batch* b, double reltol, double vntol,
+                                       double abstol, int max_iter);
+/* Parameter layout (offsets: count+1) and the parameters the DC preamble
+ * and the transient use (host arrays, packed like nsg_circuit_params per
+ * instance; any pointer may be NULL). */
+int nsg_tran_batch_params(const nsg_tran_batch* b, long long* offsets, double* params_dc,
+                          double* params_tran);
+/* Gradient of L_i = weight * sum_n (x_n[probe[i]] - target_n)^2 over instance
+ * i's recorded timepoints (n = 0 the operating point; d_targets: count *
+ * max_points device doubles) with respect to every resistance, capacitance,
+ * DC source value and MOSFET W, L, VTO, into d_grads (device, packed like
+ * the parameters; 0 elsewhere), d_loss[count] and d_status[count] (0, or a
+ * Newton / singular / bounded-wait code).  The steps are replayed with a
+ * checkpoint every `every` steps.  d_params_dc / d_params_tran (device, may
+ * be NULL: the batch's own) replace the parameters of the replay.  Refused
+ * (NSG_ERR_INVALID): no recorded run, a run that filled max_points, diodes,
+ * or MOSFETs with charge. */
+int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_targets,
+                           double weight, int every, const double* d_params_dc,
+                           const double* d_params_tran, double* d_grads, double* d_loss,
+                           int* d_status, void* stream);
 
 #ifdef __cplusplus
 }
