@@ -455,9 +455,10 @@ int nsg_tran_batch_params(const nsg_tran_batch* b, long long* offsets, double* p
                           double* params_tran);
 /* Gradient of L_i = weight * sum_n (x_n[probe[i]] - target_n)^2 over instance
  * i's recorded timepoints (n = 0 the operating point; d_targets: count *
- * max_points device doubles) with respect to every resistance, capacitance,
- * DC source value and MOSFET W, L, VTO, into d_grads (device, packed like
- * the parameters; 0 elsewhere), d_loss[count] and d_status[count] (0, or a
+ * max_points device doubles) with respect to every resistance, capacitance
+ * and MOSFET W, L, VTO, into d_grads (device, packed like the parameters; 0
+ * elsewhere: the replay starts from the recorded operating point, so source
+ * values, which move it, are not differentiated), d_loss[count] and d_status[count] (0, or a
  * Newton / singular / bounded-wait code).  The steps are replayed with a
  * checkpoint every `every` steps.  d_params_dc / d_params_tran (device, may
  * be NULL: the batch's own) replace the parameters of the replay.  Refused

@@ -1,8 +1,7 @@
 // Batched transient adjoint: gradients of
 //   L = w * sum_n (x_n[probe] - target_n)^2      (n = 0: the operating point)
 // through the discrete transient of one instance per CTA, with respect to
-// resistances, capacitances, DC source values and the W, L and VTO of
-// level-1 MOSFETs.
+// resistances, capacitances and the W, L and VTO of level-1 MOSFETs.
 //
 // The forward run (transient_kernel with recording on) fixes the timepoints
 // and, per accepted step, the integration formula (NIintegrate coefficients,
@@ -18,7 +17,7 @@
 //                                   + ag2_{n+2} C eta_{n+2})
 //   eta_n   = mu_n - B^T lambda_n
 //   dL/dC  += eta_n (ag0_n v_n + ag1_n v_{n-1} + ag2_n v_{n-2})
-//   dL/dp  -= lambda_n^T dR_n/dp      (R, DC V / I values, MOSFET W / L / VTO)
+//   dL/dp  -= lambda_n^T dR_n/dp      (R, MOSFET W / L / VTO)
 // with J_n the Newton matrix at x_n (the forward's own assembly and
 // fixed-pivot refactor) and lambda from the transposed solve; the operating
 // point closes the recursion with the DC Jacobian.  Circuits whose MOSFETs
@@ -46,8 +45,10 @@ struct AdjDesc {
 
 namespace {
 
-// -lambda^T dF/dp of resistors, DC sources and MOSFET channels at x (the
-// dc_adjoint_kernel contraction), accumulated into g.
+// -lambda^T dF/dp of resistors and MOSFET channels at x (the
+// dc_adjoint_kernel contraction), accumulated into g.  Sources are skipped:
+// the replay starts from the recorded operating point, so a source value's
+// effect through x_0 would not be the replayed transient's.
 __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32_t* prog,
                                      const double* lam, const double* x, double* g) {
     const int32_t* gp = prog + d.prog_off[DP_grad];
@@ -58,10 +59,6 @@ __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32
         if (kind == 1) {
             const double R = v.par[p];
             g[p] += (at(lam, a) - at(lam, b)) * (at(x, a) - at(x, b)) / (R * R);
-        } else if (kind == 2) {  // voltage source: F_branch = vp - vn - V
-            g[p] += at(lam, a);
-        } else if (kind == 3) {  // current source p -> n: F_p += I, F_n -= I
-            g[p] += -(at(lam, a) - at(lam, b));
         } else if (kind == 4) {
             const double* P = v.par + p;
             const double* rec = v.mrec + kMosRecCount * e[4];
