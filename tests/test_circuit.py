@@ -188,3 +188,20 @@ def test_mos_model_card_validation():
     m = c.model_mos1("nmos", VTO=0.7, KP=1e-4, RD=0.0)
     with pytest.raises(L.NsgError, match="W > 0"):
         c.M(0, 1, 2, -1, m, 0.0, 1e-6)
+
+
+def test_set_param():
+    """nsg_circuit_set_param overwrites one entry of the parameter layout and
+    rejects indexes outside it."""
+    from neospice_b200 import _lib as L
+    from neospice_b200.circuit import Circuit
+    c = Circuit(2)
+    c.R(0, 1, 10.0)
+    c.V(0, -1, 1.0)
+    c.C(1, -1, 1e-12)
+    c.finalize()
+    c.set_param(1, 2.5)
+    np.testing.assert_array_equal(c.params(), [10.0, 2.5, 1e-12, 0.0])
+    for bad in (-1, 4):
+        with pytest.raises(L.NsgError):
+            c.set_param(bad, 1.0)
