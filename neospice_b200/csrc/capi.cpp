@@ -167,6 +167,10 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.nnz_l = p.lrow_ptr[p.n];
     d.nnz_u = p.urow_ptr[p.n];
     d.kind = p.kind;
+    // grow geometrically once for this plan, so a multi-gigabyte update map
+    // is copied once (appending to an unreserved pool re-copies it)
+    const size_t need = pool.size() + static_cast<size_t>(p.device_words()) + 4 * nsg::PA_COUNT + 4;
+    if (pool.capacity() < need) pool.reserve(std::max(need, 2 * pool.capacity()));
     p.append_to(pool, d.off);
     d.words = p.device_words();
     // the span [off[0], off[0] + words) may run past the last array by the

@@ -64,7 +64,8 @@ void finish(TopologyPlan& p) {
             total += p.col_ptr[r + 1] - p.diag_pos[r] - 1;
         }
     if (total > INT32_MAX) throw std::invalid_argument("plan: update map too large");
-    p.upd_dst.assign(static_cast<size_t>(total), 0);
+    p.upd_dst.clear();
+    p.upd_dst.resize(static_cast<size_t>(total));  // every entry written below
     // First failing column of each kind (duplicate row / fill not closed),
     // so that the error does not depend on the thread schedule.
     std::atomic<int32_t> bad_dup{INT32_MAX}, bad_fill{INT32_MAX};

@@ -3,9 +3,34 @@
 // need, as flat int32 arrays ready to upload.
 #pragma once
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 namespace nsg {
+
+// An allocator whose resize() leaves new int32 elements uninitialised: the
+// refactor's update map (one word per multiply-subtract, gigabytes for large
+// grids) is written entirely by the threads that fill it, so each thread
+// first-touches its own pages instead of one thread zeroing them all.
+template <class T>
+struct UninitAllocator : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAllocator<U>;
+    };
+    UninitAllocator() = default;
+    template <class U>
+    UninitAllocator(const UninitAllocator<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... Args>
+    void construct(U* p, Args&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+    }
+};
 
 class MarkowitzOrder;
 class AmdLuFactor;
@@ -43,7 +68,8 @@ struct TopologyPlan {
     // upd_start[q] indexes upd_dst, where the |L(:, r)| destinations of
     // L(:, r)'s rows are stored in L(:, r)'s order, as positions relative to
     // the start of column j.
-    std::vector<int32_t> upd_start, upd_dst;
+    std::vector<int32_t> upd_start;
+    std::vector<int32_t, UninitAllocator<int32_t>> upd_dst;
 
     // L by rows (strictly lower, columns ascending) and U by rows (strictly
     // upper, columns ascending): LU position and column of each entry.
