@@ -27,6 +27,7 @@ import os
 import pathlib
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -119,11 +120,13 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # the raw samples: NSG_CLOCKS_DIR if set, else the system's temp dir
+        out = os.environ.get("NSG_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = pathlib.Path(out) / f"clocks_rank{index}.csv"
 
     def start(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
