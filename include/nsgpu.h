@@ -278,6 +278,9 @@ int nsg_circuit_info(const nsg_circuit* c, int* num_vars, int* num_nodes, int* n
 /* CSC pattern (col_ptr: num_vars+1, row_idx: nnz) and parameters. */
 int nsg_circuit_pattern(const nsg_circuit* c, int* col_ptr, int* row_idx);
 int nsg_circuit_params(const nsg_circuit* c, double* params);
+/* Parameters held so far (finalized or not): the index the next device's
+ * first parameter gets. */
+int nsg_circuit_param_count(const nsg_circuit* c, int* count);
 /* Overwrite one parameter (index into the layout above): a resistance,
  * capacitance, DC source value, a MOSFET's W, L or VTO (block offsets 0-2).
  * Derived entries of a diode or MOSFET block are not recomputed. */

@@ -85,6 +85,7 @@ SIGNATURES = {
     "nsg_circuit_pattern": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "nsg_circuit_params": (c_int, [c_void_p, P(c_double)]),
     "nsg_circuit_set_param": (c_int, [c_void_p, c_int, c_double]),
+    "nsg_circuit_param_count": (c_int, [c_void_p, P(c_int)]),
     "nsg_step_values": (c_int, [c_double, c_double, c_double, c_int, P(c_double), P(c_int)]),
     "nsg_circuit_initial_matrix": (c_int, [c_void_p, c_double, P(c_double), P(c_double)]),
     "nsg_dc_batch_create": (c_int, [c_int, P(c_void_p), c_int, c_int, P(c_void_p)]),

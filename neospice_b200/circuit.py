@@ -48,46 +48,66 @@ class Circuit:
     def handle(self):
         return self._h
 
+    def param_count(self) -> int:
+        """Parameters held so far: the device methods below return the index
+        of the first parameter of the device they add (for set_param, the
+        batches' parameter arrays and `.step` sweeps)."""
+        n = ctypes.c_int()
+        L.check(L.lib().nsg_circuit_param_count(self._h, ctypes.byref(n)))
+        return n.value
+
     def R(self, a: int, b: int, ohms: float):
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_resistor(self._h, int(a), int(b), float(ohms)))
+        return first
 
     def V(self, p: int, n: int, volts: float):
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_vsource(self._h, int(p), int(n), float(volts)))
+        return first
 
     def I(self, p: int, n: int, amps: float):  # noqa: E743 - the reference's name
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_isource(self._h, int(p), int(n), float(amps)))
+        return first
 
     def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0,
           VJ: float = 1.0, M: float = 0.5, FC: float = 0.5, TT: float = 0.0):
         """Level-1 diode with the card D(IS N CJO VJ M FC TT); the junction
         capacitance and transit time act in the transient."""
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_diode_card(self._h, int(anode), int(cathode), float(IS),
                                                    float(N), float(CJO), float(VJ), float(M),
                                                    float(FC), float(TT)))
+        return first
 
     def C(self, a: int, b: int, farads: float, ic: float | None = None):
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_capacitor(self._h, int(a), int(b), float(farads),
                                                   int(ic is not None),
                                                   0.0 if ic is None else float(ic)))
+        return first
 
     def _wave(self, is_v: bool, p: int, n: int, wave: int, values):
         v = np.ascontiguousarray(values, np.float64)
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_source_wave(self._h, int(is_v), int(p), int(n), int(wave),
                                                     len(v), L.dptr(v)))
+        return first
 
     def VPULSE(self, p: int, n: int, v1, v2, td=0.0, tr=0.0, tf=0.0, pw=0.0, per=0.0):
         """V source with PULSE(v1 v2 td tr tf pw per) (VSource::set_pulse)."""
-        self._wave(True, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
+        return self._wave(True, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
 
     def IPULSE(self, p: int, n: int, v1, v2, td=0.0, tr=0.0, tf=0.0, pw=0.0, per=0.0):
-        self._wave(False, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
+        return self._wave(False, p, n, L.NSG_WAVE_PULSE, [v1, v2, td, tr, tf, pw, per])
 
     def VPWL(self, p: int, n: int, points):
         """V source with PWL(t0 v0 t1 v1 ...) (VSource::set_pwl)."""
-        self._wave(True, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
+        return self._wave(True, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
 
     def IPWL(self, p: int, n: int, points):
-        self._wave(False, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
+        return self._wave(False, p, n, L.NSG_WAVE_PWL, np.asarray(points, np.float64).ravel())
 
     def model_mos1(self, mtype: str, **params) -> int:
         """A level-1 MOSFET model card, e.g. model_mos1("nmos", VTO=0.7,
@@ -102,8 +122,10 @@ class Circuit:
 
     def M(self, d: int, g: int, s: int, b: int, model: int, W: float = 1e-6, L_: float = 1e-7):
         """Circuit::M(name, d, g, s, b, model, w, l)."""
+        first = self.param_count()
         L.check(L.lib().nsg_circuit_add_mosfet(self._h, int(d), int(g), int(s), int(b), int(model),
                                                float(W), float(L_)))
+        return first
 
     def add_capacitors(self, a, b, farads):
         a, b = np.ascontiguousarray(a, np.int32), np.ascontiguousarray(b, np.int32)

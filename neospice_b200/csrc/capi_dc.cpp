@@ -353,6 +353,12 @@ int nsg_circuit_params(const nsg_circuit* c, double* params) {
     return NSG_OK;
 }
 
+int nsg_circuit_param_count(const nsg_circuit* c, int* count) {
+    if (!c || !count) return fail(NSG_ERR_INVALID, "nsg_circuit_param_count: null argument");
+    *count = static_cast<int>(c->c.params().size());
+    return NSG_OK;
+}
+
 int nsg_circuit_set_param(nsg_circuit* c, int index, double value) {
     if (!c || index < 0 || index >= static_cast<int>(c->c.params().size()))
         return fail(NSG_ERR_INVALID, "nsg_circuit_set_param: bad arguments");

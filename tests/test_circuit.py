@@ -205,3 +205,20 @@ def test_set_param():
     for bad in (-1, 4):
         with pytest.raises(L.NsgError):
             c.set_param(bad, 1.0)
+
+
+def test_device_methods_return_parameter_index():
+    """Each device method returns the index of its first parameter in
+    params(), so a stepped or swept value can be addressed directly."""
+    from neospice_b200.circuit import Circuit
+    c = Circuit(3)
+    assert c.R(0, 1, 10.0) == 0
+    assert c.C(1, -1, 1e-12, ic=0.1) == 1
+    assert c.V(0, -1, 1.0) == 3
+    assert c.VPULSE(2, -1, 0.0, 1.0, 1e-9) == 4
+    assert c.D(2, -1) == 11
+    assert c.I(-1, 1, 1e-3) == 21
+    c.finalize()
+    p = c.params()
+    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[21] == 1e-3
+    assert c.param_count() == len(p) == 22
