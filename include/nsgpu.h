@@ -297,9 +297,10 @@ int nsg_step_values(double start, double stop, double step, int cap, double* val
 int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs);
 
 /* ---- Batched DC operating point (device) ------------------------------------
- * Simulator::run_dc / solve_dc (src/core/dc.cpp:53-175, newton.cpp:51-419):
- * the direct Newton attempt, then true gmin stepping and gmin stepping
- * (src/core/convergence.cpp:216-469) for instances it fails on, for `count`
+ * Simulator::run_dc / solve_dc (src/core/dc.cpp:53-242, newton.cpp:51-419):
+ * the direct Newton attempt, then true gmin stepping, gmin stepping, source
+ * stepping, gain stepping and pseudo-transient continuation
+ * (src/core/convergence.cpp:216-703, 986-1097) for instances it fails on, for `count`
  * circuits in one launch, one thread block per circuit.  symbolic: NSG_SYMBOLIC_PER_INSTANCE orders every circuit on its own
  * first-iteration matrix (bit-identical to the reference's pivots);
  * NSG_SYMBOLIC_PER_PATTERN orders once per distinct sparsity pattern and lets
@@ -372,8 +373,10 @@ int nsg_dc_batch_set_graph(nsg_dc_batch* b, int enable);
 int nsg_dc_batch_graph_launches(const nsg_dc_batch* b, long long* count);
 int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);
 /* After a run (synchronises the device): per instance the method that gave
- * the result, as the reference's ConvergenceMethod (0 direct Newton, 1 gmin
- * stepping), and the number of Newton solves it took (either may be NULL). */
+ * the result, as the reference's ConvergenceMethod (src/core/sim_status.hpp:
+ * 0 direct Newton, 1 gmin stepping, 2 source or gain stepping, 3
+ * pseudo-transient), and the number of Newton solves it took (either may be
+ * NULL). */
 int nsg_dc_batch_methods(const nsg_dc_batch* b, int* method, int* solves);
 
 /* Engine (NSG_SOLVER_MARKOWITZ or NSG_SOLVER_AMDLU) of each instance's
