@@ -179,9 +179,13 @@ int nsg_batch_solve_transposed(nsg_batch* batch, double* d_x, void* stream);
  * exits; the call itself allocates nothing.
  *   - Batches whose unknowns total more than NSG_STATIC_SCRATCH_DOUBLES are
  *     rejected with NSG_ERR_INVALID (see nsg_last_error).
+ *   - Call it with the batch's device current (the device that was current
+ *     at nsg_batch_create); another current device gives NSG_ERR_INVALID.
  *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     (cudaGetSymbolAddress) with that device current and keeps it; make that
+ *     first call before any stream capture.  Resetting that device
+ *     (cudaDeviceReset) afterwards is not supported: the kept address would
+ *     no longer be the array's.
  *   - All calls share the one array: calls that overlap on the GPU (different
  *     streams, or different batches at once) race.  The array keeps the last
  *     call's contents; nothing in it has to start at zero. */

@@ -408,6 +408,8 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
         *out = nullptr;
         auto b = std::make_unique<nsg_batch>();
         b->count = count;
+        cudaError_t de = cudaGetDevice(&b->device);
+        if (de != cudaSuccess) return cuda_fail("nsg_batch_create: current device", de);
         std::unordered_map<const nsg_topology*, int32_t> plan_of;
         std::vector<nsg::PlanDesc> plans;
         std::vector<int32_t> pool;

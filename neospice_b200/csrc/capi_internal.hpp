@@ -40,6 +40,7 @@ struct nsg_circuit {
 
 struct nsg_batch {
     int count = 0;
+    int device = 0;  // the CUDA device current when the batch was created
     std::vector<long long> a_off, x_off, lu_off;
     int32_t* d_pool = nullptr;
     nsg::PlanDesc* d_plans = nullptr;

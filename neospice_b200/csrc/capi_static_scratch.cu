@@ -43,17 +43,17 @@ constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
 double* g_scratch_addr[kMaxDevices] = {};
 
-// Device address of the static array on the current device, looked up on the
-// first call for that device.
-cudaError_t scratch_address(double** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
+// Device address of the static array on device `dev` (which is current),
+// looked up on the first call for that device and kept for the life of the
+// process.  A cudaDeviceReset after that first call reloads the module, so
+// the kept address would be stale: resetting a device that this entry point
+// has used is not supported.
+cudaError_t scratch_address(int dev, double** out) {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (!g_scratch_addr[dev]) {
         void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_sweep_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_sweep_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_addr[dev] = static_cast<double*>(p);
     }
@@ -75,8 +75,17 @@ int nsg_batch_solve_static_scratch(nsg_batch* b, double* d_x, void* stream) {
                     "nsg_batch_solve_static_scratch: the batch has " + std::to_string(need) +
                         " unknowns in total; the static workspace holds at most " +
                         std::to_string(kStaticScratchDoubles));
+    // The plans, factors and workspace live on the batch's device; the static
+    // array used must be that device's copy.
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail("nsg_batch_solve_static_scratch: current device", e);
+    if (dev != b->device)
+        return fail(NSG_ERR_INVALID,
+                    "nsg_batch_solve_static_scratch: the current device (" + std::to_string(dev) +
+                        ") is not the batch's device (" + std::to_string(b->device) + ")");
     double* scratch = nullptr;
-    cudaError_t e = scratch_address(&scratch);
+    e = scratch_address(dev, &scratch);
     if (e != cudaSuccess) return cuda_fail("nsg_batch_solve_static_scratch: symbol address", e);
     // The sweep writes every workspace entry before reading it, so nothing in
     // the array has to be cleared between calls.
