@@ -1,23 +1,34 @@
 """Benchmark: batched DC operating point of diode-clamped resistor meshes.
 
 Workload (one step): the DC operating point (Simulator::run_dc: direct
-Newton attempt, gmin stepping where it fails) of 4096 seeded meshes per GPU, grid side drawn uniformly
-from 16..96 (257..9217 unknowns), resistors lognormal around 1 kOhm (sigma
-0.1), level-1 diodes (IS=1e-14, N=1) at 5% of the nodes, 0-1 mA current
-sources at 2%, a 1 V corner source; Newton from a zero guess, all instances in
-one kernel launch.  Metric: circuit-solves/s (whole job).
+Newton attempt, gmin stepping where it fails) of 4096 seeded meshes per GPU,
+grid side drawn uniformly from 16..96 (257..9217 unknowns), resistors
+lognormal around 1 kOhm (sigma 0.1), level-1 diodes (IS=1e-14, N=1) at 5% of
+the nodes, 0-1 mA current sources at 2%, a 1 V corner source; Newton from a
+zero guess, all instances in one kernel launch.  Metric: circuit-solves/s
+(whole job).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Under torchrun (N > 1) every rank solves its own 4096 instances (weak
 scaling, no collective on the data path); the time is the max over ranks.
 --impl reference times the reference's own CPU code (oracle/_ref, built from
-the reference sources) on this host's cores on a bounded sample per step.
+the reference sources) on this host's cores: one process pool kept for the
+whole run, each step the DC operating point of 64 instances drawn evenly
+over the size distribution.
 
-At N = 1 the line also carries "plain_vs_batched": the transient of a
-32-stage CMOS inverter chain through the plain path (one instance per
-launch) and the batched path (Monte Carlo variants in one launch), with the
-nominal instance's parity against the reference.
+Besides the headline, the line carries (at N = 1):
+  setup / e2e_cold  circuit build + host ordering + plans + upload of the
+                    batch, and one cold run through the public API;
+  plain_dc          the same DC operating points one instance per launch;
+  cpu_baseline /    the reference's solve_dc on the host cores, and its
+  cpu_newton_only   NeoSolver refactorize + solve x the Newton iterations
+                    alone (no per-instance symbolic phase);
+  plain_vs_batched  transient of a 32-stage CMOS inverter chain, plain and
+                    as Monte Carlo variants, with parity of sampled variants;
+  adjoint           transient adjoint of driven 500-node RC trees, with
+                    central-difference and .sens parity;
+  power_grid        the single-topology AMD-LU refactor/solve case.
 """
 from __future__ import annotations
 
@@ -37,6 +48,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "circuit-solves/s (batched DC operating point, diode-clamped meshes)"
 UNIT = "circuit-solves/s"
 WORKLOAD = "batched DC OP, 4096 diode-clamped R meshes per GPU, side U{16..96}, FP64"
+L2_NOTE = "working set (LU values, several GB) larger than L2; no flush"
+REF_PER_STEP = 64
 
 
 def _args():
@@ -47,8 +60,10 @@ def _args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--count", type=int, default=4096, help="instances per GPU")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-sample", type=int, default=64,
+    ap.add_argument("--cpu-sample", type=int, default=REF_PER_STEP,
                     help="instances in the CPU-baseline sample (0 = skip)")
+    ap.add_argument("--plain-sample", type=int, default=24,
+                    help="instances of the plain (one per launch) DC measurement (0 = skip)")
     ap.add_argument("--no-inverter", action="store_true",
                     help="skip the plain-vs-batched transient measurement")
     ap.add_argument("--no-adjoint", action="store_true",
@@ -71,14 +86,32 @@ def make_meshes(count, seed, rank):
     return workloads.diode_mesh_batch(count, seed=sharding.rank_seed(seed, rank))
 
 
-def sample_indices(count, k, offset=0):
-    """Every (count/k)-th instance: a stratified sample of the same size
-    distribution."""
-    stride = max(1, count // max(1, k))
-    return [(offset + i * stride) % count for i in range(min(k, count))]
+def stratified_sample(sides, k, offset=0):
+    """k instances spread evenly over the size distribution: the instances
+    sorted by grid side, every (count/k)-th of them from `offset` (mod the
+    stride).  Returned largest first, the order the host pool runs them in
+    (longest jobs first keeps the pool's tail short)."""
+    import numpy as np
+    count = len(sides)
+    k = min(k, count)
+    stride = max(1, count // k)
+    order = np.argsort(np.asarray(sides), kind="stable")
+    pick = [int(order[(offset % stride) + i * stride]) for i in range(k)]
+    return sorted(pick, key=lambda i: -int(sides[i]))
+
+
+def common_config(a):
+    """The `config` both arms print (the same workload, word for word)."""
+    return {"workload": WORKLOAD, "instances_per_gpu": a.count, "seed": a.seed, "l2": L2_NOTE}
 
 
 # --- reference CPU path (oracle/_ref), one process per core ----------------------
+
+def _ref_warm(_):
+    import oracle
+    oracle.ref()
+    return os.getpid()
+
 
 def _ref_worker(mesh):
     import oracle
@@ -87,17 +120,55 @@ def _ref_worker(mesh):
     return sol, iters, time.perf_counter() - t0
 
 
-def reference_run(meshes, processes):
-    """Solve meshes with the reference on `processes` host processes (the
-    reference keeps per-process globals, so it is not run threaded).
-    Returns (solutions, iterations, wall seconds)."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
+def _ref_newton_worker(job):
+    """The reference NeoSolver on one mesh: numeric() (ordering + first
+    factor) on the first Newton matrix, then `iters` x (refactorize + solve)
+    -- the linear algebra of the Newton iterations that the GPU kernel
+    replaces, without the per-instance symbolic phase.  Returns (numeric
+    seconds, loop seconds)."""
+    import oracle
+    mesh, iters = job
+    cp, ri, vals, rhs = oracle.ref_mesh_initjct(mesh)
+    s = oracle.RefSolver(len(cp) - 1, cp, ri)
     t0 = time.perf_counter()
-    with ctx.Pool(processes) as pool:
-        res = pool.map(_ref_worker, meshes, chunksize=1)
-    wall = time.perf_counter() - t0
-    return [r[0] for r in res], [r[1] for r in res], wall
+    if s.numeric(vals) != 0:
+        raise RuntimeError("reference numeric() failed")
+    t1 = time.perf_counter()
+    for _ in range(iters):
+        s.refactorize(vals)
+        s.solve(rhs)
+    return t1 - t0, time.perf_counter() - t1
+
+
+def _ref_tran_worker(job):
+    import oracle
+    desc, tstep, tstop = job
+    t0 = time.perf_counter()
+    tr, vr, info = oracle.ref_sim(desc, 1, tstep, tstop)
+    return tr, vr, info, time.perf_counter() - t0
+
+
+class RefPool:
+    """One pool of host processes (spawn-started: the reference keeps
+    per-process globals, so it is not run threaded) kept for a whole
+    measurement; the pool's start-up and the loading of the reference
+    library happen before any timed region."""
+
+    def __init__(self, processes):
+        import multiprocessing as mp
+        self.processes = processes
+        self.pool = mp.get_context("spawn").Pool(processes)
+        self.pool.map(_ref_warm, range(processes), chunksize=1)
+
+    def map(self, fn, jobs):
+        """fn over jobs (results in order) and the wall seconds taken."""
+        t0 = time.perf_counter()
+        res = list(self.pool.imap(fn, jobs, chunksize=1))
+        return res, time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
 
 
 def cpu_model():
@@ -196,20 +267,35 @@ def run_ours(a, rank, world, local_rank):
     from neospice_b200.circuit import DcBatch
 
     meshes = make_meshes(a.count, a.seed, rank)
+
+    # Cold: circuit build, host ordering (once per sparsity pattern), plans and
+    # upload, then one run through the public API with host buffers.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     circuits = [m.build() for m in meshes]
+    t1 = time.perf_counter()
     batch = DcBatch(circuits, symbolic=DcBatch.PER_PATTERN)
-    st = batch.instance_stats()
+    t2 = time.perf_counter()
     params_h = torch.from_numpy(batch.params()).pin_memory()
-    d_params = params_h.to("cuda")
     nsol = int(batch.solution_offsets[-1])
+    sol_h = torch.empty(nsol, dtype=torch.float64).pin_memory()
+    d_params = torch.empty(params_h.numel(), dtype=torch.float64, device="cuda")
     d_sol = torch.empty(nsol, dtype=torch.float64, device="cuda")
     d_status = torch.empty(batch.count, dtype=torch.int32, device="cuda")
     d_iters = torch.empty(batch.count, dtype=torch.int32, device="cuda")
-    sol_h = torch.empty(nsol, dtype=torch.float64).pin_memory()
+    t3 = time.perf_counter()
+    d_params.copy_(params_h, non_blocking=True)
+    batch.run(d_params, d_sol, d_status, d_iters)
+    sol_h.copy_(d_sol, non_blocking=True)
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    reorders_cold = batch.reorders()
+    st = batch.instance_stats()
 
     for _ in range(a.warmup):
         batch.run(d_params, d_sol, d_status, d_iters)
     torch.cuda.synchronize()
+    reorders_warm = batch.reorders()
 
     def barrier():
         if world > 1:
@@ -231,6 +317,7 @@ def run_ours(a, rank, world, local_rank):
     barrier()
     clk = clocks.stop()
     sec = e0.elapsed_time(e1) / 1000.0
+    reorders_timed = batch.reorders() - reorders_warm
 
     status = d_status.cpu().numpy()
     iters = d_iters.cpu().numpy()
@@ -252,7 +339,7 @@ def run_ours(a, rank, world, local_rank):
     sec_e2e = f0.elapsed_time(f1) / 1000.0
 
     from neospice_b200 import sharding
-    sec, sec_e2e = sharding.max_over_ranks([sec, sec_e2e])
+    sec, sec_e2e, cold = sharding.max_over_ranks([sec, sec_e2e, t4 - t0])
 
     if rank == 0:
         solves = world * a.count * a.steps
@@ -274,18 +361,28 @@ def run_ours(a, rank, world, local_rank):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * sec / a.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded meshes)",
-            "config": {"workload": WORKLOAD, "instances_per_gpu": a.count, "seed": a.seed,
-                       "unknowns_total": int(n.sum()), "lu_entries_total": int(nlu.sum()),
-                       "refactor_updates_total": int(upd.sum()),
-                       "newton_iterations_mean": float(it.mean()),
-                       "converged": int((status == 0).sum()),
-                       "l2": "working set (LU values, several GB) larger than L2; no flush",
-                       "symbolic": "host Markowitz ordering once per sparsity pattern, "
-                                   "GPU pivot re-validation per instance",
-                       "parallelism": f"dp{world} (independent instances)"},
+            "config": common_config(a),
+            "workload_stats": {
+                "unknowns_total": int(n.sum()), "lu_entries_total": int(nlu.sum()),
+                "refactor_updates_total": int(upd.sum()),
+                "newton_iterations_mean": float(it.mean()),
+                "converged": int((status == 0).sum()),
+                "symbolic": "host Markowitz ordering once per sparsity pattern, "
+                            "GPU pivot re-validation per instance",
+                "parallelism": f"dp{world} (independent instances)",
+                "reorders": {"cold_run": reorders_cold, "warmup": reorders_warm - reorders_cold,
+                             "timed": reorders_timed}},
             "e2e": {"value": round(e2e, 3), "unit": UNIT,
                     "h2d_bytes_per_step": int(params_h.numel() * 8),
                     "d2h_bytes_per_step": int(nsol * 8)},
+            "setup": {"circuit_build_s": round(t1 - t0, 3), "batch_create_s": round(t2 - t1, 3),
+                      "setup_s": round(t2 - t0, 3), "cold_run_s": round(t4 - t3, 3),
+                      "what": "batch_create = host ordering once per sparsity pattern, "
+                              "plans, upload"},
+            "e2e_cold": {"value": round(world * a.count / cold, 3), "unit": UNIT,
+                         "seconds": round(cold, 3),
+                         "what": "one fresh batch: circuit build + setup + H2D + first run "
+                                 "(incl. its host re-orders) + D2H"},
             "gpu_launches": a.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 5),
@@ -298,32 +395,33 @@ def run_ours(a, rank, world, local_rank):
                          "fp64_gflops": round(flops_launch / launch_s / 1e9, 2)},
             "clocks": clk,
         }
+        if a.plain_sample > 0 and world == 1:
+            try:
+                line["plain_dc"] = plain_dc(meshes, a.plain_sample, value)
+            except Exception as exc:
+                line["plain_dc"] = {"error": str(exc)}
+        pool = None
         if a.cpu_sample > 0:
-            idx = sample_indices(a.count, a.cpu_sample)
-            procs = min(os.cpu_count() or 1, len(idx))
-            ref_sols, ref_iters, wall = reference_run([meshes[i] for i in idx], procs)
-            gpu = batch.split(d_sol)
-            worst = 0.0
-            for k, i in enumerate(idx):
-                err = np.abs(gpu[i] - ref_sols[k]) / np.maximum(np.abs(ref_sols[k]), 1e-3)
-                worst = max(worst, float(err.max()))
-            line["cpu_baseline"] = {
-                "value": round(len(idx) / wall, 4), "unit": UNIT, "cores": procs, "kind": "reference",
-                "sample": f"{len(idx)} of the {a.count} instances (every {a.count // len(idx)}th), "
-                          f"reference solve_dc, one process per core, {cpu_model()}"}
-            line["parity"] = {"checked": len(idx), "max_rel_err_vs_reference": worst,
-                              "iterations_equal": bool(all(int(iters[i]) == ref_iters[k]
-                                                           for k, i in enumerate(idx)))}
+            import oracle
+            if oracle.have_ref():
+                pool = RefPool(os.cpu_count() or 1)
+                line.update(cpu_legs(pool, meshes, batch, d_sol, iters, a.cpu_sample))
         if not a.no_inverter and world == 1:
             try:
-                line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch)
+                line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch, pool)
             except Exception as exc:
                 line["plain_vs_batched"] = {"error": str(exc)}
+        if pool is not None:
+            pool.close()
         if not a.no_adjoint and world == 1:
             try:
                 line["adjoint"] = adjoint_rc_tree(a.adjoint_batch)
             except Exception as exc:
                 line["adjoint"] = {"error": str(exc)}
+            try:
+                line["adjoint"]["parity"] = adjoint_parity()
+            except Exception as exc:
+                line["adjoint"]["parity"] = {"error": str(exc)}
         if not a.no_power_grid and world == 1:
             try:
                 line["power_grid"] = power_grid_refactor(a.grid_side, a.steps, a.warmup)
@@ -336,18 +434,91 @@ def run_ours(a, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def cpu_legs(pool, meshes, batch, d_sol, iters, k):
+    """The reference on a stratified sample of k instances, over all host
+    cores: its solve_dc (cpu_baseline, and parity of our solutions), and its
+    NeoSolver refactorize + solve repeated for each instance's Newton
+    iterations (cpu_newton_only)."""
+    import numpy as np
+    sides = [m.side for m in meshes]
+    idx = stratified_sample(sides, k, 0)
+    res, wall = pool.map(_ref_worker, [meshes[i] for i in idx])
+    gpu = batch.split(d_sol)
+    worst = 0.0
+    for (sol, _, _), i in zip(res, idx):
+        err = np.abs(gpu[i] - sol) / np.maximum(np.abs(sol), 1e-3)
+        worst = max(worst, float(err.max()))
+    nres, nwall = pool.map(_ref_newton_worker, [(meshes[i], int(iters[i])) for i in idx])
+    sample = (f"{len(idx)} of the {len(meshes)} instances, evenly spread over the sorted grid "
+              f"sides, largest first; one process per core; {cpu_model()}")
+    return {
+        "cpu_baseline": {"value": round(len(idx) / wall, 4), "unit": UNIT,
+                         "cores": pool.processes, "kind": "reference",
+                         "sample": "reference solve_dc, " + sample},
+        "cpu_newton_only": {
+            "value": round(len(idx) / nwall, 4), "unit": UNIT, "cores": pool.processes,
+            "what": "reference NeoSolver refactorize + solve x each instance's Newton "
+                    "iterations (the GPU's iteration counts, equal to the reference's), "
+                    "after one untimed numeric(); no device loads, no symbolic phase",
+            "numeric_core_s": round(sum(r[0] for r in nres), 3),
+            "loop_core_s": round(sum(r[1] for r in nres), 3),
+            "solve_dc_core_s": round(sum(r[2] for r in res), 3)},
+        "parity": {"checked": len(idx), "max_rel_err_vs_reference": worst,
+                   "iterations_equal": bool(all(int(iters[i]) == r[1]
+                                                for r, i in zip(res, idx)))},
+    }
+
+
+def plain_dc(meshes, k, batched_value):
+    """The plain path of the same DC operating points: one instance per
+    launch (a one-circuit DcBatch each), a stratified sample of k instances,
+    each timed with CUDA events after one warm-up run."""
+    import torch
+    from neospice_b200.circuit import DcBatch
+    idx = stratified_sample([m.side for m in meshes], k, 1)
+    total = 0.0
+    for i in idx:
+        b = DcBatch([meshes[i].build()], symbolic=DcBatch.PER_PATTERN)
+        b.run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.run()
+        e1.record()
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+        del b
+    value = len(idx) / total
+    return {"value": round(value, 3), "unit": UNIT, "instances": len(idx),
+            "seconds": round(total, 4), "batched_over_plain": round(batched_value / value, 2),
+            "what": "one instance per launch, stratified sample of the same meshes"}
+
+
 # --- plain vs batched transient (32-stage CMOS inverter chain) ---------------------
 
 INV_PULSE = (0.0, 1.8, 0.0, 1e-10, 1e-10, 1e-9, 2e-9)
 
 
-def inverter_plain_vs_batched(batch_count):
+def _tran_parity(ours, ref):
+    """Timepoints, voltages and Newton iterations of one of our transients
+    against the reference's."""
+    import numpy as np
+    tr, vr, info = ref
+    same_pts = len(tr) == len(ours["time"])
+    err = float(np.max(np.abs(ours["values"] - vr) / np.maximum(np.abs(vr), 1e-3))) \
+        if same_pts else None
+    return {"timepoints_equal": bool(same_pts and np.allclose(tr, ours["time"], rtol=1e-12, atol=0)),
+            "max_rel_err_vs_reference": err,
+            "iterations_equal": info["iterations"] == ours["newton_iters"]}
+
+
+def inverter_plain_vs_batched(batch_count, pool=None, parity_variants=8):
     """Transient of a 32-stage level-1 CMOS inverter chain (10 fF per stage,
     VDD 1.8 V, PULSE 0->1.8 V 100p/100p 1n/2n, .tran 1p 20n): the plain path
     (one instance per launch) and the batched path (batch_count Monte Carlo
-    variants in one launch), each timed end to end through TranBatch.run
-    (device clock), plus parity of the nominal instance with the reference's
-    solve_transient."""
+    variants in one launch), each timed through TranBatch.run (device
+    clock), with parity against the reference's solve_transient for the
+    nominal instance and `parity_variants` evenly spaced variants."""
     import numpy as np
     import torch
     from neospice_b200 import workloads as W
@@ -372,7 +543,8 @@ def inverter_plain_vs_batched(batch_count):
     rp = bp.results()[0]
     mc = [W.inverter_chain_mc(np.random.default_rng([7, i])) for i in range(batch_count)]
     bb, t_batch = timed(mc, 1)
-    ok = sum(r["status"] == 0 for r in bb.results())
+    rb = bb.results()
+    ok = sum(r["status"] == 0 for r in rb)
     out = {
         "workload": "transient, 32-stage CMOS inverter chain (MOS1), PULSE input, .tran 1p 20n; "
                     f"batched = {batch_count} Monte Carlo variants (VTO sigma 30 mV, KP 5%)",
@@ -389,22 +561,48 @@ def inverter_plain_vs_batched(batch_count):
         import netlists
         if oracle.have_ref():
             t0 = time.perf_counter()
-            tr, vr, info = oracle.ref_sim(netlists.ref_desc(nominal), 1, 1e-12, 20e-9)
+            ref_nom = oracle.ref_sim(netlists.ref_desc(nominal), 1, 1e-12, 20e-9)
             t_ref = time.perf_counter() - t0
-            same_pts = len(tr) == len(rp["time"])
-            err = float(np.max(np.abs(rp["values"] - vr) / np.maximum(np.abs(vr), 1e-3))) \
-                if same_pts else None
-            out["parity"] = {"timepoints_equal": bool(same_pts and np.allclose(tr, rp["time"],
-                                                                                rtol=1e-12, atol=0)),
-                             "max_rel_err_vs_reference": err,
-                             "iterations_equal": info["iterations"] == rp["newton_iters"]}
+            out["parity"] = _tran_parity(rp, ref_nom)
             out["cpu_reference_1core"] = {"value": round(1.0 / t_ref, 4), "unit": "circuit-solves/s"}
-    except Exception as exc:  # the parity check is informative only
+            if pool is not None and parity_variants > 0:
+                pick = sorted({int(round(x)) for x in
+                               np.linspace(0, batch_count - 1, parity_variants)})
+                res, wall = pool.map(_ref_tran_worker,
+                                     [(netlists.ref_desc(mc[i]), 1e-12, 20e-9) for i in pick])
+                checks = [_tran_parity(rb[i], (r[0], r[1], r[2])) for i, r in zip(pick, res)]
+                errs = [c["max_rel_err_vs_reference"] for c in checks]
+                out["batched"]["parity"] = {
+                    "variants_checked": pick,
+                    "timepoints_equal": all(c["timepoints_equal"] for c in checks),
+                    "max_rel_err_vs_reference": None if None in errs else max(errs),
+                    "iterations_equal": all(c["iterations_equal"] for c in checks),
+                    "tolerance": "1e-9 relative voltages (1e-3 V floor), identical timepoints "
+                                 "and iteration counts"}
+                out["cpu_reference_pool"] = {
+                    "value": round(len(pick) / wall, 4), "unit": "circuit-solves/s",
+                    "cores": pool.processes, "sample": f"{len(pick)} Monte Carlo variants"}
+    except Exception as exc:  # reported, not raised: the GPU numbers stand alone
         out["parity"] = {"error": str(exc)}
     return out
 
 
 # --- batched transient adjoint (RC trees driven by CMOS inverters) -------------------
+
+ADJ_TIGHT = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15, max_iter=200)
+
+
+def _adjoint_targets(results, max_points, seed=91):
+    """Seeded synthetic targets: an exponential fall with a per-instance
+    time constant, sampled at each instance's own timepoints."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    tg = np.zeros(len(results) * max_points)
+    for i, r in enumerate(results):
+        tau = 2e-10 * np.exp(0.2 * rng.standard_normal())
+        tg[i * max_points:i * max_points + len(r["time"])] = 1.8 * np.exp(-r["time"] / tau)
+    return tg
+
 
 def adjoint_rc_tree(count, nodes=500, every=32):
     """Gradients of sum_n (v_far(t_n) - target(t_n))^2 over .tran 1p 2n of
@@ -431,13 +629,7 @@ def adjoint_rc_tree(count, nodes=500, every=32):
     ev[1].record()
     torch.cuda.synchronize()
     res = b.results()
-    # seeded synthetic targets: an exponential fall with a per-instance time constant
-    rng = np.random.default_rng(91)
-    tg = np.zeros(count * max_points)
-    for i, r in enumerate(res):
-        tau = 2e-10 * np.exp(0.2 * rng.standard_normal())
-        tg[i * max_points:i * max_points + len(r["time"])] = 1.8 * np.exp(-r["time"] / tau)
-    d_tg = torch.from_numpy(tg).cuda()
+    d_tg = torch.from_numpy(_adjoint_targets(res, max_points)).cuda()
     ev[1].record()
     g, loss, st = b.adjoint(np.full(count, far), d_tg, 1.0, every)
     ev[2].record()
@@ -457,6 +649,120 @@ def adjoint_rc_tree(count, nodes=500, every=32):
         "newton_iters_mean": float(np.mean([r["newton_iters"] for r in res])),
         "loss_mean": float(loss.mean()),
     }
+
+
+def adjoint_parity(nodes=500, instances=2, per_instance=24, every=32, h_rel=1e-6):
+    """Parity of the adjoint section at its own size: instances 0 and 1 of
+    the benchmarked batch (same seeds, same targets), a seeded sample of
+    `per_instance` parameters each (the drivers' W, L, VTO and R / C of the
+    tree), gradient against central differences of the same discrete
+    transient (h = 1e-6 relative; Newton to reltol 1e-9 in the re-solves),
+    all in one batch: per instance one unperturbed copy and a +h and a -h
+    copy per parameter.  Tolerance 1e-6 relative plus the loss's rounding
+    floor 5e-12 L / 2h.  Also instance 0's DC gradient of v_far against the
+    reference's .sens (resistors and sources, one-sided FD with a 1e-4
+    step: 5e-3 relative)."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.circuit import DcBatch, TranBatch
+
+    far = nodes - 1
+    max_points = 4096
+    base = [W.rc_tree_driven(np.random.default_rng([90, i]), nodes) for i in range(instances)]
+    sel = []
+    for i, nl in enumerate(base):
+        nl.build()
+        pidx = nl.param_index
+        kinds = [d[0] for d in nl.devices]
+        mos = [pidx[k] + o for k, kd in enumerate(kinds) if kd == "M" for o in (0, 1, 2)]
+        rs = [pidx[k] for k, kd in enumerate(kinds) if kd == "R"]
+        cs = [pidx[k] for k, kd in enumerate(kinds) if kd == "C"]
+        rng = np.random.default_rng([92, i])
+        rest = per_instance - len(mos)
+        pick = list(rng.choice(rs, rest // 2, replace=False)) + \
+            list(rng.choice(cs, rest - rest // 2, replace=False))
+        sel.append(mos + [int(x) for x in pick])
+    copies = []     # (instance, parameter index or None, sign)
+    for i in range(instances):
+        copies.append((i, None, 0))
+        for p in sel[i]:
+            copies += [(i, p, +1), (i, p, -1)]
+    b = TranBatch([base[c[0]].build() for c in copies], 1e-12, 2e-9, np.full(1, far, np.int32),
+                  max_points=max_points)
+    b.record(True)
+    b.run()
+    torch.cuda.synchronize()
+    res = b.results()
+    first = {c[0]: k for k, c in enumerate(copies) if c[1] is None}
+    same = all(len(res[k]["time"]) == len(res[first[c[0]]]["time"]) for k, c in enumerate(copies))
+    # the benchmark's targets for instances 0..instances-1, then per copy
+    tg_inst = _adjoint_targets([res[first[i]] for i in range(instances)], max_points)
+    tg = np.concatenate([tg_inst[c[0] * max_points:(c[0] + 1) * max_points] for c in copies])
+    off, pdc, ptr = b.params()
+    hs = {}
+    for k, (i, p, sgn) in enumerate(copies):
+        if p is None:
+            continue
+        h = abs(pdc[off[k] + p]) * h_rel
+        hs[(i, p)] = h
+        pdc[off[k] + p] += sgn * h
+        ptr[off[k] + p] += sgn * h
+    b.set_adjoint_options(**ADJ_TIGHT)
+    dev = lambda x: torch.from_numpy(x).cuda()
+    g, loss, st = b.adjoint(np.full(len(copies), far), dev(tg), 1.0, every, dev(pdc), dev(ptr))
+    torch.cuda.synchronize()
+    g, loss, st = g.cpu().numpy(), loss.cpu().numpy(), st.cpu().numpy()
+    worst, within, resolved = 0.0, 0, 0
+    for i in range(instances):
+        k0 = first[i]
+        for p in sel[i]:
+            kp = copies.index((i, p, +1))
+            km = copies.index((i, p, -1))
+            h = hs[(i, p)]
+            fd = (loss[kp] - loss[km]) / (2 * h)
+            ga = g[off[k0] + p]
+            floor = 5e-12 * loss[k0] / (2 * h)
+            within += int(abs(ga - fd) <= 1e-6 * abs(fd) + floor)
+            if floor < 1e-8 * abs(fd):
+                resolved += 1
+                worst = max(worst, abs(ga - fd) / abs(fd))
+    out = {"instances": instances, "parameters_checked": instances * per_instance,
+           "status_ok": bool((st == 0).all()), "schedules_equal": bool(same),
+           "within_tolerance": within, "well_resolved": resolved,
+           "max_rel_err_well_resolved": worst,
+           "tolerance": "1e-6 relative + 5e-12 L / 2h (central FD, h = 1e-6 relative)"}
+    # DC gradient of v_far against the reference's .sens
+    try:
+        import oracle
+        sys.path.insert(0, str(ROOT / "tests"))
+        import netlists
+        if oracle.have_ref():
+            nl = base[0]
+            db = DcBatch([nl.build()], symbolic=DcBatch.PER_INSTANCE)
+            sols, dst, _ = db.run()
+            cot = torch.zeros_like(sols)
+            cot[far] = 1.0
+            gd, gst = db.adjoint(sols, cot)
+            torch.cuda.synchronize()
+            gd = gd.cpu().numpy()
+            pidx = nl.param_index
+            kinds = [d[0] for d in nl.devices]
+            order = ([pidx[k] for k, kd in enumerate(kinds) if kd == "R"] +
+                     [pidx[k] for k, kd in enumerate(kinds) if kd in ("V", "VPULSE")] +
+                     [pidx[k] for k, kd in enumerate(kinds) if kd in ("I", "IPULSE")])
+            sref, _ = oracle.ref_sim_sens(netlists.ref_desc(nl), far)
+            ours = gd[np.array(order, np.int64)]
+            scale = float(np.max(np.abs(sref)))
+            dev_err = np.abs(ours - sref) - (5e-3 * np.abs(sref) + 1e-6 * scale)
+            out["dc_sens"] = {"entries": len(sref), "status_ok": int(dst.sum()) == 0 and
+                              int(gst.sum()) == 0, "all_within": bool((dev_err <= 0).all()),
+                              "max_abs_diff": float(np.max(np.abs(ours - sref))),
+                              "max_abs_sens": scale,
+                              "tolerance": "5e-3 relative + 1e-6 x max |sens|"}
+    except Exception as exc:
+        out["dc_sens"] = {"error": str(exc)}
+    return out
 
 
 # --- one large topology: power-grid refactor and solve ------------------------------
@@ -552,6 +858,11 @@ def power_grid_refactor(side, reps, warmup):
 # --- reference arm -----------------------------------------------------------------
 
 def run_reference(a, rank):
+    """The reference's solve_dc on this host's cores: one process pool for
+    the whole run (started, and the library loaded in every process, before
+    the first step); each step the DC operating points of REF_PER_STEP
+    instances spread evenly over the size distribution (a different sample
+    each step), largest first."""
     if rank != 0:
         return
     import oracle
@@ -560,26 +871,32 @@ def run_reference(a, rank):
                           "unavailable": "reference library oracle/_ref/libnsref.so not built"}))
         return
     meshes = make_meshes(a.count, a.seed, 0)
+    sides = [m.side for m in meshes]
     procs = os.cpu_count() or 1
-    per_step = max(procs, 16)
-    for w in range(a.warmup):
-        reference_run([meshes[i] for i in sample_indices(a.count, procs, offset=w)], procs)
-    solves, wall = 0, 0.0
-    for s in range(a.steps):
-        idx = sample_indices(a.count, per_step, offset=a.warmup + s)
-        _, _, t = reference_run([meshes[i] for i in idx], procs)
-        solves += len(idx)
-        wall += t
+    per_step = max(REF_PER_STEP, procs)
+    pool = RefPool(procs)
+    try:
+        for w in range(a.warmup):
+            pool.map(_ref_worker, [meshes[i] for i in stratified_sample(sides, procs, 7 + w)])
+        solves, wall = 0, 0.0
+        for s in range(a.steps):
+            idx = stratified_sample(sides, per_step, s)
+            _, t = pool.map(_ref_worker, [meshes[i] for i in idx])
+            solves += len(idx)
+            wall += t
+    finally:
+        pool.close()
     value = solves / wall
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * wall / a.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded meshes)", "impl": "reference",
-        "config": {"workload": WORKLOAD, "instances_per_gpu": a.count, "seed": a.seed},
+        "config": common_config(a),
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "reference",
-                         "sample": f"{per_step} instances per step (stratified), reference "
-                                   f"solve_dc, one process per core, {cpu_model()}"},
+                         "sample": f"{per_step} instances per step, evenly spread over the sorted "
+                                   f"grid sides (a different sample each step), largest first; "
+                                   f"reference solve_dc, one process per core, {cpu_model()}"},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

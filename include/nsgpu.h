@@ -29,12 +29,23 @@ extern "C" {
 #define NSG_ERR_NOMEM 8      /* SparseError::NoMemory */
 #define NSG_SINGULAR 102     /* SparseError::Singular / ZeroDiag */
 #define NSG_REORDER 103      /* pivot failed re-validation: run nsg_topology_numeric */
+#define NSG_TIMEOUT 104      /* a bounded dependency wait on the GPU gave up; no result */
 
 typedef struct nsg_topology nsg_topology;
 typedef struct nsg_batch nsg_batch;
 
 /* Message of the last failing call on this thread ("" if none). */
 const char* nsg_last_error(void);
+
+/* Polls a dependency wait inside the dataflow and grid-wide kernels makes
+ * before it gives up; the instance then reports NSG_TIMEOUT (104) and the
+ * kernel still runs to its end, so the context stays usable.  Default 2^22
+ * polls (seconds; a wait that runs out means a broken schedule, not a slow
+ * one).  0 gives up at the first wait that has to poll -- used by tests to
+ * exercise the give-up path.  Applies to every kernel of the library on the
+ * current device.  No counterpart in the reference (its factor runs on one
+ * thread and never waits). */
+int nsg_set_wait_limit(int polls);
 
 /* ---- Symbolic phase (host) ------------------------------------------------
  * nsg_topology_order: NeoSolver::symbolic followed by the first

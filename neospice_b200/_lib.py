@@ -31,10 +31,12 @@ NSG_WAVE_DC = 0
 NSG_WAVE_PULSE = 1
 NSG_WAVE_PWL = 2
 NSG_STATIC_SCRATCH_DOUBLES = 1 << 20
+NSG_DEFAULT_WAIT_LIMIT = 1 << 22
 
 # name -> (restype, argtypes)
 SIGNATURES = {
     "nsg_last_error": (ctypes.c_char_p, []),
+    "nsg_set_wait_limit": (c_int, [c_int]),
     "nsg_topology_order": (c_int, [c_int, c_int, P(c_int), P(c_int), P(c_double), c_double,
                                    P(c_void_p)]),
     "nsg_topology_numeric": (c_int, [c_void_p, P(c_double), c_double, P(c_int)]),

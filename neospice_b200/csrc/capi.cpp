@@ -37,6 +37,22 @@ cudaError_t launch_grid_solve(const PlanDesc* plans, const int32_t* pool, const 
                               void* scratch, cudaStream_t stream);
 }  // namespace nsg
 
+namespace nsg {
+
+// Setters of every translation unit's copy of the bounded-wait limit
+// (c_wait_limit, kernels/lu_cta.cuh), registered at library load.
+static std::vector<cudaError_t (*)(int)>& wait_limit_setters() {
+    static std::vector<cudaError_t (*)(int)> v;
+    return v;
+}
+
+bool register_wait_limit_setter(cudaError_t (*set)(int polls)) {
+    wait_limit_setters().push_back(set);
+    return true;
+}
+
+}  // namespace nsg
+
 namespace nsg_internal {
 
 thread_local std::string g_last_error;
@@ -276,6 +292,15 @@ using namespace nsg_internal;
 extern "C" {
 
 const char* nsg_last_error(void) { return nsg_internal::g_last_error.c_str(); }
+
+int nsg_set_wait_limit(int polls) {
+    if (polls < 0) return fail(NSG_ERR_INVALID, "nsg_set_wait_limit: negative poll count");
+    for (auto set : nsg::wait_limit_setters()) {
+        const cudaError_t e = set(polls);
+        if (e != cudaSuccess) return cuda_fail("nsg_set_wait_limit", e);
+    }
+    return NSG_OK;
+}
 
 int nsg_topology_order(int n, int nnz, const int* col_ptr, const int* row_idx,
                        const double* values, double diag_gmin, nsg_topology** out) {

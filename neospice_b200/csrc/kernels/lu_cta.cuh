@@ -18,7 +18,25 @@ namespace nsg {
 
 constexpr int kFlowWarps = 16;
 constexpr int kFlowThreads = kFlowWarps * 32;
-constexpr int kSpinLimit = 1 << 22;
+
+// Polls a bounded dependency wait makes before it gives up and its instance
+// reports kStatusTimeout (a wait that finds its flag set at the first look
+// makes no poll; a limit of 0 gives up at the first wait that has to poll).
+// Every translation unit that includes this header keeps its own copy in
+// constant memory and registers a setter; nsg_set_wait_limit writes all of
+// them on the current device.
+constexpr int kDefaultWaitLimit = 1 << 22;
+static __constant__ int c_wait_limit = kDefaultWaitLimit;
+
+// Host: keep `set` in the list nsg_set_wait_limit walks (defined in capi.cpp).
+bool register_wait_limit_setter(cudaError_t (*set)(int polls));
+
+namespace {
+cudaError_t set_wait_limit_here(int polls) {
+    return cudaMemcpyToSymbol(c_wait_limit, &polls, sizeof(int));
+}
+const bool wait_limit_setter_registered = register_wait_limit_setter(&set_wait_limit_here);
+}  // namespace
 // Rounds of 32 L(:, r) rows the dataflow refactor loads before applying them.
 constexpr int kColChunk = 4;
 
@@ -222,9 +240,10 @@ __device__ __forceinline__ ColumnResult refactor_column(
                      int32_t& us, int32_t& ld) -> bool {
         int ready = 0;
         if (lane == 0) {
+            const int limit = c_wait_limit;
             int spins = 0;
             while ((ready = probe(m.x)) == 0 && wait) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     timed_out = true;
                     break;
                 }
@@ -337,7 +356,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
 // SparseMatrix::order_and_factor (factor.cpp:929-947), otherwise only an
 // exact zero pivot fails, as in SparseMatrix::factor; AMD-LU plans follow
 // amd_column_status.  Every
-// wait is bounded: past kSpinLimit polls the instance reports kStatusTimeout
+// wait is bounded: past c_wait_limit polls the instance reports kStatusTimeout
 // and the warp moves on, so the CTA always finishes.  Begins and ends with
 // __syncthreads().
 // When lrows/urows are given, every L and U entry is also written to its
@@ -664,9 +683,10 @@ __host__ __device__ inline size_t flow_solve_smem_bytes(int n) {
 // producer wrote before its release store.
 __device__ __forceinline__ bool wait_flag(volatile int32_t* flag, int32_t i) {
     if (flag_acquire(flag + i) != 0) return true;
+    const int limit = c_wait_limit;
     int spins = 0;
     while (flag_acquire(flag + i) == 0) {
-        if (++spins > kSpinLimit) return false;
+        if (++spins > limit) return false;
         __nanosleep(32);
     }
     return true;

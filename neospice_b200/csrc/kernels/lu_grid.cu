@@ -9,7 +9,7 @@
 // L2-only (ld.global.cg) so no SM sees a stale L1 line of a column another SM
 // finished.  Columns are only claimed by running warps and only wait on
 // earlier claims, so the schedule cannot deadlock whatever the residency;
-// every wait is still bounded (kSpinLimit) and reports kStatusTimeout.
+// every wait is still bounded (c_wait_limit polls) and reports kStatusTimeout.
 //
 // The per-column work is refactor_column (lu_cta.cuh), so values and their
 // rounding are those of the batched kernels: bit-identical to the
@@ -41,7 +41,8 @@ __device__ __forceinline__ void gflag_release(int32_t* f, int32_t v) {
 // Bounded wait until *f >= target; false on timeout.
 __device__ __forceinline__ bool gwait(const int32_t* f, int32_t target) {
     if (gflag_acquire(f) >= target) return true;
-    for (int spins = 0; spins < kSpinLimit; ++spins) {
+    const int limit = c_wait_limit;
+    for (int spins = 0; spins < limit; ++spins) {
         __nanosleep(64);
         if (gflag_acquire(f) >= target) return true;
     }

@@ -93,29 +93,35 @@ class Netlist:
     models: dict = dataclasses.field(default_factory=dict)
 
     def build(self) -> Circuit:
+        """The finalized circuit; ``self.param_index`` receives the index of
+        each device's first parameter (creation order), the layout of
+        Circuit.params()."""
         c = Circuit(self.num_nodes)
         mid = {name: c.model_mos1(t, **p) for name, (t, p) in self.models.items()}
+        first = []
         for d in self.devices:
             kind, a, b, vals = d[0], d[1], d[2], d[3:]
             if kind == "M":
-                c.M(a, b, vals[0], vals[1], mid[vals[2]], vals[3], vals[4])
+                k = c.M(a, b, vals[0], vals[1], mid[vals[2]], vals[3], vals[4])
             elif kind == "R":
-                c.R(a, b, vals[0])
+                k = c.R(a, b, vals[0])
             elif kind == "C":
-                c.C(a, b, vals[0], vals[1] if len(vals) > 1 else None)
+                k = c.C(a, b, vals[0], vals[1] if len(vals) > 1 else None)
             elif kind == "V":
-                c.V(a, b, vals[0])
+                k = c.V(a, b, vals[0])
             elif kind == "I":
-                c.I(a, b, vals[0])
+                k = c.I(a, b, vals[0])
             elif kind in ("VPULSE", "IPULSE"):
-                (c.VPULSE if kind[0] == "V" else c.IPULSE)(a, b, *vals)
+                k = (c.VPULSE if kind[0] == "V" else c.IPULSE)(a, b, *vals)
             elif kind in ("VPWL", "IPWL"):
                 pts = np.asarray(vals, np.float64).reshape(-1, 2)
-                (c.VPWL if kind[0] == "V" else c.IPWL)(a, b, pts)
+                k = (c.VPWL if kind[0] == "V" else c.IPWL)(a, b, pts)
             elif kind == "D":
-                c.D(a, b, *vals)
+                k = c.D(a, b, *vals)
             else:
                 raise ValueError(f"unknown device kind {kind!r}")
+            first.append(k)
+        self.param_index = first
         return c.finalize()
 
 

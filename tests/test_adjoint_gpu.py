@@ -92,3 +92,29 @@ def test_autograd_function():
     torch.cuda.synchronize()
     assert torch.allclose(p.grad, g_ref, rtol=0, atol=0)
     assert float(p.grad.abs().sum()) > 0
+
+
+def test_autograd_failed_instance_gets_nan():
+    """An instance whose forward solve fails (here: a bounded wait that gives
+    up, wait limit 0, on a mesh large enough for the dataflow path) gets NaN
+    solutions and NaN gradients; a small instance beside it (warp path, no
+    waits) keeps its exact values and gradients."""
+    from neospice_b200 import _lib as L
+    small = W.resistor_network(np.random.default_rng([71, 0]), 8).build()
+    big = W.diode_mesh(np.random.default_rng([71, 1]), side=40).build()
+    batch = DcBatch([small, big], symbolic=DcBatch.PER_INSTANCE)
+    p = torch.from_numpy(batch.params()).cuda().requires_grad_(True)
+    off = batch.solution_offsets
+    assert L.lib().nsg_set_wait_limit(0) == L.NSG_OK
+    try:
+        x = dc_solve(batch, p)
+        loss = (x[int(off[0]):int(off[1])] ** 2).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+    finally:
+        assert L.lib().nsg_set_wait_limit(L.NSG_DEFAULT_WAIT_LIMIT) == L.NSG_OK
+    po = batch.param_offsets
+    assert torch.isnan(x[int(off[1]):int(off[2])]).all()
+    assert torch.isnan(p.grad[int(po[1]):int(po[2])]).all()
+    assert torch.isfinite(p.grad[:int(po[1])]).all()
+    assert torch.isfinite(x[:int(off[1])]).all()

@@ -38,3 +38,9 @@ def test_last_error_after_misuse():
     lib = L.lib()
     assert lib.nsg_batch_solve(None, None, None) == L.NSG_ERR_INVALID
     assert b"null" in lib.nsg_last_error()
+
+
+def test_negative_wait_limit_is_refused():
+    lib = L.lib()
+    assert lib.nsg_set_wait_limit(-1) == L.NSG_ERR_INVALID
+    assert b"negative" in lib.nsg_last_error()

@@ -108,3 +108,24 @@ def test_tran_adjoint_requires_recording_and_rejects_mos_charge():
     b2.run()
     with pytest.raises(L.NsgError):
         b2.adjoint([5], tg)
+
+
+def test_tran_loss_autograd_function():
+    """tran_loss's backward is the adjoint's gradient, scaled per instance by
+    the incoming gradient of each instance's loss."""
+    from neospice_b200.autodiff import tran_loss
+    nls, b, tg, probes = setup(16, 83, count=2)
+    _, pdc, _ = b.params()
+    p = torch.from_numpy(pdc).cuda().requires_grad_(True)
+    loss = tran_loss(b, probes, tg, p, every=8)
+    (2.0 * loss[0] + 3.0 * loss[1]).backward()
+    g, l_ref, st = b.adjoint(probes, tg, 1.0, 8)
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0
+    assert torch.equal(loss.detach(), l_ref)
+    off, _, _ = b.params()
+    scale = torch.repeat_interleave(torch.tensor([2.0, 3.0], dtype=torch.float64, device="cuda"),
+                                    torch.from_numpy(np.diff(off)).cuda())
+    assert torch.equal(p.grad, g * scale)
+    assert float(p.grad.abs().sum()) > 0
+    assert torch.equal(tran_loss(b, probes, tg, every=8), l_ref)
