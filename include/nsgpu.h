@@ -277,6 +277,21 @@ int nsg_circuit_add_mos1_model(nsg_circuit* c, int type, int nparams, const char
  * (the MOS1setup / MOS1temp results the device load reads). */
 int nsg_circuit_add_mosfet(nsg_circuit* c, int d, int g, int s, int b, int model, double w,
                            double l);
+/* A BSIM4v7 (LEVEL=14) model card (Circuit::model with ".model name NMOS
+ * (LEVEL=14 ...)", BSIM4v7 model factory src/devices/bsim4v7/
+ * bsim4v7_factory.cpp:10-16): type +1 NMOS / -1 PMOS and nparams (key,
+ * value) pairs.  Supported: the default card with toxe, vth0 and u0 given
+ * (level and version are accepted and ignored); other parameters are
+ * rejected (NSG_ERR_INVALID).  *model_out receives the model index. */
+int nsg_circuit_add_bsim4_model(nsg_circuit* c, int type, int nparams, const char* const* keys,
+                                const double* values, int* model_out);
+/* A BSIM4v7 instance (Circuit::M with W and L, src/core/circuit.hpp:218-219,
+ * plus the DELVTO instance parameter, src/devices/bsim4v7/
+ * bsim4v7_param.cpp:142-144): one finger, no internal nodes.  Its parameter
+ * block holds W, L, DELVTO, TOXE, then BSIM4v7setup / BSIM4v7temp's values
+ * at the circuit temperature (kernels/bsim4_model.cuh, B4Param). */
+int nsg_circuit_add_bsim4(nsg_circuit* c, int d, int g, int s, int b, int model, double w,
+                          double l, double delvto);
 /* Bulk forms: count devices in one call, arrays of terminals and values,
  * created in array order (identical to count single calls). */
 int nsg_circuit_add_capacitors(nsg_circuit* c, int count, const int* a, const int* b,

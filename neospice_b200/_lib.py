@@ -101,6 +101,10 @@ SIGNATURES = {
     "nsg_circuit_add_source_wave": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int,
                                             P(c_double)]),
     "nsg_circuit_add_capacitors": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
+    "nsg_circuit_add_bsim4_model": (c_int, [c_void_p, c_int, c_int, P(ctypes.c_char_p), P(c_double),
+                                             P(c_int)]),
+    "nsg_circuit_add_bsim4": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,
+                                      c_double, c_double]),
     "nsg_circuit_add_mos1_model": (c_int, [c_void_p, c_int, c_int, P(ctypes.c_char_p), P(c_double),
                                            P(c_int)]),
     "nsg_circuit_add_mosfet": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double,

@@ -120,6 +120,28 @@ class Circuit:
                                                    ctypes.byref(out)))
         return out.value
 
+    def model_bsim4(self, mtype: str, **params) -> int:
+        """A BSIM4v7 (LEVEL=14) model card: the default card with TOXE, VTH0
+        and U0 optionally given, e.g. model_bsim4("nmos", TOXE=2e-9);
+        returns the model index for M4()."""
+        t = {"nmos": 1, "pmos": -1}[mtype.lower()]
+        params = {k: v for k, v in params.items() if k.lower() != "level"}
+        keys = (ctypes.c_char_p * max(1, len(params)))(*[k.encode() for k in params])
+        vals = np.ascontiguousarray([float(v) for v in params.values()] or [0.0], np.float64)
+        out = ctypes.c_int()
+        L.check(L.lib().nsg_circuit_add_bsim4_model(self._h, t, len(params), keys, L.dptr(vals),
+                                                    ctypes.byref(out)))
+        return out.value
+
+    def M4(self, d: int, g: int, s: int, b: int, model: int, W: float = 1e-6, L_: float = 1e-7,
+           delvto: float = 0.0):
+        """A BSIM4v7 instance (Circuit::M on a LEVEL=14 model, with the DELVTO
+        instance parameter)."""
+        first = self.param_count()
+        L.check(L.lib().nsg_circuit_add_bsim4(self._h, int(d), int(g), int(s), int(b), int(model),
+                                              float(W), float(L_), float(delvto)))
+        return first
+
     def M(self, d: int, g: int, s: int, b: int, model: int, W: float = 1e-6, L_: float = 1e-7):
         """Circuit::M(name, d, g, s, b, model, w, l)."""
         first = self.param_count()

@@ -145,7 +145,8 @@ void fill_instance(nsg::DcDesc& d, const nsg::Circuit& c, const nsg::TopologyPla
     for (const auto& sr : c.wave_sources()) tab.insert(tab.end(), {sr.is_voltage, sr.wave, sr.param, sr.nparam});
     d.prog_off[nsg::DP_srcs] = append(prog, tab);
     tab.clear();
-    for (const auto& m : c.mosfets()) tab.insert(tab.end(), {m.d, m.g, m.s, m.b, m.param, m.state});
+    for (const auto& m : c.mosfets())
+        tab.insert(tab.end(), {m.d, m.g, m.s, m.b, m.param, m.state, m.family});
     d.prog_off[nsg::DP_mos] = append(prog, tab);
     d.prog_off[nsg::DP_grad] = append(prog, c.grad_program());
     d.n_grad = static_cast<int32_t>(c.grad_program().size() / 5);
@@ -277,6 +278,31 @@ int nsg_circuit_add_mosfet(nsg_circuit* c, int d, int g, int s, int b, int model
     return guarded("nsg_circuit_add_mosfet", [&]() -> int {
         if (!c) return fail(NSG_ERR_INVALID, "null circuit");
         c->c.add_mosfet(d, g, s, b, model, w, l);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_bsim4_model(nsg_circuit* c, int type, int nparams, const char* const* keys,
+                                const double* values, int* model_out) {
+    return guarded("nsg_circuit_add_bsim4_model", [&]() -> int {
+        if (!c || nparams < 0 || (nparams && (!keys || !values)) || !model_out)
+            return fail(NSG_ERR_INVALID, "bad arguments");
+        nsg::Bsim4Card card;
+        card.type = type;
+        for (int i = 0; i < nparams; ++i) {
+            if (!keys[i]) return fail(NSG_ERR_INVALID, "nsg_circuit_add_bsim4_model: null key");
+            card.params.emplace_back(keys[i], values[i]);
+        }
+        *model_out = c->c.add_bsim4_model(card);
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_add_bsim4(nsg_circuit* c, int d, int g, int s, int b, int model, double w,
+                          double l, double delvto) {
+    return guarded("nsg_circuit_add_bsim4", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.add_bsim4(d, g, s, b, model, w, l, delvto);
         return NSG_OK;
     });
 }

@@ -214,10 +214,12 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         int64_t work = 0, param_off = 0, x0_off = 0;
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
-            // The adjoint covers MOSFETs without charge (no oxide, overlap or
-            // junction capacitance in the parameter block) and no diodes.
-            bool ok = c.diodes().empty();
+            // The adjoint covers level-1 MOSFETs without charge (no oxide,
+            // overlap or junction capacitance in the parameter block), no
+            // diodes and no BSIM4v7 devices (which always carry charge).
+            bool ok = c.diodes().empty() && !c.has_bsim4();
             for (const auto& m : c.mosfets()) {
+                if (m.family != nsg::kFamilyMos1) continue;
                 const double* P = c.params().data() + m.param;
                 for (int q : {nsg::kMOxCapFactor, nsg::kMCgso, nsg::kMCgdo, nsg::kMCgbo,
                               nsg::kMCbd, nsg::kMCbdsw, nsg::kMCbs, nsg::kMCbssw})

@@ -1,6 +1,7 @@
 #include "circuit.hpp"
 
 #include "kernels/diode_model.cuh"
+#include "kernels/bsim4_model.cuh"
 #include "kernels/mos1_model.cuh"
 #include "kernels/source_wave.cuh"
 
@@ -152,6 +153,32 @@ int32_t Circuit::add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t 
     return id;
 }
 
+int32_t Circuit::add_bsim4_model(const Bsim4Card& card) {
+    if (finalized_) throw std::logic_error("Circuit: already finalized");
+    (void)bsim4_param_block(card, 1e-6, 1e-7, 0.0);  // validate the card now
+    b4_models_.push_back(card);
+    return static_cast<int32_t>(b4_models_.size()) - 1;
+}
+
+int32_t Circuit::add_bsim4(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
+                           double L, double delvto) {
+    check_node(s);
+    check_node(b);
+    if (model < 0 || model >= static_cast<int32_t>(b4_models_.size()))
+        throw std::out_of_range("Circuit: unknown BSIM4v7 model " + std::to_string(model));
+    const int32_t id =
+        add_device(DevKind::Bsim4, d, g, bsim4_param_block(b4_models_[model], W, L, delvto));
+    devices_.back().c = s;
+    devices_.back().e = b;
+    return id;
+}
+
+bool Circuit::has_bsim4() const {
+    for (const auto& m : mos_)
+        if (m.family == kFamilyBsim4) return true;
+    return false;
+}
+
 int32_t Circuit::offset(int32_t r, int32_t c) const {
     if (r < 0 || c < 0) return -1;
     const auto b = row_idx_.begin() + col_ptr_[c];
@@ -169,7 +196,7 @@ void Circuit::finalize() {
     // the typed API's default model/instance orders).
     std::vector<DeviceRec> order = devices_;
     std::stable_sort(order.begin(), order.end(), [](const DeviceRec& x, const DeviceRec& y) {
-        if (x.kind != y.kind) return static_cast<int32_t>(x.kind) < static_cast<int32_t>(y.kind);
+        if (kind_rank(x.kind) != kind_rank(y.kind)) return kind_rank(x.kind) < kind_rank(y.kind);
         return x.created > y.created;
     });
 
@@ -207,6 +234,14 @@ void Circuit::finalize() {
                 stamp(S, S); stamp(D, B); stamp(S, B); stamp(S, D);
                 break;
             }
+            case DevKind::Bsim4: {  // BSIM4v7setup's TSTALLOC list without internal nodes
+                const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
+                stamp(D, B); stamp(G, B); stamp(S, B); stamp(B, D); stamp(B, G); stamp(B, S);
+                stamp(B, B); stamp(D, D); stamp(G, G); stamp(S, S); stamp(D, D); stamp(S, S);
+                stamp(D, D); stamp(G, D); stamp(G, S); stamp(S, S); stamp(D, S); stamp(D, D);
+                stamp(D, G); stamp(S, G); stamp(S, S); stamp(S, D);
+                break;
+            }
         }
     }
     std::vector<char> touched(num_vars_, 0);
@@ -241,10 +276,11 @@ void Circuit::finalize() {
     int32_t state = 0;
     for (size_t k = 0; k < order.size(); ++k) {
         const auto& d = order[k];
-        if (d.kind == DevKind::Mosfet) {
+        if (d.kind == DevKind::Mosfet || d.kind == DevKind::Bsim4) {
+            const bool b4 = d.kind == DevKind::Bsim4;
             index_in_table[k] = static_cast<int32_t>(mos_.size());
-            mos_.push_back({d.a, d.b, d.c, d.e, d.param, state});
-            state += kMosStates;
+            mos_.push_back({d.a, d.b, d.c, d.e, d.param, state, b4 ? kFamilyBsim4 : kFamilyMos1});
+            state += b4 ? kB4States : kMosStates;
         } else if (d.kind == DevKind::Diode) {
             index_in_table[k] = static_cast<int32_t>(diodes_.size());
             diodes_.push_back({d.a, d.b, d.param, state});
@@ -304,6 +340,22 @@ void Circuit::finalize() {
                                            {D, D}, {G, B}, {G, D}, {G, S}, {S, S}, {B, G},
                                            {B, D}, {B, S}, {D, D}, {D, G}, {D, B}, {D, S},
                                            {S, G}, {S, S}, {S, B}, {S, D}};
+                for (int32_t w = 0; w < 22; ++w) add_slot(rc[w][0], rc[w][1], mos_term(id, w));
+                break;
+            }
+            case DevKind::Bsim4: {
+                // BSIM4v7load: the rhs updates (UCB array: dNodePrime,
+                // gNodePrime, bNodePrime, sNodePrime), then the 22 matrix
+                // adds of the default path in order (B4Term).
+                const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
+                if (D >= 0) ucb[D].push_back(mos_term(id, kB4TRhsDP));
+                if (G >= 0) ucb[G].push_back(mos_term(id, kB4TRhsGP));
+                if (B >= 0) ucb[B].push_back(mos_term(id, kB4TRhsBP));
+                if (S >= 0) ucb[S].push_back(mos_term(id, kB4TRhsSP));
+                const int32_t rc[22][2] = {{G, G}, {G, D}, {G, S}, {G, B}, {D, D}, {D, D},
+                                           {D, G}, {D, S}, {D, B}, {D, D}, {D, D}, {S, D},
+                                           {S, G}, {S, S}, {S, S}, {S, B}, {S, S}, {S, S},
+                                           {B, D}, {B, G}, {B, S}, {B, B}};
                 for (int32_t w = 0; w < 22; ++w) add_slot(rc[w][0], rc[w][1], mos_term(id, w));
                 break;
             }
@@ -374,8 +426,9 @@ void Circuit::finalize() {
         }
     }
     for (size_t m = 0; m < mos_.size(); ++m)
-        grad_.insert(grad_.end(), {kGradMosfet, mos_[m].param, mos_[m].d, mos_[m].s,
-                                   static_cast<int32_t>(m)});
+        if (mos_[m].family == kFamilyMos1)
+            grad_.insert(grad_.end(), {kGradMosfet, mos_[m].param, mos_[m].d, mos_[m].s,
+                                       static_cast<int32_t>(m)});
     const int32_t pin = konst(kTermGmin, -1);
     for (int32_t i : dead_nodes_) slot[offset(i, i)].push_back(pin);
 
@@ -493,14 +546,19 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
     }
     // MOSFETs at MODEDCOP | MODEINITJCT from zero state.
     {
-        std::vector<double> rec(kMosRec, 0.0), st(kMosStates, 0.0);
+        std::vector<double> rec(kMosRec, 0.0), st(kB4States, 0.0);
         const Mos1Integ ic{0, 0, 0, 0, 0, 0, 1, 0};
         const double v0[4] = {0, 0, 0, 0};
         for (size_t m = 0; m < mos_.size(); ++m) {
             std::fill(rec.begin(), rec.end(), 0.0);
             std::fill(st.begin(), st.end(), 0.0);
-            mos1_load(&params_[mos_[m].param], rec.data(), st.data(), st.data(), st.data(),
-                      kM1DcOp | kM1InitJct, ic, gmin, v0, &tv[mos_term_base() + kMosTerms * m]);
+            double* t = &tv[mos_term_base() + kMosTerms * m];
+            if (mos_[m].family == kFamilyBsim4)
+                bsim4_load(&params_[mos_[m].param], rec.data(), st.data(), st.data(), st.data(),
+                           kM1DcOp | kM1InitJct, ic, gmin, 1e-3, 1e-12, v0, t);
+            else
+                mos1_load(&params_[mos_[m].param], rec.data(), st.data(), st.data(), st.data(),
+                          kM1DcOp | kM1InitJct, ic, gmin, v0, t);
         }
     }
     // Waveform sources at t = 0.

@@ -18,8 +18,13 @@ namespace nsg {
 
 // ngspice load rank of each device family (src/core/circuit.cpp:34-59).
 enum class DevKind : int32_t {
-    Mosfet = 3, Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50
+    Mosfet = 3, Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50,
+    Bsim4 = 1003,  // a MOSFET too: load rank 3 (kind_rank)
 };
+// The load rank of a device family ("M" devices of every level share 3).
+inline int32_t kind_rank(DevKind k) {
+    return k == DevKind::Bsim4 ? 3 : static_cast<int32_t>(k);
+}
 
 // Independent-source waveforms (src/devices/vsource.cpp:80-131).
 enum class Wave : int32_t { DC = 0, Pulse = 1, Pwl = 2 };
@@ -48,9 +53,13 @@ enum CapTerm : int32_t { kCGeq = 0, kCNegGeq = 1, kCNegCeq = 2, kCCeq = 3, kCapT
 enum SrcTerm : int32_t { kSVal = 0, kSNegVal = 1, kSrcTerms = 2 };
 // Per MOSFET: the Mos1Term values of kernels/mos1_model.cuh (22 matrix
 // terms in MOS1load's order, then the gate, bulk, drain and source rhs).
+// A BSIM4v7 MOSFET (kernels/bsim4_model.cuh) has the same term and
+// persistent-value counts (26, 12) and 29 states (BSIM4v7numStates).
 constexpr int32_t kMosTerms = 26;
 constexpr int32_t kMosStates = 17;  // MOS1numStates
+constexpr int32_t kB4States = 29;   // BSIM4v7numStates
 constexpr int32_t kMosRec = 12;     // persistent per-load values
+enum MosFamily : int32_t { kFamilyMos1 = 0, kFamilyBsim4 = 1 };
 
 struct DeviceRec {
     DevKind kind;
@@ -78,6 +87,20 @@ struct Mos1Card {
 // mos1_temp.cpp).  Throws std::invalid_argument on an unknown or
 // unsupported parameter (nonzero RD, RS or RSH).
 std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L);
+
+// A BSIM4v7 (LEVEL=14) model card: the type and the given parameters
+// (ngspice names).  Supported: the default card with TOXE, VTH0, U0.
+struct Bsim4Card {
+    int32_t type = 1;
+    std::vector<std::pair<std::string, double>> params;
+};
+
+// The BSIM4v7 parameter block (kernels/bsim4_model.cuh, B4Param) of one
+// instance of `card` with width W, length L and threshold shift DELVTO at
+// the nominal temperature: BSIM4v7setup's defaults and BSIM4v7temp
+// (src/devices/bsim4v7/bsim4v7_setup.cpp, bsim4v7_temp.cpp).  Throws
+// std::invalid_argument on an unsupported parameter.
+std::vector<double> bsim4_param_block(const Bsim4Card& card, double W, double L, double delvto);
 
 // The diode parameter block (DiodeParam of kernels/diode_model.cuh) of the
 // card D(IS N CJO VJ M FC TT) at the nominal temperature: DIOtemp
@@ -114,12 +137,20 @@ public:
     int32_t add_mos1_model(const Mos1Card& card);
     int32_t add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
                        double L);
+    // BSIM4v7 models and instances (the reference's LEVEL=14 `.model` and an
+    // M instance with W, L and the DELVTO instance parameter,
+    // src/devices/bsim4v7/bsim4v7_param.cpp:142-144).
+    int32_t add_bsim4_model(const Bsim4Card& card);
+    int32_t add_bsim4(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
+                      double L, double delvto);
 
     void finalize();
     bool finalized() const { return finalized_; }
     // Circuit::is_linear (src/core/circuit.hpp:171-175): no nonlinear device
     // (diodes and MOSFETs here).
     bool is_linear() const { return diodes_.empty() && mos_.empty(); }
+    // Whether any MOSFET is a BSIM4v7 instance (always charge-storing).
+    bool has_bsim4() const;
 
     int32_t num_nodes() const { return num_nodes_; }
     int32_t num_vars() const { return num_vars_; }
@@ -134,7 +165,7 @@ public:
     struct DiodeRec { int32_t pos, neg, param, state; };  // state: base of kDiodeStates
     struct CapRec { int32_t pos, neg, param, has_ic, state; };  // state: base of {q, i}
     struct SrcRec { int32_t is_voltage, wave, param, nparam; };
-    struct MosRec { int32_t d, g, s, b, param, state; };
+    struct MosRec { int32_t d, g, s, b, param, state, family; };
     const std::vector<DiodeRec>& diodes() const { return diodes_; }
     const std::vector<CapRec>& caps() const { return caps_; }
     const std::vector<SrcRec>& wave_sources() const { return wsrc_; }
@@ -196,6 +227,7 @@ private:
     std::vector<SrcRec> wsrc_;
     std::vector<MosRec> mos_;
     std::vector<Mos1Card> mos_models_;
+    std::vector<Bsim4Card> b4_models_;
     int32_t num_states_ = 0;
     std::vector<int32_t> term_op_, term_param_, grad_;
     std::vector<int32_t> slot_ptr_, slot_terms_, rhs_ptr_, rhs_terms_, ucb_ptr_, ucb_terms_;

@@ -63,6 +63,10 @@ constexpr int kCapTermCount = 4;
 constexpr int kSrcTermCount = 2;
 constexpr int kMosTermCount = 26;
 constexpr int kMosRecCount = 12;
+// MOSFET table: (d, g, s, b, param, state, family) per device; family 0
+// level-1 (kernels/mos1_model.cuh), 1 BSIM4v7 (kernels/bsim4_model.cuh).
+constexpr int kMosTabStride = 7;
+constexpr int kMosFamilyBsim4 = 1;
 // CONSTKoverQ * 300.15 evaluated as the reference's diode temperature code does.
 constexpr double kKoverQTimesTnom = (1.38064852e-23 / 1.6021766208e-19) * 300.15;
 

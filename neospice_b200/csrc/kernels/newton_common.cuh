@@ -4,6 +4,7 @@
 #include "dc_device.cuh"
 #include "diode_model.cuh"
 #include "lu_cta.cuh"
+#include "bsim4_model.cuh"
 #include "mos1_model.cuh"
 #include "source_wave.cuh"
 
@@ -37,7 +38,7 @@ struct Inst {
     const int32_t* diodes;  // (pos, neg, param, state)
     const int32_t* caps;    // (pos, neg, param, has_ic, state)
     const int32_t* srcs;    // (is_voltage, wave, param, nparam)
-    const int32_t* mos;     // (d, g, s, b, param, state)
+    const int32_t* mos;     // (d, g, s, b, param, state, family): level 1 or BSIM4v7
     const double* par;
     double* x;
     double* xold;
@@ -285,12 +286,17 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
         const Mos1Integ ic{c.ag[0], c.ag[1], c.ag[2], c.xmu_ratio, c.delta, c.delta_old[1],
                            c.order, c.method};
         for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
-            const int32_t* mr = v.mos + 6 * k;
+            const int32_t* mr = v.mos + kMosTabStride * k;
             double vn[4];
             for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? v.xold[mr[q]] : 0.0;
             const int32_t s = mr[5];
-            mos1_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
-                      v.st[2] + s, mode, ic, opt.gmin, vn, tv_m + kMosTermCount * k);
+            if (mr[6] == kMosFamilyBsim4)
+                bsim4_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
+                           v.st[2] + s, mode, ic, opt.gmin, opt.reltol, opt.abstol, vn,
+                           tv_m + kMosTermCount * k);
+            else
+                mos1_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
+                          v.st[2] + s, mode, ic, opt.gmin, vn, tv_m + kMosTermCount * k);
         }
     }
     for (int32_t k = threadIdx.x; k < v.n_srcs; k += blockDim.x) {
@@ -487,9 +493,14 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
         }
         __syncthreads();
         if (v.n_mos > 0 && s_conv != 0 && iter > 0) {
-            // MOS1Device::device_converged(solution) on the new solution
+            // MOS1Device::device_converged(solution) on the new solution;
+            // BSIM4v7Device::device_converged() is the last load's verdict.
             for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
-                const int32_t* mr = v.mos + 6 * k;
+                const int32_t* mr = v.mos + kMosTabStride * k;
+                if (mr[6] == kMosFamilyBsim4) {
+                    if (v.mrec[kMosRecCount * k + kB4RNoncon] != 0.0) s_dev_conv = 0;
+                    continue;
+                }
                 double vn[4];
                 for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? v.x[mr[q]] : 0.0;
                 if (!mos1_converged(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + mr[5], vn,

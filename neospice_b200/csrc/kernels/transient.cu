@@ -57,7 +57,8 @@ __device__ inline double cap_trunc(const Inst& v, int32_t q, const IntegCtx& c,
 
 // Minimum over the charge states of capacitors, diodes and MOSFETs of their
 // proposed timestep (Device::compute_trunc: capacitor.cpp,
-// dio_device.cpp:280-290, mos1_device.cpp:352-366), reduced across the CTA.
+// dio_device.cpp:280-290, mos1_device.cpp:352-366,
+// bsim4v7_device.cpp:1006-1027), reduced across the CTA.
 // std::min semantics: a NaN proposal is ignored.
 __device__ inline double min_trunc(const Inst& v, const IntegCtx& c, const TranOptions& o,
                                    double* s_red) {
@@ -71,9 +72,16 @@ __device__ inline double min_trunc(const Inst& v, const IntegCtx& c, const TranO
         if (t < m) m = t;
     }
     for (int32_t k = threadIdx.x; k < 5 * v.n_mos; k += blockDim.x) {
-        const int r = k % 5;  // qgs, qgd, qgb, qbd, qbs
-        const int q = r == 0 ? kSQgs : r == 1 ? kSQgd : r == 2 ? kSQgb : r == 3 ? kSQbd : kSQbs;
-        const double t = cap_trunc(v, v.mos[6 * (k / 5) + 5] + q, c, o);
+        const int32_t* mr = v.mos + kMosTabStride * (k / 5);
+        const int r = k % 5;
+        int q;
+        if (mr[6] == kMosFamilyBsim4) {  // qb, qg, qd (BSIM4v7Device::compute_trunc)
+            if (r >= 3) continue;
+            q = r == 0 ? kB4SQb : r == 1 ? kB4SQg : kB4SQd;
+        } else {  // qgs, qgd, qgb, qbd, qbs
+            q = r == 0 ? kSQgs : r == 1 ? kSQgd : r == 2 ? kSQgb : r == 3 ? kSQbd : kSQbs;
+        }
+        const double t = cap_trunc(v, mr[5] + q, c, o);
         if (t < m) m = t;
     }
     for (int off = 16; off > 0; off >>= 1) {

@@ -86,8 +86,10 @@ class Netlist:
     ("I", p, n, amps), ("VPULSE"|"IPULSE", p, n, v1, v2, td, tr, tf, pw, per),
     ("VPWL"|"IPWL", p, n, t0, v0, t1, v1, ...), ("D", anode, cathode, IS, N) or
     ("D", anode, cathode, IS, N, CJO, VJ, M, FC, TT).
-    ("M", d, g, s, b, model_name, W, L) with models[model_name] =
-    ("nmos"|"pmos", {param: value}) (level-1 cards).  Node -1 is ground."""
+    ("M", d, g, s, b, model_name, W, L[, delvto]) with models[model_name] =
+    ("nmos"|"pmos", {param: value}): a level-1 card, or a BSIM4v7 card when
+    its parameters hold LEVEL=14 (DELVTO only on BSIM4v7 instances).  Node
+    -1 is ground."""
     num_nodes: int
     devices: list
     models: dict = dataclasses.field(default_factory=dict)
@@ -97,11 +99,20 @@ class Netlist:
         each device's first parameter (creation order), the layout of
         Circuit.params()."""
         c = Circuit(self.num_nodes)
-        mid = {name: c.model_mos1(t, **p) for name, (t, p) in self.models.items()}
+        mid, b4 = {}, set()
+        for name, (t, p) in self.models.items():
+            if int(p.get("LEVEL", 1)) == 14:
+                mid[name] = c.model_bsim4(t, **p)
+                b4.add(name)
+            else:
+                mid[name] = c.model_mos1(t, **p)
         first = []
         for d in self.devices:
             kind, a, b, vals = d[0], d[1], d[2], d[3:]
-            if kind == "M":
+            if kind == "M" and vals[2] in b4:
+                k = c.M4(a, b, vals[0], vals[1], mid[vals[2]], vals[3], vals[4],
+                         vals[5] if len(vals) > 5 else 0.0)
+            elif kind == "M":
                 k = c.M(a, b, vals[0], vals[1], mid[vals[2]], vals[3], vals[4])
             elif kind == "R":
                 k = c.R(a, b, vals[0])

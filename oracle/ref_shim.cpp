@@ -40,6 +40,7 @@
 #include "core/convergence.hpp"
 
 #define private public
+#include "devices/bsim4v7/bsim4v7_device.hpp"
 #include "core/neo_solver.hpp"
 #include "core/amd_lu_solver.hpp"
 #include "solver/matrix.hpp"
@@ -394,7 +395,7 @@ int nsref_mesh_initjct(int side, const double* r_h, const double* r_v, int n_dio
 //   nodes N                          nodes n0..n{N-1} (MNA indices 0..N-1)
 //   R a b ohms | C a b farads [ic] | V a b dc | I a b dc
 //   VPULSE a b v1 v2 td tr tf pw per | IPULSE ... | VPWL a b t0 v0 t1 v1 ...
-//   IPWL a b t0 v0 ... | D a k IS N | MODEL name card... | M d g s b model W L
+//   IPWL a b t0 v0 ... | D a k IS N | MODEL name card... | M d g s b model W L [DELVTO]
 //   OPT name value                   (reltol, abstol, vntol, gmin, itl4, method)
 // Node -1 is ground.  analysis 0 = DC operating point, 1 = transient.
 struct SimResult {
@@ -485,8 +486,14 @@ static void build_from_desc(Circuit& ckt, const char* desc) {
             for (size_t k = 1; k < tk.size(); ++k) card += (k > 1 ? " " : "") + tk[k];
             ckt.model(card);
         } else if (kind == "M") {
-            ckt.M(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)), node_of(nodes, I_(3)),
-                  node_of(nodes, I_(4)), tk.at(5), D_(6), D_(7));
+            DevId id = ckt.M(name, node_of(nodes, I_(1)), node_of(nodes, I_(2)),
+                             node_of(nodes, I_(3)), node_of(nodes, I_(4)), tk.at(5), D_(6), D_(7));
+            if (tk.size() > 8) {  // DELVTO of a BSIM4v7 instance (bsim4v7_param.cpp:142-144)
+                auto* b4 = dynamic_cast<BSIM4v7Device*>(ckt.devices()[static_cast<int32_t>(id)].get());
+                if (!b4) throw std::invalid_argument("delvto given for a non-BSIM4v7 MOSFET");
+                b4->inst_.BSIM4v7delvto = D_(8);
+                b4->inst_.BSIM4v7delvtoGiven = 1;
+            }
         } else if (kind == "OPT") {
             const std::string& key = tk.at(1);
             const double val = D_(2);
