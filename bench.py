@@ -28,6 +28,8 @@ Besides the headline, the line carries (at N = 1):
                     as Monte Carlo variants, with parity of sampled variants;
   adjoint           transient adjoint of driven 500-node RC trees, with
                     central-difference and .sens parity;
+  bsim4_mc          BSIM4v7 Monte Carlo transient of a 200-MOSFET ring +
+                    NAND circuit, batched and plain, with sampled parity;
   power_grid        the single-topology AMD-LU refactor/solve case.
 """
 from __future__ import annotations
@@ -76,6 +78,8 @@ def _args():
                     help="side of the power-grid mesh of that section")
     ap.add_argument("--inverter-batch", type=int, default=296,
                     help="instances of the batched inverter-chain transient")
+    ap.add_argument("--bsim4-batch", type=int, default=2048,
+                    help="Monte Carlo instances of the BSIM4v7 ring + NAND transient (0 = skip)")
     return ap.parse_args()
 
 
@@ -411,6 +415,11 @@ def run_ours(a, rank, world, local_rank):
                 line["plain_vs_batched"] = inverter_plain_vs_batched(a.inverter_batch, pool)
             except Exception as exc:
                 line["plain_vs_batched"] = {"error": str(exc)}
+        if a.bsim4_batch > 0 and world == 1:
+            try:
+                line["bsim4_mc"] = bsim4_mc_transient(a.bsim4_batch, pool)
+            except Exception as exc:
+                line["bsim4_mc"] = {"error": str(exc)}
         if pool is not None:
             pool.close()
         if not a.no_adjoint and world == 1:
@@ -583,6 +592,92 @@ def inverter_plain_vs_batched(batch_count, pool=None, parity_variants=8):
                     "value": round(len(pick) / wall, 4), "unit": "circuit-solves/s",
                     "cores": pool.processes, "sample": f"{len(pick)} Monte Carlo variants"}
     except Exception as exc:  # reported, not raised: the GPU numbers stand alone
+        out["parity"] = {"error": str(exc)}
+    return out
+
+
+# --- BSIM4v7 Monte Carlo transient (ring oscillator + NAND chain) -------------------
+
+B4_PROBES = [0, 1, 2, 7, 13, 26, 27, 99, 100]
+
+
+def bsim4_mc_transient(count, pool=None, parity_instances=4, tstep=1e-12, tstop=5e-9):
+    """Batched Monte Carlo transient of the 200-MOSFET BSIM4v7 circuit
+    (workloads.bsim4_ring_nand: 25-stage ring oscillator + 25 NAND2 gates
+    each followed by an inverter, default LEVEL=14 cards, L 90n, W_n 200n,
+    W_p 400n, per-device DELVTO sigma 30 mV and TOXE +-3 %, VDD ramped to
+    1.2 V in 50 ps), .tran 1p 5n, `count` instances in one launch with
+    per-instance timestep control; the plain path (one instance per launch);
+    parity of evenly spaced instances against the reference's
+    solve_transient (timepoints, probe voltages, Newton iterations)."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.circuit import TranBatch
+
+    probes = np.array(B4_PROBES, np.int32)
+    nls = [W.bsim4_ring_nand(np.random.default_rng([33, i])) for i in range(count)]
+    t0 = time.perf_counter()
+    circuits = [nl.build() for nl in nls]
+    b = TranBatch(circuits, tstep, tstop, probes, max_points=6000)
+    t_setup = time.perf_counter() - t0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    b.run()
+    ev[1].record()
+    torch.cuda.synchronize()
+    t_batch = ev[0].elapsed_time(ev[1]) / 1e3
+    res = b.results()
+    ok = sum(r["status"] == 0 for r in res)
+    bp = TranBatch([nls[0].build()], tstep, tstop, probes, max_points=6000)
+    bp.run()
+    torch.cuda.synchronize()
+    ev[2].record()
+    bp.run()
+    ev[3].record()
+    torch.cuda.synchronize()
+    t_plain = ev[2].elapsed_time(ev[3]) / 1e3
+    iters = np.array([r["newton_iters"] for r in res], np.float64)
+    out = {
+        "workload": f"BSIM4v7 Monte Carlo transient, {count} instances of a 200-MOSFET circuit "
+                    "(25-stage ring oscillator + 25 NAND2 + 25 INV, default LEVEL=14 cards, "
+                    "DELVTO sigma 30 mV, TOXE +-3 %, n = 102), .tran 1p 5n, FP64",
+        "batched": {"value": round(count / t_batch, 3), "unit": "circuit-solves/s",
+                    "instances": count, "seconds": round(t_batch, 4), "ok": int(ok),
+                    "setup_s": round(t_setup, 3),
+                    "points_mean": float(np.mean([len(r["time"]) for r in res])),
+                    "newton_iters_mean": float(iters.mean()),
+                    "device_loads_per_s": round(200.0 * float(iters.sum()) / t_batch, 1)},
+        "plain": {"value": round(1.0 / t_plain, 4), "unit": "circuit-solves/s",
+                  "seconds_per_solve": round(t_plain, 4)},
+        "batched_over_plain": round((count / t_batch) * t_plain, 2),
+    }
+    try:
+        import oracle
+        sys.path.insert(0, str(ROOT / "tests"))
+        import netlists
+        if oracle.have_ref() and pool is not None and parity_instances > 0:
+            pick = sorted({int(round(x)) for x in np.linspace(0, count - 1, parity_instances)})
+            ref, wall = pool.map(_ref_tran_worker,
+                                 [(netlists.ref_desc(nls[i]), tstep, tstop) for i in pick])
+            checks = [_tran_parity({"time": res[i]["time"], "values": res[i]["values"],
+                                    "newton_iters": res[i]["newton_iters"]},
+                                   (r[0], r[1][:, B4_PROBES], r[2])) for i, r in zip(pick, ref)]
+            errs = [c["max_rel_err_vs_reference"] for c in checks]
+            out["parity"] = {"instances_checked": pick,
+                             "timepoints_equal": all(c["timepoints_equal"] for c in checks),
+                             "max_rel_err_vs_reference": None if None in errs else max(errs),
+                             "iterations_equal": all(c["iterations_equal"] for c in checks),
+                             "tolerance": "1e-9 relative voltages (1e-3 V floor), identical "
+                                          "timepoints and iteration counts"}
+            per = [r[3] for r in ref]
+            out["cpu_reference"] = {
+                "value": round(pool.processes / float(np.mean(per)), 4), "unit": "circuit-solves/s",
+                "cores": pool.processes, "seconds_per_solve_1core": round(float(np.mean(per)), 3),
+                "sample": f"{len(pick)} of the Monte Carlo instances, reference solve_transient; "
+                          "value = cores / mean seconds per solve"}
+    except Exception as exc:
         out["parity"] = {"error": str(exc)}
     return out
 

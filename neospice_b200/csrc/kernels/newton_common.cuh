@@ -165,6 +165,15 @@ __device__ inline double ni_integrate(const Inst& v, const IntegCtx& c, int32_t 
 // with its charge storage), capacitors (Capacitor::evaluate, state-vector
 // path), MOSFETs, waveform sources (value_at).  Writes the dynamic terms; returns through s_dev_conv
 // whether every device reports convergence (diodes' CKTnoncon and conv_test).
+// BSIM4v7 load out of line: its few hundred live values get their own
+// register allocation instead of spilling eval_devices' loop state.
+static __device__ __noinline__ void bsim4_load_call(const double* P, double* rec, double* s0,
+                                                    double* s1, const double* s2, int mode,
+                                                    const Mos1Integ& ic, const NewtonOptions& opt,
+                                                    const double* vn, double* t) {
+    bsim4_load(P, rec, s0, s1, s2, mode, ic, opt.gmin, opt.reltol, opt.abstol, vn, t);
+}
+
 static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& c, const NewtonOptions& opt,
                                     int32_t* s_dev_conv) {
     const int mode = c.mode;
@@ -291,9 +300,9 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
             for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? v.xold[mr[q]] : 0.0;
             const int32_t s = mr[5];
             if (mr[6] == kMosFamilyBsim4)
-                bsim4_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
-                           v.st[2] + s, mode, ic, opt.gmin, opt.reltol, opt.abstol, vn,
-                           tv_m + kMosTermCount * k);
+                bsim4_load_call(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s,
+                                v.st[1] + s, v.st[2] + s, mode, ic, opt, vn,
+                                tv_m + kMosTermCount * k);
             else
                 mos1_load(v.par + mr[4], v.mrec + kMosRecCount * k, v.st[0] + s, v.st[1] + s,
                           v.st[2] + s, mode, ic, opt.gmin, vn, tv_m + kMosTermCount * k);

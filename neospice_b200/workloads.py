@@ -333,3 +333,58 @@ def rc_tree_driven(rng: np.random.Generator, nodes: int, r_ohm=50.0, c_farad=2e-
     for k in range(nodes):
         dev.append(("C", k, GND, float(cc[k])))
     return Netlist(nodes + 2, dev, models)
+
+
+def bsim4_ring_nand(rng: np.random.Generator | None = None, stages: int = 25, vdd: float = 1.2,
+                    l: float = 90e-9, w_n: float = 200e-9, w_p: float = 400e-9,
+                    sigma_vth0: float = 0.030, toxe_spread: float = 0.03,
+                    ramp: float = 50e-12) -> Netlist:
+    """BSIM4v7 Monte Carlo circuit of 200 MOSFETs: a `stages`-stage inverter
+    ring oscillator (ring node i driven by stage i-1), and a chain of
+    `stages` two-input NAND gates, each followed by an inverter: NAND k takes
+    ring node k and the previous AND output (VDD for the first), so the chain
+    ANDs the ring's taps.  Default BSIM4v7 cards (LEVEL=14), L = 90n,
+    W_n = 200n, W_p = 400n.  With `rng`, every MOSFET gets its own card with
+    TOXE uniform within +-toxe_spread of the default 3 nm and a DELVTO drawn
+    Gaussian with sigma_vth0 (the per-device VTH0 variation); without it,
+    the nominal circuit (two shared cards).  VDD ramps 0 -> vdd in `ramp`
+    (PWL), the ring's start-up kick.  Nodes: 0 VDD, 1..S ring, then per
+    stage the NAND output, the NAND's series node and the AND output."""
+    S = stages
+    vddn = 0
+    ring = [1 + i for i in range(S)]
+    nand_out = [1 + S + 3 * k for k in range(S)]
+    nand_mid = [2 + S + 3 * k for k in range(S)]
+    and_out = [3 + S + 3 * k for k in range(S)]
+    models = {}
+    dev = [("VPWL", vddn, GND, 0.0, 0.0, ramp, vdd)]
+    count = [0]
+
+    def fet(kind, d, g, s, b, w):
+        count[0] += 1
+        if rng is None:
+            name = "nch" if kind == "n" else "pch"
+            if name not in models:
+                models[name] = ("nmos" if kind == "n" else "pmos", {"LEVEL": 14})
+            dev.append(("M", d, g, s, b, name, w, l))
+            return
+        name = f"{kind}{count[0]}"
+        toxe = 3.0e-9 * (1.0 + toxe_spread * (2.0 * rng.random() - 1.0))
+        models[name] = ("nmos" if kind == "n" else "pmos", {"LEVEL": 14, "TOXE": toxe})
+        dev.append(("M", d, g, s, b, name, w, l, float(sigma_vth0 * rng.standard_normal())))
+
+    for i in range(S):
+        inp, out = ring[(i - 1) % S], ring[i]
+        fet("n", out, inp, GND, GND, w_n)
+        fet("p", out, inp, vddn, vddn, w_p)
+    for k in range(S):
+        a = ring[k]
+        b = vddn if k == 0 else and_out[k - 1]
+        o, m = nand_out[k], nand_mid[k]
+        fet("n", o, a, m, GND, w_n)      # series pull-down
+        fet("n", m, b, GND, GND, w_n)
+        fet("p", o, a, vddn, vddn, w_p)  # parallel pull-up
+        fet("p", o, b, vddn, vddn, w_p)
+        fet("n", and_out[k], o, GND, GND, w_n)
+        fet("p", and_out[k], o, vddn, vddn, w_p)
+    return Netlist(1 + S + 3 * S, dev, models)

@@ -7,6 +7,8 @@ Two checkers, loaded with ctypes:
 * ``ref()``   — oracle/_ref/libnsref.so, the reference's own C++ sources
   compiled by oracle/Makefile plus the export shim ref_shim.cpp.  Present only
   where the reference sources were available at build time.
+* ``seam()``  — oracle/_ref/libnsseam.so, the same plus gpu_seam.cpp: the
+  reference's analyses on libnsgpu through its ISolver seam.
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use
 this package.
@@ -35,6 +37,8 @@ def build(reference: bool = True) -> None:
     targets = ["port"]
     if reference and (REFERENCE_SRC / "src").is_dir():
         targets.append("ref")
+        if (HERE.parent / "neospice_b200" / "libnsgpu.so").exists():
+            targets.append("seam")
     subprocess.run(["make", "-s", f"-j{8}", *targets], cwd=HERE, check=True)
 
 
@@ -64,7 +68,34 @@ def have_ref() -> bool:
 def ref() -> ctypes.CDLL:
     global _ref
     if _ref is None:
-        lib = ctypes.CDLL(str(REF_SO))
+        _ref = _bind(ctypes.CDLL(str(REF_SO)))
+    return _ref
+
+
+SEAM_SO = OUT / "libnsseam.so"
+_seam = None
+
+
+def have_seam() -> bool:
+    return SEAM_SO.exists()
+
+
+def seam() -> ctypes.CDLL:
+    """oracle/_ref/libnsseam.so: the reference's sources with make_solver
+    overridden by oracle/gpu_seam.cpp, so that its analyses can run on
+    libnsgpu through the ISolver seam (nsseam_use_gpu).  Same entry points as
+    ref()."""
+    global _seam
+    if _seam is None:
+        lib = _bind(ctypes.CDLL(str(SEAM_SO)))
+        lib.nsseam_use_gpu.argtypes = [_I]
+        lib.nsseam_gpu_solvers.restype = ctypes.c_longlong
+        _seam = lib
+    return _seam
+
+
+def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
+    if True:
         lib.nsref_solver_create.restype = _V
         lib.nsref_solver_create.argtypes = [_I, _I, _V, _V]
         lib.nsref_solver_destroy.argtypes = [_V]
@@ -101,8 +132,7 @@ def ref() -> ctypes.CDLL:
         lib.nsref_amdlu_sizes.argtypes = [_V, _V, _V]
         lib.nsref_amdlu_export.argtypes = [_V] * 9
         lib.nsref_make_solver_name.argtypes = [_I, _I, ctypes.c_char_p, _I]
-        _ref = lib
-    return _ref
+    return lib
 
 
 def _p(a):
@@ -300,14 +330,14 @@ def _mesh_args(m):
     return args, arrs
 
 
-def ref_mesh_dc(m):
+def ref_mesh_dc(m, lib=None):
     """The reference's DC operating point of a diode mesh: (solution,
     Newton iterations, seconds)."""
     args, keep = _mesh_args(m)
     sol = np.zeros(m.num_vars)
     it = ctypes.c_int(0)
     sec = ctypes.c_double(0.0)
-    nv = ref().nsref_mesh_dc(*args, _p(sol), ctypes.addressof(it), ctypes.addressof(sec))
+    nv = (lib if lib is not None else ref()).nsref_mesh_dc(*args, _p(sol), ctypes.addressof(it), ctypes.addressof(sec))
     if nv != m.num_vars:
         raise RuntimeError(f"reference DC failed ({nv})")
     return sol, it.value, sec.value
@@ -405,13 +435,13 @@ def ref_sim_sens(desc: str, output_node: int):
     return out[:k], val.value
 
 
-def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0):
+def ref_sim(desc: str, analysis: int = 1, tstep: float = 0.0, tstop: float = 0.0, lib=None):
     """Run a circuit description (see nsref_sim_run in ref_shim.cpp) through
     the reference: analysis 0 = DC operating point, 1 = transient, 2 / 3 / 4
     = the reference's source_stepping / gain_stepping / pseudo_transient
     alone (info["method"] 2, 2, 3 when it converged, -1 when not).  Returns (times, values [npoints x
     width], info dict)."""
-    lib = ref()
+    lib = lib if lib is not None else ref()
     h = lib.nsref_sim_run(desc.encode(), int(analysis), float(tstep), float(tstop))
     try:
         nn, nv, npts, it, rej = (ctypes.c_int() for _ in range(5))

@@ -1,0 +1,108 @@
+// Test infrastructure only: the reference's own analyses running on this
+// repository's GPU solver through the reference's solver seam.
+//
+// GpuNeoSolver below is the ISolver adapter a maintainer adds to the
+// reference (src/core/solver_iface.hpp:16-41) to put libnsgpu under its
+// Newton loop.  This file is linked (oracle/Makefile, target `seam`) with the
+// reference's own objects into oracle/_ref/libnsseam.so, with make_solver's
+// definition renamed in its object file to reference_make_solver, so that
+// the make_solver below is the one solve_dc (src/core/dc.cpp:80),
+// solve_transient (src/core/transient.cpp:713-727) and every other caller
+// reach: with the GPU seam switched on it returns a GpuNeoSolver on the
+// engine the reference would pick (nsg_solver_select = make_solver's
+// policy); switched off, the reference's own solver.  The tests then compare
+// the reference's analyses on both engines.
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "core/matrix.hpp"
+#include "core/neo_solver.hpp"
+#include "core/solver_iface.hpp"
+#include "nsgpu_solver.hpp"
+
+namespace neospice {
+
+// make_solver of src/core/make_solver.cpp:156-178, renamed at link time.
+std::unique_ptr<ISolver> reference_make_solver(int num_vars, bool is_linear);
+
+namespace {
+
+long long g_gpu_solvers = 0;  // GpuNeoSolver objects created
+bool g_gpu_seam = false;
+
+class GpuNeoSolver : public ISolver {
+public:
+    explicit GpuNeoSolver(int engine) : gpu_(engine) { ++g_gpu_solvers; }
+
+    void symbolic(const SparsityPattern& pattern) override {
+        CSCData csc = pattern.to_csc();
+        gpu_.symbolic(pattern.size(), csc.col_ptr, csc.row_idx);
+        nnz_ = pattern.nnz();
+        pattern_ = &pattern;  // the caller keeps the pattern alive (make_solver.cpp:76-82)
+    }
+    bool numeric(const SparsityPattern& p, const NumericMatrix& mat, double diag_gmin) override {
+        if (equilibrate_) return cpu_.numeric(p, mat, diag_gmin);
+        return gpu_.numeric(values(mat), diag_gmin);  // true = singular, as NeoSolver
+    }
+    bool refactorize(const NumericMatrix& mat, double diag_gmin) override {
+        if (equilibrate_) return cpu_.refactorize(mat, diag_gmin);
+        return gpu_.refactorize(values(mat), diag_gmin);
+    }
+    void solve(std::vector<double>& rhs) override {
+        if (equilibrate_) cpu_.solve(rhs);
+        else gpu_.solve(rhs);
+    }
+    // Equilibration (solve_dc's last aid, dc.cpp:355-387) stays on the CPU
+    // NeoSolver; it must follow symbolic().
+    void set_equilibrate(bool on) override {
+        if (on && !pattern_)
+            throw std::logic_error("GpuNeoSolver::set_equilibrate before symbolic()");
+        if (on && !equilibrate_) cpu_.symbolic(*pattern_);
+        equilibrate_ = on;
+        cpu_.set_equilibrate(on);
+    }
+    // Complex (AC) paths stay on the CPU solver.
+    void numeric_complex(const SparsityPattern& p, const std::vector<double>& ax) override {
+        cpu_.symbolic(p);
+        cpu_.numeric_complex(p, ax);
+    }
+    bool refactorize_complex(const std::vector<double>& ax) override {
+        return cpu_.refactorize_complex(ax);
+    }
+    void solve_complex(std::vector<double>& rhs) override { cpu_.solve_complex(rhs); }
+    const char* name() const override { return equilibrate_ ? cpu_.name() : gpu_.name(); }
+
+private:
+    std::vector<double> values(const NumericMatrix& m) const {
+        return std::vector<double>(m.data(), m.data() + nnz_);
+    }
+    nsgpu::GpuSolver gpu_;
+    NeoSolver cpu_;
+    const SparsityPattern* pattern_ = nullptr;
+    bool equilibrate_ = false;
+    int nnz_ = 0;
+};
+
+}  // namespace
+
+std::unique_ptr<ISolver> make_solver(int num_vars, bool is_linear) {
+    if (g_gpu_seam)
+        return std::make_unique<GpuNeoSolver>(nsg_solver_select(num_vars, is_linear ? 1 : 0));
+    return reference_make_solver(num_vars, is_linear);
+}
+
+}  // namespace neospice
+
+extern "C" {
+
+// Route every make_solver of the reference through GpuNeoSolver (on != 0)
+// or back to its own solvers.
+void nsseam_use_gpu(int on) { neospice::g_gpu_seam = on != 0; }
+
+// GpuNeoSolver objects created so far (proof that the seam was used).
+long long nsseam_gpu_solvers(void) { return neospice::g_gpu_solvers; }
+
+}  // extern "C"

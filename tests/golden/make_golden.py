@@ -58,6 +58,17 @@ order q, row pivots pinv, L and U exactly as the solver stores them), the
 factor after refactorize() on second values (with the replay / fallback
 counters), a right-hand side and the reference's solution.
 
+bsim4.npz: BSIM4v7 (LEVEL=14) circuits.  DC cases: the reference's own
+unit-test operating point (tests/unit/test_bsim4v7_ucb_load.cpp: NMOS
+VTH0=0.4 U0=0.04 TOXE=2e-9, W/L = 1u/100n at VDS 0.1, VGS 0.8), NMOS and
+PMOS bias points, and inverter / NAND circuits with per-device TOXE and
+DELVTO; per case the netlist, solve_dc's solution, Newton iterations and
+method.  Transient cases: a BSIM4v7 inverter chain under a PULSE, and
+Monte Carlo instances of the 200-MOSFET ring-oscillator + NAND-chain
+circuit (neospice_b200.workloads.bsim4_ring_nand) over 1 ns; per case the
+timepoints, the voltages at the recorded probe nodes, the Newton
+iterations and rejected steps.
+
 Run from the repository root: ``python tests/golden/make_golden.py``.
 """
 from __future__ import annotations
@@ -560,9 +571,85 @@ def amd_main():
     print(f"wrote {len(cases)} AMD-LU cases to {path}")
 
 
+def bsim4_dc_netlists():
+    """DC cases of bsim4.npz."""
+    from neospice_b200 import workloads as W
+    cases = []
+    golden = {"LEVEL": 14, "VTH0": 0.4, "U0": 0.04, "TOXE": 2e-9}
+    # the reference's unit-test operating point (Id = 5.754970e-05 in ngspice)
+    cases.append(W.Netlist(3, [("V", 0, -1, 0.1), ("V", 1, -1, 0.8), ("V", 2, -1, 0.0),
+                               ("M", 0, 1, -1, 2, "nmod", 1e-6, 1e-7)], {"nmod": ("nmos", golden)}))
+    for vd, vg, vb in ((1.2, 1.2, 0.0), (0.05, 0.3, -0.4), (-0.3, 0.9, 0.0), (0.9, 0.2, 0.3)):
+        cases.append(W.Netlist(3, [("V", 0, -1, vd), ("V", 1, -1, vg), ("V", 2, -1, vb),
+                                   ("M", 0, 1, -1, 2, "n", 2e-7, 9e-8)],
+                               {"n": ("nmos", {"LEVEL": 14})}))
+    for vd, vg in ((-1.2, -1.2), (-0.4, -0.9), (0.2, -1.0)):
+        cases.append(W.Netlist(3, [("V", 0, -1, vd), ("V", 1, -1, vg), ("V", 2, -1, 0.0),
+                                   ("M", 0, 1, -1, 2, "p", 4e-7, 9e-8)],
+                               {"p": ("pmos", {"LEVEL": 14, "TOXE": 2.9e-9})}))
+    for k, vin in enumerate((0.0, 0.4, 0.6, 1.2)):
+        rng = np.random.default_rng([61, k])
+        dev = [("V", 0, -1, 1.2), ("V", 1, -1, vin)]
+        models = {}
+        for st in range(3):
+            inp, out = 1 + st, 2 + st
+            for kind, d, s_, w in (("n", out, -1, 2e-7), ("p", out, 0, 4e-7)):
+                name = f"{kind}{st}"
+                models[name] = ("nmos" if kind == "n" else "pmos",
+                                {"LEVEL": 14, "TOXE": 3e-9 * (1 + 0.03 * (2 * rng.random() - 1))})
+                dev.append(("M", d, inp, s_, s_ if s_ >= 0 else -1, name, w, 9e-8,
+                            float(0.03 * rng.standard_normal())))
+        cases.append(W.Netlist(5, dev, models))
+    return cases
+
+
+def bsim4_tran_cases():
+    """Transient cases of bsim4.npz: (netlist, tstep, tstop, probe nodes)."""
+    from neospice_b200 import workloads as W
+    chain = W.Netlist(5, [("V", 0, -1, 1.2),
+                          ("VPULSE", 1, -1, 0.0, 1.2, 2e-11, 5e-11, 5e-11, 3e-10, 8e-10)] +
+                      [x for st in range(3) for x in (
+                          ("M", 2 + st, 1 + st, -1, -1, "n", 2e-7, 9e-8),
+                          ("M", 2 + st, 1 + st, 0, 0, "p", 4e-7, 9e-8),
+                          ("C", 2 + st, -1, 2e-15))],
+                      {"n": ("nmos", {"LEVEL": 14}), "p": ("pmos", {"LEVEL": 14})})
+    cases = [(chain, 1e-12, 1.6e-9, list(range(5)))]
+    for k in range(2):
+        nl = W.bsim4_ring_nand(np.random.default_rng([31, k]))
+        cases.append((nl, 1e-12, 1e-9, [0, 1, 2, 7, 13, 26, 27, 99, 100]))
+    return cases
+
+
+def bsim4_main():
+    import json
+    import netlists
+    rec = {}
+    dc = bsim4_dc_netlists()
+    for k, nl in enumerate(dc):
+        _, v, info = oracle.ref_sim(netlists.ref_desc(nl), 0)
+        p = f"d{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "solution": v[0], p + "iterations": np.int32(info["iterations"]),
+                    p + "method": np.int32(info["method"])})
+    rec["dc_count"] = np.int32(len(dc))
+    tr = bsim4_tran_cases()
+    for k, (nl, tstep, tstop, probes) in enumerate(tr):
+        t, v, info = oracle.ref_sim(netlists.ref_desc(nl), 1, tstep, tstop)
+        p = f"t{k:02d}_"
+        rec.update({p + "netlist": np.array(json.dumps([nl.num_nodes, nl.devices, nl.models])),
+                    p + "tstep": np.float64(tstep), p + "tstop": np.float64(tstop),
+                    p + "probes": np.array(probes, np.int32), p + "times": t,
+                    p + "values": v[:, probes], p + "iterations": np.int32(info["iterations"]),
+                    p + "rejected": np.int32(info["rejected"])})
+    rec["tran_count"] = np.int32(len(tr))
+    path = pathlib.Path(__file__).with_name("bsim4.npz")
+    np.savez_compressed(path, **rec)
+    print(f"wrote {len(dc)} BSIM4v7 operating points and {len(tr)} transients to {path}")
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["solver", "mesh", "tran", "trandiode", "mos", "aids", "step", "sens",
-                             "amd", "linear"]
+                             "amd", "linear", "bsim4"]
     if "amd" in which:
         amd_main()
     if "linear" in which:
@@ -583,3 +670,5 @@ if __name__ == "__main__":
         step_main()
     if "sens" in which:
         sens_main()
+    if "bsim4" in which:
+        bsim4_main()

@@ -204,3 +204,29 @@ def load_linear():
                                {k2: (t, p2) for k2, (t, p2) in models.items()})
         out.append(d)
     return out
+
+
+BSIM4_PATH = pathlib.Path(__file__).resolve().parent / "golden" / "bsim4.npz"
+
+
+def _netlist_of(d):
+    import json
+    from neospice_b200.workloads import Netlist
+    nn, dev, models = json.loads(str(d["netlist"]))
+    return Netlist(nn, [tuple(x) for x in dev], {k: (t, p) for k, (t, p) in models.items()})
+
+
+def load_bsim4():
+    """(dc cases, transient cases) of bsim4.npz, each a dict with the
+    netlist rebuilt."""
+    z = np.load(BSIM4_PATH)
+    out = []
+    for pre, count in (("d", int(z["dc_count"])), ("t", int(z["tran_count"]))):
+        cases = []
+        for k in range(count):
+            p = f"{pre}{k:02d}_"
+            d = {key[len(p):]: z[key] for key in z.files if key.startswith(p)}
+            d["netlist"] = _netlist_of(d)
+            cases.append(d)
+        out.append(cases)
+    return out[0], out[1]

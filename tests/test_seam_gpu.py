@@ -1,0 +1,72 @@
+"""The drop-in claim, end to end: the reference's own analyses -- solve_dc
+(src/core/dc.cpp, with its Newton loop and continuation aids) and
+solve_transient (src/core/transient.cpp) -- run unmodified with this
+repository's GPU solver under them, through the reference's ISolver seam
+(oracle/gpu_seam.cpp: GpuNeoSolver, the adapter a maintainer adds, returned
+by make_solver).  Every solution, timepoint and iteration count must equal
+those of the same analyses on the reference's own NeoSolver / AmdLuSolver,
+bit for bit: the GPU factors and solves are bit-identical to the CPU ones,
+so the whole Newton sequence is."""
+import numpy as np
+import pytest
+
+import golden_cases
+import netlists
+import oracle
+from neospice_b200 import workloads as W
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not oracle.have_seam(), reason="seam library not built")]
+
+
+def _both(desc, analysis, tstep=0.0, tstop=0.0):
+    lib = oracle.seam()
+    out = []
+    for on in (0, 1):
+        lib.nsseam_use_gpu(on)
+        try:
+            out.append(oracle.ref_sim(desc, analysis, tstep, tstop, lib=lib))
+        finally:
+            lib.nsseam_use_gpu(0)
+    return out
+
+
+def test_reference_solve_dc_on_gpu_solver():
+    lib = oracle.seam()
+    before = lib.nsseam_gpu_solvers()
+    nls = [g["netlist"] for g in golden_cases.load_mos_dc()]
+    nls += [W.resistor_network(np.random.default_rng([72, k]), 12) for k in range(2)]
+    nls.append(W.resistor_network(np.random.default_rng([72, 9]), 300))  # AMD-LU range
+    for k, nl in enumerate(nls):
+        (_, v_cpu, i_cpu), (_, v_gpu, i_gpu) = _both(netlists.ref_desc(nl), 0)
+        np.testing.assert_array_equal(v_gpu, v_cpu, err_msg=f"case {k}")
+        assert i_gpu["iterations"] == i_cpu["iterations"], k
+        assert i_gpu["method"] == i_cpu["method"], k
+    assert lib.nsseam_gpu_solvers() >= before + len(nls)
+
+
+def test_reference_mesh_dc_on_gpu_solver():
+    lib = oracle.seam()
+    for k in range(3):
+        m = W.diode_mesh(np.random.default_rng([73, k]), side_range=(8, 20))
+        lib.nsseam_use_gpu(0)
+        s_cpu, it_cpu, _ = oracle.ref_mesh_dc(m, lib=lib)
+        lib.nsseam_use_gpu(1)
+        try:
+            s_gpu, it_gpu, _ = oracle.ref_mesh_dc(m, lib=lib)
+        finally:
+            lib.nsseam_use_gpu(0)
+        np.testing.assert_array_equal(s_gpu, s_cpu)
+        assert it_gpu == it_cpu
+
+
+def test_reference_solve_transient_on_gpu_solver():
+    cases = golden_cases.load_transients()
+    for k in (0, 1, 2):
+        g = cases[k]
+        (t_cpu, v_cpu, i_cpu), (t_gpu, v_gpu, i_gpu) = _both(
+            netlists.ref_desc(g["netlist"]), 1, float(g["tstep"]), float(g["tstop"]))
+        np.testing.assert_array_equal(t_gpu, t_cpu, err_msg=f"case {k}")
+        np.testing.assert_array_equal(v_gpu, v_cpu, err_msg=f"case {k}")
+        assert i_gpu["iterations"] == i_cpu["iterations"]
+        assert i_gpu["rejected"] == i_cpu["rejected"]
