@@ -30,6 +30,7 @@ Besides the headline, the line carries (at N = 1):
                     central-difference and .sens parity;
   bsim4_mc          BSIM4v7 Monte Carlo transient of a 200-MOSFET ring +
                     NAND circuit, batched and plain, with sampled parity;
+  ac_sweep          batched complex refactor + solve of an AC sweep;
   power_grid        the single-topology AMD-LU refactor/solve case.
 """
 from __future__ import annotations
@@ -80,6 +81,10 @@ def _args():
                     help="instances of the batched inverter-chain transient")
     ap.add_argument("--bsim4-batch", type=int, default=2048,
                     help="Monte Carlo instances of the BSIM4v7 ring + NAND transient (0 = skip)")
+    ap.add_argument("--ac-points", type=int, default=1024,
+                    help="frequency points of the batched AC sweep section (0 = skip)")
+    ap.add_argument("--ac-side", type=int, default=64,
+                    help="side of the RC mesh of the AC sweep section")
     return ap.parse_args()
 
 
@@ -431,6 +436,11 @@ def run_ours(a, rank, world, local_rank):
                 line["adjoint"]["parity"] = adjoint_parity()
             except Exception as exc:
                 line["adjoint"]["parity"] = {"error": str(exc)}
+        if a.ac_points > 0 and world == 1:
+            try:
+                line["ac_sweep"] = ac_sweep(a.ac_side, a.ac_points)
+            except Exception as exc:
+                line["ac_sweep"] = {"error": str(exc)}
         if not a.no_power_grid and world == 1:
             try:
                 line["power_grid"] = power_grid_refactor(a.grid_side, a.steps, a.warmup)
@@ -857,6 +867,104 @@ def adjoint_parity(nodes=500, instances=2, per_instance=24, every=32, h_rel=1e-6
                               "tolerance": "5e-3 relative + 1e-6 x max |sens|"}
     except Exception as exc:
         out["dc_sens"] = {"error": str(exc)}
+    return out
+
+
+# --- batched AC sweep (complex refactor + solve) -----------------------------------
+
+def ac_sweep(side, points, ref_sample=16):
+    """AC sweep of a side x side RC mesh (workloads.rc_mesh, n = side^2 + 1
+    + 1): the pivots of the first frequency point ordered on the host
+    (NeoSolver::numeric_complex), then all `points` log-spaced frequency
+    points (1 kHz .. 100 GHz) refactored (factor_complex) and solved
+    (solve_complex) in one batch on the GPU, timed with CUDA events; the
+    reference's NeoSolver refactorize_complex + solve_complex per point on
+    one host core over `ref_sample` points, with bitwise parity of those
+    points' solutions."""
+    import numpy as np
+    import torch
+    from neospice_b200 import workloads as W
+    from neospice_b200.solver import Batch, Topology, _interleave
+
+    nl = W.rc_mesh(np.random.default_rng(2027), side)
+    n, cp, ri, g, c, b = W.ac_system(nl)
+    freqs = np.logspace(3, 11, points)
+    omegas = 2 * np.pi * freqs
+    ax = np.empty((points, 2 * len(ri)))
+    ax[:, 0::2] = g[None, :]
+    ax[:, 1::2] = omegas[:, None] * c[None, :]
+    t0 = time.perf_counter()
+    topo = Topology.order_complex(n, cp, ri, ax[0])
+    t_sym = time.perf_counter() - t0
+    info = topo.info()
+    batch = Batch([topo] * points)
+    d_ax = torch.from_numpy(ax.ravel()).cuda()
+    bz = _interleave(b)
+    d_b = torch.from_numpy(np.tile(bz, points)).cuda()
+    d_x = torch.empty_like(d_b)
+    d_lu, st = batch.refactor_complex(d_ax)
+    d_x.copy_(d_b)
+    batch.solve_complex(d_lu, d_x)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    reps = 3
+    ev[0].record()
+    for _ in range(reps):
+        batch.refactor_complex(d_ax, d_lu, st)
+    ev[1].record()
+    for _ in range(reps):
+        d_x.copy_(d_b)
+        batch.solve_complex(d_lu, d_x)
+    ev[2].record()
+    torch.cuda.synchronize()
+    t_ref = ev[0].elapsed_time(ev[1]) / 1e3 / reps
+    t_sol = ev[1].elapsed_time(ev[2]) / 1e3 / reps
+    ok = int((st.cpu().numpy() == 0).sum())
+    x = d_x.cpu().numpy()
+    nnz, nlu, upd = len(ri), info["nnz_lu"], info["updates"]
+    # compulsory bytes per point: complex A in, complex LU out, index stream,
+    # then the sweeps (complex LU and vectors)
+    b_ref = 16 * nnz + 16 * nlu + 4 * (nlu + n) + 16 * n
+    b_sol = 24 * nlu + 32 * n
+    peak, peak_kind = measured_peaks()
+    out = {
+        "workload": f"AC sweep of a {side}x{side} RC mesh (n={n}), {points} log-spaced frequency "
+                    "points 1 kHz..100 GHz, complex FP64: one host ordering, then every point "
+                    "refactored (fixed pivots) and solved in one batch",
+        "value": round(points / (t_ref + t_sol), 2), "unit": "frequency points/s",
+        "refactor_ms": round(1e3 * t_ref, 3), "solve_ms": round(1e3 * t_sol, 3), "ok": ok,
+        "host_symbolic_s": round(t_sym, 4), "nnz": nnz, "nnz_lu": nlu,
+        "complex_updates_per_point": upd,
+        "refactor_gbs": round(points * b_ref / t_ref / 1e9, 2),
+        "refactor_frac_hbm": round(points * b_ref / t_ref / 1e9 / peak, 5),
+        "refactor_fp64_gflops": round(points * 8.0 * upd / t_ref / 1e9, 2),
+        "solve_gbs": round(points * b_sol / t_sol / 1e9, 2), "peak_gbs": peak,
+        "peak_source": peak_kind,
+    }
+    try:
+        import oracle
+        if oracle.have_ref():
+            rs = oracle.RefSolver(n, cp, ri)
+            rs.numeric_complex(ax[0])
+            pick = sorted({int(round(v)) for v in np.linspace(1, points - 1, ref_sample)})
+            worst_equal = True
+            t0 = time.perf_counter()
+            sols = []
+            for k in pick:
+                rs.refactorize_complex(ax[k])
+                sols.append(rs.solve_complex(b))
+            t_cpu = (time.perf_counter() - t0) / len(pick)
+            for k, xr in zip(pick, sols):
+                v = 2 * int(batch.vector_offsets[k])
+                xk = x[v:v + 2 * n]
+                worst_equal &= bool(np.array_equal(xk[0::2], xr.real) and
+                                    np.array_equal(xk[1::2], xr.imag))
+            out["cpu_reference_1core"] = {"value": round(1.0 / t_cpu, 2), "unit": "frequency points/s",
+                                          "sample": f"{len(pick)} points, refactorize_complex + "
+                                                    "solve_complex"}
+            out["parity"] = {"points_checked": len(pick), "bitwise_equal": worst_equal}
+    except Exception as exc:
+        out["parity"] = {"error": str(exc)}
     return out
 
 

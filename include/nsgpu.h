@@ -125,6 +125,16 @@ int nsg_topology_export(const nsg_topology* topo, int* int_to_ext_row,
                         int* int_to_ext_col, int* elem_row, int* elem_col,
                         int* slot_to_elem);
 
+/* NeoSolver::numeric_complex (src/core/neo_solver.cpp:228-245): the
+ * symbolic phase on complex values ax (2*nnz doubles, (re, im) per CSC slot):
+ * MNA pre-order and Markowitz order_and_factor with magnitudes |re| + |im|
+ * and complex eliminations (src/solver/factor.cpp:769-806), pivot sequence
+ * bit-identical to the reference's.  The AC sweep's first frequency point
+ * (src/core/ac.cpp:205-209).  Returns NSG_SINGULAR (and no topology) on a
+ * singular matrix, which the reference does not report. */
+int nsg_topology_order_complex(int n, int nnz, const int* col_ptr, const int* row_idx,
+                               const double* ax, nsg_topology** out);
+
 void nsg_topology_free(nsg_topology* topo);
 
 /* ---- Batches (device) -----------------------------------------------------
@@ -202,6 +212,20 @@ int nsg_batch_solve_transposed(nsg_batch* batch, double* d_x, void* stream);
  *     call's contents; nothing in it has to start at zero. */
 #define NSG_STATIC_SCRATCH_DOUBLES (1LL << 20)
 int nsg_batch_solve_static_scratch(nsg_batch* batch, double* d_x, void* stream);
+
+/* Batched AC: SparseMatrix::factor_complex (refactorize_complex,
+ * src/solver/factor.cpp:1054-1141) of every instance with the plan's fixed
+ * pivots.  d_ax: complex values interleaved (re, im), 2*value_offsets per
+ * instance (nsg_batch_layout); d_lu: caller-owned device buffer of
+ * 2*lu_offsets[count] doubles receiving the factors (same positions as the
+ * real LU, interleaved); d_status per instance: 0, 102 (zero pivot) or 104.
+ * Markowitz plans only (the reference's AC uses NeoSolver). */
+int nsg_batch_refactor_complex(nsg_batch* batch, const double* d_ax, double* d_lu, int* d_status,
+                               void* stream);
+/* SparseMatrix::solve_complex (src/solver/solve.cpp:49-100) on d_lu: d_x
+ * holds b on entry and x on return, interleaved, 2*vector_offsets per
+ * instance.  The first call allocates the batch's complex sweep workspace. */
+int nsg_batch_solve_complex(nsg_batch* batch, const double* d_lu, double* d_x, void* stream);
 
 /* Device pointer to the factored LU values (layout per nsg_batch_layout and
  * the topology export: L unscaled, U scaled by the reciprocal pivot, pivots

@@ -57,6 +57,10 @@ SIGNATURES = {
                                   P(c_int), P(c_int)]),
     "nsg_topology_export": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int), P(c_int), P(c_int)]),
     "nsg_topology_free": (None, [c_void_p]),
+    "nsg_topology_order_complex": (c_int, [c_int, c_int, P(c_int), P(c_int), P(c_double),
+                                           P(c_void_p)]),
+    "nsg_batch_refactor_complex": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "nsg_batch_solve_complex": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "nsg_batch_create": (c_int, [c_int, P(c_void_p), P(c_void_p)]),
     "nsg_batch_free": (None, [c_void_p]),
     "nsg_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll), P(c_ll)]),

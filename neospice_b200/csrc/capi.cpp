@@ -31,6 +31,13 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
                                  double* lrows, double* urows, void* scratch,
                                  cudaStream_t stream);
+cudaError_t launch_complex_refactor(const PlanDesc* plans, const int32_t* pool,
+                                    const InstDesc* insts, int count, int max_n, const double* A,
+                                    double* LU, int32_t* status, cudaStream_t stream);
+cudaError_t launch_complex_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
+                                 int count, const double* LU, double* X, double* W,
+                                 cudaStream_t stream);
+size_t complex_refactor_smem(int max_n);
 cudaError_t launch_grid_solve(const PlanDesc* plans, const int32_t* pool, const InstDesc* insts,
                               int count, const int32_t* n_of, const double* LU,
                               const double* lrows, const double* urows, double* X, double* W,
@@ -424,6 +431,39 @@ int nsg_topology_export(const nsg_topology* topo, int* int_to_ext_row, int* int_
     return NSG_OK;
 }
 
+int nsg_topology_order_complex(int n, int nnz, const int* col_ptr, const int* row_idx,
+                               const double* ax, nsg_topology** out) {
+    return guarded("nsg_topology_order_complex", [&]() -> int {
+        if (!out || n <= 0 || nnz <= 0 || !col_ptr || !row_idx || !ax)
+            return fail(NSG_ERR_INVALID, "nsg_topology_order_complex: bad arguments");
+        *out = nullptr;
+        if (col_ptr[0] != 0 || col_ptr[n] != nnz || !valid_csc(n, col_ptr, row_idx))
+            return fail(NSG_ERR_INVALID, "nsg_topology_order_complex: malformed CSC pattern");
+        auto t = std::make_unique<nsg_topology>();
+        make_markowitz(*t, n, col_ptr, row_idx);
+        t->committed = true;
+        auto& mo = *t->engine;
+        // NeoSolver::numeric_complex (src/core/neo_solver.cpp:228-245):
+        // load_complex, the MNA pre-order, order_and_factor(relThr 1e-3,
+        // absThr 1e-13, diagonal pivoting) on the complex values.
+        mo.set_complex(true);
+        mo.clear_fillins();
+        for (size_t k = 0; k < t->slot_elem.size(); ++k) {
+            mo.value(t->slot_elem[k]) = ax[2 * k];
+            mo.value_imag(t->slot_elem[k]) = ax[2 * k + 1];
+        }
+        mo.mna_preorder();
+        const nsg::OrderStatus st = mo.order_and_factor(1e-3, 1e-13, true);
+        if (st == nsg::OrderStatus::no_memory)
+            return fail(NSG_ERR_NOMEM, "nsg_topology_order_complex: out of memory");
+        if (st == nsg::OrderStatus::singular)
+            return fail(NSG_SINGULAR, "nsg_topology_order_complex: singular matrix");
+        rebuild_plan(*t);
+        *out = t.release();
+        return NSG_OK;
+    });
+}
+
 void nsg_topology_free(nsg_topology* topo) { delete topo; }
 
 int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
@@ -490,6 +530,33 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
 }
 
 void nsg_batch_free(nsg_batch* batch) { delete batch; }
+
+int nsg_batch_refactor_complex(nsg_batch* b, const double* d_ax, double* d_lu, int* d_status,
+                               void* stream) {
+    if (!b || !d_ax || !d_lu || !d_status)
+        return fail(NSG_ERR_INVALID, "nsg_batch_refactor_complex: null argument");
+    const size_t smem = nsg::complex_refactor_smem(b->max_n);
+    if (smem > 200 * 1024)
+        return fail(NSG_ERR_INVALID, "nsg_batch_refactor_complex: too many unknowns per instance "
+                                     "for the shared-memory completion flags");
+    const cudaError_t e = nsg::launch_complex_refactor(b->d_plans, b->d_pool, b->d_insts, b->count,
+                                                       b->max_n, d_ax, d_lu, d_status,
+                                                       static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor_complex", e);
+}
+
+int nsg_batch_solve_complex(nsg_batch* b, const double* d_lu, double* d_x, void* stream) {
+    if (!b || !d_lu || !d_x) return fail(NSG_ERR_INVALID, "nsg_batch_solve_complex: null argument");
+    cudaError_t e = cudaSuccess;
+    if (!b->d_cwork) {
+        e = cudaMalloc(reinterpret_cast<void**>(&b->d_cwork),
+                       sizeof(double) * 2 * static_cast<size_t>(std::max<long long>(1, b->x_off[b->count])));
+        if (e != cudaSuccess) return cuda_fail("nsg_batch_solve_complex: workspace", e);
+    }
+    e = nsg::launch_complex_solve(b->d_plans, b->d_pool, b->d_insts, b->count, d_lu, d_x,
+                                  b->d_cwork, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_solve_complex", e);
+}
 
 int nsg_batch_layout(const nsg_batch* b, long long* value_offsets, long long* vector_offsets,
                      long long* lu_offsets) {

@@ -56,7 +56,9 @@ struct nsg_batch {
     int schedule = 0;             // nsg_batch_set_schedule
     std::vector<int32_t> n_of;    // unknowns of the instance in each slot of d_insts
     void* d_grid = nullptr;       // flags and state of the grid-wide schedule
+    double* d_cwork = nullptr;    // complex sweep workspace (2 doubles per unknown)
     ~nsg_batch() {
+        cudaFree(d_cwork);
         cudaFree(d_grid);
         cudaFree(d_pool);
         cudaFree(d_plans);

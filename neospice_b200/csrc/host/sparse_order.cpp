@@ -34,7 +34,10 @@ MarkowitzOrder::MarkowitzOrder(int32_t size) : size_(size) {
     pool_.reserve(static_cast<size_t>(alloc) * 10);
 }
 
-double MarkowitzOrder::mag(int32_t e) const { return std::fabs(pool_[e].val); }
+// element_mag: |re| + |im| (the imaginary part stays 0 for real values).
+double MarkowitzOrder::mag(int32_t e) const {
+    return std::fabs(pool_[e].val) + std::fabs(pool_[e].imag);
+}
 
 // External indices get internal numbers in order of first appearance, row
 // index before column index (src/solver/build.cpp:197-249).
@@ -118,7 +121,7 @@ int32_t MarkowitzOrder::get_element(int32_t ext_row, int32_t ext_col) {
 
 void MarkowitzOrder::clear_fillins() {
     for (auto& el : pool_)
-        if (el.fill) el.val = 0.0;
+        if (el.fill) el.val = el.imag = 0.0;
 }
 
 // --- MNA pre-ordering: swap +-1 "twin" columns so that a voltage source's
@@ -612,6 +615,50 @@ void MarkowitzOrder::eliminate(int32_t pivot) {
     }
 }
 
+// Complex right-looking elimination (src/solver/factor.cpp:769-806): the
+// pivot replaced by its reciprocal (complex_ops::reciprocal), U(r, c) *=
+// that reciprocal (mult_assign), a(i, c) -= U(r, c) * L(i, r)
+// (mult_subt_assign), each with the reference's operand grouping.
+void MarkowitzOrder::eliminate_complex(int32_t pivot) {
+    Element& pv = pool_[pivot];
+    if (std::fabs(pv.val) + std::fabs(pv.imag) == 0.0) {
+        error_ = OrderStatus::singular;
+        return;
+    }
+    {
+        const double den_r = pv.val, den_i = pv.imag;
+        if ((den_r >= den_i && den_r > -den_i) || (den_r < den_i && den_r <= -den_i)) {
+            const double r = den_i / den_r;
+            pv.val = 1.0 / (den_r + r * den_i);
+            pv.imag = -r * pv.val;
+        } else {
+            const double r = den_r / den_i;
+            pv.imag = -1.0 / (den_i + r * den_r);
+            pv.val = -r * pv.imag;
+        }
+    }
+    const double pr = pool_[pivot].val, pi = pool_[pivot].imag;
+    for (int32_t up = pool_[pivot].next_in_row; up != kNone; up = pool_[up].next_in_row) {
+        {
+            const double tmp = pool_[up].val;
+            pool_[up].val = tmp * pr - pool_[up].imag * pi;
+            pool_[up].imag = tmp * pi + pool_[up].imag * pr;
+        }
+        const double ur = pool_[up].val, ui = pool_[up].imag;
+        const int32_t ucol = pool_[up].col;
+        int32_t sub = pool_[up].next_in_col;
+        for (int32_t lo = pool_[pivot].next_in_col; lo != kNone; lo = pool_[lo].next_in_col) {
+            const int32_t row = pool_[lo].row;
+            while (sub != kNone && pool_[sub].row < row) sub = pool_[sub].next_in_col;
+            if (sub == kNone || pool_[sub].row > row) sub = create_fillin(row, ucol);
+            const double lr = pool_[lo].val, li = pool_[lo].imag;
+            pool_[sub].val -= ur * lr - ui * li;
+            pool_[sub].imag -= ur * li + ui * lr;
+            sub = pool_[sub].next_in_col;
+        }
+    }
+}
+
 void MarkowitzOrder::update_markowitz(int32_t pivot) {
     for (int32_t e = pool_[pivot].next_in_col; e != kNone; e = pool_[e].next_in_col) {
         const int32_t row = pool_[e].row;
@@ -648,7 +695,8 @@ OrderStatus MarkowitzOrder::order_and_factor(double rel_threshold, double abs_th
             }
             const double largest = largest_in_col_from(pool_[p].next_in_col);
             if (largest * rel_threshold < mag(p)) {
-                eliminate(p);
+                if (complex_) eliminate_complex(p);
+                else eliminate(p);
             } else {
                 reorder = true;
                 break;
@@ -674,7 +722,8 @@ OrderStatus MarkowitzOrder::order_and_factor(double rel_threshold, double abs_th
         const int32_t p = search_for_pivot(step, diag_pivoting);
         if (p == kNone) return error_ = OrderStatus::singular;
         exchange(p, step);
-        eliminate(p);
+        if (complex_) eliminate_complex(p);
+        else eliminate(p);
         if (error_ != OrderStatus::ok) return error_;
         update_markowitz(p);
     }

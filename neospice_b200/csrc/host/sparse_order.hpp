@@ -34,9 +34,17 @@ public:
     // first ordering.
     int32_t get_element(int32_t ext_row, int32_t ext_col);
 
-    // Values of element ids.
+    // Values of element ids (real part, and imaginary part in complex mode).
     double& value(int32_t e) { return pool_[e].val; }
     double value(int32_t e) const { return pool_[e].val; }
+    double& value_imag(int32_t e) { return pool_[e].imag; }
+    double value_imag(int32_t e) const { return pool_[e].imag; }
+
+    // SparseMatrix::set_complex: complex values (AC).  Magnitudes become
+    // |re| + |im| (element_mag, src/solver/element.hpp:18-20) and the
+    // elimination complex_row_col_elimination (src/solver/factor.cpp:769-806).
+    void set_complex(bool on) { complex_ = on; }
+    bool is_complex() const { return complex_; }
 
     // NeoSolver::load_real + SparseMatrix::clear_for_load: originals are
     // overwritten by the caller; fill-ins are reset to zero here.
@@ -77,6 +85,7 @@ public:
 private:
     struct Element {
         double val = 0.0;
+        double imag = 0.0;
         int32_t row = 0;
         int32_t col = 0;
         int32_t next_in_row = -1;
@@ -89,6 +98,7 @@ private:
     bool needs_ordering_ = true;
     bool rows_linked_ = false;
     bool preordered_ = false;
+    bool complex_ = false;
     double rel_threshold_ = 1.0e-3;
     double abs_threshold_ = 0.0;
     OrderStatus error_ = OrderStatus::ok;
@@ -128,6 +138,7 @@ private:
     void swap_rows(int32_t r1, int32_t r2);
     void swap_columns(int32_t c1, int32_t c2);
     void eliminate(int32_t pivot);
+    void eliminate_complex(int32_t pivot);
     int32_t create_fillin(int32_t row, int32_t col);
     void update_markowitz(int32_t pivot);
 };

@@ -65,6 +65,18 @@ class Topology:
                                                   ctypes.byref(h)))
         return cls(h)
 
+    @classmethod
+    def order_complex(cls, n, col_ptr, row_idx, ax) -> "Topology":
+        """Symbolic phase of an AC sweep (NeoSolver::numeric_complex) on
+        complex values ax (complex array of nnz, or 2*nnz interleaved)."""
+        cp = np.ascontiguousarray(col_ptr, np.int32)
+        ri = np.ascontiguousarray(row_idx, np.int32)
+        v = _interleave(ax)
+        h = ctypes.c_void_p()
+        L.check(L.lib().nsg_topology_order_complex(int(n), len(ri), L.iptr(cp), L.iptr(ri),
+                                                   L.dptr(v), ctypes.byref(h)))
+        return cls(h)
+
     @property
     def solver(self) -> str:
         """Engine of the current plan: "markowitz" or "amdlu"."""
@@ -118,6 +130,17 @@ class Topology:
         if getattr(self, "_h", None) and L._lib is not None:
             L._lib.nsg_topology_free(self._h)
             self._h = None
+
+
+def _interleave(z) -> np.ndarray:
+    """(re, im) pairs of a complex array (or an interleaved float array)."""
+    z = np.asarray(z)
+    if np.iscomplexobj(z):
+        out = np.empty(2 * z.size)
+        out[0::2] = z.real
+        out[1::2] = z.imag
+        return out
+    return np.ascontiguousarray(z, np.float64)
 
 
 def _stream_ptr(stream):
@@ -179,6 +202,26 @@ class Batch:
 
     def solve_transposed(self, d_x, stream=None):
         L.check(L.lib().nsg_batch_solve_transposed(self._h, d_x.data_ptr(), _stream_ptr(stream)))
+        return d_x
+
+    # --- AC: complex values interleaved (re, im), twice the real offsets ---
+    def refactor_complex(self, d_ax, d_lu=None, d_status=None, stream=None):
+        """Batched factor_complex with the plans' pivots; returns (complex
+        LU device tensor, 2 doubles per LU position; status per instance)."""
+        import torch
+        if d_lu is None:
+            d_lu = torch.empty(2 * int(self.lu_offsets[-1]), dtype=torch.float64,
+                               device=d_ax.device)
+        if d_status is None:
+            d_status = torch.empty(self.count, dtype=torch.int32, device=d_ax.device)
+        L.check(L.lib().nsg_batch_refactor_complex(self._h, d_ax.data_ptr(), d_lu.data_ptr(),
+                                                   d_status.data_ptr(), _stream_ptr(stream)))
+        return d_lu, d_status
+
+    def solve_complex(self, d_lu, d_x, stream=None):
+        """Batched solve_complex in place on interleaved d_x."""
+        L.check(L.lib().nsg_batch_solve_complex(self._h, d_lu.data_ptr(), d_x.data_ptr(),
+                                                _stream_ptr(stream)))
         return d_x
 
     def lu_values(self):

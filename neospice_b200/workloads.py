@@ -388,3 +388,59 @@ def bsim4_ring_nand(rng: np.random.Generator | None = None, stages: int = 25, vd
         fet("n", and_out[k], o, GND, GND, w_n)
         fet("p", and_out[k], o, vddn, vddn, w_p)
     return Netlist(1 + S + 3 * S, dev, models)
+
+
+def ac_system(netlist: Netlist):
+    """The small-signal system of a linear R / C / V netlist for an AC sweep
+    (the matrices the reference's solve_ac builds, src/core/ac.cpp:113-140):
+    (n, col_ptr, row_idx, g, c, b) with G the conductance and source-incidence
+    values at the circuit's pattern slots, C the capacitor stamps (+C on the
+    diagonal slots of both terminals, -C on the two coupling slots) and b the
+    excitation: 1 V AC on the first voltage source's branch.  The matrix at
+    angular frequency w is G + jwC (ax = (g, w*c) per slot)."""
+    circ = netlist.build()
+    cp, ri = circ.pattern()
+    g, _ = circ.initial_matrix(0.0)
+    n = len(cp) - 1
+    c = np.zeros(len(ri))
+
+    def slot(r, col):
+        lo, hi = cp[col], cp[col + 1]
+        k = lo + int(np.searchsorted(ri[lo:hi], r))
+        assert k < hi and ri[k] == r
+        return k
+
+    for d in netlist.devices:
+        if d[0] != "C":
+            continue
+        a, b_, farads = d[1], d[2], d[3]
+        if a >= 0:
+            c[slot(a, a)] += farads
+        if b_ >= 0:
+            c[slot(b_, b_)] += farads
+        if a >= 0 and b_ >= 0:
+            c[slot(a, b_)] -= farads
+            c[slot(b_, a)] -= farads
+    b = np.zeros(n, dtype=complex)
+    branch = netlist.num_nodes  # branches follow the nodes; the first V source's
+    b[branch] = 1.0             # branch is the first branch unknown when it is the only one
+    return n, cp, ri, g, c, b
+
+
+def rc_mesh(rng: np.random.Generator, side: int, r_ohm=10.0, c_farad=1e-13,
+            sigma=0.1) -> Netlist:
+    """An RC mesh for AC sweeps: side x side nodes, lognormal resistors to
+    the four neighbours, a lognormal capacitor from every node to ground, a
+    source resistor from the 1 V (AC) source at node 0 into the corner."""
+    n = side * side
+    src = n
+    dev = [("V", src, GND, 1.0), ("R", src, 0, 50.0)]
+    for y in range(side):
+        for x in range(side):
+            k = y * side + x
+            if x + 1 < side:
+                dev.append(("R", k, k + 1, float(r_ohm * np.exp(sigma * rng.standard_normal()))))
+            if y + 1 < side:
+                dev.append(("R", k, k + side, float(r_ohm * np.exp(sigma * rng.standard_normal()))))
+            dev.append(("C", k, GND, float(c_farad * np.exp(sigma * rng.standard_normal()))))
+    return Netlist(n + 1, dev)

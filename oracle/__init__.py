@@ -132,6 +132,10 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.nsref_amdlu_sizes.argtypes = [_V, _V, _V]
         lib.nsref_amdlu_export.argtypes = [_V] * 9
         lib.nsref_make_solver_name.argtypes = [_I, _I, ctypes.c_char_p, _I]
+        lib.nsref_solver_numeric_complex.argtypes = [_V, _V]
+        lib.nsref_solver_refactor_complex.argtypes = [_V, _V]
+        lib.nsref_solver_solve_complex.argtypes = [_V, _V]
+        lib.nsref_solver_export_imag.argtypes = [_V, _V]
     return lib
 
 
@@ -210,6 +214,18 @@ def port_amd_solve(f: dict, lx, ux, b):
 
 # --- the reference itself ----------------------------------------------------
 
+def _interleaved(z) -> np.ndarray:
+    """(re, im) pairs of a complex array; an already interleaved float
+    array passes through."""
+    z = np.asarray(z)
+    if np.iscomplexobj(z):
+        out = np.empty(2 * z.size)
+        out[0::2] = z.real
+        out[1::2] = z.imag
+        return out
+    return np.ascontiguousarray(z, np.float64)
+
+
 class RefSolver:
     """The reference's NeoSolver on a CSC pattern, through the export shim."""
 
@@ -239,6 +255,29 @@ class RefSolver:
         if fn(self.h, _p(x)) != 0:
             raise RuntimeError("reference solve failed")
         return x
+
+    # --- complex (AC) path: values interleaved (re, im) per slot ---
+    def numeric_complex(self, ax) -> int:
+        v = _interleaved(ax)
+        return ref().nsref_solver_numeric_complex(self.h, _p(v))
+
+    def refactorize_complex(self, ax) -> int:
+        v = _interleaved(ax)
+        return ref().nsref_solver_refactor_complex(self.h, _p(v))
+
+    def solve_complex(self, b):
+        """Complex solve of b (complex array of n); returns a complex array."""
+        x = _interleaved(b).copy()
+        if ref().nsref_solver_solve_complex(self.h, _p(x)) != 0:
+            raise RuntimeError("reference complex solve failed")
+        return x[0::2] + 1j * x[1::2]
+
+    def export_complex(self):
+        """(Structure, complex element values) after a complex factor."""
+        st, re = self.export()
+        im = np.zeros(len(re))
+        ref().nsref_solver_export_imag(self.h, _p(im))
+        return st, re + 1j * im
 
     def export(self):
         ne = ref().nsref_solver_element_count(self.h)

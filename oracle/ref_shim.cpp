@@ -177,6 +177,53 @@ int nsref_solver_export(void* h, int* int_to_ext_row, int* int_to_ext_col,
     return e_idx;
 }
 
+// ---- complex (AC) path of NeoSolver (src/core/neo_solver.cpp:104-111,
+// 228-284) ------------------------------------------------------------------
+
+// NeoSolver::numeric_complex on interleaved (re, im) values, 2*nnz doubles.
+int nsref_solver_numeric_complex(void* h, const double* ax) {
+    auto* rs = static_cast<RefSolver*>(h);
+    try {
+        rs->solver.numeric_complex(rs->pattern, std::vector<double>(ax, ax + 2 * rs->nnz));
+    } catch (const std::exception&) {
+        return -1;
+    }
+    return 0;
+}
+
+// NeoSolver::refactorize_complex: 1 when singular.
+int nsref_solver_refactor_complex(void* h, const double* ax) {
+    auto* rs = static_cast<RefSolver*>(h);
+    try {
+        return rs->solver.refactorize_complex(std::vector<double>(ax, ax + 2 * rs->nnz)) ? 1 : 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
+// NeoSolver::solve_complex: rhs (2*n interleaved) in, solution out.
+int nsref_solver_solve_complex(void* h, double* rhs) {
+    auto* rs = static_cast<RefSolver*>(h);
+    std::vector<double> v(rhs, rhs + 2 * rs->n);
+    try {
+        rs->solver.solve_complex(v);
+    } catch (const std::exception&) {
+        return -1;
+    }
+    std::memcpy(rhs, v.data(), sizeof(double) * 2 * rs->n);
+    return 0;
+}
+
+// The imaginary parts of the factored elements, in nsref_solver_export's
+// element order.
+int nsref_solver_export_imag(void* h, double* elem_imag) {
+    auto* m = static_cast<RefSolver*>(h)->solver.matrix_.get();
+    int e_idx = 0;
+    for (int j = 1; j <= m->size_; ++j)
+        for (auto* e = m->first_in_col_[j]; e; e = e->NextInCol) elem_imag[e_idx++] = e->Imag;
+    return e_idx;
+}
+
 // ---- AMD-LU (src/core/amd.cpp, src/core/amd_lu_solver.cpp) ----------------
 
 // amd_ordering on a CSC pattern; perm receives n entries.
