@@ -18,7 +18,18 @@
 //                                   Returns true when singular.
 //   solve(rhs)                      NeoSolver::solve (spSolve), in place.
 //   solve_transposed(rhs)           spSolveTransposed, in place.
+//   numeric_complex(ax)             NeoSolver::numeric_complex: complex
+//                                   Markowitz ordering on the host (ax = 2*nnz
+//                                   doubles, (re, im) per CSC slot), factor on
+//                                   the GPU.
+//   refactorize_complex(ax)         factor_complex with those pivots on the GPU.
+//                                   Returns true when singular.
+//   solve_complex(rhs)              solve_complex (rhs = 2*n doubles), in place.
 //
+// The real and the complex factorizations are independent (the reference
+// keeps them in one matrix; an AC sweep never interleaves them).  A singular
+// first complex matrix, which NeoSolver::numeric_complex does not report,
+// leaves no factorization here: solve_complex then throws.
 // Misuse throws std::logic_error, a size mismatch std::invalid_argument, a
 // CUDA or allocation failure std::runtime_error -- as NeoSolver does.
 #pragma once
@@ -118,6 +129,53 @@ public:
     void solve(std::vector<double>& rhs) { sweep(rhs, false); }
     void solve_transposed(std::vector<double>& rhs) { sweep(rhs, true); }
 
+    void numeric_complex(const std::vector<double>& ax) {
+        require_symbolic("numeric_complex");
+        check_complex_values(ax);
+        release_complex();
+        complex_called_ = true;
+        nsg_topology* t = nullptr;
+        const int rc = nsg_topology_order_complex(n_, nnz(), col_ptr_.data(), row_idx_.data(),
+                                                  ax.data(), &t);
+        if (rc == NSG_SINGULAR) return;
+        check(rc, "numeric_complex");
+        ctopo_ = t;
+        check(nsg_batch_create(1, &ctopo_, &cbatch_), "batch");
+        long long lu_off[2] = {0, 0};
+        check(nsg_batch_layout(cbatch_, nullptr, nullptr, lu_off), "layout");
+        cuda(cudaMalloc(reinterpret_cast<void**>(&d_cax_), sizeof(double) * 2 * nnz()), "alloc");
+        cuda(cudaMalloc(reinterpret_cast<void**>(&d_clu_), sizeof(double) * 2 * lu_off[1]),
+             "alloc");
+        cuda(cudaMalloc(reinterpret_cast<void**>(&d_cx_), sizeof(double) * 2 * n_), "alloc");
+        cuda(cudaMalloc(reinterpret_cast<void**>(&d_cstatus_), sizeof(int)), "alloc");
+        complex_factored_ = (gpu_refactor_complex(ax) == NSG_OK);
+    }
+
+    bool refactorize_complex(const std::vector<double>& ax) {
+        require_symbolic("refactorize_complex");
+        if (!complex_called_)
+            throw std::logic_error("GpuSolver::refactorize_complex: numeric_complex() not called");
+        check_complex_values(ax);
+        if (!cbatch_) return true;  // the first complex matrix was singular
+        complex_factored_ = (gpu_refactor_complex(ax) == NSG_OK);
+        return !complex_factored_;
+    }
+
+    void solve_complex(std::vector<double>& rhs) {
+        require_symbolic("solve_complex");
+        if (!complex_called_)
+            throw std::logic_error("GpuSolver::solve_complex: numeric_complex() not called");
+        if (static_cast<int>(rhs.size()) != 2 * n_)
+            throw std::invalid_argument("GpuSolver::solve_complex: rhs size must be 2*n");
+        if (!complex_factored_)
+            throw std::runtime_error("GpuSolver::solve_complex: no valid factorization (singular)");
+        cuda(cudaMemcpy(d_cx_, rhs.data(), sizeof(double) * 2 * n_, cudaMemcpyHostToDevice),
+             "rhs");
+        check(nsg_batch_solve_complex(cbatch_, d_clu_, d_cx_, nullptr), "solve_complex");
+        cuda(cudaMemcpy(rhs.data(), d_cx_, sizeof(double) * 2 * n_, cudaMemcpyDeviceToHost),
+             "result");
+    }
+
 private:
     int engine_ = NSG_SOLVER_MARKOWITZ;
     int n_ = 0;
@@ -130,6 +188,15 @@ private:
     double* d_values_ = nullptr;
     double* d_x_ = nullptr;
     int* d_status_ = nullptr;
+    // complex (AC) factorization
+    bool complex_called_ = false;    // NeoSolver's factored_complex_ flag
+    bool complex_factored_ = false;  // the last complex factorization succeeded
+    nsg_topology* ctopo_ = nullptr;
+    nsg_batch* cbatch_ = nullptr;
+    double* d_cax_ = nullptr;
+    double* d_clu_ = nullptr;
+    double* d_cx_ = nullptr;
+    int* d_cstatus_ = nullptr;
 
     int nnz() const { return static_cast<int>(row_idx_.size()); }
 
@@ -149,6 +216,33 @@ private:
     void check_values(const std::vector<double>& v) const {
         if (static_cast<int>(v.size()) != nnz())
             throw std::invalid_argument("GpuSolver: values size mismatch");
+    }
+    void check_complex_values(const std::vector<double>& ax) const {
+        if (static_cast<int>(ax.size()) != 2 * nnz())
+            throw std::invalid_argument("GpuSolver: complex values size must be 2*nnz");
+    }
+    int gpu_refactor_complex(const std::vector<double>& ax) {
+        cuda(cudaMemcpy(d_cax_, ax.data(), sizeof(double) * 2 * nnz(), cudaMemcpyHostToDevice),
+             "upload");
+        check(nsg_batch_refactor_complex(cbatch_, d_cax_, d_clu_, d_cstatus_, nullptr),
+              "refactor_complex");
+        int st = 0;
+        cuda(cudaMemcpy(&st, d_cstatus_, sizeof(int), cudaMemcpyDeviceToHost), "status");
+        if (st == 104) throw std::runtime_error("GpuSolver: complex refactor wait timed out");
+        return st;
+    }
+    void release_complex() {
+        if (cbatch_) nsg_batch_free(cbatch_);
+        if (ctopo_) nsg_topology_free(ctopo_);
+        if (d_cax_) cudaFree(d_cax_);
+        if (d_clu_) cudaFree(d_clu_);
+        if (d_cx_) cudaFree(d_cx_);
+        if (d_cstatus_) cudaFree(d_cstatus_);
+        cbatch_ = nullptr;
+        ctopo_ = nullptr;
+        d_cax_ = d_clu_ = d_cx_ = nullptr;
+        d_cstatus_ = nullptr;
+        complex_factored_ = false;
     }
     void rebuild_batch() {
         if (batch_) nsg_batch_free(batch_);
@@ -186,6 +280,8 @@ private:
         cuda(cudaMemcpy(rhs.data(), d_x_, sizeof(double) * n_, cudaMemcpyDeviceToHost), "result");
     }
     void release() {
+        release_complex();
+        complex_called_ = false;
         if (batch_) nsg_batch_free(batch_);
         if (topo_) nsg_topology_free(topo_);
         if (d_values_) cudaFree(d_values_);

@@ -90,8 +90,34 @@ def seam() -> ctypes.CDLL:
         lib = _bind(ctypes.CDLL(str(SEAM_SO)))
         lib.nsseam_use_gpu.argtypes = [_I]
         lib.nsseam_gpu_solvers.restype = ctypes.c_longlong
+        lib.nsseam_ac_sweep.argtypes = [_I, _I, _V, _V, _V, _V, _V, _I, _V, _V, _V]
         _seam = lib
     return _seam
+
+
+def seam_ac_sweep(n, col_ptr, row_idx, g, c, rhs, omegas, gpu: bool):
+    """An AC sweep (solve_ac's per-frequency steps) through the ISolver that
+    make_solver returns: the reference's NeoSolver (gpu=False) or the GPU
+    adapter (gpu=True).  rhs is complex (n,); returns (complex (points, n)
+    solutions, per-point singular flags)."""
+    lib = seam()
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_idx, np.int32)
+    g = np.ascontiguousarray(g, np.float64)
+    c = np.ascontiguousarray(c, np.float64)
+    z = np.ascontiguousarray(_interleaved(np.asarray(rhs, np.complex128)))
+    om = np.ascontiguousarray(omegas, np.float64)
+    out = np.zeros((len(om), 2 * n))
+    sing = np.zeros(len(om), np.int32)
+    lib.nsseam_use_gpu(1 if gpu else 0)
+    try:
+        rc = lib.nsseam_ac_sweep(int(n), len(ri), _p(cp), _p(ri), _p(g), _p(c), _p(z), len(om),
+                                 _p(om), _p(out), _p(sing))
+    finally:
+        lib.nsseam_use_gpu(0)
+    if rc != 0:
+        raise RuntimeError("nsseam_ac_sweep: the solver threw")
+    return out[:, 0::2] + 1j * out[:, 1::2], sing
 
 
 def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:

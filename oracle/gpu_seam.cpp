@@ -16,6 +16,7 @@
 #include <cstring>
 #include <memory>
 #include <stdexcept>
+#include <utility>
 #include <vector>
 
 #include "core/matrix.hpp"
@@ -64,15 +65,15 @@ public:
         equilibrate_ = on;
         cpu_.set_equilibrate(on);
     }
-    // Complex (AC) paths stay on the CPU solver.
-    void numeric_complex(const SparsityPattern& p, const std::vector<double>& ax) override {
-        cpu_.symbolic(p);
-        cpu_.numeric_complex(p, ax);
+    // Complex (AC): Markowitz ordering on the host, factor and sweeps on the
+    // GPU (the reference's AC uses NeoSolver whatever the circuit).
+    void numeric_complex(const SparsityPattern&, const std::vector<double>& ax) override {
+        gpu_.numeric_complex(ax);
     }
     bool refactorize_complex(const std::vector<double>& ax) override {
-        return cpu_.refactorize_complex(ax);
+        return gpu_.refactorize_complex(ax);
     }
-    void solve_complex(std::vector<double>& rhs) override { cpu_.solve_complex(rhs); }
+    void solve_complex(std::vector<double>& rhs) override { gpu_.solve_complex(rhs); }
     const char* name() const override { return equilibrate_ ? cpu_.name() : gpu_.name(); }
 
 private:
@@ -104,5 +105,42 @@ void nsseam_use_gpu(int on) { neospice::g_gpu_seam = on != 0; }
 
 // GpuNeoSolver objects created so far (proof that the seam was used).
 long long nsseam_gpu_solvers(void) { return neospice::g_gpu_solvers; }
+
+// An AC sweep through whatever ISolver make_solver returns, with the
+// per-frequency steps of solve_ac (src/core/ac.cpp:196-216): ax = G + j*omega*C
+// in interleaved CSC order, numeric_complex at the first point and
+// refactorize_complex after, solve_complex of the excitation.  out receives
+// 2*n doubles per point; singular[f] the refactor's verdict (0 at f = 0).
+// Returns 0, or -1 when the solver threw.
+int nsseam_ac_sweep(int n, int nnz, const int* col_ptr, const int* row_idx, const double* g,
+                    const double* c, const double* rhs, int npoints, const double* omega,
+                    double* out, int* singular) {
+    try {
+        std::vector<std::pair<int32_t, int32_t>> entries;
+        entries.reserve(nnz);
+        for (int j = 0; j < n; ++j)
+            for (int k = col_ptr[j]; k < col_ptr[j + 1]; ++k) entries.emplace_back(row_idx[k], j);
+        neospice::SparsityPattern pattern(n, std::move(entries));
+        auto solver = neospice::make_solver(n, false);
+        solver->symbolic(pattern);
+        std::vector<double> ax(2 * static_cast<size_t>(nnz));
+        std::vector<double> z(2 * static_cast<size_t>(n));
+        for (int f = 0; f < npoints; ++f) {
+            for (int k = 0; k < nnz; ++k) {
+                ax[2 * k] = g[k];
+                ax[2 * k + 1] = omega[f] * c[k];
+            }
+            singular[f] = 0;
+            if (f == 0) solver->numeric_complex(pattern, ax);
+            else singular[f] = solver->refactorize_complex(ax) ? 1 : 0;
+            z.assign(rhs, rhs + 2 * static_cast<size_t>(n));
+            solver->solve_complex(z);
+            std::memcpy(out + 2 * static_cast<size_t>(n) * f, z.data(), sizeof(double) * z.size());
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
 
 }  // extern "C"

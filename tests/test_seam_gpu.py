@@ -70,3 +70,19 @@ def test_reference_solve_transient_on_gpu_solver():
         np.testing.assert_array_equal(v_gpu, v_cpu, err_msg=f"case {k}")
         assert i_gpu["iterations"] == i_cpu["iterations"]
         assert i_gpu["rejected"] == i_cpu["rejected"]
+
+
+@pytest.mark.parametrize("kind", ["ladder", "mesh"])
+def test_ac_sweep_through_the_seam(kind):
+    """solve_ac's frequency loop (numeric_complex, refactorize_complex,
+    solve_complex) on the ISolver adapter: GPU solutions equal NeoSolver's
+    bit for bit at every point."""
+    nl = W.rc_ladder(np.random.default_rng(15), 40) if kind == "ladder" else \
+        W.rc_mesh(np.random.default_rng(16), 10)
+    n, cp, ri, g, c, b = W.ac_system(nl)
+    omegas = 2 * np.pi * np.logspace(2, 10, 33)
+    z_cpu, s_cpu = oracle.seam_ac_sweep(n, cp, ri, g, c, b, omegas, gpu=False)
+    z_gpu, s_gpu = oracle.seam_ac_sweep(n, cp, ri, g, c, b, omegas, gpu=True)
+    np.testing.assert_array_equal(s_gpu, s_cpu)
+    np.testing.assert_array_equal(z_gpu.real, z_cpu.real)
+    np.testing.assert_array_equal(z_gpu.imag, z_cpu.imag)
