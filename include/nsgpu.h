@@ -349,6 +349,21 @@ int nsg_step_values(double start, double stop, double step, int cap, double* val
  * MODEINITJCT from a zero guess), in slot order -- what the reference's
  * first NeoSolver::numeric orders on. */
 int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values, double* rhs);
+/* Matrix values and rhs of one Newton iteration evaluated on the host, as
+ * Circuit::load does it for every device (src/core/newton.cpp:150-170):
+ * guess x (num_vars), CKTmode `mode` (ngspice MODE* bits), integrator
+ * fields ctx = {ag0, ag1, ag2, xmu_ratio, delta, delta_old1, time}, order
+ * and method (0 trapezoidal, 1 Gear); options gmin, reltol, abstol.
+ * states: the state ring state0..state2 (3 * nsg_circuit_state_count
+ * doubles, updated in place as the loads write state0); mos_rec: 12 values
+ * per MOSFET carried from load to load (zero before the first).  For
+ * checking device models against the reference on the CPU; circuits with
+ * diodes are refused. */
+int nsg_circuit_eval_matrix(const nsg_circuit* c, int mode, const double* x, const double* ctx,
+                            int order, int method, double gmin, double reltol, double abstol,
+                            double* states, double* mos_rec, double* values, double* rhs);
+/* Length of one state vector of the circuit (CKTnumStates). */
+int nsg_circuit_state_count(const nsg_circuit* c);
 
 /* ---- Batched DC operating point (device) ------------------------------------
  * Simulator::run_dc / solve_dc (src/core/dc.cpp:53-242, newton.cpp:51-419):

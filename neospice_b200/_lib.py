@@ -94,6 +94,10 @@ SIGNATURES = {
     "nsg_circuit_param_count": (c_int, [c_void_p, P(c_int)]),
     "nsg_step_values": (c_int, [c_double, c_double, c_double, c_int, P(c_double), P(c_int)]),
     "nsg_circuit_initial_matrix": (c_int, [c_void_p, c_double, P(c_double), P(c_double)]),
+    "nsg_circuit_eval_matrix": (c_int, [c_void_p, c_int, P(c_double), P(c_double), c_int, c_int,
+                                        c_double, c_double, c_double, P(c_double), P(c_double),
+                                        P(c_double), P(c_double)]),
+    "nsg_circuit_state_count": (c_int, [c_void_p]),
     "nsg_dc_batch_create": (c_int, [c_int, P(c_void_p), c_int, c_int, P(c_void_p)]),
     "nsg_dc_batch_free": (None, [c_void_p]),
     "nsg_dc_batch_layout": (c_int, [c_void_p, P(c_ll), P(c_ll)]),

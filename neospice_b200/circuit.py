@@ -209,6 +209,31 @@ class Circuit:
         L.check(L.lib().nsg_circuit_initial_matrix(self._h, float(gmin), L.dptr(a), L.dptr(r)))
         return a, r
 
+    def state_count(self) -> int:
+        n = L.lib().nsg_circuit_state_count(self._h)
+        if n < 0:
+            L.check(n)
+        return n
+
+    def eval_matrix(self, mode, x, ctx, order, method, states, mos_rec, gmin=1e-12,
+                    reltol=1e-3, abstol=1e-12):
+        """One Newton iteration's matrix and rhs evaluated on the host
+        (nsg_circuit_eval_matrix).  ctx = (ag0, ag1, ag2, xmu_ratio, delta,
+        delta_old1, time); states (3 * state_count()) and mos_rec (12 per
+        MOSFET) are float64 arrays updated in place."""
+        i = self.info()
+        a = np.zeros(i["nnz"])
+        r = np.zeros(i["num_vars"])
+        x = np.ascontiguousarray(x, np.float64)
+        c = np.ascontiguousarray(ctx, np.float64)
+        assert states.dtype == np.float64 and states.flags.c_contiguous
+        assert mos_rec.dtype == np.float64 and mos_rec.flags.c_contiguous
+        L.check(L.lib().nsg_circuit_eval_matrix(self._h, int(mode), L.dptr(x), L.dptr(c),
+                                                int(order), int(method), float(gmin),
+                                                float(reltol), float(abstol), L.dptr(states),
+                                                L.dptr(mos_rec), L.dptr(a), L.dptr(r)))
+        return a, r
+
     def __del__(self):
         if getattr(self, "_h", None) and L._lib is not None:
             L._lib.nsg_circuit_free(self._h)

@@ -2,6 +2,7 @@
 #include "capi_internal.hpp"
 
 #include "host/circuit.hpp"
+#include "kernels/mos1_model.cuh"
 #include "kernels/dc_device.cuh"
 
 #include <algorithm>
@@ -420,6 +421,27 @@ int nsg_circuit_initial_matrix(const nsg_circuit* c, double gmin, double* values
         if (rhs) std::memcpy(rhs, r.data(), sizeof(double) * r.size());
         return NSG_OK;
     });
+}
+
+int nsg_circuit_eval_matrix(const nsg_circuit* c, int mode, const double* x, const double* ctx,
+                            int order, int method, double gmin, double reltol, double abstol,
+                            double* states, double* mos_rec, double* values, double* rhs) {
+    return guarded("nsg_circuit_eval_matrix", [&]() -> int {
+        if (!c || !c->c.finalized()) return fail(NSG_ERR_INVALID, "not finalized");
+        if (!x || !ctx || !states || !mos_rec)
+            return fail(NSG_ERR_INVALID, "nsg_circuit_eval_matrix: null argument");
+        const nsg::Mos1Integ ic{ctx[0], ctx[1], ctx[2], ctx[3], ctx[4], ctx[5], order, method};
+        std::vector<double> a, r;
+        c->c.eval_values(mode, x, ic, ctx[6], gmin, reltol, abstol, states, mos_rec, a, r);
+        if (values) std::memcpy(values, a.data(), sizeof(double) * a.size());
+        if (rhs) std::memcpy(rhs, r.data(), sizeof(double) * r.size());
+        return NSG_OK;
+    });
+}
+
+int nsg_circuit_state_count(const nsg_circuit* c) {
+    if (!c || !c->c.finalized()) return fail(NSG_ERR_INVALID, "not finalized");
+    return c->c.num_states();
 }
 
 int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, int threads,

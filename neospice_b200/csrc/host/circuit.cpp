@@ -570,4 +570,76 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
     sum_program(tv, &a, &rhs);
 }
 
+void Circuit::eval_values(int mode, const double* x, const Mos1Integ& ic, double time,
+                          double gmin, double reltol, double abstol, double* states,
+                          double* mos_rec, std::vector<double>& a,
+                          std::vector<double>& rhs) const {
+    if (!finalized_) throw std::logic_error("Circuit: not finalized");
+    if (!diodes_.empty()) throw std::invalid_argument("Circuit::eval_values: diodes not supported");
+    std::vector<double> tv;
+    const_term_values(tv, gmin);
+    double* st[3] = {states, states + num_states_, states + 2 * static_cast<size_t>(num_states_)};
+    auto volt = [&](int32_t node) { return node >= 0 ? x[node] : 0.0; };
+    // Capacitors: the state-vector companion of Capacitor::evaluate
+    // (capacitor.cpp:28-100), as the kernels' device loads.
+    for (size_t k = 0; k < caps_.size(); ++k) {
+        const CapRec& cr = caps_[k];
+        const double cap = params_[cr.param];
+        double* t = &tv[cap_term_base() + kCapTerms * k];
+        const int32_t s = cr.state;
+        if (!(mode & (kM1Tran | 0x2 | kM1TranOp))) {
+            t[0] = t[1] = t[2] = t[3] = 0.0;
+            continue;
+        }
+        const bool cond1 = ((mode & 0x70) && (mode & kM1InitJct)) ||
+                           ((mode & 0x10000) && (mode & kM1InitTran));
+        const double vcap = cond1 ? (cr.has_ic ? params_[cr.param + 1] : 0.0)
+                                  : volt(cr.pos) - volt(cr.neg);
+        if (mode & (kM1Tran | 0x2)) {
+            double* s0 = st[0];
+            double* s1 = st[1];
+            if (mode & kM1InitPred) {
+                s0[s] = s1[s];
+            } else {
+                s0[s] = cap * vcap;
+                if (mode & kM1InitTran) s1[s] = s0[s];
+            }
+            const int order = ic.order < 1 ? 1 : (ic.order > 2 ? 2 : ic.order);
+            double deriv;
+            if (order == 1) deriv = ic.ag0 * s0[s] + ic.ag1 * s1[s];
+            else if (ic.method == 0) deriv = -s1[s + 1] * ic.xmu_ratio + ic.ag0 * s0[s] + ic.ag1 * s1[s];
+            else deriv = ic.ag0 * s0[s] + ic.ag1 * s1[s] + ic.ag2 * st[2][s];
+            s0[s + 1] = deriv;
+            const double geq = ic.ag0 * cap;
+            const double ceq = s0[s + 1] - ic.ag0 * s0[s];
+            if (mode & kM1InitTran) s1[s + 1] = s0[s + 1];
+            t[0] = 1.0 * geq;
+            t[1] = -1.0 * geq;
+            t[2] = -1.0 * ceq;
+            t[3] = 1.0 * ceq;
+        } else {
+            st[0][s] = cap * vcap;
+            t[0] = t[1] = t[2] = t[3] = 0.0;
+        }
+    }
+    for (size_t m = 0; m < mos_.size(); ++m) {
+        const MosRec& mr = mos_[m];
+        const double vn[4] = {volt(mr.d), volt(mr.g), volt(mr.s), volt(mr.b)};
+        double* t = &tv[mos_term_base() + kMosTerms * m];
+        double* rec = mos_rec + kMosRec * m;
+        if (mr.family == kFamilyBsim4)
+            bsim4_load(&params_[mr.param], rec, st[0] + mr.state, st[1] + mr.state,
+                       st[2] + mr.state, mode, ic, gmin, reltol, abstol, vn, t);
+        else
+            mos1_load(&params_[mr.param], rec, st[0] + mr.state, st[1] + mr.state,
+                      st[2] + mr.state, mode, ic, gmin, vn, t);
+    }
+    for (size_t s = 0; s < wsrc_.size(); ++s) {
+        const double v = wave_value(wsrc_[s].wave, &params_[wsrc_[s].param], wsrc_[s].nparam, time);
+        tv[src_term_base() + kSrcTerms * s + kSVal] = v;
+        tv[src_term_base() + kSrcTerms * s + kSNegVal] = -v;
+    }
+    sum_program(tv, &a, &rhs);
+}
+
 }  // namespace nsg

@@ -16,6 +16,8 @@
 
 namespace nsg {
 
+struct Mos1Integ;  // integrator fields of a device load (kernels/mos1_model.cuh)
+
 // ngspice load rank of each device family (src/core/circuit.cpp:34-59).
 enum class DevKind : int32_t {
     Mosfet = 3, Capacitor = 17, Diode = 22, ISource = 31, Resistor = 41, VSource = 50,
@@ -214,6 +216,17 @@ public:
     // (MODETRANOP | MODEINITJCT gives the same values for these devices.)
     void initjct_values(std::vector<double>& a, std::vector<double>& rhs,
                         double gmin) const;
+
+    // Host evaluation of the matrix and rhs of one Newton iteration at the
+    // guess x in CKTmode `mode`, with the integrator fields ic at time
+    // `time`: the same device loads as the GPU kernels' (R, V, I, waveform
+    // sources, capacitors, MOSFETs of both families), with host libm.
+    // states: the ring state0..state2 (3 * num_states, updated in place as
+    // the loads write state0); mos_rec: kMosRec values per MOSFET (the
+    // previous load's von, mode, ... ; updated).  Diodes are not supported.
+    void eval_values(int mode, const double* x, const Mos1Integ& ic, double time, double gmin,
+                     double reltol, double abstol, double* states, double* mos_rec,
+                     std::vector<double>& a, std::vector<double>& rhs) const;
 
 private:
     int32_t num_nodes_;

@@ -140,6 +140,7 @@ def _bind(lib: ctypes.CDLL) -> ctypes.CDLL:
         lib.nsref_sim_error.argtypes = [_V]
         lib.nsref_sim_free.argtypes = [_V]
         lib.nsref_sim_initjct.argtypes = [ctypes.c_char_p, _V, _V, _V, _V, _V]
+        lib.nsref_sim_eval_seq.argtypes = [ctypes.c_char_p, _I, _V, _V, _V, _V, _V, _V]
         lib.nsref_sim_method.argtypes = [_V]
         lib.nsref_sim_sens.argtypes = [ctypes.c_char_p, _I, _V, _V]
         lib.nsref_step_dc.argtypes = [ctypes.c_char_p, _I, _D, _D, _D, _I, _V, _V, _V]
@@ -439,6 +440,26 @@ def ref_sim_initjct(desc: str):
     if lib.nsref_sim_initjct(d, ctypes.addressof(nv), _p(cp), _p(ri), _p(vals), _p(rhs)) != nnz:
         raise RuntimeError("reference INITJCT evaluation failed")
     return cp, ri, vals, rhs
+
+
+def ref_sim_eval_seq(desc: str, state_ops, modes, xs, ctx):
+    """A sequence of the reference's device evaluations (nsref_sim_eval_seq):
+    xs (steps, n) guesses, ctx (steps, 8) integrator fields; returns the
+    matrices (steps, nnz) in slot order and the rhs (steps, n)."""
+    lib = ref()
+    xs = np.ascontiguousarray(xs, np.float64)
+    steps, n = xs.shape
+    ops = np.ascontiguousarray(state_ops, np.int32)
+    md = np.ascontiguousarray(modes, np.int32)
+    c = np.ascontiguousarray(ctx, np.float64)
+    nv = ctypes.c_int(0)
+    nnz = lib.nsref_sim_initjct(desc.encode(), ctypes.addressof(nv), None, None, None, None)
+    vals = np.zeros((steps, max(nnz, 0)))
+    rhs = np.zeros((steps, n))
+    if nnz < 0 or nv.value != n or lib.nsref_sim_eval_seq(
+            desc.encode(), steps, _p(ops), _p(md), _p(xs), _p(c), _p(vals), _p(rhs)) != nnz:
+        raise RuntimeError("reference evaluation sequence failed")
+    return vals, rhs
 
 
 def ref_step_dc(desc: str, device_line: int, start: float, stop: float, step: float,

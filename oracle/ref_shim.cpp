@@ -778,6 +778,76 @@ extern "C" int nsref_sim_initjct(const char* desc, int* num_vars, int* col_ptr, 
     }
 }
 
+// A sequence of device evaluations of a described circuit, as Newton
+// iterations would run them (Device::evaluate of every device in load
+// order, UCB rhs folded in), for comparing device loads on the CPU.  Step s
+// first applies state_op[s] (0 nothing, 1 rotate_state (circuit.cpp:328),
+// 2 copy state0 into state1..3 as the transient's seeding does,
+// transient.cpp:790-800), then evaluates at the guess xs + s*n in CKTmode
+// modes[s] with ctx + 8*s = {ag0, ag1, ag2, xmu_ratio, delta, delta_old1,
+// time, order + 10 * method}; values / rhs receive the matrix (slot order)
+// and rhs of each step.  Returns nnz, or -1.
+extern "C" int nsref_sim_eval_seq(const char* desc, int nsteps, const int* state_op,
+                                  const int* modes, const double* xs, const double* ctx,
+                                  double* values, double* rhs_out) {
+    try {
+        Circuit ckt;
+        build_from_desc(ckt, desc);
+        const int n = ckt.num_vars();
+        const auto& pattern = ckt.pattern();
+        const int ns = ckt.num_states();
+        ckt.integrator_ctx.options = &ckt.options;
+        for (int s = 0; s < nsteps; ++s) {
+            if (state_op[s] == 1) {
+                ckt.rotate_state();
+            } else if (state_op[s] == 2) {
+                std::copy_n(ckt.state0(), ns, ckt.state1());
+                std::copy_n(ckt.state0(), ns, ckt.state2());
+                std::copy_n(ckt.state0(), ns, ckt.state3());
+            }
+            const double* c = ctx + 8 * s;
+            IntegratorCtx& ic = ckt.integrator_ctx;
+            ic.mode = modes[s];
+            ic.ag[0] = c[0];
+            ic.ag[1] = c[1];
+            ic.ag[2] = c[2];
+            ic.xmu_ratio = c[3];
+            ic.delta = c[4];
+            ic.delta_old[0] = c[4];
+            ic.delta_old[1] = c[5];
+            ic.current_time = c[6];
+            for (auto& dev : ckt.devices()) {  // update_source_time (transient.cpp:383-393)
+                if (auto* vs = dynamic_cast<VSource*>(dev.get())) vs->set_time(c[6]);
+                else if (auto* is = dynamic_cast<ISource*>(dev.get())) is->set_time(c[6]);
+            }
+            ic.order = static_cast<int>(c[7]) % 10;
+            ic.integrate_method = static_cast<int>(c[7]) / 10;
+            NumericMatrix mat(pattern);
+            std::vector<double> solution(xs + static_cast<size_t>(s) * n,
+                                         xs + static_cast<size_t>(s + 1) * n);
+            std::vector<double> rhs(n, 0.0);
+            std::vector<double> ob_sol(n + 1, 0.0), ob_rhs(n + 1, 0.0);
+            for (int i = 0; i < n; ++i) ob_sol[i + 1] = solution[i];
+            OneBasedEvalArrays arrays{ob_sol.data(), ob_rhs.data(), n + 1};
+            tls_integrator_ctx = &ckt.integrator_ctx;
+            tls_one_based_eval_arrays = &arrays;
+            for (Device* dev : ckt.device_load_order()) dev->evaluate(solution, mat, rhs);
+            tls_one_based_eval_arrays = nullptr;
+            tls_integrator_ctx = nullptr;
+            for (int i = 0; i < n; ++i) rhs[i] += ob_rhs[i + 1];
+            for (int k = 0; k < pattern.nnz(); ++k)
+                values[static_cast<size_t>(s) * pattern.nnz() + k] = mat.data()[k];
+            for (int i = 0; i < n; ++i) rhs_out[static_cast<size_t>(s) * n + i] = rhs[i];
+        }
+        return pattern.nnz();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "nsref_sim_eval_seq: %s\n", e.what());
+        tls_one_based_eval_arrays = nullptr;
+        tls_integrator_ctx = nullptr;
+        return -1;
+    }
+}
+
 // The DC convergence method of a finished run (ConvergenceMethod as an int:
 // 0 = the direct Newton attempt, 1 = gmin stepping).
 extern "C" int nsref_sim_method(void* h) { return static_cast<SimResult*>(h)->method; }

@@ -60,3 +60,73 @@ def test_unsupported_card_parameter_is_refused():
     m = c.model_bsim4("nmos", TOXE=2.5e-9, VTH0=0.45, U0=0.03)
     with pytest.raises(L.NsgError):
         c.M4(0, 1, -1, -1, m, W=1e-6, L_=-1e-7)
+
+
+def _eval_sequence(nl, rng, dt=1e-12):
+    """Ten device evaluations as a DC solve, the transient seeding, backward
+    Euler, trapezoidal and Gear-2 steps would run them (INITJCT, INITFLOAT,
+    INITTRAN, INITPRED), at random guesses with every terminal bias sign;
+    returns (ours, reference) lists of (matrix, rhs)."""
+    c = nl.build()
+    n = c.info()["num_vars"]
+    nn = nl.num_nodes
+
+    def guess():
+        x = np.zeros(n)
+        x[:nn] = rng.uniform(-0.2, 1.3, nn)
+        x[nn:] = rng.normal(0.0, 1e-4, n - nn)
+        return x
+
+    h0, h1 = dt, 1.5 * dt
+    be = [1 / dt, -1 / dt, 0, 0, dt, dt, dt, 1]
+    trap = [2 / dt, -2 / dt, 0, 1.0, dt, dt, 2 * dt, 2]
+    gear = [(2 * h0 + h1) / (h0 * (h0 + h1)), -(h0 + h1) / (h0 * h1), h0 / (h1 * (h0 + h1)),
+            0, h0, h1, 3 * dt, 12]
+    dc = [0, 0, 0, 0, 0, 0, 0, 1]
+    x2 = guess()
+    steps = [(0, 0x210, np.zeros(n), dc), (0, 0x110, guess(), dc), (0, 0x110, x2, dc),
+             (2, 0x1001, x2, be), (0, 0x101, guess(), be), (0, 0x101, guess(), be),
+             (1, 0x2001, guess(), trap), (0, 0x101, guess(), trap),
+             (1, 0x2001, guess(), gear), (0, 0x101, guess(), gear)]
+    ops, modes, xs, ctx = (np.array([s[k] for s in steps]) for k in range(4))
+    rv, rr = oracle.ref_sim_eval_seq(netlists.ref_desc(nl), ops, modes, xs.astype(float),
+                                     ctx.astype(float))
+    ns = c.state_count()
+    st = np.zeros(3 * ns)
+    rec = np.zeros(12 * sum(1 for d in nl.devices if d[0] == "M"))
+    ours = []
+    for s, (op, mode, x, cx) in enumerate(steps):
+        if op == 1:  # rotate_state: state2 <- state1 <- copy of state0
+            st[2 * ns:] = st[ns:2 * ns]
+            st[ns:2 * ns] = st[:ns]
+        elif op == 2:  # the transient's seeding from the operating point
+            st[ns:2 * ns] = st[:ns]
+            st[2 * ns:] = st[:ns]
+        ours.append(c.eval_matrix(mode, x, cx[:7], int(cx[7]) % 10, int(cx[7]) // 10, st, rec))
+    return ours, list(zip(rv, rr))
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["chain", "ring0", "ring1"])
+def test_transient_mode_loads_bitwise(case):
+    """The host load in every transient mode -- charges, NIintegrate, the
+    predictor, junction and overlap capacitances, reverse mode, body bias --
+    equals the reference's matrix and rhs bit for bit, step after step with
+    the state ring carried along."""
+    nl = TRAN[0]["netlist"] if case == "chain" else \
+        W.bsim4_ring_nand(np.random.default_rng([31, int(case[-1])]))
+    ours, ref = _eval_sequence(nl, np.random.default_rng([44, len(case), int(case[-1] == "1")]))
+    for s, ((a, r), (ra, rr)) in enumerate(zip(ours, ref)):
+        np.testing.assert_array_equal(a, ra, err_msg=f"step {s} matrix")
+        np.testing.assert_array_equal(r, rr, err_msg=f"step {s} rhs")
+
+
+def test_eval_matrix_refuses_diodes():
+    c = Circuit(2)
+    c.V(0, -1, 1.0)
+    c.D(0, 1)
+    c.R(1, -1, 1e3)
+    c.finalize()
+    with pytest.raises(L.NsgError):
+        c.eval_matrix(0x210, np.zeros(3), np.zeros(7), 1, 0, np.zeros(3 * c.state_count()),
+                      np.zeros(1))
