@@ -77,7 +77,7 @@ def _args():
                     help="skip the single large power-grid refactor/solve section")
     ap.add_argument("--grid-side", type=int, default=300,
                     help="side of the power-grid mesh of that section")
-    ap.add_argument("--inverter-batch", type=int, default=296,
+    ap.add_argument("--inverter-batch", type=int, default=1184,
                     help="instances of the batched inverter-chain transient")
     ap.add_argument("--bsim4-batch", type=int, default=2048,
                     help="Monte Carlo instances of the BSIM4v7 ring + NAND transient (0 = skip)")

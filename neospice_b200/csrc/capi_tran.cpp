@@ -19,7 +19,7 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params_tran, double* work, const double* bps,
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
-                             const TranOptions& o, int max_col, int max_n, long long max_stage,
+                             const TranOptions& o, const TranShape& shape,
                              StepRecord* rec_steps, double* rec_x0, cudaStream_t stream);
 size_t tran_smem_bytes(int max_col, int max_n);
 struct AdjDesc {
@@ -96,6 +96,22 @@ struct nsg_tran_batch {
             cudaFree(p);
     }
 };
+
+namespace {
+
+// Launch shape of a transient batch (nsg::TranShape).
+nsg::TranShape tran_shape(const nsg_tran_batch& b) {
+    nsg::TranShape sh{b.max_col, b.max_n, max_stage_len(b.descs), 0, 0, 0};
+    for (const auto& t : b.topos) {
+        sh.max_small_lu = std::max(sh.max_small_lu, t->plan.nnz_lu + t->plan.n);
+        sh.max_plan_words = std::max<int64_t>(sh.max_plan_words, t->plan.device_words());
+    }
+    for (const auto& d : b.descs)
+        sh.max_devices = std::max({sh.max_devices, d.n_mos, d.n_diodes, d.n_caps, d.n_srcs});
+    return sh;
+}
+
+}  // namespace
 
 namespace {
 
@@ -294,7 +310,7 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                                          n, b->d_prog, b->d_params_dc, b->d_params_tran, b->d_work,
                                          b->d_bps, b->d_probes, b->d_times, b->d_values,
                                          b->d_npoints, b->d_status, b->d_stats, b->d_ctl, b->opt,
-                                         b->max_col, b->max_n, max_stage_len(b->descs),
+                                         tran_shape(*b),
                                          b->record ? b->d_rec : nullptr,
                                          b->record ? b->d_x0 : nullptr, st);
         };

@@ -490,11 +490,18 @@ __device__ inline void cta_solve(const PlanDesc& pd, const int32_t* __restrict__
 }
 
 // Small instances: the whole LU lives in shared memory and warp 0 alone
-// refactors and sweeps it, column after column / level after level with
-// __syncwarp only -- no completion flags and no global-memory round trips on
-// the dependency chain, which dominate for circuits of a few dozen unknowns.
-// Same operations in the same order as cta_refactor_flow / cta_solve_flow,
-// so the values are bit-identical.  lu_s: pd.nnz_lu doubles; w_s: pd.n.
+// refactors and sweeps it -- no completion flags and no global-memory round
+// trips on the dependency chain, which dominate for circuits of a few dozen
+// unknowns.  The chain itself is the cost there (a 32-stage inverter chain
+// factors as a 32-deep sequence of single columns), so the work is laid out
+// to keep it short: every column's A values are scattered by the whole CTA
+// before the elimination starts, U entries whose L(:, r) is short are applied
+// by lane 0 alone with no warp barrier, and the sweeps run row after row on
+// lane 0 in pivot order (a topological order of the triangular solves), so
+// no level bookkeeping or barrier sits between dependent rows.  Same
+// operations in the same order per entry as cta_refactor_flow /
+// cta_solve_flow, so the values are bit-identical.  lu_s: pd.nnz_lu doubles;
+// w_s: pd.n.
 // Dynamic shared memory of a Newton kernel launch: the LU scratch (flow or
 // small path) followed by an optional stage for instance workspaces, capped
 // so that two CTAs still fit on an SM.
@@ -509,6 +516,10 @@ __host__ __device__ inline size_t stage_bytes_for(size_t scratch_bytes, long lon
 __host__ __device__ inline bool small_fits(int n, int nnz_lu, int smem_doubles) {
     return n <= 128 && nnz_lu + n <= smem_doubles;
 }
+
+// U entries whose L(:, r) has at most this many rows are applied by lane 0
+// alone; longer ones by the whole warp.
+constexpr int kSmallSerialRows = 4;
 
 // Refactor into lu_s (and lu, written back at the end).  Begins and ends with
 // __syncthreads().
@@ -528,61 +539,97 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
     const int lane = threadIdx.x & 31;
     __shared__ int32_t s_fail_step, s_fail_code;
     __syncthreads();
-    if (threadIdx.x < 32) {
+    // A values of every column at once (the scatter does not depend on the
+    // elimination), then diag_gmin on each column's gmin row.
+    for (int32_t t = threadIdx.x; t < pd.nnz_lu; t += blockDim.x) {
+        const int32_t src = lu_src[t];
+        lu_s[t] = (src >= 0) ? a[src] : 0.0;
+    }
+    if (diag_gmin != 0.0) {
+        __syncthreads();
+        for (int32_t j = threadIdx.x; j < n; j += blockDim.x) {
+            const int32_t gp = amd ? gmin_pos[j] : diag_pos[j] - col_ptr[j];
+            if (gp >= 0) lu_s[col_ptr[j] + gp] = __dadd_rn(lu_s[col_ptr[j] + gp], diag_gmin);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_fail_step = INT32_MAX;
+    if (threadIdx.x < 32 && n > 0) {
         int32_t fail_step = INT32_MAX, fail_code = kStatusOk;
         bool any_growth = false;
+        const bool lane0_pivots = !amd && check_pivots != kCheckNumeric;
+        int32_t nc0 = col_ptr[0], nc1 = col_ptr[1], ndp = diag_pos[0];
         for (int32_t j = 0; j < n; ++j) {
-            const int32_t c0 = col_ptr[j];
-            const int32_t len = col_ptr[j + 1] - c0;
-            const int32_t dj = diag_pos[j] - c0;
-            const int32_t gp = amd ? gmin_pos[j] : dj;
-            for (int32_t t = lane; t < len; t += 32) {
-                const int32_t src = lu_src[c0 + t];
-                double v = (src >= 0) ? a[src] : 0.0;
-                if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
-                lu_s[c0 + t] = v;
+            const int32_t c0 = nc0, len = nc1 - nc0, dj = ndp - nc0;
+            if (j + 1 < n) {  // the next column's bounds, off the dependency chain
+                nc0 = nc1;
+                nc1 = col_ptr[j + 2];
+                ndp = diag_pos[j + 1];
             }
-            __syncwarp();
-            double colmax = 0.0;
+            double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied (lane 0)
             for (int32_t q = 0; q < dj; ++q) {
                 const int4 m = umeta[c0 + q];  // r, diag_pos[r], |L(:, r)|, upd_start
-                const double u = amd ? lu_s[c0 + q] : lu_mul(lu_s[c0 + q], lu_s[m.y]);
-                colmax = fmax(colmax, fabs(u));
-                for (int32_t t = lane; t < m.z; t += 32) {
-                    const int32_t d = upd_dst[m.w + t];
-                    lu_s[c0 + d] = lu_sub(lu_s[c0 + d], lu_mul(u, lu_s[m.y + 1 + t]));
+                if (m.z <= kSmallSerialRows) {
+                    if (lane == 0) {
+                        const double u = amd ? lu_s[c0 + q] : lu_mul(lu_s[c0 + q], lu_s[m.y]);
+                        colmax = fmax(colmax, fabs(u));
+                        lu_s[c0 + q] = u;
+                        for (int32_t t = 0; t < m.z; ++t) {
+                            const int32_t d = c0 + upd_dst[m.w + t];
+                            lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
+                        }
+                    }
+                } else {
+                    __syncwarp();  // lane 0's serial updates visible to the warp
+                    double u = 0.0;
+                    if (lane == 0) {
+                        u = amd ? lu_s[c0 + q] : lu_mul(lu_s[c0 + q], lu_s[m.y]);
+                        colmax = fmax(colmax, fabs(u));
+                        lu_s[c0 + q] = u;
+                    }
+                    u = __shfl_sync(0xffffffffu, u, 0);
+                    for (int32_t t = lane; t < m.z; t += 32) {
+                        const int32_t d = c0 + upd_dst[m.w + t];
+                        lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
+                    }
+                    __syncwarp();
+                }
+            }
+            int32_t code = kStatusOk;
+            if (lane0_pivots) {
+                // refactorize(): a zero pivot fails; the reciprocal is stored.
+                if (lane == 0) {
+                    const double piv = lu_s[c0 + dj];
+                    code = (piv == 0.0) ? kStatusSingular : kStatusOk;
+                    lu_s[c0 + dj] = __drcp_rn(piv);
+                }
+            } else {
+                __syncwarp();
+                const double piv = lu_s[c0 + dj];
+                if (amd) {
+                    colmax = __shfl_sync(0xffffffffu, colmax, 0);
+                    const AmdColumn v = amd_column_status(lu_s + c0, dj, len, colmax,
+                                                          check_pivots, piv_rank[j], gmin_pos[j],
+                                                          lane);
+                    code = v.code;
+                    any_growth = any_growth || v.growth_fail;
+                    for (int32_t t = dj + 1 + lane; t < len; t += 32)
+                        lu_s[c0 + t] = __ddiv_rn(lu_s[c0 + t], piv);
+                } else {
+                    double largest = 0.0;
+                    for (int32_t t = dj + 1 + lane; t < len; t += 32)
+                        largest = fmax(largest, fabs(lu_s[c0 + t]));
+                    largest = warp_max(largest);
+                    code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
+                    __syncwarp();
+                    if (lane == 0) lu_s[c0 + dj] = __drcp_rn(piv);
                 }
                 __syncwarp();
-                if (lane == 0) lu_s[c0 + q] = u;
-                __syncwarp();
             }
-            const double piv = lu_s[c0 + dj];
-            int32_t code;
-            if (amd) {
-                const AmdColumn v = amd_column_status(lu_s + c0, dj, len, colmax, check_pivots,
-                                                      piv_rank[j], gmin_pos[j], lane);
-                code = v.code;
-                any_growth = any_growth || v.growth_fail;
-            } else if (check_pivots == kCheckNumeric) {
-                double largest = 0.0;
-                for (int32_t t = dj + 1 + lane; t < len; t += 32) largest = fmax(largest, fabs(lu_s[c0 + t]));
-                largest = warp_max(largest);
-                code = !(largest * rel_threshold < fabs(piv)) ? kStatusReorder : kStatusOk;
-            } else {
-                code = (piv == 0.0) ? kStatusSingular : kStatusOk;
-            }
-            if (code != kStatusOk && j < fail_step) {
+            if (lane == 0 && code != kStatusOk && j < fail_step) {
                 fail_step = j;
                 fail_code = code;
             }
-            __syncwarp();
-            if (amd) {
-                for (int32_t t = dj + 1 + lane; t < len; t += 32)
-                    lu_s[c0 + t] = __ddiv_rn(lu_s[c0 + t], piv);
-            } else if (lane == 0) {
-                lu_s[c0 + dj] = 1.0 / piv;
-            }
-            __syncwarp();
         }
         if (amd && !amd_verdict_counts(check_pivots, any_growth)) fail_step = INT32_MAX;
         if (lane == 0) {
@@ -599,8 +646,9 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
     return res;
 }
 
-// x <- A^{-1} x from the LU in lu_s (warp 0, level by level).  Begins and ends
-// with __syncthreads().
+// x <- A^{-1} x from the LU in lu_s: lane 0, row after row in pivot order
+// (forward: ascending, backward: descending), each row's entries in the
+// order of the level-scheduled sweeps.  Begins and ends with __syncthreads().
 static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
                                                     const int32_t* __restrict__ pool,
                                                     const double* lu_s, double* __restrict__ x,
@@ -610,34 +658,28 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const bool amd = pd.kind == kPlanAmdLu;
-    const int lane = threadIdx.x & 31;
     __syncthreads();
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
     __syncthreads();
-    if (threadIdx.x < 32) {
-        {   // forward: L (Markowitz: then the reciprocal pivot)
+    if (threadIdx.x == 0) {
+        {   // forward: L (Markowitz: skip zero operands, then the reciprocal pivot)
             const int32_t* lp = pool + pd.off[PA_lrow_ptr];
             const int32_t* lpos = pool + pd.off[PA_lrow_pos];
             const int32_t* lcol = pool + pd.off[PA_lrow_col];
-            const int32_t* lev_ptr = pool + pd.off[PA_fwd_lev_ptr];
-            const int32_t* lev = pool + pd.off[PA_fwd_lev];
-            for (int32_t l = 0; l < pd.n_fwd_lev; ++l) {
-                for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
-                    const int32_t i = lev[k];
-                    double t = w[i];
-                    if (amd) {
-                        for (int32_t e = lp[i]; e < lp[i + 1]; ++e)
-                            t = lu_sub(t, lu_mul(lu_s[lpos[e]], w[lcol[e]]));
-                        w[i] = t;
-                        continue;
-                    }
-                    for (int32_t e = lp[i]; e < lp[i + 1]; ++e) {
-                        const double xc = w[lcol[e]];
-                        if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu_s[lpos[e]]));
-                    }
-                    w[i] = (t != 0.0) ? lu_mul(t, lu_s[diag_pos[i]]) : t;
+            int32_t e = lp[0];
+            for (int32_t i = 0; i < n; ++i) {
+                const int32_t e1 = lp[i + 1];
+                double t = w[i];
+                if (amd) {
+                    for (; e < e1; ++e) t = lu_sub(t, lu_mul(lu_s[lpos[e]], w[lcol[e]]));
+                    w[i] = t;
+                    continue;
                 }
-                __syncwarp();
+                for (; e < e1; ++e) {
+                    const double xc = w[lcol[e]];
+                    if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu_s[lpos[e]]));
+                }
+                w[i] = (t != 0.0) ? lu_mul(t, lu_s[diag_pos[i]]) : t;
             }
         }
         {   // backward: U row dot products (AMD-LU: columns descending, then
@@ -645,23 +687,17 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
             const int32_t* up = pool + pd.off[PA_urow_ptr];
             const int32_t* upos = pool + pd.off[PA_urow_pos];
             const int32_t* ucol = pool + pd.off[PA_urow_col];
-            const int32_t* lev_ptr = pool + pd.off[PA_bwd_lev_ptr];
-            const int32_t* lev = pool + pd.off[PA_bwd_lev];
-            for (int32_t l = 0; l < pd.n_bwd_lev; ++l) {
-                for (int32_t k = lev_ptr[l] + lane; k < lev_ptr[l + 1]; k += 32) {
-                    const int32_t i = lev[k];
-                    double t = w[i];
-                    if (amd) {
-                        for (int32_t e = up[i + 1] - 1; e >= up[i]; --e)
-                            t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
-                        w[i] = __ddiv_rn(t, lu_s[diag_pos[i]]);
-                        continue;
-                    }
-                    for (int32_t e = up[i]; e < up[i + 1]; ++e)
+            for (int32_t i = n - 1; i >= 0; --i) {
+                const int32_t e0 = up[i], e1 = up[i + 1];
+                double t = w[i];
+                if (amd) {
+                    for (int32_t e = e1 - 1; e >= e0; --e)
                         t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
-                    w[i] = t;
+                    w[i] = __ddiv_rn(t, lu_s[diag_pos[i]]);
+                    continue;
                 }
-                __syncwarp();
+                for (int32_t e = e0; e < e1; ++e) t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
+                w[i] = t;
             }
         }
     }

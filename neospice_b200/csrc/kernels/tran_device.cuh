@@ -58,6 +58,18 @@ struct TranCtl {
     int32_t stperm[4];      // buffer of state0..state3 in the ring
 };
 
+// What the launch needs to size one CTA: the batch's largest LU column and
+// unknown count (dataflow scratch), largest staged workspace, largest
+// small-path LU (nnz_lu + n doubles), largest plan (int32 words) and most
+// devices of one family in one instance (the device loads' parallelism).
+struct TranShape {
+    int32_t max_col, max_n;
+    int64_t max_stage;
+    int32_t max_small_lu;
+    int64_t max_plan_words;
+    int32_t max_devices;
+};
+
 // Per-instance transient status.
 enum : int32_t {
     kTranOk = 0,

@@ -185,8 +185,10 @@ __device__ inline void finish(const DcDesc& d, double* work, double* stage, Tran
 
 }  // namespace
 
-// One CTA per instance.  subset (optional): descriptor positions to run.
-__global__ void __launch_bounds__(kFlowThreads, 2)
+// One CTA of kThreads threads per instance (1024 / kThreads CTAs per SM at
+// 64 registers).  subset (optional): descriptor positions to run.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1024 / kThreads)
 transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ lu_pool,
                  const DcDesc* __restrict__ descs, const TranDesc* __restrict__ tdescs,
                  const int32_t* __restrict__ subset, const int32_t* __restrict__ prog,
@@ -195,7 +197,7 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  const int32_t* __restrict__ probes, double* __restrict__ times,
                  double* __restrict__ values, int32_t* __restrict__ npoints,
                  int32_t* __restrict__ status, int32_t* __restrict__ stats,
-                 TranCtl* __restrict__ ctls, TranOptions o, int colbuf, int scratch_doubles,
+                 TranCtl* __restrict__ ctls, TranOptions o_in, int colbuf, int scratch_doubles,
                  int stage_doubles, StepRecord* __restrict__ rec_steps,
                  double* __restrict__ rec_x0, int plan_words) {
     extern __shared__ double smem[];
@@ -208,13 +210,23 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     __shared__ int32_t s_flag;
     double* stage = (d.stage_len <= stage_doubles) ? smem + scratch_doubles : nullptr;
     stage_copy(d, work, stage, true);
-    Inst v = make_inst(d, prog, params_dc, work, stage);
+    // The instance's views, once per CTA in shared memory (a per-thread copy
+    // would sit in every thread's stack frame, far beyond L1).
+    __shared__ Inst s_v;
+    if (threadIdx.x == 0) s_v = make_inst(d, prog, params_dc, work, stage);
+    Inst& v = s_v;
     double* hist = ws_at(d, work, stage, td.hist_off);  // three history vectors (ring)
     const double* bp = bps + td.bp_off;
     constexpr int kFirst = kModeTranOp | kModeInitJct, kCont = kModeTranOp | kModeInitFloat;
 
-    if (threadIdx.x == 0) k = *g;
+    // Options by reference from shared memory, not from a per-thread copy.
+    __shared__ TranOptions s_o;
+    if (threadIdx.x == 0) {
+        k = *g;
+        s_o = o_in;
+    }
     __syncthreads();
+    const TranOptions& o = s_o;
     if (k.phase == kTrInit) {
         for (int32_t i = threadIdx.x; i < kMosRecCount * v.n_mos; i += blockDim.x) v.mrec[i] = 0.0;
         for (int32_t i = threadIdx.x; i < 4 * d.n_states; i += blockDim.x) v.st[0][i] = 0.0;
@@ -232,10 +244,11 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         }
         __syncthreads();
     }
-    {
+    if (threadIdx.x == 0) {
         double* base = ws_at(d, work, stage, d.state_off);
         for (int q = 0; q < 4; ++q) v.st[q] = base + static_cast<int64_t>(k.stperm[q]) * d.n_states;
     }
+    __syncthreads();
 
     // Small instances read their plan from shared memory (the DC plan now,
     // the transient plan for the timestep loop).
@@ -289,7 +302,9 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
         }
         __syncthreads();
     }
-    v.par = params_tran + d.param_off;  // PULSE defaults resolved for the transient
+    __syncthreads();
+    if (threadIdx.x == 0) v.par = params_tran + d.param_off;  // PULSE defaults resolved
+    __syncthreads();
     load_constants(v, o.nopt.gmin);
 
     // ---- 3. the adaptive timestep loop (transient.cpp:873-1052)
@@ -426,12 +441,13 @@ transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
             k.ctx.order = k.order;
         }
         // rotate_state (circuit.cpp:328): state3 <- state2 <- state1, state1 = state0
-        {
+        if (threadIdx.x == 0) {
             double* t3 = v.st[3];
             v.st[3] = v.st[2];
             v.st[2] = v.st[1];
             v.st[1] = t3;
         }
+        __syncthreads();
         for (int32_t i = threadIdx.x; i < d.n_states; i += blockDim.x) v.st[1][i] = v.st[0][i];
         store_point(td, o, probes, times, values, k.points, k.time, v.x);
         for (int32_t i = threadIdx.x; i < v.n; i += blockDim.x) sol_prev3[i] = v.x[i];
@@ -497,34 +513,90 @@ size_t tran_smem_bytes(int max_col, int max_n) {
     return a > b ? a : b;
 }
 
+namespace {
+
+template <int kThreads>
+cudaError_t configure_transient() {
+    static bool configured = false;
+    if (configured) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(transient_kernel<kThreads>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) configured = true;
+    return e;
+}
+
+int sm_count() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return sms;
+}
+
+}  // namespace
+
+// Launch shapes.  Latency of one instance is the cost for a few hundred
+// instances: one 512-thread CTA per instance, two per SM, each staging its
+// plan and workspace in shared memory.  When every instance takes the
+// shared-memory LU path (n <= 128) and the batch is larger than those two
+// CTAs per SM can hold at once, throughput is the cost: CTAs of 128 or 256
+// threads (as many as the instances' largest device family needs for one
+// pass of the device loads), eight or four per SM, with the LU and the plan
+// in shared memory and the workspace staged only where it fits.
 cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
                              const TranDesc* tdescs, const int32_t* subset, int count,
                              const int32_t* prog, const double* params_dc,
                              const double* params_tran, double* work, const double* bps,
                              const int32_t* probes, double* times, double* values,
                              int32_t* npoints, int32_t* status, int32_t* stats, TranCtl* ctls,
-                             const TranOptions& o, int max_col, int max_n, long long max_stage,
+                             const TranOptions& o, const TranShape& sh,
                              StepRecord* rec_steps, double* rec_x0, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
-    const int colbuf = (max_col + 31) & ~31;
-    const size_t scratch = (tran_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
-    const size_t plan = (max_n <= 128) ? kPlanStageBytes : 0;
-    const size_t stage = stage_bytes_for(scratch + plan, max_stage);
+    const int colbuf = (sh.max_col + 31) & ~31;
+    int threads = kFlowThreads;
+    if (sh.max_n <= 128 && count > 2 * sm_count())
+        threads = sh.max_devices <= 128 ? 128 : (sh.max_devices <= 256 ? 256 : kFlowThreads);
+    size_t scratch, plan, stage;
+    if (threads == kFlowThreads) {
+        scratch = (tran_smem_bytes(sh.max_col, sh.max_n) + 15) & ~size_t{15};
+        plan = (sh.max_n <= 128) ? kPlanStageBytes : 0;
+        stage = stage_bytes_for(scratch + plan, sh.max_stage);
+    } else {
+        // Per-CTA share of the SM's 228 KB, less the CTA's static shared
+        // memory and the 1 KB the runtime reserves per CTA.
+        const size_t blocks = 1024 / threads;
+        const size_t budget = (228 * 1024) / blocks - 3 * 1024;
+        scratch = (sizeof(double) * static_cast<size_t>(sh.max_small_lu) + 15) & ~size_t{15};
+        plan = (sh.max_plan_words * 4 <= static_cast<int64_t>(kPlanStageBytes))
+                   ? ((static_cast<size_t>(sh.max_plan_words) * 4 + 15) & ~size_t{15})
+                   : 0;
+        if (scratch + plan > budget) plan = 0;
+        const size_t want = static_cast<size_t>(sh.max_stage) * sizeof(double);
+        stage = (scratch + plan + want <= budget) ? want : 0;
+    }
     const size_t smem = scratch + stage + plan;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(transient_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             200 * 1024);
-        if (e != cudaSuccess) return e;
-        configured = true;
+    const int scratch_d = static_cast<int>(scratch / sizeof(double));
+    const int stage_d = static_cast<int>(stage / sizeof(double));
+    const int plan_w = static_cast<int>(plan / sizeof(int32_t));
+    cudaError_t e;
+#define NSG_LAUNCH_TRAN(T)                                                                     \
+    if ((e = configure_transient<T>()) != cudaSuccess) return e;                               \
+    transient_kernel<T><<<count, T, smem, stream>>>(                                           \
+        plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes, \
+        times, values, npoints, status, stats, ctls, o, colbuf, scratch_d, stage_d, rec_steps,  \
+        rec_x0, plan_w);
+    if (threads == 128) {
+        NSG_LAUNCH_TRAN(128)
+    } else if (threads == 256) {
+        NSG_LAUNCH_TRAN(256)
+    } else {
+        NSG_LAUNCH_TRAN(kFlowThreads)
     }
-    transient_kernel<<<count, kFlowThreads, smem, stream>>>(
-        plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes,
-        times, values, npoints, status, stats, ctls, o, colbuf,
-        static_cast<int>(scratch / sizeof(double)), static_cast<int>(stage / sizeof(double)),
-        rec_steps, rec_x0, static_cast<int>(plan / sizeof(int32_t)));
+#undef NSG_LAUNCH_TRAN
     return cudaGetLastError();
 }
 
