@@ -170,6 +170,11 @@ int nsg_batch_refactor(nsg_batch* batch, const double* d_values, double diag_gmi
  * refactored and swept by every SM, for a few large topologies).  All
  * produce bit-identical values. */
 int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
+/* Shared column buffer per warp of the grid-wide refactor (schedule 2):
+ * 1024, 2048 or 4096 doubles, or 0 (default) for the smallest that holds the
+ * longest column.  Longer columns are eliminated in place in global memory.
+ * No counterpart in the reference (a tuning knob of this schedule). */
+int nsg_batch_set_grid_buffer(nsg_batch* batch, int doubles);
 
 /* Schedule autotuner: refactor d_values (as a refactorize()) and solve d_x
  * under each schedule (0 dataflow, 1 level-synchronous, 2 grid-wide), reps

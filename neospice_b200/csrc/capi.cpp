@@ -29,8 +29,8 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  const InstDesc* insts, int count, const int32_t* n_of,
                                  const double* A, double* LU, double diag_gmin, int check_pivots,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
-                                 double* lrows, double* urows, void* scratch,
-                                 cudaStream_t stream);
+                                 double* lrows, double* urows, void* scratch, int colbuf,
+                                 int max_col, cudaStream_t stream);
 cudaError_t launch_complex_refactor(const PlanDesc* plans, const int32_t* pool,
                                     const InstDesc* insts, int count, int max_n, const double* A,
                                     double* LU, int32_t* status, cudaStream_t stream);
@@ -583,7 +583,7 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
         cudaError_t e = nsg::launch_grid_refactor(
             b->d_plans, b->d_pool, b->d_insts, b->count, b->n_of.data(), d_values, b->d_lu,
             diag_gmin, mode, 1e-3, d_status, d_fail_step, b->d_lrows, b->d_urows, b->d_grid,
-            static_cast<cudaStream_t>(stream));
+            b->grid_colbuf, b->max_col, static_cast<cudaStream_t>(stream));
         if (e == cudaSuccess) b->rows_valid = true;
         return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
     }
@@ -619,6 +619,13 @@ int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
 }
 
 const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
+
+int nsg_batch_set_grid_buffer(nsg_batch* b, int doubles) {
+    if (!b || (doubles != 0 && doubles != 1024 && doubles != 2048 && doubles != 4096))
+        return fail(NSG_ERR_INVALID, "nsg_batch_set_grid_buffer: bad arguments");
+    b->grid_colbuf = doubles;
+    return NSG_OK;
+}
 
 int nsg_batch_set_schedule(nsg_batch* b, int schedule) {
     if (!b || schedule < 0 || schedule > 2)

@@ -54,6 +54,7 @@ struct nsg_batch {
     int max_n = 0;
     bool allow_flow = true;
     int schedule = 0;             // nsg_batch_set_schedule
+    int grid_colbuf = 0;          // nsg_batch_set_grid_buffer (0: automatic)
     std::vector<int32_t> n_of;    // unknowns of the instance in each slot of d_insts
     void* d_grid = nullptr;       // flags and state of the grid-wide schedule
     double* d_cwork = nullptr;    // complex sweep workspace (2 doubles per unknown)

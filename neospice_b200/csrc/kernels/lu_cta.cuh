@@ -648,11 +648,14 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
 
 // x <- A^{-1} x from the LU in lu_s: lane 0, row after row in pivot order
 // (forward: ascending, backward: descending), each row's entries in the
-// order of the level-scheduled sweeps.  Begins and ends with __syncthreads().
+// order of the level-scheduled sweeps.  The next row's bounds and pivot are
+// fetched while the current row is computed, so only the values carry the
+// dependency from row to row.  Begins and ends with __syncthreads().
 static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
                                                     const int32_t* __restrict__ pool,
-                                                    const double* lu_s, double* __restrict__ x,
-                                                    double* w) {
+                                                    const double* __restrict__ lu_s,
+                                                    double* __restrict__ x,
+                                                    double* __restrict__ w) {
     const int32_t n = pd.n;
     const int32_t* perm_row = pool + pd.off[PA_perm_row];
     const int32_t* perm_col = pool + pd.off[PA_perm_col];
@@ -661,25 +664,31 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
     __syncthreads();
     for (int32_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = x[perm_row[i]];
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && n > 0) {
         {   // forward: L (Markowitz: skip zero operands, then the reciprocal pivot)
             const int32_t* lp = pool + pd.off[PA_lrow_ptr];
             const int32_t* lpos = pool + pd.off[PA_lrow_pos];
             const int32_t* lcol = pool + pd.off[PA_lrow_col];
-            int32_t e = lp[0];
+            int32_t e = lp[0], e1 = lp[1];
+            double piv = amd ? 0.0 : lu_s[diag_pos[0]];
             for (int32_t i = 0; i < n; ++i) {
-                const int32_t e1 = lp[i + 1];
+                const bool more = i + 1 < n;
+                const int32_t e1n = more ? lp[i + 2] : 0;
+                const double pivn = (more && !amd) ? lu_s[diag_pos[i + 1]] : 0.0;
                 double t = w[i];
                 if (amd) {
                     for (; e < e1; ++e) t = lu_sub(t, lu_mul(lu_s[lpos[e]], w[lcol[e]]));
                     w[i] = t;
-                    continue;
+                } else {
+                    for (; e < e1; ++e) {
+                        const double l = lu_s[lpos[e]];
+                        const double xc = w[lcol[e]];
+                        if (xc != 0.0) t = lu_sub(t, lu_mul(xc, l));
+                    }
+                    w[i] = (t != 0.0) ? lu_mul(t, piv) : t;
                 }
-                for (; e < e1; ++e) {
-                    const double xc = w[lcol[e]];
-                    if (xc != 0.0) t = lu_sub(t, lu_mul(xc, lu_s[lpos[e]]));
-                }
-                w[i] = (t != 0.0) ? lu_mul(t, lu_s[diag_pos[i]]) : t;
+                e1 = e1n;
+                piv = pivn;
             }
         }
         {   // backward: U row dot products (AMD-LU: columns descending, then
@@ -687,17 +696,25 @@ static __device__ __noinline__ void cta_solve_small(const PlanDesc& pd,
             const int32_t* up = pool + pd.off[PA_urow_ptr];
             const int32_t* upos = pool + pd.off[PA_urow_pos];
             const int32_t* ucol = pool + pd.off[PA_urow_col];
+            int32_t e0 = up[n - 1], e1 = up[n];
+            double piv = amd ? lu_s[diag_pos[n - 1]] : 0.0;
             for (int32_t i = n - 1; i >= 0; --i) {
-                const int32_t e0 = up[i], e1 = up[i + 1];
+                const bool more = i > 0;
+                const int32_t e0n = more ? up[i - 1] : 0;
+                const double pivn = (more && amd) ? lu_s[diag_pos[i - 1]] : 0.0;
                 double t = w[i];
                 if (amd) {
                     for (int32_t e = e1 - 1; e >= e0; --e)
                         t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
-                    w[i] = __ddiv_rn(t, lu_s[diag_pos[i]]);
-                    continue;
+                    w[i] = __ddiv_rn(t, piv);
+                } else {
+                    for (int32_t e = e0; e < e1; ++e)
+                        t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
+                    w[i] = t;
                 }
-                for (int32_t e = e0; e < e1; ++e) t = lu_sub(t, lu_mul(lu_s[upos[e]], w[ucol[e]]));
-                w[i] = t;
+                e1 = e0;
+                e0 = e0n;
+                piv = pivn;
             }
         }
     }

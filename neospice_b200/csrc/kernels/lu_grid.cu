@@ -24,9 +24,8 @@ namespace nsg {
 
 namespace {
 
-constexpr int kGridWarps = 8;
+constexpr int kGridWarps = 8;    // warps per CTA of the grid-wide sweeps
 constexpr int kGridThreads = kGridWarps * 32;
-constexpr int kGridColbuf = 1024;  // doubles of shared column buffer per warp
 
 __device__ __forceinline__ int32_t gflag_acquire(const int32_t* f) {
     int32_t v;
@@ -60,7 +59,10 @@ struct GridState {
     unsigned long long fail_inv;   // max of ~fail_key over failing columns (0: none)
 };
 
-__global__ void __launch_bounds__(kGridThreads)
+// kWarps warps per CTA, each with a shared column buffer of kColbuf doubles
+// (columns longer than that are eliminated in place in lu).
+template <int kWarps, int kColbuf>
+__global__ void __launch_bounds__(kWarps * 32)
 grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
                      const InstDesc* __restrict__ insts, int inst, const double* __restrict__ A,
                      double* LU, double diag_gmin, int check_pivots, double rel_threshold,
@@ -71,7 +73,7 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
     const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    double* sbuf = smem + warp * kGridColbuf;
+    double* sbuf = smem + warp * kColbuf;
     double* lu = LU + id.lu_off;
     double* lr = lrows ? lrows + id.lrows_off : nullptr;
     double* ur = urows ? urows + id.urows_off : nullptr;
@@ -81,7 +83,7 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
         j = __shfl_sync(0xffffffffu, j, 0);
         if (j >= pd.n) break;
         const int32_t len = col_ptr[j + 1] - col_ptr[j];
-        double* buf = (len <= kGridColbuf) ? sbuf : lu + col_ptr[j];
+        double* buf = (len <= kColbuf) ? sbuf : lu + col_ptr[j];
         const ColumnResult c = refactor_column<true>(
             pd, pool, A + id.a_off, lu, diag_gmin, check_pivots, rel_threshold, j, buf, lr, ur,
             [&](int32_t r) { return gflag_acquire(done + r); });
@@ -188,18 +190,20 @@ grid_solve_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict_
     if (!ok) atomicExch(&st->timeout, 1);
 }
 
+template <int kWarps, int kColbuf>
 int grid_refactor_blocks() {
     static int blocks = 0;
     if (blocks == 0) {
-        const size_t smem = sizeof(double) * kGridWarps * kGridColbuf;
-        if (cudaFuncSetAttribute(grid_refactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const size_t smem = sizeof(double) * kWarps * kColbuf;
+        if (cudaFuncSetAttribute(grid_refactor_kernel<kWarps, kColbuf>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)) != cudaSuccess)
             return 0;
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_refactor_kernel, kGridThreads,
-                                                      smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_refactor_kernel<kWarps, kColbuf>,
+                                                      kWarps * 32, smem);
         blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     return blocks;
@@ -222,26 +226,53 @@ size_t grid_scratch_bytes(int max_n) {
     return sizeof(GridState) * 2 + sizeof(int32_t) * static_cast<size_t>(max_n);
 }
 
-// Refactor every instance of the batch in turn with the whole GPU.
+// Refactor every instance of the batch in turn with the whole GPU.  The
+// per-warp column buffer: colbuf doubles (1024, 2048 or 4096; 0 = the
+// smallest that holds the longest column, max_col).  1024: 8 warps and
+// 64 KB per CTA, three CTAs per SM; 2048: 8 warps, 128 KB, one per SM;
+// 4096: 4 warps, 128 KB.  Fewer warps in flight, but the long separator
+// columns at the top of the elimination stay in shared memory instead of
+// being updated in place in global memory.
 cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  const InstDesc* insts, int count, const int32_t* n_of,
                                  const double* A, double* LU, double diag_gmin, int check_pivots,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
-                                 double* lrows, double* urows, void* scratch,
-                                 cudaStream_t stream) {
-    const int blocks = grid_refactor_blocks();
+                                 double* lrows, double* urows, void* scratch, int colbuf,
+                                 int max_col, cudaStream_t stream) {
+    if (colbuf == 0) colbuf = max_col <= 1024 ? 1024 : (max_col <= 2048 ? 2048 : 4096);
+    int blocks = 0, threads = 0;
+    size_t smem = 0;
+    if (colbuf == 1024) {
+        blocks = grid_refactor_blocks<8, 1024>();
+        threads = 256;
+        smem = sizeof(double) * 8 * 1024;
+    } else if (colbuf == 2048) {
+        blocks = grid_refactor_blocks<8, 2048>();
+        threads = 256;
+        smem = sizeof(double) * 8 * 2048;
+    } else if (colbuf == 4096) {
+        blocks = grid_refactor_blocks<4, 4096>();
+        threads = 128;
+        smem = sizeof(double) * 4 * 4096;
+    } else {
+        return cudaErrorInvalidValue;
+    }
     if (blocks == 0) return cudaErrorInvalidConfiguration;
     GridState* st = static_cast<GridState*>(scratch);
     int32_t* done = reinterpret_cast<int32_t*>(st + 2);
-    const size_t smem = sizeof(double) * kGridWarps * kGridColbuf;
     for (int i = 0; i < count; ++i) {
         cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(GridState) * 2 +
                                                         sizeof(int32_t) * static_cast<size_t>(n_of[i]),
                                         stream);
         if (e != cudaSuccess) return e;
-        grid_refactor_kernel<<<blocks, kGridThreads, smem, stream>>>(
-            plans, pool, insts, i, A, LU, diag_gmin, check_pivots, rel_threshold, lrows, urows,
-            done, st);
+#define NSG_GRID_REFACTOR(W, C)                                                                \
+        grid_refactor_kernel<W, C><<<blocks, threads, smem, stream>>>(                         \
+            plans, pool, insts, i, A, LU, diag_gmin, check_pivots, rel_threshold, lrows, urows, \
+            done, st)
+        if (colbuf == 1024) NSG_GRID_REFACTOR(8, 1024);
+        else if (colbuf == 2048) NSG_GRID_REFACTOR(8, 2048);
+        else NSG_GRID_REFACTOR(4, 4096);
+#undef NSG_GRID_REFACTOR
         grid_refactor_status_kernel<<<1, 32, 0, stream>>>(plans, insts, i, check_pivots, st,
                                                           status, fail_step);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -22,7 +22,7 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  const int32_t* __restrict__ prog, const double* __restrict__ params,
                  double* __restrict__ work, double* __restrict__ solutions,
                  int32_t* __restrict__ status, int32_t* __restrict__ iterations,
-                 DcCtl* __restrict__ ctls, NewtonOptions opt_in, int colbuf, int scratch_doubles,
+                 DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf, int scratch_doubles,
                  int stage_doubles, int plan_words) {
     extern __shared__ double smem[];
     const DcDesc d = descs[subset ? subset[blockIdx.x] : blockIdx.x];
@@ -34,17 +34,10 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     const PlanDesc& pd = s_pd;
     double* stage = (d.stage_len <= stage_doubles) ? smem + scratch_doubles : nullptr;
     stage_copy(d, work, stage, true);
-    // The instance's views, once per CTA in shared memory (a per-thread copy
-    // would sit in every thread's stack frame, far beyond L1).
-    __shared__ Inst s_v;
-    __shared__ NewtonOptions s_opt;  // options by reference, not a per-thread copy
-    if (threadIdx.x == 0) {
-        s_v = make_inst(d, prog, params, work, stage);
-        s_opt = opt_in;
-    }
-    __syncthreads();
-    const Inst& v = s_v;
-    const NewtonOptions& opt = s_opt;
+    // Per-thread views (not a shared copy as in the transient kernel): the
+    // dataflow scratch of large meshes fills the shared memory of two CTAs
+    // per SM to within a few hundred bytes.
+    const Inst v = make_inst(d, prog, params, work, stage);
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
     __shared__ int32_t s_fresh;

@@ -174,6 +174,11 @@ class Batch:
         """0 = dataflow refactor (default), 1 = level-synchronous."""
         L.check(L.lib().nsg_batch_set_schedule(self._h, int(schedule)))
 
+    def set_grid_buffer(self, doubles: int):
+        """Shared column buffer per warp of the grid-wide refactor (1024,
+        2048, 4096; 0 = automatic)."""
+        L.check(L.lib().nsg_batch_set_grid_buffer(self._h, int(doubles)))
+
     def refactor(self, d_values, diag_gmin=0.0, check_pivots=False, d_status=None,
                  d_fail_step=None, stream=None):
         """Batched spFactor; returns the device status tensor (int32)."""
