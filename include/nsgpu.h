@@ -175,6 +175,13 @@ int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
  * longest column.  Longer columns are eliminated in place in global memory.
  * No counterpart in the reference (a tuning knob of this schedule). */
 int nsg_batch_set_grid_buffer(nsg_batch* batch, int doubles);
+/* Largest refactor update map (int32 words, one per multiply-subtract) a
+ * topology ordered from now on may carry; default 2^30 (4 GiB).  A larger
+ * factorization gets no map: its batches run only the grid-wide schedule,
+ * which finds each update's destination through a per-warp row -> position
+ * map (n words per warp of the grid), and circuit batches refuse it.  No
+ * counterpart in the reference (its refactor walks linked lists). */
+int nsg_set_update_map_limit(long long words);
 
 /* Schedule autotuner: refactor d_values (as a refactorize()) and solve d_x
  * under each schedule (0 dataflow, 1 level-synchronous, 2 grid-wide), reps

@@ -30,7 +30,9 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  const double* A, double* LU, double diag_gmin, int check_pivots,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
                                  double* lrows, double* urows, void* scratch, int colbuf,
-                                 int max_col, cudaStream_t stream);
+                                 int max_col, int32_t* rmaps, int64_t rmap_words,
+                                 cudaStream_t stream);
+int64_t grid_rmap_words(int colbuf, int max_col, int max_n);
 cudaError_t launch_complex_refactor(const PlanDesc* plans, const int32_t* pool,
                                     const InstDesc* insts, int count, int max_n, const double* A,
                                     double* LU, int32_t* status, cudaStream_t stream);
@@ -190,6 +192,7 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.nnz_l = p.lrow_ptr[p.n];
     d.nnz_u = p.urow_ptr[p.n];
     d.kind = p.kind;
+    d.has_map = p.has_update_map ? 1 : 0;
     // grow geometrically once for this plan, so a multi-gigabyte update map
     // is copied once (appending to an unreserved pool re-copies it)
     const size_t need = pool.size() + static_cast<size_t>(p.device_words()) + 4 * nsg::PA_COUNT + 4;
@@ -272,6 +275,8 @@ int refresh_plans(const std::vector<std::unique_ptr<nsg_topology>>& topos, int32
     std::vector<int32_t> pool;
     std::vector<nsg::PlanDesc> plans;
     for (const auto& t : topos) {
+        if (!t->plan.has_update_map)
+            return fail(NSG_ERR_INVALID, "circuit too large for the batched Newton kernels");
         plans.push_back(make_plan_desc(t->plan, pool));
         *max_col = std::max(*max_col, t->plan.max_col);
         *max_n = std::max(*max_n, t->plan.n);
@@ -492,6 +497,7 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
                 plans.push_back(make_plan_desc(t->plan, pool));
             }
             const auto& p = t->plan;
+            if (!p.has_update_map) b->unmapped = true;
             b->max_col = std::max(b->max_col, p.max_col);
             b->max_n = std::max(b->max_n, p.n);
             insts[i].plan = it->second;
@@ -524,6 +530,12 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             (e = upload<double>(&b->d_lrows, nullptr, lrows)) != cudaSuccess ||
             (e = upload<double>(&b->d_urows, nullptr, urows)) != cudaSuccess)
             return cuda_fail("nsg_batch_create", e);
+        // A plan too large for an update map runs only on the grid-wide
+        // schedule (per-warp row maps instead).
+        if (b->unmapped) {
+            b->schedule = 2;
+            b->allow_flow = false;
+        }
         *out = b.release();
         return NSG_OK;
     });
@@ -535,6 +547,9 @@ int nsg_batch_refactor_complex(nsg_batch* b, const double* d_ax, double* d_lu, i
                                void* stream) {
     if (!b || !d_ax || !d_lu || !d_status)
         return fail(NSG_ERR_INVALID, "nsg_batch_refactor_complex: null argument");
+    if (b->unmapped)
+        return fail(NSG_ERR_INVALID, "nsg_batch_refactor_complex: topology too large for an "
+                                     "update map");
     const size_t smem = nsg::complex_refactor_smem(b->max_n);
     if (smem > 200 * 1024)
         return fail(NSG_ERR_INVALID, "nsg_batch_refactor_complex: too many unknowns per instance "
@@ -580,10 +595,23 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
             cudaError_t e = cudaMalloc(&b->d_grid, nsg::grid_scratch_bytes(b->max_n));
             if (e != cudaSuccess) return cuda_fail("nsg_batch_refactor", e);
         }
+        if (b->unmapped) {
+            const int64_t words = nsg::grid_rmap_words(b->grid_colbuf, b->max_col, b->max_n);
+            if (words > b->rmap_cap) {
+                cudaFree(b->d_rmap);
+                b->d_rmap = nullptr;
+                b->rmap_cap = 0;
+                cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_rmap),
+                                           sizeof(int32_t) * static_cast<size_t>(words));
+                if (e != cudaSuccess) return cuda_fail("nsg_batch_refactor", e);
+                b->rmap_cap = words;
+            }
+        }
         cudaError_t e = nsg::launch_grid_refactor(
             b->d_plans, b->d_pool, b->d_insts, b->count, b->n_of.data(), d_values, b->d_lu,
             diag_gmin, mode, 1e-3, d_status, d_fail_step, b->d_lrows, b->d_urows, b->d_grid,
-            b->grid_colbuf, b->max_col, static_cast<cudaStream_t>(stream));
+            b->grid_colbuf, b->max_col, b->unmapped ? b->d_rmap : nullptr, b->max_n,
+            static_cast<cudaStream_t>(stream));
         if (e == cudaSuccess) b->rows_valid = true;
         return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
     }
@@ -620,6 +648,12 @@ int nsg_batch_solve_transposed(nsg_batch* b, double* d_x, void* stream) {
 
 const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
 
+int nsg_set_update_map_limit(long long words) {
+    if (words < 0) return fail(NSG_ERR_INVALID, "nsg_set_update_map_limit: negative limit");
+    nsg::set_update_map_limit(words);
+    return NSG_OK;
+}
+
 int nsg_batch_set_grid_buffer(nsg_batch* b, int doubles) {
     if (!b || (doubles != 0 && doubles != 1024 && doubles != 2048 && doubles != 4096))
         return fail(NSG_ERR_INVALID, "nsg_batch_set_grid_buffer: bad arguments");
@@ -630,6 +664,9 @@ int nsg_batch_set_grid_buffer(nsg_batch* b, int doubles) {
 int nsg_batch_set_schedule(nsg_batch* b, int schedule) {
     if (!b || schedule < 0 || schedule > 2)
         return fail(NSG_ERR_INVALID, "nsg_batch_set_schedule: bad arguments");
+    if (b->unmapped && schedule != 2)
+        return fail(NSG_ERR_INVALID, "nsg_batch_set_schedule: a topology of this batch is too "
+                                     "large for an update map; only schedule 2 runs it");
     b->allow_flow = (schedule == 0);
     b->schedule = schedule;
     b->rows_valid = false;

@@ -510,6 +510,9 @@ int nsg_dc_batch_create(int count, nsg_circuit* const* circuits, int symbolic, i
         std::vector<int32_t> lu_pool, prog;
         std::vector<nsg::PlanDesc> plans;
         for (const auto& t : b->topos) {
+            if (!t->plan.has_update_map)
+                throw std::invalid_argument("circuit too large for the batched Newton kernels "
+                                            "(its factorization has no update map)");
             plans.push_back(make_plan_desc(t->plan, lu_pool));
             b->max_col = std::max(b->max_col, t->plan.max_col);
             b->max_n = std::max(b->max_n, t->plan.n);

@@ -55,10 +55,14 @@ struct nsg_batch {
     bool allow_flow = true;
     int schedule = 0;             // nsg_batch_set_schedule
     int grid_colbuf = 0;          // nsg_batch_set_grid_buffer (0: automatic)
+    bool unmapped = false;        // a plan has no update map (grid-wide schedule only)
+    int32_t* d_rmap = nullptr;    // per-warp row -> position maps of such plans
+    int64_t rmap_cap = 0;         // words allocated at d_rmap
     std::vector<int32_t> n_of;    // unknowns of the instance in each slot of d_insts
     void* d_grid = nullptr;       // flags and state of the grid-wide schedule
     double* d_cwork = nullptr;    // complex sweep workspace (2 doubles per unknown)
     ~nsg_batch() {
+        cudaFree(d_rmap);
         cudaFree(d_cwork);
         cudaFree(d_grid);
         cudaFree(d_pool);

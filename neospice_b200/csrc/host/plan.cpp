@@ -13,6 +13,13 @@
 namespace nsg {
 
 namespace {
+std::atomic<int64_t> g_update_map_limit{int64_t{1} << 30};
+}  // namespace
+
+int64_t update_map_limit() { return g_update_map_limit.load(); }
+void set_update_map_limit(int64_t words) { g_update_map_limit.store(words); }
+
+namespace {
 
 // Counting sort of items by level; returns (ptr over levels, members).
 void level_sort(const std::vector<int32_t>& level, std::vector<int32_t>& ptr,
@@ -59,13 +66,20 @@ void finish(TopologyPlan& p) {
     for (int32_t j = 0; j < n; ++j)
         for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j]; ++q) {
             const int32_t r = p.row_idx[q];
-            if (total > INT32_MAX) break;
-            p.upd_start[q] = static_cast<int32_t>(total);
             total += p.col_ptr[r + 1] - p.diag_pos[r] - 1;
         }
-    if (total > INT32_MAX) throw std::invalid_argument("plan: update map too large");
+    p.has_update_map = total <= update_map_limit();
+    if (p.has_update_map) {
+        int64_t start = 0;
+        for (int32_t j = 0; j < n; ++j)
+            for (int32_t q = p.col_ptr[j]; q < p.diag_pos[j]; ++q) {
+                p.upd_start[q] = static_cast<int32_t>(start);
+                const int32_t r = p.row_idx[q];
+                start += p.col_ptr[r + 1] - p.diag_pos[r] - 1;
+            }
+    }
     p.upd_dst.clear();
-    p.upd_dst.resize(static_cast<size_t>(total));  // every entry written below
+    if (p.has_update_map) p.upd_dst.resize(static_cast<size_t>(total));  // every entry written below
     // First failing column of each kind (duplicate row / fill not closed),
     // so that the error does not depend on the thread schedule.
     std::atomic<int32_t> bad_dup{INT32_MAX}, bad_fill{INT32_MAX};
@@ -107,7 +121,7 @@ void finish(TopologyPlan& p) {
             }
         }
     };
-    {
+    if (p.has_update_map) {
         std::atomic<int32_t> next_col{0};
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
         const int nthreads = total >= (int64_t{1} << 25) ? static_cast<int>(std::min(hw, 16u)) : 1;

@@ -9,6 +9,11 @@
 
 namespace nsg {
 
+// Largest update map a plan carries (int32 words; default 2^30, 4 GiB),
+// process-wide (nsg_set_update_map_limit).
+int64_t update_map_limit();
+void set_update_map_limit(int64_t words);
+
 // An allocator whose resize() leaves new int32 elements uninitialised: the
 // refactor's update map (one word per multiply-subtract, gigabytes for large
 // grids) is written entirely by the threads that fill it, so each thread
@@ -70,6 +75,10 @@ struct TopologyPlan {
     // the start of column j.
     std::vector<int32_t> upd_start;
     std::vector<int32_t, UninitAllocator<int32_t>> upd_dst;
+    // False when the map would exceed update_map_limit(): upd_start is then
+    // all zero, upd_dst empty, and the grid-wide refactor finds each
+    // destination through a per-warp row -> position map instead.
+    bool has_update_map = true;
 
     // L by rows (strictly lower, columns ascending) and U by rows (strictly
     // upper, columns ascending): LU position and column of each entry.

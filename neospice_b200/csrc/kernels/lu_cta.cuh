@@ -193,12 +193,16 @@ __device__ __forceinline__ double lu_peer(const double* p) {
 // (through lu_src, diag_gmin added), applies every U entry in stored order
 // after column r is done, judges the pivot (check_pivots, kCheck*), and
 // writes the column (and its row-major copies) to lu.  Ends with
-// __syncwarp(); the caller publishes completion.
+// __syncwarp(); the caller publishes completion.  The position in column j
+// of each row of L(:, r) comes from the plan's update map, or, for plans
+// without one (pd.has_map == 0), from rmap: this warp's row -> position
+// scratch (pd.n words), written for column j's rows first.
 template <bool kCrossSm, class Probe>
 __device__ __forceinline__ ColumnResult refactor_column(
     const PlanDesc& pd, const int32_t* __restrict__ pool, const double* __restrict__ a,
     double* lu, double diag_gmin, int check_pivots, double rel_threshold, int32_t j, double* buf,
-    double* __restrict__ lrows, double* __restrict__ urows, Probe probe) {
+    double* __restrict__ lrows, double* __restrict__ urows, Probe probe,
+    int32_t* rmap = nullptr) {
     const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
@@ -212,13 +216,20 @@ __device__ __forceinline__ ColumnResult refactor_column(
     const int32_t len = col_ptr[j + 1] - c0;
     const int32_t dj = diag_pos[j] - c0;
     const int32_t gp = amd ? gmin_pos[j] : dj;
+    const int32_t* row_idx = pool + pd.off[PA_row_idx];
+    const bool mapped = pd.has_map != 0;
     for (int32_t t = lane; t < len; t += 32) {
         const int32_t s = lu_src[c0 + t];
         double v = (s >= 0) ? a[s] : 0.0;
         if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
         buf[t] = v;
+        if (!mapped) rmap[row_idx[c0 + t]] = t;
     }
     __syncwarp();
+    // Position in column j of entry t of L(:, r) (its k-th update).
+    auto dest = [&](int32_t us, int32_t l0, int32_t t) -> int32_t {
+        return mapped ? upd_dst[us + t] : rmap[row_idx[l0 + t]];
+    };
     double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
     // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
     // entries at a time in registers (lane k holds entry base+k) and
@@ -259,7 +270,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
         cnt = m.z;
         us = m.w;
         lv = (lane < cnt) ? lu_peer<kCrossSm>(lu + l0 + lane) : 0.0;
-        ld = (lane < cnt) ? upd_dst[us + lane] : 0;
+        ld = (lane < cnt) ? dest(us, l0, lane) : 0;
         return true;
     };
     auto meta = [&](int32_t q) -> int4 {
@@ -302,7 +313,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
 #pragma unroll
             for (int k = 0; k < kColChunk; ++k) {
                 const int32_t t = t0 + 32 * k + lane;
-                dd[k] = (t < cnt_c) ? upd_dst[us_c + t] : 0;
+                dd[k] = (t < cnt_c) ? dest(us_c, l0_c, t) : 0;
                 ll[k] = (t < cnt_c) ? lu_peer<kCrossSm>(lu + l0_c + t) : 0.0;
             }
 #pragma unroll

@@ -20,6 +20,7 @@ struct PlanDesc {
     int32_t max_col;  // longest LU column
     int32_t nnz_l, nnz_u;  // strictly lower / upper entries
     int32_t kind;          // kPlanMarkowitz or kPlanAmdLu
+    int32_t has_map;       // 1: PA_upd_start / PA_upd_dst hold the update map
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
     int64_t words;          // words from off[0] that hold all of the plan's arrays
 };

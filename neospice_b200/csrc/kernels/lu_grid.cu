@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(kWarps * 32)
 grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
                      const InstDesc* __restrict__ insts, int inst, const double* __restrict__ A,
                      double* LU, double diag_gmin, int check_pivots, double rel_threshold,
-                     double* lrows, double* urows, int32_t* done, GridState* st) {
+                     double* lrows, double* urows, int32_t* done, GridState* st,
+                     int32_t* rmaps, int64_t rmap_words) {
     extern __shared__ double smem[];
     const InstDesc id = insts[inst];
     const PlanDesc& pd = plans[id.plan];
@@ -74,6 +75,9 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     double* sbuf = smem + warp * kColbuf;
+    // row -> position scratch of this warp (plans without an update map)
+    int32_t* rmap = rmaps ? rmaps + (static_cast<int64_t>(blockIdx.x) * kWarps + warp) * rmap_words
+                          : nullptr;
     double* lu = LU + id.lu_off;
     double* lr = lrows ? lrows + id.lrows_off : nullptr;
     double* ur = urows ? urows + id.urows_off : nullptr;
@@ -86,7 +90,7 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
         double* buf = (len <= kColbuf) ? sbuf : lu + col_ptr[j];
         const ColumnResult c = refactor_column<true>(
             pd, pool, A + id.a_off, lu, diag_gmin, check_pivots, rel_threshold, j, buf, lr, ur,
-            [&](int32_t r) { return gflag_acquire(done + r); });
+            [&](int32_t r) { return gflag_acquire(done + r); }, rmap);
         __threadfence();
         __syncwarp();
         if (lane == 0) {
@@ -233,13 +237,30 @@ size_t grid_scratch_bytes(int max_n) {
 // 4096: 4 warps, 128 KB.  Fewer warps in flight, but the long separator
 // columns at the top of the elimination stay in shared memory instead of
 // being updated in place in global memory.
+static int grid_colbuf(int colbuf, int max_col) {
+    return colbuf != 0 ? colbuf : (max_col <= 1024 ? 1024 : (max_col <= 2048 ? 2048 : 4096));
+}
+
+// Words of the per-warp row -> position maps a launch with these settings
+// needs for plans without an update map (every warp of the grid, n words
+// each).
+int64_t grid_rmap_words(int colbuf, int max_col, int max_n) {
+    colbuf = grid_colbuf(colbuf, max_col);
+    int warps = 0;
+    if (colbuf == 1024) warps = grid_refactor_blocks<8, 1024>() * 8;
+    else if (colbuf == 2048) warps = grid_refactor_blocks<8, 2048>() * 8;
+    else warps = grid_refactor_blocks<4, 4096>() * 4;
+    return static_cast<int64_t>(warps) * max_n;
+}
+
 cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  const InstDesc* insts, int count, const int32_t* n_of,
                                  const double* A, double* LU, double diag_gmin, int check_pivots,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
                                  double* lrows, double* urows, void* scratch, int colbuf,
-                                 int max_col, cudaStream_t stream) {
-    if (colbuf == 0) colbuf = max_col <= 1024 ? 1024 : (max_col <= 2048 ? 2048 : 4096);
+                                 int max_col, int32_t* rmaps, int64_t rmap_words,
+                                 cudaStream_t stream) {
+    colbuf = grid_colbuf(colbuf, max_col);
     int blocks = 0, threads = 0;
     size_t smem = 0;
     if (colbuf == 1024) {
@@ -268,7 +289,7 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
 #define NSG_GRID_REFACTOR(W, C)                                                                \
         grid_refactor_kernel<W, C><<<blocks, threads, smem, stream>>>(                         \
             plans, pool, insts, i, A, LU, diag_gmin, check_pivots, rel_threshold, lrows, urows, \
-            done, st)
+            done, st, rmaps, rmap_words)
         if (colbuf == 1024) NSG_GRID_REFACTOR(8, 1024);
         else if (colbuf == 2048) NSG_GRID_REFACTOR(8, 2048);
         else NSG_GRID_REFACTOR(4, 4096);

@@ -66,3 +66,39 @@ def test_grid_schedule_power_grid_matches_reference():
                              for k in range(n)])
     np.testing.assert_array_equal(lu, packed)
     np.testing.assert_array_equal(x, x_ref)
+
+
+@pytest.mark.parametrize("engine", ["amdlu", "markowitz"])
+@pytest.mark.parametrize("colbuf", [0, 1024, 2048, 4096])
+def test_plans_without_update_map(engine, colbuf):
+    """A factorization too large for an update map (forced here by a zero
+    limit) runs on the grid-wide schedule with per-warp row -> position maps:
+    factors and solutions bit-identical to the mapped plan's, for every
+    column-buffer size; other schedules and circuit batches refuse it."""
+    from neospice_b200 import _lib as L
+    from neospice_b200.circuit import DcBatch
+    rng = np.random.default_rng(11)
+    n, cp, ri, vals = grid_matrix(60, 12, 30, 4)
+    b = rng.standard_normal(n)
+    mapped = Topology.order(n, cp, ri, vals, solver=engine)
+    st0, lu0, x0 = factor_and_solve(mapped, vals, b, 2)
+    assert L.lib().nsg_set_update_map_limit(0) == L.NSG_OK
+    try:
+        bare = Topology.order(n, cp, ri, vals, solver=engine)
+        batch = Batch([bare])
+        with pytest.raises(L.NsgError):
+            batch.set_schedule(0)
+        batch.set_grid_buffer(colbuf)
+        d_a = torch.from_numpy(np.asarray(vals, np.float64)).cuda()
+        for _ in range(2):  # the second call reuses the row maps
+            st, _ = batch.refactor(d_a)
+            d_x = torch.from_numpy(b.copy()).cuda()
+            batch.solve(d_x)
+            torch.cuda.synchronize()
+            assert int(st.cpu()[0]) == st0 == 0
+            np.testing.assert_array_equal(batch.lu_values()[:len(lu0)], lu0)
+            np.testing.assert_array_equal(d_x.cpu().numpy(), x0)
+        with pytest.raises(L.NsgError):
+            DcBatch([W.power_grid(np.random.default_rng(1), 12, 6, 4).build()])
+    finally:
+        assert L.lib().nsg_set_update_map_limit(1 << 30) == L.NSG_OK
