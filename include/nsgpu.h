@@ -542,15 +542,17 @@ int nsg_tran_batch_params(const nsg_tran_batch* b, long long* offsets, double* p
                           double* params_tran);
 /* Gradient of L_i = weight * sum_n (x_n[probe[i]] - target_n)^2 over instance
  * i's recorded timepoints (n = 0 the operating point; d_targets: count *
- * max_points device doubles) with respect to every resistance, capacitance
- * and MOSFET W, L, VTO, into d_grads (device, packed like the parameters; 0
- * elsewhere: the replay starts from the recorded operating point, so source
- * values, which move it, are not differentiated), d_loss[count] and d_status[count] (0, or a
- * Newton / singular / bounded-wait code).  The steps are replayed with a
+ * max_points device doubles) with respect to every resistance, capacitance,
+ * DC source value and MOSFET W, L, VTO, into d_grads (device, packed like the
+ * parameters; 0 elsewhere: waveform-source and diode parameters), d_loss[count]
+ * and d_status[count] (0, or a Newton / singular / bounded-wait code).  The
+ * replay re-solves the operating point with the replayed parameters, starting
+ * from the recorded one.  The steps are replayed with a
  * checkpoint every `every` steps.  d_params_dc / d_params_tran (device, may
  * be NULL: the batch's own) replace the parameters of the replay.  Refused
- * (NSG_ERR_INVALID): no recorded run, a run that filled max_points, diodes,
- * or MOSFETs with charge. */
+ * (NSG_ERR_INVALID): no recorded run, a run that filled max_points, or
+ * MOSFETs with charge (diodes and their charge are covered; diode
+ * parameters are not differentiated). */
 int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_targets,
                            double weight, int every, const double* d_params_dc,
                            const double* d_params_tran, double* d_grads, double* d_loss,

@@ -11,8 +11,9 @@ entries of the parameter blocks).
 ``tran_loss(batch, probes, targets, params)`` returns, per instance of a
 recorded ``TranBatch``, L_i = weight * sum_n (x_n[probe_i] - target_n)^2 over
 the recorded timepoints, and its backward is the transient adjoint (a
-transposed solve on each step's LU, checkpointed replay, capacitor-charge
-recursion) with respect to resistances, capacitances and MOSFET W, L and VTO.
+transposed solve on each step's LU, checkpointed replay, capacitor- and
+diode-charge recursion) with respect to resistances, capacitances, DC source
+values and MOSFET W, L and VTO.
 
 Failed instances do not produce silent garbage: an instance whose forward
 solve did not converge (status != 0) gets NaN solutions / loss, and an
@@ -96,7 +97,8 @@ def tran_loss(batch, probes, targets: torch.Tensor, params: torch.Tensor | None 
     replayed at ``params`` (packed like ``batch.params()``'s DC vector; None:
     the batch's own, and no gradient flows).  ``targets`` holds
     ``max_points`` values per instance, at the recorded timepoints.
-    Differentiable with respect to ``params`` (R, C, MOSFET W / L / VTO)."""
+    Differentiable with respect to ``params`` (R, C, DC sources, MOSFET W / L /
+    VTO)."""
     probes = np.ascontiguousarray(probes, np.int32)
     if params is None:
         _, p_dc, _ = batch.params()

@@ -234,9 +234,9 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
             // The adjoint covers level-1 MOSFETs without charge (no oxide,
-            // overlap or junction capacitance in the parameter block), no
-            // diodes and no BSIM4v7 devices (which always carry charge).
-            bool ok = c.diodes().empty() && !c.has_bsim4();
+            // overlap or junction capacitance in the parameter block),
+            // diodes, and no BSIM4v7 devices (which always carry charge).
+            bool ok = !c.has_bsim4();
             for (const auto& m : c.mosfets()) {
                 if (m.family != nsg::kFamilyMos1) continue;
                 const double* P = c.params().data() + m.param;
@@ -513,7 +513,7 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             if (!b->adjoint_ok[i])
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
                                                  std::to_string(i) +
-                                                 " has diodes or MOSFETs with charge (not covered)");
+                                                 " has MOSFETs with charge (not covered)");
             if (probe[i] < 0 || probe[i] >= d.n)
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: probe out of range");
             nsg::AdjDesc& a = ad[i];
@@ -527,7 +527,7 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             a.ckpt_len = (2 * d.n + 2 * d.n_states + nsg::kMosRecCount * nmos + 3) & ~int64_t{3};
             a.ws_off = ws;
             ws += a.n_ckpt * a.ckpt_len + (every + 2) * (int64_t{d.n} + d.n_states) +
-                  3 * int64_t{d.n_caps} + d.n;
+                  3 * (int64_t{d.n_caps} + d.n_diodes) + d.n;
             ws = (ws + 3) & ~int64_t{3};
             // The LU region must hold both the DC and the transient plan.
             const auto& pd = b->topos[d.plan]->plan;

@@ -20,10 +20,15 @@
 //   dL/dp  -= lambda_n^T dR_n/dp      (R, MOSFET W / L / VTO)
 // with J_n the Newton matrix at x_n (the forward's own assembly and
 // fixed-pivot refactor) and lambda from the transposed solve; the operating
-// point closes the recursion with the DC Jacobian.  Circuits whose MOSFETs
-// carry charge (oxide, overlap or junction capacitance), and circuits with
-// diodes, are rejected by the host: their charge history is not part of
-// this recursion.
+// point closes the recursion with the DC Jacobian.  A diode's charge
+// q(v) (depletion plus transit-time charge, a function of its junction
+// voltage) enters the same recursion as a capacitor with C replaced by
+// dq/dv at the step whose charge it is (q_s appears in i_s, i_{s+1} and
+// i_{s+2}); diode parameters are not differentiated.  Circuits whose
+// MOSFETs carry charge (oxide, overlap or junction capacitance) are
+// rejected by the host: the Meyer charges are accumulated from capacitance
+// averages, not a function of the voltages, and are not part of this
+// recursion.
 #include "newton_common.cuh"
 #include "tran_device.cuh"
 
@@ -45,10 +50,10 @@ struct AdjDesc {
 
 namespace {
 
-// -lambda^T dF/dp of resistors and MOSFET channels at x (the
-// dc_adjoint_kernel contraction), accumulated into g.  Sources are skipped:
-// the replay starts from the recorded operating point, so a source value's
-// effect through x_0 would not be the replayed transient's.
+// -lambda^T dF/dp of resistors, DC sources and MOSFET channels at x (the
+// dc_adjoint_kernel contraction), accumulated into g.  A DC source's value
+// enters every step's branch (or node) equation and the operating point,
+// which the replay re-solves with the replayed parameters.
 __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32_t* prog,
                                      const double* lam, const double* x, double* g) {
     const int32_t* gp = prog + d.prog_off[DP_grad];
@@ -59,6 +64,10 @@ __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32
         if (kind == 1) {
             const double R = v.par[p];
             g[p] += (at(lam, a) - at(lam, b)) * (at(x, a) - at(x, b)) / (R * R);
+        } else if (kind == 2) {  // voltage source: F_branch = vp - vn - V
+            g[p] += at(lam, a);
+        } else if (kind == 3) {  // current source p -> n: F_p += I, F_n -= I
+            g[p] += -(at(lam, a) - at(lam, b));
         } else if (kind == 4) {
             const double* P = v.par + p;
             const double* rec = v.mrec + kMosRecCount * e[4];
@@ -72,6 +81,17 @@ __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32
             g[p + kMVto] += dl * dm * rec[kRGm];
         }
     }
+}
+
+// dq/dv of diode k's charge at junction voltage vd (DIOload's capd, without
+// limiting: vd is the voltage its last load used).
+__device__ inline double diode_capd(const Inst& v, int32_t k, double vd, double gmin) {
+    const int32_t* dr = v.diodes + 4 * k;
+    const DiodeDC r = diode_eval(vd, false, vd, v.dconst[3 * k], v.dconst[3 * k + 1],
+                                 v.dconst[3 * k + 2], gmin);
+    double q, capd;
+    diode_charge(v.par + dr[2], r.vd, r.cdb, r.gdb, &q, &capd);
+    return capd;
 }
 
 // Integrator context of accepted step n (1-based) from its record.
@@ -125,10 +145,12 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     double* ckpt = ws;
     double* seg_x = ckpt + ad.n_ckpt * ad.ckpt_len;
     double* seg_s = seg_x + (K + 2) * n;
+    // charge units: capacitors 0 .. n_caps-1, then diodes
+    const int32_t nq = v.n_caps + v.n_diodes;
     double* eta1 = seg_s + (K + 2) * ns;
-    double* eta2 = eta1 + v.n_caps;
-    double* mu = eta2 + v.n_caps;
-    double* lam = mu + v.n_caps;
+    double* eta2 = eta1 + nq;
+    double* mu = eta2 + nq;
+    double* lam = mu + nq;
     double* w = work + d.w_off;
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
@@ -169,7 +191,9 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         return 2.0 * weight * (x[ad.probe] - tg[s]);
     };
 
-    // ---- 1. operating point: the recorded x_0; states seeded from it
+    // ---- 1. operating point: re-solved with the replayed parameters by
+    // Newton from the recorded x_0 (the DC plan's pivots); states seeded
+    // from it
     v.par = params_dc + d.param_off;
     load_constants(v, opt.gmin);
     vcopy(v.x, rec_x0 + td.x0_off, n);
@@ -180,11 +204,26 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         ctx = IntegCtx{};
         ctx.mode = kModeTranOp | kModeInitFloat;
         ctx.order = 1;
+        solver.factored = 1;
         s_dev_conv = 1;
         s_fail = 0;
         s_loss = 0.0;
     }
     __syncthreads();
+    {
+        const NewtonOutcome r0 = newton(v, dpd, lu_pool, &ctx, opt, max_iter, &solver, smem,
+                                        colbuf, -1, -1, 1, false, scratch_doubles, true);
+        if (r0.code != kDcConverged) {
+            fail_with(kTranDcFailed);
+            return;
+        }
+        vcopy(v.xold, v.x, n);
+        if (threadIdx.x == 0) {
+            ctx.mode = kModeTranOp | kModeInitFloat;
+            s_dev_conv = 1;
+        }
+        __syncthreads();
+    }
     // states at x_0 (q = C v_0; MOSFET voltages, twice so that the second
     // load's limiting starts from x_0's own voltages)
     for (int pass = 0; pass < 2; ++pass) {
@@ -230,7 +269,7 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     if (threadIdx.x == 0) loss[d.index] = s_loss;
 
     // ---- 3. backward, segment by segment
-    for (int32_t k = threadIdx.x; k < v.n_caps; k += blockDim.x) eta1[k] = eta2[k] = 0.0;
+    for (int32_t k = threadIdx.x; k < nq; k += blockDim.x) eta1[k] = eta2[k] = 0.0;
     __syncthreads();
     for (int64_t c0 = ((ad.n_steps - 1) / K) * K; c0 >= 0; c0 -= K) {
         const int64_t c1 = (c0 + K < ad.n_steps) ? c0 + K : ad.n_steps;
@@ -296,6 +335,18 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
                 if (cr[0] >= 0) atomicAdd(lam + cr[0], cc);
                 if (cr[1] >= 0) atomicAdd(lam + cr[1], -cc);
             }
+            for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+                const int32_t* dr = v.diodes + 4 * k;
+                const int32_t u = v.n_caps + k;
+                const double capd = diode_capd(v, k, v.st[0][dr[3] + kDsV], opt.gmin);
+                const double m = has1 ? -rec[s + 1].xmu_ratio * eta1[u] : 0.0;
+                mu[u] = m;
+                double cc = rec[s].ag[0] * capd * m;
+                if (has1) cc += rec[s + 1].ag[1] * capd * eta1[u];
+                if (has2) cc += rec[s + 2].ag[2] * capd * eta2[u];
+                if (dr[0] >= 0) atomicAdd(lam + dr[0], cc);
+                if (dr[1] >= 0) atomicAdd(lam + dr[1], -cc);
+            }
             __syncthreads();
             cta_solve_transposed(tpd, lu_pool, v.lu, lam, w);
             // capacitor adjoints and dL/dC
@@ -310,13 +361,21 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
                 eta2[k] = eta1[k];
                 eta1[k] = e;
             }
+            for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+                const int32_t* dr = v.diodes + 4 * k;
+                const int32_t u = v.n_caps + k;
+                auto at = [&](const double* vec, int32_t i) { return i >= 0 ? vec[i] : 0.0; };
+                const double e = mu[u] - (at(lam, dr[0]) - at(lam, dr[1]));
+                eta2[u] = eta1[u];
+                eta1[u] = e;
+            }
             grad_contract(v, d, prog, lam, xs, g);
             __syncthreads();
         }
     }
 
     // ---- 4. the operating point: DC Jacobian, cotangent from steps 1 and 2
-    const double* x0 = rec_x0 + td.x0_off;
+    const double* x0 = ckpt;  // checkpoint 0 holds the re-solved x_0
     v.par = params_dc + d.param_off;
     load_constants(v, opt.gmin);
     vcopy(v.xold, x0, n);
@@ -351,6 +410,17 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         if (ad.n_steps >= 2) cc += rec[2].ag[2] * C * eta2[k];
         if (cr[0] >= 0) atomicAdd(lam + cr[0], cc);
         if (cr[1] >= 0) atomicAdd(lam + cr[1], -cc);
+    }
+    for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
+        const int32_t* dr = v.diodes + 4 * k;
+        const int32_t u = v.n_caps + k;
+        auto at = [&](const double* vec, int32_t i) { return i >= 0 ? vec[i] : 0.0; };
+        const double capd = diode_capd(v, k, at(x0, dr[0]) - at(x0, dr[1]), opt.gmin);
+        double cc = 0.0;
+        if (ad.n_steps >= 1) cc += rec[1].ag[1] * capd * eta1[u];
+        if (ad.n_steps >= 2) cc += rec[2].ag[2] * capd * eta2[u];
+        if (dr[0] >= 0) atomicAdd(lam + dr[0], cc);
+        if (dr[1] >= 0) atomicAdd(lam + dr[1], -cc);
     }
     __syncthreads();
     cta_solve_transposed(dpd, lu_pool, v.lu, lam, w);

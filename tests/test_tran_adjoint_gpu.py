@@ -1,6 +1,7 @@
 """GPU transient adjoint: gradients of a squared-error loss on the far-end
 voltage of an RC tree driven by a level-1 CMOS inverter, with respect to
-every R and C and the drivers' W, L and VTO, against central finite
+every R and C, the DC supply and the drivers' W, L and VTO (and on diode-RC
+transients with diode charge, every R and C), against central finite
 differences (h = 1e-6 relative) of the same discrete transient (the recorded
 timepoints and integration formulas, Newton to reltol 1e-9) to 1e-6
 relative, wherever the difference quotient resolves the gradient: the loss
@@ -58,6 +59,7 @@ def test_tran_adjoint_matches_central_differences():
         starts.append((d[0], at))
         at += sizes[d[0]]
     idx = [s for k, s in starts if k == "R"][:8] + [s for k, s in starts if k == "C"][:8]
+    idx += [s for k, s in starts if k in ("V", "I")]  # DC sources (VDD)
     for k, s in starts:
         if k == "M":
             idx += [s + 0, s + 1, s + 2]  # W, L, VTO
@@ -129,3 +131,56 @@ def test_tran_loss_autograd_function():
     assert torch.equal(p.grad, g * scale)
     assert float(p.grad.abs().sum()) > 0
     assert torch.equal(tran_loss(b, probes, tg, every=8), l_ref)
+
+
+@pytest.mark.parametrize("case", [0, 2, 3])
+def test_tran_adjoint_with_diode_charge(case):
+    """Diodes with depletion and transit-time charge (the reference's diode
+    transients: a half-wave rectifier into an RC load and seeded diode-RC
+    networks across the FC*VJ knee): gradients with respect to every R and C
+    against central differences of the same discrete transient, as above.
+    The loss of a replay through a strongly conducting diode with 5 ns
+    transit time carries the Newton tolerance of the replays (reltol 1e-9)
+    rather than only LU rounding: its central quotients move by a few 1e-6
+    between h = 1e-5 and 1e-7, so the floor here is 1e-10 L / (2h)."""
+    import pathlib
+    import golden_cases
+    g = golden_cases.load_transients(str(pathlib.Path(__file__).resolve().parent / "golden" /
+                                         "tran_diode.npz"))[case]
+    nl = g["netlist"]
+    probe = nl.num_nodes - 1
+    b = TranBatch([nl.build()], float(g["tstep"]), float(g["tstop"]),
+                  np.array([probe], np.int32), max_points=20000)
+    b.record(True)
+    b.run()
+    r = b.results()[0]
+    assert r["status"] == 0
+    tg = np.zeros(b.max_points)
+    v = r["values"][:, 0]
+    tg[:len(v)] = 0.97 * v + 0.01
+    tg = torch.from_numpy(tg).cuda()
+    b.set_adjoint_options(**TIGHT)
+    _, pdc, ptr = b.params()
+    grads, loss, st = b.adjoint([probe], tg, 1.0, 16)
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0 and float(loss[0]) > 0
+    grads = grads.cpu().numpy()
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 10, "M": 43}
+    idx, at = [], 0
+    for d in nl.devices:
+        if d[0] in ("R", "C"):
+            idx.append(at)
+        at += sizes[d[0]]
+    dev = lambda a: torch.from_numpy(a).cuda()
+    for i in idx:
+        h = abs(pdc[i]) * 1e-6
+        hi_dc, lo_dc, hi_tr, lo_tr = pdc.copy(), pdc.copy(), ptr.copy(), ptr.copy()
+        hi_dc[i] += h
+        hi_tr[i] += h
+        lo_dc[i] -= h
+        lo_tr[i] -= h
+        lp = loss_at(b, [probe], tg, dev(hi_dc), dev(hi_tr))[0]
+        lm = loss_at(b, [probe], tg, dev(lo_dc), dev(lo_tr))[0]
+        fd = (lp - lm) / (2 * h)
+        floor = 1e-10 * float(loss[0]) / (2 * h)
+        assert abs(grads[i] - fd) <= 1e-6 * abs(fd) + floor, (case, i, grads[i], fd, floor)
