@@ -83,6 +83,8 @@ def _args():
                     help="Monte Carlo instances of the BSIM4v7 ring + NAND transient (0 = skip)")
     ap.add_argument("--ac-points", type=int, default=1024,
                     help="frequency points of the batched AC sweep section (0 = skip)")
+    ap.add_argument("--row-maps", action="store_true",
+                    help="refactor destinations from per-warp row maps instead of the update maps")
     ap.add_argument("--ac-side", type=int, default=64,
                     help="side of the RC mesh of the AC sweep section")
     return ap.parse_args()
@@ -284,6 +286,8 @@ def run_ours(a, rank, world, local_rank):
     circuits = [m.build() for m in meshes]
     t1 = time.perf_counter()
     batch = DcBatch(circuits, symbolic=DcBatch.PER_PATTERN)
+    if a.row_maps:
+        batch.set_row_maps(True)
     t2 = time.perf_counter()
     params_h = torch.from_numpy(batch.params()).pin_memory()
     nsol = int(batch.solution_offsets[-1])

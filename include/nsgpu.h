@@ -450,6 +450,13 @@ int nsg_dc_batch_set_reorder(nsg_dc_batch* b, int enable);
  * the graph; it is captured again on a later run.  Results are those of a
  * plain launch, bit for bit. */
 int nsg_dc_batch_set_graph(nsg_dc_batch* b, int enable);
+/* Update destinations of the dataflow refactor: from the plans' update maps
+ * (enable 0, default) or from per-warp row -> position maps in a scratch of
+ * count x 16 x max_n int32 (enable != 0), which read L(:, r)'s row indices
+ * -- shared by every column that uses r -- instead of one map word per
+ * multiply-subtract.  Same values either way.  No counterpart in the
+ * reference. */
+int nsg_dc_batch_set_row_maps(nsg_dc_batch* b, int enable);
 /* Runs that replayed a graph so far. */
 int nsg_dc_batch_graph_launches(const nsg_dc_batch* b, long long* count);
 int nsg_dc_batch_reorders(const nsg_dc_batch* b, long long* count);

@@ -47,6 +47,7 @@ SIGNATURES = {
     "nsg_amd_order": (c_int, [c_int, P(c_int), P(c_int), P(c_int)]),
     "nsg_dc_batch_engines": (c_int, [c_void_p, P(c_int)]),
     "nsg_dc_batch_set_graph": (c_int, [c_void_p, c_int]),
+    "nsg_dc_batch_set_row_maps": (c_int, [c_void_p, c_int]),
     "nsg_dc_batch_graph_launches": (c_int, [c_void_p, P(c_ll)]),
     "nsg_batch_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_int, P(ctypes.c_float),
                                    P(c_int), c_void_p]),

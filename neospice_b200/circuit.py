@@ -302,6 +302,11 @@ class DcBatch:
         nsg_dc_batch_set_graph)."""
         L.check(L.lib().nsg_dc_batch_set_graph(self._h, int(bool(enable))))
 
+    def set_row_maps(self, enable: bool = True):
+        """Update destinations of the refactor from per-warp row maps
+        instead of the plans' update maps (nsg_dc_batch_set_row_maps)."""
+        L.check(L.lib().nsg_dc_batch_set_row_maps(self._h, int(bool(enable))))
+
     def graph_launches(self) -> int:
         n = ctypes.c_longlong()
         L.check(L.lib().nsg_dc_batch_graph_launches(self._h, ctypes.byref(n)))

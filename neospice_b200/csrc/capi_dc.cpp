@@ -19,7 +19,7 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params, double* work, double* solutions,
                              int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
-                             long long max_stage, cudaStream_t stream);
+                             long long max_stage, int32_t* rmaps, cudaStream_t stream);
 size_t dc_smem_bytes(int max_col, int max_n);
 cudaError_t launch_dc_adjoint(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
                               int count, const int32_t* prog, const double* params, double* work,
@@ -39,6 +39,9 @@ struct nsg_dc_batch {
     long long updates = 0, nnz_lu = 0, nnz = 0, n = 0;
     int max_col = 0, max_n = 0;
     nsg::NewtonOptions opt{1e-3, 1e-6, 1e-12, 1e-12, 0.0, 100, nsg::kAidDirect};
+    bool row_maps = false;        // nsg_dc_batch_set_row_maps
+    int32_t* d_rmap = nullptr;    // per-warp row -> position maps (count x warps x max_n)
+    int64_t rmap_cap = 0;
     int32_t* d_lu_pool = nullptr;
     nsg::PlanDesc* d_plans = nullptr;
     int32_t* d_prog = nullptr;
@@ -68,6 +71,7 @@ struct nsg_dc_batch {
     ~nsg_dc_batch() {
         drop_graph();
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        cudaFree(d_rmap);
         cudaFree(d_lu_pool);
         cudaFree(d_plans);
         cudaFree(d_prog);
@@ -645,6 +649,13 @@ int nsg_dc_batch_set_graph(nsg_dc_batch* b, int enable) {
     });
 }
 
+int nsg_dc_batch_set_row_maps(nsg_dc_batch* b, int enable) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_dc_batch_set_row_maps: null batch");
+    b->row_maps = enable != 0;
+    b->drop_graph();
+    return NSG_OK;
+}
+
 int nsg_dc_batch_graph_launches(const nsg_dc_batch* b, long long* count) {
     if (!b || !count) return fail(NSG_ERR_INVALID, "nsg_dc_batch_graph_launches: null argument");
     *count = b->graph_launches;
@@ -701,13 +712,28 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
             return fail(NSG_ERR_INVALID, "nsg_dc_batch_run: null argument");
         const cudaStream_t st = static_cast<cudaStream_t>(stream);
         const double* params = d_params ? d_params : b->d_params;
+        if (b->row_maps) {
+            // warps per CTA of newton_dc_kernel (16), max_n words each
+            const int64_t words = int64_t{b->count} * 16 * b->max_n;
+            if (words > b->rmap_cap) {
+                b->drop_graph();
+                cudaFree(b->d_rmap);
+                b->d_rmap = nullptr;
+                b->rmap_cap = 0;
+                const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_rmap),
+                                                 sizeof(int32_t) * static_cast<size_t>(words));
+                if (e != cudaSuccess) return cuda_fail("nsg_dc_batch_run", e);
+                b->rmap_cap = words;
+            }
+        }
+        int32_t* rmaps = b->row_maps ? b->d_rmap : nullptr;
         auto first_launch = [&](cudaStream_t s) -> cudaError_t {
             cudaError_t r = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::DcCtl) * b->count, s);
             if (r == cudaSuccess)
                 r = nsg::launch_newton_dc(b->d_plans, b->d_lu_pool, b->d_descs, nullptr, b->count,
                                           b->d_prog, params, b->d_work, d_solutions, d_status,
                                           d_iterations, b->d_ctl, b->opt, b->max_col, b->max_n,
-                                          max_stage_len(b->descs), s);
+                                          max_stage_len(b->descs), rmaps, s);
             return r;
         };
         cudaError_t e = cudaSuccess;
@@ -790,7 +816,7 @@ int nsg_dc_batch_run(nsg_dc_batch* b, const double* d_params, double* d_solution
                                            static_cast<int>(subset.size()), b->d_prog, params,
                                            b->d_work, d_solutions, d_status, d_iterations,
                                            b->d_ctl, b->opt, b->max_col, b->max_n,
-                                           max_stage_len(b->descs), st)) !=
+                                           max_stage_len(b->descs), rmaps, st)) !=
                     cudaSuccess)
                 return cuda_fail("nsg_dc_batch_run", e);
         }

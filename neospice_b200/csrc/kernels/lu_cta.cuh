@@ -194,9 +194,11 @@ __device__ __forceinline__ double lu_peer(const double* p) {
 // after column r is done, judges the pivot (check_pivots, kCheck*), and
 // writes the column (and its row-major copies) to lu.  Ends with
 // __syncwarp(); the caller publishes completion.  The position in column j
-// of each row of L(:, r) comes from the plan's update map, or, for plans
-// without one (pd.has_map == 0), from rmap: this warp's row -> position
-// scratch (pd.n words), written for column j's rows first.
+// of each row of L(:, r) comes from the plan's update map, or, when rmap is
+// given (always for plans without a map, pd.has_map == 0), from rmap: this
+// warp's row -> position scratch (pd.n words), written for column j's rows
+// first.  The row map reads L(:, r)'s row indices, which every consumer
+// column of r shares, instead of a map entry per update.
 template <bool kCrossSm, class Probe>
 __device__ __forceinline__ ColumnResult refactor_column(
     const PlanDesc& pd, const int32_t* __restrict__ pool, const double* __restrict__ a,
@@ -217,7 +219,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
     const int32_t dj = diag_pos[j] - c0;
     const int32_t gp = amd ? gmin_pos[j] : dj;
     const int32_t* row_idx = pool + pd.off[PA_row_idx];
-    const bool mapped = pd.has_map != 0;
+    const bool mapped = rmap == nullptr;
     for (int32_t t = lane; t < len; t += 32) {
         const int32_t s = lu_src[c0 + t];
         double v = (s >= 0) ? a[s] : 0.0;
@@ -377,13 +379,16 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
                                                    double diag_gmin, int check_pivots,
                                                    double rel_threshold, double* smem, int colbuf,
                                                    double* __restrict__ lrows = nullptr,
-                                                   double* __restrict__ urows = nullptr) {
+                                                   double* __restrict__ urows = nullptr,
+                                                   int32_t* rmaps = nullptr,
+                                                   int64_t rmap_stride = 0) {
     const int32_t n = pd.n;
     const bool amd = pd.kind == kPlanAmdLu;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     double* buf = smem + warp * colbuf;
     volatile int32_t* done = reinterpret_cast<volatile int32_t*>(smem + kFlowWarps * colbuf);
+    int32_t* rmap = rmaps ? rmaps + warp * rmap_stride : nullptr;
 
     __shared__ int32_t s_next, s_timeout, s_growth;
     __shared__ unsigned long long s_fail;
@@ -404,7 +409,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_flow(const PlanDesc& 
         if (j >= n) break;
         const ColumnResult c = refactor_column<false>(
             pd, pool, a, lu, diag_gmin, check_pivots, rel_threshold, j, buf, lrows, urows,
-            [&](int32_t r) { return flag_acquire(done + r); });
+            [&](int32_t r) { return flag_acquire(done + r); }, rmap);
         if (lane == 0) {
             if (c.timed_out) s_timeout = 1;
             else if (c.code != kStatusOk) atomicMin(&s_fail, fail_key(j, c.code));

@@ -51,6 +51,8 @@ struct Inst {
     double* st[4];          // device state ring state0..state3
     double* mrec;           // per-MOSFET load values (kMosRecCount each)
     int32_t n, num_nodes, nnz, n_const, n_diodes, n_caps, n_srcs, n_mos;
+    int32_t* rmaps = nullptr;  // optional row -> position maps of the CTA's warps
+    int64_t rmap_stride = 0;   // words per warp
 };
 
 // Address of workspace offset `off`: in the shared-memory stage when the
@@ -455,7 +457,7 @@ __device__ inline NewtonOutcome newton(const Inst& v, const PlanDesc& pd, const 
         const RefactorResult fr =
             small ? cta_refactor_small(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, lu_s)
                   : cta_refactor_flow(pd, lu_pool, v.a, v.lu, opt.diag_gmin, check, 1e-3, smem,
-                                      colbuf, v.lrows, v.urows);
+                                      colbuf, v.lrows, v.urows, v.rmaps, v.rmap_stride);
         if (fr.code == kStatusTimeout) {
             out = {kStatusTimeout, iter + 1, -1, 0, 1};
             break;

@@ -23,7 +23,7 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
                  double* __restrict__ work, double* __restrict__ solutions,
                  int32_t* __restrict__ status, int32_t* __restrict__ iterations,
                  DcCtl* __restrict__ ctls, NewtonOptions opt, int colbuf, int scratch_doubles,
-                 int stage_doubles, int plan_words) {
+                 int stage_doubles, int plan_words, int32_t* rmaps, int64_t rmap_stride) {
     extern __shared__ double smem[];
     const DcDesc d = descs[subset ? subset[blockIdx.x] : blockIdx.x];
     __shared__ PlanDesc s_pd;
@@ -37,7 +37,12 @@ newton_dc_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__
     // Per-thread views (not a shared copy as in the transient kernel): the
     // dataflow scratch of large meshes fills the shared memory of two CTAs
     // per SM to within a few hundred bytes.
-    const Inst v = make_inst(d, prog, params, work, stage);
+    Inst v = make_inst(d, prog, params, work, stage);
+    static_assert(kFlowWarps == 16, "the host sizes the row maps for 16 warps per CTA");
+    if (rmaps) {
+        v.rmaps = rmaps + static_cast<int64_t>(blockIdx.x) * kFlowWarps * rmap_stride;
+        v.rmap_stride = rmap_stride;
+    }
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
     __shared__ int32_t s_fresh;
@@ -86,7 +91,7 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                              const double* params, double* work, double* solutions,
                              int32_t* status, int32_t* iterations, DcCtl* ctls,
                              const NewtonOptions& opt, int max_col, int max_n,
-                             long long max_stage, cudaStream_t stream) {
+                             long long max_stage, int32_t* rmaps, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (max_col + 31) & ~31;
     const size_t scratch = (dc_smem_bytes(max_col, max_n) + 15) & ~size_t{15};
@@ -107,7 +112,8 @@ cudaError_t launch_newton_dc(const PlanDesc* plans, const int32_t* lu_pool, cons
                                                              iterations, ctls, opt, colbuf,
                                                              static_cast<int>(scratch / sizeof(double)),
                                                              static_cast<int>(stage / sizeof(double)),
-                                                             static_cast<int>(plan / sizeof(int32_t)));
+                                                             static_cast<int>(plan / sizeof(int32_t)),
+                                                             rmaps, max_n);
     return cudaGetLastError();
 }
 

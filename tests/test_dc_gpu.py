@@ -88,3 +88,24 @@ def test_dc_graph_replay_matches_plain_launch():
         torch.cuda.synchronize()
         assert torch.equal(sol, s0) and torch.equal(st, st0) and torch.equal(it, it0)
     assert batch.graph_launches() == 2
+
+
+def test_dc_row_maps_bitwise():
+    """Update destinations from per-warp row maps instead of the plans'
+    update maps: identical solutions, statuses and iteration counts on the
+    golden meshes, MOS circuits and AMD-LU-sized linear grids, and through a
+    captured graph."""
+    nets = [g["mesh"].build for g in MESHES] + [g["netlist"].build for g in golden_cases.load_mos_dc()]
+    nets += [workloads.power_grid(np.random.default_rng([33, k]), 24, 8, 10).build for k in range(2)]
+    base = DcBatch([f() for f in nets])
+    s0, st0, it0 = base.run()
+    torch.cuda.synchronize()
+    rows = DcBatch([f() for f in nets])
+    rows.set_row_maps(True)
+    for graph in (False, True):
+        rows.set_graph(graph)
+        for _ in range(2):
+            s1, st1, it1 = rows.run()
+            torch.cuda.synchronize()
+            assert torch.equal(st1, st0) and torch.equal(it1, it0)
+            assert torch.equal(s1, s0)
