@@ -521,6 +521,13 @@ def plain_dc(meshes, k, batched_value):
 
 INV_PULSE = (0.0, 1.8, 0.0, 1e-10, 1e-10, 1e-9, 2e-9)
 
+# FP64 operations per Newton iteration of one instance of the BSIM4v7 ring +
+# NAND circuit (DADD + DMUL + 2 DFMA thread instructions of the transient
+# kernel counted by ncu over every launch of 592 instances, .tran 1p 0.2n,
+# divided by their 275,593 Newton iterations), and B200's nominal FP64 rate.
+B4_FLOPS_PER_ITER = 6.41e5
+FP64_NOMINAL_FLOPS = 37e12
+
 
 def _tran_parity(ours, ref):
     """Timepoints, voltages and Newton iterations of one of our transients
@@ -664,7 +671,14 @@ def bsim4_mc_transient(count, pool=None, parity_instances=4, tstep=1e-12, tstop=
                     "setup_s": round(t_setup, 3),
                     "points_mean": float(np.mean([len(r["time"]) for r in res])),
                     "newton_iters_mean": float(iters.mean()),
-                    "device_loads_per_s": round(200.0 * float(iters.sum()) / t_batch, 1)},
+                    "device_loads_per_s": round(200.0 * float(iters.sum()) / t_batch, 1),
+                    "fp64_gflops": round(B4_FLOPS_PER_ITER * float(iters.sum()) / t_batch / 1e9, 1),
+                    "fp64_frac_of_nominal": round(B4_FLOPS_PER_ITER * float(iters.sum()) / t_batch
+                                                  / FP64_NOMINAL_FLOPS, 4),
+                    "fp64_note": "FP64 operations per Newton iteration of this circuit (DADD + "
+                                 "DMUL + 2 DFMA thread instructions counted by ncu on 592 "
+                                 "instances, .tran 1p 0.2n: 6.41e5) x iterations / time; peak = "
+                                 "nominal 37 TFLOP/s (no measured FP64 peak)"},
         "plain": {"value": round(1.0 / t_plain, 4), "unit": "circuit-solves/s",
                   "seconds_per_solve": round(t_plain, 4)},
         "batched_over_plain": round((count / t_batch) * t_plain, 2),
