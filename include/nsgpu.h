@@ -506,6 +506,13 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
                           int max_points, int nprobe, const int* probes, int threads,
                           nsg_tran_batch** out);
 void nsg_tran_batch_free(nsg_tran_batch* b);
+/* Launch shape of the transient kernel: threads per CTA (128, 256 or 512)
+ * and CTAs per SM (128: 8; 256: 4; 512: 2; 0 = that default), or 0, 0 for
+ * the automatic choice (512 for a few hundred instances or any instance
+ * above 128 unknowns; else 128 or 256, enough for one pass of the device
+ * loads).  Tuning only: the shapes give the same results.  No counterpart
+ * in the reference. */
+int nsg_tran_batch_set_shape(nsg_tran_batch* b, int threads, int blocks_per_sm);
 /* Run the whole batch on a stream.  Instances stop for the host when a
  * solver needs ordering -- the transient solver on the first transient
  * iteration's matrix as the device computes it, either solver after a failed

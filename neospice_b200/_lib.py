@@ -131,6 +131,7 @@ SIGNATURES = {
     "nsg_tran_batch_free": (None, [c_void_p]),
     "nsg_tran_batch_orderings": (c_int, [c_void_p, P(c_ll)]),
     "nsg_tran_batch_run": (c_int, [c_void_p, c_void_p]),
+    "nsg_tran_batch_set_shape": (c_int, [c_void_p, c_int, c_int]),
     "nsg_tran_batch_record": (c_int, [c_void_p, c_int]),
     "nsg_tran_batch_set_adjoint_options": (c_int, [c_void_p, c_double, c_double, c_double, c_int]),
     "nsg_tran_batch_params": (c_int, [c_void_p, P(c_ll), P(c_double), P(c_double)]),

@@ -396,6 +396,11 @@ class TranBatch:
     def count(self):
         return len(self.circuits)
 
+    def set_shape(self, threads: int = 0, blocks_per_sm: int = 0):
+        """Launch shape of the transient kernel (nsg_tran_batch_set_shape;
+        0, 0: automatic)."""
+        L.check(L.lib().nsg_tran_batch_set_shape(self._h, int(threads), int(blocks_per_sm)))
+
     def run(self, stream=None):
         import torch
         sp = torch.cuda.current_stream().cuda_stream if stream is None else \

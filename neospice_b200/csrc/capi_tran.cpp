@@ -47,6 +47,7 @@ struct nsg_tran_batch {
     std::vector<std::vector<int32_t>> col_ptr, row_idx;  // per-instance pattern
     std::vector<int> solver;  // per-instance engine (NSG_SOLVER_*), as make_solver picks it
     int max_col = 0, max_n = 0;
+    int force_threads = 0, force_blocks = 0;  // nsg_tran_batch_set_shape
     int64_t work_size = 0, work_cap = 0;
     long long orderings = 0;
     int32_t* d_lu_pool = nullptr;
@@ -101,7 +102,8 @@ namespace {
 
 // Launch shape of a transient batch (nsg::TranShape).
 nsg::TranShape tran_shape(const nsg_tran_batch& b) {
-    nsg::TranShape sh{b.max_col, b.max_n, max_stage_len(b.descs), 0, 0, 0};
+    nsg::TranShape sh{b.max_col, b.max_n, max_stage_len(b.descs), 0, 0, 0,
+                      b.force_threads, b.force_blocks};
     for (const auto& t : b.topos) {
         sh.max_small_lu = std::max(sh.max_small_lu, t->plan.nnz_lu + t->plan.n);
         sh.max_plan_words = std::max<int64_t>(sh.max_plan_words, t->plan.device_words());
@@ -303,6 +305,21 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
 }
 
 void nsg_tran_batch_free(nsg_tran_batch* b) { delete b; }
+
+int nsg_tran_batch_set_shape(nsg_tran_batch* b, int threads, int blocks_per_sm) {
+    if (!b) return fail(NSG_ERR_INVALID, "nsg_tran_batch_set_shape: null batch");
+    const bool ok = (threads == 0 && blocks_per_sm == 0) ||
+                    (threads == 128 && (blocks_per_sm == 0 || blocks_per_sm == 8)) ||
+                    (threads == 256 && (blocks_per_sm == 0 || blocks_per_sm == 4)) ||
+                    (threads == 512 && (blocks_per_sm == 0 || blocks_per_sm == 2));
+    if (!ok) return fail(NSG_ERR_INVALID, "nsg_tran_batch_set_shape: unsupported shape");
+    if (threads != 0 && threads != 512 && b->max_n > 128)
+        return fail(NSG_ERR_INVALID, "nsg_tran_batch_set_shape: instances above 128 unknowns "
+                                     "need 512-thread CTAs");
+    b->force_threads = threads;
+    b->force_blocks = blocks_per_sm;
+    return NSG_OK;
+}
 
 int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
     return guarded("nsg_tran_batch_run", [&]() -> int {

@@ -68,6 +68,8 @@ struct TranShape {
     int32_t max_small_lu;
     int64_t max_plan_words;
     int32_t max_devices;
+    int32_t force_threads;   // nsg_tran_batch_set_shape (0: automatic)
+    int32_t force_blocks;
 };
 
 // Per-instance transient status.

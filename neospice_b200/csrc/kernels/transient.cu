@@ -185,10 +185,11 @@ __device__ inline void finish(const DcDesc& d, double* work, double* stage, Tran
 
 }  // namespace
 
-// One CTA of kThreads threads per instance (1024 / kThreads CTAs per SM at
-// 64 registers).  subset (optional): descriptor positions to run.
-template <int kThreads>
-__global__ void __launch_bounds__(kThreads, 1024 / kThreads)
+// One CTA of kThreads threads per instance, kBlocks CTAs per SM (registers
+// capped at 65536 / (kThreads * kBlocks)).  subset (optional): descriptor
+// positions to run.
+template <int kThreads, int kBlocks>
+__global__ void __launch_bounds__(kThreads, kBlocks)
 transient_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ lu_pool,
                  const DcDesc* __restrict__ descs, const TranDesc* __restrict__ tdescs,
                  const int32_t* __restrict__ subset, const int32_t* __restrict__ prog,
@@ -515,11 +516,11 @@ size_t tran_smem_bytes(int max_col, int max_n) {
 
 namespace {
 
-template <int kThreads>
+template <int kThreads, int kBlocks>
 cudaError_t configure_transient() {
     static bool configured = false;
     if (configured) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(transient_kernel<kThreads>,
+    cudaError_t e = cudaFuncSetAttribute(transient_kernel<kThreads, kBlocks>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     if (e == cudaSuccess) configured = true;
     return e;
@@ -545,7 +546,10 @@ int sm_count() {
 // CTAs per SM can hold at once, throughput is the cost: CTAs of 128 or 256
 // threads (as many as the instances' largest device family needs for one
 // pass of the device loads), eight or four per SM, with the LU and the plan
-// in shared memory and the workspace staged only where it fits.
+// in shared memory and the workspace staged only where it fits.  (Two
+// 256-thread CTAs per SM at 128 registers spill less in the BSIM4v7 loads
+// but ran 20 % slower than four at 64 on the ring + NAND Monte Carlo.)
+// sh.force_threads / force_blocks (0: automatic) override the choice.
 cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, const DcDesc* descs,
                              const TranDesc* tdescs, const int32_t* subset, int count,
                              const int32_t* prog, const double* params_dc,
@@ -556,19 +560,26 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
                              StepRecord* rec_steps, double* rec_x0, cudaStream_t stream) {
     if (count <= 0) return cudaSuccess;
     const int colbuf = (sh.max_col + 31) & ~31;
-    int threads = kFlowThreads;
-    if (sh.max_n <= 128 && count > 2 * sm_count())
+    int threads = kFlowThreads, blocks = 2;
+    if (sh.max_n <= 128 && count > 2 * sm_count()) {
         threads = sh.max_devices <= 128 ? 128 : (sh.max_devices <= 256 ? 256 : kFlowThreads);
+        blocks = threads == 128 ? 8 : (threads == 256 ? 4 : 2);
+    }
+    if (sh.force_threads > 0) {
+        threads = sh.force_threads;
+        blocks = sh.force_blocks > 0 ? sh.force_blocks : 1024 / threads;
+    }
+    const bool small_shape = threads != kFlowThreads;
+    if (small_shape && sh.max_n > 128) return cudaErrorInvalidValue;
     size_t scratch, plan, stage;
-    if (threads == kFlowThreads) {
+    if (!small_shape) {
         scratch = (tran_smem_bytes(sh.max_col, sh.max_n) + 15) & ~size_t{15};
         plan = (sh.max_n <= 128) ? kPlanStageBytes : 0;
         stage = stage_bytes_for(scratch + plan, sh.max_stage);
     } else {
         // Per-CTA share of the SM's 228 KB, less the CTA's static shared
         // memory and the 1 KB the runtime reserves per CTA.
-        const size_t blocks = 1024 / threads;
-        const size_t budget = (228 * 1024) / blocks - 3 * 1024;
+        const size_t budget = (228 * 1024) / static_cast<size_t>(blocks) - 3 * 1024;
         scratch = (sizeof(double) * static_cast<size_t>(sh.max_small_lu) + 15) & ~size_t{15};
         plan = (sh.max_plan_words * 4 <= static_cast<int64_t>(kPlanStageBytes))
                    ? ((static_cast<size_t>(sh.max_plan_words) * 4 + 15) & ~size_t{15})
@@ -583,18 +594,20 @@ cudaError_t launch_transient(const PlanDesc* plans, const int32_t* lu_pool, cons
     const int stage_d = static_cast<int>(stage / sizeof(double));
     const int plan_w = static_cast<int>(plan / sizeof(int32_t));
     cudaError_t e;
-#define NSG_LAUNCH_TRAN(T)                                                                     \
-    if ((e = configure_transient<T>()) != cudaSuccess) return e;                               \
-    transient_kernel<T><<<count, T, smem, stream>>>(                                           \
+#define NSG_LAUNCH_TRAN(T, B)                                                                  \
+    if ((e = configure_transient<T, B>()) != cudaSuccess) return e;                            \
+    transient_kernel<T, B><<<count, T, smem, stream>>>(                                        \
         plans, lu_pool, descs, tdescs, subset, prog, params_dc, params_tran, work, bps, probes, \
         times, values, npoints, status, stats, ctls, o, colbuf, scratch_d, stage_d, rec_steps,  \
         rec_x0, plan_w);
-    if (threads == 128) {
-        NSG_LAUNCH_TRAN(128)
-    } else if (threads == 256) {
-        NSG_LAUNCH_TRAN(256)
+    if (threads == 128 && blocks == 8) {
+        NSG_LAUNCH_TRAN(128, 8)
+    } else if (threads == 256 && blocks == 4) {
+        NSG_LAUNCH_TRAN(256, 4)
+    } else if (threads == kFlowThreads && blocks == 2) {
+        NSG_LAUNCH_TRAN(kFlowThreads, 2)
     } else {
-        NSG_LAUNCH_TRAN(kFlowThreads)
+        return cudaErrorInvalidValue;
     }
 #undef NSG_LAUNCH_TRAN
     return cudaGetLastError();

@@ -68,3 +68,28 @@ def test_large_bsim4_batch_equals_single_instance():
         np.testing.assert_array_equal(r["time"], r1["time"])
         np.testing.assert_array_equal(r["values"], r1["values"])
         assert r["newton_iters"] == r1["newton_iters"]
+
+
+def test_forced_shapes_identical():
+    """nsg_tran_batch_set_shape: every supported shape gives the automatic
+    shape's results bit for bit; unsupported shapes are refused."""
+    from neospice_b200 import _lib as L
+    cases = golden_cases.load_transients()
+    (tstep, tstop), ks = next(iter(_groups(cases).items()))
+    nmin = min(cases[k]["netlist"].num_nodes for k in ks)
+    args = (tstep, tstop, np.arange(nmin, dtype=np.int32))
+    mp = max(len(cases[k]["times"]) for k in ks) + 8
+    out = []
+    for shape in ((0, 0), (128, 8), (256, 4), (512, 2)):
+        b = TranBatch([cases[k]["netlist"].build() for k in ks], *args, max_points=mp)
+        b.set_shape(*shape)
+        b.run()
+        out.append([(r["time"], r["values"], r["newton_iters"]) for r in b.results()])
+    for other in out[1:]:
+        for (t0, v0, i0), (t1, v1, i1) in zip(out[0], other):
+            np.testing.assert_array_equal(t1, t0)
+            np.testing.assert_array_equal(v1, v0)
+            assert i1 == i0
+    b = TranBatch([cases[ks[0]]["netlist"].build()], *args, max_points=mp)
+    with pytest.raises(L.NsgError):
+        b.set_shape(256, 2)
