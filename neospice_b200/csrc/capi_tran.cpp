@@ -48,6 +48,12 @@ struct nsg_tran_batch {
     std::vector<int> solver;  // per-instance engine (NSG_SOLVER_*), as make_solver picks it
     int max_col = 0, max_n = 0;
     int force_threads = 0, force_blocks = 0;  // nsg_tran_batch_set_shape
+    // Descriptors and workspace size as created: every run starts from them
+    // (the DC plan ordered on the first DC matrix, no transient plan yet),
+    // as the reference's solve_transient starts from fresh solvers.
+    std::vector<nsg::DcDesc> descs0;
+    std::vector<nsg::TranDesc> tdescs0;
+    int64_t work_size0 = 0;
     int64_t work_size = 0, work_cap = 0;
     long long orderings = 0;
     int32_t* d_lu_pool = nullptr;
@@ -274,6 +280,9 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
             b->row_idx.push_back(c.row_idx());
         }
         b->work_size = b->work_cap = work;
+        b->descs0 = b->descs;
+        b->tdescs0 = b->tdescs;
+        b->work_size0 = work;
         const size_t smem = nsg::tran_smem_bytes(b->max_col, b->max_n);
         if (smem > 200 * 1024)
             return fail(NSG_ERR_INVALID, "nsg_tran_batch_create: instance too large for the "
@@ -335,7 +344,20 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                                          b->record ? b->d_x0 : nullptr, st);
         };
         b->recorded = false;
-        cudaError_t e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::TranCtl) * b->count, st);
+        // Start from the batch as created: the plans and LU regions a
+        // previous run's re-orderings placed are not this run's (a reused
+        // transient plan would also hand the DC phase an LU region sized for
+        // another plan).
+        b->descs = b->descs0;
+        b->tdescs = b->tdescs0;
+        b->work_size = b->work_size0;
+        cudaError_t e = cudaMemcpy(b->d_descs, b->descs.data(), sizeof(nsg::DcDesc) * b->count,
+                                   cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_tdescs, b->tdescs.data(), sizeof(nsg::TranDesc) * b->count,
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(b->d_ctl, 0, sizeof(nsg::TranCtl) * b->count, st);
         if (e == cudaSuccess) e = launch(nullptr, b->count);
         if (e != cudaSuccess) return cuda_fail("nsg_tran_batch_run", e);
         // Instances stop for the host when a solver needs its first ordering
