@@ -30,6 +30,16 @@
 // keeps them in one matrix; an AC sweep never interleaves them).  A singular
 // first complex matrix, which NeoSolver::numeric_complex does not report,
 // leaves no factorization here: solve_complex then throws.
+//   set_equilibrate(on)             NeoSolver's row/column equilibration
+//                                   (neo_solver.cpp:57-102, 148-226): numeric()
+//                                   and refactorize() factor D_r A D_c (radix-2
+//                                   scale factors from the values, diag_gmin
+//                                   scaled onto each diagonal), solve() scales
+//                                   b by D_r and the result by D_c.  Like the
+//                                   reference, only the Markowitz engine honors
+//                                   it (AmdLuSolver and the auto-fallback
+//                                   wrapper ignore the toggle).
+//
 // Misuse throws std::logic_error, a size mismatch std::invalid_argument, a
 // CUDA or allocation failure std::runtime_error -- as NeoSolver does.
 #pragma once
@@ -37,6 +47,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -65,14 +77,21 @@ public:
         n_ = n;
         col_ptr_ = col_ptr;
         row_idx_ = row_idx;
+        col_of_.resize(row_idx.size());
+        for (int j = 0; j < n; ++j)
+            for (int k = col_ptr[j]; k < col_ptr[j + 1]; ++k) col_of_[k] = j;
         symbolized_ = true;
         numeric_called_ = false;
         factored_ = false;
     }
 
-    bool numeric(const std::vector<double>& values, double diag_gmin = 0.0) {
+    void set_equilibrate(bool on) { equilibrate_ = on && engine_ == NSG_SOLVER_MARKOWITZ; }
+
+    bool numeric(const std::vector<double>& values_in, double diag_gmin = 0.0) {
         require_symbolic("numeric");
-        check_values(values);
+        check_values(values_in);
+        const std::vector<double>& values = equilibrate_ ? scaled(values_in, diag_gmin) : values_in;
+        if (equilibrate_) diag_gmin = 0.0;  // already on the scaled diagonal
         numeric_called_ = true;
         if (!topo_) {
             nsg_topology* t = nullptr;
@@ -100,12 +119,14 @@ public:
         return !factored_;
     }
 
-    bool refactorize(const std::vector<double>& values, double diag_gmin = 0.0) {
+    bool refactorize(const std::vector<double>& values_in, double diag_gmin = 0.0) {
         require_symbolic("refactorize");
         if (!numeric_called_)
             throw std::logic_error("GpuSolver::refactorize: numeric() not called");
         if (!topo_) return true;  // the first numeric() found the matrix singular
-        check_values(values);
+        check_values(values_in);
+        const std::vector<double>& values = equilibrate_ ? scaled(values_in, diag_gmin) : values_in;
+        if (equilibrate_) diag_gmin = 0.0;
         upload(values);
         int st = gpu_refactor(diag_gmin, 0);
         if (st == NSG_REORDER) {
@@ -126,8 +147,23 @@ public:
         return !factored_;
     }
 
-    void solve(std::vector<double>& rhs) { sweep(rhs, false); }
-    void solve_transposed(std::vector<double>& rhs) { sweep(rhs, true); }
+    void solve(std::vector<double>& rhs) {
+        if (!equilibrate_) {
+            sweep(rhs, false);
+            return;
+        }
+        // (D_r A D_c) y = D_r b, then x = D_c y
+        if (static_cast<int>(rhs.size()) != n_)
+            throw std::invalid_argument("GpuSolver::solve: rhs size mismatch");
+        for (int i = 0; i < n_; ++i) rhs[i] = dr_[i] * rhs[i];
+        sweep(rhs, false);
+        for (int i = 0; i < n_; ++i) rhs[i] = dc_[i] * rhs[i];
+    }
+    void solve_transposed(std::vector<double>& rhs) {
+        if (equilibrate_)
+            throw std::logic_error("GpuSolver::solve_transposed: not defined with equilibration");
+        sweep(rhs, true);
+    }
 
     void numeric_complex(const std::vector<double>& ax) {
         require_symbolic("numeric_complex");
@@ -179,6 +215,9 @@ public:
 private:
     int engine_ = NSG_SOLVER_MARKOWITZ;
     int n_ = 0;
+    bool equilibrate_ = false;
+    std::vector<int> col_of_;           // column of each CSC slot
+    std::vector<double> dr_, dc_, scaled_;  // scale factors and D_r A D_c
     bool symbolized_ = false;
     bool numeric_called_ = false;  // NeoSolver's factored_ flag
     bool factored_ = false;        // the last factorization succeeded
@@ -216,6 +255,49 @@ private:
     void check_values(const std::vector<double>& v) const {
         if (static_cast<int>(v.size()) != nnz())
             throw std::invalid_argument("GpuSolver: values size mismatch");
+    }
+    // The nearest power of two to v in log2 (the boundary is v = 2^k *
+    // sqrt(2)/2 below 2^k): scaling by it only moves exponents.  1 for
+    // zero, negative or non-finite v.
+    static double nearest_pow2(double v) {
+        if (!(v > 0.0) || !std::isfinite(v)) return 1.0;
+        int e = 0;
+        const double m = std::frexp(v, &e);  // v = m * 2^e, m in [0.5, 1)
+        return std::ldexp(1.0, m < 0.70710678118654752440 ? e - 1 : e);
+    }
+    // D_r A D_c with diag_gmin * D_r[i] * D_c[i] added to each diagonal slot:
+    // row infinity norms, column norms of the row-scaled matrix, then one
+    // refining row pass on the fully scaled one, each rounded to powers of two.
+    const std::vector<double>& scaled(const std::vector<double>& a, double diag_gmin) {
+        const int nz = nnz();
+        dr_.assign(n_, 1.0);
+        dc_.assign(n_, 1.0);
+        std::vector<double> mx(n_, 0.0);
+        for (int k = 0; k < nz; ++k) {
+            const double v = std::abs(a[k]);
+            if (v > mx[row_idx_[k]]) mx[row_idx_[k]] = v;
+        }
+        for (int i = 0; i < n_; ++i) dr_[i] = nearest_pow2(mx[i] > 0.0 ? 1.0 / mx[i] : 1.0);
+        std::fill(mx.begin(), mx.end(), 0.0);
+        for (int k = 0; k < nz; ++k) {
+            const double v = std::abs(dr_[row_idx_[k]] * a[k]);
+            if (v > mx[col_of_[k]]) mx[col_of_[k]] = v;
+        }
+        for (int j = 0; j < n_; ++j) dc_[j] = nearest_pow2(mx[j] > 0.0 ? 1.0 / mx[j] : 1.0);
+        std::fill(mx.begin(), mx.end(), 0.0);
+        for (int k = 0; k < nz; ++k) {
+            const double v = std::abs(dr_[row_idx_[k]] * a[k] * dc_[col_of_[k]]);
+            if (v > mx[row_idx_[k]]) mx[row_idx_[k]] = v;
+        }
+        for (int i = 0; i < n_; ++i)
+            if (mx[i] > 0.0) dr_[i] *= nearest_pow2(1.0 / mx[i]);
+        scaled_.resize(nz);
+        for (int k = 0; k < nz; ++k) scaled_[k] = dr_[row_idx_[k]] * a[k] * dc_[col_of_[k]];
+        if (diag_gmin != 0.0)
+            for (int k = 0; k < nz; ++k)
+                if (row_idx_[k] == col_of_[k])
+                    scaled_[k] += dr_[row_idx_[k]] * dc_[row_idx_[k]] * diag_gmin;
+        return scaled_;
     }
     void check_complex_values(const std::vector<double>& ax) const {
         if (static_cast<int>(ax.size()) != 2 * nnz())

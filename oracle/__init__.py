@@ -91,8 +91,35 @@ def seam() -> ctypes.CDLL:
         lib.nsseam_use_gpu.argtypes = [_I]
         lib.nsseam_gpu_solvers.restype = ctypes.c_longlong
         lib.nsseam_ac_sweep.argtypes = [_I, _I, _V, _V, _V, _V, _V, _I, _V, _V, _V]
+        lib.nsseam_solve_sequence.argtypes = [_I, _I, _V, _V, _V, _V, _I, _D, _I, _I, _V, _V]
         _seam = lib
     return _seam
+
+
+def seam_solve_sequence(n, col_ptr, row_idx, values_seq, rhs, gpu: bool, equilibrate=True,
+                        diag_gmin=0.0, is_linear=False):
+    """numeric() then refactorize() on each value vector of values_seq, each
+    followed by solve(rhs), through make_solver's ISolver: the reference's
+    (gpu=False) or the GPU adapter (gpu=True).  Returns ((points, n)
+    solutions, per-point singular flags)."""
+    lib = seam()
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_idx, np.int32)
+    vals = np.ascontiguousarray(values_seq, np.float64)
+    b = np.ascontiguousarray(rhs, np.float64)
+    pts = vals.shape[0]
+    out = np.zeros((pts, n))
+    sing = np.zeros(pts, np.int32)
+    lib.nsseam_use_gpu(1 if gpu else 0)
+    try:
+        rc = lib.nsseam_solve_sequence(int(n), len(ri), _p(cp), _p(ri), _p(vals), _p(b), pts,
+                                       float(diag_gmin), int(bool(equilibrate)),
+                                       int(bool(is_linear)), _p(out), _p(sing))
+    finally:
+        lib.nsseam_use_gpu(0)
+    if rc != 0:
+        raise RuntimeError("nsseam_solve_sequence: the solver threw")
+    return out, sing
 
 
 def seam_ac_sweep(n, col_ptr, row_idx, g, c, rhs, omegas, gpu: bool):

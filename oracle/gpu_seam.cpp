@@ -42,29 +42,18 @@ public:
         CSCData csc = pattern.to_csc();
         gpu_.symbolic(pattern.size(), csc.col_ptr, csc.row_idx);
         nnz_ = pattern.nnz();
-        pattern_ = &pattern;  // the caller keeps the pattern alive (make_solver.cpp:76-82)
     }
-    bool numeric(const SparsityPattern& p, const NumericMatrix& mat, double diag_gmin) override {
-        if (equilibrate_) return cpu_.numeric(p, mat, diag_gmin);
+    bool numeric(const SparsityPattern&, const NumericMatrix& mat, double diag_gmin) override {
         return gpu_.numeric(values(mat), diag_gmin);  // true = singular, as NeoSolver
     }
     bool refactorize(const NumericMatrix& mat, double diag_gmin) override {
-        if (equilibrate_) return cpu_.refactorize(mat, diag_gmin);
         return gpu_.refactorize(values(mat), diag_gmin);
     }
-    void solve(std::vector<double>& rhs) override {
-        if (equilibrate_) cpu_.solve(rhs);
-        else gpu_.solve(rhs);
-    }
-    // Equilibration (solve_dc's last aid, dc.cpp:355-387) stays on the CPU
-    // NeoSolver; it must follow symbolic().
-    void set_equilibrate(bool on) override {
-        if (on && !pattern_)
-            throw std::logic_error("GpuNeoSolver::set_equilibrate before symbolic()");
-        if (on && !equilibrate_) cpu_.symbolic(*pattern_);
-        equilibrate_ = on;
-        cpu_.set_equilibrate(on);
-    }
+    void solve(std::vector<double>& rhs) override { gpu_.solve(rhs); }
+    // Row/column equilibration (solve_dc's last aid, dc.cpp:355-387): the
+    // scaled matrix is factored on the GPU; only the Markowitz engine honors
+    // it, as only NeoSolver does in the reference.
+    void set_equilibrate(bool on) override { gpu_.set_equilibrate(on); }
     // Complex (AC): Markowitz ordering on the host, factor and sweeps on the
     // GPU (the reference's AC uses NeoSolver whatever the circuit).
     void numeric_complex(const SparsityPattern&, const std::vector<double>& ax) override {
@@ -74,16 +63,13 @@ public:
         return gpu_.refactorize_complex(ax);
     }
     void solve_complex(std::vector<double>& rhs) override { gpu_.solve_complex(rhs); }
-    const char* name() const override { return equilibrate_ ? cpu_.name() : gpu_.name(); }
+    const char* name() const override { return gpu_.name(); }
 
 private:
     std::vector<double> values(const NumericMatrix& m) const {
         return std::vector<double>(m.data(), m.data() + nnz_);
     }
     nsgpu::GpuSolver gpu_;
-    NeoSolver cpu_;
-    const SparsityPattern* pattern_ = nullptr;
-    bool equilibrate_ = false;
     int nnz_ = 0;
 };
 
@@ -105,6 +91,39 @@ void nsseam_use_gpu(int on) { neospice::g_gpu_seam = on != 0; }
 
 // GpuNeoSolver objects created so far (proof that the seam was used).
 long long nsseam_gpu_solvers(void) { return neospice::g_gpu_solvers; }
+
+// numeric() on values[0] and refactorize() on values[1..npoints-1], each
+// followed by solve() of rhs, through whatever ISolver make_solver returns,
+// with equilibration on (equilibrate != 0) as solve_dc's last aid switches
+// it on; out receives n doubles per point, singular[f] each call's verdict.
+// Returns 0, or -1 when the solver threw.
+int nsseam_solve_sequence(int n, int nnz, const int* col_ptr, const int* row_idx,
+                          const double* values, const double* rhs, int npoints, double diag_gmin,
+                          int equilibrate, int is_linear, double* out, int* singular) {
+    try {
+        std::vector<std::pair<int32_t, int32_t>> entries;
+        entries.reserve(nnz);
+        for (int j = 0; j < n; ++j)
+            for (int k = col_ptr[j]; k < col_ptr[j + 1]; ++k) entries.emplace_back(row_idx[k], j);
+        neospice::SparsityPattern pattern(n, std::move(entries));
+        auto solver = neospice::make_solver(n, is_linear != 0);
+        solver->symbolic(pattern);
+        solver->set_equilibrate(equilibrate != 0);
+        neospice::NumericMatrix mat(pattern);
+        std::vector<double> z(n);
+        for (int f = 0; f < npoints; ++f) {
+            std::memcpy(mat.data(), values + static_cast<size_t>(nnz) * f, sizeof(double) * nnz);
+            singular[f] = (f == 0 ? solver->numeric(pattern, mat, diag_gmin)
+                                  : solver->refactorize(mat, diag_gmin)) ? 1 : 0;
+            z.assign(rhs, rhs + n);
+            if (!singular[f]) solver->solve(z);
+            std::memcpy(out + static_cast<size_t>(n) * f, z.data(), sizeof(double) * n);
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
 
 // An AC sweep through whatever ISolver make_solver returns, with the
 // per-frequency steps of solve_ac (src/core/ac.cpp:196-216): ax = G + j*omega*C
