@@ -565,8 +565,9 @@ int nsg_tran_batch_params(const nsg_tran_batch* b, long long* offsets, double* p
  * checkpoint every `every` steps.  d_params_dc / d_params_tran (device, may
  * be NULL: the batch's own) replace the parameters of the replay.  Refused
  * (NSG_ERR_INVALID): no recorded run, a run that filled max_points, or
- * MOSFETs with charge (diodes and their charge are covered; diode
- * parameters are not differentiated). */
+ * BSIM4v7 devices.  Diode charge and level-1 MOSFET charge (Meyer gate,
+ * overlap and bulk-junction capacitance) are in the recursion; diode
+ * parameters are not differentiated. */
 int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_targets,
                            double weight, int every, const double* d_params_dc,
                            const double* d_params_tran, double* d_grads, double* d_loss,

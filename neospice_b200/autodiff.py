@@ -11,9 +11,9 @@ entries of the parameter blocks).
 ``tran_loss(batch, probes, targets, params)`` returns, per instance of a
 recorded ``TranBatch``, L_i = weight * sum_n (x_n[probe_i] - target_n)^2 over
 the recorded timepoints, and its backward is the transient adjoint (a
-transposed solve on each step's LU, checkpointed replay, capacitor- and
-diode-charge recursion) with respect to resistances, capacitances, DC source
-values and MOSFET W, L and VTO.
+transposed solve on each step's LU, checkpointed replay, capacitor, diode
+and level-1 MOSFET charge recursion) with respect to resistances,
+capacitances, DC source values and MOSFET W, L and VTO.
 
 Failed instances do not produce silent garbage: an instance whose forward
 solve did not converge (status != 0) gets NaN solutions / loss, and an

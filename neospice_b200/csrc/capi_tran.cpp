@@ -2,6 +2,7 @@
 #include "capi_internal.hpp"
 
 #include "host/circuit.hpp"
+#include "kernels/mos1_charge_adjoint.cuh"
 #include "kernels/mos1_model.cuh"
 #include "kernels/tran_device.cuh"
 
@@ -56,6 +57,19 @@ struct nsg_tran_batch {
     int64_t work_size0 = 0;
     int64_t work_size = 0, work_cap = 0;
     long long orderings = 0;
+    // Host orderings made by earlier runs, per instance: the request (first
+    // ordering or re-ordering from plan `from`, diag_gmin), the matrix it was
+    // made from and the topology it gave.  The ordering is a deterministic
+    // function of these, so a run that stops with a bit-identical request
+    // takes the topology without ordering again (a re-run with unchanged
+    // parameters re-orders nothing).
+    struct OrderMemo {
+        int need, from;
+        double diag_gmin;
+        std::vector<double> a;
+        int topo;
+    };
+    std::vector<std::vector<OrderMemo>> memo;
     int32_t* d_lu_pool = nullptr;
     nsg::PlanDesc* d_plans = nullptr;
     int32_t* d_prog = nullptr;
@@ -75,7 +89,7 @@ struct nsg_tran_batch {
     int32_t* d_subset = nullptr;
     // Adjoint: recording of the forward run's steps and operating points,
     // the replay's Newton options, whether each circuit's devices are ones
-    // the adjoint covers (no MOSFET charge), and its workspace.
+    // the adjoint covers (no BSIM4v7), and its workspace.
     bool record = false, recorded = false;
     nsg::StepRecord* d_rec = nullptr;
     double* d_x0 = nullptr;
@@ -241,18 +255,10 @@ int nsg_tran_batch_create(int count, nsg_circuit* const* circuits, double tstep,
         int64_t work = 0, param_off = 0, x0_off = 0;
         for (int i = 0; i < count; ++i) {
             const auto& c = circuits[i]->c;
-            // The adjoint covers level-1 MOSFETs without charge (no oxide,
-            // overlap or junction capacitance in the parameter block),
-            // diodes, and no BSIM4v7 devices (which always carry charge).
-            bool ok = !c.has_bsim4();
-            for (const auto& m : c.mosfets()) {
-                if (m.family != nsg::kFamilyMos1) continue;
-                const double* P = c.params().data() + m.param;
-                for (int q : {nsg::kMOxCapFactor, nsg::kMCgso, nsg::kMCgdo, nsg::kMCgbo,
-                              nsg::kMCbd, nsg::kMCbdsw, nsg::kMCbs, nsg::kMCbssw})
-                    if (P[q] != 0.0) ok = false;
-            }
-            b->adjoint_ok.push_back(ok ? 1 : 0);
+            // The adjoint covers resistors, capacitors, sources, diodes and
+            // level-1 MOSFETs with their Meyer and junction charges; not
+            // BSIM4v7 devices.
+            b->adjoint_ok.push_back(c.has_bsim4() ? 0 : 1);
             b->param_count.push_back(static_cast<int64_t>(c.params().size()));
             nsg::DcDesc& d = b->descs[i];
             fill_instance(d, c, b->topos[plan_dc[i]]->plan, prog, work);
@@ -390,11 +396,28 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
             // Order them on the host threads (instances are independent: a
             // first ordering of a fresh topology, or NeoSolver::numeric on a
             // copy of the current one), then share and place the results.
+            // Requests an earlier run answered take its topology.
+            b->memo.resize(b->count);
+            std::vector<int> from(nt), hit(nt, -1);
+            for (int k = 0; k < nt; ++k) {
+                const int i = todo[k];
+                const nsg::TranCtl& ctl = ctls[k];
+                from[k] = ctl.need == 105 ? -1
+                                          : (ctl.need_plan == 0 ? b->descs[i].plan
+                                                                : b->tdescs[i].tran_plan);
+                for (const auto& m : b->memo[i])
+                    if (m.need == (ctl.need == 105 ? 105 : 0) && m.from == from[k] &&
+                        std::memcmp(&m.diag_gmin, &ctl.need_diag_gmin, sizeof(double)) == 0 &&
+                        m.a.size() == mats[k].size() &&
+                        std::memcmp(m.a.data(), mats[k].data(), sizeof(double) * m.a.size()) == 0)
+                        hit[k] = m.topo;
+            }
             std::vector<std::unique_ptr<nsg_topology>> made(nt);
             std::vector<int> rcs(nt, NSG_OK);
             std::atomic<int> next_item{0};
             auto worker = [&]() {
                 for (int k; (k = next_item.fetch_add(1)) < nt;) {
+                    if (hit[k] >= 0) continue;
                     const int i = todo[k];
                     const nsg::DcDesc& d = b->descs[i];
                     const nsg::TranCtl& ctl = ctls[k];
@@ -404,8 +427,7 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                                                     b->row_idx[i].data(), mats[k].data(),
                                                     ctl.need_diag_gmin, made[k], b->solver[i]);
                         } else {
-                            const int cur = ctl.need_plan == 0 ? d.plan : b->tdescs[i].tran_plan;
-                            made[k] = clone_topology(*b->topos[cur]);
+                            made[k] = clone_topology(*b->topos[from[k]]);
                             rcs[k] = numeric_on_engine(*made[k], mats[k].data(), ctl.need_diag_gmin);
                             if (rcs[k] == NSG_OK) rebuild_plan(*made[k]);
                         }
@@ -423,11 +445,19 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                 for (int t = 0; t < nthreads; ++t) pool.emplace_back(worker);
                 for (auto& th : pool) th.join();
             }
+            const size_t ntopos = b->topos.size();
             for (int k = 0; k < nt; ++k) {
-                if (rcs[k] != NSG_OK || !made[k]) continue;  // keeps its status: not ordered
                 const int i = todo[k];
+                int topo = hit[k];
+                if (topo < 0) {
+                    if (rcs[k] != NSG_OK || !made[k]) continue;  // keeps its status: not ordered
+                    topo = intern_topology(b->topos, std::move(made[k]));
+                    auto& mi = b->memo[i];
+                    if (mi.size() >= 4) mi.erase(mi.begin());
+                    mi.push_back({ctls[k].need == 105 ? 105 : 0, from[k], ctls[k].need_diag_gmin,
+                                  std::move(mats[k]), topo});
+                }
                 nsg::DcDesc& d = b->descs[i];
-                const int topo = intern_topology(b->topos, std::move(made[k]));
                 if (ctls[k].need_plan == 0) d.plan = topo;
                 else b->tdescs[i].tran_plan = topo;
                 place_lu_workspace(d, b->topos[topo]->plan, b->work_size);
@@ -438,8 +468,11 @@ int nsg_tran_batch_run(nsg_tran_batch* b, void* stream) {
                 b->recorded = b->record;
                 break;
             }
-            int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col, &b->max_n);
-            if (rc != NSG_OK) return rc;
+            if (b->topos.size() != ntopos) {  // new plans to upload
+                int rc = refresh_plans(b->topos, &b->d_lu_pool, &b->d_plans, &b->max_col,
+                                       &b->max_n);
+                if (rc != NSG_OK) return rc;
+            }
             if (nsg::tran_smem_bytes(b->max_col, b->max_n) > 200 * 1024)
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_run: an ordered instance is too "
                                              "large for the shared-memory refactor");
@@ -552,7 +585,7 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             if (!b->adjoint_ok[i])
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: instance " +
                                                  std::to_string(i) +
-                                                 " has MOSFETs with charge (not covered)");
+                                                 " has BSIM4v7 devices (not covered)");
             if (probe[i] < 0 || probe[i] >= d.n)
                 return fail(NSG_ERR_INVALID, "nsg_tran_batch_adjoint: probe out of range");
             nsg::AdjDesc& a = ad[i];
@@ -566,7 +599,7 @@ int nsg_tran_batch_adjoint(nsg_tran_batch* b, const int* probe, const double* d_
             a.ckpt_len = (2 * d.n + 2 * d.n_states + nsg::kMosRecCount * nmos + 3) & ~int64_t{3};
             a.ws_off = ws;
             ws += a.n_ckpt * a.ckpt_len + (every + 2) * (int64_t{d.n} + d.n_states) +
-                  3 * (int64_t{d.n_caps} + d.n_diodes) + d.n;
+                  7 * (int64_t{d.n_caps} + d.n_diodes + nsg::kMos1ChargeUnits * nmos) + d.n;
             ws = (ws + 3) & ~int64_t{3};
             // The LU region must hold both the DC and the transient plan.
             const auto& pd = b->topos[d.plan]->plan;

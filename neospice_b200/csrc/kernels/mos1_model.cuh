@@ -129,10 +129,13 @@ NSG_HD inline double m1_fetlim(double vnew, double vold, double vto) {
     return vnew;
 }
 
-// Meyer gate capacitances (half of the voltage-dependent part).
-NSG_HD inline void m1_qmeyer(double vgs, double vgd, double von, double vdsat, double* capgs,
-                             double* capgd, double* capgb, double phi, double cox) {
-    const double vgst = vgs - von;
+// Meyer gate capacitances (half of the voltage-dependent part).  T is
+// double in the load; the transient adjoint evaluates the same expressions
+// on a derivative-carrying number type.
+template <class T>
+NSG_HD inline void m1_qmeyer(T vgs, T vgd, T von, T vdsat, T* capgs, T* capgd, T* capgb,
+                             double phi, double cox) {
+    const T vgst = vgs - von;
     vdsat = fmax(vdsat, 0.025);
     if (vgst <= -phi) {
         *capgb = cox / 2;
@@ -145,26 +148,26 @@ NSG_HD inline void m1_qmeyer(double vgs, double vgd, double von, double vdsat, d
     } else if (vgst <= 0) {
         *capgb = -vgst * cox / (2 * phi);
         *capgs = vgst * cox / (1.5 * phi) + cox / 3;
-        const double vds = vgs - vgd;
+        const T vds = vgs - vgd;
         if (vds >= vdsat) {
             *capgd = 0;
         } else {
-            const double vddif = 2.0 * vdsat - vds;
-            const double vddif1 = vdsat - vds;
-            const double vddif2 = vddif * vddif;
+            const T vddif = 2.0 * vdsat - vds;
+            const T vddif1 = vdsat - vds;
+            const T vddif2 = vddif * vddif;
             *capgd = *capgs * (1.0 - vdsat * vdsat / vddif2);
             *capgs = *capgs * (1.0 - vddif1 * vddif1 / vddif2);
         }
     } else {
-        const double vds = vgs - vgd;
+        const T vds = vgs - vgd;
         if (vdsat <= vds) {
             *capgs = cox / 3;
             *capgd = 0;
             *capgb = 0;
         } else {
-            const double vddif = 2.0 * vdsat - vds;
-            const double vddif1 = vdsat - vds;
-            const double vddif2 = vddif * vddif;
+            const T vddif = 2.0 * vdsat - vds;
+            const T vddif1 = vdsat - vds;
+            const T vddif2 = vddif * vddif;
             *capgd = cox * (1.0 - vdsat * vdsat / vddif2) / 3;
             *capgs = cox * (1.0 - vddif1 * vddif1 / vddif2) / 3;
             *capgb = 0;
@@ -200,6 +203,32 @@ NSG_HD inline void m1_junction_sargs(double mj, double mjsw, double arg, double*
     }
     *sarg = (mj == .5) ? 1 / sqrt(arg) : exp(-mj * log(arg));
     *sargsw = (mjsw == .5) ? 1 / sqrt(arg) : exp(-mjsw * log(arg));
+}
+
+// Charge and capacitance of the bulk-drain (drain) or bulk-source junction
+// at junction voltage v (MOS1load's depletion charge; zero when the
+// junction has no capacitance).
+NSG_HD inline void m1_bulk_charge(const double* P, double v, bool drain, double* q, double* cap) {
+    const double cz = P[drain ? kMCbd : kMCbs], czsw = P[drain ? kMCbdsw : kMCbssw];
+    if (cz == 0 && czsw == 0) {
+        *q = 0;
+        *cap = 0;
+        return;
+    }
+    if (v < P[kMTDepCap]) {
+        const double pb = P[kMTBulkPot], mj = P[kMMj], mjsw = P[kMMjsw];
+        const double arg = 1 - v / pb;
+        double sarg, sargsw;
+        m1_junction_sargs(mj, mjsw, arg, &sarg, &sargsw);
+        *q = pb * (cz * (1 - arg * sarg) / (1 - mj) + czsw * (1 - arg * sargsw) / (1 - mjsw));
+        *cap = cz * sarg + czsw * sargsw;
+    } else if (drain) {
+        *q = P[kMF4d] + v * (P[kMF2d] + v * P[kMF3d] / 2);
+        *cap = P[kMF2d] + v * P[kMF3d];
+    } else {
+        *q = P[kMF4s] + v * (P[kMF2s] + v * (P[kMF3s] / 2));
+        *cap = P[kMF2s] + P[kMF3s] * v;
+    }
 }
 
 // One MOS1load of one instance.  P: parameter block; rec: persistent
@@ -357,40 +386,9 @@ NSG_HD inline void mos1_load(const double* P, double* rec, double* s0, double* s
     double cd = dm * cdrain - cbd;
 
     if (mode & (kM1Tran | kM1TranOp | kM1InitSmsig)) {
-        const double pb = P[kMTBulkPot], mj = P[kMMj], mjsw = P[kMMjsw];
         double capbs, capbd;
-        if (P[kMCbs] != 0 || P[kMCbssw] != 0) {
-            if (vbs < P[kMTDepCap]) {
-                const double arg = 1 - vbs / pb;
-                double sarg, sargsw;
-                m1_junction_sargs(mj, mjsw, arg, &sarg, &sargsw);
-                s0[kSQbs] = pb * (P[kMCbs] * (1 - arg * sarg) / (1 - mj) +
-                                  P[kMCbssw] * (1 - arg * sargsw) / (1 - mjsw));
-                capbs = P[kMCbs] * sarg + P[kMCbssw] * sargsw;
-            } else {
-                s0[kSQbs] = P[kMF4s] + vbs * (P[kMF2s] + vbs * (P[kMF3s] / 2));
-                capbs = P[kMF2s] + P[kMF3s] * vbs;
-            }
-        } else {
-            s0[kSQbs] = 0;
-            capbs = 0;
-        }
-        if (P[kMCbd] != 0 || P[kMCbdsw] != 0) {
-            if (vbd < P[kMTDepCap]) {
-                const double arg = 1 - vbd / pb;
-                double sarg, sargsw;
-                m1_junction_sargs(mj, mjsw, arg, &sarg, &sargsw);
-                s0[kSQbd] = pb * (P[kMCbd] * (1 - arg * sarg) / (1 - mj) +
-                                  P[kMCbdsw] * (1 - arg * sargsw) / (1 - mjsw));
-                capbd = P[kMCbd] * sarg + P[kMCbdsw] * sargsw;
-            } else {
-                s0[kSQbd] = P[kMF4d] + vbd * (P[kMF2d] + vbd * P[kMF3d] / 2);
-                capbd = P[kMF2d] + vbd * P[kMF3d];
-            }
-        } else {
-            s0[kSQbd] = 0;
-            capbd = 0;
-        }
+        m1_bulk_charge(P, vbs, false, &s0[kSQbs], &capbs);
+        m1_bulk_charge(P, vbd, true, &s0[kSQbd], &capbd);
         if ((mode & kM1Tran) || ((mode & kM1InitTran) && !(mode & kM1Uic))) {
             double geq, ceq;
             m1_integrate(ic, s0, s1, s2, kSQbd, capbd, &geq, &ceq);

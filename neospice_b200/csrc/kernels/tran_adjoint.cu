@@ -24,11 +24,26 @@
 // q(v) (depletion plus transit-time charge, a function of its junction
 // voltage) enters the same recursion as a capacitor with C replaced by
 // dq/dv at the step whose charge it is (q_s appears in i_s, i_{s+1} and
-// i_{s+2}); diode parameters are not differentiated.  Circuits whose
-// MOSFETs carry charge (oxide, overlap or junction capacitance) are
-// rejected by the host: the Meyer charges are accumulated from capacitance
-// averages, not a function of the voltages, and are not part of this
-// recursion.
+// i_{s+2}); diode parameters are not differentiated.
+//
+// Level-1 MOSFET charges (mos1_model.cuh) enter as five more units per
+// instance.  The bulk junctions are charges q(v) like the diode's.  The
+// Meyer gate charges are accumulated, q_n = G_n = q_{n-1} + (v_n - v_{n-1})
+// c_n with c_n = h(x_n) + h(x_{n-1}) + overlap, and the current a Meyer
+// unit puts into the step residual is I_n = i_n + ag0 q_n (1 - c_n) (the
+// charge integration MOS1load calls returns ceq = i - geq q, and the load
+// adds ag0 q back), so each unit carries a charge adjoint kappa besides
+// eta (beta_n = B^T lambda_n):
+//   kappa_n = ag0_n eta_n + ag1_{n+1} eta_{n+1} + ag2_{n+2} eta_{n+2}
+//             + kappa_{n+1} - ag0_n (1 - c_n) beta_n
+// (dG_n/dx_n)^T kappa_n, (dG_{n+1}/dx_n)^T kappa_{n+1} and I_{n+1}'s
+// dependence on h(x_n) enter the x_n equation (the parts through lambda_n
+// land in the matrix, the rest in the right-hand side), the step matrix
+// gets what the Newton matrix leaves out of dI_n/dx_n, and
+//   dL/dp += kappa_n dG_n/dp + beta_n ag0_n q_n dc_n/dp
+// (W, L through the oxide and overlap capacitances, VTO through von) with
+// dh/dx and dh/dVTO from m1_meyer_dual.
+#include "mos1_charge_adjoint.cuh"
 #include "newton_common.cuh"
 #include "tran_device.cuh"
 
@@ -114,6 +129,209 @@ __device__ inline void vcopy(double* dst, const double* src, int64_t n) {
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
+// Node voltages d, g, s, b of MOSFET record mr in x (0 for ground).
+__device__ inline void mos_volts(const int32_t* mr, const double* x, double vn[4]) {
+    for (int q = 0; q < 4; ++q) vn[q] = mr[q] >= 0 ? x[mr[q]] : 0.0;
+}
+
+__device__ inline bool mos_charged(const Inst& v, const int32_t* mr) {
+    return mr[6] != kMosFamilyBsim4 && m1_has_charge(v.par + mr[4]);
+}
+
+__device__ inline void meyer_at(const double* P, const double vn[4], Dual4 h[3]) {
+    const double type = P[kMType];
+    m1_meyer_dual(P, type * (vn[1] - vn[2]), type * (vn[0] - vn[2]), type * (vn[3] - vn[2]), h);
+}
+
+// The MOSFET stamp terms of the instance's term vector.
+__device__ inline double* mos_terms(const Inst& v) {
+    return v.tv + v.n_const + kDiodeTermCount * v.n_diodes + kCapTermCount * v.n_caps +
+           kSrcTermCount * v.n_srcs;
+}
+
+// Step n's Jacobian.  A Meyer unit's current in the step residual is
+// I_n = i_n + ag0 q_n (1 - c_n): the charge integration MOS1load calls
+// returns ceq = i - geq q (mos1_shim.cpp's NIintegrate) and the load adds
+// ag0 q back.  Its exact derivative is
+//   ag0 (2 - c_n) B dq_n/dx_n - ag0 q_n B dh(x_n)/dx
+// with dq_n/dx_n = c_n B^T + (v_n - v_{n-1}) dh(x_n)/dx; the Newton matrix
+// holds ag0 c_n B B^T of it, this adds the rest.
+__device__ __noinline__ void meyer_jacobian(const Inst& v, const double* xs, const double* xp,
+                                            double ag0) {
+    double* tv_m = mos_terms(v);
+    for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
+        const int32_t* mr = v.mos + kMosTabStride * k;
+        if (!mos_charged(v, mr)) continue;
+        const double* P = v.par + mr[4];
+        const double* st0 = v.st[0] + mr[5];
+        const double* st1 = v.st[1] + mr[5];
+        const double type = P[kMType];
+        double vn[4], vp[4];
+        mos_volts(mr, xs, vn);
+        mos_volts(mr, xp, vp);
+        Dual4 h[3];
+        meyer_at(P, vn, h);
+        double* t = tv_m + kMosTermCount * k;
+        for (int j = 0; j < 3; ++j) {
+            const int a = m1_unit_pos(j), b = m1_unit_neg(j);
+            const int slot = m1_unit_cap_slot(j);
+            double dW, dL;
+            const double c = st0[slot] + st1[slot] + m1_overlap(P, j, &dW, &dL);
+            const double q = type * st0[slot + 1];
+            const double dv = (vn[a] - vn[b]) - (vp[a] - vp[b]);
+            const double gh = ag0 * ((2.0 - c) * dv - q);
+            const double gb = ag0 * c * (1.0 - c);
+            double gn[4];
+            m1_node_grad(h[j], type, gn);
+            for (int r = 0; r < 4; ++r) {
+                t[m1_term_at(a, r)] += gh * gn[r];
+                t[m1_term_at(b, r)] -= gh * gn[r];
+            }
+            t[m1_term_at(a, a)] += gb;
+            t[m1_term_at(a, b)] -= gb;
+            t[m1_term_at(b, a)] -= gb;
+            t[m1_term_at(b, b)] += gb;
+        }
+    }
+}
+
+// Integration coefficients the backward recursion of step n reads: its own
+// ag0 and the next steps' ag1 / ag2 / trapezoidal ratio.
+struct AdjCoef {
+    double ag0, ag1n, ag2n, r1;
+    bool has1, has2, op;  // op: the operating point (q_0 = v_0 (2 h_0 + o), no ag0 term)
+};
+
+// MOSFET charges' part of step n's adjoint right-hand side:
+//   (dG_n/dx_n)^T (ag0 mu + K) + (dG_{n+1}/dx_n)^T kappa_{n+1}
+//   + beta_{n+1} ag0_{n+1} q_{n+1} dh(x_n)/dx
+// per Meyer unit (K = ag1 eta_{n+1} + ag2 eta_{n+2} + kappa_{n+1}; the last
+// term is step n+1's I_{n+1} through c_{n+1}'s h(x_n), beta = B^T lambda,
+// kept in p1), and dq/dv B (ag0 mu + ag1 eta_{n+1} + ag2 eta_{n+2}) per
+// junction.  Writes mu.
+__device__ __noinline__ void mos_charge_rhs(const Inst& v, int32_t base, const double* xs,
+                                            const double* xp, const AdjCoef& cf,
+                                            const double* eta1, const double* eta2, double* mu,
+                                            const double* kap1, const double* c1,
+                                            const double* w1, const double* p1, double* lam) {
+    for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
+        const int32_t* mr = v.mos + kMosTabStride * k;
+        if (!mos_charged(v, mr)) continue;
+        const double* P = v.par + mr[4];
+        const double* st0 = v.st[0] + mr[5];
+        const double* st1 = v.st[1] + mr[5];
+        double vn[4], vp[4];
+        mos_volts(mr, xs, vn);
+        if (!cf.op) mos_volts(mr, xp, vp);
+        Dual4 h[3];
+        meyer_at(P, vn, h);
+        for (int j = 0; j < kMos1ChargeUnits; ++j) {
+            const int32_t u = base + kMos1ChargeUnits * k + j;
+            const int a = m1_unit_pos(j), b = m1_unit_neg(j);
+            const double m = (cf.has1 && !cf.op) ? -cf.r1 * eta1[u] : 0.0;
+            if (!cf.op) mu[u] = m;
+            double kj = 0.0;
+            if (cf.has1) kj += cf.ag1n * eta1[u];
+            if (cf.has2) kj += cf.ag2n * eta2[u];
+            const double z0 = cf.op ? 0.0 : cf.ag0 * m;
+            double cb;
+            if (j < 3) {
+                const int slot = m1_unit_cap_slot(j);
+                double dW, dL;
+                const double o = m1_overlap(P, j, &dW, &dL);
+                const double vs = vn[a] - vn[b];
+                const double c = cf.op ? 2 * st0[slot] + o : st0[slot] + st1[slot] + o;
+                const double self = cf.op ? 2 * vs : vs - (vp[a] - vp[b]);
+                const double z = z0 + kj + kap1[u];
+                cb = z * c - kap1[u] * c1[u];
+                const double ch = z * self + kap1[u] * (w1[u] - vs) + p1[u];
+                double gn[4];
+                m1_node_grad(h[j], P[kMType], gn);
+                for (int q = 0; q < 4; ++q)
+                    if (mr[q] >= 0) atomicAdd(lam + mr[q], ch * gn[q]);
+            } else {
+                double q, capj;
+                m1_bulk_charge(P, st0[j == 3 ? kSVbd : kSVbs], j == 3, &q, &capj);
+                cb = capj * (z0 + kj);
+            }
+            if (mr[a] >= 0) atomicAdd(lam + mr[a], cb);
+            if (mr[b] >= 0) atomicAdd(lam + mr[b], -cb);
+        }
+    }
+}
+
+// After step n's transposed solve, per Meyer unit with beta_n = B^T lambda_n:
+//   eta_n   = mu_n - beta_n
+//   kappa_n = ag0 eta_n + K - ag0 (1 - c_n) beta_n
+// (the last term from I_n's ag0 q_n (1 - c_n)), and
+//   dL/dp  += (kappa_n dv_n + beta_n ag0 q_n) (dh(x_n)/dp + do/dp)
+//           + (kappa_{n+1} dv_{n+1} + beta_{n+1} ag0_{n+1} q_{n+1}) dh(x_n)/dp
+// (dv_n = v_n - v_{n-1}; the second line is c_{n+1}'s h(x_n) part).  At
+// the operating point (q_0 = v_0 (2 h_0 + o), no current in R_0) kappa_0 = K
+// and only the gradients.  Junction units: eta only.
+__device__ __noinline__ void mos_charge_update(const Inst& v, int32_t base, const double* xs,
+                                               const double* xp, const AdjCoef& cf,
+                                               const double* lam, double* eta1, double* eta2,
+                                               const double* mu, double* kap1, double* c1,
+                                               double* w1, double* p1, double* g) {
+    for (int32_t k = threadIdx.x; k < v.n_mos; k += blockDim.x) {
+        const int32_t* mr = v.mos + kMosTabStride * k;
+        if (!mos_charged(v, mr)) continue;
+        const double* P = v.par + mr[4];
+        const double* st0 = v.st[0] + mr[5];
+        const double* st1 = v.st[1] + mr[5];
+        const double type = P[kMType];
+        double vn[4], vp[4];
+        mos_volts(mr, xs, vn);
+        if (!cf.op) mos_volts(mr, xp, vp);
+        Dual4 h[3];
+        meyer_at(P, vn, h);
+        const double W = P[kMW], leff = P[kML] - 2 * P[kMLatDiff];
+        double gW = 0.0, gL = 0.0, gV = 0.0;
+        for (int j = 0; j < kMos1ChargeUnits; ++j) {
+            const int32_t u = base + kMos1ChargeUnits * k + j;
+            const int a = m1_unit_pos(j), b = m1_unit_neg(j);
+            auto at = [&](int32_t i) { return i >= 0 ? lam[i] : 0.0; };
+            const double beta = cf.op ? 0.0 : at(mr[a]) - at(mr[b]);
+            const double e = cf.op ? 0.0 : mu[u] - beta;
+            if (j < 3) {
+                const int slot = m1_unit_cap_slot(j);
+                double dW, dL;
+                const double o = m1_overlap(P, j, &dW, &dL);
+                const double c = st0[slot] + st1[slot] + o;
+                const double q = type * st0[slot + 1];
+                double kj = 0.0;
+                if (cf.has1) kj += cf.ag1n * eta1[u];
+                if (cf.has2) kj += cf.ag2n * eta2[u];
+                const double kap =
+                    cf.op ? kj + kap1[u] : cf.ag0 * e + kj + kap1[u] - cf.ag0 * (1.0 - c) * beta;
+                const double vs = vn[a] - vn[b];
+                const double own =
+                    cf.op ? kap * vs : kap * (vs - (vp[a] - vp[b])) + beta * cf.ag0 * q;
+                const double hf = cf.op ? 2.0 : 1.0;
+                const double nxt = kap1[u] * (w1[u] - vs) + p1[u];
+                const double hv = h[j].v;
+                gW += own * (hf * hv / W + dW) + nxt * hv / W;
+                gL += own * (hf * hv / leff + dL) + nxt * hv / leff;
+                gV += own * hf * h[j].d[3] + nxt * h[j].d[3];
+                if (!cf.op) {
+                    c1[u] = c;
+                    w1[u] = vs;
+                    kap1[u] = kap;
+                    p1[u] = beta * cf.ag0 * q;
+                }
+            }
+            if (!cf.op) {
+                eta2[u] = eta1[u];
+                eta1[u] = e;
+            }
+        }
+        g[mr[4] + kMW] += gW;
+        g[mr[4] + kML] += gL;
+        g[mr[4] + kMVto] += gV;
+    }
+}
+
 }  // namespace
 
 __global__ void __launch_bounds__(kFlowThreads, 2)
@@ -141,16 +359,23 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     const double* tg = targets + ad.rec_off;
     double* g = grads + d.param_off;
     double* ws = adj_ws + ad.ws_off;
-    // workspace: checkpoints | segment x (K+2) | segment states (K+2) | eta1 | eta2 | mu | lam
+    // workspace: checkpoints | segment x (K+2) | segment states (K+2) |
+    // eta1 | eta2 | mu | kap1 | cap1 | w1 | p1 | lam
     double* ckpt = ws;
     double* seg_x = ckpt + ad.n_ckpt * ad.ckpt_len;
     double* seg_s = seg_x + (K + 2) * n;
-    // charge units: capacitors 0 .. n_caps-1, then diodes
-    const int32_t nq = v.n_caps + v.n_diodes;
+    // charge units: capacitors 0 .. n_caps-1, then diodes, then five per
+    // MOSFET (kappa, c and v of the next step for the Meyer units)
+    const int32_t mos_base = v.n_caps + v.n_diodes;
+    const int32_t nq = mos_base + kMos1ChargeUnits * v.n_mos;
     double* eta1 = seg_s + (K + 2) * ns;
     double* eta2 = eta1 + nq;
     double* mu = eta2 + nq;
-    double* lam = mu + nq;
+    double* kap1 = mu + nq;
+    double* cap1 = kap1 + nq;
+    double* w1 = cap1 + nq;
+    double* p1 = w1 + nq;
+    double* lam = p1 + nq;
     double* w = work + d.w_off;
     __shared__ IntegCtx ctx;
     __shared__ SolverState solver;
@@ -269,7 +494,8 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
     if (threadIdx.x == 0) loss[d.index] = s_loss;
 
     // ---- 3. backward, segment by segment
-    for (int32_t k = threadIdx.x; k < nq; k += blockDim.x) eta1[k] = eta2[k] = 0.0;
+    for (int32_t k = threadIdx.x; k < nq; k += blockDim.x)
+        eta1[k] = eta2[k] = kap1[k] = cap1[k] = w1[k] = p1[k] = 0.0;
     __syncthreads();
     for (int64_t c0 = ((ad.n_steps - 1) / K) * K; c0 >= 0; c0 -= K) {
         const int64_t c1 = (c0 + K < ad.n_steps) ? c0 + K : ad.n_steps;
@@ -310,6 +536,10 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
             __syncthreads();
             eval_devices(v, ctx, opt, &s_dev_conv);
             __syncthreads();
+            if (v.n_mos > 0) {
+                meyer_jacobian(v, xs, x1, rec[s].ag[0]);
+                __syncthreads();
+            }
             assemble(v);
             const RefactorResult fr = cta_refactor_flow(tpd, lu_pool, v.a, v.lu, opt.diag_gmin,
                                                         kCheckNone, 1e-3, smem, colbuf,
@@ -347,6 +577,10 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
                 if (dr[0] >= 0) atomicAdd(lam + dr[0], cc);
                 if (dr[1] >= 0) atomicAdd(lam + dr[1], -cc);
             }
+            AdjCoef cf{rec[s].ag[0], has1 ? rec[s + 1].ag[1] : 0.0, has2 ? rec[s + 2].ag[2] : 0.0,
+                       has1 ? rec[s + 1].xmu_ratio : 0.0, has1, has2, false};
+            if (v.n_mos > 0)
+                mos_charge_rhs(v, mos_base, xs, x1, cf, eta1, eta2, mu, kap1, cap1, w1, p1, lam);
             __syncthreads();
             cta_solve_transposed(tpd, lu_pool, v.lu, lam, w);
             // capacitor adjoints and dL/dC
@@ -368,6 +602,11 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
                 const double e = mu[u] - (at(lam, dr[0]) - at(lam, dr[1]));
                 eta2[u] = eta1[u];
                 eta1[u] = e;
+            }
+            if (v.n_mos > 0) {
+                mos_charge_update(v, mos_base, xs, x1, cf, lam, eta1, eta2, mu, kap1, cap1, w1, p1,
+                                  g);
+                __syncthreads();
             }
             grad_contract(v, d, prog, lam, xs, g);
             __syncthreads();
@@ -422,8 +661,18 @@ tran_adjoint_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restric
         if (dr[0] >= 0) atomicAdd(lam + dr[0], cc);
         if (dr[1] >= 0) atomicAdd(lam + dr[1], -cc);
     }
+    const AdjCoef cf0{0.0, ad.n_steps >= 1 ? rec[1].ag[1] : 0.0,
+                      ad.n_steps >= 2 ? rec[2].ag[2] : 0.0, 0.0, ad.n_steps >= 1,
+                      ad.n_steps >= 2, true};
+    if (v.n_mos > 0)
+        mos_charge_rhs(v, mos_base, x0, x0, cf0, eta1, eta2, mu, kap1, cap1, w1, p1, lam);
     __syncthreads();
     cta_solve_transposed(dpd, lu_pool, v.lu, lam, w);
+    if (v.n_mos > 0) {
+        mos_charge_update(v, mos_base, x0, x0, cf0, lam, eta1, eta2, mu, kap1, cap1, w1, p1,
+                          g);
+        __syncthreads();
+    }
     grad_contract(v, d, prog, lam, x0, g);
     __syncthreads();
     if (threadIdx.x == 0) status[d.index] = kStatusOk;

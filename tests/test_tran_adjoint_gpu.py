@@ -1,7 +1,8 @@
 """GPU transient adjoint: gradients of a squared-error loss on the far-end
 voltage of an RC tree driven by a level-1 CMOS inverter, with respect to
-every R and C, the DC supply and the drivers' W, L and VTO (and on diode-RC
-transients with diode charge, every R and C), against central finite
+every R and C, the DC supply and the drivers' W, L and VTO (also with the
+drivers' Meyer gate charge, overlap and junction capacitances; and on
+diode-RC transients with diode charge, every R and C), against central finite
 differences (h = 1e-6 relative) of the same discrete transient (the recorded
 timepoints and integration formulas, Newton to reltol 1e-9) to 1e-6
 relative, wherever the difference quotient resolves the gradient: the loss
@@ -20,8 +21,11 @@ pytestmark = pytest.mark.gpu
 TIGHT = dict(reltol=1e-9, vntol=1e-12, abstol=1e-15, max_iter=200)
 
 
-def setup(nodes, seed, tstep=1e-12, tstop=3e-10, count=1):
+def setup(nodes, seed, tstep=1e-12, tstop=3e-10, count=1, cards=None):
     nls = [W.rc_tree_driven(np.random.default_rng([seed, k]), nodes) for k in range(count)]
+    for nl in nls:
+        for name, extra in (cards or {}).items():
+            nl.models[name][1].update(extra)
     far = nodes - 1
     b = TranBatch([nl.build() for nl in nls], tstep, tstop, np.array([far], np.int32),
                   max_points=20000)
@@ -45,8 +49,11 @@ def loss_at(b, probes, targets, p_dc, p_tr):
     return loss.cpu().numpy()
 
 
-def test_tran_adjoint_matches_central_differences():
-    nls, b, tg, probes = setup(24, 81)
+def check_against_fd(nls, b, tg, probes, floor_rel=5e-12, h_rel=1e-6, resolved_below=1e-8):
+    """Every R and C (first eight of each), the DC sources and each MOSFET's
+    W, L and VTO against central differences with step h_rel relative;
+    returns the worst relative error among the quotients whose rounding
+    floor is below resolved_below |fd|, and their number."""
     off, pdc, ptr = b.params()
     g, loss, st = b.adjoint(probes, tg, 1.0, 16)
     torch.cuda.synchronize()
@@ -63,9 +70,9 @@ def test_tran_adjoint_matches_central_differences():
     for k, s in starts:
         if k == "M":
             idx += [s + 0, s + 1, s + 2]  # W, L, VTO
-    worst = 0.0
+    worst, resolved = 0.0, 0
     for i in idx:
-        h = abs(pdc[i]) * 1e-6
+        h = abs(pdc[i]) * h_rel
         lo_dc, hi_dc, lo_tr, hi_tr = pdc.copy(), pdc.copy(), ptr.copy(), ptr.copy()
         hi_dc[i] += h
         hi_tr[i] += h
@@ -75,11 +82,44 @@ def test_tran_adjoint_matches_central_differences():
         lp = loss_at(b, probes, tg, dev(hi_dc), dev(hi_tr))[0]
         lm = loss_at(b, probes, tg, dev(lo_dc), dev(lo_tr))[0]
         fd = (lp - lm) / (2 * h)
-        floor = 5e-12 * float(loss[0]) / (2 * h)
+        floor = floor_rel * float(loss[0]) / (2 * h)
         assert abs(g[i] - fd) <= 1e-6 * abs(fd) + floor, (i, g[i], fd, floor)
-        if floor < 1e-8 * abs(fd):  # well resolved: the adjoint to 1e-6
+        if floor < resolved_below * abs(fd):  # well resolved: the adjoint to 1e-6
             worst = max(worst, abs(g[i] - fd) / abs(fd))
-    assert worst < 1e-6
+            resolved += 1
+    return worst, resolved
+
+
+def test_tran_adjoint_matches_central_differences():
+    nls, b, tg, probes = setup(24, 81)
+    assert check_against_fd(nls, b, tg, probes)[0] < 1e-6
+
+
+MEYER = {"TOX": 1e-6, "CGSO": 2e-11, "CGDO": 2e-11, "CGBO": 1e-11}
+MEYER_STRONG = {"TOX": 2e-8, "CGSO": 4e-10, "CGDO": 4e-10, "CGBO": 2e-10}
+JUNCTION = {"CBD": 5e-15, "CBS": 4e-15, "GAMMA": 0.4}
+
+
+@pytest.mark.parametrize("extra,min_resolved", [("meyer", 6), ("meyer+junction", 6),
+                                                ("strong+junction", 0)])
+def test_tran_adjoint_with_mos_charge(extra, min_resolved):
+    """The drivers carry Meyer gate charge (TOX) with overlap capacitances,
+    and bulk-junction charge with body effect: the adjoint's charge units
+    and the Meyer terms of the step Jacobian against central differences for
+    every R, C, the supply and both drivers' W, L, VTO.  The quotients use
+    h = 1e-5 relative: with the Meyer capacitances' kinks the loss curves
+    enough that the truncation error is about 2e-6 at h = 1e-4 and falls as
+    h^2 (2e-8 at 1e-5), while the rounding floor stays 5e-12 L / 2h.  With
+    moderate oxide and overlap capacitance the six W / L / VTO gradients are
+    resolved (floor below 1e-7 |fd|) and must be within 1e-6; at TOX = 20 nm
+    (the gate-drain charge dominates the output and the loss is small) each
+    gradient is checked against its floor only."""
+    card = dict(MEYER_STRONG if extra.startswith("strong") else MEYER)
+    if extra.endswith("junction"):
+        card.update(JUNCTION)
+    nls, b, tg, probes = setup(12, 84, cards={"nch": card, "pch": card})
+    worst, resolved = check_against_fd(nls, b, tg, probes, h_rel=1e-5, resolved_below=1e-7)
+    assert resolved >= min_resolved and worst < 1e-6, (resolved, worst)
 
 
 def test_tran_adjoint_checkpoint_spacing_and_batching():
@@ -97,18 +137,20 @@ def test_tran_adjoint_checkpoint_spacing_and_batching():
         np.testing.assert_array_equal(l, outs[0][1])
 
 
-def test_tran_adjoint_requires_recording_and_rejects_mos_charge():
+def test_tran_adjoint_requires_recording_and_rejects_bsim4():
     nl = W.rc_tree_driven(np.random.default_rng(3), 6)
     b = TranBatch([nl.build()], 1e-12, 1e-10, np.array([5], np.int32), max_points=5000)
     b.run()
     tg = torch.zeros(5000, dtype=torch.float64, device="cuda")
     with pytest.raises(L.NsgError):
         b.adjoint([5], tg)
-    nl.models["nch"][1]["TOX"] = 2e-8  # Meyer gate capacitance: not covered
+    for name in ("nch", "pch"):  # BSIM4v7 drivers: not covered
+        nl.models[name] = (nl.models[name][0], {"LEVEL": 14})
     b2 = TranBatch([nl.build()], 1e-12, 1e-10, np.array([5], np.int32), max_points=5000)
     b2.record(True)
     b2.run()
-    with pytest.raises(L.NsgError):
+    assert b2.results()[0]["status"] == 0
+    with pytest.raises(L.NsgError, match="BSIM4v7"):
         b2.adjoint([5], tg)
 
 
