@@ -199,7 +199,7 @@ __device__ __forceinline__ double lu_peer(const double* p) {
 // warp's row -> position scratch (pd.n words), written for column j's rows
 // first.  The row map reads L(:, r)'s row indices, which every consumer
 // column of r shares, instead of a map entry per update.
-template <bool kCrossSm, class Probe>
+template <bool kCrossSm, class Probe, int kChunk = kColChunk>
 __device__ __forceinline__ ColumnResult refactor_column(
     const PlanDesc& pd, const int32_t* __restrict__ pool, const double* __restrict__ a,
     double* lu, double diag_gmin, int check_pivots, double rel_threshold, int32_t j, double* buf,
@@ -306,20 +306,20 @@ __device__ __forceinline__ ColumnResult refactor_column(
         if (lane == 0) buf[q] = u;
         if (lane < cnt_c) buf[ld_c] = lu_sub(buf[ld_c], lu_mul(u, lv_c));
         // L(:, r) beyond its first 32 rows: destinations and values are
-        // loaded kColChunk rounds at a time before they are applied (the
+        // loaded kChunk rounds at a time before they are applied (the
         // destinations of one entry are distinct, so the order among them
         // does not matter).
-        for (int32_t t0 = 32; t0 < cnt_c; t0 += 32 * kColChunk) {
-            int32_t dd[kColChunk];
-            double ll[kColChunk];
+        for (int32_t t0 = 32; t0 < cnt_c; t0 += 32 * kChunk) {
+            int32_t dd[kChunk];
+            double ll[kChunk];
 #pragma unroll
-            for (int k = 0; k < kColChunk; ++k) {
+            for (int k = 0; k < kChunk; ++k) {
                 const int32_t t = t0 + 32 * k + lane;
                 dd[k] = (t < cnt_c) ? dest(us_c, l0_c, t) : 0;
                 ll[k] = (t < cnt_c) ? lu_peer<kCrossSm>(lu + l0_c + t) : 0.0;
             }
 #pragma unroll
-            for (int k = 0; k < kColChunk; ++k)
+            for (int k = 0; k < kChunk; ++k)
                 if (t0 + 32 * k + lane < cnt_c) buf[dd[k]] = lu_sub(buf[dd[k]], lu_mul(u, ll[k]));
         }
         __syncwarp();

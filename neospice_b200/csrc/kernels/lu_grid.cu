@@ -25,6 +25,10 @@ namespace nsg {
 namespace {
 
 constexpr int kGridWarps = 8;    // warps per CTA of the grid-wide sweeps
+// Rounds of 32 rows of L(:, r) a warp loads before applying them: long L
+// columns (the separators' hundreds of rows) then cost one L2 round trip
+// per 512 rows instead of per 128.
+constexpr int kGridChunk = 16;
 constexpr int kGridThreads = kGridWarps * 32;
 
 __device__ __forceinline__ int32_t gflag_acquire(const int32_t* f) {
@@ -88,9 +92,10 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
         if (j >= pd.n) break;
         const int32_t len = col_ptr[j + 1] - col_ptr[j];
         double* buf = (len <= kColbuf) ? sbuf : lu + col_ptr[j];
-        const ColumnResult c = refactor_column<true>(
+        auto probe = [&](int32_t r) { return gflag_acquire(done + r); };
+        const ColumnResult c = refactor_column<true, decltype(probe), kGridChunk>(
             pd, pool, A + id.a_off, lu, diag_gmin, check_pivots, rel_threshold, j, buf, lr, ur,
-            [&](int32_t r) { return gflag_acquire(done + r); }, rmap);
+            probe, rmap);
         __threadfence();
         __syncwarp();
         if (lane == 0) {

@@ -444,3 +444,21 @@ def rc_mesh(rng: np.random.Generator, side: int, r_ohm=10.0, c_farad=1e-13,
                 dev.append(("R", k, k + side, float(r_ohm * np.exp(sigma * rng.standard_normal()))))
             dev.append(("C", k, GND, float(c_farad * np.exp(sigma * rng.standard_normal()))))
     return Netlist(n + 1, dev)
+
+
+def power_grid_transient(side: int, seed: int = 2026):
+    """The transient companion matrix of the seeded side x side power grid
+    (power_grid with VDD pads on a pitch-50 lattice and side^2/100 loads):
+    conductances plus C/h on every capacitor node's diagonal (1 pF, h =
+    10 ps).  Returns (n, col_ptr, row_idx, values) of the CSC pattern."""
+    nl = power_grid(np.random.default_rng(seed), side, 50, max(1, side * side // 100))
+    c = nl.build()
+    cp, ri = c.pattern()
+    g, _ = c.initial_matrix(0.0)
+    n = len(cp) - 1
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    capn = np.zeros(n, bool)
+    capn[[d[1] for d in nl.devices if d[0] == "C"]] = True
+    tran = g.copy()
+    tran[(ri == cols) & capn[cols]] += 1e-12 / 1e-11
+    return n, cp, ri, tran
