@@ -175,6 +175,13 @@ int nsg_batch_set_schedule(nsg_batch* batch, int schedule);
  * longest column.  Longer columns are eliminated in place in global memory.
  * No counterpart in the reference (a tuning knob of this schedule). */
 int nsg_batch_set_grid_buffer(nsg_batch* batch, int doubles);
+/* Columns of an AMD-LU instance the grid-wide refactor (schedule 2, with a
+ * 2048- or 4096-double column buffer) hands to whole CTAs instead of single
+ * warps: the last `columns` columns, 0 for none, or -1 (default) for the
+ * longest suffix of columns that each apply at least 128 updates (the top
+ * separators).  Same values either way.  No counterpart in the reference
+ * (a tuning knob of this schedule). */
+int nsg_batch_set_grid_tail(nsg_batch* batch, int columns);
 /* Largest refactor update map (int32 words, one per multiply-subtract) a
  * topology ordered from now on may carry; default 2^30 (4 GiB).  A larger
  * factorization gets no map: its batches run only the grid-wide schedule,

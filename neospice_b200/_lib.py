@@ -69,6 +69,7 @@ SIGNATURES = {
                                    c_void_p]),
     "nsg_batch_set_schedule": (c_int, [c_void_p, c_int]),
     "nsg_batch_set_grid_buffer": (c_int, [c_void_p, c_int]),
+    "nsg_batch_set_grid_tail": (c_int, [c_void_p, c_int]),
     "nsg_set_update_map_limit": (c_int, [c_ll]),
     "nsg_batch_solve": (c_int, [c_void_p, c_void_p, c_void_p]),
     "nsg_batch_solve_transposed": (c_int, [c_void_p, c_void_p, c_void_p]),

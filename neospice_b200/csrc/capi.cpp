@@ -31,7 +31,7 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
                                  double* lrows, double* urows, void* scratch, int colbuf,
                                  int max_col, int32_t* rmaps, int64_t rmap_words,
-                                 cudaStream_t stream);
+                                 const int32_t* cta_from_of, cudaStream_t stream);
 int64_t grid_rmap_words(int colbuf, int max_col, int max_n);
 cudaError_t launch_complex_refactor(const PlanDesc* plans, const int32_t* pool,
                                     const InstDesc* insts, int count, int max_n, const double* A,
@@ -240,6 +240,19 @@ int reorder_instance(std::vector<std::unique_ptr<nsg_topology>>& topos, int topo
     rebuild_plan(*c);
     *new_topo = intern_topology(topos, std::move(c));
     return NSG_OK;
+}
+
+// First column of the grid-wide refactor's CTA-mode tail for an AMD-LU plan:
+// the longest suffix of columns that each apply at least kGridTailUpdates
+// updates (the top separators, whose updates would otherwise run serially
+// in one warp each); n (no tail) for Markowitz plans or a suffix shorter
+// than two columns.
+int32_t grid_tail_from(const nsg::TopologyPlan& p) {
+    constexpr int32_t kGridTailUpdates = 128;
+    if (p.kind != nsg::kPlanKindAmdLu || p.n < 2) return p.n;
+    int32_t j = p.n;
+    while (j > 0 && p.diag_pos[j - 1] - p.col_ptr[j - 1] >= kGridTailUpdates) --j;
+    return (p.n - j >= 2) ? j : p.n;
 }
 
 void place_lu_workspace(nsg::DcDesc& d, const nsg::TopologyPlan& p, int64_t& work_size) {
@@ -520,7 +533,11 @@ int nsg_batch_create(int count, nsg_topology* const* topos, nsg_batch** out) {
             return topos[x.index]->plan.updates > topos[y.index]->plan.updates;
         });
         // Unknowns per launch slot (the grid-wide schedule walks insts[]).
-        for (const auto& d : insts) b->n_of.push_back(topos[d.index]->plan.n);
+        for (const auto& d : insts) {
+            b->n_of.push_back(topos[d.index]->plan.n);
+            b->tail_from_of.push_back(grid_tail_from(topos[d.index]->plan));
+            b->amd_of.push_back(topos[d.index]->plan.kind == nsg::kPlanKindAmdLu ? 1 : 0);
+        }
         cudaError_t e;
         if ((e = upload(&b->d_pool, pool.data(), pool.size())) != cudaSuccess ||
             (e = upload(&b->d_plans, plans.data(), plans.size())) != cudaSuccess ||
@@ -607,11 +624,16 @@ int nsg_batch_refactor(nsg_batch* b, const double* d_values, double diag_gmin,
                 b->rmap_cap = words;
             }
         }
+        std::vector<int32_t> cta_from(b->n_of);
+        for (int i = 0; i < b->count; ++i) {
+            if (b->grid_tail < 0) cta_from[i] = b->tail_from_of[i];
+            else if (b->amd_of[i]) cta_from[i] = std::max(0, b->n_of[i] - b->grid_tail);
+        }
         cudaError_t e = nsg::launch_grid_refactor(
             b->d_plans, b->d_pool, b->d_insts, b->count, b->n_of.data(), d_values, b->d_lu,
             diag_gmin, mode, 1e-3, d_status, d_fail_step, b->d_lrows, b->d_urows, b->d_grid,
             b->grid_colbuf, b->max_col, b->unmapped ? b->d_rmap : nullptr, b->max_n,
-            static_cast<cudaStream_t>(stream));
+            cta_from.data(), static_cast<cudaStream_t>(stream));
         if (e == cudaSuccess) b->rows_valid = true;
         return e == cudaSuccess ? NSG_OK : cuda_fail("nsg_batch_refactor", e);
     }
@@ -651,6 +673,12 @@ const double* nsg_batch_lu(const nsg_batch* b) { return b ? b->d_lu : nullptr; }
 int nsg_set_update_map_limit(long long words) {
     if (words < 0) return fail(NSG_ERR_INVALID, "nsg_set_update_map_limit: negative limit");
     nsg::set_update_map_limit(words);
+    return NSG_OK;
+}
+
+int nsg_batch_set_grid_tail(nsg_batch* b, int columns) {
+    if (!b || columns < -1) return fail(NSG_ERR_INVALID, "nsg_batch_set_grid_tail: bad arguments");
+    b->grid_tail = columns;
     return NSG_OK;
 }
 

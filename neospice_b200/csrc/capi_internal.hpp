@@ -59,6 +59,12 @@ struct nsg_batch {
     int32_t* d_rmap = nullptr;    // per-warp row -> position maps of such plans
     int64_t rmap_cap = 0;         // words allocated at d_rmap
     std::vector<int32_t> n_of;    // unknowns of the instance in each slot of d_insts
+    // Grid-wide refactor: per slot, the first column claimed by whole CTAs
+    // (the chosen tail; n for none), and nsg_batch_set_grid_tail's setting
+    // (-1: the tail of columns with at least kGridTailUpdates U entries).
+    std::vector<int32_t> tail_from_of;
+    std::vector<char> amd_of;     // the slot's plan is AMD-LU (CTA mode needs it)
+    int grid_tail = -1;
     void* d_grid = nullptr;       // flags and state of the grid-wide schedule
     double* d_cwork = nullptr;    // complex sweep workspace (2 doubles per unknown)
     ~nsg_batch() {
@@ -150,6 +156,7 @@ int reorder_instance(std::vector<std::unique_ptr<nsg_topology>>& topos, int topo
                      const double* values, double diag_gmin, int* new_topo);
 // Fresh LU / row-copy regions for a re-ordered instance at the end of the
 // workspace (work_size grows).
+int32_t grid_tail_from(const nsg::TopologyPlan& p);
 void place_lu_workspace(nsg::DcDesc& d, const nsg::TopologyPlan& p, int64_t& work_size);
 // Reallocate the device workspace to hold `needed` doubles, keeping contents.
 cudaError_t grow_workspace(double** d_work, int64_t* capacity, int64_t needed);

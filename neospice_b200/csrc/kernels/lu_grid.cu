@@ -52,27 +52,226 @@ __device__ __forceinline__ bool gwait(const int32_t* f, int32_t target) {
     return false;
 }
 
+// Asynchronous global -> shared copies (LDGSTS).  The 16-byte form goes
+// through L2 only (.cg), so, like ld.global.cg, it never sees a stale L1
+// line of a column another SM finished; the 4-byte form (.ca) is used only
+// for the plan's read-only index arrays.
+__device__ __forceinline__ void cp_async16_cg(void* sdst, const void* gsrc) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async4_ca(void* sdst, const void* gsrc) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(sdst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+// Wait until at most `pending` of this thread's most recent copy groups are
+// still in flight (pending < kCtaRing).
+__device__ __forceinline__ void cp_async_wait(int pending) {
+    switch (pending) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+        case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+        case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+    }
+}
+
 }  // namespace
 
-// Shared state of one grid-wide launch, zeroed by the host before it.
+// Tail columns by whole CTAs.  The last columns of an elimination (the top
+// separators) each apply hundreds to thousands of updates, and they form a
+// chain: one warp per column leaves most of the GPU idle while each tail
+// column works through its updates one L2 round trip at a time.  Columns
+// from cta_from on are instead claimed by whole CTAs: the rows of L(:, r)
+// of each update are spread over all threads, and the next kCtaRing
+// updates' L(:, r) rows (up to kCtaSlot each) and destinations are staged
+// into shared memory by cp.async as soon as warp 0 has seen their source
+// columns complete (one batched poll of several flags), so an update costs
+// two CTA barriers instead of a round trip.  Every entry still receives its
+// updates in the column's stored order, one at a time, with the same
+// operations: values are those of refactor_column.
+constexpr int kCtaRing = 8;      // updates staged ahead
+constexpr int kCtaSlot = 1024;   // rows of L(:, r) staged per update
+constexpr int kCtaBuf = 8192;    // the column's shared buffer (longer: in place in lu)
+
+struct CtaRing {
+    double val[kCtaRing][kCtaSlot + 2];  // 16-byte aligned pairs, from the aligned start
+    int32_t dst[kCtaRing][kCtaSlot];     // update map entries, or L(:, r)'s row indices
+};
+
+__host__ __device__ constexpr size_t cta_smem_bytes() {
+    return sizeof(double) * kCtaBuf + sizeof(CtaRing);
+}
+
+struct CtaShared {
+    int32_t j, nstage, timeout;
+    ColumnResult res;
+};
+
+
 struct GridState {
     int32_t next;                  // claim counter
     int32_t timeout;               // a bounded wait gave up
     int32_t growth;                // AMD-LU: a replay growth test failed
-    int32_t pad;
+    int32_t next_cta;              // claim counter of the CTA-mode tail
     unsigned long long fail_inv;   // max of ~fail_key over failing columns (0: none)
 };
 
+// Column j of an AMD-LU plan by the whole CTA (kThreads threads); buf is
+// kCtaBuf doubles of shared memory or the column's place in lu.  Same
+// result as refactor_column<true> for the same column.
+template <int kThreads>
+__device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* __restrict__ pool,
+                                            const double* __restrict__ a, double* lu,
+                                            double diag_gmin, int check_pivots, int32_t j,
+                                            double* buf, double* lrows, double* urows,
+                                            const int32_t* done, int32_t* rmap, CtaRing& ring,
+                                            CtaShared& sh) {
+    const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
+    const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
+    const int32_t* lu_src = pool + pd.off[PA_lu_src];
+    const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int32_t* row_idx = pool + pd.off[PA_row_idx];
+    const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
+    const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int32_t c0 = col_ptr[j];
+    const int32_t len = col_ptr[j + 1] - c0;
+    const int32_t dj = diag_pos[j] - c0;
+    const int32_t gp = gmin_pos[j];
+    const bool mapped = rmap == nullptr;
+    for (int32_t t = tid; t < len; t += kThreads) {
+        const int32_t s = lu_src[c0 + t];
+        double v = (s >= 0) ? a[s] : 0.0;
+        if (t == gp && diag_gmin != 0.0) v = __dadd_rn(v, diag_gmin);
+        buf[t] = v;
+        if (!mapped) rmap[row_idx[c0 + t]] = t;
+    }
+    const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]) + c0;
+    if (tid == 0) sh.timeout = 0;
+    __syncthreads();
+    // L(:, r) of update q from its 16-byte aligned start: the pair holding
+    // row l0 may begin one value early (the pivot of column r); a last value
+    // without its pair is read directly when applied.
+    auto span = [&](const int4& m, int32_t& l0, int32_t& ns, int& off) {
+        l0 = m.y + 1;
+        ns = m.z < kCtaSlot ? m.z : kCtaSlot;
+        off = static_cast<int>((reinterpret_cast<uintptr_t>(lu + l0) >> 3) & 1);
+    };
+    auto stage = [&](int32_t q) {
+        const int4 m = umeta[q];
+        const int slot = q % kCtaRing;
+        int32_t l0, ns;
+        int off;
+        span(m, l0, ns, off);
+        const double* g0 = lu + l0 - off;
+        const int32_t pairs = (off + ns) >> 1;
+        for (int32_t p = tid; p < pairs; p += kThreads)
+            cp_async16_cg(&ring.val[slot][2 * p], g0 + 2 * p);
+        const int32_t* src = mapped ? upd_dst + m.w : row_idx + l0;
+        for (int32_t k = tid; k < ns; k += kThreads) cp_async4_ca(&ring.dst[slot][k], src + k);
+        cp_async_commit();
+    };
+    double colmax = 0.0;  // the same in every thread: largest |U(r, j)| applied
+    int32_t staged = 0;   // updates whose copies are issued
+    bool timed_out = false;
+    for (int32_t q = 0; q < dj; ++q) {
+        if (staged < dj && staged - q <= kCtaRing / 2) {
+            // warp 0 polls the flags of the next updates at once and the
+            // CTA stages the prefix whose source columns are done; update
+            // q itself is waited for when nothing is staged for it
+            const int32_t want = ((dj < q + kCtaRing) ? dj : q + kCtaRing) - staged;
+            if (warp == 0) {
+                const bool ready =
+                    lane < want && gflag_acquire(done + umeta[staged + lane].x) >= 1;
+                const unsigned mask = __ballot_sync(0xffffffffu, ready);
+                int32_t nready = __ffs(~mask) - 1;
+                if (nready > want) nready = want;
+                if (nready == 0 && staged == q) {
+                    int ok = 1;
+                    if (lane == 0) ok = gwait(done + umeta[q].x, 1) ? 1 : 0;
+                    ok = __shfl_sync(0xffffffffu, ok, 0);
+                    nready = ok;
+                    if (!ok && lane == 0) sh.timeout = 1;
+                }
+                if (lane == 0) sh.nstage = nready;
+            }
+            __syncthreads();
+            if (sh.timeout) {
+                timed_out = true;
+                break;
+            }
+            const int32_t nst = sh.nstage;
+            for (int32_t i = 0; i < nst; ++i) stage(staged + i);
+            staged += nst;
+        }
+        cp_async_wait(staged - q - 1);
+        __syncthreads();
+        const int4 m = umeta[q];
+        const int slot = q % kCtaRing;
+        int32_t l0, ns;
+        int off;
+        span(m, l0, ns, off);
+        const double u = buf[q];
+        colmax = fmax(colmax, fabs(u));
+        const bool tail = ((off + ns) & 1) != 0;
+        for (int32_t k = tid; k < ns; k += kThreads) {
+            const double lv = (tail && k == ns - 1) ? __ldcg(lu + l0 + k) : ring.val[slot][off + k];
+            const int32_t d = mapped ? ring.dst[slot][k] : rmap[ring.dst[slot][k]];
+            buf[d] = lu_sub(buf[d], lu_mul(u, lv));
+        }
+        for (int32_t k = ns + tid; k < m.z; k += kThreads) {
+            const int32_t d = mapped ? upd_dst[m.w + k] : rmap[row_idx[l0 + k]];
+            buf[d] = lu_sub(buf[d], lu_mul(u, __ldcg(lu + l0 + k)));
+        }
+        __syncthreads();  // the column's new values before the next u; slot q free
+    }
+    cp_async_wait(0);
+    __syncthreads();
+    if (warp == 0) {
+        const AmdColumn v = amd_column_status(buf, dj, len, colmax, check_pivots, piv_rank[j],
+                                              gp, lane);
+        if (lane == 0) {
+            sh.res.code = v.code;
+            sh.res.growth_fail = v.growth_fail;
+        }
+    }
+    __syncthreads();
+    const ColumnResult res{sh.res.code, sh.res.growth_fail, timed_out};
+    const double piv = buf[dj];
+    const int32_t* rowcopy = pool + pd.off[PA_rowcopy_pos];
+    for (int32_t t = tid; t < len; t += kThreads) {
+        const double v = lu_store_value(true, buf[t], t, dj, piv);
+        lu[c0 + t] = v;
+        if (lrows) {
+            if (t < dj) urows[rowcopy[c0 + t]] = v;
+            else if (t > dj) lrows[rowcopy[c0 + t]] = v;
+        }
+    }
+    __syncthreads();
+    return res;
+}
+
 // kWarps warps per CTA, each with a shared column buffer of kColbuf doubles
-// (columns longer than that are eliminated in place in lu).
+// (columns longer than that are eliminated in place in lu).  Columns from
+// cta_from on (AMD-LU plans, kColbuf >= 2048) are claimed by whole CTAs
+// once all of a CTA's warps have run out of warp-mode columns; a CTA-mode
+// column waits only on columns claimed earlier, so the schedule still needs
+// no residency guarantee.
 template <int kWarps, int kColbuf>
 __global__ void __launch_bounds__(kWarps * 32)
 grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ pool,
                      const InstDesc* __restrict__ insts, int inst, const double* __restrict__ A,
                      double* LU, double diag_gmin, int check_pivots, double rel_threshold,
                      double* lrows, double* urows, int32_t* done, GridState* st,
-                     int32_t* rmaps, int64_t rmap_words) {
-    extern __shared__ double smem[];
+                     int32_t* rmaps, int64_t rmap_words, int32_t cta_from) {
+    extern __shared__ __align__(16) double smem[];  // 16-byte cp.async destinations
     const InstDesc id = insts[inst];
     const PlanDesc& pd = plans[id.plan];
     const int32_t* col_ptr = pool + pd.off[PA_col_ptr];
@@ -85,11 +284,12 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
     double* lu = LU + id.lu_off;
     double* lr = lrows ? lrows + id.lrows_off : nullptr;
     double* ur = urows ? urows + id.urows_off : nullptr;
+    const int32_t warp_end = pd.n < cta_from ? pd.n : cta_from;
     for (;;) {
         int32_t j = 0;
         if (lane == 0) j = atomicAdd(&st->next, 1);
         j = __shfl_sync(0xffffffffu, j, 0);
-        if (j >= pd.n) break;
+        if (j >= warp_end) break;
         const int32_t len = col_ptr[j + 1] - col_ptr[j];
         double* buf = (len <= kColbuf) ? sbuf : lu + col_ptr[j];
         auto probe = [&](int32_t r) { return gflag_acquire(done + r); };
@@ -105,6 +305,34 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
             gflag_release(done + j, 1);
         }
         __syncwarp();
+    }
+    if constexpr (kColbuf >= 2048) {
+        if (warp_end < pd.n) {
+            __shared__ CtaShared sh;
+            __syncthreads();
+            CtaRing& ring = *reinterpret_cast<CtaRing*>(smem + kCtaBuf);
+            int32_t* crmap =
+                rmaps ? rmaps + static_cast<int64_t>(blockIdx.x) * kWarps * rmap_words : nullptr;
+            const double* a = A + id.a_off;
+            for (;;) {
+                if (threadIdx.x == 0) sh.j = warp_end + atomicAdd(&st->next_cta, 1);
+                __syncthreads();
+                const int32_t j = sh.j;
+                if (j >= pd.n) break;
+                const int32_t len = col_ptr[j + 1] - col_ptr[j];
+                double* buf = (len <= kCtaBuf) ? smem : lu + col_ptr[j];
+                const ColumnResult c = refactor_column_cta<kWarps * 32>(
+                    pd, pool, a, lu, diag_gmin, check_pivots, j, buf, lr, ur, done, crmap, ring, sh);
+                __threadfence();
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    if (c.timed_out) atomicExch(&st->timeout, 1);
+                    else if (c.code != kStatusOk) atomicMax(&st->fail_inv, ~fail_key(j, c.code));
+                    if (c.growth_fail) atomicExch(&st->growth, 1);
+                    gflag_release(done + j, 1);
+                }
+            }
+        }
     }
 }
 
@@ -199,11 +427,20 @@ grid_solve_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict_
     if (!ok) atomicExch(&st->timeout, 1);
 }
 
+// Dynamic shared memory of a refactor variant: the warps' column buffers,
+// or the CTA-mode column buffer and staging ring if larger.
+template <int kWarps, int kColbuf>
+constexpr size_t grid_refactor_smem() {
+    return (kColbuf >= 2048 && cta_smem_bytes() > sizeof(double) * kWarps * kColbuf)
+               ? cta_smem_bytes()
+               : sizeof(double) * kWarps * kColbuf;
+}
+
 template <int kWarps, int kColbuf>
 int grid_refactor_blocks() {
     static int blocks = 0;
     if (blocks == 0) {
-        const size_t smem = sizeof(double) * kWarps * kColbuf;
+        const size_t smem = grid_refactor_smem<kWarps, kColbuf>();
         if (cudaFuncSetAttribute(grid_refactor_kernel<kWarps, kColbuf>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)) != cudaSuccess)
@@ -264,22 +501,22 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
                                  double rel_threshold, int32_t* status, int32_t* fail_step,
                                  double* lrows, double* urows, void* scratch, int colbuf,
                                  int max_col, int32_t* rmaps, int64_t rmap_words,
-                                 cudaStream_t stream) {
+                                 const int32_t* cta_from_of, cudaStream_t stream) {
     colbuf = grid_colbuf(colbuf, max_col);
     int blocks = 0, threads = 0;
     size_t smem = 0;
     if (colbuf == 1024) {
         blocks = grid_refactor_blocks<8, 1024>();
         threads = 256;
-        smem = sizeof(double) * 8 * 1024;
+        smem = grid_refactor_smem<8, 1024>();
     } else if (colbuf == 2048) {
         blocks = grid_refactor_blocks<8, 2048>();
         threads = 256;
-        smem = sizeof(double) * 8 * 2048;
+        smem = grid_refactor_smem<8, 2048>();
     } else if (colbuf == 4096) {
         blocks = grid_refactor_blocks<4, 4096>();
         threads = 128;
-        smem = sizeof(double) * 4 * 4096;
+        smem = grid_refactor_smem<4, 4096>();
     } else {
         return cudaErrorInvalidValue;
     }
@@ -294,7 +531,7 @@ cudaError_t launch_grid_refactor(const PlanDesc* plans, const int32_t* pool,
 #define NSG_GRID_REFACTOR(W, C)                                                                \
         grid_refactor_kernel<W, C><<<blocks, threads, smem, stream>>>(                         \
             plans, pool, insts, i, A, LU, diag_gmin, check_pivots, rel_threshold, lrows, urows, \
-            done, st, rmaps, rmap_words)
+            done, st, rmaps, rmap_words, colbuf >= 2048 ? cta_from_of[i] : n_of[i])
         if (colbuf == 1024) NSG_GRID_REFACTOR(8, 1024);
         else if (colbuf == 2048) NSG_GRID_REFACTOR(8, 2048);
         else NSG_GRID_REFACTOR(4, 4096);

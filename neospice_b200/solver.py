@@ -179,6 +179,11 @@ class Batch:
         2048, 4096; 0 = automatic)."""
         L.check(L.lib().nsg_batch_set_grid_buffer(self._h, int(doubles)))
 
+    def set_grid_tail(self, columns: int):
+        """Columns the grid-wide refactor hands to whole CTAs: the last
+        `columns`, 0 for none, -1 (default) for the heavy top separators."""
+        L.check(L.lib().nsg_batch_set_grid_tail(self._h, int(columns)))
+
     def refactor(self, d_values, diag_gmin=0.0, check_pivots=False, d_status=None,
                  d_fail_step=None, stream=None):
         """Batched spFactor; returns the device status tensor (int32)."""

@@ -102,3 +102,58 @@ def test_plans_without_update_map(engine, colbuf):
             DcBatch([W.power_grid(np.random.default_rng(1), 12, 6, 4).build()])
     finally:
         assert L.lib().nsg_set_update_map_limit(1 << 30) == L.NSG_OK
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built")
+@pytest.mark.parametrize("mapped", [True, False])
+@pytest.mark.parametrize("colbuf", [2048, 4096])
+def test_cta_tail_matches_reference(mapped, colbuf):
+    """The grid-wide refactor's CTA-mode tail (columns claimed by whole CTAs,
+    L(:, r) staged by cp.async): with the default tail (the columns with at
+    least 128 updates), with the last 64 and with every column, mapped and
+    map-less plans, refactorize() gives the reference AmdLuSolver's factor
+    and solution bit for bit, and numeric() (pivot re-validation on the
+    perturbed values) gives the all-warp schedule's verdict and values."""
+    from neospice_b200 import _lib as L
+    rng = np.random.default_rng(21)
+    n, cp, ri, vals = W.power_grid_transient(90)
+    ref = oracle.RefAmdLu(n, cp, ri)
+    assert ref.numeric(vals) == 0
+    vals2 = vals * np.exp(0.02 * rng.standard_normal(len(vals)))
+    assert ref.refactorize(vals2) == 0
+    b = rng.standard_normal(n)
+    x_ref = ref.solve(b)
+    f = ref.export()
+    packed = np.concatenate([np.concatenate([f["Ux"][f["Up"][k]:f["Up"][k + 1]],
+                                             f["Lx"][f["Lp"][k] + 1:f["Lp"][k + 1]]])
+                             for k in range(n)])
+    if not mapped:
+        assert L.lib().nsg_set_update_map_limit(0) == L.NSG_OK
+    try:
+        topo = Topology.order(n, cp, ri, vals, solver="amdlu")
+    finally:
+        assert L.lib().nsg_set_update_map_limit(1 << 30) == L.NSG_OK
+    d_a = torch.from_numpy(np.asarray(vals2, np.float64)).cuda()
+
+    def run(tail, check):
+        batch = Batch([topo])
+        batch.set_schedule(2)
+        batch.set_grid_buffer(colbuf)
+        batch.set_grid_tail(tail)
+        st, fs = batch.refactor(d_a, 0.0, check_pivots=check)
+        d_x = torch.from_numpy(b.copy()).cuda()
+        batch.solve(d_x)
+        torch.cuda.synchronize()
+        return (int(st.cpu()[0]), int(fs.cpu()[0]), batch.lu_values()[:len(packed)],
+                d_x.cpu().numpy())
+
+    numeric0 = run(0, True)
+    for tail in (-1, 64, n):
+        st, _, lu, x = run(tail, False)
+        assert st == 0, tail
+        np.testing.assert_array_equal(lu, packed)
+        np.testing.assert_array_equal(x, x_ref)
+        st, fs, lu, x = run(tail, True)
+        assert (st, fs) == numeric0[:2], tail
+        if st == 0:
+            np.testing.assert_array_equal(lu, numeric0[2])
