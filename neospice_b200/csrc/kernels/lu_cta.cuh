@@ -85,9 +85,56 @@ struct AmdColumn {
     bool growth_fail;
 };
 
-__device__ inline AmdColumn amd_column_status(const double* col, int32_t dj, int32_t len,
-                                              double colmax, int check, int32_t piv_rank,
-                                              int32_t gpos, int lane) {
+// The pivot candidate search of amd_column_status, split so a whole CTA can
+// run it: each thread scans positions dj + start, dj + start + stride, ...
+// and the partial results merge in any order (largest |x|, then lowest
+// rank: a total order, since ranks are distinct).
+struct AmdCand {
+    double best;
+    int32_t rank, pos;
+};
+
+__device__ __forceinline__ void amd_cand_merge(AmdCand& a, double ob, int32_t orank,
+                                               int32_t opos) {
+    if (ob > a.best || (ob == a.best && orank < a.rank)) {
+        a.best = ob;
+        a.rank = orank;
+        a.pos = opos;
+    }
+}
+
+__device__ inline AmdCand amd_cand_scan(const double* col, int32_t dj, int32_t len,
+                                        int32_t piv_rank, int start, int stride) {
+    AmdCand c{-1.0, INT32_MAX, -1};
+    for (int32_t t = dj + start; t < len; t += stride) {
+        int32_t rank;
+        if (t == dj) {
+            if (piv_rank < 0) continue;  // the pivot was not in the reach
+            rank = piv_rank;
+        } else {
+            const int32_t m = t - dj - 1;
+            rank = (piv_rank >= 0 && m >= piv_rank) ? m + 1 : m;
+        }
+        amd_cand_merge(c, fabs(col[t]), rank, t);
+    }
+    return c;
+}
+
+__device__ __forceinline__ AmdCand amd_cand_warp(AmdCand c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, c.best, o);
+        const int32_t orank = __shfl_xor_sync(0xffffffffu, c.rank, o);
+        const int32_t opos = __shfl_xor_sync(0xffffffffu, c.pos, o);
+        amd_cand_merge(c, ob, orank, opos);
+    }
+    return c;
+}
+
+// The verdict from the column's pivot, colmax and (for kCheckNumeric /
+// kCheckRefactor) the merged candidate.
+__device__ inline AmdColumn amd_verdict(const double* col, int32_t dj, double colmax, int check,
+                                        int32_t gpos, const AmdCand& c) {
     const double piv = col[dj];
     AmdColumn r{(piv == 0.0) ? kStatusSingular : kStatusOk, false};
     if (check == kCheckRefactor) {
@@ -96,43 +143,24 @@ __device__ inline AmdColumn amd_column_status(const double* col, int32_t dj, int
         r.growth_fail = (piv == 0.0 || (cm > 0.0 && a < 1e-3 * cm));
     }
     if (check == kCheckNumeric || check == kCheckRefactor) {
-        double best = -1.0;
-        int32_t best_rank = INT32_MAX, best_pos = -1;
-        for (int32_t t = dj + lane; t < len; t += 32) {
-            int32_t rank;
-            if (t == dj) {
-                if (piv_rank < 0) continue;  // the pivot was not in the reach
-                rank = piv_rank;
-            } else {
-                const int32_t m = t - dj - 1;
-                rank = (piv_rank >= 0 && m >= piv_rank) ? m + 1 : m;
-            }
-            const double v = fabs(col[t]);
-            if (v > best || (v == best && rank < best_rank)) {
-                best = v;
-                best_rank = rank;
-                best_pos = t;
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int32_t orank = __shfl_xor_sync(0xffffffffu, best_rank, o);
-            const int32_t opos = __shfl_xor_sync(0xffffffffu, best_pos, o);
-            if (ob > best || (ob == best && orank < best_rank)) {
-                best = ob;
-                best_rank = orank;
-                best_pos = opos;
-            }
-        }
-        if (best_pos < 0 || best <= 0.0) {
+        if (c.pos < 0 || c.best <= 0.0) {
             r.code = kStatusSingular;
         } else {
-            int32_t chosen = best_pos;
-            if (gpos >= dj && fabs(col[gpos]) >= best * 1e-3) chosen = gpos;
+            int32_t chosen = c.pos;
+            if (gpos >= dj && fabs(col[gpos]) >= c.best * 1e-3) chosen = gpos;
             r.code = (chosen != dj) ? kStatusReorder : (piv == 0.0 ? kStatusSingular : kStatusOk);
         }
     }
+    return r;
+}
+
+__device__ inline AmdColumn amd_column_status(const double* col, int32_t dj, int32_t len,
+                                              double colmax, int check, int32_t piv_rank,
+                                              int32_t gpos, int lane) {
+    AmdCand c{-1.0, INT32_MAX, -1};
+    if (check == kCheckNumeric || check == kCheckRefactor)
+        c = amd_cand_warp(amd_cand_scan(col, dj, len, piv_rank, lane, 32));
+    const AmdColumn r = amd_verdict(col, dj, colmax, check, gpos, c);
     __syncwarp();
     return r;
 }

@@ -112,6 +112,7 @@ __host__ __device__ constexpr size_t cta_smem_bytes() {
 struct CtaShared {
     int32_t j, nstage, timeout;
     ColumnResult res;
+    AmdCand part[32];  // per-warp pivot candidates
 };
 
 
@@ -234,13 +235,21 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
     }
     cp_async_wait(0);
     __syncthreads();
-    if (warp == 0) {
-        const AmdColumn v = amd_column_status(buf, dj, len, colmax, check_pivots, piv_rank[j],
-                                              gp, lane);
-        if (lane == 0) {
-            sh.res.code = v.code;
-            sh.res.growth_fail = v.growth_fail;
-        }
+    // amd_column_status with the candidate search spread over the CTA
+    const bool scan = check_pivots == kCheckNumeric || check_pivots == kCheckRefactor;
+    AmdCand cand{-1.0, INT32_MAX, -1};
+    if (scan) {
+        cand = amd_cand_warp(amd_cand_scan(buf, dj, len, piv_rank[j], tid, kThreads));
+        if (lane == 0) sh.part[warp] = cand;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (scan)
+            for (int w = 1; w < kThreads / 32; ++w)
+                amd_cand_merge(cand, sh.part[w].best, sh.part[w].rank, sh.part[w].pos);
+        const AmdColumn v = amd_verdict(buf, dj, colmax, check_pivots, gp, cand);
+        sh.res.code = v.code;
+        sh.res.growth_fail = v.growth_fail;
     }
     __syncthreads();
     const ColumnResult res{sh.res.code, sh.res.growth_fail, timed_out};
@@ -323,9 +332,11 @@ grid_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restri
                 double* buf = (len <= kCtaBuf) ? smem : lu + col_ptr[j];
                 const ColumnResult c = refactor_column_cta<kWarps * 32>(
                     pd, pool, a, lu, diag_gmin, check_pivots, j, buf, lr, ur, done, crmap, ring, sh);
-                __threadfence();
-                __syncthreads();
+                // refactor_column_cta ends with a CTA barrier after the
+                // column's stores; thread 0's fence then publishes them (the
+                // barrier-then-fence pattern of a grid-wide barrier)
                 if (threadIdx.x == 0) {
+                    __threadfence();
                     if (c.timed_out) atomicExch(&st->timeout, 1);
                     else if (c.code != kStatusOk) atomicMax(&st->fail_inv, ~fail_key(j, c.code));
                     if (c.growth_fail) atomicExch(&st->growth, 1);
