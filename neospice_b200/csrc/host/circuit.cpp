@@ -76,13 +76,18 @@ int32_t Circuit::add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wav
 // neutral) temperature adjustment, F1..F3 and the depletion-capacitance
 // knee, each by the reference's expression.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
-                                      double fc, double tt) {
+                                      double fc, double tt, double bv, double ibv, double nbv) {
     if (!(is > 0.0) || !(n > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
     if (!(cjo >= 0.0) || !(vj > 0.0) || !(m >= 0.0 && m < 1.0) || !(fc >= 0.0 && fc < 1.0) ||
         !(tt >= 0.0) || !std::isfinite(cjo) || !std::isfinite(vj) || !std::isfinite(tt))
         throw std::invalid_argument(
             "Circuit: diode needs CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0");
+    const bool brk = !std::isnan(bv);
+    if (std::isnan(nbv)) nbv = n;  // DIOsetup: NBV defaults to N
+    if (brk && (!(bv > 0.0) || !std::isfinite(bv) || !(ibv > 0.0) || !std::isfinite(ibv) ||
+                !(nbv > 0.0) || !std::isfinite(nbv)))
+        throw std::invalid_argument("Circuit: diode breakdown needs BV > 0, IBV > 0, NBV > 0");
     constexpr double kBoltz = 1.38064852e-23, kCharge = 1.6021766208e-19, kRefTemp = 300.15;
     const double temp = kTNominal, tnom = kTNominal, dt = temp - tnom;
     const double vtnom = kKoverQ * tnom;
@@ -124,13 +129,37 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     p[kDpF3] = f3;
     p[kDpGrad] = grad;
     p[kDpTt] = ttt;
+    // DIOtemp's breakdown voltage (dio_temp.cpp:233-270; TLEV = 0, TCV = 0,
+    // level 1, the circuit's RELTOL at its default 1e-3): the voltage at
+    // which the reverse current matches IBV, by up to 25 fixed-point steps.
+    double xbv = 0.0;
+    if (brk) {
+        const double tbv = bv - 0.0 * dt;
+        double cbv = ibv;
+        if (cbv < is * tbv / vt) {
+            cbv = is * tbv / vt;
+            xbv = tbv;
+        } else {
+            const double tol = 1e-3 * cbv;
+            xbv = tbv - nbv * vt * std::log(1 + cbv / (is));
+            for (int iter = 0; iter < 25; iter++) {
+                xbv = tbv - nbv * vt * std::log(cbv / (is) + 1 - xbv / vt);
+                const double xcbv = is * (std::exp((tbv - xbv) / (nbv * vt)) - 1 + xbv / vt);
+                if (std::fabs(xcbv - cbv) <= tol) break;
+            }
+        }
+    }
+    p[kDpBrk] = brk ? 1.0 : 0.0;
+    p[kDpTbv] = xbv;
+    p[kDpNbv] = nbv;
     return p;
 }
 
 int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
-                           double cjo, double vj, double m, double fc, double tt) {
+                           double cjo, double vj, double m, double fc, double tt, double bv,
+                           double ibv, double nbv) {
     return add_device(DevKind::Diode, anode, cathode,
-                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt));
+                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv));
 }
 
 int32_t Circuit::add_mos1_model(const Mos1Card& card) {
@@ -535,7 +564,8 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
     for (size_t d = 0; d < diodes_.size(); ++d) {
         const double csat = params_[diodes_[d].param];
         const double vte = params_[diodes_[d].param + 1] * vt;
-        const DiodeDC r = diode_dc_load(true, 0.0, 0.0, 0.0, csat, vte, diode_vcrit(vte, csat), gmin);
+        const DiodeDC r = diode_dc_load(true, 0.0, 0.0, 0.0, csat, vte, diode_vcrit(vte, csat), gmin,
+                                        diode_brk(&params_[diodes_[d].param], vt));
         double* t = &tv[diode_term_base() + kDiodeTerms * d];
         const double cdeq = r.cd - r.gd * r.vd;
         t[kDGd] = r.gd;

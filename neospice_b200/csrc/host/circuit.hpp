@@ -9,6 +9,7 @@
 // reference's devices add them, so the GPU sums every entry in the same
 // sequence of IEEE additions.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <utility>
@@ -105,11 +106,14 @@ struct Bsim4Card {
 std::vector<double> bsim4_param_block(const Bsim4Card& card, double W, double L, double delvto);
 
 // The diode parameter block (DiodeParam of kernels/diode_model.cuh) of the
-// card D(IS N CJO VJ M FC TT) at the nominal temperature: DIOtemp
-// (src/devices/dio/dio_temp.cpp:91-292).  Throws std::invalid_argument
-// outside IS > 0, N > 0, CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0.
+// card D(IS N CJO VJ M FC TT [BV IBV NBV]) at the nominal temperature:
+// DIOtemp (src/devices/dio/dio_temp.cpp:91-292).  bv NaN: no breakdown (BV
+// not given); nbv NaN: N.  Throws std::invalid_argument outside IS > 0,
+// N > 0, CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0 and, with BV,
+// BV > 0, IBV > 0, NBV > 0.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
-                                      double fc, double tt);
+                                      double fc, double tt, double bv = NAN, double ibv = 1e-3,
+                                      double nbv = NAN);
 
 class Circuit {
 public:
@@ -132,7 +136,7 @@ public:
     // (src/devices/dio/dio_setup.cpp:55-82) for the junction values.
     int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
                       double cjo = 0.0, double vj = 1.0, double m = 0.5, double fc = 0.5,
-                      double tt = 0.0);
+                      double tt = 0.0, double bv = NAN, double ibv = 1e-3, double nbv = NAN);
     // Level-1 MOSFET models and instances (Circuit::model,
     // src/core/circuit.hpp:259, and Circuit::M with W and L, :218-219).
     // Returns the model / device index.

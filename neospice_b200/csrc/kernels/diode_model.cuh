@@ -1,5 +1,5 @@
-// Load of the level-1 junction diode (RS = 0, no breakdown, no knee
-// currents, no sidewall, T = TNOM), shared by the host (first-iteration
+// Load of the level-1 junction diode (RS = 0, no knee currents, no sidewall,
+// T = TNOM; reverse breakdown when BV is given), shared by the host (first-iteration
 // values for the symbolic phase) and the GPU Newton kernels: the DC current
 // and conductance, and the depletion and diffusion charge of the transient.
 // Follows DIOload (src/devices/dio/dio_load.cpp:98-383) and DEVpnjlim
@@ -30,8 +30,22 @@ enum DiodeParam : int {
     kDpF3 = 7,      // DIOtF3
     kDpGrad = 8,    // DIOtGradingCoeff
     kDpTt = 9,      // DIOtTransitTime
-    kDiodeParams = 10
+    kDpBrk = 10,    // 1 when BV is given (DIObreakdownVoltageGiven), else 0
+    kDpTbv = 11,    // DIOtBrkdwnV (DIOtemp's breakdown voltage matched to IBV)
+    kDpNbv = 12,    // NBV (DIObrkdEmissionCoeff; N when not given)
+    kDiodeParams = 13
 };
+
+// Reverse breakdown of one diode: whether BV is given, DIOtBrkdwnV and
+// vtebrk = NBV * vt.
+struct DiodeBrk {
+    bool on;
+    double tbv, vtebrk;
+};
+
+NSG_HD inline DiodeBrk diode_brk(const double* p, double vt) {
+    return DiodeBrk{p[kDpBrk] != 0.0, p[kDpTbv], p[kDpNbv] * vt};
+}
 
 // Diode state slots (src/devices/dio/dio_def.hpp:160-164).
 enum DiodeState : int {
@@ -77,18 +91,33 @@ struct DiodeDC {
 
 // Current and conductance at the junction voltage vd, limited against
 // vd_old by DEVpnjlim when `limit` (every mode but the junction
-// initialisation and MODEINITTRAN).  csat = area-scaled saturation current
-// at T, vte = N*vt, tvcrit = Vcrit.
+// initialisation and MODEINITTRAN; in the breakdown region the limiting
+// acts on -(vd + tBrkdwnV) with vtebrk, dio_load.cpp:158-168).  csat =
+// area-scaled saturation current at T, vte = N*vt, tvcrit = Vcrit.
 NSG_HD inline DiodeDC diode_eval(double vd, bool limit, double vd_old, double csat, double vte,
-                                 double tvcrit, double gmin) {
+                                 double tvcrit, double gmin,
+                                 const DiodeBrk& bk = DiodeBrk{false, 0.0, 0.0}) {
     DiodeDC r;
     r.check = 1;
-    if (limit) vd = pnjlim(vd, vd_old, vte, tvcrit, &r.check);
+    if (limit) {
+        const double knee = -bk.tbv + 10 * bk.vtebrk;
+        if (bk.on && vd < ((0 < knee) ? 0 : knee)) {  // MIN(0, -tBrkdwnV + 10 vtebrk)
+            double vdtemp = -(vd + bk.tbv);
+            vdtemp = pnjlim(vdtemp, -(vd_old + bk.tbv), bk.vtebrk, tvcrit, &r.check);
+            vd = -(vdtemp + bk.tbv);
+        } else {
+            vd = pnjlim(vd, vd_old, vte, tvcrit, &r.check);
+        }
+    }
     double cd, gd;
     if (vd >= -3 * vte) {
         const double evd = exp(vd / vte);
         cd = csat * (evd - 1);
         gd = csat * evd / vte;
+    } else if (bk.on && !(vd >= -bk.tbv)) {  // breakdown
+        const double evrev = exp(-(bk.tbv + vd) / bk.vtebrk);
+        cd = -csat * evrev;
+        gd = csat * evrev / bk.vtebrk;
     } else {
         double arg = 3 * vte / (vd * 2.7182818284590452354);
         arg = arg * arg * arg;
@@ -110,8 +139,10 @@ NSG_HD inline DiodeDC diode_eval(double vd, bool limit, double vd_old, double cs
 // The DC operating-point load: Vcrit at MODEINITJCT, else the node voltages
 // limited against the previous junction voltage.
 NSG_HD inline DiodeDC diode_dc_load(bool initjct, double v_pos, double v_neg, double vd_old,
-                                    double csat, double vte, double tvcrit, double gmin) {
-    return diode_eval(initjct ? tvcrit : v_pos - v_neg, !initjct, vd_old, csat, vte, tvcrit, gmin);
+                                    double csat, double vte, double tvcrit, double gmin,
+                                    const DiodeBrk& bk = DiodeBrk{false, 0.0, 0.0}) {
+    return diode_eval(initjct ? tvcrit : v_pos - v_neg, !initjct, vd_old, csat, vte, tvcrit, gmin,
+                      bk);
 }
 
 // Junction charge and capacitance of the charge-storage block of DIOload

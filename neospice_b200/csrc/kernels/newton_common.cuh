@@ -212,7 +212,8 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
             limit = true;
         }
         const DiodeDC r = diode_eval(vd, limit, s0[kDsV], v.dconst[3 * k], v.dconst[3 * k + 1],
-                                     v.dconst[3 * k + 2], opt.gmin);
+                                     v.dconst[3 * k + 2], opt.gmin,
+                                     diode_brk(v.par + dr[2], kKoverQTimesTnom));
         double cd = r.cd, gd = r.gd;
         if (charges) {  // charge storage (dio_load.cpp:309-373)
             double charge, capd;

@@ -102,8 +102,9 @@ __device__ inline void grad_contract(const Inst& v, const DcDesc& d, const int32
 // limiting: vd is the voltage its last load used).
 __device__ inline double diode_capd(const Inst& v, int32_t k, double vd, double gmin) {
     const int32_t* dr = v.diodes + 4 * k;
-    const DiodeDC r = diode_eval(vd, false, vd, v.dconst[3 * k], v.dconst[3 * k + 1],
-                                 v.dconst[3 * k + 2], gmin);
+    const DiodeDC r =
+        diode_eval(vd, false, vd, v.dconst[3 * k], v.dconst[3 * k + 1], v.dconst[3 * k + 2], gmin,
+                   diode_brk(v.par + dr[2], kKoverQTimesTnom));
     double q, capd;
     diode_charge(v.par + dr[2], r.vd, r.cdb, r.gdb, &q, &capd);
     return capd;

@@ -517,9 +517,15 @@ static void build_from_desc(Circuit& ckt, const char* desc) {
                 else static_cast<ISource*>(d)->set_pwl(pw);
             }
         } else if (kind == "D") {
-            // D a k IS N [CJO VJ M FC TT]
+            // D a k IS N [CJO VJ M FC TT [BV IBV NBV]]
             char card[400];
-            if (tk.size() > 5)
+            if (tk.size() > 10)
+                std::snprintf(card, sizeof card,
+                              ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g FC=%.17g "
+                              "TT=%.17g BV=%.17g IBV=%.17g NBV=%.17g)",
+                              dev, D_(3), D_(4), D_(5), D_(6), D_(7), D_(8), D_(9), D_(10), D_(11),
+                              D_(12));
+            else if (tk.size() > 5)
                 std::snprintf(card, sizeof card,
                               ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g FC=%.17g "
                               "TT=%.17g)",

@@ -137,9 +137,27 @@ def test_diode_param_block():
     d = diode_params()
     assert d[2] == 0.0 and d[9] == 0.0
     for bad in (dict(CJO=-1e-12), dict(VJ=0.0), dict(M=1.0), dict(FC=1.0), dict(TT=-1e-9),
-                dict(IS=0.0)):
+                dict(IS=0.0), dict(BV=-5.0), dict(BV=5.0, IBV=0.0), dict(BV=5.0, NBV=0.0)):
         with pytest.raises(L.NsgError):
             diode_params(**bad)
+
+
+def test_diode_breakdown_param_block():
+    """DIOtemp's breakdown voltage: without BV the block says so; with BV
+    the voltage is where the reverse current matches IBV to the loop's
+    exit tolerance (RELTOL 1e-3 of IBV), NBV defaults to N, and an IBV below
+    IS*BV/vt keeps BV itself."""
+    from neospice_b200.circuit import diode_params
+    vt = 1.38064852e-23 / 1.6021766208e-19 * 300.15
+    assert diode_params()[10] == 0.0
+    p = diode_params(1e-14, 1.2, BV=5.1, IBV=1e-3)
+    assert p[10] == 1.0 and p[12] == 1.2
+    xbv = p[11]
+    assert 4.0 < xbv < 5.1
+    xcbv = 1e-14 * (np.exp((5.1 - xbv) / (1.2 * vt)) - 1 + xbv / vt)
+    assert abs(xcbv - 1e-3) <= 1e-3 * 1e-3
+    q = diode_params(1e-6, 1.0, BV=50.0, IBV=1e-9, NBV=2.0)
+    assert q[11] == 50.0 and q[12] == 2.0
 
 
 def test_tran_batch_rejects_bad_probes():
@@ -217,8 +235,8 @@ def test_device_methods_return_parameter_index():
     assert c.V(0, -1, 1.0) == 3
     assert c.VPULSE(2, -1, 0.0, 1.0, 1e-9) == 4
     assert c.D(2, -1) == 11
-    assert c.I(-1, 1, 1e-3) == 21
+    assert c.I(-1, 1, 1e-3) == 24  # a diode holds 13 values
     c.finalize()
     p = c.params()
-    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[21] == 1e-3
-    assert c.param_count() == len(p) == 22
+    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[24] == 1e-3
+    assert c.param_count() == len(p) == 25
