@@ -263,8 +263,10 @@ int nsg_batch_lu_to_host(const nsg_batch* batch, double* out);
  * ngspice load order, branch unknowns after the nodes, sparsity pattern,
  * dead-node placeholders.  Parameters are kept in creation order: resistor
  * {ohms}, capacitor {farads, ic}, DC source {value}, PULSE source {v1, v2,
- * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode: the 13
- * values of nsg_diode_param_block. */
+ * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode: the 14
+ * values of nsg_diode_param_block.  A diode with RS gets an internal node
+ * (posPrime) after the external nodes, in load order, as DIOsetup's
+ * CKTmkVolt does; nsg_circuit_info's node count includes it. */
 typedef struct nsg_circuit nsg_circuit;
 
 #define NSG_WAVE_DC 0
@@ -290,22 +292,26 @@ int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, dou
 int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is,
                                double n_emission, double cjo, double vj, double m, double fc,
                                double tt);
-/* The same with reverse breakdown: the card D(IS N CJO VJ M FC TT BV IBV
- * NBV).  bv NaN means BV not given (no breakdown region); nbv NaN means N
- * (DIOsetup's default); the reference's IBV default is 1e-3.  With BV,
- * requires BV > 0, IBV > 0, NBV > 0.  The load follows DIOload's breakdown
- * limiting and current (src/devices/dio/dio_load.cpp:158-168, :232-258). */
-int nsg_circuit_add_diode_card_bv(nsg_circuit* c, int anode, int cathode, double is,
+/* The same with reverse breakdown and series resistance: the card D(IS N
+ * CJO VJ M FC TT BV IBV NBV RS).  bv NaN means BV not given (no breakdown
+ * region); nbv NaN means N (DIOsetup's default); the reference's IBV
+ * default is 1e-3; rs 0 means no series resistance.  With BV, requires
+ * BV > 0, IBV > 0, NBV > 0; RS >= 0.  The load follows DIOload's breakdown
+ * limiting and current (src/devices/dio/dio_load.cpp:158-168, :232-258)
+ * and its series-conductance stamps between pos and the internal posPrime
+ * (DIOsetup, dio_setup.cpp:232-266). */
+int nsg_circuit_add_diode_card_ex(nsg_circuit* c, int anode, int cathode, double is,
                                   double n_emission, double cjo, double vj, double m, double fc,
-                                  double tt, double bv, double ibv, double nbv);
-/* The diode parameter block of a card (13 doubles into out): IS, N, then
+                                  double tt, double bv, double ibv, double nbv, double rs);
+/* The diode parameter block of a card (14 doubles into out): IS, N, then
  * DIOtemp's junction capacitance, junction potential, depletion knee FC*VJ,
  * F1, F2, F3, grading coefficient and transit time at T = TNOM
  * (src/devices/dio/dio_temp.cpp:91-292), then 1/0 for BV given, DIOtemp's
  * breakdown voltage matched to IBV (dio_temp.cpp:233-270, the circuit's
- * RELTOL at its default 1e-3) and NBV.  bv NaN: no breakdown. */
+ * RELTOL at its default 1e-3), NBV and RS.  bv NaN: no breakdown. */
 int nsg_diode_param_block(double is, double n_emission, double cjo, double vj, double m,
-                          double fc, double tt, double bv, double ibv, double nbv, double* out);
+                          double fc, double tt, double bv, double ibv, double nbv, double rs,
+                          double* out);
 /* Circuit::C (src/core/circuit.hpp:180) with an optional IC= value
  * (has_ic != 0). */
 int nsg_circuit_add_capacitor(nsg_circuit* c, int a, int b, double farads, int has_ic,

@@ -85,10 +85,11 @@ SIGNATURES = {
     "nsg_circuit_add_diode_card": (c_int, [c_void_p, c_int, c_int, c_double, c_double, c_double,
                                            c_double, c_double, c_double, c_double]),
     "nsg_diode_param_block": (c_int, [c_double, c_double, c_double, c_double, c_double, c_double,
-                                      c_double, c_double, c_double, c_double, P(c_double)]),
-    "nsg_circuit_add_diode_card_bv": (c_int, [c_void_p, c_int, c_int, c_double, c_double,
+                                      c_double, c_double, c_double, c_double, c_double,
+                                      P(c_double)]),
+    "nsg_circuit_add_diode_card_ex": (c_int, [c_void_p, c_int, c_int, c_double, c_double,
                                               c_double, c_double, c_double, c_double, c_double,
-                                              c_double, c_double, c_double]),
+                                              c_double, c_double, c_double, c_double]),
     "nsg_circuit_add_resistors": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
     "nsg_circuit_add_isources": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double)]),
     "nsg_circuit_add_diodes": (c_int, [c_void_p, c_int, P(c_int), P(c_int), P(c_double),

@@ -28,16 +28,16 @@ AIDS = {"direct": 0, "source": 1, "gain": 2, "ptc": 3}
 
 def diode_params(IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0, VJ: float = 1.0,
                  M: float = 0.5, FC: float = 0.5, TT: float = 0.0, BV: float | None = None,
-                 IBV: float = 1e-3, NBV: float | None = None) -> np.ndarray:
-    """The 13-value parameter block a diode with this card holds in
+                 IBV: float = 1e-3, NBV: float | None = None, RS: float = 0.0) -> np.ndarray:
+    """The 14-value parameter block a diode with this card holds in
     Circuit.params(): IS, N, then the junction values at the nominal
-    temperature, then the breakdown flag, DIOtemp's breakdown voltage and
-    NBV (nsg_diode_param_block)."""
-    out = np.zeros(13, np.float64)
+    temperature, then the breakdown flag, DIOtemp's breakdown voltage, NBV
+    and RS (nsg_diode_param_block)."""
+    out = np.zeros(14, np.float64)
     L.check(L.lib().nsg_diode_param_block(float(IS), float(N), float(CJO), float(VJ), float(M),
                                           float(FC), float(TT),
                                           float("nan") if BV is None else float(BV), float(IBV),
-                                          float("nan") if NBV is None else float(NBV),
+                                          float("nan") if NBV is None else float(NBV), float(RS),
                                           L.dptr(out)))
     return out
 
@@ -78,20 +78,23 @@ class Circuit:
 
     def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0,
           VJ: float = 1.0, M: float = 0.5, FC: float = 0.5, TT: float = 0.0,
-          BV: float | None = None, IBV: float = 1e-3, NBV: float | None = None):
-        """Level-1 diode with the card D(IS N CJO VJ M FC TT [BV IBV NBV]);
-        the junction capacitance and transit time act in the transient, BV
-        (when given) adds the reverse breakdown region."""
+          BV: float | None = None, IBV: float = 1e-3, NBV: float | None = None,
+          RS: float = 0.0):
+        """Level-1 diode with the card D(IS N CJO VJ M FC TT [BV IBV NBV]
+        [RS]); the junction capacitance and transit time act in the
+        transient, BV (when given) adds the reverse breakdown region, RS > 0
+        a series resistance through an internal node."""
         first = self.param_count()
-        if BV is None:
+        if BV is None and RS == 0.0:
             L.check(L.lib().nsg_circuit_add_diode_card(self._h, int(anode), int(cathode),
                                                        float(IS), float(N), float(CJO), float(VJ),
                                                        float(M), float(FC), float(TT)))
         else:
-            L.check(L.lib().nsg_circuit_add_diode_card_bv(
+            nan = float("nan")
+            L.check(L.lib().nsg_circuit_add_diode_card_ex(
                 self._h, int(anode), int(cathode), float(IS), float(N), float(CJO), float(VJ),
-                float(M), float(FC), float(TT), float(BV), float(IBV),
-                float("nan") if NBV is None else float(NBV)))
+                float(M), float(FC), float(TT), nan if BV is None else float(BV), float(IBV),
+                nan if NBV is None else float(NBV), float(RS)))
         return first
 
     def C(self, a: int, b: int, farads: float, ic: float | None = None):

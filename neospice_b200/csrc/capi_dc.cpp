@@ -230,22 +230,23 @@ int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is
     });
 }
 
-int nsg_circuit_add_diode_card_bv(nsg_circuit* c, int anode, int cathode, double is,
+int nsg_circuit_add_diode_card_ex(nsg_circuit* c, int anode, int cathode, double is,
                                   double n_emission, double cjo, double vj, double m, double fc,
-                                  double tt, double bv, double ibv, double nbv) {
-    return guarded("nsg_circuit_add_diode_card_bv", [&]() -> int {
+                                  double tt, double bv, double ibv, double nbv, double rs) {
+    return guarded("nsg_circuit_add_diode_card_ex", [&]() -> int {
         if (!c) return fail(NSG_ERR_INVALID, "null circuit");
-        c->c.add_diode(anode, cathode, is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv);
+        c->c.add_diode(anode, cathode, is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv, rs);
         return NSG_OK;
     });
 }
 
 int nsg_diode_param_block(double is, double n_emission, double cjo, double vj, double m,
-                          double fc, double tt, double bv, double ibv, double nbv, double* out) {
+                          double fc, double tt, double bv, double ibv, double nbv, double rs,
+                          double* out) {
     return guarded("nsg_diode_param_block", [&]() -> int {
         if (!out) return fail(NSG_ERR_INVALID, "nsg_diode_param_block: null out");
         const std::vector<double> p =
-            nsg::diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv);
+            nsg::diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv, rs);
         std::copy(p.begin(), p.end(), out);
         return NSG_OK;
     });

@@ -76,7 +76,8 @@ int32_t Circuit::add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wav
 // neutral) temperature adjustment, F1..F3 and the depletion-capacitance
 // knee, each by the reference's expression.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
-                                      double fc, double tt, double bv, double ibv, double nbv) {
+                                      double fc, double tt, double bv, double ibv, double nbv,
+                                      double rs) {
     if (!(is > 0.0) || !(n > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
     if (!(cjo >= 0.0) || !(vj > 0.0) || !(m >= 0.0 && m < 1.0) || !(fc >= 0.0 && fc < 1.0) ||
@@ -88,6 +89,8 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     if (brk && (!(bv > 0.0) || !std::isfinite(bv) || !(ibv > 0.0) || !std::isfinite(ibv) ||
                 !(nbv > 0.0) || !std::isfinite(nbv)))
         throw std::invalid_argument("Circuit: diode breakdown needs BV > 0, IBV > 0, NBV > 0");
+    if (!(rs >= 0.0) || !std::isfinite(rs))
+        throw std::invalid_argument("Circuit: diode needs RS >= 0");
     constexpr double kBoltz = 1.38064852e-23, kCharge = 1.6021766208e-19, kRefTemp = 300.15;
     const double temp = kTNominal, tnom = kTNominal, dt = temp - tnom;
     const double vtnom = kKoverQ * tnom;
@@ -152,14 +155,15 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     p[kDpBrk] = brk ? 1.0 : 0.0;
     p[kDpTbv] = xbv;
     p[kDpNbv] = nbv;
+    p[kDpRs] = rs;
     return p;
 }
 
 int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
                            double cjo, double vj, double m, double fc, double tt, double bv,
-                           double ibv, double nbv) {
+                           double ibv, double nbv, double rs) {
     return add_device(DevKind::Diode, anode, cathode,
-                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv));
+                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv, rs));
 }
 
 int32_t Circuit::add_mos1_model(const Mos1Card& card) {
@@ -229,8 +233,14 @@ void Circuit::finalize() {
         return x.created > y.created;
     });
 
-    // Branch unknowns follow all node unknowns, in load order.
+    // Internal nodes, in load order after the external nodes (each device's
+    // declare_internal_nodes, src/core/circuit.cpp:205-211): a diode with
+    // RS gets posPrime (DIOsetup's CKTmkVolt).  Branch unknowns follow all
+    // node unknowns, in load order.
     int32_t next = num_nodes_;
+    for (auto& d : order)
+        if (d.kind == DevKind::Diode && params_[d.param + kDpRs] != 0.0) d.prime = next++;
+    num_internal_ = next - num_nodes_;
     for (auto& d : order)
         if (d.kind == DevKind::VSource) d.branch = next++;
     num_vars_ = next;
@@ -250,8 +260,14 @@ void Circuit::finalize() {
             case DevKind::VSource:
                 stamp(d.a, d.branch); stamp(d.b, d.branch); stamp(d.branch, d.a); stamp(d.branch, d.b);
                 break;
-            case DevKind::Diode:  // pos == posPrime (RS = 0)
-                stamp(d.a, d.a); stamp(d.b, d.a); stamp(d.a, d.b); stamp(d.b, d.b);
+            case DevKind::Diode:
+                if (d.prime < 0) {  // pos == posPrime (RS = 0)
+                    stamp(d.a, d.a); stamp(d.b, d.a); stamp(d.a, d.b); stamp(d.b, d.b);
+                } else {  // DIOsetup's TSTALLOC list
+                    const int32_t P = d.a, N = d.b, Pp = d.prime;
+                    stamp(P, Pp); stamp(N, Pp); stamp(Pp, P); stamp(Pp, N);
+                    stamp(P, P); stamp(N, N); stamp(Pp, Pp);
+                }
                 break;
             case DevKind::ISource:
                 break;
@@ -276,7 +292,7 @@ void Circuit::finalize() {
     std::vector<char> touched(num_vars_, 0);
     for (const auto& [c, r] : ent) touched[r] = touched[c] = 1;
     dead_nodes_.clear();
-    for (int32_t i = 0; i < num_nodes_; ++i)
+    for (int32_t i = 0; i < num_nodes(); ++i)
         if (!touched[i]) {
             ent.emplace_back(i, i);
             dead_nodes_.push_back(i);
@@ -312,7 +328,7 @@ void Circuit::finalize() {
             state += b4 ? kB4States : kMosStates;
         } else if (d.kind == DevKind::Diode) {
             index_in_table[k] = static_cast<int32_t>(diodes_.size());
-            diodes_.push_back({d.a, d.b, d.param, state});
+            diodes_.push_back({d.prime >= 0 ? d.prime : d.a, d.b, d.param, state});
             state += kDiodeStates;
         } else if (d.kind == DevKind::Capacitor) {
             index_in_table[k] = static_cast<int32_t>(caps_.size());
@@ -397,18 +413,26 @@ void Circuit::finalize() {
                 if (d.b >= 0) rhs[d.b].push_back(cap_term(id, kCCeq));
                 break;
             case DevKind::Diode: {
+                const int32_t P = d.a, N = d.b, Pp = d.prime >= 0 ? d.prime : d.a;
                 // rhs (UCB array): neg += cdeq, posPrime -= cdeq
-                if (d.b >= 0) ucb[d.b].push_back(diode_term(id, kDCdeq));
-                if (d.a >= 0) ucb[d.a].push_back(diode_term(id, kDNegCdeq));
-                // matrix, in DIOload's order
-                const int32_t zero = konst(kTermZero, -1), mzero = konst(kTermMinusZero, -1);
-                add_slot(d.a, d.a, zero);                          // PosPos += gspr
-                add_slot(d.b, d.b, diode_term(id, kDGd));          // NegNeg += gd
-                add_slot(d.a, d.a, diode_term(id, kDGdPlusGspr));  // PosPrimePosPrime += gd + gspr
-                add_slot(d.a, d.a, mzero);                         // PosPosPrime -= gspr
-                add_slot(d.b, d.a, diode_term(id, kDNegGd));       // NegPosPrime -= gd
-                add_slot(d.a, d.a, mzero);                         // PosPrimePos -= gspr
-                add_slot(d.a, d.b, diode_term(id, kDNegGd));       // PosPrimeNeg -= gd
+                if (N >= 0) ucb[N].push_back(diode_term(id, kDCdeq));
+                if (Pp >= 0) ucb[Pp].push_back(diode_term(id, kDNegCdeq));
+                // matrix, in DIOload's order; gspr = 1 / RS (0.0 without RS)
+                int32_t gspr, mgspr;
+                if (d.prime >= 0) {
+                    gspr = konst(kTermRecip, d.param + kDpRs);
+                    mgspr = konst(kTermNegRecip, d.param + kDpRs);
+                } else {
+                    gspr = konst(kTermZero, -1);
+                    mgspr = konst(kTermMinusZero, -1);
+                }
+                add_slot(P, P, gspr);                              // PosPos += gspr
+                add_slot(N, N, diode_term(id, kDGd));              // NegNeg += gd
+                add_slot(Pp, Pp, diode_term(id, kDGdPlusGspr));    // PosPrimePosPrime += gd + gspr
+                add_slot(P, Pp, mgspr);                            // PosPosPrime -= gspr
+                add_slot(N, Pp, diode_term(id, kDNegGd));          // NegPosPrime -= gd
+                add_slot(Pp, P, mgspr);                            // PosPrimePos -= gspr
+                add_slot(Pp, N, diode_term(id, kDNegGd));          // PosPrimeNeg -= gd
                 break;
             }
             case DevKind::ISource:
@@ -569,7 +593,7 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
         double* t = &tv[diode_term_base() + kDiodeTerms * d];
         const double cdeq = r.cd - r.gd * r.vd;
         t[kDGd] = r.gd;
-        t[kDGdPlusGspr] = r.gd + 0.0;
+        t[kDGdPlusGspr] = r.gd + diode_gspr(&params_[diodes_[d].param]);
         t[kDNegGd] = -r.gd;
         t[kDCdeq] = cdeq;
         t[kDNegCdeq] = -cdeq;

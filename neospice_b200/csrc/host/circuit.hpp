@@ -74,6 +74,7 @@ struct DeviceRec {
     int32_t branch;    // VSource branch unknown, else -1
     Wave wave;         // sources
     bool has_ic;       // capacitors
+    int32_t prime = -1;  // diode with RS: its internal node posPrime (assigned at finalize)
 };
 
 // A level-1 MOSFET model card: the type (+1 NMOS, -1 PMOS) and the given
@@ -106,14 +107,15 @@ struct Bsim4Card {
 std::vector<double> bsim4_param_block(const Bsim4Card& card, double W, double L, double delvto);
 
 // The diode parameter block (DiodeParam of kernels/diode_model.cuh) of the
-// card D(IS N CJO VJ M FC TT [BV IBV NBV]) at the nominal temperature:
+// card D(IS N CJO VJ M FC TT [BV IBV NBV] [RS]) at the nominal temperature:
 // DIOtemp (src/devices/dio/dio_temp.cpp:91-292).  bv NaN: no breakdown (BV
-// not given); nbv NaN: N.  Throws std::invalid_argument outside IS > 0,
-// N > 0, CJO >= 0, VJ > 0, 0 <= M < 1, 0 <= FC < 1, TT >= 0 and, with BV,
-// BV > 0, IBV > 0, NBV > 0.
+// not given); nbv NaN: N; rs 0: no series resistance.  Throws
+// std::invalid_argument outside IS > 0, N > 0, CJO >= 0, VJ > 0,
+// 0 <= M < 1, 0 <= FC < 1, TT >= 0, RS >= 0 and, with BV, BV > 0, IBV > 0,
+// NBV > 0.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
                                       double fc, double tt, double bv = NAN, double ibv = 1e-3,
-                                      double nbv = NAN);
+                                      double nbv = NAN, double rs = 0.0);
 
 class Circuit {
 public:
@@ -136,7 +138,8 @@ public:
     // (src/devices/dio/dio_setup.cpp:55-82) for the junction values.
     int32_t add_diode(int32_t anode, int32_t cathode, double is, double n_emission,
                       double cjo = 0.0, double vj = 1.0, double m = 0.5, double fc = 0.5,
-                      double tt = 0.0, double bv = NAN, double ibv = 1e-3, double nbv = NAN);
+                      double tt = 0.0, double bv = NAN, double ibv = 1e-3, double nbv = NAN,
+                      double rs = 0.0);
     // Level-1 MOSFET models and instances (Circuit::model,
     // src/core/circuit.hpp:259, and Circuit::M with W and L, :218-219).
     // Returns the model / device index.
@@ -158,7 +161,9 @@ public:
     // Whether any MOSFET is a BSIM4v7 instance (always charge-storing).
     bool has_bsim4() const;
 
-    int32_t num_nodes() const { return num_nodes_; }
+    // Node unknowns: the external nodes, then (after finalize) the devices'
+    // internal nodes, as the reference's Circuit::num_nodes counts them.
+    int32_t num_nodes() const { return num_nodes_ + num_internal_; }
     int32_t num_vars() const { return num_vars_; }
     int32_t nnz() const { return static_cast<int32_t>(row_idx_.size()); }
     const std::vector<int32_t>& col_ptr() const { return col_ptr_; }
@@ -234,6 +239,7 @@ public:
 
 private:
     int32_t num_nodes_;
+    int32_t num_internal_ = 0;
     int32_t num_vars_ = 0;
     bool finalized_ = false;
     std::vector<DeviceRec> devices_;

@@ -1,5 +1,6 @@
-// Load of the level-1 junction diode (RS = 0, no knee currents, no sidewall,
-// T = TNOM; reverse breakdown when BV is given), shared by the host (first-iteration
+// Load of the level-1 junction diode (no knee currents, no sidewall,
+// T = TNOM; series resistance RS through an internal node, reverse
+// breakdown when BV is given), shared by the host (first-iteration
 // values for the symbolic phase) and the GPU Newton kernels: the DC current
 // and conductance, and the depletion and diffusion charge of the transient.
 // Follows DIOload (src/devices/dio/dio_load.cpp:98-383) and DEVpnjlim
@@ -33,8 +34,15 @@ enum DiodeParam : int {
     kDpBrk = 10,    // 1 when BV is given (DIObreakdownVoltageGiven), else 0
     kDpTbv = 11,    // DIOtBrkdwnV (DIOtemp's breakdown voltage matched to IBV)
     kDpNbv = 12,    // NBV (DIObrkdEmissionCoeff; N when not given)
-    kDiodeParams = 13
+    kDpRs = 13,     // RS (0: no series resistance, posPrime == pos)
+    kDiodeParams = 14
 };
+
+// Series conductance gspr = DIOtConductance * area of DIOtemp at T = TNOM
+// (1 / RS, divided by the unit temperature factor; 0 without RS).
+NSG_HD inline double diode_gspr(const double* p) {
+    return p[kDpRs] != 0.0 ? (1 / p[kDpRs]) / 1.0 * 1.0 : 0.0;
+}
 
 // Reverse breakdown of one diode: whether BV is given, DIOtBrkdwnV and
 // vtebrk = NBV * vt.

@@ -233,7 +233,7 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
         const double cdeq = cd - gd * r.vd;
         double* t = tv_d + kDiodeTermCount * k;
         t[0] = gd;
-        t[1] = gd + 0.0;
+        t[1] = gd + diode_gspr(v.par + dr[2]);
         t[2] = -gd;
         t[3] = cdeq;
         t[4] = -cdeq;

@@ -517,15 +517,20 @@ static void build_from_desc(Circuit& ckt, const char* desc) {
                 else static_cast<ISource*>(d)->set_pwl(pw);
             }
         } else if (kind == "D") {
-            // D a k IS N [CJO VJ M FC TT [BV IBV NBV]]
+            // D a k IS N [CJO VJ M FC TT [BV IBV NBV [RS]]]; BV nan: not given
             char card[400];
-            if (tk.size() > 10)
-                std::snprintf(card, sizeof card,
-                              ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g FC=%.17g "
-                              "TT=%.17g BV=%.17g IBV=%.17g NBV=%.17g)",
-                              dev, D_(3), D_(4), D_(5), D_(6), D_(7), D_(8), D_(9), D_(10), D_(11),
-                              D_(12));
-            else if (tk.size() > 5)
+            if (tk.size() > 10) {
+                int w = std::snprintf(card, sizeof card,
+                                      ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g "
+                                      "FC=%.17g TT=%.17g",
+                                      dev, D_(3), D_(4), D_(5), D_(6), D_(7), D_(8), D_(9));
+                if (!std::isnan(D_(10)))
+                    w += std::snprintf(card + w, sizeof card - w, " BV=%.17g IBV=%.17g NBV=%.17g",
+                                       D_(10), D_(11), D_(12));
+                if (tk.size() > 13 && D_(13) != 0.0)
+                    w += std::snprintf(card + w, sizeof card - w, " RS=%.17g", D_(13));
+                std::snprintf(card + w, sizeof card - w, ")");
+            } else if (tk.size() > 5)
                 std::snprintf(card, sizeof card,
                               ".model dm%d D(IS=%.17g N=%.17g CJO=%.17g VJ=%.17g M=%.17g FC=%.17g "
                               "TT=%.17g)",

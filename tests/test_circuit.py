@@ -4,6 +4,7 @@ import numpy as np
 import pytest
 
 import golden_cases
+import netlists
 import oracle
 from neospice_b200 import _lib as L
 from neospice_b200 import workloads
@@ -235,8 +236,59 @@ def test_device_methods_return_parameter_index():
     assert c.V(0, -1, 1.0) == 3
     assert c.VPULSE(2, -1, 0.0, 1.0, 1e-9) == 4
     assert c.D(2, -1) == 11
-    assert c.I(-1, 1, 1e-3) == 24  # a diode holds 13 values
+    assert c.I(-1, 1, 1e-3) == 25  # a diode holds 14 values
     c.finalize()
     p = c.params()
-    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[24] == 1e-3
-    assert c.param_count() == len(p) == 25
+    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[25] == 1e-3
+    assert c.param_count() == len(p) == 26
+
+
+def _diode_netlists():
+    """Diode networks with series resistance (internal posPrime nodes),
+    breakdown and plain diodes mixed with sources, resistors and capacitors,
+    in varied creation orders."""
+    from neospice_b200.workloads import Netlist
+    nan = float("nan")
+    out = []
+    for k in range(6):
+        rng = np.random.default_rng([77, k])
+        devs = [("V", 0, -1, float(rng.uniform(1, 10)))]
+        for i in range(1, 5):
+            devs.append(("R", int(rng.integers(0, i)), i, float(10 ** rng.uniform(1, 4))))
+            rs = float(10 ** rng.uniform(-1, 2)) if rng.random() < 0.6 else 0.0
+            bv = float(rng.uniform(3, 8)) if rng.random() < 0.5 else nan
+            a, b = (i, -1) if rng.random() < 0.5 else (-1, i)
+            devs.append(("D", a, b, 1e-14, 1.2, 1e-12, 0.8, 0.4, 0.5, 1e-9, bv, 1e-3, 1.3, rs))
+            if rng.random() < 0.4:
+                devs.append(("C", i, -1, 1e-12))
+        out.append(Netlist(5, devs, {}))
+    return out
+
+
+@pytest.mark.skipif(not oracle.have_ref(), reason="reference library not built")
+@pytest.mark.parametrize("k", range(6))
+def test_diode_series_resistance_first_matrix_bitwise(k):
+    """Diodes with RS get the reference's internal node numbering (after the
+    external nodes, in load order, before the branch unknowns) and DIOload's
+    series-conductance stamps: pattern, first DC matrix and rhs equal the
+    reference's bit for bit."""
+    nl = _diode_netlists()[k]
+    c = nl.build()
+    cp, ri = c.pattern()
+    a, rhs = c.initial_matrix(1e-12)
+    rcp, rri, ra, rrhs = oracle.ref_sim_initjct(netlists.ref_desc(nl))
+    np.testing.assert_array_equal(cp, rcp)
+    np.testing.assert_array_equal(ri, rri)
+    np.testing.assert_array_equal(a, ra)
+    np.testing.assert_array_equal(rhs, rrhs)
+    n_rs = sum(1 for d in nl.devices if d[0] == "D" and d[13] != 0.0)
+    assert c.info()["num_nodes"] == 5 + n_rs
+
+
+def test_diode_rs_validation():
+    from neospice_b200 import _lib as L
+    from neospice_b200.circuit import Circuit, diode_params
+    assert diode_params(RS=5.0)[13] == 5.0 and diode_params()[13] == 0.0
+    c = Circuit(2)
+    with pytest.raises(L.NsgError):
+        c.D(0, 1, RS=-1.0)

@@ -1,7 +1,8 @@
-"""Diodes with reverse breakdown (BV, IBV, NBV) on the GPU against the
-reference, run here through the oracle on the same netlists: seeded Zener
-clamps and regulators whose operating points sit below, at and beyond the
-breakdown knee.  DC: solutions to 1e-9 relative (the GPU's exp rounds
+"""Diodes with reverse breakdown (BV, IBV, NBV) and series resistance (RS,
+an internal posPrime node) on the GPU against the reference, run here
+through the oracle on the same netlists: seeded Zener clamps and
+regulators whose operating points sit below, at and beyond the breakdown
+knee, half of them with RS.  DC: solutions to 1e-9 relative (the GPU's exp rounds
 differently from the host C library in the last bits) with equal Newton
 iteration counts.  Transient (a PULSE swinging the cathode from forward
 bias into breakdown, with junction capacitance and transit time):
@@ -21,15 +22,17 @@ pytestmark = [pytest.mark.gpu,
 GND = -1
 
 
-def zener(rng, transient=False):
+def zener(rng, transient=False, rs=False):
     """Source -> R -> node 1, a diode from ground (anode) to node 1 (cathode,
-    reverse biased when node 1 is positive), a load resistor on node 1."""
+    reverse biased when node 1 is positive), a load resistor on node 1; with
+    rs, the diode has a series resistance."""
     bv = float(rng.uniform(2.5, 12.0))
     n = float(rng.uniform(1.0, 1.5))
     card = [float(10 ** rng.uniform(-15, -12)), n,
             float(rng.uniform(0.5e-12, 5e-12)) if transient else 0.0, 0.8, 0.4, 0.5,
             float(10 ** rng.uniform(-10, -8)) if transient else 0.0,
-            bv, float(10 ** rng.uniform(-5, -2)), float(rng.uniform(1.0, 2.0))]
+            bv, float(10 ** rng.uniform(-5, -2)), float(rng.uniform(1.0, 2.0)),
+            float(10 ** rng.uniform(0, 2.5)) if rs else 0.0]
     if transient:
         src = ("VPULSE", 0, GND, -2.0, float(rng.uniform(1.2, 2.0)) * bv, 1e-9, 2e-9, 2e-9,
                4e-9, 1e-8)
@@ -41,7 +44,7 @@ def zener(rng, transient=False):
 
 
 def test_breakdown_dc_matches_reference():
-    nls = [zener(np.random.default_rng([51, k])) for k in range(16)]
+    nls = [zener(np.random.default_rng([51, k]), rs=k % 2 == 1) for k in range(16)]
     refs = [oracle.ref_sim(netlists.ref_desc(nl), 0) for nl in nls]
     batch = DcBatch([nl.build() for nl in nls], symbolic=DcBatch.PER_INSTANCE)
     sols, status, iters = batch.run()
@@ -59,7 +62,8 @@ def test_breakdown_dc_matches_reference():
 
 
 def test_breakdown_transient_matches_reference():
-    nls = [zener(np.random.default_rng([52, k]), transient=True) for k in range(4)]
+    nls = [zener(np.random.default_rng([52, k]), transient=True, rs=k % 2 == 1)
+           for k in range(4)]
     tstep, tstop = 1e-10, 2e-8
     refs = [oracle.ref_sim(netlists.ref_desc(nl), 1, tstep, tstop) for nl in nls]
     b = TranBatch([nl.build() for nl in nls], tstep, tstop, np.array([0, 1], np.int32),
