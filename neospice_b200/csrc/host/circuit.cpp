@@ -238,8 +238,13 @@ void Circuit::finalize() {
     // RS gets posPrime (DIOsetup's CKTmkVolt).  Branch unknowns follow all
     // node unknowns, in load order.
     int32_t next = num_nodes_;
-    for (auto& d : order)
+    for (auto& d : order) {
         if (d.kind == DevKind::Diode && params_[d.param + kDpRs] != 0.0) d.prime = next++;
+        if (d.kind == DevKind::Mosfet) {  // MOS1setup: drain', then source'
+            if (params_[d.param + kMDrainCond] != 0.0) d.prime = next++;
+            if (params_[d.param + kMSourceCond] != 0.0) d.prime2 = next++;
+        }
+    }
     num_internal_ = next - num_nodes_;
     for (auto& d : order)
         if (d.kind == DevKind::VSource) d.branch = next++;
@@ -271,12 +276,13 @@ void Circuit::finalize() {
                 break;
             case DevKind::ISource:
                 break;
-            case DevKind::Mosfet: {  // MOS1setup's TSTALLOC list with dNodePrime = d, sNodePrime = s
+            case DevKind::Mosfet: {  // MOS1setup's TSTALLOC list
                 const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
-                stamp(D, D); stamp(G, G); stamp(S, S); stamp(B, B); stamp(D, D); stamp(S, S);
-                stamp(D, D); stamp(G, B); stamp(G, D); stamp(G, S); stamp(S, S); stamp(B, D);
-                stamp(B, S); stamp(D, S); stamp(D, D); stamp(B, G); stamp(D, G); stamp(S, G);
-                stamp(S, S); stamp(D, B); stamp(S, B); stamp(S, D);
+                const int32_t Dp = d.prime >= 0 ? d.prime : D, Sp = d.prime2 >= 0 ? d.prime2 : S;
+                stamp(D, D); stamp(G, G); stamp(S, S); stamp(B, B); stamp(Dp, Dp); stamp(Sp, Sp);
+                stamp(D, Dp); stamp(G, B); stamp(G, Dp); stamp(G, Sp); stamp(S, Sp); stamp(B, Dp);
+                stamp(B, Sp); stamp(Dp, Sp); stamp(Dp, D); stamp(B, G); stamp(Dp, G); stamp(Sp, G);
+                stamp(Sp, S); stamp(Dp, B); stamp(Sp, B); stamp(Sp, Dp);
                 break;
             }
             case DevKind::Bsim4: {  // BSIM4v7setup's TSTALLOC list without internal nodes
@@ -324,7 +330,9 @@ void Circuit::finalize() {
         if (d.kind == DevKind::Mosfet || d.kind == DevKind::Bsim4) {
             const bool b4 = d.kind == DevKind::Bsim4;
             index_in_table[k] = static_cast<int32_t>(mos_.size());
-            mos_.push_back({d.a, d.b, d.c, d.e, d.param, state, b4 ? kFamilyBsim4 : kFamilyMos1});
+            // the load sees drain' and source' (the terminals without RD / RS)
+            mos_.push_back({d.prime >= 0 ? d.prime : d.a, d.b, d.prime2 >= 0 ? d.prime2 : d.c, d.e,
+                            d.param, state, b4 ? kFamilyBsim4 : kFamilyMos1});
             state += b4 ? kB4States : kMosStates;
         } else if (d.kind == DevKind::Diode) {
             index_in_table[k] = static_cast<int32_t>(diodes_.size());
@@ -377,14 +385,16 @@ void Circuit::finalize() {
                 // MOS1load: the four rhs updates (UCB array: gate, bulk,
                 // drain', source'), then the 22 matrix adds in order.
                 const int32_t D = d.a, G = d.b, S = d.c, B = d.e;
+                const int32_t Dp = d.prime >= 0 ? d.prime : D, Sp = d.prime2 >= 0 ? d.prime2 : S;
                 if (G >= 0) ucb[G].push_back(mos_term(id, kTRhsG));
                 if (B >= 0) ucb[B].push_back(mos_term(id, kTRhsB));
-                if (D >= 0) ucb[D].push_back(mos_term(id, kTRhsDP));
-                if (S >= 0) ucb[S].push_back(mos_term(id, kTRhsSP));
-                const int32_t rc[22][2] = {{D, D}, {G, G}, {S, S}, {B, B}, {D, D}, {S, S},
-                                           {D, D}, {G, B}, {G, D}, {G, S}, {S, S}, {B, G},
-                                           {B, D}, {B, S}, {D, D}, {D, G}, {D, B}, {D, S},
-                                           {S, G}, {S, S}, {S, B}, {S, D}};
+                if (Dp >= 0) ucb[Dp].push_back(mos_term(id, kTRhsDP));
+                if (Sp >= 0) ucb[Sp].push_back(mos_term(id, kTRhsSP));
+                const int32_t rc[22][2] = {{D, D},   {G, G},   {S, S},   {B, B},   {Dp, Dp},
+                                           {Sp, Sp}, {D, Dp},  {G, B},   {G, Dp},  {G, Sp},
+                                           {S, Sp},  {B, G},   {B, Dp},  {B, Sp},  {Dp, D},
+                                           {Dp, G},  {Dp, B},  {Dp, Sp}, {Sp, G},  {Sp, S},
+                                           {Sp, B},  {Sp, Dp}};
                 for (int32_t w = 0; w < 22; ++w) add_slot(rc[w][0], rc[w][1], mos_term(id, w));
                 break;
             }

@@ -74,7 +74,9 @@ struct DeviceRec {
     int32_t branch;    // VSource branch unknown, else -1
     Wave wave;         // sources
     bool has_ic;       // capacitors
-    int32_t prime = -1;  // diode with RS: its internal node posPrime (assigned at finalize)
+    // Internal nodes assigned at finalize: a diode's posPrime (RS != 0), a
+    // level-1 MOSFET's dNodePrime (prime) and sNodePrime (prime2).
+    int32_t prime = -1, prime2 = -1;
 };
 
 // A level-1 MOSFET model card: the type (+1 NMOS, -1 PMOS) and the given
@@ -89,7 +91,7 @@ struct Mos1Card {
 // instance of `card` with width W and length L at the nominal temperature:
 // MOS1setup's defaults and MOS1temp (src/devices/mos1/mos1_setup.cpp,
 // mos1_temp.cpp).  Throws std::invalid_argument on an unknown or
-// unsupported parameter (nonzero RD, RS or RSH).
+// unsupported parameter (RD = 0 or RS = 0 given beside a nonzero RSH).
 std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L);
 
 // A BSIM4v7 (LEVEL=14) model card: the type and the given parameters

@@ -71,8 +71,12 @@ Card parse(const Mos1Card& in) {
         g->v = (k == "tnom") ? val + kCtoK : val;  // MOS1mParam stores TNOM in kelvin
         if (k == "tpg") g->v = static_cast<double>(static_cast<int>(val));
     }
-    if ((c.rd.on && c.rd.v != 0.0) || (c.rs.on && c.rs.v != 0.0) || (c.rsh.on && c.rsh.v != 0.0))
-        throw std::invalid_argument("MOS1 model: drain/source resistance (RD, RS, RSH) is not "
+    // MOS1setup gives a terminal an internal node when RD (RS) or RSH is
+    // nonzero, MOS1temp a conductance from RD (RS) when given, else from
+    // RSH: they disagree only for RD = 0 (RS = 0) given beside RSH != 0 (a
+    // node without conductance), which is refused.
+    if (c.rsh.on && c.rsh.v != 0.0 && ((c.rd.on && c.rd.v == 0.0) || (c.rs.on && c.rs.v == 0.0)))
+        throw std::invalid_argument("MOS1 model: RD = 0 or RS = 0 given with RSH != 0 is not "
                                     "supported");
     return c;
 }
@@ -237,7 +241,21 @@ std::vector<double> mos1_param_block(const Mos1Card& in, double W, double L) {
     P[kMMj] = mj;
     P[kMMjsw] = mjsw;
     P[kMVt] = kKoverQ * temp;
-    return P;  // initial conditions, OFF and the series conductances stay 0
+    // MOS1temp's series conductances (mos1_temp.cpp:298-334): M / RD (M / RS)
+    // when given, else M / (RSH * NRD) (NRS) with the default one square.
+    const double drainSquares = 1, sourceSquares = 1;
+    if (c.rd.on) {
+        if (c.rd.v != 0) P[kMDrainCond] = m / c.rd.v;
+    } else if (c.rsh.on) {
+        if (c.rsh.v != 0) P[kMDrainCond] = m / (c.rsh.v * drainSquares);
+    }
+    if (c.rs.on) {
+        if (c.rs.v != 0) P[kMSourceCond] = m / c.rs.v;
+    } else if (c.rsh.on) {
+        if ((c.rsh.v != 0) && (sourceSquares != 0))
+            P[kMSourceCond] = m / (c.rsh.v * sourceSquares);
+    }
+    return P;  // initial conditions and OFF stay 0
 }
 
 }  // namespace nsg

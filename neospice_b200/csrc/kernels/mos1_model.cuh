@@ -1,6 +1,8 @@
 // MOS1 (Shichman-Hodges, level 1) device evaluation shared by host and device:
-// MOS1load (src/devices/mos1/mos1_load.cpp:21-900) for one instance with
-// RD = RS = 0 (no internal nodes), bypass off (the reference's
+// MOS1load (src/devices/mos1/mos1_load.cpp:21-900) for one instance (the
+// node voltages are those of drain' and source', the internal nodes that
+// RD / RS / RSH add; the series conductances are stamped between them and
+// the terminals), bypass off (the reference's
 // MOS1Device::evaluate sets CKTbypass = 0), device gain 1.  The limiting
 // helpers follow src/devices/mos1/mos1_shim.cpp:98-204 and the charge
 // integration NIintegrate (mos1_shim.cpp:44-73).  Every expression keeps the

@@ -203,7 +203,8 @@ def test_mos_model_card_validation():
     with pytest.raises(L.NsgError, match="unknown parameter"):
         c.model_mos1("nmos", VTO=0.7, BOGUS=1.0)
     with pytest.raises(L.NsgError, match="not supported"):
-        c.model_mos1("nmos", VTO=0.7, RD=10.0)
+        c.model_mos1("nmos", VTO=0.7, RD=0.0, RSH=10.0)  # node without conductance
+    c.model_mos1("nmos", VTO=0.7, RD=10.0)  # series resistance: internal drain' node
     m = c.model_mos1("nmos", VTO=0.7, KP=1e-4, RD=0.0)
     with pytest.raises(L.NsgError, match="W > 0"):
         c.M(0, 1, 2, -1, m, 0.0, 1e-6)

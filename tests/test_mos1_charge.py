@@ -41,3 +41,38 @@ def test_mos1_charge_loads_bitwise(case):
     for s, ((a, r), (ra, rr)) in enumerate(zip(ours, ref)):
         np.testing.assert_array_equal(a, ra, err_msg=f"{case} step {s} matrix")
         np.testing.assert_array_equal(r, rr, err_msg=f"{case} step {s} rhs")
+
+
+SERIES = [{"RD": 25.0, "RS": 10.0}, {"RSH": 40.0}, {"RD": 15.0}, {"RS": 30.0, "RSH": 20.0}]
+
+
+@needs_ref
+@pytest.mark.parametrize("k", range(len(SERIES)))
+def test_mos1_series_resistance_bitwise(k):
+    """Drain / source series resistance (RD, RS, or RSH with one square):
+    the internal drain' and source' nodes are numbered as the reference
+    numbers them (after the external nodes, in load order, drain' first),
+    and the first DC matrix plus the whole transient-mode load sequence,
+    charges included, equal the reference's bit for bit."""
+    import netlists
+    nl = _driven(64 + k, dict(MEYER, **JUNCTION, **SERIES[k]))
+    c = nl.build()
+    cp, ri = c.pattern()
+    a, rhs = c.initial_matrix(1e-12)
+    rcp, rri, ra, rrhs = oracle.ref_sim_initjct(netlists.ref_desc(nl))
+    np.testing.assert_array_equal(cp, rcp)
+    np.testing.assert_array_equal(ri, rri)
+    np.testing.assert_array_equal(a, ra)
+    np.testing.assert_array_equal(rhs, rrhs)
+    assert c.info()["num_nodes"] > nl.num_nodes
+    ours, ref = _eval_sequence(nl, np.random.default_rng([46, k]))
+    for s, ((a, r), (ra, rr)) in enumerate(zip(ours, ref)):
+        np.testing.assert_array_equal(a, ra, err_msg=f"step {s} matrix")
+        np.testing.assert_array_equal(r, rr, err_msg=f"step {s} rhs")
+
+
+def test_mos1_zero_rd_beside_rsh_is_refused():
+    from neospice_b200 import _lib as L
+    nl = _driven(70, {"RSH": 40.0, "RD": 0.0})
+    with pytest.raises(L.NsgError):
+        nl.build()
