@@ -101,7 +101,7 @@ JUNCTION = {"CBD": 5e-15, "CBS": 4e-15, "GAMMA": 0.4}
 
 
 @pytest.mark.parametrize("extra,min_resolved", [("meyer", 6), ("meyer+junction", 6),
-                                                ("strong+junction", 0)])
+                                                ("strong+junction", 0), ("meyer+series", 6)])
 def test_tran_adjoint_with_mos_charge(extra, min_resolved):
     """The drivers carry Meyer gate charge (TOX) with overlap capacitances,
     and bulk-junction charge with body effect: the adjoint's charge units
@@ -113,10 +113,13 @@ def test_tran_adjoint_with_mos_charge(extra, min_resolved):
     moderate oxide and overlap capacitance the six W / L / VTO gradients are
     resolved (floor below 1e-7 |fd|) and must be within 1e-6; at TOX = 20 nm
     (the gate-drain charge dominates the output and the loss is small) each
-    gradient is checked against its floor only."""
+    gradient is checked against its floor only.  With RD / RS the channel
+    and the charges sit on the internal drain' and source' nodes."""
     card = dict(MEYER_STRONG if extra.startswith("strong") else MEYER)
     if extra.endswith("junction"):
         card.update(JUNCTION)
+    if extra.endswith("series"):  # drain' / source' internal nodes carry the charges
+        card.update({"RD": 25.0, "RS": 10.0})
     nls, b, tg, probes = setup(12, 84, cards={"nch": card, "pch": card})
     worst, resolved = check_against_fd(nls, b, tg, probes, h_rel=1e-5, resolved_below=1e-7)
     assert resolved >= min_resolved and worst < 1e-6, (resolved, worst)
