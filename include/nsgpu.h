@@ -325,10 +325,13 @@ int nsg_circuit_add_source_wave(nsg_circuit* c, int is_voltage, int p, int n, in
 /* A level-1 MOSFET model card (Circuit::model with ".model NAME NMOS|PMOS
  * (LEVEL=1 ...)", src/core/circuit.hpp:259): type +1 NMOS / -1 PMOS and
  * nparams (key, value) pairs with the MOS1 parameter names of
- * src/devices/mos1/mos1_devsup.cpp:123-159 (vto kp gamma phi lambda cbd cbs is
- * pb cgso cgdo cgbo cj mj cjsw mjsw js tox ld u0 fc nsub tpg nss tnom; kf, af
- * and level are accepted and ignored).  Nonzero rd, rs or rsh (internal
- * nodes) are rejected.  *model_out receives the model index. */
+ * src/devices/mos1/mos1_devsup.cpp:123-159 (vto kp gamma phi lambda rd rs rsh
+ * cbd cbs is pb cgso cgdo cgbo cj mj cjsw mjsw js tox ld u0 fc nsub tpg nss
+ * tnom; kf, af and level are accepted and ignored).  Nonzero rd / rs (or rsh,
+ * one square each) give each MOSFET of the card an internal drain' / source'
+ * node after the external nodes, in load order, as MOS1setup does; rd = 0 or
+ * rs = 0 given beside a nonzero rsh is rejected.  *model_out receives the
+ * model index. */
 int nsg_circuit_add_mos1_model(nsg_circuit* c, int type, int nparams, const char* const* keys,
                                const double* values, int* model_out);
 /* Circuit::M with W and L (src/core/circuit.hpp:218-219).  Its parameter
