@@ -263,8 +263,8 @@ int nsg_batch_lu_to_host(const nsg_batch* batch, double* out);
  * ngspice load order, branch unknowns after the nodes, sparsity pattern,
  * dead-node placeholders.  Parameters are kept in creation order: resistor
  * {ohms}, capacitor {farads, ic}, DC source {value}, PULSE source {v1, v2,
- * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode: the 14
- * values of nsg_diode_param_block.  A diode with RS gets an internal node
+ * td, tr, tf, pw, per}, PWL source {t0, v0, t1, v1, ...}, diode: the 15
+ * values of nsg_diode_param_block (at the circuit temperature).  A diode with RS gets an internal node
  * (posPrime) after the external nodes, in load order, as DIOsetup's
  * CKTmkVolt does; nsg_circuit_info's node count includes it. */
 typedef struct nsg_circuit nsg_circuit;
@@ -281,6 +281,13 @@ int nsg_circuit_add_resistor(nsg_circuit* c, int a, int b, double ohms);
 int nsg_circuit_add_vsource(nsg_circuit* c, int p, int n, double volts);
 /* Circuit::I with a DC value (src/core/circuit.hpp:189). */
 int nsg_circuit_add_isource(nsg_circuit* c, int p, int n, double amps);
+/* The circuit temperature in kelvin (the reference's options.temp, default
+ * 300.15 = TNOM; `.step TEMP` sets it to the step value + 273.15,
+ * src/api/neospice.cpp:255-256).  DIOtemp and MOS1temp apply it to every
+ * diode and level-1 MOSFET added afterwards, so it must be set before any
+ * device is added (NSG_ERR_INVALID otherwise); BSIM4v7 devices are
+ * supported at TNOM only. */
+int nsg_circuit_set_temperature(nsg_circuit* c, double kelvin);
 /* Circuit::D with a level-1 model card D(IS=is N=n) (src/core/circuit.hpp:210;
  * series resistance 0, T = TNOM). */
 int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, double n_emission);
@@ -303,12 +310,14 @@ int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is
 int nsg_circuit_add_diode_card_ex(nsg_circuit* c, int anode, int cathode, double is,
                                   double n_emission, double cjo, double vj, double m, double fc,
                                   double tt, double bv, double ibv, double nbv, double rs);
-/* The diode parameter block of a card (14 doubles into out): IS, N, then
+/* The diode parameter block of a card at TNOM (15 doubles into out): IS, N, then
  * DIOtemp's junction capacitance, junction potential, depletion knee FC*VJ,
  * F1, F2, F3, grading coefficient and transit time at T = TNOM
  * (src/devices/dio/dio_temp.cpp:91-292), then 1/0 for BV given, DIOtemp's
  * breakdown voltage matched to IBV (dio_temp.cpp:233-270, the circuit's
- * RELTOL at its default 1e-3), NBV and RS.  bv NaN: no breakdown. */
+ * RELTOL at its default 1e-3), NBV, RS and vt.  bv NaN: no breakdown.  At
+ * another circuit temperature IS becomes DIOtemp's saturation current (EG
+ * 1.11, XTI 3) and the junction values and vt follow the temperature. */
 int nsg_diode_param_block(double is, double n_emission, double cjo, double vj, double m,
                           double fc, double tt, double bv, double ibv, double nbv, double rs,
                           double* out);

@@ -82,6 +82,7 @@ SIGNATURES = {
     "nsg_circuit_add_vsource": (c_int, [c_void_p, c_int, c_int, c_double]),
     "nsg_circuit_add_isource": (c_int, [c_void_p, c_int, c_int, c_double]),
     "nsg_circuit_add_diode": (c_int, [c_void_p, c_int, c_int, c_double, c_double]),
+    "nsg_circuit_set_temperature": (c_int, [c_void_p, c_double]),
     "nsg_circuit_add_diode_card": (c_int, [c_void_p, c_int, c_int, c_double, c_double, c_double,
                                            c_double, c_double, c_double, c_double]),
     "nsg_diode_param_block": (c_int, [c_double, c_double, c_double, c_double, c_double, c_double,

@@ -29,11 +29,11 @@ AIDS = {"direct": 0, "source": 1, "gain": 2, "ptc": 3}
 def diode_params(IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0, VJ: float = 1.0,
                  M: float = 0.5, FC: float = 0.5, TT: float = 0.0, BV: float | None = None,
                  IBV: float = 1e-3, NBV: float | None = None, RS: float = 0.0) -> np.ndarray:
-    """The 14-value parameter block a diode with this card holds in
-    Circuit.params(): IS, N, then the junction values at the nominal
-    temperature, then the breakdown flag, DIOtemp's breakdown voltage, NBV
-    and RS (nsg_diode_param_block)."""
-    out = np.zeros(14, np.float64)
+    """The 15-value parameter block a diode with this card holds in
+    Circuit.params() at the nominal temperature: IS, N, then the junction
+    values, then the breakdown flag, DIOtemp's breakdown voltage, NBV, RS
+    and vt (nsg_diode_param_block)."""
+    out = np.zeros(15, np.float64)
     L.check(L.lib().nsg_diode_param_block(float(IS), float(N), float(CJO), float(VJ), float(M),
                                           float(FC), float(TT),
                                           float("nan") if BV is None else float(BV), float(IBV),
@@ -75,6 +75,11 @@ class Circuit:
         first = self.param_count()
         L.check(L.lib().nsg_circuit_add_isource(self._h, int(p), int(n), float(amps)))
         return first
+
+    def set_temperature(self, kelvin: float):
+        """The circuit temperature (the reference's options.temp, default
+        300.15 K); set it before adding devices."""
+        L.check(L.lib().nsg_circuit_set_temperature(self._h, float(kelvin)))
 
     def D(self, anode: int, cathode: int, IS: float = 1e-14, N: float = 1.0, CJO: float = 0.0,
           VJ: float = 1.0, M: float = 0.5, FC: float = 0.5, TT: float = 0.0,

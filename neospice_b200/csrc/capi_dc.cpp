@@ -220,6 +220,14 @@ int nsg_circuit_add_diode(nsg_circuit* c, int anode, int cathode, double is, dou
     });
 }
 
+int nsg_circuit_set_temperature(nsg_circuit* c, double kelvin) {
+    return guarded("nsg_circuit_set_temperature", [&]() -> int {
+        if (!c) return fail(NSG_ERR_INVALID, "null circuit");
+        c->c.set_temperature(kelvin);
+        return NSG_OK;
+    });
+}
+
 int nsg_circuit_add_diode_card(nsg_circuit* c, int anode, int cathode, double is,
                                double n_emission, double cjo, double vj, double m, double fc,
                                double tt) {

@@ -77,7 +77,7 @@ int32_t Circuit::add_source_wave(bool is_voltage, int32_t p, int32_t n, Wave wav
 // knee, each by the reference's expression.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
                                       double fc, double tt, double bv, double ibv, double nbv,
-                                      double rs) {
+                                      double rs, double temp) {
     if (!(is > 0.0) || !(n > 0.0))
         throw std::invalid_argument("Circuit: diode needs IS > 0 and N > 0");
     if (!(cjo >= 0.0) || !(vj > 0.0) || !(m >= 0.0 && m < 1.0) || !(fc >= 0.0 && fc < 1.0) ||
@@ -92,7 +92,9 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     if (!(rs >= 0.0) || !std::isfinite(rs))
         throw std::invalid_argument("Circuit: diode needs RS >= 0");
     constexpr double kBoltz = 1.38064852e-23, kCharge = 1.6021766208e-19, kRefTemp = 300.15;
-    const double temp = kTNominal, tnom = kTNominal, dt = temp - tnom;
+    if (!(temp > 0.0) || !std::isfinite(temp))
+        throw std::invalid_argument("Circuit: temperature must be positive (kelvin)");
+    const double tnom = kTNominal, dt = temp - tnom;
     const double vtnom = kKoverQ * tnom;
     const double xfc = std::log(1 - fc);
     double grad = m * (1.0 + (0.0 * dt) + (0.0 * dt * dt));
@@ -121,8 +123,13 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     const double ttt = tt * (1.0 + (0.0 * dt) + (0.0 * dt * dt));
     const double f2 = std::exp((1 + grad) * xfc);
     const double f3 = 1 - fc * (1 + grad);
+    // DIOtemp's saturation current at the device temperature (EG 1.11,
+    // XTI 3, area 1): IS itself at TNOM.
+    const double eg = 1.11, xti = 3.0;
+    const double tsat = is * 1.0 * std::exp(((temp / tnom) - 1) * eg / (n * vt) +
+                                            xti / n * std::log(temp / tnom));
     std::vector<double> p(kDiodeParams);
-    p[kDpCsat] = is;
+    p[kDpCsat] = tsat;
     p[kDpN] = n;
     p[kDpCj] = cj;
     p[kDpPot] = pot;
@@ -139,15 +146,15 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     if (brk) {
         const double tbv = bv - 0.0 * dt;
         double cbv = ibv;
-        if (cbv < is * tbv / vt) {
-            cbv = is * tbv / vt;
+        if (cbv < tsat * tbv / vt) {
+            cbv = tsat * tbv / vt;
             xbv = tbv;
         } else {
             const double tol = 1e-3 * cbv;
-            xbv = tbv - nbv * vt * std::log(1 + cbv / (is));
+            xbv = tbv - nbv * vt * std::log(1 + cbv / (tsat));
             for (int iter = 0; iter < 25; iter++) {
-                xbv = tbv - nbv * vt * std::log(cbv / (is) + 1 - xbv / vt);
-                const double xcbv = is * (std::exp((tbv - xbv) / (nbv * vt)) - 1 + xbv / vt);
+                xbv = tbv - nbv * vt * std::log(cbv / (tsat) + 1 - xbv / vt);
+                const double xcbv = tsat * (std::exp((tbv - xbv) / (nbv * vt)) - 1 + xbv / vt);
                 if (std::fabs(xcbv - cbv) <= tol) break;
             }
         }
@@ -156,6 +163,7 @@ std::vector<double> diode_param_block(double is, double n, double cjo, double vj
     p[kDpTbv] = xbv;
     p[kDpNbv] = nbv;
     p[kDpRs] = rs;
+    p[kDpVt] = vt;
     return p;
 }
 
@@ -163,7 +171,17 @@ int32_t Circuit::add_diode(int32_t anode, int32_t cathode, double is, double n_e
                            double cjo, double vj, double m, double fc, double tt, double bv,
                            double ibv, double nbv, double rs) {
     return add_device(DevKind::Diode, anode, cathode,
-                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv, rs));
+                      diode_param_block(is, n_emission, cjo, vj, m, fc, tt, bv, ibv, nbv, rs,
+                                        temp_));
+}
+
+void Circuit::set_temperature(double kelvin) {
+    if (finalized_) throw std::logic_error("Circuit: already finalized");
+    if (!devices_.empty())
+        throw std::logic_error("Circuit: set the temperature before adding devices");
+    if (!(kelvin > 0.0) || !std::isfinite(kelvin))
+        throw std::invalid_argument("Circuit: temperature must be positive (kelvin)");
+    temp_ = kelvin;
 }
 
 int32_t Circuit::add_mos1_model(const Mos1Card& card) {
@@ -180,7 +198,8 @@ int32_t Circuit::add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t 
     if (model < 0 || model >= static_cast<int32_t>(mos_models_.size()))
         throw std::out_of_range("Circuit: unknown MOSFET model " + std::to_string(model));
     if (!(W > 0.0) || !(L > 0.0)) throw std::invalid_argument("Circuit: MOSFET needs W > 0, L > 0");
-    const int32_t id = add_device(DevKind::Mosfet, d, g, mos1_param_block(mos_models_[model], W, L));
+    const int32_t id =
+        add_device(DevKind::Mosfet, d, g, mos1_param_block(mos_models_[model], W, L, temp_));
     devices_.back().c = s;
     devices_.back().e = b;
     return id;
@@ -199,6 +218,8 @@ int32_t Circuit::add_bsim4(int32_t d, int32_t g, int32_t s, int32_t b, int32_t m
     check_node(b);
     if (model < 0 || model >= static_cast<int32_t>(b4_models_.size()))
         throw std::out_of_range("Circuit: unknown BSIM4v7 model " + std::to_string(model));
+    if (temp_ != kTNominal)
+        throw std::invalid_argument("Circuit: BSIM4v7 devices are supported at TNOM only");
     const int32_t id =
         add_device(DevKind::Bsim4, d, g, bsim4_param_block(b4_models_[model], W, L, delvto));
     devices_.back().c = s;
@@ -594,9 +615,9 @@ void Circuit::initjct_values(std::vector<double>& a, std::vector<double>& rhs, d
     if (!finalized_) throw std::logic_error("Circuit: not finalized");
     std::vector<double> tv;
     const_term_values(tv, gmin);
-    const double vt = kKoverQ * kTNominal;
     for (size_t d = 0; d < diodes_.size(); ++d) {
         const double csat = params_[diodes_[d].param];
+        const double vt = params_[diodes_[d].param + kDpVt];
         const double vte = params_[diodes_[d].param + 1] * vt;
         const DiodeDC r = diode_dc_load(true, 0.0, 0.0, 0.0, csat, vte, diode_vcrit(vte, csat), gmin,
                                         diode_brk(&params_[diodes_[d].param], vt));

@@ -92,7 +92,8 @@ struct Mos1Card {
 // MOS1setup's defaults and MOS1temp (src/devices/mos1/mos1_setup.cpp,
 // mos1_temp.cpp).  Throws std::invalid_argument on an unknown or
 // unsupported parameter (RD = 0 or RS = 0 given beside a nonzero RSH).
-std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L);
+std::vector<double> mos1_param_block(const Mos1Card& card, double W, double L,
+                                     double temp = 300.15);
 
 // A BSIM4v7 (LEVEL=14) model card: the type and the given parameters
 // (ngspice names).  Supported: the default card with TOXE, VTH0, U0.
@@ -117,7 +118,7 @@ std::vector<double> bsim4_param_block(const Bsim4Card& card, double W, double L,
 // NBV > 0.
 std::vector<double> diode_param_block(double is, double n, double cjo, double vj, double m,
                                       double fc, double tt, double bv = NAN, double ibv = 1e-3,
-                                      double nbv = NAN, double rs = 0.0);
+                                      double nbv = NAN, double rs = 0.0, double temp = 300.15);
 
 class Circuit {
 public:
@@ -145,6 +146,12 @@ public:
     // Level-1 MOSFET models and instances (Circuit::model,
     // src/core/circuit.hpp:259, and Circuit::M with W and L, :218-219).
     // Returns the model / device index.
+    // The circuit temperature in kelvin (the reference's options.temp;
+    // default 300.15 = TNOM), applied by DIOtemp / MOS1temp to every device
+    // added afterwards; set it before adding devices.  BSIM4v7 devices are
+    // supported at TNOM only.
+    void set_temperature(double kelvin);
+    double temperature() const { return temp_; }
     int32_t add_mos1_model(const Mos1Card& card);
     int32_t add_mosfet(int32_t d, int32_t g, int32_t s, int32_t b, int32_t model, double W,
                        double L);
@@ -242,6 +249,7 @@ public:
 private:
     int32_t num_nodes_;
     int32_t num_internal_ = 0;
+    double temp_ = 300.15;  // circuit temperature (kelvin): the options' TEMP
     int32_t num_vars_ = 0;
     bool finalized_ = false;
     std::vector<DeviceRec> devices_;

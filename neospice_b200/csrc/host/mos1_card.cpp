@@ -1,7 +1,7 @@
 // Level-1 MOSFET model cards: parameter defaulting (MOS1setup,
 // src/devices/mos1/mos1_setup.cpp:24-100) and temperature preprocessing
 // (MOS1temp, src/devices/mos1/mos1_temp.cpp:21-340) at the circuit
-// temperature 300.15 K, evaluated with the same operations and the host's
+// temperature (TNOM 300.15 K), evaluated with the same operations and the host's
 // libm, so every constant equals the reference's bit for bit.
 #include "circuit.hpp"
 
@@ -85,7 +85,7 @@ double val(const Given& g, double dflt) { return g.on ? g.v : dflt; }
 
 }  // namespace
 
-std::vector<double> mos1_param_block(const Mos1Card& in, double W, double L) {
+std::vector<double> mos1_param_block(const Mos1Card& in, double W, double L, double circuit_temp) {
     if (in.type != 1 && in.type != -1) throw std::invalid_argument("MOS1 model: type must be +1 or -1");
     const Card c = parse(in);
     const double type = in.type;
@@ -145,8 +145,11 @@ std::vector<double> mos1_param_block(const Mos1Card& in, double W, double L) {
         }
     }
 
-    // MOS1temp, instance part (T = 300.15 K, M = 1, AD = AS = PD = PS = 0)
-    const double temp = 300.15 + 0.0;
+    // MOS1temp, instance part (T = the circuit temperature, M = 1,
+    // AD = AS = PD = PS = 0)
+    if (!(circuit_temp > 0.0) || !std::isfinite(circuit_temp))
+        throw std::invalid_argument("MOS1: temperature must be positive (kelvin)");
+    const double temp = circuit_temp + 0.0;  // MOS1temp: CKTtemp + dtemp
     const double m = 1.0, drainArea = 0.0, sourceArea = 0.0, drainPerim = 0.0, sourcePerim = 0.0;
     const double vt = temp * kKoverQ;
     const double ratio = temp / tnom;

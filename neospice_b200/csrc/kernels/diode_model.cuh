@@ -1,5 +1,5 @@
-// Load of the level-1 junction diode (no knee currents, no sidewall,
-// T = TNOM; series resistance RS through an internal node, reverse
+// Load of the level-1 junction diode (no knee currents, no sidewall; at the
+// circuit temperature; series resistance RS through an internal node, reverse
 // breakdown when BV is given), shared by the host (first-iteration
 // values for the symbolic phase) and the GPU Newton kernels: the DC current
 // and conductance, and the depletion and diffusion charge of the transient.
@@ -35,7 +35,8 @@ enum DiodeParam : int {
     kDpTbv = 11,    // DIOtBrkdwnV (DIOtemp's breakdown voltage matched to IBV)
     kDpNbv = 12,    // NBV (DIObrkdEmissionCoeff; N when not given)
     kDpRs = 13,     // RS (0: no series resistance, posPrime == pos)
-    kDiodeParams = 14
+    kDpVt = 14,     // vt = CONSTKoverQ * DIOtemp (the device temperature)
+    kDiodeParams = 15
 };
 
 // Series conductance gspr = DIOtConductance * area of DIOtemp at T = TNOM

@@ -127,7 +127,8 @@ __device__ __forceinline__ double term_value(int32_t op, double p, double gmin) 
     }
 }
 
-// Constant term values, diode constants (csat, vte, Vcrit at T = TNOM).
+// Constant term values, diode constants (csat, vte, Vcrit at the diode's
+// temperature).
 // DC source values are scaled by src_fact as VSource / ISource::evaluate do
 // (vsource.cpp:208-209, isource.cpp:173-176): the value times the factor,
 // then its negation where the stamp subtracts it.
@@ -141,7 +142,7 @@ __device__ inline void load_constants(const Inst& v, double gmin, double src_fac
     for (int32_t k = threadIdx.x; k < v.n_diodes; k += blockDim.x) {
         const int32_t pi = v.diodes[4 * k + 2];
         const double csat = v.par[pi];
-        const double vte = v.par[pi + 1] * kKoverQTimesTnom;
+        const double vte = v.par[pi + 1] * v.par[pi + kDpVt];
         v.dconst[3 * k] = csat;
         v.dconst[3 * k + 1] = vte;
         v.dconst[3 * k + 2] = diode_vcrit(vte, csat);
@@ -213,7 +214,7 @@ static __device__ __noinline__ void eval_devices(const Inst& v, const IntegCtx& 
         }
         const DiodeDC r = diode_eval(vd, limit, s0[kDsV], v.dconst[3 * k], v.dconst[3 * k + 1],
                                      v.dconst[3 * k + 2], opt.gmin,
-                                     diode_brk(v.par + dr[2], kKoverQTimesTnom));
+                                     diode_brk(v.par + dr[2], v.par[dr[2] + kDpVt]));
         double cd = r.cd, gd = r.gd;
         if (charges) {  // charge storage (dio_load.cpp:309-373)
             double charge, capd;

@@ -104,7 +104,7 @@ __device__ inline double diode_capd(const Inst& v, int32_t k, double vd, double 
     const int32_t* dr = v.diodes + 4 * k;
     const DiodeDC r =
         diode_eval(vd, false, vd, v.dconst[3 * k], v.dconst[3 * k + 1], v.dconst[3 * k + 2], gmin,
-                   diode_brk(v.par + dr[2], kKoverQTimesTnom));
+                   diode_brk(v.par + dr[2], v.par[dr[2] + kDpVt]));
     double q, capd;
     diode_charge(v.par + dr[2], r.vd, r.cdb, r.gdb, &q, &capd);
     return capd;

@@ -72,3 +72,30 @@ def sweep_transient(build, param: int, values, tstep: float, tstop: float, probe
     b = TranBatch(circuits, tstep, tstop, np.asarray(probes, np.int32), max_points=max_points)
     b.run()
     return b.results()
+
+
+def sweep_dc_temperature(build, temps_celsius, symbolic=DcBatch.PER_INSTANCE):
+    """`.step TEMP` of an operating point: the reference sets the circuit
+    temperature to each step value + 273.15 K and re-runs the analysis
+    (src/api/neospice.cpp:255-256), so every step is one instance built by
+    `build(kelvin)` (a finalized Circuit with its devices at that
+    temperature) of one batched launch.  Returns (solutions
+    [len(temps), n], status, iterations) per step."""
+    import torch
+
+    temps = np.asarray(temps_celsius, np.float64).ravel()
+    batch = DcBatch([build(t + 273.15) for t in temps], symbolic=symbolic)
+    sols, status, iters = batch.run()
+    torch.cuda.synchronize()
+    return (np.stack(batch.split(sols)), status.cpu().numpy(), iters.cpu().numpy())
+
+
+def sweep_transient_temperature(build, temps_celsius, tstep: float, tstop: float, probes,
+                                max_points: int = 100000):
+    """`.step TEMP` of a transient: one TranBatch instance per step value,
+    built by `build(kelvin)`.  Returns the batch's results() list."""
+    temps = np.asarray(temps_celsius, np.float64).ravel()
+    b = TranBatch([build(t + 273.15) for t in temps], tstep, tstop,
+                  np.asarray(probes, np.int32), max_points=max_points)
+    b.run()
+    return b.results()

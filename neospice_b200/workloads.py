@@ -94,11 +94,14 @@ class Netlist:
     devices: list
     models: dict = dataclasses.field(default_factory=dict)
 
-    def build(self) -> Circuit:
-        """The finalized circuit; ``self.param_index`` receives the index of
-        each device's first parameter (creation order), the layout of
-        Circuit.params()."""
+    def build(self, temp: float | None = None) -> Circuit:
+        """The finalized circuit (at `temp` kelvin when given: the circuit
+        temperature DIOtemp / MOS1temp apply); ``self.param_index`` receives
+        the index of each device's first parameter (creation order), the
+        layout of Circuit.params()."""
         c = Circuit(self.num_nodes)
+        if temp is not None:
+            c.set_temperature(temp)
         mid, b4 = {}, set()
         for name, (t, p) in self.models.items():
             if int(p.get("LEVEL", 1)) == 14:

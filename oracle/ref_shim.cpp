@@ -443,7 +443,7 @@ int nsref_mesh_initjct(int side, const double* r_h, const double* r_v, int n_dio
 //   R a b ohms | C a b farads [ic] | V a b dc | I a b dc
 //   VPULSE a b v1 v2 td tr tf pw per | IPULSE ... | VPWL a b t0 v0 t1 v1 ...
 //   IPWL a b t0 v0 ... | D a k IS N | MODEL name card... | M d g s b model W L [DELVTO]
-//   OPT name value                   (reltol, abstol, vntol, gmin, itl4, method)
+//   OPT name value                   (reltol, abstol, vntol, gmin, itl4, method, temp)
 // Node -1 is ground.  analysis 0 = DC operating point, 1 = transient.
 struct SimResult {
     std::string error;
@@ -562,6 +562,7 @@ static void build_from_desc(Circuit& ckt, const char* desc) {
             else if (key == "itl4") ckt.options.itl4 = static_cast<int>(val);
             else if (key == "gear") ckt.options.method = val != 0.0 ? "gear" : "trap";
             else if (key == "verbose") ckt.options.verbose = val != 0.0;
+            else if (key == "temp") ckt.options.temp = val;  // kelvin
         } else {
             throw std::invalid_argument("unknown line kind: " + kind);
         }

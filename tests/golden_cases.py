@@ -157,7 +157,7 @@ def load_sens():
 def param_starts(netlist):
     """(kind, first parameter index) of every device of a Netlist, in
     creation order (the layout of Circuit.params())."""
-    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 14, "M": 43}
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 15, "M": 43}
     out, at = [], 0
     for d in netlist.devices:
         k = d[0]

@@ -62,12 +62,13 @@ def test_unsupported_card_parameter_is_refused():
         c.M4(0, 1, -1, -1, m, W=1e-6, L_=-1e-7)
 
 
-def _eval_sequence(nl, rng, dt=1e-12):
+def _eval_sequence(nl, rng, dt=1e-12, temp=None):
     """Ten device evaluations as a DC solve, the transient seeding, backward
     Euler, trapezoidal and Gear-2 steps would run them (INITJCT, INITFLOAT,
-    INITTRAN, INITPRED), at random guesses with every terminal bias sign;
-    returns (ours, reference) lists of (matrix, rhs)."""
-    c = nl.build()
+    INITTRAN, INITPRED), at random guesses with every terminal bias sign
+    (at circuit temperature `temp` kelvin when given); returns (ours,
+    reference) lists of (matrix, rhs)."""
+    c = nl.build(temp=temp)
     n = c.info()["num_vars"]
     nn = nl.num_nodes
 
@@ -89,7 +90,8 @@ def _eval_sequence(nl, rng, dt=1e-12):
              (1, 0x2001, guess(), trap), (0, 0x101, guess(), trap),
              (1, 0x2001, guess(), gear), (0, 0x101, guess(), gear)]
     ops, modes, xs, ctx = (np.array([s[k] for s in steps]) for k in range(4))
-    rv, rr = oracle.ref_sim_eval_seq(netlists.ref_desc(nl), ops, modes, xs.astype(float),
+    rv, rr = oracle.ref_sim_eval_seq(netlists.ref_desc(nl, None if temp is None else {"temp": temp}),
+                                     ops, modes, xs.astype(float),
                                      ctx.astype(float))
     ns = c.state_count()
     st = np.zeros(3 * ns)

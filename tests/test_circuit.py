@@ -237,11 +237,11 @@ def test_device_methods_return_parameter_index():
     assert c.V(0, -1, 1.0) == 3
     assert c.VPULSE(2, -1, 0.0, 1.0, 1e-9) == 4
     assert c.D(2, -1) == 11
-    assert c.I(-1, 1, 1e-3) == 25  # a diode holds 14 values
+    assert c.I(-1, 1, 1e-3) == 26  # a diode holds 15 values
     c.finalize()
     p = c.params()
-    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[25] == 1e-3
-    assert c.param_count() == len(p) == 26
+    assert p[0] == 10.0 and p[1] == 1e-12 and p[3] == 1.0 and p[26] == 1e-3
+    assert c.param_count() == len(p) == 27
 
 
 def _diode_netlists():

@@ -61,7 +61,7 @@ def check_against_fd(nls, b, tg, probes, floor_rel=5e-12, h_rel=1e-6, resolved_b
     g = g.cpu().numpy()
     nl = nls[0]
     starts, at = [], 0
-    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 14, "M": 43}
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 15, "M": 43}
     for d in nl.devices:
         starts.append((d[0], at))
         at += sizes[d[0]]
@@ -210,7 +210,7 @@ def test_tran_adjoint_with_diode_charge(case):
     torch.cuda.synchronize()
     assert int(st.abs().sum()) == 0 and float(loss[0]) > 0
     grads = grads.cpu().numpy()
-    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 14, "M": 43}
+    sizes = {"R": 1, "C": 2, "V": 1, "I": 1, "VPULSE": 7, "IPULSE": 7, "D": 15, "M": 43}
     idx, at = [], 0
     for d in nl.devices:
         if d[0] in ("R", "C"):
