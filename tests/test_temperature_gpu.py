@@ -33,6 +33,8 @@ def test_step_temp_dc_matches_reference(which):
 
 def test_step_temp_transient_matches_reference():
     nl = mos_net(11)
+    for name in ("nch", "pch"):  # moderate gate charge: a full transient in the reference
+        nl.models[name][1].update({"TOX": 1e-6, "CGSO": 2e-11, "CGDO": 2e-11})
     temps = step_values(-40.0, 125.0, 82.5)
     tstep, tstop = 1e-12, 2e-10
     refs = [oracle.ref_sim(netlists.ref_desc(nl, {"temp": t + 273.15}), 1, tstep, tstop)
