@@ -17,5 +17,5 @@ def ref_desc(netlist, options=None) -> str:
         lines.append(" ".join([d[0]] + [repr(int(x)) for x in d[1:3]] +
                               [repr(float(x)) for x in d[3:]]))
     for k, v in (options or {}).items():
-        lines.append(f"OPT {k} {v!r}")
+        lines.append(f"OPT {k} {float(v)!r}")  # plain float repr (not numpy's np.float64(...))
     return "\n".join(lines) + "\n"
