@@ -14,6 +14,12 @@ per-instance results) after the timed region.
 * ``max_over_ranks(values)``: the element-wise maximum across ranks of a few
   host doubles (timings), via torch.distributed on whatever backend the
   process group uses (NCCL on GPUs, gloo on CPU).
+* ``run_partitioned(costs, run)``: strong scaling of a fixed global batch:
+  this rank runs ``run(indices)`` on its share and every rank receives all
+  results in global instance order (one gather after the work).
+* ``dc_solve_global(circuits, costs)``: the batched DC operating point of a
+  fixed global list of circuits split across the process group's ranks,
+  each rank solving its share on its own GPU.
 """
 from __future__ import annotations
 
@@ -51,3 +57,51 @@ def max_over_ranks(values):
     t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return [float(x) for x in t.cpu()]
+
+
+def run_partitioned(costs, run):
+    """Run a fixed global batch across the process group: this rank calls
+    ``run(indices)`` on its share of ``partition(costs, world)`` (a list of
+    per-instance results, in the order of ``indices``), and the results of
+    every rank are gathered (all_gather_object, host objects) into one list
+    in global instance order, returned on every rank.  Without a process
+    group (or with one rank) it is ``run(range(len(costs)))``."""
+    import torch.distributed as dist
+    n = len(costs)
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return list(run(list(range(n))))
+    world, rank = dist.get_world_size(), dist.get_rank()
+    mine = partition(costs, world)[rank]
+    local = list(run(mine)) if mine else []
+    if len(local) != len(mine):
+        raise ValueError("run returned a result count different from its indices")
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (mine, local))
+    out = [None] * n
+    for idx, res in gathered:
+        for i, r in zip(idx, res):
+            out[i] = r
+    return out
+
+
+def dc_solve_global(circuits, costs=None, symbolic=None):
+    """Operating points of a fixed global list of finalized circuits split
+    across the ranks (each rank solves its share as one DcBatch on its
+    current GPU); returns, on every rank, a list of (solution as a numpy
+    array, status, Newton iterations) in global order.  ``costs`` default to
+    each circuit's nnz (a proxy for its LU work)."""
+    import torch
+    from .circuit import DcBatch
+    if costs is None:
+        costs = [float(c.info()["nnz"]) for c in circuits]
+
+    def run(indices):
+        batch = DcBatch([circuits[i] for i in indices],
+                        symbolic=DcBatch.PER_INSTANCE if symbolic is None else symbolic)
+        sols, status, iters = batch.run()
+        torch.cuda.synchronize()
+        st, it = status.cpu().numpy(), iters.cpu().numpy()
+        return [(s.cpu().numpy() if hasattr(s, "cpu") else s, int(st[k]), int(it[k]))
+                for k, s in enumerate(batch.split(sols))]
+
+    return run_partitioned(costs, run)

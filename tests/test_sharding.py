@@ -1,7 +1,8 @@
 """Multi-rank host logic on CPU (gloo, world size 2): instance partitioning
 covers every instance exactly once and balances the estimated cost, ranks
-generate distinct weak-scaling batches, and the timing reduction returns the
-maximum over ranks on every rank."""
+generate distinct weak-scaling batches, the timing reduction returns the
+maximum over ranks on every rank, and a partitioned fixed batch gathers
+every rank's results in global order on every rank."""
 import os
 
 import numpy as np
@@ -36,7 +37,11 @@ def _worker(rank, world, port, out):
         # each rank's stand-in for its device time; the job time is the max
         mx = sharding.max_over_ranks([1.0 + rank, 10.0 - rank])
         parts = sharding.partition([float(s * s) for s in range(20)], world)
-        out.put((rank, sizes, mx, parts[rank]))
+        # strong scaling of a fixed batch: each rank runs its share, all
+        # results come back in global order on every rank
+        gathered = sharding.run_partitioned([float(s * s) for s in range(20)],
+                                            lambda idx: [(i * i, rank) for i in idx])
+        out.put((rank, sizes, mx, parts[rank], gathered))
     finally:
         dist.destroy_process_group()
 
@@ -53,7 +58,10 @@ def test_two_rank_gloo():
         p.join(timeout=60)
         assert p.exitcode == 0
     res.sort()
-    (_, s0, m0, p0), (_, s1, m1, p1) = res
+    (_, s0, m0, p0, g0), (_, s1, m1, p1, g1) = res
     assert s0 != s1                      # distinct per-rank batches
     assert m0 == m1 == [2.0, 10.0]       # max over ranks, on both ranks
     assert sorted(p0 + p1) == list(range(20))
+    assert g0 == g1                      # the gathered results, on both ranks
+    assert [v for v, _ in g0] == [i * i for i in range(20)]
+    assert [r for _, r in g0] == [0 if i in p0 else 1 for i in range(20)]
