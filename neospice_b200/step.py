@@ -99,3 +99,31 @@ def sweep_transient_temperature(build, temps_celsius, tstep: float, tstop: float
                   np.asarray(probes, np.int32), max_points=max_points)
     b.run()
     return b.results()
+
+
+def sweep_dc_multi(circuit: Circuit, params, values, symbolic=DcBatch.PER_PATTERN):
+    """`.step PARAM` of an operating point: a `.param` may enter several
+    device values, and the reference re-parses the netlist per step value
+    (src/api/neospice.cpp:258-290); here the caller gives, per step, the
+    values those devices take (`values` [steps x len(params)] for the
+    parameter indices `params` of Circuit.params()), and every step is one
+    instance of one batched launch.  Returns (solutions [steps, n], status,
+    iterations)."""
+    import torch
+
+    params = [int(p) for p in params]
+    values = np.asarray(values, np.float64).reshape(-1, len(params))
+    base = circuit.params()
+    for p in params:
+        if not 0 <= p < len(base):
+            raise IndexError(f"parameter {p} out of range (circuit has {len(base)})")
+    batch = DcBatch([circuit] * len(values), symbolic=symbolic)
+    off = batch.param_offsets
+    flat = np.zeros(int(off[-1]), np.float64)
+    for i, row in enumerate(values):
+        flat[off[i]:off[i + 1]] = base
+        for p, v in zip(params, row):
+            flat[off[i] + p] = v
+    sols, status, iters = batch.run(torch.from_numpy(flat).cuda())
+    torch.cuda.synchronize()
+    return (np.stack(batch.split(sols)), status.cpu().numpy(), iters.cpu().numpy())
