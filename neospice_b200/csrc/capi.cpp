@@ -193,6 +193,7 @@ nsg::PlanDesc make_plan_desc(const nsg::TopologyPlan& p, std::vector<int32_t>& p
     d.nnz_u = p.urow_ptr[p.n];
     d.kind = p.kind;
     d.has_map = p.has_update_map ? 1 : 0;
+    d.map16 = p.map16() ? 1 : 0;
     // grow geometrically once for this plan, so a multi-gigabyte update map
     // is copied once (appending to an unreserved pool re-copies it)
     const size_t need = pool.size() + static_cast<size_t>(p.device_words()) + 4 * nsg::PA_COUNT + 4;

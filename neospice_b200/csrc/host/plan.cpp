@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <functional>
 #include <stdexcept>
 #include <string>
@@ -240,9 +241,35 @@ void finish(TopologyPlan& p) {
     X(bwd_lev_ptr) X(bwd_lev) X(tbw_lev_ptr) X(tbw_lev) X(rowcopy_pos) X(umeta) \
     X(piv_rank) X(gmin_pos)
 
+namespace {
+template <class V>
+bool is_update_map(const TopologyPlan& p, const V& v) {
+    return static_cast<const void*>(&v) == static_cast<const void*>(&p.upd_dst);
+}
+
+// v's values (each below 65,536) as consecutive uint16, in ceil(|v| / 2)
+// words; the last half word of an odd count is zero.
+template <class V>
+void append_packed16(std::vector<int32_t>& pool, const V& v) {
+    const size_t at = pool.size();
+    pool.resize(at + (v.size() + 1) / 2, 0);
+    char* out = reinterpret_cast<char*>(pool.data() + at);
+    uint16_t chunk[4096];
+    for (size_t k0 = 0; k0 < v.size(); k0 += 4096) {
+        const size_t m = std::min<size_t>(4096, v.size() - k0);
+        for (size_t k = 0; k < m; ++k) chunk[k] = static_cast<uint16_t>(v[k0 + k]);
+        std::memcpy(out + 2 * k0, chunk, 2 * m);
+    }
+}
+}  // namespace
+
+// A packed update map takes one int32 word per two positions.
 int64_t TopologyPlan::device_words() const {
     int64_t w = 0;
-#define NSG_COUNT(name) w += static_cast<int64_t>(name.size()) + 4;  // 16 B align
+#define NSG_COUNT(name)                                                          \
+    w += (is_update_map(*this, name) && map16() ? (static_cast<int64_t>(name.size()) + 1) / 2 \
+                                                 : static_cast<int64_t>(name.size())) +       \
+         4;  // 16 B align
     NSG_PLAN_ARRAYS(NSG_COUNT)
 #undef NSG_COUNT
     return w;
@@ -250,10 +277,15 @@ int64_t TopologyPlan::device_words() const {
 
 void TopologyPlan::append_to(std::vector<int32_t>& pool, int64_t* off) const {
     int idx = 0;
+    const bool pack = map16();
 #define NSG_APPEND(name)                                          \
     while (pool.size() % 4) pool.push_back(0);                    \
     off[idx++] = static_cast<int64_t>(pool.size());               \
-    pool.insert(pool.end(), name.begin(), name.end());
+    if (pack && is_update_map(*this, name)) {                     \
+        append_packed16(pool, name);                              \
+    } else {                                                      \
+        pool.insert(pool.end(), name.begin(), name.end());        \
+    }
     NSG_PLAN_ARRAYS(NSG_APPEND)
 #undef NSG_APPEND
 }

@@ -119,8 +119,12 @@ struct TopologyPlan {
     // Compulsory bytes of one refactor: read A, write LU, the index stream
     // (update map + LU pattern), the reciprocal diagonal.
     int64_t refactor_bytes() const {
-        return 8LL * nnz_a + 8LL * nnz_lu + 4LL * (updates + nnz_lu + n) + 8LL * n;
+        return 8LL * nnz_a + 8LL * nnz_lu + (map16() ? 2LL : 4LL) * updates +
+               4LL * (nnz_lu + n) + 8LL * n;
     }
+    // The device copy of the update map is packed as uint16 positions when
+    // every column is short enough for them.
+    bool map16() const { return has_update_map && max_col <= 65536; }
     int64_t solve_bytes() const { return 12LL * nnz_lu + 16LL * n; }
 
     // Total int32 words this plan occupies on the device.

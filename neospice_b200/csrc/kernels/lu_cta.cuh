@@ -258,7 +258,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
     __syncwarp();
     // Position in column j of entry t of L(:, r) (its k-th update).
     auto dest = [&](int32_t us, int32_t l0, int32_t t) -> int32_t {
-        return mapped ? upd_dst[us + t] : rmap[row_idx[l0 + t]];
+        return mapped ? upd_at(upd_dst, pd.map16, us + t) : rmap[row_idx[l0 + t]];
     };
     double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
     // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
@@ -619,7 +619,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
                         colmax = fmax(colmax, fabs(u));
                         lu_s[c0 + q] = u;
                         for (int32_t t = 0; t < m.z; ++t) {
-                            const int32_t d = c0 + upd_dst[m.w + t];
+                            const int32_t d = c0 + upd_at(upd_dst, pd.map16, m.w + t);
                             lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
                         }
                     }
@@ -633,7 +633,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
                     }
                     u = __shfl_sync(0xffffffffu, u, 0);
                     for (int32_t t = lane; t < m.z; t += 32) {
-                        const int32_t d = c0 + upd_dst[m.w + t];
+                        const int32_t d = c0 + upd_at(upd_dst, pd.map16, m.w + t);
                         lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
                     }
                     __syncwarp();

@@ -21,9 +21,21 @@ struct PlanDesc {
     int32_t nnz_l, nnz_u;  // strictly lower / upper entries
     int32_t kind;          // kPlanMarkowitz or kPlanAmdLu
     int32_t has_map;       // 1: PA_upd_start / PA_upd_dst hold the update map
+    int32_t map16;         // 1: the update map is packed as uint16 positions
+                           // (every column is shorter than 65,537 rows)
     int64_t off[PA_COUNT];  // int32-word offsets into the plan pool
     int64_t words;          // words from off[0] that hold all of the plan's arrays
 };
+
+#ifdef __CUDACC__
+// Entry k of a plan's update map: the position in column j that update k
+// of U(r, j) writes.  Packed plans (map16) hold it in 16 bits, halving the
+// map reads of the refactor; the values are the same.
+__device__ __forceinline__ int32_t upd_at(const int32_t* upd_dst, int32_t map16, int64_t k) {
+    return map16 ? static_cast<int32_t>(reinterpret_cast<const uint16_t*>(upd_dst)[k])
+                 : upd_dst[k];
+}
+#endif
 
 struct InstDesc {
     int32_t plan;   // index into the PlanDesc array

@@ -175,8 +175,17 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
         const int32_t pairs = (off + ns) >> 1;
         for (int32_t p = tid; p < pairs; p += kThreads)
             cp_async16_cg(&ring.val[slot][2 * p], g0 + 2 * p);
-        const int32_t* src = mapped ? upd_dst + m.w : row_idx + l0;
-        for (int32_t k = tid; k < ns; k += kThreads) cp_async4_ca(&ring.dst[slot][k], src + k);
+        if (mapped && pd.map16) {
+            // packed map: the words holding positions m.w .. m.w + ns - 1,
+            // from the even position at or below m.w (4-byte aligned)
+            const int32_t* src = reinterpret_cast<const int32_t*>(
+                reinterpret_cast<const uint16_t*>(upd_dst) + (m.w & ~1));
+            const int32_t words = ((m.w & 1) + ns + 1) >> 1;
+            for (int32_t k = tid; k < words; k += kThreads) cp_async4_ca(&ring.dst[slot][k], src + k);
+        } else {
+            const int32_t* src = mapped ? upd_dst + m.w : row_idx + l0;
+            for (int32_t k = tid; k < ns; k += kThreads) cp_async4_ca(&ring.dst[slot][k], src + k);
+        }
         cp_async_commit();
     };
     double colmax = 0.0;  // the same in every thread: largest |U(r, j)| applied
@@ -222,13 +231,16 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
         const double u = buf[q];
         colmax = fmax(colmax, fabs(u));
         const bool tail = ((off + ns) & 1) != 0;
+        const uint16_t* dst16 = reinterpret_cast<const uint16_t*>(ring.dst[slot]) + (m.w & 1);
+        const bool packed = mapped && pd.map16;
         for (int32_t k = tid; k < ns; k += kThreads) {
             const double lv = (tail && k == ns - 1) ? __ldcg(lu + l0 + k) : ring.val[slot][off + k];
-            const int32_t d = mapped ? ring.dst[slot][k] : rmap[ring.dst[slot][k]];
+            const int32_t d = packed ? static_cast<int32_t>(dst16[k])
+                                     : (mapped ? ring.dst[slot][k] : rmap[ring.dst[slot][k]]);
             buf[d] = lu_sub(buf[d], lu_mul(u, lv));
         }
         for (int32_t k = ns + tid; k < m.z; k += kThreads) {
-            const int32_t d = mapped ? upd_dst[m.w + k] : rmap[row_idx[l0 + k]];
+            const int32_t d = mapped ? upd_at(upd_dst, pd.map16, m.w + k) : rmap[row_idx[l0 + k]];
             buf[d] = lu_sub(buf[d], lu_mul(u, __ldcg(lu + l0 + k)));
         }
         __syncthreads();  // the column's new values before the next u; slot q free

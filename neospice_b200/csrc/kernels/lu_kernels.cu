@@ -98,10 +98,10 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
                 if (lane == 0) lu[q] = u;
                 const int32_t l0 = diag_pos[r] + 1;
                 const int32_t cnt = col_ptr[r + 1] - l0;
-                const int32_t* dst = upd_dst + upd_start[q];
+                const int32_t us = upd_start[q];
                 const int32_t c0 = col_ptr[j];
                 for (int32_t t = lane; t < cnt; t += 32) {
-                    const int32_t d = c0 + dst[t];
+                    const int32_t d = c0 + upd_at(upd_dst, pd.map16, us + t);
                     lu[d] = sub(lu[d], mul(u, lu[l0 + t]));
                 }
                 __syncwarp();

@@ -2,12 +2,14 @@
 // several host threads) equals the map recomputed here one column after
 // another: for every U(r, j), the positions in column j of the rows of
 // L(:, r).  A 5-point resistor-grid Laplacian of side 160 (about 1e8
-// updates) takes the multi-threaded path.  Prints "0 failure(s)" on success.
+// updates) takes the multi-threaded path.  The device pool holds the map
+// packed as uint16 positions.  Prints "0 failure(s)" on success.
 #include "host/amd_lu.hpp"
 #include "host/plan.hpp"
 
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 int main() {
@@ -54,6 +56,34 @@ int main() {
             }
         }
         for (int32_t q = p.col_ptr[j]; q < p.col_ptr[j + 1]; ++q) where[p.row_idx[q]] = -1;
+    }
+    // The device copy: every column is short, so the map is packed as
+    // uint16 positions; device_words() is the pool's exact size.
+    if (!p.map16()) {
+        std::printf("plan not packed (longest column %d)\n", p.max_col);
+        ++failures;
+    }
+    std::vector<int32_t> pool;
+    int64_t off[32] = {};
+    p.append_to(pool, off);
+    if (static_cast<int64_t>(pool.size()) > p.device_words()) {
+        std::printf("pool %zu words, device_words %lld\n", pool.size(),
+                    static_cast<long long>(p.device_words()));
+        ++failures;
+    }
+    const int upd_dst_array = 7;  // position of upd_dst in the pool's array order
+    std::vector<uint16_t> packed(p.upd_dst.size());
+    std::memcpy(packed.data(), pool.data() + off[upd_dst_array], 2 * packed.size());
+    for (size_t k = 0; k < packed.size() && failures < 10; ++k)
+        if (packed[k] != p.upd_dst[k]) {
+            std::printf("packed map mismatch at update %zu\n", k);
+            ++failures;
+        }
+    if (off[upd_dst_array + 1] - off[upd_dst_array] != ((int64_t(packed.size()) + 1) / 2 + 3) / 4 * 4) {
+        std::printf("packed map region %lld words for %zu positions\n",
+                    static_cast<long long>(off[upd_dst_array + 1] - off[upd_dst_array]),
+                    packed.size());
+        ++failures;
     }
     if (at != p.updates) {
         std::printf("update count %lld, plan says %lld\n", static_cast<long long>(at),
