@@ -1062,7 +1062,10 @@ def power_grid_refactor(side, reps, warmup):
     t_sol = ev[1].elapsed_time(ev[2]) / 1e3 / reps
     x = d_x.cpu().numpy()
     nnz, nlu, upd = len(ri), info["nnz_lu"], info["updates"]
-    b_ref = 8 * nnz + 8 * nlu + 4 * (upd + nlu + n) + 8 * n
+    # the device update map holds uint16 positions when every LU column is
+    # shorter than 65,537 rows, else int32
+    map_b = 2 if int(np.bincount(topo.export()[3]).max()) <= 65536 else 4
+    b_ref = 8 * nnz + 8 * nlu + map_b * upd + 4 * (nlu + n) + 8 * n
     b_sol = 12 * nlu + 16 * n
     peak, peak_kind = measured_peaks()
     out = {

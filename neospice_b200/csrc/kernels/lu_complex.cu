@@ -56,6 +56,7 @@ complex_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __res
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int32_t map16 = pd.map16;
     const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]);
     const double* a = A + 2 * id.a_off;
     double* lu = LU + 2 * id.lu_off;
@@ -111,7 +112,7 @@ complex_refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __res
             }
             const double* lcol = lu + 2 * (static_cast<int64_t>(m.y) + 1);
             for (int32_t t = lane; t < m.z; t += 32) {
-                const int32_t dst = upd_at(upd_dst, pd.map16, m.w + t);
+                const int32_t dst = upd_at(upd_dst, map16, m.w + t);
                 const double lr = lcol[2 * t], li = lcol[2 * t + 1];
                 col[2 * dst] = __dsub_rn(col[2 * dst], c_re(ur, ui, lr, li));
                 col[2 * dst + 1] = __dsub_rn(col[2 * dst + 1], c_im(ur, ui, lr, li));

@@ -237,6 +237,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int32_t map16 = pd.map16;
     const bool amd = pd.kind == kPlanAmdLu;
     const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
     const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
@@ -258,7 +259,7 @@ __device__ __forceinline__ ColumnResult refactor_column(
     __syncwarp();
     // Position in column j of entry t of L(:, r) (its k-th update).
     auto dest = [&](int32_t us, int32_t l0, int32_t t) -> int32_t {
-        return mapped ? upd_at(upd_dst, pd.map16, us + t) : rmap[row_idx[l0 + t]];
+        return mapped ? upd_at(upd_dst, map16, us + t) : rmap[row_idx[l0 + t]];
     };
     double colmax = 0.0;  // AMD-LU: largest |U(r, j)| applied
     // U-entry metadata {r, diag_pos[r], |L(:,r)|, upd_start} is held 32
@@ -576,6 +577,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int32_t map16 = pd.map16;
     const int4* umeta = reinterpret_cast<const int4*>(pool + pd.off[PA_umeta]);
     const bool amd = pd.kind == kPlanAmdLu;
     const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
@@ -619,7 +621,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
                         colmax = fmax(colmax, fabs(u));
                         lu_s[c0 + q] = u;
                         for (int32_t t = 0; t < m.z; ++t) {
-                            const int32_t d = c0 + upd_at(upd_dst, pd.map16, m.w + t);
+                            const int32_t d = c0 + upd_at(upd_dst, map16, m.w + t);
                             lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
                         }
                     }
@@ -633,7 +635,7 @@ static __device__ __noinline__ RefactorResult cta_refactor_small(
                     }
                     u = __shfl_sync(0xffffffffu, u, 0);
                     for (int32_t t = lane; t < m.z; t += 32) {
-                        const int32_t d = c0 + upd_at(upd_dst, pd.map16, m.w + t);
+                        const int32_t d = c0 + upd_at(upd_dst, map16, m.w + t);
                         lu_s[d] = lu_sub(lu_s[d], lu_mul(u, lu_s[m.y + 1 + t]));
                     }
                     __syncwarp();

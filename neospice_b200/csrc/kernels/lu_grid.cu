@@ -138,6 +138,7 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
     const int32_t* diag_pos = pool + pd.off[PA_diag_pos];
     const int32_t* lu_src = pool + pd.off[PA_lu_src];
     const int32_t* upd_dst = pool + pd.off[PA_upd_dst];
+    const int32_t map16 = pd.map16;
     const int32_t* row_idx = pool + pd.off[PA_row_idx];
     const int32_t* piv_rank = pool + pd.off[PA_piv_rank];
     const int32_t* gmin_pos = pool + pd.off[PA_gmin_pos];
@@ -175,7 +176,7 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
         const int32_t pairs = (off + ns) >> 1;
         for (int32_t p = tid; p < pairs; p += kThreads)
             cp_async16_cg(&ring.val[slot][2 * p], g0 + 2 * p);
-        if (mapped && pd.map16) {
+        if (mapped && map16) {
             // packed map: the words holding positions m.w .. m.w + ns - 1,
             // from the even position at or below m.w (4-byte aligned)
             const int32_t* src = reinterpret_cast<const int32_t*>(
@@ -232,7 +233,7 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
         colmax = fmax(colmax, fabs(u));
         const bool tail = ((off + ns) & 1) != 0;
         const uint16_t* dst16 = reinterpret_cast<const uint16_t*>(ring.dst[slot]) + (m.w & 1);
-        const bool packed = mapped && pd.map16;
+        const bool packed = mapped && map16;
         for (int32_t k = tid; k < ns; k += kThreads) {
             const double lv = (tail && k == ns - 1) ? __ldcg(lu + l0 + k) : ring.val[slot][off + k];
             const int32_t d = packed ? static_cast<int32_t>(dst16[k])
@@ -240,7 +241,7 @@ __device__ ColumnResult refactor_column_cta(const PlanDesc& pd, const int32_t* _
             buf[d] = lu_sub(buf[d], lu_mul(u, lv));
         }
         for (int32_t k = ns + tid; k < m.z; k += kThreads) {
-            const int32_t d = mapped ? upd_at(upd_dst, pd.map16, m.w + k) : rmap[row_idx[l0 + k]];
+            const int32_t d = mapped ? upd_at(upd_dst, map16, m.w + k) : rmap[row_idx[l0 + k]];
             buf[d] = lu_sub(buf[d], lu_mul(u, __ldcg(lu + l0 + k)));
         }
         __syncthreads();  // the column's new values before the next u; slot q free

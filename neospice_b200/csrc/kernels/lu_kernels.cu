@@ -55,6 +55,7 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
     const int32_t* lu_src = p[PA_lu_src];
     const int32_t* upd_start = p[PA_upd_start];
     const int32_t* upd_dst = p[PA_upd_dst];
+    const int32_t map16 = pd.map16;
     const int32_t* lev_ptr = p[PA_col_lev_ptr];
     const int32_t* lev = p[PA_col_lev];
     const double* a = A + inst.a_off;
@@ -101,7 +102,7 @@ refactor_kernel(const PlanDesc* __restrict__ plans, const int32_t* __restrict__ 
                 const int32_t us = upd_start[q];
                 const int32_t c0 = col_ptr[j];
                 for (int32_t t = lane; t < cnt; t += 32) {
-                    const int32_t d = c0 + upd_at(upd_dst, pd.map16, us + t);
+                    const int32_t d = c0 + upd_at(upd_dst, map16, us + t);
                     lu[d] = sub(lu[d], mul(u, lu[l0 + t]));
                 }
                 __syncwarp();
